@@ -1,0 +1,1129 @@
+// fgpu_host.cu -- C ABI of the B200 backend (include/fosite_gpu.h): config
+// validation, host-side metric precompute, device memory, and the two time
+// integration drivers:
+//   * Shu-Osher "modified Euler" (timedisc_modeuler.f90, fixed step): fully
+//     device-resident -- dt, time and the stop/break flags live in a device
+//     control block, each step is a fixed kernel sequence replayed from a
+//     captured CUDA graph;
+//   * embedded Butcher engine (timedisc_rkfehlberg.f90 with the Dormand-Prince,
+//     Fehlberg, Cash-Karp and SSPRK tableaus): one stage kernel per stage, the
+//     accept/reject logic of IntegrationStep (timedisc_base.f90:649-750) runs on
+//     the host after one 8-byte read of the error norm per attempt.
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cfloat>
+#include <cstring>
+#include <cstdio>
+#include <string>
+#include <vector>
+#include <algorithm>
+#include "../../include/fosite_gpu.h"
+#include "fgpu_kernels_misc.cuh"
+
+using namespace fgpu;
+
+namespace {
+
+std::string g_create_error;
+
+struct Tableau {
+  int m = 0, order = 0;
+  std::vector<double> A, bh, bl, c;
+};
+
+bool make_tableau(int method, int order, Tableau& T) {
+  auto set = [&](int m, int o, std::initializer_list<double> bh, std::initializer_list<double> bl,
+                 std::initializer_list<double> c, std::initializer_list<double> a) {
+    T.m = m; T.order = o; T.bh = bh; T.bl = bl; T.c = c; T.A = a;
+  };
+  // timedisc_dormand_prince.f90:91-114
+  if (method == FGPU_DORMAND_PRINCE && order == 5) {
+    set(7, 5, {35./384., 0., 500./1113., 125./192., -2187./6784., 11./84., 0.},
+        {5179./57600., 0., 7571./16695., 393./640., -92097./339200., 187./2100., 1./40.},
+        {0., .2, 3./10., 4./5., 8./9., 1., 1.},
+        {0., 0., 0., 0., 0., 0., 0.,
+         .2, 0., 0., 0., 0., 0., 0.,
+         3./40., 9./40., 0., 0., 0., 0., 0.,
+         44./45., -56./15., 32./9., 0., 0., 0., 0.,
+         19372./6561., -25360./2187., 64448./6561., -212./729., 0., 0., 0.,
+         9017./3168., -355./33., 46732./5247., 49./176., -5103./18656., 0., 0.,
+         35./384., 0., 500./1113., 125./192., -2187./6784., 11./84., 0.});
+    return true;
+  }
+  // timedisc_rkfehlberg.f90:305-335
+  if (method == FGPU_RK_FEHLBERG && order == 3) {
+    set(3, 3, {1.0/6.0, 2.0/3.0, 1.0/6.0}, {0.0, 1.0, 0.0}, {0.0, 0.5, 1.0},
+        {0.0, 0.0, 0.0, 0.5, 0.0, 0.0, -1.0, 2.0, 0.0});
+    return true;
+  }
+  if (method == FGPU_RK_FEHLBERG && order == 5) {
+    set(6, 5, {16.0/135.0, 0.0, 6656.0/12825.0, 28561.0/56430.0, -9.0/50.0, 2.0/55.0},
+        {25.0/216.0, 0.0, 1408.0/2565.0, 2197.0/4104.0, -0.2, 0.0},
+        {0.0, 0.25, 3.0/8.0, 12.0/13.0, 1.0, 0.5},
+        {0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+         0.25, 0.0, 0.0, 0.0, 0.0, 0.0,
+         3.0/32.0, 9.0/32.0, 0.0, 0.0, 0.0, 0.0,
+         1932.0/2197.0, -7200.0/2197.0, 7296.0/2197.0, 0.0, 0.0, 0.0,
+         439.0/216.0, -8.0, 3680.0/513.0, -845.0/4104.0, 0.0, 0.0,
+         -8.0/27.0, 2.0, -3544.0/2565.0, 1859.0/4104.0, -11.0/40.0, 0.0});
+    return true;
+  }
+  // timedisc_cashkarp.f90:95-117
+  if (method == FGPU_CASH_KARP && order == 5) {
+    set(6, 5, {37.0/378.0, 0.0, 250.0/621.0, 125.0/594.0, 0.0, 512.0/1771.0},
+        {2825.0/27648.0, 0.0, 18575.0/48384.0, 13525.0/55296.0, 277.0/14336.0, 0.25},
+        {0.0, 0.2, 0.3, 0.6, 1.0, 7.0/8.0},
+        {0.0, 0.0, 0.0, 0.0, 0.0, 0.0,
+         0.2, 0.0, 0.0, 0.0, 0.0, 0.0,
+         0.075, 0.225, 0.0, 0.0, 0.0, 0.0,
+         0.3, -0.9, 1.2, 0.0, 0.0, 0.0,
+         -11.0/54.0, 2.5, -70.0/27.0, 35.0/27.0, 0.0, 0.0,
+         1631.0/55296.0, 175.0/512.0, 575.0/13824.0, 44275.0/110592.0, 253.0/4096.0, 0.0});
+    return true;
+  }
+  // timedisc_ssprk.f90:93-126
+  if (method == FGPU_SSPRK && order == 3) {
+    set(3, 3, {1./6., 1./6., 2./3.}, {0.5, 0.5, 0.}, {0., 1., 0.5},
+        {0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.25, 0.25, 0.0});
+    return true;
+  }
+  if (method == FGPU_SSPRK && order == 5) {
+    set(5, 5, {0.17279, 0.094505, 0.12947, 0.29899, 0.30424},
+        {0.12293, 0.31981, -0.15316, 0.31887, 0.39155},
+        {0., 0.36717, 0.58522, 0.44156, 0.8464},
+        {0., 0., 0., 0., 0.,
+         0.36717, 0., 0., 0., 0.,
+         0.26802, 0.3172, 0., 0., 0.,
+         0.11606, 0.13735, 0.18816, 0., 0.,
+         0.11212, 0.13269, 0.18178, 0.4198, 0.});
+    return true;
+  }
+  return false;
+}
+
+}  // namespace
+
+struct fgpu_handle {
+  fgpu_config cfg;
+  std::string err;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int nd = 2, V = 4;
+  bool euler = true, prim = false, roundtrip_cfg = false, curv = false, has_accel = false;
+  Grid g;
+  PhysP ph;
+  MetricP mt;
+  double invd[3];
+  double* d_metric = nullptr;
+  std::vector<double> h_metric;
+  int nxp = 0;
+  // state buffers: [0] P (stored state), then scheme-specific
+  std::vector<double*> buf;
+  double* d_pad = nullptr;      // padded download scratch (2 * npad * V)
+  long long npad = 0;
+  Ctl* d_ctl = nullptr;
+  Ctl* h_ctl = nullptr;         // pinned
+  // timedisc
+  bool butcher = false;
+  int order = 3;
+  Tableau T;
+  double tol_rel, beta, cfl, dtlimit, stoptime, tout;
+  double tol_abs[FGPU_MAXVAR];
+  // host-side bookkeeping (Butcher engine) / mirror of the control block
+  double time = 0, dt = 0, dtold = 0, dtmin = 0, maxerrold = 0, last_err = 0;
+  int dtcause = 0;
+  bool brk = false;
+  long long iter = -1, n_adj = 0;
+  int checkflags = 0;
+  bool first_done = false;
+  bool state_pre = false;       // buffer P holds a state whose fosite cvar is its CHECK_PMIN round trip
+  // graph of G Shu-Osher steps
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+  // launch shape
+  int tile_x = 32, tile_y = 8, kchunk = 16;
+  // instrumentation
+  cudaStream_t own_stream = nullptr;
+  bool profiling = false;
+  struct Timed { cudaEvent_t a, b; double bytes; int stage; };
+  std::vector<Timed> timed;
+  fgpu_stats stats;
+  int kernels_per_step = 0;
+};
+
+namespace {
+
+int set_err(fgpu_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg; else g_create_error = msg;
+  return code;
+}
+#define CUDA_TRY(h, call)                                                                    \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return set_err(h, e_ == cudaErrorMemoryAllocation ? FGPU_ENOMEM : FGPU_ECUDA,          \
+                     std::string(#call) + ": " + cudaGetErrorString(e_));                    \
+  } while (0)
+
+// ---------------------------------------------------------------- metric
+// Restatement of mesh_base.f90:570-729 and mesh_midpoint.f90:97-145 for
+// geometries whose scale factors depend on the first coordinate only.
+void scale(int geo, double gp, double x, double& hx, double& hy, double& hz) {
+  if (geo == FGPU_CYLINDRICAL) { hx = 1.0; hy = x; hz = 1.0; }
+  else if (geo == FGPU_LOGCYLINDRICAL) { hx = gp * std::exp(x); hy = hx; hz = 1.0; }
+  else { hx = hy = hz = 1.0; }
+}
+
+enum { M_dAxW, M_dAyS, M_dAzB, M_dydzdV, M_dzdxdV, M_dxdydV, M_cxyx, M_cxzx, M_cyxy, M_cyzy, M_czxz, M_czyz,
+       M_dlx, M_dly, M_dlz, M_offxW, M_offxE, M_accel0, M_accel1, M_cs0, M_NI = M_cs0 + 7 };
+
+int build_metric(fgpu_handle* h) {
+  const fgpu_config& c = h->cfg;
+  int nx = c.inum, ny = c.jnum, nz = c.knum;
+  double dx = (c.xmax - c.xmin) / nx, mdx = dx;
+  double dy = (c.ymax - c.ymin) / ny, mdy = dy;
+  double dz = (c.zmax - c.zmin) / nz, mdz = dz;
+  if (dx < 2 * DBL_EPSILON) { if (nx == 1) { dx = 1.0; mdx = 0.0; } else return set_err(h, FGPU_EBADCFG, "INUM > 1 conflicts with zero x-extent"); }
+  if (dy < 2 * DBL_EPSILON) { if (ny == 1) { dy = 1.0; mdy = 0.0; } else return set_err(h, FGPU_EBADCFG, "JNUM > 1 conflicts with zero y-extent"); }
+  if (dz < 2 * DBL_EPSILON) { if (nz == 1) { dz = 1.0; mdz = 0.0; } else return set_err(h, FGPU_EBADCFG, "KNUM > 1 conflicts with zero z-extent"); }
+  h->invd[0] = 1. / dx; h->invd[1] = 1. / dy; h->invd[2] = 1. / dz;
+  int nxp = nx + 4, nyp = ny + 4, nzp = nz + 4;
+  h->nxp = nxp;
+  // layout: M_NI arrays of nxp, then offyS, offyN (nyp), offzB, offzT (nzp)
+  size_t base_y = (size_t)M_NI * nxp;
+  size_t total = base_y + 2 * (size_t)nyp + 2 * (size_t)nzp;
+  std::vector<double>& m = h->h_metric;
+  m.assign(total, 0.0);
+  auto A = [&](int which, int ip) -> double& { return m[(size_t)which * nxp + ip]; };
+  int geo = c.geometry;
+  double gp = c.gparam;
+  // the centre z coordinate of a 2D mesh (KNUM = 1): zmin + 0.5*0
+  double zc2d = c.zmin + ((double)(2 * 1 - 1) * 0.5) * mdz;
+  for (int ip = 0; ip < nxp; ++ip) {
+    int I = ip - 1;   // fosite 1-based index
+    double x = c.xmin + ((double)(2 * I - 1) * 0.5) * mdx;
+    double xw = x + (-0.5 * mdx), xe = x + 0.5 * mdx;
+    double hxc, hyc, hzc, hxw, hyw, hzw, hxe, hye, hze;
+    scale(geo, gp, x, hxc, hyc, hzc);
+    scale(geo, gp, xw, hxw, hyw, hzw);
+    scale(geo, gp, xe, hxe, hye, hze);
+    // S/N/B/T faces share the centre's first coordinate
+    double sqrtg = hxc * (hyc * hzc);
+    double volume = sqrtg * dx * dy * dz;
+    double dxdydV = dx * dy / (volume + DBL_MIN);
+    double dydzdV = dy * dz / (volume + DBL_MIN);
+    double dzdxdV = dz * dx / (volume + DBL_MIN);
+    A(M_dAxW, ip) = hyw * hzw;
+    A(M_dAyS, ip) = hzc * hxc;
+    A(M_dAzB, ip) = hxc * hyc;
+    A(M_dydzdV, ip) = dydzdV;
+    A(M_dzdxdV, ip) = dzdxdV;
+    A(M_dxdydV, ip) = dxdydV;
+    A(M_cyxy, ip) = 0.5 * (hze + hzw) * (hye - hyw) * dydzdV;
+    A(M_cyzy, ip) = 0.5 * (hxc + hxc) * (hyc - hyc) * dxdydV;
+    A(M_cxyx, ip) = 0.5 * (hzc + hzc) * (hxc - hxc) * dzdxdV;
+    A(M_cxzx, ip) = 0.5 * (hyc + hyc) * (hxc - hxc) * dxdydV;
+    A(M_czxz, ip) = 0.5 * (hye + hyw) * (hze - hzw) * dydzdV;
+    A(M_czyz, ip) = 0.5 * (hxc + hxc) * (hzc - hzc) * dzdxdV;
+    A(M_dlx, ip) = hxc * dx;
+    A(M_dly, ip) = hyc * dy;
+    A(M_dlz, ip) = hzc * dz;
+    A(M_offxW, ip) = xw - x;
+    A(M_offxE, ip) = xe - x;
+    if (h->has_accel) {
+      // gravity_pointmass.f90:263-282 with the point mass at the origin, NEWTON potential
+      double r, posx;
+      if (geo == FGPU_LOGCYLINDRICAL) { double rr = gp * std::exp(x); r = std::sqrt(rr * rr + zc2d * zc2d); posx = r; }
+      else { r = std::sqrt(x * x + zc2d * zc2d); posx = r; }
+      double om2 = 1. / std::max(10 * DBL_MIN, ((r * ((r - 0.0) * (r - 0.0))) + 0.0 * 0.0 * 0.0) / (c.gn * c.pm_mass));
+      A(M_accel0, ip) = -om2 * posx;
+      A(M_accel1, ip) = -om2 * 0.0;
+    }
+    if (!h->euler && c.csiso > 0.0)
+      for (int q = 0; q < 7; ++q) A(M_cs0 + q, ip) = c.csiso;
+  }
+  for (int jp = 0; jp < nyp; ++jp) {
+    int J = jp - 1;
+    double y = c.ymin + ((double)(2 * J - 1) * 0.5) * mdy;
+    m[base_y + jp] = (y + (-0.5 * mdy)) - y;
+    m[base_y + nyp + jp] = (y + 0.5 * mdy) - y;
+  }
+  for (int kp = 0; kp < nzp; ++kp) {
+    int K = kp - 1;
+    double z = c.zmin + ((double)(2 * K - 1) * 0.5) * mdz;
+    m[base_y + 2 * nyp + kp] = (z + (-0.5 * mdz)) - z;
+    m[base_y + 2 * nyp + nzp + kp] = (z + 0.5 * mdz) - z;
+  }
+  return FGPU_OK;
+}
+
+int upload_metric(fgpu_handle* h) {
+  size_t bytes = h->h_metric.size() * sizeof(double);
+  if (!h->d_metric) CUDA_TRY(h, cudaMalloc(&h->d_metric, bytes));
+  CUDA_TRY(h, cudaMemcpyAsync(h->d_metric, h->h_metric.data(), bytes, cudaMemcpyHostToDevice, h->stream));
+  int nxp = h->nxp, nyp = h->cfg.jnum + 4, nzp = h->cfg.knum + 4;
+  const double* b = h->d_metric;
+  auto P = [&](int which) { return b + (size_t)which * nxp; };
+  MetricP& M = h->mt;
+  M.dAxW = P(M_dAxW); M.dAyS = P(M_dAyS); M.dAzB = P(M_dAzB);
+  M.dydzdV = P(M_dydzdV); M.dzdxdV = P(M_dzdxdV); M.dxdydV = P(M_dxdydV);
+  M.cxyx = P(M_cxyx); M.cxzx = P(M_cxzx); M.cyxy = P(M_cyxy); M.cyzy = P(M_cyzy); M.czxz = P(M_czxz); M.czyz = P(M_czyz);
+  M.dlx = P(M_dlx); M.dly = P(M_dly); M.dlz = P(M_dlz);
+  M.offxW = P(M_offxW); M.offxE = P(M_offxE);
+  size_t base_y = (size_t)M_NI * nxp;
+  M.offyS = b + base_y; M.offyN = b + base_y + nyp;
+  M.offzB = b + base_y + 2 * nyp; M.offzT = b + base_y + 2 * nyp + nzp;
+  M.accel = h->has_accel ? P(M_accel0) : nullptr;
+  M.cs = P(M_cs0);
+  M.nxp = nxp;
+  M.curv = h->curv ? 1 : 0;
+  return FGPU_OK;
+}
+
+// ---------------------------------------------------------------- launchers
+template <int ND, bool EU, bool PRIM>
+int launch_stage_t(fgpu_handle* h, StageArgs& A) {
+  A.kchunk = h->kchunk;
+  const Grid& g = h->g;
+  if constexpr (ND == 2) {
+    dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, 1);
+    stage_kernel<ND, EU, PRIM, 32, 8><<<grid, 256, 0, h->stream>>>(A);
+  } else {
+    dim3 grid((g.nx + 31) / 32, (g.ny + 3) / 4, (g.nz + h->kchunk - 1) / h->kchunk);
+    stage_kernel<ND, EU, PRIM, 32, 4><<<grid, 128, 0, h->stream>>>(A);
+  }
+  CUDA_TRY(h, cudaGetLastError());
+  return FGPU_OK;
+}
+
+int launch_stage_raw(fgpu_handle* h, StageArgs& A) {
+  bool e = h->euler, p = h->prim;
+  if (h->nd == 2) {
+    if (e) return p ? launch_stage_t<2, true, true>(h, A) : launch_stage_t<2, true, false>(h, A);
+    return p ? launch_stage_t<2, false, true>(h, A) : launch_stage_t<2, false, false>(h, A);
+  }
+  if (e) return p ? launch_stage_t<3, true, true>(h, A) : launch_stage_t<3, true, false>(h, A);
+  return p ? launch_stage_t<3, false, true>(h, A) : launch_stage_t<3, false, false>(h, A);
+}
+
+template <int ND, bool EU>
+int launch_misc_t(fgpu_handle* h, int which, BndArgs& B) {
+  if (which == 0) {
+    long long blocks = std::min<long long>((B.nghost + 255) / 256, 4096);
+    if (blocks < 1) blocks = 1;
+    boundary_kernel<ND, EU><<<(unsigned)blocks, 256, 0, h->stream>>>(B);
+  } else if (which == 1) {
+    long long blocks = std::min<long long>((h->g.n + 255) / 256, 148 * 16);
+    interior_cfl_kernel<ND, EU><<<(unsigned)blocks, 256, 0, h->stream>>>(B);
+  } else {
+    long long blocks = std::min<long long>((h->g.n + 255) / 256, 148 * 16);
+    pack_interior_kernel<ND, EU><<<(unsigned)blocks, 256, 0, h->stream>>>(B);
+  }
+  CUDA_TRY(h, cudaGetLastError());
+  return FGPU_OK;
+}
+int launch_misc_raw(fgpu_handle* h, int which, BndArgs& B) {
+  if (h->nd == 2) return h->euler ? launch_misc_t<2, true>(h, which, B) : launch_misc_t<2, false>(h, which, B);
+  return h->euler ? launch_misc_t<3, true>(h, which, B) : launch_misc_t<3, false>(h, which, B);
+}
+// Algorithmic HBM arrays of one stage launch: the stencil input arrays once,
+// the start-of-step state for the Shu-Osher update, and every output written.
+double stage_bytes(const fgpu_handle* h, const StageArgs& A) {
+  int arrays = 1 + A.in.nk;
+  if (A.out_mode == OUT_SSPRK) arrays += 1;
+  arrays += 1;
+  if (A.out_base) arrays += 1;
+  if (A.last_stage && A.out_high) arrays += 1;
+  return (double)arrays * h->V * (double)h->g.n * 8.0;
+}
+
+template <class F>
+int timed_launch(fgpu_handle* h, bool stage, double bytes, F&& fn) {
+  h->stats.launches += 1;
+  if (stage) h->stats.stage_launches += 1;
+  if (!h->profiling) return fn();
+  fgpu_handle::Timed t;
+  t.bytes = bytes;
+  t.stage = stage ? 1 : 0;
+  CUDA_TRY(h, cudaEventCreate(&t.a));
+  CUDA_TRY(h, cudaEventCreate(&t.b));
+  CUDA_TRY(h, cudaEventRecord(t.a, h->stream));
+  int rc = fn();
+  CUDA_TRY(h, cudaEventRecord(t.b, h->stream));
+  h->timed.push_back(t);
+  return rc;
+}
+
+int launch_stage(fgpu_handle* h, StageArgs& A) {
+  return timed_launch(h, true, stage_bytes(h, A), [&] { return launch_stage_raw(h, A); });
+}
+int launch_misc(fgpu_handle* h, int which, BndArgs& B) {
+  return timed_launch(h, false, 0.0, [&] { return launch_misc_raw(h, which, B); });
+}
+
+int launch_roundtrip(fgpu_handle* h, const double* in, double* out) {
+  long long blocks = std::min<long long>((h->g.n + 255) / 256, 148 * 16);
+  if (h->nd == 2) {
+    if (h->euler) roundtrip_kernel<2, true><<<(unsigned)blocks, 256, 0, h->stream>>>(in, out, h->g.n, h->ph);
+  } else {
+    if (h->euler) roundtrip_kernel<3, true><<<(unsigned)blocks, 256, 0, h->stream>>>(in, out, h->g.n, h->ph);
+  }
+  if (!h->euler) CUDA_TRY(h, cudaMemcpyAsync(out, in, sizeof(double) * h->V * h->g.n, cudaMemcpyDeviceToDevice, h->stream));
+  CUDA_TRY(h, cudaGetLastError());
+  return FGPU_OK;
+}
+
+long long ghost_count(const fgpu_handle* h) {
+  long long NXp = h->g.nx + 4, NYp = h->g.ny + 4, NZp = h->nd == 3 ? h->g.nz + 4 : 1;
+  return NXp * NYp * NZp - h->g.n;
+}
+
+StateRef plain_state(const double* s, bool roundtrip) {
+  StateRef S;
+  std::memset(&S, 0, sizeof(S));
+  S.base = s;
+  S.nk = 0;
+  S.roundtrip = roundtrip ? 1 : 0;
+  return S;
+}
+
+StageArgs base_args(fgpu_handle* h) {
+  StageArgs A;
+  std::memset(&A, 0, sizeof(A));
+  A.g = h->g; A.ph = h->ph; A.mt = h->mt;
+  A.limiter = h->cfg.limiter; A.theta = h->cfg.theta;
+  A.constant_recon = h->cfg.order == FGPU_CONSTANT ? 1 : 0;
+  for (int d = 0; d < 3; ++d) A.invd[d] = h->invd[d];
+  A.has_accel = h->has_accel ? 1 : 0;
+  A.checkdata = h->cfg.checkdata;
+  A.ctl = h->d_ctl;
+  A.tol_rel = h->tol_rel;
+  for (int v = 0; v < FGPU_MAXV; ++v) A.tol_abs[v] = h->tol_abs[v];
+  return A;
+}
+
+BndArgs bnd_args(fgpu_handle* h, const double* state, bool roundtrip, int finalize) {
+  BndArgs B;
+  std::memset(&B, 0, sizeof(B));
+  B.g = h->g; B.ph = h->ph; B.mt = h->mt;
+  B.in = plain_state(state, roundtrip);
+  B.roundtrip = roundtrip ? 1 : 0;
+  B.checkdata = h->cfg.checkdata;
+  B.ctl = h->d_ctl;
+  B.finalize = finalize;
+  B.nghost = ghost_count(h);
+  return B;
+}
+
+int read_ctl(fgpu_handle* h) {
+  CUDA_TRY(h, cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return FGPU_OK;
+}
+int write_ctl(fgpu_handle* h) {
+  CUDA_TRY(h, cudaMemcpyAsync(h->d_ctl, h->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice, h->stream));
+  return FGPU_OK;
+}
+double ctl_invdt(const fgpu_handle* h) {
+  const Ctl* c = h->h_ctl;
+  auto D = [](unsigned long long b) { double d; std::memcpy(&d, &b, 8); return d; };
+  if (h->nd == 2) return D(c->invdt[0]);
+  double ix = D(c->invdt[0]), iy = D(c->invdt[1]), iz = D(c->invdt[2]);
+  return std::max(std::max(iy, iz), ix);
+}
+
+// ---------------------------------------------------------------- Shu-Osher (device clock)
+// eta(n,order), timedisc_modeuler.f90:74-77
+const double kEta[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.5, 0.0}, {0.0, 0.75, 1.0 / 3.0}};
+
+int enqueue_shu_osher_step(fgpu_handle* h) {
+  double* P = h->buf[0];
+  double* Abuf = h->buf[1];
+  double* Bbuf = h->buf[2];
+  const double* in = P;
+  for (int n = 1; n <= h->order; ++n) {
+    StageArgs A = base_args(h);
+    A.in = plain_state(in, n == 1 && h->roundtrip_cfg);
+    A.out_mode = OUT_SSPRK;
+    A.eta = kEta[h->order - 1][n - 1];
+    A.y0 = P;
+    A.y0_roundtrip = h->roundtrip_cfg ? 1 : 0;
+    A.dt_dev = &h->d_ctl->dt;
+    double* out;
+    if (n == h->order && h->order > 1) out = P;
+    else out = (n % 2 == 1) ? Abuf : Bbuf;
+    A.out = out;
+    if (n == h->order) { A.cfl_mode = 1; A.cfl_roundtrip = h->roundtrip_cfg ? 1 : 0; }
+    if (int rc = launch_stage(h, A)) return rc;
+    in = out;
+  }
+  if (h->order == 1)
+    CUDA_TRY(h, cudaMemcpyAsync(P, Abuf, sizeof(double) * h->V * h->g.n, cudaMemcpyDeviceToDevice, h->stream));
+  BndArgs B = bnd_args(h, P, h->roundtrip_cfg, FIN_STEP);
+  return launch_misc(h, 0, B);
+}
+
+int build_graph(fgpu_handle* h, int steps) {
+  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+  cudaGraph_t gr;
+  fgpu_stats saved = h->stats;
+  CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = 0;
+  for (int s = 0; s < steps && !rc; ++s) rc = enqueue_shu_osher_step(h);
+  cudaError_t e = cudaStreamEndCapture(h->stream, &gr);
+  h->kernels_per_step = (int)((h->stats.launches - saved.launches) / steps);
+  h->stats = saved;
+  if (rc) return rc;
+  if (e != cudaSuccess) return set_err(h, FGPU_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&h->graph, gr, 0);
+  cudaGraphDestroy(gr);
+  if (e != cudaSuccess) return set_err(h, FGPU_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  h->graph_steps = steps;
+  return FGPU_OK;
+}
+
+void sync_from_ctl(fgpu_handle* h) {
+  const Ctl* c = h->h_ctl;
+  h->time = c->time; h->dt = c->dt; h->dtold = c->dtold; h->dtmin = c->dtmin;
+  h->iter = c->iter; h->dtcause = c->dtcause; h->brk = c->brk != 0; h->checkflags = c->flags;
+}
+
+// ---------------------------------------------------------------- Butcher engine (host clock)
+int enqueue_k1(fgpu_handle* h, bool from_pre, bool cfl) {
+  // ComputeRHS of the current state into K1.  from_pre: the stored state in P
+  // gets the end-of-step CHECK_ALL treatment and its round trip goes to the
+  // base buffer (cold = cvar); otherwise RejectSolution's CHECK_NOTHING RHS of base.
+  double* P = h->buf[0];
+  double* base = h->buf[1];
+  double* K1 = h->buf[2];
+  StageArgs A = base_args(h);
+  A.out_mode = OUT_RHS;
+  A.out = K1;
+  if (from_pre) {
+    A.in = plain_state(P, h->roundtrip_cfg);
+    A.out_base = base;
+    if (cfl) A.cfl_mode = 2;
+  } else {
+    A.in = plain_state(base, false);
+  }
+  return launch_stage(h, A);
+}
+
+double adjust_timestep(fgpu_handle* h, double maxerr, double dtold_) {
+  // timedisc_base.f90:759-814
+  double dtnew, dttmp;
+  if (h->tol_rel >= 1.0) return DBL_MAX;
+  if (maxerr > 0.) dttmp = 0.9 * dtold_ * std::exp(-std::log(maxerr) / h->T.order);
+  else dttmp = 4. * dtold_;
+  if (h->maxerrold > 0.) dtnew = dttmp * std::exp(-h->beta * std::log(h->maxerrold / maxerr));
+  else dtnew = dttmp;
+  if (maxerr < 1.0) {
+    dtnew = std::min(dtnew, 4. * dtold_);
+    if (dtnew < dtold_) h->dtcause = FGPU_DTCAUSE_SMALLERR;
+  } else {
+    if (dtnew > dtold_) dtnew = dttmp;
+    dtnew = std::max(dtnew, 0.25 * dtold_);
+  }
+  h->maxerrold = maxerr;
+  return dtnew;
+}
+
+int butcher_attempt(fgpu_handle* h, double dtv, double& err) {
+  const Tableau& T = h->T;
+  double* P = h->buf[0];
+  double* base = h->buf[1];
+  h->stats.attempts += 1;
+  for (int m = 2; m <= T.m; ++m) {
+    StageArgs A = base_args(h);
+    A.in.base = base;
+    A.in.nk = m - 1;
+    A.in.roundtrip = 0;
+    for (int q = 0; q < m - 1; ++q) {
+      A.in.K[q] = h->buf[2 + q];
+      A.in.coef[q] = T.A[(m - 1) * T.m + q] * dtv;
+    }
+    A.out_mode = OUT_RHS;
+    A.out = h->buf[2 + m - 1];
+    if (m == T.m) {
+      A.last_stage = 1;
+      A.nstage = T.m;
+      for (int q = 0; q < T.m; ++q) { A.bh_dt[q] = T.bh[q] * dtv; A.bl_dt[q] = T.bl[q] * dtv; }
+      A.out_high = P;
+    }
+    if (int rc = launch_stage(h, A)) return rc;
+  }
+  if (int rc = read_ctl(h)) return rc;
+  double e;
+  std::memcpy(&e, &h->h_ctl->err, 8);
+  h->h_ctl->err = 0ULL;
+  CUDA_TRY(h, cudaMemsetAsync(&h->d_ctl->err, 0, sizeof(unsigned long long), h->stream));
+  err = e;
+  return FGPU_OK;
+}
+
+int finish_cfl_host(fgpu_handle* h, const double* state, bool roundtrip, double& dtcfl) {
+  BndArgs B = bnd_args(h, state, roundtrip, FIN_NONE);
+  if (int rc = launch_misc(h, 0, B)) return rc;
+  if (int rc = read_ctl(h)) return rc;
+  double invdt = ctl_invdt(h);
+  h->checkflags |= h->h_ctl->flags;
+  if (h->h_ctl->flags) h->brk = true;
+  h->h_ctl->flags = 0;
+  h->h_ctl->invdt[0] = h->h_ctl->invdt[1] = h->h_ctl->invdt[2] = 0ULL;
+  CUDA_TRY(h, cudaMemsetAsync(h->d_ctl, 0, sizeof(unsigned long long) * 3, h->stream));
+  CUDA_TRY(h, cudaMemsetAsync(&h->d_ctl->flags, 0, sizeof(int), h->stream));
+  dtcfl = h->cfl / invdt;
+  return FGPU_OK;
+}
+
+int butcher_integration_step(fgpu_handle* h) {
+  // timedisc_base.f90:649-750 IntegrationStep
+  double t = h->time, d = h->dt;
+  if (d < h->dtmin && h->dtcause != FGPU_DTCAUSE_FILEIO) h->dtmin = d;
+  double dtold_ = 0.0;
+  bool rhs_done_at_t = false;   // AcceptSolution already evaluated ComputeRHS(checkdatabm)
+  while (!h->brk && t + d <= h->time + h->dt) {
+    dtold_ = d;
+    double e = 0.0;
+    if (int rc = butcher_attempt(h, d, e)) return rc;
+    h->last_err = e;
+    d = adjust_timestep(h, e, d);
+    rhs_done_at_t = false;
+    if (e != e) h->brk = true;
+    else if (e > DBL_MAX) h->brk = true;
+    else if (e >= 1.0) {   // RejectSolution: cvar = cold, RHS with CHECK_NOTHING
+      if (int rc = enqueue_k1(h, false, false)) return rc;
+      h->n_adj++;
+      h->dtcause = FGPU_DTCAUSE_ERRADJ;
+      if (d < h->dtmin) h->dtmin = d;
+    } else {               // AcceptSolution
+      t = t + dtold_;
+      if (t < h->time + h->dt) {
+        if (int rc = enqueue_k1(h, true, false)) return rc;
+        rhs_done_at_t = true;
+      }
+      h->iter++;
+      h->stats.cell_updates += h->g.n;
+    }
+    if (d < h->dtlimit) h->brk = true;
+  }
+  if (!h->brk) {
+    h->dt = t - h->time;
+    h->time = t;
+    h->dtold = d;
+    if (rhs_done_at_t) {
+      // the state in base already went through one CHECK_ALL ComputeRHS; fosite applies a second one
+      CUDA_TRY(h, cudaMemcpyAsync(h->buf[0], h->buf[1], sizeof(double) * h->V * h->g.n, cudaMemcpyDeviceToDevice,
+                                  h->stream));
+    }
+    if (int rc = enqueue_k1(h, true, true)) return rc;
+    h->state_pre = true;
+  }
+  return FGPU_OK;
+}
+
+int validate(fgpu_handle* h) {
+  const fgpu_config& c = h->cfg;
+  if (c.inum < 2 || c.jnum < 2 || c.knum < 1)
+    return set_err(h, FGPU_EUNSUPPORTED, "meshes must be 2D (x-y) or 3D; 1D and collapsed-x/y meshes are not supported");
+  h->nd = c.knum > 1 ? 3 : 2;
+  if (c.physics != FGPU_EULER && c.physics != FGPU_EULER_ISOTHERM) return set_err(h, FGPU_EBADCFG, "unknown physics");
+  h->euler = c.physics == FGPU_EULER;
+  h->V = 1 + h->nd + (h->euler ? 1 : 0);
+  if (c.geometry != FGPU_CARTESIAN && c.geometry != FGPU_CYLINDRICAL && c.geometry != FGPU_LOGCYLINDRICAL)
+    return set_err(h, FGPU_EUNSUPPORTED, "geometry not supported (cartesian, cylindrical, logcylindrical)");
+  if (c.fluxtype != FGPU_KT) return set_err(h, FGPU_EBADCFG, "only KT fluxes exist");
+  if (c.order != FGPU_CONSTANT && c.order != FGPU_LINEAR) return set_err(h, FGPU_EBADCFG, "reconstruction order must be CONSTANT or LINEAR");
+  if (c.order == FGPU_LINEAR && (c.limiter < 1 || c.limiter > 8)) return set_err(h, FGPU_EBADCFG, "Unknown limiter");
+  if (c.order == FGPU_LINEAR && c.limiter == FGPU_PP) return set_err(h, FGPU_EUNSUPPORTED, "PP limiter currently not supported.");
+  h->prim = c.variables == FGPU_PRIMITIVE;
+  for (int f = 0; f < 6; ++f) {
+    if (h->nd == 2 && f >= 4) continue;
+    int t = c.bc[f];
+    if (t != FGPU_PERIODIC && t != FGPU_REFLECTING && t != FGPU_ABSORBING && t != FGPU_NO_GRADIENTS)
+      return set_err(h, FGPU_EUNSUPPORTED, "boundary condition not supported (periodic, reflecting, absorbing, no_gradients)");
+  }
+  for (int d = 0; d < h->nd; ++d)
+    if ((c.bc[2 * d] == FGPU_PERIODIC) != (c.bc[2 * d + 1] == FGPU_PERIODIC))
+      return set_err(h, FGPU_EBADCFG, "periodic boundaries must be paired");
+  if (c.fargo_method != 0) return set_err(h, FGPU_EUNSUPPORTED, "fargo transport is not available on this backend yet");
+  h->curv = c.geometry != FGPU_CARTESIAN;
+  if (c.pointmass) {
+    if (c.geometry == FGPU_CARTESIAN || h->nd != 2)
+      return set_err(h, FGPU_EUNSUPPORTED, "point mass supported on 2D cylindrical/logcylindrical meshes");
+    h->has_accel = true;
+  }
+  if (!h->euler && c.csiso < 0.0) return set_err(h, FGPU_EBADCFG, "negative isothermal sound speed");
+  // timedisc
+  h->tol_rel = c.tol_rel; h->beta = c.beta; h->cfl = c.cfl; h->stoptime = c.stoptime;
+  h->dtlimit = c.dtlimit > 0 ? c.dtlimit : DBL_EPSILON * c.stoptime;
+  h->tout = c.tout > 0 ? c.tout : c.stoptime;
+  for (int v = 0; v < FGPU_MAXVAR; ++v) h->tol_abs[v] = c.tol_abs[v];
+  if (c.method == FGPU_MODIFIED_EULER) {
+    h->butcher = false;
+    h->order = c.tdorder ? c.tdorder : 3;
+    if (h->order < 1 || h->order > 3) return set_err(h, FGPU_EBADCFG, "time order must be one of 1,2,3");
+    if (h->order == 1) { h->tol_rel = 10.0; for (int v = 0; v < FGPU_MAXVAR; ++v) h->tol_abs[v] = 1.0; }
+    if (h->tol_rel < 1.0)
+      return set_err(h, FGPU_EUNSUPPORTED, "modified Euler with adaptive step control (tol_rel < 1) is not supported; use tol_rel >= 1 or an embedded RK method");
+  } else {
+    h->butcher = true;
+    int ord = c.tdorder ? c.tdorder : 5;
+    if (!make_tableau(c.method, ord, h->T)) return set_err(h, FGPU_EBADCFG, "unknown timedisc method/order");
+    h->order = ord;
+    if (h->tol_rel > 1.0) return set_err(h, FGPU_EUNSUPPORTED, "embedded RK with disabled step control is not supported");
+  }
+  if (c.tol_rel < 0.0) return set_err(h, FGPU_EBADCFG, "error tolerance levels must be greater than 0");
+  if (c.stoptime <= 0.0) return set_err(h, FGPU_EBADCFG, "stoptime must be positive");
+  if (c.tmin > 1.e-10 && (c.checkdata & FGPU_CHECK_TMIN) && h->euler)
+    return set_err(h, FGPU_EUNSUPPORTED, "CHECK_TMIN with tmin > 1e-10 is not supported");
+  h->roundtrip_cfg = h->euler && (c.checkdata & FGPU_CHECK_PMIN);
+  return FGPU_OK;
+}
+
+}  // namespace
+
+// ======================================================================= C ABI
+extern "C" {
+
+void fgpu_config_init(fgpu_config* c) {
+  std::memset(c, 0, sizeof(*c));
+  c->inum = c->jnum = c->knum = 1;
+  c->geometry = FGPU_CARTESIAN;
+  c->gparam = 1.0;
+  c->physics = FGPU_EULER;
+  c->gamma = 1.4;
+  c->gn = 1.0;
+  c->fluxtype = FGPU_KT;
+  c->order = FGPU_LINEAR;
+  c->variables = FGPU_CONSERVATIVE;
+  c->limiter = FGPU_MINMOD;
+  c->theta = 1.0;
+  for (int f = 0; f < 6; ++f) c->bc[f] = FGPU_PERIODIC;
+  c->method = FGPU_MODIFIED_EULER;
+  c->cfl = 0.4;
+  c->stoptime = 1.0;
+  c->tol_rel = 0.01;
+  c->beta = 0.08;
+  for (int v = 0; v < FGPU_MAXVAR; ++v) c->tol_abs[v] = 0.001;
+  c->checkdata = FGPU_CHECK_ALL;
+  c->pmin = c->rhomin = c->tmin = DBL_MIN;
+  c->pm_mass = 1.0;
+}
+
+int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
+  if (!cfg || !out) return set_err(nullptr, FGPU_EARG, "null argument");
+  *out = nullptr;
+  fgpu_handle* h = new fgpu_handle();
+  std::memset(&h->stats, 0, sizeof(h->stats));
+  h->cfg = *cfg;
+  int rc = validate(h);
+  if (!rc) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) rc = set_err(h, FGPU_ECUDA, "no CUDA device");
+  }
+  if (!rc) {
+    if (device >= 0) { if (cudaSetDevice(device) != cudaSuccess) rc = set_err(h, FGPU_ECUDA, "cudaSetDevice failed"); }
+    cudaGetDevice(&h->device);
+  }
+  if (!rc) rc = build_metric(h);
+  if (!rc) {
+    h->g.nx = cfg->inum; h->g.ny = cfg->jnum; h->g.nz = h->nd == 3 ? cfg->knum : 1;
+    h->g.n = (long long)h->g.nx * h->g.ny * h->g.nz;
+    for (int f = 0; f < 6; ++f) h->g.bc[f] = cfg->bc[f];
+    h->ph.gamma = cfg->gamma; h->ph.gm1 = cfg->gamma - 1.; h->ph.pmin = cfg->pmin; h->ph.rhomin = cfg->rhomin;
+    h->ph.tiny2 = 2.0 * DBL_MIN;
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) rc = set_err(h, FGPU_ECUDA, "stream");
+  }
+  if (!rc) rc = upload_metric(h);
+  if (!rc) {
+    int nbuf = h->butcher ? 2 + h->T.m : 3;
+    size_t bytes = sizeof(double) * h->V * h->g.n;
+    for (int b = 0; b < nbuf && !rc; ++b) {
+      double* p = nullptr;
+      cudaError_t e = cudaMalloc(&p, bytes);
+      if (e != cudaSuccess) { rc = set_err(h, FGPU_ENOMEM, "device memory for state arrays"); break; }
+      cudaMemsetAsync(p, 0, bytes, h->stream);
+      h->buf.push_back(p);
+    }
+  }
+  if (!rc) {
+    if (cudaMalloc(&h->d_ctl, sizeof(Ctl)) != cudaSuccess) rc = set_err(h, FGPU_ENOMEM, "control block");
+    else if (cudaMallocHost(&h->h_ctl, sizeof(Ctl)) != cudaSuccess) rc = set_err(h, FGPU_ENOMEM, "pinned control block");
+  }
+  if (!rc) {
+    std::memset(h->h_ctl, 0, sizeof(Ctl));
+    h->h_ctl->stoptime = h->stoptime; h->h_ctl->tout = h->tout; h->h_ctl->cfl = h->cfl;
+    h->h_ctl->dtlimit = h->dtlimit; h->h_ctl->dt = h->stoptime; h->h_ctl->dtmin = h->stoptime;
+    h->h_ctl->iter = -1;
+    rc = write_ctl(h);
+    h->dt = h->stoptime; h->dtold = h->dt; h->dtmin = h->dt;
+  }
+  if (!rc) {
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) rc = set_err(h, FGPU_ECUDA, cudaGetErrorString(e));
+  }
+  if (rc) { g_create_error = h->err; fgpu_destroy(h); return rc; }
+  *out = h;
+  return FGPU_OK;
+}
+
+void fgpu_destroy(fgpu_handle* h) {
+  if (!h) return;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  for (double* p : h->buf) cudaFree(p);
+  if (h->d_pad) cudaFree(h->d_pad);
+  if (h->d_metric) cudaFree(h->d_metric);
+  if (h->d_ctl) cudaFree(h->d_ctl);
+  if (h->h_ctl) cudaFreeHost(h->h_ctl);
+  if (h->own_stream) h->stream = h->own_stream;
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+int fgpu_last_error(const fgpu_handle* h, char* buf, int len) {
+  const std::string& s = h ? h->err : g_create_error;
+  if (buf && len > 0) {
+    int n = std::min<int>((int)s.size(), len - 1);
+    std::memcpy(buf, s.data(), n);
+    buf[n] = 0;
+  }
+  return (int)s.size();
+}
+
+int64_t fgpu_cell_count(const fgpu_handle* h) {
+  return (int64_t)(h->g.nx + 4) * (h->g.ny + 4) * (h->nd == 3 ? h->g.nz + 4 : 1);
+}
+int64_t fgpu_state_size(const fgpu_handle* h) { return fgpu_cell_count(h) * h->V; }
+int fgpu_vnum(const fgpu_handle* h) { return h->V; }
+
+int fgpu_get_mesh(fgpu_handle* h, int which, double* out, int64_t n) {
+  if (!h || !out) return FGPU_EARG;
+  if (n < fgpu_cell_count(h)) return set_err(h, FGPU_EARG, "output too small");
+  const fgpu_config& c = h->cfg;
+  int NXp = h->g.nx + 4, NYp = h->g.ny + 4, NZp = h->nd == 3 ? h->g.nz + 4 : 1;
+  double mdx = (c.xmax - c.xmin) / c.inum, mdy = (c.ymax - c.ymin) / c.jnum, mdz = (c.zmax - c.zmin) / c.knum;
+  if (mdz < 2 * DBL_EPSILON && c.knum == 1) mdz = 0.0;
+  for (int kp = 0; kp < NZp; ++kp)
+    for (int jp = 0; jp < NYp; ++jp)
+      for (int ip = 0; ip < NXp; ++ip) {
+        int I = ip - 1, J = jp - 1, K = h->nd == 3 ? kp - 1 : 1;
+        double x = c.xmin + ((double)(2 * I - 1) * 0.5) * mdx;
+        double y = c.ymin + ((double)(2 * J - 1) * 0.5) * mdy;
+        double z = c.zmin + ((double)(2 * K - 1) * 0.5) * mdz;
+        double v;
+        switch (which) {
+          case FGPU_MESH_X: v = x; break;
+          case FGPU_MESH_Y: v = y; break;
+          case FGPU_MESH_Z: v = z; break;
+          case FGPU_MESH_RADIUS:
+            if (c.geometry == FGPU_LOGCYLINDRICAL) { double r = c.gparam * std::exp(x); v = std::sqrt(r * r + z * z); }
+            else if (c.geometry == FGPU_CYLINDRICAL) v = std::sqrt(x * x + z * z);
+            else v = std::sqrt(x * x + y * y + z * z);
+            break;
+          default: return set_err(h, FGPU_EARG, "unknown mesh array");
+        }
+        out[ip + (long long)NXp * (jp + (long long)NYp * kp)] = v;
+      }
+  return FGPU_OK;
+}
+
+int fgpu_set_sound_speeds(fgpu_handle* h, const double* bcc, int64_t nb, const double* fcs, int64_t nf) {
+  if (!h) return FGPU_EARG;
+  if (h->euler) return set_err(h, FGPU_EBADCFG, "sound speeds are computed for ideal-gas physics");
+  long long nc = fgpu_cell_count(h);
+  int nfaces = 2 * h->nd;
+  if (nb < nc || nf < nc * nfaces) return set_err(h, FGPU_EARG, "sound speed arrays too small");
+  int NXp = h->g.nx + 4, NYp = h->g.ny + 4, NZp = h->nd == 3 ? h->g.nz + 4 : 1;
+  // the profiles must depend on the first coordinate only
+  for (int q = 0; q <= nfaces; ++q) {
+    const double* a = q == 0 ? bcc : fcs + (long long)(q - 1) * nc;
+    for (int kp = 0; kp < NZp; ++kp)
+      for (int jp = 0; jp < NYp; ++jp)
+        for (int ip = 0; ip < NXp; ++ip) {
+          double v = a[ip + (long long)NXp * (jp + (long long)NYp * kp)];
+          double r = a[ip + (long long)NXp * (2 + (long long)NYp * (h->nd == 3 ? 2 : 0))];
+          if (v != r) return set_err(h, FGPU_EUNSUPPORTED, "sound speed profiles that vary along y or z are not supported");
+        }
+  }
+  int row = NXp * (2 + NYp * (h->nd == 3 ? 2 : 0));
+  for (int ip = 0; ip < NXp; ++ip) {
+    h->h_metric[(size_t)(M_cs0 + 0) * NXp + ip] = bcc[row + ip];
+    for (int q = 0; q < nfaces; ++q) h->h_metric[(size_t)(M_cs0 + 1 + q) * NXp + ip] = fcs[(long long)q * nc + row + ip];
+    if (h->nd == 2) {   // B/T profiles unused in 2D
+      h->h_metric[(size_t)(M_cs0 + 5) * NXp + ip] = bcc[row + ip];
+      h->h_metric[(size_t)(M_cs0 + 6) * NXp + ip] = bcc[row + ip];
+    }
+  }
+  int rc = upload_metric(h);
+  if (rc) return rc;
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return FGPU_OK;
+}
+
+int fgpu_upload_state(fgpu_handle* h, int which, const double* data, int64_t n) {
+  if (!h || !data) return FGPU_EARG;
+  if (n < fgpu_state_size(h)) return set_err(h, FGPU_EARG, "state array too small");
+  if (which != FGPU_CVAR && which != FGPU_PVAR) return set_err(h, FGPU_EARG, "upload CVAR or PVAR");
+  long long nc = fgpu_cell_count(h);
+  if (!h->d_pad) CUDA_TRY(h, cudaMalloc(&h->d_pad, sizeof(double) * 2 * nc * h->V));
+  CUDA_TRY(h, cudaMemcpyAsync(h->d_pad, data, sizeof(double) * nc * h->V, cudaMemcpyHostToDevice, h->stream));
+  long long blocks = std::min<long long>((h->g.n + 255) / 256, 148 * 16);
+  int prim = which == FGPU_PVAR;
+  h->stats.launches += 1;
+  if (h->nd == 2) {
+    if (h->euler) unpack_kernel<2, true><<<(unsigned)blocks, 256, 0, h->stream>>>(h->d_pad, h->buf[0], h->g, nc, prim, h->ph);
+    else unpack_kernel<2, false><<<(unsigned)blocks, 256, 0, h->stream>>>(h->d_pad, h->buf[0], h->g, nc, prim, h->ph);
+  } else {
+    if (h->euler) unpack_kernel<3, true><<<(unsigned)blocks, 256, 0, h->stream>>>(h->d_pad, h->buf[0], h->g, nc, prim, h->ph);
+    else unpack_kernel<3, false><<<(unsigned)blocks, 256, 0, h->stream>>>(h->d_pad, h->buf[0], h->g, nc, prim, h->ph);
+  }
+  CUDA_TRY(h, cudaGetLastError());
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  h->state_pre = false;
+  return FGPU_OK;
+}
+
+int fgpu_download(fgpu_handle* h, int which, double* out, int64_t n) {
+  if (!h || !out) return FGPU_EARG;
+  long long nc = fgpu_cell_count(h);
+  if (which == FGPU_RHS) {
+    if (n < nc * h->V) return set_err(h, FGPU_EARG, "output too small");
+    // the RHS of the last fgpu_compute_rhs lives in a stage scratch buffer
+    const double* src = h->butcher ? h->buf[2 + h->T.m - 1] : h->buf[1];
+    std::vector<double> tmp((size_t)h->V * h->g.n);
+    CUDA_TRY(h, cudaMemcpyAsync(tmp.data(), src, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    std::memset(out, 0, sizeof(double) * nc * h->V);
+    int NXp = h->g.nx + 4, NYp = h->g.ny + 4, kofs = h->nd == 3 ? 2 : 0;
+    for (int l = 0; l < h->V; ++l)
+      for (int k = 0; k < h->g.nz; ++k)
+        for (int j = 0; j < h->g.ny; ++j)
+          for (int i = 0; i < h->g.nx; ++i)
+            out[(i + 2) + (long long)NXp * ((j + 2) + (long long)NYp * (k + kofs)) + nc * l] =
+                tmp[i + (long long)h->g.nx * (j + (long long)h->g.ny * k) + h->g.n * l];
+    return FGPU_OK;
+  }
+  if (which == FGPU_BCCSOUND) {
+    if (n < nc) return set_err(h, FGPU_EARG, "output too small");
+    std::vector<double> pv((size_t)nc * h->V);
+    int rc = fgpu_download(h, FGPU_PVAR, pv.data(), (int64_t)pv.size());
+    if (rc) return rc;
+    int NXp = h->g.nx + 4;
+    for (long long x = 0; x < nc; ++x) {
+      if (h->euler) out[x] = std::sqrt(std::max(2.0 * DBL_MIN, h->cfg.gamma * pv[x + nc * (h->V - 1)] / pv[x]));
+      else out[x] = h->h_metric[(size_t)M_cs0 * NXp + (x % NXp)];
+    }
+    return FGPU_OK;
+  }
+  if (which != FGPU_CVAR && which != FGPU_PVAR) return set_err(h, FGPU_EARG, "unknown array");
+  if (n < nc * h->V) return set_err(h, FGPU_EARG, "output too small");
+  if (!h->d_pad) CUDA_TRY(h, cudaMalloc(&h->d_pad, sizeof(double) * 2 * nc * h->V));
+  CUDA_TRY(h, cudaMemsetAsync(h->d_pad, 0, sizeof(double) * 2 * nc * h->V, h->stream));
+  bool rt = h->state_pre && h->roundtrip_cfg;
+  BndArgs B = bnd_args(h, h->buf[0], rt, FIN_NONE);
+  B.ctl = nullptr;
+  B.out_p = h->d_pad;
+  B.out_c = h->d_pad + nc * h->V;
+  B.npad = nc;
+  if (int rc = launch_misc(h, 2, B)) return rc;
+  if (int rc = launch_misc(h, 0, B)) return rc;
+  CUDA_TRY(h, cudaMemcpyAsync(out, which == FGPU_PVAR ? B.out_p : B.out_c, sizeof(double) * nc * h->V,
+                              cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return FGPU_OK;
+}
+
+int fgpu_first_step(fgpu_handle* h) {
+  if (!h) return FGPU_EARG;
+  if (h->first_done) return set_err(h, FGPU_EBADCFG, "FirstStep should only be called once.");
+  h->first_done = true;
+  h->iter = 0;
+  h->time = 0.0;
+  if (h->butcher) {
+    if (int rc = enqueue_k1(h, true, true)) return rc;
+    double dtc;
+    if (int rc = finish_cfl_host(h, h->buf[0], h->roundtrip_cfg, dtc)) return rc;
+    h->dt = dtc;
+    h->dtcause = 0;
+    h->state_pre = true;
+    if (h->brk) return set_err(h, FGPU_BREAK, "FirstStep: Initial data invalid!");
+    // first fosite%Step clip happens in fgpu_step
+    return FGPU_OK;
+  }
+  // device clock: interior + boundary CFL, finalize computes dt and the clip for step 1
+  Ctl* c = h->h_ctl;
+  std::memset(c, 0, sizeof(Ctl));
+  c->stoptime = h->stoptime; c->tout = h->tout; c->cfl = h->cfl; c->dtlimit = h->dtlimit;
+  c->time = 0.0; c->dtmin = h->stoptime; c->iter = 0;
+  if (int rc = write_ctl(h)) return rc;
+  BndArgs B = bnd_args(h, h->buf[0], h->roundtrip_cfg, FIN_FIRST);
+  if (int rc = launch_misc(h, 1, B)) return rc;
+  if (int rc = launch_misc(h, 0, B)) return rc;
+  if (int rc = read_ctl(h)) return rc;
+  sync_from_ctl(h);
+  h->state_pre = true;
+  if (h->brk) return set_err(h, FGPU_BREAK, "FirstStep: Initial data invalid!");
+  return FGPU_OK;
+}
+
+static int butcher_step(fgpu_handle* h) {
+  // fosite%Step (fosite.f90:367-464) around the Butcher IntegrationStep
+  if (std::fabs(h->stoptime - h->time) <= 1.0E-05 * h->stoptime) return FGPU_STOPTIME;
+  if ((h->time + h->dt) / h->tout > 1.0) { h->dt = h->tout - h->time; h->dtcause = FGPU_DTCAUSE_FILEIO; }
+  else if ((h->time + 1.5 * h->dt) / h->tout > 1.0) { h->dt = 0.5 * (h->tout - h->time); h->dtcause = FGPU_DTCAUSE_FILEIO; }
+  if (int rc = butcher_integration_step(h)) return rc;
+  if (h->brk) return FGPU_BREAK;
+  double dtc;
+  if (int rc = finish_cfl_host(h, h->buf[0], h->roundtrip_cfg, dtc)) return rc;
+  if (h->brk) return FGPU_BREAK;
+  h->dt = dtc;
+  h->dtcause = 0;
+  return FGPU_OK;
+}
+
+int fgpu_run(fgpu_handle* h, int64_t n, int64_t* done) {
+  if (!h) return FGPU_EARG;
+  if (!h->first_done) { int rc = fgpu_first_step(h); if (rc) return rc; }
+  int64_t k = 0;
+  if (h->butcher) {
+    int rc = FGPU_OK;
+    for (; k < n; ++k) {
+      rc = butcher_step(h);
+      if (rc) break;
+    }
+    if (done) *done = k;
+    return rc;
+  }
+  // device clock: graph of G steps, replayed
+  long long it0 = h->iter;
+  const int G = 16;
+  int64_t full = n / G, rest = n % G;
+  if (h->profiling) { rest += full * G; full = 0; }   // per-launch timing needs direct launches
+  if (full > 0) {
+    if (h->graph_steps != G) { if (int rc = build_graph(h, G)) return rc; }
+    for (int64_t r = 0; r < full; ++r) {
+      CUDA_TRY(h, cudaGraphLaunch(h->graph, h->stream));
+      h->stats.launches += (int64_t)h->kernels_per_step * G;
+      h->stats.stage_launches += (int64_t)h->order * G;
+    }
+  }
+  for (int64_t r = 0; r < rest; ++r) { if (int rc = enqueue_shu_osher_step(h)) return rc; }
+  if (int rc = read_ctl(h)) return rc;
+  sync_from_ctl(h);
+  h->stats.attempts += h->iter - it0;
+  h->stats.cell_updates += (h->iter - it0) * h->g.n;
+  if (done) *done = h->iter - it0;
+  if (h->brk) return FGPU_BREAK;
+  if (h->h_ctl->stop) return FGPU_STOPTIME;
+  return FGPU_OK;
+}
+
+int fgpu_step(fgpu_handle* h) {
+  if (!h) return FGPU_EARG;
+  if (!h->first_done) { int rc = fgpu_first_step(h); if (rc) return rc; }
+  if (h->butcher) return butcher_step(h);
+  if (h->h_ctl->stop || h->h_ctl->brk) return h->h_ctl->brk ? FGPU_BREAK : FGPU_STOPTIME;
+  int64_t d = 0;
+  return fgpu_run(h, 1, &d);
+}
+
+int fgpu_compute_rhs(fgpu_handle* h) {
+  if (!h) return FGPU_EARG;
+  // ComputeRHS(CHECK_NOTHING) of fosite's current cvar
+  double* P = h->buf[0];
+  const double* src = P;
+  // K_m and K_(m-1) of the Butcher engine are recomputed by every attempt,
+  // so between steps they are free scratch (m >= 3 for all tableaus)
+  double* out = h->butcher ? h->buf[2 + h->T.m - 1] : h->buf[1];
+  double* scratch = h->butcher ? h->buf[2 + h->T.m - 2] : h->buf[2];
+  if (h->state_pre && h->roundtrip_cfg) {
+    if (int rc = launch_roundtrip(h, P, scratch)) return rc;
+    src = scratch;
+  }
+  StageArgs A = base_args(h);
+  A.in = plain_state(src, false);
+  A.out_mode = OUT_RHS;
+  A.out = out;
+  A.ctl = nullptr;
+  if (int rc = launch_stage(h, A)) return rc;
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return FGPU_OK;
+}
+
+int fgpu_calc_timestep(fgpu_handle* h, double* dt) {
+  if (!h || !dt) return FGPU_EARG;
+  bool rt = h->state_pre && h->roundtrip_cfg;
+  Ctl save = *h->h_ctl;
+  if (int rc = read_ctl(h)) return rc;
+  save = *h->h_ctl;
+  h->h_ctl->invdt[0] = h->h_ctl->invdt[1] = h->h_ctl->invdt[2] = 0ULL;
+  h->h_ctl->flags = 0;
+  h->h_ctl->stop = 0; h->h_ctl->brk = 0;
+  if (int rc = write_ctl(h)) return rc;
+  BndArgs B = bnd_args(h, h->buf[0], rt, FIN_NONE);
+  if (int rc = launch_misc(h, 1, B)) return rc;
+  if (int rc = launch_misc(h, 0, B)) return rc;
+  if (int rc = read_ctl(h)) return rc;
+  *dt = h->cfl / ctl_invdt(h);
+  *h->h_ctl = save;
+  return write_ctl(h);
+}
+
+int fgpu_get_status(fgpu_handle* h, fgpu_status* st) {
+  if (!h || !st) return FGPU_EARG;
+  std::memset(st, 0, sizeof(*st));
+  st->time = h->time; st->dt = h->dt; st->dtold = h->dtold; st->dtmin = h->dtmin; st->maxerr = h->last_err;
+  st->iter = h->iter; st->n_adj = h->n_adj; st->dtcause = h->dtcause; st->brk = h->brk ? 1 : 0;
+  st->checkflags = h->checkflags;
+  return FGPU_OK;
+}
+
+int fgpu_synchronize(fgpu_handle* h) {
+  if (!h) return FGPU_EARG;
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return FGPU_OK;
+}
+
+int fgpu_set_stream(fgpu_handle* h, void* stream) {
+  if (!h) return FGPU_EARG;
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  if (!h->own_stream) h->own_stream = h->stream;
+  h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+  return FGPU_OK;
+}
+
+int fgpu_set_profiling(fgpu_handle* h, int on) {
+  if (!h) return FGPU_EARG;
+  h->profiling = on != 0;
+  return FGPU_OK;
+}
+
+int fgpu_get_stats(fgpu_handle* h, fgpu_stats* st) {
+  if (!h || !st) return FGPU_EARG;
+  if (!h->timed.empty()) {
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    for (auto& t : h->timed) {
+      float ms = 0.f;
+      CUDA_TRY(h, cudaEventElapsedTime(&ms, t.a, t.b));
+      if (t.stage) { h->stats.stage_ms += ms; h->stats.stage_bytes += t.bytes; }
+      else h->stats.other_ms += ms;
+      cudaEventDestroy(t.a);
+      cudaEventDestroy(t.b);
+    }
+    h->timed.clear();
+  }
+  *st = h->stats;
+  return FGPU_OK;
+}
+
+int fgpu_reset_stats(fgpu_handle* h) {
+  if (!h) return FGPU_EARG;
+  fgpu_stats tmp;
+  int rc = fgpu_get_stats(h, &tmp);
+  std::memset(&h->stats, 0, sizeof(h->stats));
+  return rc;
+}
+
+}  // extern "C"

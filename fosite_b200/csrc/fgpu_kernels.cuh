@@ -1,0 +1,451 @@
+// fgpu_kernels.cuh -- fused stage kernel and the boundary / reduction kernels.
+//
+// One launch of stage_kernel is one right-hand-side evaluation of fosite's
+// ComputeRHS (timedisc_base.f90:1073-1271) fused with what consumes it:
+//   * the stage input state is formed on the fly (base - sum coef*K), so the
+//     Butcher stages of timedisc_rkfehlberg.f90:170-302 read their k-arrays
+//     once and never materialise ctmp;
+//   * ghost cells are synthesised in the tile loader (no ghost-fill pass);
+//   * reconstruction (reconstruction_linear.f90:215-630), KT fluxes
+//     (fluxes_kt.f90:109-208), flux divergence and geometric / point-mass
+//     sources are computed per tile in shared memory;
+//   * the result is either written as k_m (Butcher engine) or consumed by the
+//     Shu-Osher update of timedisc_modeuler.f90:279-291;
+//   * epilogues: CFL maximum (CalcTimestep), CheckData flags, the embedded
+//     error norm (ComputeError) and the high-order solution.
+// 2D meshes use one x-y tile per block; 3D meshes march a 2.5D x-y tile
+// along z so each plane is loaded once.
+#pragma once
+#include "fgpu_device.cuh"
+
+namespace fgpu {
+
+enum { OUT_RHS = 0, OUT_SSPRK = 1 };
+
+struct StageArgs {
+  Grid g;
+  PhysP ph;
+  MetricP mt;
+  StateRef in;
+  int limiter;
+  double theta;
+  int constant_recon;
+  double invd[3];
+  int has_accel;
+  int out_mode;
+  double* out;             // k_m (OUT_RHS) or the new state (OUT_SSPRK)
+  const double* y0;        // OUT_SSPRK: state at the start of the step (cold)
+  int y0_roundtrip;        // cold is the CHECK_PMIN round trip of y0
+  double eta;
+  const double* dt_dev;    // device-resident dt, or null to use dt
+  double dt;
+  double* out_base;        // optional: write the (round-tripped) input state
+  // Butcher last stage: high/low order combination and error norm
+  int last_stage;
+  int nstage;
+  double bh_dt[FGPU_MAXK], bl_dt[FGPU_MAXK];
+  double* out_high;
+  double tol_rel;
+  double tol_abs[FGPU_MAXV];
+  // CFL/CheckData epilogue: 0 none, 1 on the OUT_SSPRK result, 2 on the input state
+  int cfl_mode;
+  int cfl_roundtrip;       // the checked state gets the CHECK_PMIN round trip
+  int checkdata;
+  Ctl* ctl;
+  int kchunk;
+};
+
+// block-wide max of up to 3 non-negative doubles + OR of flags, then one atomic per block
+template <int NT>
+__device__ __forceinline__ void block_reduce_emit(double* vals, int nv, int flags, unsigned long long* dst,
+                                                  int* dflags, double* sred) {
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int q = 0; q < nv; ++q) {
+    double x = vals[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = dmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+    vals[q] = x;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) flags |= __shfl_xor_sync(0xffffffffu, flags, o);
+  __syncthreads();
+  if (lane == 0) {
+    for (int q = 0; q < nv; ++q) sred[warp * 4 + q] = vals[q];
+    sred[warp * 4 + 3] = __longlong_as_double((long long)flags);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    constexpr int NW = (NT + 31) / 32;
+    int f = 0;
+    for (int q = 0; q < nv; ++q) {
+      double m = 0.0;
+      for (int w = 0; w < NW; ++w) m = dmax(m, sred[w * 4 + q]);
+      if (dst) atomicMax(dst + q, (unsigned long long)__double_as_longlong(m));
+    }
+    for (int w = 0; w < NW; ++w) f |= (int)__double_as_longlong(sred[w * 4 + 3]);
+    if (f && dflags) atomicOr(dflags, f);
+  }
+}
+
+template <int ND, bool EU, bool PRIM, int TX, int TY>
+__global__ void __launch_bounds__(TX* TY) stage_kernel(const __grid_constant__ StageArgs A) {
+  using PH = Phys<ND, EU>;
+  using CE = Cells<ND, EU>;
+  constexpr int V = PH::V;
+  constexpr int NT = TX * TY;
+  constexpr int RW = TX + 4, RH = TY + 4;
+  constexpr int SW = TX + 2, SH = TY + 2;
+  constexpr int FW = TX + 1, FH = TY + 1;
+  __shared__ double Rs[V * RH * RW];
+  __shared__ double Ss[V * SH * SW];
+  __shared__ double Fs[V * FH * FW];
+  __shared__ double sred[4 * ((NT + 31) / 32)];
+
+  if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
+  const Grid& g = A.g;
+  const PhysP& P = A.ph;
+  const MetricP& M = A.mt;
+  const double dt = A.dt_dev ? *A.dt_dev : A.dt;
+  const bool roundtrip = EU && A.in.roundtrip;
+  const int tid = threadIdx.x;
+  const int tx = tid % TX, ty = tid / TX;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int ex = min(TX, g.nx - i0), ey = min(TY, g.ny - j0);
+  const bool own = tx < ex && ty < ey;
+  const int i = i0 + tx, j = j0 + ty;
+  int k0 = 0, k1 = 1;
+  if (ND == 3) { k0 = blockIdx.z * A.kchunk; k1 = min(g.nz, k0 + A.kchunk); }
+
+  auto RS = [&](int v, int ly, int lx) -> double& { return Rs[(v * RH + ly) * RW + lx]; };
+  auto SS = [&](int v, int r, int c) -> double& { return Ss[(v * SH + r) * SW + c]; };
+  auto FS = [&](int v, int r, int c) -> double& { return Fs[(v * FH + r) * FW + c]; };
+
+  // reconstruction variables at a cross point (interior or face ghost)
+  auto recon_at = [&](int gi, int gj, int gk, double* R) {
+    double p[V];
+    bool inx = gi >= 0 && gi < g.nx, iny = gj >= 0 && gj < g.ny, inz = gk >= 0 && gk < g.nz;
+    if (inx && iny && inz) {
+      double u[V];
+      state_at<V>(A.in, g.n, CE::lin(g, gi, gj, gk), u);
+      if (PRIM) {
+        PH::c2p(u, p, P);
+        if (roundtrip) p[V - 1] = dmax(p[V - 1], P.pmin);
+#pragma unroll
+        for (int l = 0; l < V; ++l) R[l] = p[l];
+      } else if (roundtrip) {
+        PH::c2p(u, p, P);
+        p[V - 1] = dmax(p[V - 1], P.pmin);
+        PH::p2c(p, R, P);
+      } else {
+#pragma unroll
+        for (int l = 0; l < V; ++l) R[l] = u[l];
+      }
+    } else {
+      int d = !inx ? 0 : (!iny ? 1 : 2);
+      CE::face_ghost_p(A.in, g, P, M, d, gi, gj, gk, p);
+      if (roundtrip) p[V - 1] = dmax(p[V - 1], P.pmin);
+      if (PRIM) {
+#pragma unroll
+        for (int l = 0; l < V; ++l) R[l] = p[l];
+      } else {
+        PH::p2c(p, R, P);
+      }
+    }
+  };
+
+  const int ip = i + 2;   // padded i of the own cell
+  double cflv[3] = {0.0, 0.0, 0.0};
+  double errv = 0.0;
+  int flags = 0;
+
+  // z-direction state of the own column (3D): R at k, k+1, z-slope at k, flux at k-1/2
+  double Rz0[V], Rz1[V], sz0[V], Fzm[V];
+  if (ND == 3 && own) {
+    double Ra[V], Rb[V];
+    recon_at(i, j, k0 - 2, Ra);
+    recon_at(i, j, k0 - 1, Rb);
+    recon_at(i, j, k0, Rz0);
+    recon_at(i, j, k0 + 1, Rz1);
+    double szm[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      szm[v] = A.constant_recon ? 0.0 : slope(A.limiter, A.theta, A.invd[2], Ra[v], Rb[v], Rz0[v]);
+      sz0[v] = A.constant_recon ? 0.0 : slope(A.limiter, A.theta, A.invd[2], Rb[v], Rz0[v], Rz1[v]);
+    }
+    double RL[V], RR[V];
+    double oT = M.offzT[k0 - 1 + 2], oB = M.offzB[k0 + 2];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      RL[v] = A.constant_recon ? Rb[v] : Rb[v] + szm[v] * oT;
+      RR[v] = A.constant_recon ? Rz0[v] : Rz0[v] + sz0[v] * oB;
+    }
+    kt_flux<ND, EU, PRIM>(2, RL, RR, EU ? 0.0 : M.cs[6 * M.nxp + ip], EU ? 0.0 : M.cs[5 * M.nxp + ip],
+                          M.dAzB[ip], P, Fzm);
+  }
+
+  for (int k = k0; k < k1; ++k) {
+    double divZ[V];
+    // ---- own cell: plane k into shared memory; z-flux at k+1/2
+    if (own) {
+      double Rc[V];
+      if (ND == 3) {
+        double Rz2[V], sz1[V], Fzp[V];
+        recon_at(i, j, k + 2, Rz2);
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+          sz1[v] = A.constant_recon ? 0.0 : slope(A.limiter, A.theta, A.invd[2], Rz0[v], Rz1[v], Rz2[v]);
+        double RL[V], RR[V];
+        double oT = M.offzT[k + 2], oB = M.offzB[k + 1 + 2];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          RL[v] = A.constant_recon ? Rz0[v] : Rz0[v] + sz0[v] * oT;
+          RR[v] = A.constant_recon ? Rz1[v] : Rz1[v] + sz1[v] * oB;
+        }
+        kt_flux<ND, EU, PRIM>(2, RL, RR, EU ? 0.0 : M.cs[6 * M.nxp + ip], EU ? 0.0 : M.cs[5 * M.nxp + ip],
+                              M.dAzB[ip], P, Fzp);
+        double dV = M.dxdydV[ip];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          divZ[v] = dV * (Fzp[v] - Fzm[v]);
+          Rc[v] = Rz0[v];
+          Rz0[v] = Rz1[v];
+          Rz1[v] = Rz2[v];
+          sz0[v] = sz1[v];
+          Fzm[v] = Fzp[v];
+        }
+      } else {
+        recon_at(i, j, k, Rc);
+      }
+#pragma unroll
+      for (int v = 0; v < V; ++v) RS(v, ty + 2, tx + 2) = Rc[v];
+    }
+    // ---- x-y cross halo of plane k
+    {
+      const int H = 4 * (ex + ey);
+      for (int h = tid; h < H; h += NT) {
+        int lx, ly;
+        if (h < 4 * ey) {
+          int r = h >> 2, q = h & 3;
+          ly = r;
+          lx = q < 2 ? q - 2 : ex + (q - 2);
+        } else {
+          int hh = h - 4 * ey;
+          int c = hh >> 2, q = hh & 3;
+          lx = c;
+          ly = q < 2 ? q - 2 : ey + (q - 2);
+        }
+        double R[V];
+        recon_at(i0 + lx, j0 + ly, k, R);
+#pragma unroll
+        for (int v = 0; v < V; ++v) RS(v, ly + 2, lx + 2) = R[v];
+      }
+    }
+    __syncthreads();
+
+    double divX[V], divY[V];
+    // ---- x direction: slopes, interface fluxes, divergence
+    if (!A.constant_recon) {
+      for (int t = tid; t < (ex + 2) * ey; t += NT) {
+        int r = t / (ex + 2), c = t % (ex + 2) - 1;
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+          SS(v, r, c + 1) = slope(A.limiter, A.theta, A.invd[0], RS(v, r + 2, c + 1), RS(v, r + 2, c + 2), RS(v, r + 2, c + 3));
+      }
+      __syncthreads();
+    }
+    for (int t = tid; t < (ex + 1) * ey; t += NT) {
+      int r = t / (ex + 1), f = t % (ex + 1);
+      int gl = i0 + f - 1 + 2;   // padded i of the left cell
+      double RL[V], RR[V], F[V];
+      double oE = M.offxE[gl], oW = M.offxW[gl + 1];
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        RL[v] = A.constant_recon ? RS(v, r + 2, f + 1) : RS(v, r + 2, f + 1) + SS(v, r, f) * oE;
+        RR[v] = A.constant_recon ? RS(v, r + 2, f + 2) : RS(v, r + 2, f + 2) + SS(v, r, f + 1) * oW;
+      }
+      kt_flux<ND, EU, PRIM>(0, RL, RR, EU ? 0.0 : M.cs[2 * M.nxp + gl], EU ? 0.0 : M.cs[1 * M.nxp + gl + 1],
+                            M.dAxW[gl + 1], P, F);
+#pragma unroll
+      for (int v = 0; v < V; ++v) FS(v, r, f) = F[v];
+    }
+    __syncthreads();
+    if (own) {
+      double dV = M.dydzdV[ip];
+#pragma unroll
+      for (int v = 0; v < V; ++v) divX[v] = dV * (FS(v, ty, tx + 1) - FS(v, ty, tx));
+    }
+    __syncthreads();
+    // ---- y direction
+    if (!A.constant_recon) {
+      for (int t = tid; t < ex * (ey + 2); t += NT) {
+        int c = t % ex, r = t / ex - 1;
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+          SS(v, r + 1, c) = slope(A.limiter, A.theta, A.invd[1], RS(v, r + 1, c + 2), RS(v, r + 2, c + 2), RS(v, r + 3, c + 2));
+      }
+      __syncthreads();
+    }
+    for (int t = tid; t < ex * (ey + 1); t += NT) {
+      int c = t % ex, f = t / ex;
+      int gjl = j0 + f - 1 + 2;     // padded j of the lower cell
+      int gi = i0 + c + 2;          // padded i of the column
+      double RL[V], RR[V], F[V];
+      double oN = M.offyN[gjl], oS = M.offyS[gjl + 1];
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        RL[v] = A.constant_recon ? RS(v, f + 1, c + 2) : RS(v, f + 1, c + 2) + SS(v, f, c) * oN;
+        RR[v] = A.constant_recon ? RS(v, f + 2, c + 2) : RS(v, f + 2, c + 2) + SS(v, f + 1, c) * oS;
+      }
+      kt_flux<ND, EU, PRIM>(1, RL, RR, EU ? 0.0 : M.cs[4 * M.nxp + gi], EU ? 0.0 : M.cs[3 * M.nxp + gi],
+                            M.dAyS[gi], P, F);
+#pragma unroll
+      for (int v = 0; v < V; ++v) FS(v, f, c) = F[v];
+    }
+    __syncthreads();
+
+    if (own) {
+      double dV = M.dzdxdV[ip];
+#pragma unroll
+      for (int v = 0; v < V; ++v) divY[v] = dV * (FS(v, ty + 1, tx) - FS(v, ty, tx));
+      const long long idx = CE::lin(g, i, j, k);
+      // centre primitive / conservative state as ComputeRHS sees it
+      double pc[V], cc[V];
+      double R0[V];
+#pragma unroll
+      for (int v = 0; v < V; ++v) R0[v] = RS(v, ty + 2, tx + 2);
+      if (PRIM) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) pc[v] = R0[v];
+        PH::p2c(pc, cc, P);
+      } else {
+#pragma unroll
+        for (int v = 0; v < V; ++v) cc[v] = R0[v];
+        if (roundtrip) {
+          double u[V];
+          state_at<V>(A.in, g.n, idx, u);
+          PH::c2p(u, pc, P);
+          pc[V - 1] = dmax(pc[V - 1], P.pmin);
+        } else {
+          PH::c2p(cc, pc, P);
+        }
+      }
+      double rhs[V];
+#pragma unroll
+      for (int v = 0; v < V; ++v) rhs[v] = (divX[v] + divY[v]) + (ND == 3 ? divZ[v] : 0.0);
+      // geometric sources (physics_euler.f90:1706-1847 / physics_eulerisotherm.f90:689-832)
+      if (M.curv) {
+        double Pp = EU ? pc[V - 1] : pc[0] * (M.cs[ip] * M.cs[ip]);
+        double vx = pc[1], vy = pc[2];
+        double cxyx = M.cxyx[ip], cyxy = M.cyxy[ip], czxz = M.czxz[ip], czyz = M.czyz[ip];
+        if (ND == 2) {
+          double mx = cc[1], my = cc[2];
+          rhs[1] = rhs[1] - (my * (cyxy * vy - cxyx * vx) + (cyxy + czxz) * Pp);
+          rhs[2] = rhs[2] - (mx * (cxyx * vx - cyxy * vy) + (cxyx + czyz) * Pp);
+        } else {
+          double vz = pc[3], mx = cc[1], my = cc[2], mz = cc[3];
+          double cxzx = M.cxzx[ip], cyzy = M.cyzy[ip];
+          rhs[1] = rhs[1] - (my * (cyxy * vy - cxyx * vx) + mz * (czxz * vz - cxzx * vx) + (cyxy + czxz) * Pp);
+          rhs[2] = rhs[2] - (mz * (czyz * vz - cyzy * vy) + mx * (cxyx * vx - cyxy * vy) + (cxyx + czyz) * Pp);
+          rhs[3] = rhs[3] - (mx * (cxzx * vx - czxz * vz) + my * (cyzy * vy - czyz * vz) + (cxzx + cyzy) * Pp);
+        }
+      }
+      // point-mass gravity (gravity_pointmass.f90:263-282, physics ExternalSources)
+      if (A.has_accel) {
+        double ax = M.accel[ip], ay = M.accel[M.nxp + ip];
+        rhs[1] = rhs[1] - cc[0] * ax;
+        rhs[2] = rhs[2] - cc[0] * ay;
+        if (EU) rhs[V - 1] = rhs[V - 1] - (cc[1] * ax + cc[2] * ay);
+      }
+
+      if (A.out_mode == OUT_RHS) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) A.out[(long long)v * g.n + idx] = rhs[v];
+      } else {
+        // Shu-Osher update y = yn - dt*rhs + eta*(y0 - yn + dt*rhs) (timedisc_modeuler.f90:289)
+        double yn[V], y0[V], y[V];
+        if (!PRIM) {
+#pragma unroll
+          for (int v = 0; v < V; ++v) yn[v] = cc[v];
+        } else if (roundtrip) {
+#pragma unroll
+          for (int v = 0; v < V; ++v) yn[v] = cc[v];
+        } else {
+          state_at<V>(A.in, g.n, idx, yn);
+        }
+#pragma unroll
+        for (int v = 0; v < V; ++v) y0[v] = __ldg(A.y0 + (long long)v * g.n + idx);
+        if (EU && A.y0_roundtrip) {
+          double q[V];
+          PH::c2p(y0, q, P);
+          q[V - 1] = dmax(q[V - 1], P.pmin);
+          PH::p2c(q, y0, P);
+        }
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          y[v] = yn[v] - dt * rhs[v] + A.eta * (y0[v] - yn[v] + dt * rhs[v]);
+          A.out[(long long)v * g.n + idx] = y[v];
+        }
+        if (A.cfl_mode == 1) {
+          double p[V], c[V];
+          PH::c2p(y, p, P);
+          if (EU && A.cfl_roundtrip) p[V - 1] = dmax(p[V - 1], P.pmin);
+          double cs = EU ? PH::cs_of(p, P) : M.cs[ip];
+          CE::cfl_cell(p, cs, M, ip, cflv);
+          if (EU && A.cfl_roundtrip) PH::p2c(p, c, P);
+          else { for (int v = 0; v < V; ++v) c[v] = y[v]; }
+          if ((A.checkdata & 0x01) && !(cs > 0.)) flags |= 0x01;
+          if (EU && (A.checkdata & 0x02) && p[V - 1] < P.pmin) flags |= 0x02;
+          if ((A.checkdata & 0x04) && p[0] < P.rhomin) flags |= 0x04;
+          if (A.checkdata & 0x08)
+            for (int v = 0; v < V; ++v) if (!isfinite(p[v]) || !isfinite(c[v])) flags |= 0x08;
+        }
+      }
+      if (A.out_base) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) A.out_base[(long long)v * g.n + idx] = cc[v];
+      }
+      if (A.cfl_mode == 2) {
+        double cs = EU ? PH::cs_of(pc, P) : M.cs[ip];
+        CE::cfl_cell(pc, cs, M, ip, cflv);
+        if ((A.checkdata & 0x01) && !(cs > 0.)) flags |= 0x01;
+        if (EU && (A.checkdata & 0x02) && pc[V - 1] < P.pmin) flags |= 0x02;
+        if ((A.checkdata & 0x04) && pc[0] < P.rhomin) flags |= 0x04;
+        if (A.checkdata & 0x08)
+          for (int v = 0; v < V; ++v) if (!isfinite(pc[v]) || !isfinite(cc[v])) flags |= 0x08;
+      }
+      if (A.last_stage) {
+        // high/low order solutions and ComputeError (timedisc_rkfehlberg.f90:198-265,
+        // timedisc_base.f90:1012-1053)
+        double hi[V], lo[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          double b = __ldg(A.in.base + (long long)v * g.n + idx);
+          double h = b, l = b;
+          for (int q = 0; q < A.nstage - 1; ++q) {
+            double kq = __ldg(A.in.K[q] + (long long)v * g.n + idx);
+            l = l - A.bl_dt[q] * kq;
+            h = h - A.bh_dt[q] * kq;
+          }
+          l = l - A.bl_dt[A.nstage - 1] * rhs[v];
+          h = h - A.bh_dt[A.nstage - 1] * rhs[v];
+          hi[v] = h;
+          lo[v] = l;
+          A.out_high[(long long)v * g.n + idx] = h;
+          double e = fabs(h - l) / (A.tol_rel * fabs(h) + A.tol_abs[v]);
+          errv = v == 0 ? e : dmax(errv, e);
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  if (A.ctl && (A.cfl_mode || A.last_stage)) {
+    int nv = A.cfl_mode ? (ND == 3 ? 3 : 1) : 0;
+    double vals[3] = {cflv[0], cflv[1], cflv[2]};
+    if (A.last_stage && !A.cfl_mode) { vals[0] = errv; nv = 1; }
+    if (nv) block_reduce_emit<NT>(vals, nv, flags, A.last_stage && !A.cfl_mode ? &A.ctl->err : A.ctl->invdt,
+                                  &A.ctl->flags, sred);
+  }
+}
+
+}  // namespace fgpu

@@ -1,0 +1,227 @@
+// fgpu_kernels_misc.cuh -- boundary-cell CFL/CheckData reduction with the
+// step finalisation, interior CFL pass, and the padded download kernel.
+#pragma once
+#include "fgpu_kernels.cuh"
+
+namespace fgpu {
+
+enum { FIN_NONE = 0, FIN_FIRST = 1, FIN_STEP = 2 };
+
+struct BndArgs {
+  Grid g;
+  PhysP ph;
+  MetricP mt;
+  StateRef in;
+  int roundtrip;
+  int checkdata;
+  Ctl* ctl;
+  int finalize;
+  long long nghost;
+  double* out_p;   // optional: padded primitive output (ghost cells)
+  double* out_c;   // optional: padded conservative output (ghost cells)
+  long long npad;  // padded cell count (field stride of out_p/out_c)
+};
+
+// ghost cell number t -> padded coordinates (x slabs, then y slabs, then z slabs)
+template <int ND>
+__device__ __forceinline__ void ghost_coords(const Grid& g, long long t, int& px, int& py, int& pz) {
+  const int NXp = g.nx + 4, NYp = g.ny + 4, NZp = ND == 3 ? g.nz + 4 : 1;
+  long long nxs = 4LL * NYp * NZp;
+  if (t < nxs) {
+    int q = (int)(t % 4); long long r = t / 4;
+    px = q < 2 ? q : NXp - 4 + q;
+    py = (int)(r % NYp); pz = (int)(r / NYp);
+    return;
+  }
+  t -= nxs;
+  long long nys = 4LL * g.nx * NZp;
+  if (t < nys) {
+    int q = (int)(t % 4); long long r = t / 4;
+    py = q < 2 ? q : NYp - 4 + q;
+    px = 2 + (int)(r % g.nx); pz = (int)(r / g.nx);
+    return;
+  }
+  t -= nys;
+  int q = (int)(t % 4); long long r = t / 4;
+  pz = q < 2 ? q : NZp - 4 + q;
+  px = 2 + (int)(r % g.nx); py = 2 + (int)(r / g.nx);
+}
+
+// The step's closing scalar work, run by the last block of the boundary pass:
+// CalcTimestep (timedisc_base.f90:818-909), the time advance of IntegrationStep
+// (timedisc_base.f90:714-720), the stop test of fosite%Step (fosite.f90:383-388)
+// and the output-time clip of fileio%AdjustTimestep (io/fileio_base.f90:604-621).
+template <int ND>
+__device__ void finalize_step(Ctl* c, int mode) {
+  if (mode == FIN_STEP) {
+    c->time = c->time + c->dt;
+    c->dtold = c->dt;
+    c->iter += 1;
+  }
+  if (c->flags) c->brk = 1;
+  double invdt;
+  if (ND == 2) invdt = __longlong_as_double((long long)c->invdt[0]);
+  else {
+    double ix = __longlong_as_double((long long)c->invdt[0]);
+    double iy = __longlong_as_double((long long)c->invdt[1]);
+    double iz = __longlong_as_double((long long)c->invdt[2]);
+    invdt = dmax(dmax(iy, iz), ix);
+  }
+  c->invdt[0] = c->invdt[1] = c->invdt[2] = 0ULL;
+  if (c->brk) { c->stop = 1; return; }
+  double dt = c->cfl / invdt;
+  int cause = 0;
+  if (fabs(c->stoptime - c->time) <= 1.0E-05 * c->stoptime) { c->stop = 1; c->dt = dt; c->dtcause = cause; return; }
+  double tout = c->tout;
+  if ((c->time + dt) / tout > 1.0) { dt = tout - c->time; cause = -4; }
+  else if ((c->time + 1.5 * dt) / tout > 1.0) { dt = 0.5 * (tout - c->time); cause = -4; }
+  if (dt < c->dtmin && cause != -4) c->dtmin = dt;
+  c->dt = dt;
+  c->dtcause = cause;
+}
+
+template <int ND, bool EU>
+__global__ void __launch_bounds__(256) boundary_kernel(const __grid_constant__ BndArgs A) {
+  using PH = Phys<ND, EU>;
+  using CE = Cells<ND, EU>;
+  constexpr int V = PH::V;
+  __shared__ double sred[4 * 8];
+  __shared__ bool is_last;
+  if (A.ctl && A.finalize != FIN_FIRST && (A.ctl->stop | A.ctl->brk)) return;
+  const MetricP& M = A.mt;
+  double cflv[3] = {0.0, 0.0, 0.0};
+  int flags = 0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < A.nghost;
+       t += (long long)gridDim.x * blockDim.x) {
+    int px, py, pz;
+    ghost_coords<ND>(A.g, t, px, py, pz);
+    double p[V], c[V];
+    CE::cell_p(A.in, A.g, A.ph, M, px - 2, py - 2, ND == 3 ? pz - 2 : 0, p);
+    if (EU && A.roundtrip) p[V - 1] = dmax(p[V - 1], A.ph.pmin);
+    PH::p2c(p, c, A.ph);
+    double cs = EU ? PH::cs_of(p, A.ph) : M.cs[px];
+    double v3[3];
+    CE::cfl_cell(p, cs, M, px, v3);
+    cflv[0] = dmax(cflv[0], v3[0]);
+    if (ND == 3) { cflv[1] = dmax(cflv[1], v3[1]); cflv[2] = dmax(cflv[2], v3[2]); }
+    if ((A.checkdata & 0x01) && !(cs > 0.)) flags |= 0x01;
+    if (A.checkdata & 0x08)
+      for (int v = 0; v < V; ++v) if (!isfinite(p[v]) || !isfinite(c[v])) flags |= 0x08;
+    if (A.out_p) {
+      long long pi = px + (long long)(A.g.nx + 4) * (py + (long long)(A.g.ny + 4) * pz);
+      for (int v = 0; v < V; ++v) {
+        A.out_p[v * A.npad + pi] = p[v];
+        A.out_c[v * A.npad + pi] = c[v];
+      }
+    }
+  }
+  if (!A.ctl) return;
+  block_reduce_emit<256>(cflv, ND == 3 ? 3 : 1, flags, A.ctl->invdt, &A.ctl->flags, sred);
+  if (A.finalize == FIN_NONE) return;
+  __threadfence();
+  if (threadIdx.x == 0) {
+    unsigned int done = atomicAdd(&A.ctl->blocks_done, 1u);
+    is_last = (done == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (is_last && threadIdx.x == 0) {
+    __threadfence();
+    A.ctl->blocks_done = 0;
+    finalize_step<ND>(A.ctl, A.finalize);
+  }
+}
+
+// CFL and CheckData of the interior cells of a stored state (FirstStep).
+template <int ND, bool EU>
+__global__ void __launch_bounds__(256) interior_cfl_kernel(const __grid_constant__ BndArgs A) {
+  using PH = Phys<ND, EU>;
+  using CE = Cells<ND, EU>;
+  constexpr int V = PH::V;
+  __shared__ double sred[4 * 8];
+  const MetricP& M = A.mt;
+  double cflv[3] = {0.0, 0.0, 0.0};
+  int flags = 0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < A.g.n;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(t % A.g.nx);
+    double u[V], p[V], c[V];
+    state_at<V>(A.in, A.g.n, t, u);
+    PH::c2p(u, p, A.ph);
+    if (EU && A.roundtrip) { p[V - 1] = dmax(p[V - 1], A.ph.pmin); PH::p2c(p, c, A.ph); }
+    else { for (int v = 0; v < V; ++v) c[v] = u[v]; }
+    double cs = EU ? PH::cs_of(p, A.ph) : M.cs[i + 2];
+    double v3[3];
+    CE::cfl_cell(p, cs, M, i + 2, v3);
+    cflv[0] = dmax(cflv[0], v3[0]);
+    if (ND == 3) { cflv[1] = dmax(cflv[1], v3[1]); cflv[2] = dmax(cflv[2], v3[2]); }
+    if ((A.checkdata & 0x01) && !(cs > 0.)) flags |= 0x01;
+    if (EU && (A.checkdata & 0x02) && p[V - 1] < A.ph.pmin) flags |= 0x02;
+    if ((A.checkdata & 0x04) && p[0] < A.ph.rhomin) flags |= 0x04;
+    if (A.checkdata & 0x08)
+      for (int v = 0; v < V; ++v) if (!isfinite(p[v]) || !isfinite(c[v])) flags |= 0x08;
+  }
+  block_reduce_emit<256>(cflv, ND == 3 ? 3 : 1, flags, A.ctl->invdt, &A.ctl->flags, sred);
+}
+
+// Interior cells of a stored state into padded primitive/conservative arrays.
+template <int ND, bool EU>
+__global__ void __launch_bounds__(256) pack_interior_kernel(const __grid_constant__ BndArgs A) {
+  using PH = Phys<ND, EU>;
+  constexpr int V = PH::V;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < A.g.n;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(t % A.g.nx);
+    long long r = t / A.g.nx;
+    int j = (int)(r % A.g.ny), k = (int)(r / A.g.ny);
+    double u[V], p[V], c[V];
+    state_at<V>(A.in, A.g.n, t, u);
+    PH::c2p(u, p, A.ph);
+    if (EU && A.roundtrip) { p[V - 1] = dmax(p[V - 1], A.ph.pmin); PH::p2c(p, c, A.ph); }
+    else { for (int v = 0; v < V; ++v) c[v] = u[v]; }
+    int kk = ND == 3 ? k + 2 : 0;
+    long long pi = (i + 2) + (long long)(A.g.nx + 4) * ((j + 2) + (long long)(A.g.ny + 4) * kk);
+    for (int v = 0; v < V; ++v) {
+      A.out_p[v * A.npad + pi] = p[v];
+      A.out_c[v * A.npad + pi] = c[v];
+    }
+  }
+}
+
+// Interior cells of a ghost-padded caller array into the stored state
+// (fgpu_upload_state); primitive input is converted with Prim2Cons.
+template <int ND, bool EU>
+__global__ void __launch_bounds__(256) unpack_kernel(const double* __restrict__ pad, double* __restrict__ out,
+                                                     Grid g, long long npad, int prim, PhysP P) {
+  using PH = Phys<ND, EU>;
+  constexpr int V = PH::V;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < g.n; t += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(t % g.nx);
+    long long r = t / g.nx;
+    int j = (int)(r % g.ny), k = (int)(r / g.ny);
+    int kk = ND == 3 ? k + 2 : 0;
+    long long pi = (i + 2) + (long long)(g.nx + 4) * ((j + 2) + (long long)(g.ny + 4) * kk);
+    double u[V], c[V];
+    for (int v = 0; v < V; ++v) u[v] = pad[v * npad + pi];
+    if (prim) PH::p2c(u, c, P);
+    else for (int v = 0; v < V; ++v) c[v] = u[v];
+    for (int v = 0; v < V; ++v) out[v * g.n + t] = c[v];
+  }
+}
+
+// Apply the CHECK_PMIN round trip to a stored state: out = P2C(MAX(C2P(in),pmin)).
+template <int ND, bool EU>
+__global__ void __launch_bounds__(256) roundtrip_kernel(const double* __restrict__ in, double* __restrict__ out,
+                                                        long long n, PhysP P) {
+  using PH = Phys<ND, EU>;
+  constexpr int V = PH::V;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    double u[V], p[V], c[V];
+    for (int v = 0; v < V; ++v) u[v] = in[v * n + t];
+    PH::c2p(u, p, P);
+    if (EU) p[V - 1] = dmax(p[V - 1], P.pmin);
+    PH::p2c(p, c, P);
+    for (int v = 0; v < V; ++v) out[v * n + t] = c[v];
+  }
+}
+
+}  // namespace fgpu

@@ -1,0 +1,176 @@
+"""Python host mirror of the fosite time-step interface, driving the C ABI.
+
+``Simulation`` follows the sequence of fosite's own driver (fosite.f90:
+Setup -> InitData -> FirstStep -> Step/Run) with the state kept on the GPU:
+``set_state`` stands for InitData's Timedisc%pvar/cvar fill, ``first_step`` for
+fosite%FirstStep, ``step``/``run`` for fosite%Step/Run, and ``get`` for reading
+Timedisc%cvar/pvar back.  Every call goes through include/fosite_gpu.h; there
+is no CPU path: if the CUDA library is missing the import fails.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_libs = {}
+
+
+def lib_path(exact=False):
+    name = "libfosite_gpu_exact.so" if exact else "libfosite_gpu.so"
+    return os.path.join(_HERE, "lib", name)
+
+
+def lib(exact=False):
+    """Load the CUDA library; raise if it was not built (no fallback exists)."""
+    if exact in _libs:
+        return _libs[exact]
+    path = lib_path(exact)
+    if not os.path.exists(path):
+        raise RuntimeError("fosite_b200: CUDA library %s is missing; run fosite_b200/build.py" % path)
+    L = C.CDLL(path)
+    L.fgpu_config_init.argtypes = [C.POINTER(abi.Config)]
+    L.fgpu_create.argtypes = [C.POINTER(abi.Config), C.c_int, C.POINTER(C.c_void_p)]
+    L.fgpu_destroy.argtypes = [C.c_void_p]
+    L.fgpu_last_error.argtypes = [C.c_void_p, C.c_char_p, C.c_int]
+    L.fgpu_state_size.argtypes = [C.c_void_p]
+    L.fgpu_state_size.restype = C.c_int64
+    L.fgpu_cell_count.argtypes = [C.c_void_p]
+    L.fgpu_cell_count.restype = C.c_int64
+    L.fgpu_vnum.argtypes = [C.c_void_p]
+    L.fgpu_get_mesh.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int64]
+    L.fgpu_set_sound_speeds.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64]
+    L.fgpu_upload_state.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int64]
+    L.fgpu_download.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int64]
+    L.fgpu_first_step.argtypes = [C.c_void_p]
+    L.fgpu_step.argtypes = [C.c_void_p]
+    L.fgpu_run.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]
+    L.fgpu_compute_rhs.argtypes = [C.c_void_p]
+    L.fgpu_calc_timestep.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    L.fgpu_get_status.argtypes = [C.c_void_p, C.POINTER(abi.Status)]
+    L.fgpu_synchronize.argtypes = [C.c_void_p]
+    L.fgpu_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+    L.fgpu_set_profiling.argtypes = [C.c_void_p, C.c_int]
+    L.fgpu_get_stats.argtypes = [C.c_void_p, C.POINTER(abi.Stats)]
+    L.fgpu_reset_stats.argtypes = [C.c_void_p]
+    _libs[exact] = L
+    return L
+
+
+class FositeError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("fosite_b200 error %d: %s" % (code, msg))
+        self.code = code
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Simulation:
+    """One grid, one CUDA stream, state resident in HBM."""
+
+    def __init__(self, cfg, device=-1, exact=False):
+        self.L = lib(exact)
+        self.cfg = abi.finalize_config(abi.config_copy(cfg))
+        h = C.c_void_p()
+        rc = self.L.fgpu_create(C.byref(self.cfg), device, C.byref(h))
+        if rc != 0:
+            buf = C.create_string_buffer(512)
+            self.L.fgpu_last_error(None, buf, 512)
+            raise FositeError(rc, buf.value.decode())
+        self.h = h
+        self.vnum = int(self.L.fgpu_vnum(h))
+        self.ncells = int(self.L.fgpu_cell_count(h))
+        g = lambda n: 2 if n > 1 else 0
+        c = self.cfg
+        self.shape = (c.knum + 2 * g(c.knum), c.jnum + 2 * g(c.jnum), c.inum + 2 * g(c.inum))
+        self.nfaces = 2 * sum(1 for n in (c.inum, c.jnum, c.knum) if n > 1)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.fgpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, soft_ok=True):
+        if rc < 0 or (rc > 0 and not soft_ok):
+            buf = C.create_string_buffer(512)
+            self.L.fgpu_last_error(self.h, buf, 512)
+            raise FositeError(rc, buf.value.decode())
+        return rc
+
+    # ---- mesh / physics data
+    def mesh(self, which):
+        out = np.zeros(self.ncells)
+        self._check(self.L.fgpu_get_mesh(self.h, which, _ptr(out), out.size))
+        return out.reshape(self.shape)
+
+    def set_sound_speeds(self, bccsound, fcsound):
+        b = np.ascontiguousarray(bccsound, dtype=np.float64)
+        f = np.ascontiguousarray(fcsound, dtype=np.float64)
+        self._check(self.L.fgpu_set_sound_speeds(self.h, _ptr(b), b.size, _ptr(f), f.size))
+
+    # ---- state
+    def set_state(self, which, data):
+        d = np.ascontiguousarray(data, dtype=np.float64)
+        self._check(self.L.fgpu_upload_state(self.h, which, _ptr(d), d.size))
+
+    def get(self, which):
+        n = self.ncells if which == abi.BCCSOUND else self.ncells * self.vnum
+        out = np.zeros(n)
+        self._check(self.L.fgpu_download(self.h, which, _ptr(out), out.size))
+        if which == abi.BCCSOUND:
+            return out.reshape(self.shape)
+        return out.reshape((self.vnum,) + self.shape)
+
+    # ---- stepping
+    def first_step(self):
+        return self._check(self.L.fgpu_first_step(self.h))
+
+    def step(self):
+        return self._check(self.L.fgpu_step(self.h))
+
+    def run(self, n):
+        done = C.c_int64(0)
+        rc = self._check(self.L.fgpu_run(self.h, int(n), C.byref(done)))
+        return rc, int(done.value)
+
+    def compute_rhs(self):
+        self._check(self.L.fgpu_compute_rhs(self.h))
+        return self.get(abi.RHS)
+
+    def calc_timestep(self):
+        d = C.c_double()
+        self._check(self.L.fgpu_calc_timestep(self.h, C.byref(d)))
+        return d.value
+
+    def status(self):
+        st = abi.Status()
+        self._check(self.L.fgpu_get_status(self.h, C.byref(st)))
+        return st
+
+    def synchronize(self):
+        self._check(self.L.fgpu_synchronize(self.h))
+
+    def set_stream(self, stream_handle):
+        """Enqueue on a caller stream (e.g. torch.cuda.current_stream().cuda_stream)."""
+        self._check(self.L.fgpu_set_stream(self.h, C.c_void_p(stream_handle or None)))
+
+    def set_profiling(self, on):
+        self._check(self.L.fgpu_set_profiling(self.h, 1 if on else 0))
+
+    def stats(self):
+        st = abi.Stats()
+        self._check(self.L.fgpu_get_stats(self.h, C.byref(st)))
+        return st
+
+    def reset_stats(self):
+        self._check(self.L.fgpu_reset_stats(self.h))

@@ -1,0 +1,260 @@
+/*
+ * fosite_gpu.h -- C ABI of the B200 (sm_100a) backend for fosite's explicit
+ * finite-volume time step.
+ *
+ * The entry points below are what a Fortran 2008 caller binds with
+ * ISO_C_BINDING (see INTEGRATION.md for the BIND(C) interface block).  Every
+ * call takes plain pointers and sizes; no C++ or torch type crosses the
+ * boundary.  All state arrays exchanged with the caller use fosite's own
+ * layout: Fortran order, i fastest, ghost-padded by two cells in every active
+ * direction (mesh/marray_base.f90:146-290, mesh/marray_compound.f90:275-391),
+ * i.e. data4d(IGMIN:IGMAX, JGMIN:JGMAX, KGMIN:KGMAX, 1:VNUM) flattened.
+ *
+ * Ownership: the library copies on upload and download and owns all device
+ * memory for the lifetime of a handle.  One handle owns one CUDA stream;
+ * calls on one handle must be serialised by the caller, distinct handles may
+ * be used from different threads.
+ *
+ * Return codes: FGPU_OK (0); positive values are soft conditions that the
+ * fosite shim maps onto Timedisc%break; negative values are hard errors that
+ * it maps onto this%Error (fgpu_last_error() gives the message).  Nothing in
+ * the library calls exit(), abort() or traps on the device.
+ */
+#ifndef FOSITE_GPU_H
+#define FOSITE_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- fosite's own integer identifiers (same values as the Fortran code) ---- */
+/* geometries: mesh/geometry_base.f90:345-361 */
+#define FGPU_CARTESIAN        1
+#define FGPU_CYLINDRICAL      30
+#define FGPU_LOGCYLINDRICAL   31
+/* physics: physics/physics_base.f90:496-498 */
+#define FGPU_EULER_ISOTHERM   16
+#define FGPU_EULER            17
+/* fluxes: fluxes/fluxes_base.f90:104 */
+#define FGPU_KT               1
+/* reconstruction order: fluxes/reconstruction_base.f90:78-79 */
+#define FGPU_CONSTANT         1
+#define FGPU_LINEAR           2
+/* reconstruction variables: physics/physics_base.f90:67 */
+#define FGPU_PRIMITIVE        1
+#define FGPU_CONSERVATIVE     2
+/* limiters: fluxes/reconstruction_linear.f90:71-78 (PP=6 is rejected, as in fosite) */
+#define FGPU_MINMOD           1
+#define FGPU_MONOCENT         2
+#define FGPU_SWEBY            3
+#define FGPU_SUPERBEE         4
+#define FGPU_OSPRE            5
+#define FGPU_PP               6
+#define FGPU_VANLEER          7
+#define FGPU_NOLIMIT          8
+/* boundary conditions: boundary/boundary_base.f90:110-126 */
+#define FGPU_NO_GRADIENTS     0x01
+#define FGPU_PERIODIC         0x02
+#define FGPU_REFLECTING       0x03
+#define FGPU_ABSORBING        0x0D
+/* boundary orientation: mesh/mesh_base.f90:102-107 (1-based there, 0-based here) */
+#define FGPU_WEST   0
+#define FGPU_EAST   1
+#define FGPU_SOUTH  2
+#define FGPU_NORTH  3
+#define FGPU_BOTTOM 4
+#define FGPU_TOP    5
+/* time integrators: timedisc/timedisc_base.f90:187-191 */
+#define FGPU_MODIFIED_EULER   1
+#define FGPU_RK_FEHLBERG      2
+#define FGPU_CASH_KARP        3
+#define FGPU_DORMAND_PRINCE   4
+#define FGPU_SSPRK            5
+/* checkdata bit mask: timedisc/timedisc_base.f90:197-204 */
+#define FGPU_CHECK_NOTHING    0x00
+#define FGPU_CHECK_CSOUND     0x01
+#define FGPU_CHECK_PMIN       0x02
+#define FGPU_CHECK_RHOMIN     0x04
+#define FGPU_CHECK_INVALID    0x08
+#define FGPU_CHECK_TMIN       0x10
+#define FGPU_CHECK_ALL        0xFF
+/* dtcause: timedisc/timedisc_base.f90:192-196 */
+#define FGPU_DTCAUSE_CFL       0
+#define FGPU_DTCAUSE_ERRADJ   -1
+#define FGPU_DTCAUSE_SMALLERR -2
+#define FGPU_DTCAUSE_FILEIO   -4
+
+/* ---- return codes ---- */
+#define FGPU_OK               0
+#define FGPU_BREAK            1   /* soft: NaN/Inf error norm, dt < dtlimit or CheckData failure */
+#define FGPU_STOPTIME         2   /* soft: |stoptime - time| <= 1e-5 stoptime, nothing was done */
+#define FGPU_EBADCFG         -1
+#define FGPU_ENOMEM          -2
+#define FGPU_ECUDA           -3
+#define FGPU_ETIMEOUT        -4
+#define FGPU_EUNSUPPORTED    -5
+#define FGPU_EARG            -6
+
+#define FGPU_MAXVAR 5
+
+/*
+ * Flat POD mirror of the fosite Dict keys read on the time-step path.  Field
+ * names follow the Dict keys (mesh/mesh_base.f90:31-63,
+ * timedisc/timedisc_base.f90:30-48,285-350, fluxes/reconstruction_linear.f90:
+ * 116-117, physics/physics_base.f90, sources/gravity_pointmass.f90:160-190,
+ * boundary/boundary_generic.f90:145-245).  fgpu_config_init() fills fosite's
+ * defaults; a Fortran shim translates the caller's Dict into this struct.
+ */
+typedef struct fgpu_config {
+    /* mesh */
+    int32_t inum, jnum, knum;      /* interior cells per direction (1 = collapsed) */
+    int32_t geometry;              /* FGPU_CARTESIAN / _CYLINDRICAL / _LOGCYLINDRICAL */
+    double  xmin, xmax, ymin, ymax, zmin, zmax;
+    double  gparam;                /* logcylindrical scale, default 1.0 */
+    /* physics */
+    int32_t physics;               /* FGPU_EULER or FGPU_EULER_ISOTHERM */
+    double  gamma;                 /* default 1.4 */
+    double  csiso;                 /* isothermal sound speed; 0 = caller-supplied profile */
+    double  gn;                    /* gravitational constant of the unit system (1 = geometrical) */
+    /* fluxes / reconstruction */
+    int32_t fluxtype;              /* FGPU_KT */
+    int32_t order;                 /* FGPU_CONSTANT or FGPU_LINEAR */
+    int32_t variables;             /* FGPU_PRIMITIVE or FGPU_CONSERVATIVE (default) */
+    int32_t limiter;               /* default FGPU_MINMOD */
+    double  theta;                 /* MC / Sweby parameter, default 1.0 */
+    /* boundary conditions, indexed by FGPU_WEST..FGPU_TOP */
+    int32_t bc[6];
+    /* timedisc */
+    int32_t method;                /* FGPU_MODIFIED_EULER, FGPU_DORMAND_PRINCE, ... */
+    int32_t tdorder;               /* 0 = the method's default order */
+    double  cfl;                   /* default 0.4 */
+    double  stoptime;
+    double  dtlimit;               /* default EPSILON*stoptime */
+    double  tol_rel;               /* default 0.01 */
+    double  tol_abs[FGPU_MAXVAR];  /* default 0.001 */
+    double  beta;                  /* PI controller, default 0.08 */
+    int32_t maxiter;
+    int32_t checkdata;             /* default FGPU_CHECK_ALL */
+    double  pmin, rhomin, tmin;    /* default TINY(1.0) */
+    /* sources: central point mass (gravity/pointmass), 0 = off */
+    int32_t pointmass;
+    double  pm_mass;               /* default 1.0 */
+    /* fargo transport: method 0 off, 1 dynamic, 2 fixed background velocity */
+    int32_t fargo_method;
+    int32_t fargo_direction;       /* only 2 (azimuth) is supported */
+    /* output clip time for AdjustTimestep (io/fileio_base.f90:604-621); 0 = stoptime */
+    double  tout;
+} fgpu_config;
+
+/* Step bookkeeping returned to the caller (mirrors Timedisc%time/dt/...). */
+typedef struct fgpu_status {
+    double  time;        /* Timedisc%time */
+    double  dt;          /* Timedisc%dt: next step size */
+    double  dtold;       /* Timedisc%dtold */
+    double  dtmin;       /* Timedisc%dtmin */
+    double  maxerr;      /* last error norm returned by SolveODE */
+    int64_t iter;        /* accepted (sub-)steps, fosite%iter */
+    int64_t n_adj;       /* rejected attempts, Timedisc%n_adj */
+    int32_t dtcause;
+    int32_t brk;         /* Timedisc%break */
+    int32_t checkflags;  /* FGPU_CHECK_* bits that failed in CheckData */
+    int32_t pad;
+} fgpu_status;
+
+typedef struct fgpu_handle fgpu_handle;
+
+/* which-selectors for fgpu_download / fgpu_upload_state / fgpu_get_mesh */
+#define FGPU_CVAR        1   /* conservative state, ghost-padded, ghosts as CenterBoundary leaves them */
+#define FGPU_PVAR        2   /* primitive state, ghost-padded */
+#define FGPU_RHS         3   /* right-hand side of the last fgpu_compute_rhs (interior cells valid) */
+#define FGPU_BCCSOUND    4   /* cell-centre sound speed (ghost-padded) */
+#define FGPU_MESH_X      10  /* curvilinear cell-centre coordinates, ghost-padded scalar arrays */
+#define FGPU_MESH_Y      11
+#define FGPU_MESH_Z      12
+#define FGPU_MESH_RADIUS 13  /* Mesh%radius%bcenter */
+
+/* Fill a config with fosite's defaults (the GetAttr default values). */
+void fgpu_config_init(fgpu_config* cfg);
+
+/* Replaces the factories new_mesh/new_physics/new_fluxes/new_reconstruction/
+ * new_timedisc/new_boundary/InitSources (fosite.f90:184-248,
+ * timedisc/timedisc_generic.f90:45-87, fluxes/fluxes_generic.f90:46-68,
+ * boundary/boundary_generic.f90:104-283): validates the config, builds the
+ * metric on the host (mesh/mesh_base.f90:446-729, mesh/mesh_midpoint.f90:
+ * 97-145) and allocates device memory.  device < 0 uses the current device. */
+int  fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out);
+void fgpu_destroy(fgpu_handle* h);
+/* Copies the last error message of h (or of the last failed create when h is
+ * NULL) into buf; returns the message length. */
+int  fgpu_last_error(const fgpu_handle* h, char* buf, int len);
+
+/* Number of doubles of a ghost-padded state array (cells x VNUM) and of a
+ * ghost-padded scalar mesh array (cells). */
+int64_t fgpu_state_size(const fgpu_handle* h);
+int64_t fgpu_cell_count(const fgpu_handle* h);
+int     fgpu_vnum(const fgpu_handle* h);
+
+/* Mesh arrays for building initial data (Mesh%center / Mesh%radius). */
+int fgpu_get_mesh(fgpu_handle* h, int which, double* out, int64_t n);
+
+/* physics_eulerisotherm%SetSoundSpeeds (physics/physics_eulerisotherm.f90:
+ * 288-309): bccsound(IG,JG,KG) and fcsound(IG,JG,KG,NFACES).  The profiles
+ * may vary with the first coordinate only (disk setups set cs(r)); other
+ * profiles are rejected with FGPU_EUNSUPPORTED. */
+int fgpu_set_sound_speeds(fgpu_handle* h, const double* bccsound, int64_t nb,
+                          const double* fcsound, int64_t nf);
+
+/* Upload Timedisc%cvar (which = FGPU_CVAR) or Timedisc%pvar (FGPU_PVAR, then
+ * converted with Convert2Conservative).  Only interior cells are read. */
+int fgpu_upload_state(fgpu_handle* h, int which, const double* data, int64_t n);
+/* Download a ghost-padded array (FGPU_CVAR, FGPU_PVAR, FGPU_RHS, FGPU_BCCSOUND). */
+int fgpu_download(fgpu_handle* h, int which, double* out, int64_t n);
+
+/* fosite%FirstStep (fosite.f90:258-348): full ComputeRHS with CHECK_ALL and
+ * CalcTimestep.  Must be called once after the initial upload. */
+int fgpu_first_step(fgpu_handle* h);
+/* One fosite%Step (fosite.f90:367-464): stop-time test, dt clip to the
+ * output time, IntegrationStep (timedisc_base.f90:649-750) and
+ * CalcTimestep (timedisc_base.f90:818-909). */
+int fgpu_step(fgpu_handle* h);
+/* n consecutive fgpu_step calls; fixed-step schemes replay a captured CUDA
+ * graph with dt kept on the device.  *done receives the steps taken. */
+int fgpu_run(fgpu_handle* h, int64_t n, int64_t* done);
+/* Timedisc%ComputeRHS (timedisc_base.f90:1073-1271) of the current state with
+ * CHECK_NOTHING; the result is available through fgpu_download(FGPU_RHS). */
+int fgpu_compute_rhs(fgpu_handle* h);
+/* Timedisc%CalcTimestep of the current state (does not change the status). */
+int fgpu_calc_timestep(fgpu_handle* h, double* dt);
+int fgpu_get_status(fgpu_handle* h, fgpu_status* st);
+/* Block until all device work of h has finished. */
+int fgpu_synchronize(fgpu_handle* h);
+/* Enqueue all further work of h on a caller-owned CUDA stream (a cudaStream_t
+ * passed as void*); NULL returns to the handle's own stream.  No counterpart
+ * in the reference (host-only code); lets a caller order the solver with its
+ * own device work and time it with its own events. */
+int fgpu_set_stream(fgpu_handle* h, void* stream);
+
+/* Instrumentation (no counterpart in the reference, which only prints wall
+ * clock run times, fosite.f90:515-575).  With profiling on, every stage-kernel
+ * launch is bracketed by CUDA events on the handle's stream and its algorithmic
+ * HBM bytes (arrays read + written x VNUM x cells x 8) are accumulated;
+ * captured graphs are bypassed so each launch can be timed. */
+typedef struct fgpu_stats {
+    int64_t launches;         /* kernels launched by the library since the last reset */
+    int64_t stage_launches;   /* fused stage (RHS) kernels */
+    int64_t attempts;         /* time-step attempts (accepted + rejected) */
+    int64_t cell_updates;     /* interior cells x accepted steps */
+    double  stage_ms;         /* summed CUDA-event time of stage kernels (profiling on) */
+    double  stage_bytes;      /* algorithmic bytes of the timed stage kernels */
+    double  other_ms;         /* boundary / reduction kernels (profiling on) */
+} fgpu_stats;
+int fgpu_set_profiling(fgpu_handle* h, int on);
+int fgpu_get_stats(fgpu_handle* h, fgpu_stats* st);
+int fgpu_reset_stats(fgpu_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FOSITE_GPU_H */

@@ -1,0 +1,142 @@
+"""Small seeded parity cases shared by the oracle and GPU tests.
+
+Every case is a (name, builder) pair; builders return (cfg, pvar, extra) like
+fosite_b200.problems.  Sizes are deliberately not multiples of the kernel
+tiles so partial tiles and all boundary code paths are exercised.
+"""
+import numpy as np
+
+from fosite_b200 import abi, problems
+
+
+def _khi(n=(40, 36), limiter=abi.VANLEER, variables=abi.CONSERVATIVE, theta=1.0, order=abi.LINEAR,
+         method=abi.MODIFIED_EULER, tdorder=3, bcs=None, seed=11):
+    c = abi.default_config()
+    c.inum, c.jnum, c.knum = n[0], n[1], 1
+    c.xmin, c.xmax, c.ymin, c.ymax = -0.5, 0.5, -0.5, 0.5
+    c.physics = abi.EULER
+    c.gamma = 1.4
+    c.limiter = limiter
+    c.theta = theta
+    c.order = order
+    c.variables = variables
+    c.method = method
+    c.tdorder = tdorder
+    c.tol_rel = 10.0 if method == abi.MODIFIED_EULER else 1e-4
+    if method != abi.MODIFIED_EULER:
+        for v in range(abi.MAXVAR):
+            c.tol_abs[v] = 1e-4
+    c.cfl = 0.4
+    c.stoptime = 1.0e3
+    if bcs:
+        for f, t in enumerate(bcs):
+            c.bc[f] = t
+    abi.finalize_config(c)
+    X, Y, Z, _ = problems.centers(c)
+    rng = np.random.default_rng(seed)
+    p = np.zeros((4,) + X.shape)
+    band = np.abs(Y) < 0.25
+    p[0] = np.where(band, 2.0, 1.0)
+    p[1] = np.where(band, 0.5, -0.5) + rng.uniform(-1e-2, 1e-2, X.shape)
+    p[2] = 0.05 * np.sin(4 * np.pi * X) + rng.uniform(-1e-2, 1e-2, X.shape)
+    p[3] = 2.5 + 0.1 * np.exp(-((X - 0.1) ** 2 + Y ** 2) / 0.01)
+    return c, p, {}
+
+
+def _gauss3d(n=(20, 18, 16), variables=abi.PRIMITIVE, limiter=abi.MONOCENT, method=abi.DORMAND_PRINCE, tdorder=5,
+             bcs=None, tol=1e-5, seed=21):
+    c = abi.default_config()
+    c.inum, c.jnum, c.knum = n
+    c.xmin, c.xmax, c.ymin, c.ymax, c.zmin, c.zmax = -0.5, 0.5, -0.5, 0.5, -0.5, 0.5
+    for f in range(6):
+        c.bc[f] = abi.REFLECTING if bcs is None else bcs[f]
+    c.physics = abi.EULER
+    c.gamma = 1.4
+    c.limiter = limiter
+    c.variables = variables
+    c.method = method
+    c.tdorder = tdorder
+    c.tol_rel = tol
+    for v in range(abi.MAXVAR):
+        c.tol_abs[v] = tol
+    c.cfl = 0.4
+    c.stoptime = 1.0e3
+    abi.finalize_config(c)
+    X, Y, Z, _ = problems.centers(c)
+    rng = np.random.default_rng(seed)
+    p = np.zeros((5,) + X.shape)
+    p[0] = 1.0 + 1e-2 * rng.uniform(-1.0, 1.0, X.shape)
+    p[1] = 0.05 * rng.uniform(-1.0, 1.0, X.shape)
+    p[2] = 0.05 * rng.uniform(-1.0, 1.0, X.shape)
+    p[3] = 0.05 * rng.uniform(-1.0, 1.0, X.shape)
+    p[4] = 1.0 + 10.0 * np.exp(-((X - 0.05) ** 2 + Y ** 2 + (Z + 0.03) ** 2) / 0.01)
+    return c, p, {}
+
+
+def _disk(n=(32, 48), geometry=abi.LOGCYLINDRICAL, seed=31, hratio=0.05, variables=abi.PRIMITIVE):
+    c, p, extra = problems.disk2d(nr=n[0], nphi=n[1], seed=seed, hratio=hratio, geometry=geometry, fargo=0)
+    c.variables = variables
+    rng = np.random.default_rng(seed + 1)
+    p[1] = 0.01 * rng.uniform(-1, 1, p[1].shape)
+    return c, p, extra
+
+
+def _iso3d(n=(18, 16, 20), seed=41):
+    c = abi.default_config()
+    c.inum, c.jnum, c.knum = n
+    c.xmin, c.xmax, c.ymin, c.ymax, c.zmin, c.zmax = 0.0, 1.0, 0.0, 1.2, 0.0, 0.8
+    c.bc[:] = [abi.REFLECTING, abi.NO_GRADIENTS, abi.PERIODIC, abi.PERIODIC, abi.ABSORBING, abi.ABSORBING]
+    c.physics = abi.EULER_ISOTHERM
+    c.csiso = 0.7
+    c.limiter = abi.MINMOD
+    c.variables = abi.CONSERVATIVE
+    c.method = abi.CASH_KARP
+    c.tdorder = 5
+    c.tol_rel = 1e-4
+    for v in range(abi.MAXVAR):
+        c.tol_abs[v] = 1e-4
+    c.stoptime = 1.0e3
+    abi.finalize_config(c)
+    X, Y, Z, _ = problems.centers(c)
+    rng = np.random.default_rng(seed)
+    p = np.zeros((4,) + X.shape)
+    p[0] = 1.0 + 0.5 * np.exp(-((X - 0.4) ** 2 + (Y - 0.6) ** 2 + (Z - 0.4) ** 2) / 0.02) + 1e-3 * rng.uniform(-1, 1, X.shape)
+    p[1] = 0.1 * rng.uniform(-1, 1, X.shape)
+    p[2] = 0.2
+    p[3] = 0.1 * rng.uniform(-1, 1, X.shape)
+    return c, p, {}
+
+
+CASES = {
+    "khi_ssprk3_vanleer_cons": lambda: _khi(),
+    "khi_ssprk3_mc_prim": lambda: _khi(limiter=abi.MONOCENT, variables=abi.PRIMITIVE, theta=1.2),
+    "khi_superbee": lambda: _khi(limiter=abi.SUPERBEE, n=(33, 35)),
+    "khi_sweby": lambda: _khi(limiter=abi.SWEBY, theta=1.5, n=(24, 40)),
+    "khi_ospre": lambda: _khi(limiter=abi.OSPRE, n=(31, 17)),
+    "khi_nolimit_order2": lambda: _khi(limiter=abi.NOLIMIT, tdorder=2),
+    "khi_constant_order1": lambda: _khi(order=abi.CONSTANT, tdorder=1),
+    "euler2d_absorbing": lambda: _khi(bcs=[abi.ABSORBING] * 4, variables=abi.PRIMITIVE, n=(36, 34)),
+    "euler2d_reflect_nograd_ssprk5": lambda: _khi(bcs=[abi.REFLECTING, abi.REFLECTING, abi.NO_GRADIENTS, abi.NO_GRADIENTS],
+                                                 method=abi.SSPRK, tdorder=5, n=(30, 26)),
+    "euler2d_rkf45": lambda: _khi(method=abi.RK_FEHLBERG, tdorder=5, n=(28, 30)),
+    "gauss3d_dopri_mc_prim": lambda: _gauss3d(),
+    "gauss3d_rkf3_minmod_cons": lambda: _gauss3d(variables=abi.CONSERVATIVE, limiter=abi.MINMOD, method=abi.RK_FEHLBERG,
+                                                tdorder=3, n=(17, 20, 14),
+                                                bcs=[abi.REFLECTING, abi.REFLECTING, abi.NO_GRADIENTS, abi.NO_GRADIENTS,
+                                                     abi.PERIODIC, abi.PERIODIC]),
+    "gauss3d_ssprk3_absorbing": lambda: _gauss3d(method=abi.MODIFIED_EULER, tdorder=3, limiter=abi.VANLEER,
+                                                bcs=[abi.ABSORBING] * 6, n=(16, 14, 18)),
+    "disk_logcyl_pointmass": lambda: _disk(),
+    "disk_cyl_pointmass_cons": lambda: _disk(geometry=abi.CYLINDRICAL, n=(40, 32), variables=abi.CONSERVATIVE),
+    "iso3d_cashkarp_mixed_bc": lambda: _iso3d(),
+}
+
+
+def fixed_step(cfg):
+    return cfg.method == abi.MODIFIED_EULER
+
+
+def fix_modeuler(c):
+    if c.method == abi.MODIFIED_EULER:
+        c.tol_rel = 10.0
+    return c
