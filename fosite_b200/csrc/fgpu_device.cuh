@@ -358,7 +358,7 @@ struct Cells {
       double mn = dmin(0., v - cs), mx = dmax(0., v + cs);
       a[m] = dmax(mx, -mn) / dl[m];
     }
-    if (ND == 2) { out[0] = a[0] + a[1]; }
+    if (ND == 2) { out[0] = a[0] + a[1]; out[1] = 0.0; out[2] = 0.0; }
     else { out[0] = a[0]; out[1] = a[1]; out[2] = a[2]; }
   }
 };

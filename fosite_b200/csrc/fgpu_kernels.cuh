@@ -390,7 +390,10 @@ __global__ void __launch_bounds__(TX* TY) stage_kernel(const __grid_constant__ S
           PH::c2p(y, p, P);
           if (EU && A.cfl_roundtrip) p[V - 1] = dmax(p[V - 1], P.pmin);
           double cs = EU ? PH::cs_of(p, P) : M.cs[ip];
-          CE::cfl_cell(p, cs, M, ip, cflv);
+          double v3[3];
+          CE::cfl_cell(p, cs, M, ip, v3);
+#pragma unroll
+          for (int q = 0; q < 3; ++q) cflv[q] = dmax(cflv[q], v3[q]);
           if (EU && A.cfl_roundtrip) PH::p2c(p, c, P);
           else { for (int v = 0; v < V; ++v) c[v] = y[v]; }
           if ((A.checkdata & 0x01) && !(cs > 0.)) flags |= 0x01;
@@ -406,7 +409,10 @@ __global__ void __launch_bounds__(TX* TY) stage_kernel(const __grid_constant__ S
       }
       if (A.cfl_mode == 2) {
         double cs = EU ? PH::cs_of(pc, P) : M.cs[ip];
-        CE::cfl_cell(pc, cs, M, ip, cflv);
+        double v3[3];
+        CE::cfl_cell(pc, cs, M, ip, v3);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) cflv[q] = dmax(cflv[q], v3[q]);
         if ((A.checkdata & 0x01) && !(cs > 0.)) flags |= 0x01;
         if (EU && (A.checkdata & 0x02) && pc[V - 1] < P.pmin) flags |= 0x02;
         if ((A.checkdata & 0x04) && pc[0] < P.rhomin) flags |= 0x04;
@@ -432,7 +438,7 @@ __global__ void __launch_bounds__(TX* TY) stage_kernel(const __grid_constant__ S
           lo[v] = l;
           A.out_high[(long long)v * g.n + idx] = h;
           double e = fabs(h - l) / (A.tol_rel * fabs(h) + A.tol_abs[v]);
-          errv = v == 0 ? e : dmax(errv, e);
+          errv = dmax(errv, e);
         }
       }
     }

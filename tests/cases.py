@@ -56,7 +56,7 @@ def _gauss3d(n=(20, 18, 16), variables=abi.PRIMITIVE, limiter=abi.MONOCENT, meth
     c.variables = variables
     c.method = method
     c.tdorder = tdorder
-    c.tol_rel = tol
+    c.tol_rel = tol if method != abi.MODIFIED_EULER else 10.0
     for v in range(abi.MAXVAR):
         c.tol_abs[v] = tol
     c.cfl = 0.4

@@ -25,6 +25,11 @@ def _interior(a, cfg):
 
 
 def rel_l1(a, b):
+    """Relative L1 norm of the state-vector difference: sum|a-b| / sum|b| over all cells and variables."""
+    return float(np.abs(a - b).sum() / (np.abs(b).sum() + 1e-300))
+
+
+def rel_l1_per_var(a, b):
     num = np.abs(a - b).reshape(a.shape[0], -1).sum(axis=1)
     den = np.abs(b).reshape(b.shape[0], -1).sum(axis=1) + 1e-300
     return float(np.max(num / den))
@@ -61,6 +66,8 @@ def _compare(cfg, o, g, tol, what):
         else:
             r = rel_l1(a, b)
             assert r <= tol, "%s %s rel L1 %.3e > %.1e" % (what, nm, r, tol)
+            rv = rel_l1_per_var(a, b)
+            assert rv <= 10 * tol, "%s %s per-variable rel L1 %.3e > %.1e" % (what, nm, rv, 10 * tol)
 
 
 @pytest.mark.gpu
