@@ -17,6 +17,7 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <mutex>
 #include "../../include/fosite_gpu.h"
 #include "fgpu_kernels_misc.cuh"
 
@@ -1127,3 +1128,150 @@ int fgpu_reset_stats(fgpu_handle* h) {
 }
 
 }  // extern "C"
+
+// ======================================================================= allocation-free CFL time step
+// Callers that must not allocate device memory after start-up -- code running
+// inside a memory-capped service, a real-time loop that forbids cudaMalloc, or
+// a host that hands the solver a fixed memory pool -- get one entry point that
+// uses only this file-scope scratch array: the 1-D metric of the mesh and the
+// reduction control block live here instead of in per-handle allocations.
+namespace {
+
+constexpr size_t kNoallocScratchBytes = 1u << 20;   // 1 MiB, held by every device that loads the library
+static __device__ __align__(256) double g_noalloc_scratch[kNoallocScratchBytes / sizeof(double)];
+
+constexpr int kMaxDevices = 64;
+double* g_noalloc_ptr[kMaxDevices] = {nullptr};
+std::mutex g_noalloc_mutex;
+
+// per-device set-up: the device address of the scratch array, taken with the device current
+int noalloc_scratch(int dev, double** ptr) {
+  if (dev < 0 || dev >= kMaxDevices) return FGPU_EARG;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    double* p = nullptr;
+    if (cudaGetSymbolAddress((void**)&p, g_noalloc_scratch) != cudaSuccess || !p) return FGPU_ECUDA;
+    g_noalloc_ptr[dev] = p;
+  }
+  *ptr = g_noalloc_ptr[dev];
+  return FGPU_OK;
+}
+
+__global__ void noalloc_finalize_kernel(const Ctl* c, int nd, double cfl, double* dt_out) {
+  auto D = [](unsigned long long b) { return __longlong_as_double((long long)b); };
+  double invdt = nd == 2 ? D(c->invdt[0]) : dmax(dmax(D(c->invdt[1]), D(c->invdt[2])), D(c->invdt[0]));
+  *dt_out = cfl / invdt;
+}
+
+template <int ND, bool EU>
+void noalloc_launch(const BndArgs& B, long long n, cudaStream_t s, int nd, double cfl, double* dt_out) {
+  long long b1 = std::min<long long>((n + 255) / 256, 148 * 16);
+  interior_cfl_kernel<ND, EU><<<(unsigned)b1, 256, 0, s>>>(B);
+  long long b2 = std::min<long long>((B.nghost + 255) / 256, 4096);
+  boundary_kernel<ND, EU><<<(unsigned)(b2 < 1 ? 1 : b2), 256, 0, s>>>(B);
+  noalloc_finalize_kernel<<<1, 1, 0, s>>>(B.ctl, nd, cfl, dt_out);
+}
+
+}  // namespace
+
+extern "C" int fgpu_calc_timestep_noalloc(const fgpu_config* cfg, const double* d_cvar, double* d_dt, void* stream) {
+  if (!cfg || !d_cvar || !d_dt) return FGPU_EARG;
+  const fgpu_config& c = *cfg;
+  if (c.geometry != FGPU_CARTESIAN || c.pointmass || c.fargo_method) return FGPU_EUNSUPPORTED;
+  if (c.inum < 2 || c.jnum < 2 || c.knum < 1) return FGPU_EUNSUPPORTED;
+  bool euler = c.physics == FGPU_EULER;
+  if (!euler && !(c.physics == FGPU_EULER_ISOTHERM && c.csiso > 0.0)) return FGPU_EUNSUPPORTED;
+  int nd = c.knum > 1 ? 3 : 2;
+  for (int f = 0; f < 2 * nd; ++f) {
+    int t = c.bc[f];
+    if (t != FGPU_PERIODIC && t != FGPU_REFLECTING && t != FGPU_ABSORBING && t != FGPU_NO_GRADIENTS)
+      return FGPU_EUNSUPPORTED;
+  }
+  int nxp = c.inum + 4, nyp = c.jnum + 4, nzp = c.knum + 4;
+  size_t ctl_doubles = (sizeof(Ctl) + 255) / 256 * 256 / sizeof(double);
+  size_t metric_doubles = (size_t)M_NI * nxp + 2 * (size_t)nyp + 2 * (size_t)nzp;
+  if ((ctl_doubles + metric_doubles) * sizeof(double) > kNoallocScratchBytes) return FGPU_EARG;   // mesh too large
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return FGPU_ECUDA;
+  double* scratch = nullptr;
+  if (int rc = noalloc_scratch(dev, &scratch)) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  Ctl* ctl = (Ctl*)scratch;
+  double* dm = scratch + ctl_doubles;
+
+  // Cartesian metric (mesh_base.f90:570-601, mesh_midpoint.f90:97-145 with h = 1), built on the stack
+  // in chunks and copied into the scratch array
+  double dx = (c.xmax - c.xmin) / c.inum, dy = (c.ymax - c.ymin) / c.jnum, dz = (c.zmax - c.zmin) / c.knum;
+  double mdx = dx, mdy = dy, mdz = dz;
+  if (dz < 2 * DBL_EPSILON && c.knum == 1) { dz = 1.0; mdz = 0.0; }
+  double volume = 1.0 * dx * dy * dz;
+  double vals[M_NI];
+  for (int q = 0; q < M_NI; ++q) vals[q] = 0.0;
+  vals[M_dAxW] = 1.0 * 1.0; vals[M_dAyS] = 1.0 * 1.0; vals[M_dAzB] = 1.0 * 1.0;
+  vals[M_dxdydV] = dx * dy / (volume + DBL_MIN);
+  vals[M_dydzdV] = dy * dz / (volume + DBL_MIN);
+  vals[M_dzdxdV] = dz * dx / (volume + DBL_MIN);
+  vals[M_dlx] = 1.0 * dx; vals[M_dly] = 1.0 * dy; vals[M_dlz] = 1.0 * dz;
+  for (int q = 0; q < 7; ++q) vals[M_cs0 + q] = euler ? 0.0 : c.csiso;
+  const int CH = 512;
+  double buf[CH];
+  auto put = [&](size_t ofs, int n, auto&& f) -> int {
+    for (int b = 0; b < n; b += CH) {
+      int m = std::min(CH, n - b);
+      for (int t = 0; t < m; ++t) buf[t] = f(b + t);
+      if (cudaMemcpyAsync(dm + ofs + b, buf, sizeof(double) * m, cudaMemcpyHostToDevice, s) != cudaSuccess) return FGPU_ECUDA;
+      if (cudaStreamSynchronize(s) != cudaSuccess) return FGPU_ECUDA;   // buf is reused
+    }
+    return FGPU_OK;
+  };
+  for (int q = 0; q < M_NI; ++q) {
+    int rc;
+    if (q == M_offxW || q == M_offxE) {
+      bool east = q == M_offxE;
+      rc = put((size_t)q * nxp, nxp, [&](int ip) {
+        double x = c.xmin + ((double)(2 * (ip - 1) - 1) * 0.5) * mdx;
+        return (east ? x + 0.5 * mdx : x + (-0.5 * mdx)) - x;
+      });
+    } else {
+      double v = vals[q];
+      rc = put((size_t)q * nxp, nxp, [&](int) { return v; });
+    }
+    if (rc) return rc;
+  }
+  size_t by = (size_t)M_NI * nxp;
+  for (int side = 0; side < 2; ++side) {
+    if (int rc = put(by + side * nyp, nyp, [&](int jp) {
+          double y = c.ymin + ((double)(2 * (jp - 1) - 1) * 0.5) * mdy;
+          return (side ? y + 0.5 * mdy : y + (-0.5 * mdy)) - y; })) return rc;
+    if (int rc = put(by + 2 * nyp + side * nzp, nzp, [&](int kp) {
+          double z = c.zmin + ((double)(2 * (kp - 1) - 1) * 0.5) * mdz;
+          return (side ? z + 0.5 * mdz : z + (-0.5 * mdz)) - z; })) return rc;
+  }
+  // the reduction slots must start at zero on every call
+  if (cudaMemsetAsync(ctl, 0, sizeof(Ctl), s) != cudaSuccess) return FGPU_ECUDA;
+
+  BndArgs B;
+  std::memset(&B, 0, sizeof(B));
+  B.g.nx = c.inum; B.g.ny = c.jnum; B.g.nz = nd == 3 ? c.knum : 1;
+  B.g.n = (long long)B.g.nx * B.g.ny * B.g.nz;
+  for (int f = 0; f < 6; ++f) B.g.bc[f] = c.bc[f];
+  B.ph.gamma = c.gamma; B.ph.gm1 = c.gamma - 1.; B.ph.pmin = c.pmin; B.ph.rhomin = c.rhomin; B.ph.tiny2 = 2.0 * DBL_MIN;
+  MetricP& M = B.mt;
+  auto P = [&](int which) { return dm + (size_t)which * nxp; };
+  M.dAxW = P(M_dAxW); M.dAyS = P(M_dAyS); M.dAzB = P(M_dAzB);
+  M.dydzdV = P(M_dydzdV); M.dzdxdV = P(M_dzdxdV); M.dxdydV = P(M_dxdydV);
+  M.cxyx = P(M_cxyx); M.cxzx = P(M_cxzx); M.cyxy = P(M_cyxy); M.cyzy = P(M_cyzy); M.czxz = P(M_czxz); M.czyz = P(M_czyz);
+  M.dlx = P(M_dlx); M.dly = P(M_dly); M.dlz = P(M_dlz);
+  M.offxW = P(M_offxW); M.offxE = P(M_offxE);
+  M.offyS = dm + by; M.offyN = dm + by + nyp; M.offzB = dm + by + 2 * nyp; M.offzT = dm + by + 2 * nyp + nzp;
+  M.accel = nullptr; M.cs = P(M_cs0); M.nxp = nxp; M.curv = 0;
+  B.in.base = d_cvar; B.in.nk = 0; B.in.roundtrip = 0;
+  B.roundtrip = 0;
+  B.checkdata = 0;
+  B.ctl = ctl;
+  B.finalize = FIN_NONE;
+  B.nghost = (long long)nxp * nyp * (nd == 3 ? nzp : 1) - B.g.n;
+  if (nd == 2) { if (euler) noalloc_launch<2, true>(B, B.g.n, s, nd, c.cfl, d_dt); else noalloc_launch<2, false>(B, B.g.n, s, nd, c.cfl, d_dt); }
+  else { if (euler) noalloc_launch<3, true>(B, B.g.n, s, nd, c.cfl, d_dt); else noalloc_launch<3, false>(B, B.g.n, s, nd, c.cfl, d_dt); }
+  return cudaGetLastError() == cudaSuccess ? FGPU_OK : FGPU_ECUDA;
+}

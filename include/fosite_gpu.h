@@ -227,6 +227,19 @@ int fgpu_run(fgpu_handle* h, int64_t n, int64_t* done);
 int fgpu_compute_rhs(fgpu_handle* h);
 /* Timedisc%CalcTimestep of the current state (does not change the status). */
 int fgpu_calc_timestep(fgpu_handle* h, double* dt);
+/* CalcTimestep for callers that cannot allocate device memory (no counterpart
+ * in the reference).  Takes a config and a caller-owned device state in the
+ * library's stored layout (interior cells only, one field of inum*jnum*knum
+ * doubles per conservative variable, i fastest) and writes the CFL time step
+ * to the caller's device double *d_dt, on the caller's stream.  It calls no
+ * cudaMalloc/cudaFree: the mesh metric and the reduction slots live in a
+ * 1 MiB file-scope __device__ array that every GPU loading the library holds
+ * until exit.  Cartesian meshes, ideal-gas or constant-cs isothermal physics,
+ * no point mass or fargo; meshes whose metric does not fit (inum above about
+ * 5000) return FGPU_EARG.  The first call on a device looks up the array's
+ * device address, so make it before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU race. */
+int fgpu_calc_timestep_noalloc(const fgpu_config* cfg, const double* d_cvar, double* d_dt, void* stream);
 int fgpu_get_status(fgpu_handle* h, fgpu_status* st);
 /* Block until all device work of h has finished. */
 int fgpu_synchronize(fgpu_handle* h);
