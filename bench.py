@@ -28,6 +28,8 @@ import numpy as np  # noqa: E402
 WORKLOADS = {
     "gauss3d": "3D Euler Gaussian pulse 256^3, reflecting, KT+MC(prim), Dormand-Prince 5(4) tol 1e-5, CFL 0.4",
     "khi2d": "2D Kelvin-Helmholtz 256^2, periodic, KT+van Leer(cons), SSPRK3 fixed CFL 0.4",
+    "disk2d": "2D isothermal Keplerian disk, logcylindrical 512x1024, point mass GM=1, sigma~1/r, cs/vK=0.05, "
+              "FARGO shift, KT+van Leer(prim), SSPRK3 fixed CFL 0.4, absorbing r / periodic phi",
 }
 
 
@@ -35,7 +37,18 @@ def make_problem(name, size):
     from fosite_b200 import problems
     if name == "gauss3d":
         return problems.gauss3d(n=size or 256)
+    if name == "disk2d":
+        nr = size or 512
+        return problems.disk2d(nr=nr, nphi=2 * nr, fargo=1)
     return problems.khi2d(n=size or 256)
+
+
+def apply_extra(sim, cfg, extra):
+    """Radial sound-speed profiles of the isothermal disk (cell centres and faces)."""
+    if "bccsound" in extra:
+        shape = (cfg.knum, cfg.jnum + 4, cfg.inum + 4)
+        sim.set_sound_speeds(np.broadcast_to(extra["bccsound"], shape),
+                             np.broadcast_to(extra["fcsound"], (4,) + shape))
 
 
 def algorithmic_bytes_per_cell_update(name, vnum):
@@ -45,9 +58,11 @@ def algorithmic_bytes_per_cell_update(name, vnum):
     k1 and the round-tripped base (1+2), stages m=2..7 read base+k1..k_{m-1}
     and write k_m (27+6), the last stage also writes the new state (1):
     37 arrays.  SSPRK3 (modified Euler): 3 stages read the stage input and the
-    start state, write the stage output: 8 arrays.
+    start state, write the stage output: 8 arrays.  With FARGO the background
+    velocity pass reads the state (1), the last stage writes a scratch state
+    and the transport reads it and writes the state (2): 11 arrays.
     """
-    arrays = 37 if name == "gauss3d" else 8
+    arrays = {"gauss3d": 37, "disk2d": 11}.get(name, 8)
     return arrays * vnum * 8.0
 
 
@@ -120,9 +135,10 @@ def cpu_baseline(name, budget_s=20.0):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     from fosite_b200 import abi
-    size = 48 if name == "gauss3d" else 256
-    cfg, p, _ = make_problem(name, size)
+    size = {"gauss3d": 48, "disk2d": 128}.get(name, 256)
+    cfg, p, extra = make_problem(name, size)
     o = pyoracle.Oracle(cfg)
+    apply_extra(o, cfg, extra)
     o.set_state(abi.PVAR, p)
     o.first_step()
     t0 = time.perf_counter()
@@ -201,8 +217,12 @@ def run_own(args, world, rank, local):
     cfg, p, extra = make_problem(args.workload, args.size)
     sim = Simulation(cfg, device=local)
     sim.set_stream(stream.cuda_stream)
+    apply_extra(sim, cfg, extra)
     sim.set_state(abi.PVAR, p)
     sim.first_step()
+    # stage-kernel layout: measured on this GPU by the library's tuner unless forced
+    forced = os.environ.get("FGPU_STAGE_VARIANT")
+    variant = int(forced) if forced is not None else sim.autotune(3)
     for _ in range(args.warmup):
         sim.step()
     n_cells = cfg.inum * cfg.jnum * cfg.knum
@@ -269,11 +289,15 @@ def run_own(args, world, rank, local):
         "config": {"workload": args.workload, "description": WORKLOADS[args.workload],
                    "grid": [cfg.inum, cfg.jnum, cfg.knum], "parallelism": "replicas x%d" % world,
                    "l2": "inputs larger than L2: each state array is %.0f MB" % (n_cells * sim.vnum * 8 / 1e6),
-                   "accepted_steps_per_rank": int(st.cell_updates // n_cells), "attempts": int(st.attempts)},
+                   "accepted_steps_per_rank": int(st.cell_updates // n_cells), "attempts": int(st.attempts),
+                   "stage_variant": variant, "stage_variant_source": "forced" if forced is not None else "autotuned"},
         "achieved_gbps_step": value / world * bpc / 1e9,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "kernel": "stage_kernel (fused RHS + stage update)", "peak_kind": peak_kind + " copy bandwidth"},
+                     "kernel": "stage_kernel (fused RHS + stage update)",
+                     "peak_kind": peak_kind + " copy bandwidth (burst)",
+                     "algorithmic_bytes_per_launch": st.stage_bytes / max(1, st.stage_launches),
+                     "launch_ms_avg": st.stage_ms / max(1, st.stage_launches)},
         "cpu_baseline": cb,
         "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": nstate * 8,
                 "d2h_bytes_per_step": nstate * 8},
@@ -284,20 +308,114 @@ def run_own(args, world, rank, local):
     sim.close()
 
 
+ENSEMBLE_DESC = ("96 independent 2D isothermal disks, Nr in [64,384], Nphi in [128,768] (multiples of 32), "
+                 "cs/vK in [0.03,0.1], sigma index in [-1.5,-0.5], mixed cylindrical/logcylindrical, SSPRK3, "
+                 "point mass, one persistent launch per stage, CUDA-graph captured, autotuned")
+
+
+def ensemble_members(n=96, seed=4000):
+    from fosite_b200 import abi, problems
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        nr = 32 * int(rng.integers(2, 13))
+        nphi = 32 * int(rng.integers(4, 25))
+        geo = abi.LOGCYLINDRICAL if k % 2 == 0 else abi.CYLINDRICAL
+        out.append(problems.disk2d(nr=nr, nphi=nphi, seed=seed + k, hratio=float(rng.uniform(0.03, 0.1)),
+                                   sigma_index=float(rng.uniform(-1.5, -0.5)), geometry=geo, fargo=0))
+    return out
+
+
+def run_ensemble(args):
+    """Batched ensemble against a loop of plain per-grid runs of the same members."""
+    from fosite_b200 import abi
+    from fosite_b200.sim import Batch, Simulation
+    probs = ensemble_members(args.members)
+
+    def make():
+        sims = []
+        for cfg, p, extra in probs:
+            s = Simulation(cfg)
+            apply_extra(s, cfg, extra)
+            s.set_state(abi.PVAR, p)
+            s.first_step()
+            sims.append(s)
+        return sims
+    members, plain = make(), make()
+    cells = sum(c.inum * c.jnum for c, _, _ in probs)
+    b = Batch(members)
+    variant = b.autotune(3)
+    b.run(args.warmup)
+    for s in plain:
+        s.run(args.warmup)
+    clk = ClockSampler(0)
+    clk.start()
+    t0 = time.perf_counter()
+    b.run(args.steps)
+    t_batch = time.perf_counter() - t0
+    clocks = clk.stop()
+    t0 = time.perf_counter()
+    for s in plain:
+        s.run(args.steps)
+    t_plain = time.perf_counter() - t0
+    same = all(np.array_equal(m.get(abi.CVAR), s.get(abi.CVAR)) for m, s in zip(members, plain))
+    value = cells * args.steps / t_batch
+    line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_batch / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": "ensemble", "description": ENSEMBLE_DESC, "members": len(probs),
+                       "cells": cells, "tiles": b.tiles, "variant": variant},
+            "member_steps_per_s": len(probs) * args.steps / t_batch,
+            "plain_loop": {"value": cells * args.steps / t_plain, "ms_per_step": 1e3 * t_plain / args.steps},
+            "speedup_vs_plain": t_plain / t_batch, "identical_to_plain": bool(same), "clocks": clocks}
+    print(json.dumps(line), flush=True)
+    b.close()
+
+
+def run_serve(args):
+    """Poisson request streams at swept rates through the continuous-batching server."""
+    from fosite_b200.serve import Server, poisson_stream
+    import torch
+    free, total = torch.cuda.mem_get_info()
+    out = []
+    for rate in [float(r) for r in args.rates.split(",")]:
+        reqs = poisson_stream(rate, args.requests, seed=int(rate), t_scale=args.t_scale)
+        srv = Server(hbm_budget_bytes=int(0.8 * free), chunk=args.chunk, autotune=False)
+        rep = srv.serve(reqs, timeout_s=900)
+        rep["rate_req_s"] = rate
+        out.append(rep)
+    line = {"metric": "p50/p99 time-to-solution, cell-updates/s", "unit": "s", "n_gpus": 1,
+            "higher_is_better": False, "dtype": "f64", "data": "synthetic (seeded Poisson streams)",
+            "config": {"workload": "serve", "requests_per_rate": args.requests, "t_scale": args.t_scale,
+                       "chunk_steps": args.chunk,
+                       "mix": "2D KHI 64^2-1024^2, 2D disks 64x128-512x1024, 3D pulses 32^3-128^3"},
+            "rates": out}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fosite_b200", choices=["fosite_b200", "reference"])
-    ap.add_argument("--workload", default="gauss3d", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="gauss3d", choices=sorted(WORKLOADS) + ["ensemble", "serve"])
+    ap.add_argument("--members", type=int, default=96)
+    ap.add_argument("--rates", default="10,50,200,500")
+    ap.add_argument("--requests", type=int, default=200)
+    ap.add_argument("--t-scale", type=float, default=0.01)
+    ap.add_argument("--chunk", type=int, default=8)
     ap.add_argument("--size", type=int, default=0)
     ap.add_argument("--ref-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:
-        if args.impl == "reference":
+        if args.workload in ("ensemble", "serve"):
+            if rank == 0:
+                run_ensemble(args) if args.workload == "ensemble" else run_serve(args)
+        elif args.impl == "reference":
             run_reference(args, world, rank)
         else:
             run_own(args, world, rank, local)

@@ -28,7 +28,7 @@ def build(verbose=False, variants=("fast", "exact")):
     src = os.path.join(CSRC, "fgpu_host.cu")
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(HERE, "..", "include", "fosite_gpu.h")]
     newest = max(os.path.getmtime(d) for d in deps)
-    outs = []
+    outs, procs = [], []
     for var in variants:
         name = "libfosite_gpu.so" if var == "fast" else "libfosite_gpu_exact.so"
         out = os.path.join(LIBDIR, name)
@@ -36,13 +36,24 @@ def build(verbose=False, variants=("fast", "exact")):
         if os.path.exists(out) and os.path.getmtime(out) >= newest:
             continue
         cmd = [nvcc(), "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC", "-lineinfo",
-               "--expt-relaxed-constexpr", *ARCH, "-o", out, src]
+               "--expt-relaxed-constexpr", *ARCH, "-o", out + ".tmp", src]
         if var == "exact":
-            cmd.insert(1, "--fmad=false")
+            cmd[1:1] = ["--fmad=false", "-DFGPU_EXACT"]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd), file=sys.stderr)
-        subprocess.check_call(cmd)
+        procs.append((subprocess.Popen(cmd), out))   # the two variants compile concurrently
+    failed = []
+    for p, out in procs:
+        if p.wait() != 0:
+            failed.append(out)
+        else:
+            os.replace(out + ".tmp", out)
+            # stamp the library with the sources' time, so that a source edited while
+            # nvcc ran still counts as newer than the library
+            os.utime(out, (newest, newest))
+    if failed:
+        raise RuntimeError("nvcc failed for " + ", ".join(failed))
     return outs
 
 

@@ -1,0 +1,345 @@
+// fgpu_batch.cuh -- batched ensembles of independent grids and the launch
+// autotuner (included at the end of fgpu_host.cu; uses its helpers).
+//
+// fosite integrates one grid per process.  An ensemble of many small grids
+// (parameter studies of disks, a serving queue of mixed requests) leaves most
+// of a B200 idle when each grid is stepped by its own launches: a 64x128 disk
+// is 32 tiles, a fifth of one wave.  A batch advances all its grids with ONE
+// persistent stage launch per Runge-Kutta stage over the flattened tile queue
+// of every grid (grid, bx, by, bz), plus one ghost/CFL/finalize launch whose
+// blocks are distributed over the grids.  Every grid keeps its own arguments
+// (metric, limiter, boundaries, dt, time, stop flags) in a device table, so a
+// grid's results are bitwise the same alone or in any batch.
+
+struct fgpu_batch {
+  std::vector<fgpu_handle*> m;
+  int nd = 2, order = 3;
+  bool euler = false, prim = false;
+  cudaStream_t stream = nullptr;
+  int variant = 0;
+  StageArgs* d_args = nullptr;   // [order][n] step stages, then [n] RHS probes of the tuner
+  BndArgs* d_bnd = nullptr;      // [n]
+  int4* d_tiles = nullptr;
+  int ntiles = 0;
+  int4* d_bblocks = nullptr;
+  int nbblocks = 0;
+  Ctl* h_ctls = nullptr;         // pinned [n]
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+  int graph_variant = -1;
+  int sms = 148;
+  int64_t pending_steps = 0;     // enqueued since the last collect
+  std::vector<long long> it0;    // member iteration counts at the first enqueue
+  std::string err;
+};
+
+namespace {
+
+int bset_err(fgpu_batch* b, int code, const std::string& msg) {
+  if (b) b->err = msg; else g_create_error = msg;
+  return code;
+}
+#define BCUDA_TRY(b, call)                                                                   \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return bset_err(b, e_ == cudaErrorMemoryAllocation ? FGPU_ENOMEM : FGPU_ECUDA,         \
+                      std::string(#call) + ": " + cudaGetErrorString(e_));                   \
+  } while (0)
+
+template <class K>
+int persistent_grid(fgpu_batch* b, K kernel, int threads, int ntiles) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return std::max(1, std::min(ntiles, per_sm * b->sms));
+}
+
+template <int ND, bool EU, bool PRIM>
+int launch_batched_stage_t(fgpu_batch* b, const StageArgs* args, int variant) {
+  constexpr int TY = ND == 2 ? 8 : 4;
+  constexpr int T = 32 * TY;
+  constexpr int M2 = ND == 2 ? 2 : 4, M3 = ND == 2 ? 3 : 6;
+  if (variant == 2) {
+    auto k = batched_stage_kernel<ND, EU, PRIM, 32, TY, M2>;
+    k<<<persistent_grid(b, k, T, b->ntiles), T, 0, b->stream>>>(args, b->d_tiles, b->ntiles);
+  } else if (variant == 3) {
+    auto k = batched_stage_kernel<ND, EU, PRIM, 32, TY, M3>;
+    k<<<persistent_grid(b, k, T, b->ntiles), T, 0, b->stream>>>(args, b->d_tiles, b->ntiles);
+  } else {
+    auto k = batched_stage_kernel<ND, EU, PRIM, 32, TY, 1>;
+    k<<<persistent_grid(b, k, T, b->ntiles), T, 0, b->stream>>>(args, b->d_tiles, b->ntiles);
+  }
+  BCUDA_TRY(b, cudaGetLastError());
+  return FGPU_OK;
+}
+
+int launch_batched_stage(fgpu_batch* b, const StageArgs* args, int variant) {
+  if (b->nd == 2) {
+    if (b->euler) return b->prim ? launch_batched_stage_t<2, true, true>(b, args, variant)
+                                 : launch_batched_stage_t<2, true, false>(b, args, variant);
+    return b->prim ? launch_batched_stage_t<2, false, true>(b, args, variant)
+                   : launch_batched_stage_t<2, false, false>(b, args, variant);
+  }
+  if (b->euler) return b->prim ? launch_batched_stage_t<3, true, true>(b, args, variant)
+                               : launch_batched_stage_t<3, true, false>(b, args, variant);
+  return b->prim ? launch_batched_stage_t<3, false, true>(b, args, variant)
+                 : launch_batched_stage_t<3, false, false>(b, args, variant);
+}
+
+int launch_batched_boundary(fgpu_batch* b) {
+  if (b->nd == 2) {
+    if (b->euler) batched_boundary_kernel<2, true><<<b->nbblocks, 256, 0, b->stream>>>(b->d_bnd, b->d_bblocks);
+    else batched_boundary_kernel<2, false><<<b->nbblocks, 256, 0, b->stream>>>(b->d_bnd, b->d_bblocks);
+  } else {
+    if (b->euler) batched_boundary_kernel<3, true><<<b->nbblocks, 256, 0, b->stream>>>(b->d_bnd, b->d_bblocks);
+    else batched_boundary_kernel<3, false><<<b->nbblocks, 256, 0, b->stream>>>(b->d_bnd, b->d_bblocks);
+  }
+  BCUDA_TRY(b, cudaGetLastError());
+  return FGPU_OK;
+}
+
+int enqueue_batch_step(fgpu_batch* b) {
+  const int n = (int)b->m.size();
+  for (int s = 0; s < b->order; ++s)
+    if (int rc = launch_batched_stage(b, b->d_args + (size_t)s * n, b->variant)) return rc;
+  return launch_batched_boundary(b);
+}
+
+int build_batch_graph(fgpu_batch* b, int steps) {
+  if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+  cudaGraph_t gr;
+  BCUDA_TRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = 0;
+  for (int s = 0; s < steps && !rc; ++s) rc = enqueue_batch_step(b);
+  cudaError_t e = cudaStreamEndCapture(b->stream, &gr);
+  if (rc) return rc;
+  if (e != cudaSuccess) return bset_err(b, FGPU_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&b->graph, gr, 0);
+  cudaGraphDestroy(gr);
+  if (e != cudaSuccess) return bset_err(b, FGPU_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  b->graph_steps = steps;
+  b->graph_variant = b->variant;
+  return FGPU_OK;
+}
+
+// time reps launches of fn on stream s (CUDA events), milliseconds per launch
+template <class F>
+double time_launches(cudaStream_t s, int reps, F&& fn) {
+  cudaEvent_t a, z;
+  cudaEventCreate(&a);
+  cudaEventCreate(&z);
+  fn();   // warm-up (first-touch, instruction cache)
+  cudaEventRecord(a, s);
+  for (int r = 0; r < reps; ++r) fn();
+  cudaEventRecord(z, s);
+  cudaEventSynchronize(z);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, z);
+  cudaEventDestroy(a);
+  cudaEventDestroy(z);
+  return (double)ms / reps;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
+  if (!members || n < 1 || !out) return bset_err(nullptr, FGPU_EARG, "null argument or empty batch");
+  *out = nullptr;
+  fgpu_batch* b = new fgpu_batch();
+  auto fail = [&](int code, const std::string& msg) { g_create_error = msg; fgpu_batch_destroy(b); return code; };
+  const fgpu_handle* h0 = members[0];
+  if (!h0) return fail(FGPU_EARG, "null member");
+  b->nd = h0->nd; b->euler = h0->euler; b->prim = h0->prim; b->order = h0->order;
+  for (int i = 0; i < n; ++i) {
+    fgpu_handle* h = members[i];
+    if (!h) return fail(FGPU_EARG, "null member");
+    if (h->butcher) return fail(FGPU_EUNSUPPORTED, "batch members use the fixed-step modified Euler scheme");
+    if (h->fargo) return fail(FGPU_EUNSUPPORTED, "batch members without FARGO transport");
+    if (h->order < 2) return fail(FGPU_EUNSUPPORTED, "batch members of time order 2 or 3");
+    if (h->nd != b->nd || h->euler != b->euler || h->prim != b->prim || h->order != b->order)
+      return fail(FGPU_EBADCFG, "batch members differ in dimensionality, physics, reconstruction variables or order");
+    if (h->device != h0->device) return fail(FGPU_EBADCFG, "batch members live on different devices");
+    if (!h->first_done) return fail(FGPU_EBADCFG, "call fgpu_first_step on every member before batching");
+    b->m.push_back(h);
+  }
+  cudaSetDevice(h0->device);
+  cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, h0->device);
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(FGPU_ECUDA, "stream");
+  b->variant = h0->variant == 1 ? 0 : h0->variant;
+  // argument tables: step stages of every member, then the tuner's RHS probes
+  std::vector<StageArgs> args((size_t)(b->order + 1) * n);
+  std::vector<BndArgs> bnd(n);
+  std::vector<int4> tiles, bblocks;
+  for (int i = 0; i < n; ++i) {
+    fgpu_handle* h = b->m[i];
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return fail(FGPU_ECUDA, "member stream");
+    for (int s = 1; s <= b->order; ++s) {
+      StageArgs A = shu_osher_stage(h, s);
+      A.kchunk = h->kchunk;
+      args[(size_t)(s - 1) * n + i] = A;
+    }
+    StageArgs R = base_args(h);
+    R.in = plain_state(h->buf[0], false);
+    R.out_mode = OUT_RHS;
+    R.out = h->buf[2];
+    R.ctl = nullptr;
+    R.kchunk = h->kchunk;
+    args[(size_t)b->order * n + i] = R;
+    bnd[i] = bnd_args(h, h->buf[0], h->roundtrip_cfg, FIN_STEP);
+    const Grid& g = h->g;
+    const int TY = b->nd == 2 ? 8 : 4;
+    const int tx = (g.nx + 31) / 32, ty = (g.ny + TY - 1) / TY;
+    const int tz = b->nd == 3 ? (g.nz + h->kchunk - 1) / h->kchunk : 1;
+    for (int z = 0; z < tz; ++z)
+      for (int y = 0; y < ty; ++y)
+        for (int x = 0; x < tx; ++x) tiles.push_back(make_int4(i, x, y, z));
+    long long nb = std::min<long long>((bnd[i].nghost + 255) / 256, 4096);
+    if (nb < 1) nb = 1;
+    for (int q = 0; q < (int)nb; ++q) bblocks.push_back(make_int4(i, q, (int)nb, 0));
+  }
+  b->ntiles = (int)tiles.size();
+  b->nbblocks = (int)bblocks.size();
+  if (cudaMalloc(&b->d_args, sizeof(StageArgs) * args.size()) != cudaSuccess ||
+      cudaMalloc(&b->d_bnd, sizeof(BndArgs) * bnd.size()) != cudaSuccess ||
+      cudaMalloc(&b->d_tiles, sizeof(int4) * tiles.size()) != cudaSuccess ||
+      cudaMalloc(&b->d_bblocks, sizeof(int4) * bblocks.size()) != cudaSuccess ||
+      cudaMallocHost(&b->h_ctls, sizeof(Ctl) * n) != cudaSuccess)
+    return fail(FGPU_ENOMEM, "batch tables");
+  cudaMemcpyAsync(b->d_args, args.data(), sizeof(StageArgs) * args.size(), cudaMemcpyHostToDevice, b->stream);
+  cudaMemcpyAsync(b->d_bnd, bnd.data(), sizeof(BndArgs) * bnd.size(), cudaMemcpyHostToDevice, b->stream);
+  cudaMemcpyAsync(b->d_tiles, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice, b->stream);
+  cudaMemcpyAsync(b->d_bblocks, bblocks.data(), sizeof(int4) * bblocks.size(), cudaMemcpyHostToDevice, b->stream);
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess) return fail(FGPU_ECUDA, "batch table upload");
+  *out = b;
+  return FGPU_OK;
+}
+
+void fgpu_batch_destroy(fgpu_batch* b) {
+  if (!b) return;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->d_args) cudaFree(b->d_args);
+  if (b->d_bnd) cudaFree(b->d_bnd);
+  if (b->d_tiles) cudaFree(b->d_tiles);
+  if (b->d_bblocks) cudaFree(b->d_bblocks);
+  if (b->h_ctls) cudaFreeHost(b->h_ctls);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+int fgpu_batch_last_error(const fgpu_batch* b, char* buf, int len) {
+  const std::string& s = b ? b->err : g_create_error;
+  if (buf && len > 0) {
+    int k = std::min<int>((int)s.size(), len - 1);
+    std::memcpy(buf, s.data(), k);
+    buf[k] = 0;
+  }
+  return (int)s.size();
+}
+
+int fgpu_batch_size(const fgpu_batch* b, int* members, int* tiles) {
+  if (!b) return FGPU_EARG;
+  if (members) *members = (int)b->m.size();
+  if (tiles) *tiles = b->ntiles;
+  return FGPU_OK;
+}
+
+int fgpu_batch_enqueue(fgpu_batch* b, int64_t nsteps) {
+  if (!b || nsteps < 0) return FGPU_EARG;
+  if (b->pending_steps == 0) {
+    b->it0.resize(b->m.size());
+    for (size_t i = 0; i < b->m.size(); ++i) b->it0[i] = b->m[i]->iter;
+  }
+  const int G = 16;
+  int64_t full = nsteps / G, rest = nsteps % G;
+  if (full > 0) {
+    if (b->graph_steps != G || b->graph_variant != b->variant) { if (int rc = build_batch_graph(b, G)) return rc; }
+    for (int64_t r = 0; r < full; ++r) BCUDA_TRY(b, cudaGraphLaunch(b->graph, b->stream));
+  }
+  for (int64_t r = 0; r < rest; ++r) { if (int rc = enqueue_batch_step(b)) return rc; }
+  const int n = (int)b->m.size();
+  for (int i = 0; i < n; ++i)
+    BCUDA_TRY(b, cudaMemcpyAsync(b->h_ctls + i, b->m[i]->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, b->stream));
+  b->pending_steps += nsteps;
+  return FGPU_OK;
+}
+
+int fgpu_batch_collect(fgpu_batch* b, int* active) {
+  if (!b) return FGPU_EARG;
+  BCUDA_TRY(b, cudaStreamSynchronize(b->stream));
+  const int n = (int)b->m.size();
+  int act = 0;
+  const int64_t ns = b->pending_steps;
+  for (int i = 0; i < n; ++i) {
+    fgpu_handle* h = b->m[i];
+    if (ns > 0) {
+      *h->h_ctl = b->h_ctls[i];
+      sync_from_ctl(h);
+      h->stats.attempts += h->iter - b->it0[i];
+      h->stats.cell_updates += (h->iter - b->it0[i]) * h->g.n;
+      h->stats.stage_launches += (int64_t)b->order * ns;
+      h->stats.launches += (int64_t)(b->order + 1) * ns;
+    }
+    if (!h->h_ctl->stop && !h->h_ctl->brk) ++act;
+  }
+  b->pending_steps = 0;
+  if (active) *active = act;
+  return FGPU_OK;
+}
+
+int fgpu_batch_run(fgpu_batch* b, int64_t nsteps, int* active) {
+  if (int rc = fgpu_batch_enqueue(b, nsteps)) return rc;
+  return fgpu_batch_collect(b, active);
+}
+
+int fgpu_batch_autotune(fgpu_batch* b, int reps, int* variant) {
+  if (!b) return FGPU_EARG;
+  if (reps < 1) reps = 3;
+  const StageArgs* probe = b->d_args + (size_t)b->order * b->m.size();
+  const int cand[3] = {0, 2, 3};
+  double best = 1e300;
+  int bv = b->variant;
+  for (int v : cand) {
+    int rc = FGPU_OK;
+    double ms = time_launches(b->stream, reps, [&] { if (!rc) rc = launch_batched_stage(b, probe, v); });
+    if (rc) return rc;
+    BCUDA_TRY(b, cudaGetLastError());
+    if (ms < best) { best = ms; bv = v; }
+  }
+  b->variant = bv;
+  if (variant) *variant = bv;
+  return FGPU_OK;
+}
+
+// Measures each stage-kernel layout on this grid (RHS evaluations into a
+// scratch array, the state is not touched) and keeps the fastest.
+int fgpu_autotune(fgpu_handle* h, int reps, int* variant) {
+  if (!h) return FGPU_EARG;
+  if (reps < 1) reps = 3;
+  double* scratch = h->butcher ? h->buf[2 + h->T.m - 1] : h->buf[2];
+  StageArgs A = base_args(h);
+  A.in = plain_state(h->buf[0], false);
+  A.out_mode = OUT_RHS;
+  A.out = scratch;
+  A.ctl = nullptr;
+  const int cand[4] = {0, 2, 3, 1};
+  double best = 1e300;
+  int bv = h->variant, keep = h->variant;
+  for (int v : cand) {
+    h->variant = v;
+    int rc = FGPU_OK;
+    double ms = time_launches(h->stream, reps, [&] { if (!rc) rc = launch_stage_raw(h, A); });
+    if (rc) { h->variant = keep; return rc; }
+    if (ms < best) { best = ms; bv = v; }
+  }
+  h->variant = bv;
+  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; h->graph_steps = 0; }
+  if (variant) *variant = bv;
+  return FGPU_OK;
+}
+
+}  // extern "C"

@@ -21,6 +21,7 @@ namespace fgpu {
 
 struct PhysP {
   double gamma, gm1, pmin, rhomin, tiny2;   // tiny2 = 2*TINY(1.0)
+  double inv_gm1;                            // 1/(gamma-1), used by the product build only
 };
 
 struct Grid {
@@ -43,6 +44,18 @@ struct MetricP {
   int curv;                                  // geometric sources active
 };
 
+// A sequence of FARGO frame changes of the y momentum, m_y = m_y + s_q*(rho*w_q(i)),
+// applied in order.  It reproduces the in-place Add/SubtractBackgroundVelocityY
+// calls (physics_eulerisotherm.f90:1263-1413) that IntegrationStep and ComputeRHS
+// make on cvar (timedisc_base.f90:662-674, 1096-1110, 1190-1208): every stored
+// state is kept untransformed and the transforms are replayed pointwise where
+// the state is read, so the rounding of each in-place update is reproduced.
+struct Chain {
+  int n;
+  const double* w[4];   // background velocity by padded i
+  double s[4];          // +1 add, -1 subtract
+};
+
 // The stage input state at a cell: base - coef[0]*K[0] - coef[1]*K[1] - ...
 // evaluated in that order (timedisc_rkfehlberg.f90:277-302); nk = 0 for a
 // plain state.  roundtrip = 1 applies fosite's CHECK_PMIN pass of the
@@ -54,7 +67,15 @@ struct StateRef {
   double coef[FGPU_MAXK];
   int nk;
   int roundtrip;
+  // FARGO (2D isothermal): frame changes applied to the state before the
+  // boundary fill, i.e. the real-frame cvar that CenterBoundary sees
+  Chain pre;
 };
+
+// apply a frame-change chain to the conservative state c of a cell in padded column ip
+__device__ __forceinline__ void apply_chain(const Chain& C, double* c, int ip) {
+  for (int q = 0; q < C.n; ++q) c[2] = c[2] + C.s[q] * (c[0] * C.w[q][ip]);
+}
 
 // Device control block for device-resident stepping.
 struct Ctl {
@@ -72,9 +93,16 @@ enum { LIM_MINMOD = 1, LIM_MC = 2, LIM_SWEBY = 3, LIM_SUPERBEE = 4, LIM_OSPRE = 
 
 __device__ __forceinline__ double fsign1(double b) { return signbit(b) ? -1.0 : 1.0; }
 __device__ __forceinline__ double fsign(double a, double b) { return signbit(b) ? -fabs(a) : fabs(a); }
-// Fortran MIN/MAX on non-NaN operands
+// Fortran MIN/MAX on non-NaN operands.  The --fmad=false build keeps the
+// compare-and-select form (the operand returned for +0/-0 ties is the first,
+// as in the oracle); the product build uses the native FP64 min/max.
+#ifdef FGPU_EXACT
 __device__ __forceinline__ double dmin(double a, double b) { return b < a ? b : a; }
 __device__ __forceinline__ double dmax(double a, double b) { return b > a ? b : a; }
+#else
+__device__ __forceinline__ double dmin(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ double dmax(double a, double b) { return fmax(a, b); }
+#endif
 
 // ---------------------------------------------------------------- physics
 // Variables: 0 density, 1..ND velocity/momentum, ND+1 pressure/energy (Euler).
@@ -102,7 +130,11 @@ struct Phys {
     if (EU) {
       double s = p[1] * p[1] + p[2] * p[2];
       if (ND == 3) s = s + p[3] * p[3];
+#ifdef FGPU_EXACT
       c[V - 1] = p[V - 1] / P.gm1 + 0.5 * p[0] * s;
+#else
+      c[V - 1] = p[V - 1] * P.inv_gm1 + 0.5 * p[0] * s;
+#endif
     }
   }
   // GetSoundSpeed (physics_euler.f90:2682-2689)
@@ -152,13 +184,20 @@ __device__ __forceinline__ double slope(int lim, double theta, double invd, doub
 // ---------------------------------------------------------------- state access
 template <int V>
 __device__ __forceinline__ void state_at(const StateRef& S, long long n, long long idx, double* u) {
+  const double* b = S.base + idx;
 #pragma unroll
-  for (int v = 0; v < V; ++v) {
-    double x = __ldg(S.base + (long long)v * n + idx);
+  for (int v = 0; v < V; ++v) u[v] = __ldg(b + (long long)v * n);
+  // one k-array at a time, in the reference's accumulation order; only the
+  // stage's own arrays are touched (no predicated loads of unused slots)
+#pragma unroll 1
+  for (int q = 0; q < S.nk; ++q) {
+    const double* kq = S.K[q] + idx;
+    const double a = S.coef[q];
+    double t[V];
 #pragma unroll
-    for (int q = 0; q < FGPU_MAXK; ++q)
-      if (q < S.nk) x = x - S.coef[q] * __ldg(S.K[q] + (long long)v * n + idx);
-    u[v] = x;
+    for (int v = 0; v < V; ++v) t[v] = __ldg(kq + (long long)v * n);
+#pragma unroll
+    for (int v = 0; v < V; ++v) u[v] = u[v] - a * t[v];
   }
 }
 
@@ -177,13 +216,14 @@ struct Cells {
                                                     int i, int j, int k, double* p) {
     double u[V];
     state_at<V>(S, g.n, lin(g, i, j, k), u);
+    if (ND == 2 && !EU && S.pre.n) apply_chain(S.pre, u, i + 2);
     PH::c2p(u, p, P);
   }
 
   // Face ghost: exactly one of (i,j,k) outside the interior, in direction d.
   // boundary_periodic.f90:73-116, boundary_reflecting.f90:89-204,
   // boundary_nogradients.f90:75-125, boundary_absorbing.f90:114-211.
-  static __device__ void face_ghost_p(const StateRef& S, const Grid& g, const PhysP& P, const MetricP& M,
+  static __device__ __noinline__ void face_ghost_p(const StateRef& S, const Grid& g, const PhysP& P, const MetricP& M,
                                       int d, int i, int j, int k, double* p) {
     int ijk[3] = {i, j, k};
     int nd = d == 0 ? g.nx : d == 1 ? g.ny : g.nz;

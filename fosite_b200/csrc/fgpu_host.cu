@@ -18,8 +18,11 @@
 #include <vector>
 #include <algorithm>
 #include <mutex>
+#include <cstdlib>
 #include "../../include/fosite_gpu.h"
 #include "fgpu_kernels_misc.cuh"
+#include "fgpu_stage2.cuh"
+#include "fgpu_fargo.cuh"
 
 using namespace fgpu;
 
@@ -143,6 +146,8 @@ struct fgpu_handle {
   int graph_steps = 0;
   // launch shape
   int tile_x = 32, tile_y = 8, kchunk = 16;
+  int variant = 0;              // stage kernel layout: 0 shared-memory tile, 1 warp-shuffle window,
+                                // 2/3 tile with a register cap for more resident blocks
   // instrumentation
   cudaStream_t own_stream = nullptr;
   bool profiling = false;
@@ -150,6 +155,13 @@ struct fgpu_handle {
   std::vector<Timed> timed;
   fgpu_stats stats;
   int kernels_per_step = 0;
+  // FARGO transport (type 1, direction 2): d_w = [w | w_new], each by padded i.
+  // fargo_phase 0: before FirstStep; 1: after FirstStep (the stored state is
+  // FirstStep's real-frame cvar); 2: after a step (the stored state is the
+  // transported state, w the background velocity of its closing ComputeRHS)
+  bool fargo = false;
+  double* d_w = nullptr;
+  int fargo_phase = 0;
 };
 
 namespace {
@@ -176,7 +188,7 @@ void scale(int geo, double gp, double x, double& hx, double& hy, double& hz) {
 }
 
 enum { M_dAxW, M_dAyS, M_dAzB, M_dydzdV, M_dzdxdV, M_dxdydV, M_cxyx, M_cxzx, M_cyxy, M_cyzy, M_czxz, M_czyz,
-       M_dlx, M_dly, M_dlz, M_offxW, M_offxE, M_accel0, M_accel1, M_cs0, M_NI = M_cs0 + 7 };
+       M_dlx, M_dly, M_dlz, M_offxW, M_offxE, M_accel0, M_accel1, M_wfac, M_cs0, M_NI = M_cs0 + 7 };
 
 int build_metric(fgpu_handle* h) {
   const fgpu_config& c = h->cfg;
@@ -231,6 +243,12 @@ int build_metric(fgpu_handle* h) {
     A(M_dlz, ip) = hzc * dz;
     A(M_offxW, ip) = xw - x;
     A(M_offxE, ip) = xe - x;
+    // FARGO wfactor (timedisc_base.f90:433-441): the narrowest y-width of the cell over its
+    // W/E and B/T faces relative to the width through the centre
+    {
+      auto mn = [](double a, double b) { return b < a ? b : a; };
+      A(M_wfac, ip) = mn(mn(hyw, hye), mn(hyc, hyc)) / hyc;
+    }
     if (h->has_accel) {
       // gravity_pointmass.f90:263-282 with the point mass at the origin, NEWTON potential
       double r, posx;
@@ -286,12 +304,24 @@ template <int ND, bool EU, bool PRIM>
 int launch_stage_t(fgpu_handle* h, StageArgs& A) {
   A.kchunk = h->kchunk;
   const Grid& g = h->g;
-  if constexpr (ND == 2) {
+  const int kz = ND == 3 ? (g.nz + h->kchunk - 1) / h->kchunk : 1;
+  if (h->variant == 1) {
+    // warp-shuffle layout: 32 x 8 points per block, 30 x 6 output cells
+    constexpr int NW = 8;
+    dim3 grid((g.nx + 29) / 30, (g.ny + NW - 3) / (NW - 2), kz);
+    stage2_kernel<ND, EU, PRIM, NW><<<grid, 32 * NW, 0, h->stream>>>(A);
+  } else if constexpr (ND == 2) {
+    // shared-memory tile 32 x 8; variants 2/3 cap registers for 2/3 resident blocks per SM
     dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, 1);
-    stage_kernel<ND, EU, PRIM, 32, 8><<<grid, 256, 0, h->stream>>>(A);
+    if (h->variant == 2) stage_kernel<ND, EU, PRIM, 32, 8, 2><<<grid, 256, 0, h->stream>>>(A);
+    else if (h->variant == 3) stage_kernel<ND, EU, PRIM, 32, 8, 3><<<grid, 256, 0, h->stream>>>(A);
+    else stage_kernel<ND, EU, PRIM, 32, 8><<<grid, 256, 0, h->stream>>>(A);
   } else {
-    dim3 grid((g.nx + 31) / 32, (g.ny + 3) / 4, (g.nz + h->kchunk - 1) / h->kchunk);
-    stage_kernel<ND, EU, PRIM, 32, 4><<<grid, 128, 0, h->stream>>>(A);
+    // shared-memory tile 32 x 4 marching in z; variants 2/3 cap registers for 4/6 resident blocks per SM
+    dim3 grid((g.nx + 31) / 32, (g.ny + 3) / 4, kz);
+    if (h->variant == 2) stage_kernel<ND, EU, PRIM, 32, 4, 4><<<grid, 128, 0, h->stream>>>(A);
+    else if (h->variant == 3) stage_kernel<ND, EU, PRIM, 32, 4, 6><<<grid, 128, 0, h->stream>>>(A);
+    else stage_kernel<ND, EU, PRIM, 32, 4><<<grid, 128, 0, h->stream>>>(A);
   }
   CUDA_TRY(h, cudaGetLastError());
   return FGPU_OK;
@@ -437,32 +467,150 @@ double ctl_invdt(const fgpu_handle* h) {
 // eta(n,order), timedisc_modeuler.f90:74-77
 const double kEta[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.5, 0.0}, {0.0, 0.75, 1.0 / 3.0}};
 
-int enqueue_shu_osher_step(fgpu_handle* h) {
+// Arguments of Shu-Osher stage n (1-based) of one grid: stage 1 reads the
+// stored state P (with the CHECK_PMIN round trip of the last ComputeRHS),
+// stages alternate between the scratch states A and B, the last stage writes P
+// and reduces the CFL of the new state (order 1 goes through A and a copy).
+StageArgs shu_osher_stage(fgpu_handle* h, int n) {
   double* P = h->buf[0];
   double* Abuf = h->buf[1];
   double* Bbuf = h->buf[2];
+  const double* in = n == 1 ? P : ((n - 1) % 2 == 1 ? Abuf : Bbuf);
+  StageArgs A = base_args(h);
+  A.in = plain_state(in, n == 1 && h->roundtrip_cfg);
+  A.out_mode = OUT_SSPRK;
+  A.eta = kEta[h->order - 1][n - 1];
+  A.y0 = P;
+  A.y0_roundtrip = h->roundtrip_cfg ? 1 : 0;
+  A.dt_dev = &h->d_ctl->dt;
+  A.out = (n == h->order && h->order > 1) ? P : ((n % 2 == 1) ? Abuf : Bbuf);
+  if (n == h->order) { A.cfl_mode = 1; A.cfl_roundtrip = h->roundtrip_cfg ? 1 : 0; }
+  return A;
+}
+
+int enqueue_shu_osher_step(fgpu_handle* h) {
+  for (int n = 1; n <= h->order; ++n) {
+    StageArgs A = shu_osher_stage(h, n);
+    if (int rc = launch_stage(h, A)) return rc;
+  }
+  if (h->order == 1)
+    CUDA_TRY(h, cudaMemcpyAsync(h->buf[0], h->buf[1], sizeof(double) * h->V * h->g.n, cudaMemcpyDeviceToDevice,
+                                h->stream));
+  BndArgs B = bnd_args(h, h->buf[0], h->roundtrip_cfg, FIN_STEP);
+  return launch_misc(h, 0, B);
+}
+
+// ---------------------------------------------------------------- FARGO (device clock)
+Chain chain_add(Chain c, const double* w, double sgn) {
+  c.w[c.n] = w;
+  c.s[c.n] = sgn;
+  c.n += 1;
+  return c;
+}
+Chain chain_none() {
+  Chain c;
+  std::memset(&c, 0, sizeof(c));
+  return c;
+}
+// Frame changes that turn the stored state into the real-frame cvar of the last
+// ComputeRHS: none after FirstStep, AddBackgroundVelocityY(w) after a step.
+Chain fargo_pre(const fgpu_handle* h) {
+  return h->fargo_phase == 2 ? chain_add(chain_none(), h->d_w, 1.0) : chain_none();
+}
+const double* fargo_wfac(const fgpu_handle* h) { return h->d_metric + (size_t)M_wfac * h->nxp; }
+
+int launch_fargo_w(fgpu_handle* h, const StateRef& in, const double* w_prev, double* w_out) {
+  FargoWArgs F;
+  std::memset(&F, 0, sizeof(F));
+  F.g = h->g; F.ph = h->ph; F.mt = h->mt;
+  F.in = in;
+  F.w_prev = w_prev;
+  F.wfac = fargo_wfac(h);
+  F.w_out = w_out;
+  F.ctl = h->d_ctl;
+  return timed_launch(h, false, 0.0, [&] {
+    unsigned blocks = (unsigned)((h->g.nx + 4 + 127) / 128);
+    fargo_w_kernel<<<blocks, 128, 0, h->stream>>>(F);
+    CUDA_TRY(h, cudaGetLastError());
+    return FGPU_OK;
+  });
+}
+
+int launch_fargo_advect(fgpu_handle* h, const double* in, double* out, const double* w) {
+  FargoAdvArgs X;
+  std::memset(&X, 0, sizeof(X));
+  X.g = h->g; X.ph = h->ph; X.mt = h->mt;
+  X.in = plain_state(in, false);
+  X.w = w;
+  X.out = out;
+  X.ctl = h->d_ctl;
+  X.checkdata = h->cfg.checkdata;
+  X.chunk = 16;
+  return timed_launch(h, false, 0.0, [&] {
+    constexpr int TX = 32, TY = 4;
+    dim3 grid((h->g.nx + TX - 1) / TX, (h->g.ny + TY * X.chunk - 1) / (TY * X.chunk));
+    fargo_advect_kernel<TX, TY><<<grid, TX * TY, 0, h->stream>>>(X);
+    CUDA_TRY(h, cudaGetLastError());
+    return FGPU_OK;
+  });
+}
+
+// One fosite%Step with FARGO transport (timedisc_base.f90:649-750 with the
+// modified-Euler SolveODE, timedisc_modeuler.f90:279-291):
+//   CalcBackgroundVelocity -> w_new; the Shu-Osher stages on the co-moving
+//   state; FargoAdvectionY; the closing ComputeRHS's CheckData and
+//   CalcTimestep.  The in-place frame changes of cvar are carried as chains:
+//   fosite's cvar at stage 1 is pre + [-w, +w, -w_new] applied to the stored
+//   state, cold is pre + [-w], later stages read the previous stage's result
+//   with [+w_new] (ComputeRHS's AddBackgroundVelocityY) and their Shu-Osher
+//   base is [+w_new, -w_new].
+int enqueue_fargo_step(fgpu_handle* h) {
+  double* P = h->buf[0];
+  double* Abuf = h->buf[1];
+  double* Bbuf = h->buf[2];
+  const double* W = h->d_w;
+  double* Wn = h->d_w + h->nxp;
+  const Chain pre = fargo_pre(h);
+  {
+    StateRef S = plain_state(P, false);
+    S.pre = pre;
+    if (int rc = launch_fargo_w(h, S, W, Wn)) return rc;
+  }
+  const Chain cold = chain_add(pre, W, -1.0);
   const double* in = P;
   for (int n = 1; n <= h->order; ++n) {
     StageArgs A = base_args(h);
-    A.in = plain_state(in, n == 1 && h->roundtrip_cfg);
+    A.in = plain_state(in, false);
+    if (n == 1) {
+      A.in.pre = pre;
+      A.w_sub = W;
+      A.yn_chain = chain_add(chain_add(cold, W, 1.0), Wn, -1.0);
+    } else {
+      A.in.pre = chain_add(chain_none(), Wn, 1.0);
+      A.w_sub = Wn;
+      A.yn_chain = chain_add(A.in.pre, Wn, -1.0);
+    }
     A.out_mode = OUT_SSPRK;
     A.eta = kEta[h->order - 1][n - 1];
     A.y0 = P;
-    A.y0_roundtrip = h->roundtrip_cfg ? 1 : 0;
+    A.y0_chain = cold;
     A.dt_dev = &h->d_ctl->dt;
-    double* out;
-    if (n == h->order && h->order > 1) out = P;
-    else out = (n % 2 == 1) ? Abuf : Bbuf;
+    double* out = (n % 2 == 1) ? Abuf : Bbuf;
     A.out = out;
-    if (n == h->order) { A.cfl_mode = 1; A.cfl_roundtrip = h->roundtrip_cfg ? 1 : 0; }
     if (int rc = launch_stage(h, A)) return rc;
     in = out;
   }
-  if (h->order == 1)
-    CUDA_TRY(h, cudaMemcpyAsync(P, Abuf, sizeof(double) * h->V * h->g.n, cudaMemcpyDeviceToDevice, h->stream));
-  BndArgs B = bnd_args(h, P, h->roundtrip_cfg, FIN_STEP);
-  return launch_misc(h, 0, B);
+  if (int rc = launch_fargo_advect(h, in, P, Wn)) return rc;
+  BndArgs B = bnd_args(h, P, false, FIN_STEP);
+  B.in.pre = chain_add(chain_none(), Wn, 1.0);
+  B.w_sub = Wn;
+  if (int rc = launch_misc(h, 0, B)) return rc;
+  CUDA_TRY(h, cudaMemcpyAsync(h->d_w, Wn, sizeof(double) * h->nxp, cudaMemcpyDeviceToDevice, h->stream));
+  h->fargo_phase = 2;
+  return FGPU_OK;
 }
+
+int enqueue_step(fgpu_handle* h) { return h->fargo ? enqueue_fargo_step(h) : enqueue_shu_osher_step(h); }
 
 int build_graph(fgpu_handle* h, int steps) {
   if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
@@ -470,7 +618,7 @@ int build_graph(fgpu_handle* h, int steps) {
   fgpu_stats saved = h->stats;
   CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
   int rc = 0;
-  for (int s = 0; s < steps && !rc; ++s) rc = enqueue_shu_osher_step(h);
+  for (int s = 0; s < steps && !rc; ++s) rc = enqueue_step(h);
   cudaError_t e = cudaStreamEndCapture(h->stream, &gr);
   h->kernels_per_step = (int)((h->stats.launches - saved.launches) / steps);
   h->stats = saved;
@@ -647,7 +795,6 @@ int validate(fgpu_handle* h) {
   for (int d = 0; d < h->nd; ++d)
     if ((c.bc[2 * d] == FGPU_PERIODIC) != (c.bc[2 * d + 1] == FGPU_PERIODIC))
       return set_err(h, FGPU_EBADCFG, "periodic boundaries must be paired");
-  if (c.fargo_method != 0) return set_err(h, FGPU_EUNSUPPORTED, "fargo transport is not available on this backend yet");
   h->curv = c.geometry != FGPU_CARTESIAN;
   if (c.pointmass) {
     if (c.geometry == FGPU_CARTESIAN || h->nd != 2)
@@ -679,6 +826,14 @@ int validate(fgpu_handle* h) {
   if (c.tmin > 1.e-10 && (c.checkdata & FGPU_CHECK_TMIN) && h->euler)
     return set_err(h, FGPU_EUNSUPPORTED, "CHECK_TMIN with tmin > 1e-10 is not supported");
   h->roundtrip_cfg = h->euler && (c.checkdata & FGPU_CHECK_PMIN);
+  if (c.fargo_method != 0) {
+    if (c.fargo_method != 1)
+      return set_err(h, FGPU_EUNSUPPORTED, "fargo: only type 1 (background velocity computed every step) is supported");
+    if (c.fargo_direction != 2) return set_err(h, FGPU_EUNSUPPORTED, "fargo: only transport along y (direction 2) is supported");
+    if (h->nd != 2 || h->euler) return set_err(h, FGPU_EUNSUPPORTED, "fargo: 2D x-y meshes with isothermal physics only");
+    if (h->butcher) return set_err(h, FGPU_EUNSUPPORTED, "fargo: fixed-step modified Euler (Shu-Osher) time stepping only");
+    h->fargo = true;
+  }
   return FGPU_OK;
 }
 
@@ -727,6 +882,11 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
     if (device >= 0) { if (cudaSetDevice(device) != cudaSuccess) rc = set_err(h, FGPU_ECUDA, "cudaSetDevice failed"); }
     cudaGetDevice(&h->device);
   }
+  if (!rc) {
+    // FGPU_STAGE_VARIANT / FGPU_KCHUNK force a stage-kernel layout and z chunk (the tuner's choice otherwise)
+    if (const char* e = std::getenv("FGPU_STAGE_VARIANT")) h->variant = std::max(0, std::min(3, std::atoi(e)));
+    if (const char* e = std::getenv("FGPU_KCHUNK")) { int v = std::atoi(e); if (v > 0) h->kchunk = v; }
+  }
   if (!rc) rc = build_metric(h);
   if (!rc) {
     h->g.nx = cfg->inum; h->g.ny = cfg->jnum; h->g.nz = h->nd == 3 ? cfg->knum : 1;
@@ -734,6 +894,7 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
     for (int f = 0; f < 6; ++f) h->g.bc[f] = cfg->bc[f];
     h->ph.gamma = cfg->gamma; h->ph.gm1 = cfg->gamma - 1.; h->ph.pmin = cfg->pmin; h->ph.rhomin = cfg->rhomin;
     h->ph.tiny2 = 2.0 * DBL_MIN;
+    h->ph.inv_gm1 = 1.0 / h->ph.gm1;
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) rc = set_err(h, FGPU_ECUDA, "stream");
   }
   if (!rc) rc = upload_metric(h);
@@ -747,6 +908,10 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
       cudaMemsetAsync(p, 0, bytes, h->stream);
       h->buf.push_back(p);
     }
+  }
+  if (!rc && h->fargo) {
+    if (cudaMalloc(&h->d_w, sizeof(double) * 2 * h->nxp) != cudaSuccess) rc = set_err(h, FGPU_ENOMEM, "fargo arrays");
+    else cudaMemsetAsync(h->d_w, 0, sizeof(double) * 2 * h->nxp, h->stream);
   }
   if (!rc) {
     if (cudaMalloc(&h->d_ctl, sizeof(Ctl)) != cudaSuccess) rc = set_err(h, FGPU_ENOMEM, "control block");
@@ -776,6 +941,7 @@ void fgpu_destroy(fgpu_handle* h) {
   for (double* p : h->buf) cudaFree(p);
   if (h->d_pad) cudaFree(h->d_pad);
   if (h->d_metric) cudaFree(h->d_metric);
+  if (h->d_w) cudaFree(h->d_w);
   if (h->d_ctl) cudaFree(h->d_ctl);
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
   if (h->own_stream) h->stream = h->own_stream;
@@ -883,6 +1049,9 @@ int fgpu_upload_state(fgpu_handle* h, int which, const double* data, int64_t n) 
   CUDA_TRY(h, cudaGetLastError());
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   h->state_pre = false;
+  // FARGO: after FirstStep an uploaded cvar is in the co-moving frame (what fgpu_download
+  // returns); it takes the place of the transported state of the last step
+  if (h->fargo && h->fargo_phase >= 1) h->fargo_phase = 2;
   return FGPU_OK;
 }
 
@@ -924,6 +1093,7 @@ int fgpu_download(fgpu_handle* h, int which, double* out, int64_t n) {
   CUDA_TRY(h, cudaMemsetAsync(h->d_pad, 0, sizeof(double) * 2 * nc * h->V, h->stream));
   bool rt = h->state_pre && h->roundtrip_cfg;
   BndArgs B = bnd_args(h, h->buf[0], rt, FIN_NONE);
+  if (h->fargo) { B.in.pre = fargo_pre(h); B.w_sub = h->d_w; }
   B.ctl = nullptr;
   B.out_p = h->d_pad;
   B.out_c = h->d_pad + nc * h->V;
@@ -960,6 +1130,14 @@ int fgpu_first_step(fgpu_handle* h) {
   c->time = 0.0; c->dtmin = h->stoptime; c->iter = 0;
   if (int rc = write_ctl(h)) return rc;
   BndArgs B = bnd_args(h, h->buf[0], h->roundtrip_cfg, FIN_FIRST);
+  if (h->fargo) {
+    // FirstStep's CenterBoundary + CalcBackgroundVelocity (fosite.f90:315-321), then the
+    // CFL of its ComputeRHS on the co-moving state
+    if (int rc = launch_fargo_w(h, plain_state(h->buf[0], false), nullptr, h->d_w)) return rc;
+    CUDA_TRY(h, cudaMemcpyAsync(h->d_w + h->nxp, h->d_w, sizeof(double) * h->nxp, cudaMemcpyDeviceToDevice, h->stream));
+    B.w_sub = h->d_w;
+    h->fargo_phase = 1;
+  }
   if (int rc = launch_misc(h, 1, B)) return rc;
   if (int rc = launch_misc(h, 0, B)) return rc;
   if (int rc = read_ctl(h)) return rc;
@@ -999,6 +1177,11 @@ int fgpu_run(fgpu_handle* h, int64_t n, int64_t* done) {
   }
   // device clock: graph of G steps, replayed
   long long it0 = h->iter;
+  if (h->fargo && h->fargo_phase < 2 && n > 0) {
+    // the first FARGO step after FirstStep has its own frame chains: direct launches
+    if (int rc = enqueue_fargo_step(h)) return rc;
+    n -= 1;
+  }
   const int G = 16;
   int64_t full = n / G, rest = n % G;
   if (h->profiling) { rest += full * G; full = 0; }   // per-launch timing needs direct launches
@@ -1010,7 +1193,7 @@ int fgpu_run(fgpu_handle* h, int64_t n, int64_t* done) {
       h->stats.stage_launches += (int64_t)h->order * G;
     }
   }
-  for (int64_t r = 0; r < rest; ++r) { if (int rc = enqueue_shu_osher_step(h)) return rc; }
+  for (int64_t r = 0; r < rest; ++r) { if (int rc = enqueue_step(h)) return rc; }
   if (int rc = read_ctl(h)) return rc;
   sync_from_ctl(h);
   h->stats.attempts += h->iter - it0;
@@ -1045,6 +1228,12 @@ int fgpu_compute_rhs(fgpu_handle* h) {
   }
   StageArgs A = base_args(h);
   A.in = plain_state(src, false);
+  if (h->fargo) {
+    // fosite's cvar is pre + [-w]; ComputeRHS adds w back before the boundary fill.
+    // The stored state is left as it is (the reference's in-place round trip is not applied).
+    if (h->fargo_phase >= 1) A.in.pre = chain_add(chain_add(fargo_pre(h), h->d_w, -1.0), h->d_w, 1.0);
+    A.w_sub = h->d_w;
+  }
   A.out_mode = OUT_RHS;
   A.out = out;
   A.ctl = nullptr;
@@ -1064,6 +1253,7 @@ int fgpu_calc_timestep(fgpu_handle* h, double* dt) {
   h->h_ctl->stop = 0; h->h_ctl->brk = 0;
   if (int rc = write_ctl(h)) return rc;
   BndArgs B = bnd_args(h, h->buf[0], rt, FIN_NONE);
+  if (h->fargo) { B.in.pre = fargo_pre(h); B.w_sub = h->d_w; }
   if (int rc = launch_misc(h, 1, B)) return rc;
   if (int rc = launch_misc(h, 0, B)) return rc;
   if (int rc = read_ctl(h)) return rc;
@@ -1128,6 +1318,9 @@ int fgpu_reset_stats(fgpu_handle* h) {
 }
 
 }  // extern "C"
+
+// ======================================================================= batched ensembles, autotuner
+#include "fgpu_batch.cuh"
 
 // ======================================================================= allocation-free CFL time step
 // Callers that must not allocate device memory after start-up -- code running
@@ -1256,6 +1449,7 @@ extern "C" int fgpu_calc_timestep_noalloc(const fgpu_config* cfg, const double* 
   B.g.n = (long long)B.g.nx * B.g.ny * B.g.nz;
   for (int f = 0; f < 6; ++f) B.g.bc[f] = c.bc[f];
   B.ph.gamma = c.gamma; B.ph.gm1 = c.gamma - 1.; B.ph.pmin = c.pmin; B.ph.rhomin = c.rhomin; B.ph.tiny2 = 2.0 * DBL_MIN;
+  B.ph.inv_gm1 = 1.0 / B.ph.gm1;
   MetricP& M = B.mt;
   auto P = [&](int which) { return dm + (size_t)which * nxp; };
   M.dAxW = P(M_dAxW); M.dAyS = P(M_dAyS); M.dAzB = P(M_dAzB);

@@ -53,6 +53,10 @@ struct StageArgs {
   int checkdata;
   Ctl* ctl;
   int kchunk;
+  // FARGO (2D isothermal): co-moving frame of the fluxes (SubtractBackgroundVelocityY after the
+  // sources) and the Shu-Osher base states as chains of frame changes of the stored states
+  const double* w_sub;
+  Chain yn_chain, y0_chain;
 };
 
 // block-wide max of up to 3 non-negative doubles + OR of flags, then one atomic per block
@@ -87,8 +91,11 @@ __device__ __forceinline__ void block_reduce_emit(double* vals, int nv, int flag
   }
 }
 
+// One TX x TY tile (bx, by) of one grid, z chunk bz.  Shared by the single-grid
+// kernel (arguments in the parameter space) and the batched kernel (per-grid
+// arguments in global memory, tiles from a flattened queue).
 template <int ND, bool EU, bool PRIM, int TX, int TY>
-__global__ void __launch_bounds__(TX* TY) stage_kernel(const __grid_constant__ StageArgs A) {
+__device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, const int by, const int bz) {
   using PH = Phys<ND, EU>;
   using CE = Cells<ND, EU>;
   constexpr int V = PH::V;
@@ -107,14 +114,15 @@ __global__ void __launch_bounds__(TX* TY) stage_kernel(const __grid_constant__ S
   const MetricP& M = A.mt;
   const double dt = A.dt_dev ? *A.dt_dev : A.dt;
   const bool roundtrip = EU && A.in.roundtrip;
+  constexpr bool FG = ND == 2 && !EU;   // FARGO transforms are compiled for 2D isothermal physics only
   const int tid = threadIdx.x;
   const int tx = tid % TX, ty = tid / TX;
-  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int i0 = bx * TX, j0 = by * TY;
   const int ex = min(TX, g.nx - i0), ey = min(TY, g.ny - j0);
   const bool own = tx < ex && ty < ey;
   const int i = i0 + tx, j = j0 + ty;
   int k0 = 0, k1 = 1;
-  if (ND == 3) { k0 = blockIdx.z * A.kchunk; k1 = min(g.nz, k0 + A.kchunk); }
+  if (ND == 3) { k0 = bz * A.kchunk; k1 = min(g.nz, k0 + A.kchunk); }
 
   auto RS = [&](int v, int ly, int lx) -> double& { return Rs[(v * RH + ly) * RW + lx]; };
   auto SS = [&](int v, int r, int c) -> double& { return Ss[(v * SH + r) * SW + c]; };
@@ -127,9 +135,11 @@ __global__ void __launch_bounds__(TX* TY) stage_kernel(const __grid_constant__ S
     if (inx && iny && inz) {
       double u[V];
       state_at<V>(A.in, g.n, CE::lin(g, gi, gj, gk), u);
+      if (FG && A.in.pre.n) apply_chain(A.in.pre, u, gi + 2);
       if (PRIM) {
         PH::c2p(u, p, P);
         if (roundtrip) p[V - 1] = dmax(p[V - 1], P.pmin);
+        if (FG && A.w_sub) p[2] = p[2] - A.w_sub[gi + 2];
 #pragma unroll
         for (int l = 0; l < V; ++l) R[l] = p[l];
       } else if (roundtrip) {
@@ -139,16 +149,19 @@ __global__ void __launch_bounds__(TX* TY) stage_kernel(const __grid_constant__ S
       } else {
 #pragma unroll
         for (int l = 0; l < V; ++l) R[l] = u[l];
+        if (FG && A.w_sub) R[2] = R[2] - R[0] * A.w_sub[gi + 2];
       }
     } else {
       int d = !inx ? 0 : (!iny ? 1 : 2);
       CE::face_ghost_p(A.in, g, P, M, d, gi, gj, gk, p);
       if (roundtrip) p[V - 1] = dmax(p[V - 1], P.pmin);
       if (PRIM) {
+        if (FG && A.w_sub) p[2] = p[2] - A.w_sub[gi + 2];
 #pragma unroll
         for (int l = 0; l < V; ++l) R[l] = p[l];
       } else {
         PH::p2c(p, R, P);
+        if (FG && A.w_sub) R[2] = R[2] - R[0] * A.w_sub[gi + 2];
       }
     }
   };
@@ -332,8 +345,28 @@ __global__ void __launch_bounds__(TX* TY) stage_kernel(const __grid_constant__ S
       double rhs[V];
 #pragma unroll
       for (int v = 0; v < V; ++v) rhs[v] = (divX[v] + divY[v]) + (ND == 3 ? divZ[v] : 0.0);
+      // with FARGO the sources see the real frame: cvar after AddBackgroundVelocityY and the
+      // primitive state CenterBoundary derives from it
+      const bool fsrc = FG && A.w_sub;
+      if (fsrc) {
+        state_at<V>(A.in, g.n, idx, cc);
+        if (A.in.pre.n) apply_chain(A.in.pre, cc, ip);
+        PH::c2p(cc, pc, P);
+      }
       // geometric sources (physics_euler.f90:1706-1847 / physics_eulerisotherm.f90:689-832)
-      if (M.curv) {
+      double geo2 = 0.0;
+      if (M.curv && ND == 2 && fsrc) {
+        double Pp = pc[0] * (M.cs[ip] * M.cs[ip]);
+        double vx = pc[1], vy = pc[2];
+        double cxyx = M.cxyx[ip], cyxy = M.cyxy[ip], czxz = M.czxz[ip], czyz = M.czyz[ip];
+        rhs[1] = rhs[1] - (cc[2] * (cyxy * vy - cxyx * vx) + (cyxy + czxz) * Pp);
+        geo2 = cc[1] * (cxyx * vx - cyxy * vy) + (cxyx + czyz) * Pp;
+      }
+      if (fsrc) {
+        // AddFargoSourcesY (physics_eulerisotherm.f90:1531-1586) into the geometric source
+        geo2 = geo2 - cc[1] * 0.5 * (A.w_sub[ip + 1] - A.w_sub[ip - 1]) / M.dlx[ip];
+        rhs[2] = rhs[2] - geo2;
+      } else if (M.curv) {
         double Pp = EU ? pc[V - 1] : pc[0] * (M.cs[ip] * M.cs[ip]);
         double vx = pc[1], vy = pc[2];
         double cxyx = M.cxyx[ip], cyxy = M.cyxy[ip], czxz = M.czxz[ip], czyz = M.czyz[ip];
@@ -363,7 +396,10 @@ __global__ void __launch_bounds__(TX* TY) stage_kernel(const __grid_constant__ S
       } else {
         // Shu-Osher update y = yn - dt*rhs + eta*(y0 - yn + dt*rhs) (timedisc_modeuler.f90:289)
         double yn[V], y0[V], y[V];
-        if (!PRIM) {
+        if (FG && A.yn_chain.n) {
+          state_at<V>(A.in, g.n, idx, yn);
+          apply_chain(A.yn_chain, yn, ip);
+        } else if (!PRIM) {
 #pragma unroll
           for (int v = 0; v < V; ++v) yn[v] = cc[v];
         } else if (roundtrip) {
@@ -374,6 +410,7 @@ __global__ void __launch_bounds__(TX* TY) stage_kernel(const __grid_constant__ S
         }
 #pragma unroll
         for (int v = 0; v < V; ++v) y0[v] = __ldg(A.y0 + (long long)v * g.n + idx);
+        if (FG && A.y0_chain.n) apply_chain(A.y0_chain, y0, ip);
         if (EU && A.y0_roundtrip) {
           double q[V];
           PH::c2p(y0, q, P);
@@ -451,6 +488,22 @@ __global__ void __launch_bounds__(TX* TY) stage_kernel(const __grid_constant__ S
     if (A.last_stage && !A.cfl_mode) { vals[0] = errv; nv = 1; }
     if (nv) block_reduce_emit<NT>(vals, nv, flags, A.last_stage && !A.cfl_mode ? &A.ctl->err : A.ctl->invdt,
                                   &A.ctl->flags, sred);
+  }
+}
+
+template <int ND, bool EU, bool PRIM, int TX, int TY, int MINB = 1>
+__global__ void __launch_bounds__(TX* TY, MINB) stage_kernel(const __grid_constant__ StageArgs A) {
+  stage_tile<ND, EU, PRIM, TX, TY>(A, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Batched ensemble: one persistent launch over the flattened tile queue of
+// many independent grids; tile t = (grid, bx, by, bz), args[grid] its stage.
+template <int ND, bool EU, bool PRIM, int TX, int TY, int MINB = 1>
+__global__ void __launch_bounds__(TX* TY, MINB) batched_stage_kernel(const StageArgs* __restrict__ args,
+                                                                      const int4* __restrict__ tiles, int ntiles) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int4 T = tiles[t];
+    stage_tile<ND, EU, PRIM, TX, TY>(args[T.x], T.y, T.z, T.w);
   }
 }
 

@@ -20,7 +20,21 @@ struct BndArgs {
   double* out_p;   // optional: padded primitive output (ghost cells)
   double* out_c;   // optional: padded conservative output (ghost cells)
   long long npad;  // padded cell count (field stride of out_p/out_c)
+  // FARGO: background velocity subtracted after the boundary fill (the co-moving
+  // frame that CalcTimestep and the caller's cvar/pvar see); null = off
+  const double* w_sub;
 };
+
+// FARGO frame of a checked cell: the real-frame p/c computed from the state go
+// to the co-moving frame, SubtractBackgroundVelocityY (physics_eulerisotherm.f90:1336-1413)
+template <int ND, bool EU>
+__device__ __forceinline__ void to_comoving(const double* w_sub, int ip, double* p, double* c) {
+  if (ND == 2 && !EU && w_sub) {
+    double w = w_sub[ip];
+    p[2] = p[2] - w;
+    c[2] = c[2] - c[0] * w;
+  }
+}
 
 // ghost cell number t -> padded coordinates (x slabs, then y slabs, then z slabs)
 template <int ND>
@@ -80,8 +94,9 @@ __device__ void finalize_step(Ctl* c, int mode) {
   c->dtcause = cause;
 }
 
+// Block blk of nblk (256 threads each) of the ghost-cell pass of one grid.
 template <int ND, bool EU>
-__global__ void __launch_bounds__(256) boundary_kernel(const __grid_constant__ BndArgs A) {
+__device__ __forceinline__ void boundary_block(const BndArgs& A, const int blk, const int nblk) {
   using PH = Phys<ND, EU>;
   using CE = Cells<ND, EU>;
   constexpr int V = PH::V;
@@ -91,8 +106,7 @@ __global__ void __launch_bounds__(256) boundary_kernel(const __grid_constant__ B
   const MetricP& M = A.mt;
   double cflv[3] = {0.0, 0.0, 0.0};
   int flags = 0;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < A.nghost;
-       t += (long long)gridDim.x * blockDim.x) {
+  for (long long t = blk * 256LL + threadIdx.x; t < A.nghost; t += nblk * 256LL) {
     int px, py, pz;
     ghost_coords<ND>(A.g, t, px, py, pz);
     double p[V], c[V];
@@ -100,13 +114,14 @@ __global__ void __launch_bounds__(256) boundary_kernel(const __grid_constant__ B
     if (EU && A.roundtrip) p[V - 1] = dmax(p[V - 1], A.ph.pmin);
     PH::p2c(p, c, A.ph);
     double cs = EU ? PH::cs_of(p, A.ph) : M.cs[px];
+    if ((A.checkdata & 0x01) && !(cs > 0.)) flags |= 0x01;
+    if (A.checkdata & 0x08)
+      for (int v = 0; v < V; ++v) if (!isfinite(p[v]) || !isfinite(c[v])) flags |= 0x08;
+    to_comoving<ND, EU>(A.w_sub, px, p, c);
     double v3[3];
     CE::cfl_cell(p, cs, M, px, v3);
     cflv[0] = dmax(cflv[0], v3[0]);
     if (ND == 3) { cflv[1] = dmax(cflv[1], v3[1]); cflv[2] = dmax(cflv[2], v3[2]); }
-    if ((A.checkdata & 0x01) && !(cs > 0.)) flags |= 0x01;
-    if (A.checkdata & 0x08)
-      for (int v = 0; v < V; ++v) if (!isfinite(p[v]) || !isfinite(c[v])) flags |= 0x08;
     if (A.out_p) {
       long long pi = px + (long long)(A.g.nx + 4) * (py + (long long)(A.g.ny + 4) * pz);
       for (int v = 0; v < V; ++v) {
@@ -121,7 +136,7 @@ __global__ void __launch_bounds__(256) boundary_kernel(const __grid_constant__ B
   __threadfence();
   if (threadIdx.x == 0) {
     unsigned int done = atomicAdd(&A.ctl->blocks_done, 1u);
-    is_last = (done == gridDim.x - 1);
+    is_last = (done == (unsigned)nblk - 1);
   }
   __syncthreads();
   if (is_last && threadIdx.x == 0) {
@@ -129,6 +144,19 @@ __global__ void __launch_bounds__(256) boundary_kernel(const __grid_constant__ B
     A.ctl->blocks_done = 0;
     finalize_step<ND>(A.ctl, A.finalize);
   }
+}
+
+template <int ND, bool EU>
+__global__ void __launch_bounds__(256) boundary_kernel(const __grid_constant__ BndArgs A) {
+  boundary_block<ND, EU>(A, blockIdx.x, gridDim.x);
+}
+
+// Batched ensemble: block b runs block (y) of (z) of grid (x) of entry b.
+template <int ND, bool EU>
+__global__ void __launch_bounds__(256) batched_boundary_kernel(const BndArgs* __restrict__ args,
+                                                               const int4* __restrict__ blocks) {
+  const int4 T = blocks[blockIdx.x];
+  boundary_block<ND, EU>(args[T.x], T.y, T.z);
 }
 
 // CFL and CheckData of the interior cells of a stored state (FirstStep).
@@ -146,19 +174,21 @@ __global__ void __launch_bounds__(256) interior_cfl_kernel(const __grid_constant
     int i = (int)(t % A.g.nx);
     double u[V], p[V], c[V];
     state_at<V>(A.in, A.g.n, t, u);
+    if (ND == 2 && !EU && A.in.pre.n) apply_chain(A.in.pre, u, i + 2);
     PH::c2p(u, p, A.ph);
     if (EU && A.roundtrip) { p[V - 1] = dmax(p[V - 1], A.ph.pmin); PH::p2c(p, c, A.ph); }
     else { for (int v = 0; v < V; ++v) c[v] = u[v]; }
     double cs = EU ? PH::cs_of(p, A.ph) : M.cs[i + 2];
-    double v3[3];
-    CE::cfl_cell(p, cs, M, i + 2, v3);
-    cflv[0] = dmax(cflv[0], v3[0]);
-    if (ND == 3) { cflv[1] = dmax(cflv[1], v3[1]); cflv[2] = dmax(cflv[2], v3[2]); }
     if ((A.checkdata & 0x01) && !(cs > 0.)) flags |= 0x01;
     if (EU && (A.checkdata & 0x02) && p[V - 1] < A.ph.pmin) flags |= 0x02;
     if ((A.checkdata & 0x04) && p[0] < A.ph.rhomin) flags |= 0x04;
     if (A.checkdata & 0x08)
       for (int v = 0; v < V; ++v) if (!isfinite(p[v]) || !isfinite(c[v])) flags |= 0x08;
+    to_comoving<ND, EU>(A.w_sub, i + 2, p, c);
+    double v3[3];
+    CE::cfl_cell(p, cs, M, i + 2, v3);
+    cflv[0] = dmax(cflv[0], v3[0]);
+    if (ND == 3) { cflv[1] = dmax(cflv[1], v3[1]); cflv[2] = dmax(cflv[2], v3[2]); }
   }
   block_reduce_emit<256>(cflv, ND == 3 ? 3 : 1, flags, A.ctl->invdt, &A.ctl->flags, sred);
 }
@@ -175,9 +205,11 @@ __global__ void __launch_bounds__(256) pack_interior_kernel(const __grid_constan
     int j = (int)(r % A.g.ny), k = (int)(r / A.g.ny);
     double u[V], p[V], c[V];
     state_at<V>(A.in, A.g.n, t, u);
+    if (ND == 2 && !EU && A.in.pre.n) apply_chain(A.in.pre, u, i + 2);
     PH::c2p(u, p, A.ph);
     if (EU && A.roundtrip) { p[V - 1] = dmax(p[V - 1], A.ph.pmin); PH::p2c(p, c, A.ph); }
     else { for (int v = 0; v < V; ++v) c[v] = u[v]; }
+    to_comoving<ND, EU>(A.w_sub, i + 2, p, c);
     int kk = ND == 3 ? k + 2 : 0;
     long long pi = (i + 2) + (long long)(A.g.nx + 4) * ((j + 2) + (long long)(A.g.ny + 4) * kk);
     for (int v = 0; v < V; ++v) {

@@ -66,8 +66,12 @@ def khi2d(n=256, seed=1000, steps=1000):
     return c, p, {"steps": steps}
 
 
-def gauss3d(n=256, seed=2000, mc_theta=1.0):
-    """3D Euler Gaussian pressure pulse, reflecting walls, KT + MC, Dormand-Prince (tol 1e-5)."""
+def gauss3d(n=256, seed=2000, mc_theta=1.0, method=None):
+    """3D Euler Gaussian pressure pulse, reflecting walls, KT + MC, Dormand-Prince (tol 1e-5).
+
+    method=abi.MODIFIED_EULER gives the fixed-step SSPRK3 variant (CFL 0.4) that
+    batched ensembles and the serving loop use.
+    """
     c = _base((n, n, n), 3)
     c.xmin, c.xmax, c.ymin, c.ymax, c.zmin, c.zmax = -0.5, 0.5, -0.5, 0.5, -0.5, 0.5
     for f in range(6):
@@ -82,6 +86,10 @@ def gauss3d(n=256, seed=2000, mc_theta=1.0):
     c.tol_rel = 1e-5
     for v in range(abi.MAXVAR):
         c.tol_abs[v] = 1e-5
+    if method == abi.MODIFIED_EULER:
+        c.method = abi.MODIFIED_EULER
+        c.tdorder = 3
+        c.tol_rel = 10.0
     c.cfl = 0.4
     c.stoptime = 1.0e3
     abi.finalize_config(c)

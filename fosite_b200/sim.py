@@ -55,6 +55,15 @@ def lib(exact=False):
     L.fgpu_set_profiling.argtypes = [C.c_void_p, C.c_int]
     L.fgpu_get_stats.argtypes = [C.c_void_p, C.POINTER(abi.Stats)]
     L.fgpu_reset_stats.argtypes = [C.c_void_p]
+    L.fgpu_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+    L.fgpu_batch_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]
+    L.fgpu_batch_destroy.argtypes = [C.c_void_p]
+    L.fgpu_batch_last_error.argtypes = [C.c_void_p, C.c_char_p, C.c_int]
+    L.fgpu_batch_size.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.fgpu_batch_run.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_int)]
+    L.fgpu_batch_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+    L.fgpu_batch_enqueue.argtypes = [C.c_void_p, C.c_int64]
+    L.fgpu_batch_collect.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
     _libs[exact] = L
     return L
 
@@ -174,3 +183,74 @@ class Simulation:
 
     def reset_stats(self):
         self._check(self.L.fgpu_reset_stats(self.h))
+
+    def autotune(self, reps=3):
+        """Time every stage-kernel layout on this grid and keep the fastest; returns its id."""
+        v = C.c_int(0)
+        self._check(self.L.fgpu_autotune(self.h, int(reps), C.byref(v)))
+        return int(v.value)
+
+
+class Batch:
+    """Ensemble of Simulations advanced together by batched persistent launches.
+
+    The members must have run ``first_step``; they stay usable (status, get)
+    and must outlive the batch.  Stepping a member on its own while it belongs
+    to a live batch is not allowed.
+    """
+
+    def __init__(self, sims):
+        if not sims:
+            raise ValueError("empty batch")
+        self.sims = list(sims)
+        self.L = self.sims[0].L
+        arr = (C.c_void_p * len(self.sims))(*[s.h for s in self.sims])
+        b = C.c_void_p()
+        rc = self.L.fgpu_batch_create(arr, len(self.sims), C.byref(b))
+        if rc != 0:
+            buf = C.create_string_buffer(512)
+            self.L.fgpu_batch_last_error(None, buf, 512)
+            raise FositeError(rc, buf.value.decode())
+        self.b = b
+        m, t = C.c_int(0), C.c_int(0)
+        self.L.fgpu_batch_size(b, C.byref(m), C.byref(t))
+        self.tiles = int(t.value)
+
+    def _check(self, rc):
+        if rc < 0:
+            buf = C.create_string_buffer(512)
+            self.L.fgpu_batch_last_error(self.b, buf, 512)
+            raise FositeError(rc, buf.value.decode())
+        return rc
+
+    def run(self, n):
+        """Advance every member by n steps; returns how many are still running."""
+        a = C.c_int(0)
+        self._check(self.L.fgpu_batch_run(self.b, int(n), C.byref(a)))
+        return int(a.value)
+
+    def enqueue(self, n):
+        """Queue n steps of every member without waiting (see collect)."""
+        self._check(self.L.fgpu_batch_enqueue(self.b, int(n)))
+
+    def collect(self):
+        """Wait for the queued steps; returns how many members are still running."""
+        a = C.c_int(0)
+        self._check(self.L.fgpu_batch_collect(self.b, C.byref(a)))
+        return int(a.value)
+
+    def autotune(self, reps=3):
+        v = C.c_int(0)
+        self._check(self.L.fgpu_batch_autotune(self.b, int(reps), C.byref(v)))
+        return int(v.value)
+
+    def close(self):
+        if getattr(self, "b", None):
+            self.L.fgpu_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

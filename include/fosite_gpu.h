@@ -141,9 +141,11 @@ typedef struct fgpu_config {
     /* sources: central point mass (gravity/pointmass), 0 = off */
     int32_t pointmass;
     double  pm_mass;               /* default 1.0 */
-    /* fargo transport: method 0 off, 1 dynamic, 2 fixed background velocity */
+    /* fargo transport (timedisc_base.f90:369-452): method 0 off, 1 background velocity
+     * computed every step (the only type this backend runs; 2D x-y isothermal meshes with
+     * the fixed-step modified Euler scheme), 2 fixed user-supplied background velocity */
     int32_t fargo_method;
-    int32_t fargo_direction;       /* only 2 (azimuth) is supported */
+    int32_t fargo_direction;       /* only 2 (transport along y) is supported */
     /* output clip time for AdjustTimestep (io/fileio_base.f90:604-621); 0 = stoptime */
     double  tout;
 } fgpu_config;
@@ -207,7 +209,9 @@ int fgpu_set_sound_speeds(fgpu_handle* h, const double* bccsound, int64_t nb,
                           const double* fcsound, int64_t nf);
 
 /* Upload Timedisc%cvar (which = FGPU_CVAR) or Timedisc%pvar (FGPU_PVAR, then
- * converted with Convert2Conservative).  Only interior cells are read. */
+ * converted with Convert2Conservative).  Only interior cells are read.  With
+ * FARGO transport, a state uploaded after fgpu_first_step is taken to be in
+ * the co-moving frame, the frame fgpu_download returns. */
 int fgpu_upload_state(fgpu_handle* h, int which, const double* data, int64_t n);
 /* Download a ghost-padded array (FGPU_CVAR, FGPU_PVAR, FGPU_RHS, FGPU_BCCSOUND). */
 int fgpu_download(fgpu_handle* h, int which, double* out, int64_t n);
@@ -227,6 +231,42 @@ int fgpu_run(fgpu_handle* h, int64_t n, int64_t* done);
 int fgpu_compute_rhs(fgpu_handle* h);
 /* Timedisc%CalcTimestep of the current state (does not change the status). */
 int fgpu_calc_timestep(fgpu_handle* h, double* dt);
+/* Measure every stage-kernel layout on this grid (reps RHS evaluations each into
+ * a scratch array; the state is untouched) and keep the fastest for later
+ * steps.  *variant receives the choice.  No counterpart in the reference. */
+int fgpu_autotune(fgpu_handle* h, int reps, int* variant);
+
+/* ---- batched ensembles (no counterpart in the reference, which integrates one
+ * grid per process) ---------------------------------------------------------
+ * A batch advances many independent grids with one persistent launch per
+ * Runge-Kutta stage over the flattened tile queue of all grids, plus one
+ * ghost-cell / CFL / finalize launch.  Members are handles created, uploaded
+ * and past fgpu_first_step, all with the fixed-step modified Euler scheme of
+ * time order 2 or 3, the same dimensionality, physics and reconstruction
+ * variables, no FARGO, on one device; mesh sizes, geometry, limiters,
+ * boundaries and physical parameters may differ.  Each member keeps its own
+ * dt, time and stop state (a member that reached its stop time idles), and its
+ * results are bitwise those of stepping it alone.  The handles stay owned by
+ * the caller and must outlive the batch; while a batch runs, do not step its
+ * members individually. */
+typedef struct fgpu_batch fgpu_batch;
+int  fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out);
+void fgpu_batch_destroy(fgpu_batch* b);
+int  fgpu_batch_last_error(const fgpu_batch* b, char* buf, int len);
+/* number of members and of tiles in the flattened queue */
+int  fgpu_batch_size(const fgpu_batch* b, int* members, int* tiles);
+/* Advance every member by nsteps steps (replayed CUDA graphs of 16 steps);
+ * the members' status (fgpu_get_status) is current on return.  *active
+ * receives the number of members that have neither stopped nor broken. */
+int  fgpu_batch_run(fgpu_batch* b, int64_t nsteps, int* active);
+/* fgpu_batch_run in two halves, so that batches on different streams overlap:
+ * enqueue returns without waiting; collect waits for everything enqueued and
+ * updates the members' status. */
+int  fgpu_batch_enqueue(fgpu_batch* b, int64_t nsteps);
+int  fgpu_batch_collect(fgpu_batch* b, int* active);
+/* fgpu_autotune for the batched stage kernel. */
+int  fgpu_batch_autotune(fgpu_batch* b, int reps, int* variant);
+
 /* CalcTimestep for callers that cannot allocate device memory (no counterpart
  * in the reference).  Takes a config and a caller-owned device state in the
  * library's stored layout (interior cells only, one field of inum*jnum*knum

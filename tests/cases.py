@@ -81,6 +81,21 @@ def _disk(n=(32, 48), geometry=abi.LOGCYLINDRICAL, seed=31, hratio=0.05, variabl
     return c, p, extra
 
 
+def _disk_fargo(n=(32, 48), geometry=abi.LOGCYLINDRICAL, seed=51, variables=abi.PRIMITIVE, tdorder=3,
+                bcs=None, limiter=abi.VANLEER):
+    c, p, extra = problems.disk2d(nr=n[0], nphi=n[1], seed=seed, geometry=geometry, fargo=1)
+    c.variables = variables
+    c.tdorder = tdorder
+    c.limiter = limiter
+    if bcs:
+        for f, t in enumerate(bcs):
+            c.bc[f] = t
+    rng = np.random.default_rng(seed + 1)
+    p[1] = 0.01 * rng.uniform(-1, 1, p[1].shape)
+    p[2] = p[2] * (1.0 + 0.02 * rng.uniform(-1, 1, p[2].shape))
+    return c, p, extra
+
+
 def _iso3d(n=(18, 16, 20), seed=41):
     c = abi.default_config()
     c.inum, c.jnum, c.knum = n
@@ -129,6 +144,12 @@ CASES = {
     "disk_logcyl_pointmass": lambda: _disk(),
     "disk_cyl_pointmass_cons": lambda: _disk(geometry=abi.CYLINDRICAL, n=(40, 32), variables=abi.CONSERVATIVE),
     "iso3d_cashkarp_mixed_bc": lambda: _iso3d(),
+    "disk_fargo_logcyl": lambda: _disk_fargo(),
+    "disk_fargo_cyl_cons_reflect": lambda: _disk_fargo(geometry=abi.CYLINDRICAL, n=(36, 40), variables=abi.CONSERVATIVE,
+                                                       bcs=[abi.REFLECTING, abi.NO_GRADIENTS, abi.PERIODIC, abi.PERIODIC],
+                                                       limiter=abi.MONOCENT),
+    "disk_fargo_order1_minmod": lambda: _disk_fargo(n=(30, 44), tdorder=1, limiter=abi.MINMOD,
+                                                    bcs=[abi.REFLECTING, abi.REFLECTING, abi.PERIODIC, abi.PERIODIC]),
 }
 
 

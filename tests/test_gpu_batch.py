@@ -1,0 +1,146 @@
+"""Batched ensembles (fgpu_batch_*): one persistent launch per stage over the
+tile queue of many independent grids must give every grid exactly the
+results of stepping it alone, with its own dt, time and stop state."""
+import numpy as np
+import pytest
+
+from fosite_b200 import abi, problems
+from cases import _khi, _gauss3d
+
+pytestmark = pytest.mark.gpu
+
+
+def _disk_member(nr, nphi, geometry, hratio, sigma, seed, exact):
+    from fosite_b200.sim import Simulation
+    cfg, p, extra = problems.disk2d(nr=nr, nphi=nphi, seed=seed, hratio=hratio, sigma_index=sigma,
+                                    geometry=geometry, fargo=0)
+    s = Simulation(cfg, exact=exact)
+    shape = (1, nphi + 4, nr + 4)
+    s.set_sound_speeds(np.broadcast_to(extra["bccsound"], shape), np.broadcast_to(extra["fcsound"], (4,) + shape))
+    s.set_state(abi.PVAR, p)
+    assert s.first_step() == 0
+    return s
+
+
+def _disk_specs(n, seed=7):
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        nr = int(rng.integers(1, 5)) * 16 + 8          # deliberately not tile multiples
+        nphi = int(rng.integers(2, 6)) * 16 + 4
+        geo = abi.CYLINDRICAL if k % 2 else abi.LOGCYLINDRICAL
+        out.append((nr, nphi, geo, float(rng.uniform(0.03, 0.1)), float(rng.uniform(-1.5, -0.5)), 100 + k))
+    return out
+
+
+@pytest.mark.parametrize("exact", [True, False])
+def test_disk_ensemble_matches_single_grids(exact):
+    from fosite_b200.sim import Batch
+    specs = _disk_specs(7)
+    members = [_disk_member(*sp, exact=exact) for sp in specs]
+    alone = [_disk_member(*sp, exact=exact) for sp in specs]
+    b = Batch(members)
+    assert b.tiles == sum(((sp[0] + 31) // 32) * ((sp[1] + 7) // 8) for sp in specs)
+    assert b.run(21) == len(members)     # 16-step graph + 5 direct steps
+    for s in alone:
+        rc, done = s.run(21)
+        assert rc == 0 and done == 21
+    for m, s in zip(members, alone):
+        assert m.status().iter == s.status().iter == 21
+        assert m.status().time == s.status().time
+        assert m.status().dt == s.status().dt
+        assert np.array_equal(m.get(abi.CVAR), s.get(abi.CVAR))
+    b.close()
+
+
+def test_members_stop_independently():
+    """A member that reaches its stop time idles while the others go on."""
+    from fosite_b200.sim import Batch, Simulation
+    sims = []
+    for k, stop in enumerate((0.02, 1.0, 0.05)):
+        cfg, p, _ = _khi(n=(40 + 8 * k, 36), seed=3 + k)
+        cfg.stoptime = stop
+        abi.finalize_config(cfg)
+        s = Simulation(cfg, exact=True)
+        s.set_state(abi.PVAR, p)
+        s.first_step()
+        sims.append(s)
+    b = Batch(sims)
+    active = b.run(200)
+    st = [s.status() for s in sims]
+    assert abs(st[0].time - 0.02) <= 1e-5 * 0.02
+    assert abs(st[2].time - 0.05) <= 1e-5 * 0.05
+    assert active == 1 and st[1].time < 1.0
+    frozen = sims[0].get(abi.CVAR)
+    b.run(16)
+    assert np.array_equal(sims[0].get(abi.CVAR), frozen)
+    # the stopped member took exactly the steps a lone run takes to its stop time
+    cfg, p, _ = _khi(n=(40, 36), seed=3)
+    cfg.stoptime = 0.02
+    abi.finalize_config(cfg)
+    lone = Simulation(cfg, exact=True)
+    lone.set_state(abi.PVAR, p)
+    lone.first_step()
+    rc, done = lone.run(200)
+    assert rc == abi.STOPTIME
+    assert done == st[0].iter
+    assert np.array_equal(lone.get(abi.CVAR), frozen)
+
+
+def test_euler3d_ensemble_and_autotune():
+    from fosite_b200.sim import Batch, Simulation
+    sizes = [(12, 14, 10), (20, 9, 17), (16, 16, 16)]
+    def make():
+        out = []
+        for k, n in enumerate(sizes):
+            cfg, p, _ = _gauss3d(n=n, method=abi.MODIFIED_EULER, tdorder=3, limiter=abi.VANLEER, seed=60 + k)
+            s = Simulation(cfg, exact=True)
+            s.set_state(abi.PVAR, p)
+            s.first_step()
+            out.append(s)
+        return out
+    members, alone = make(), make()
+    b = Batch(members)
+    v = b.autotune(2)
+    assert v in (0, 2, 3)
+    b.run(18)
+    for s in alone:
+        s.run(18)
+    for m, s in zip(members, alone):
+        assert np.array_equal(m.get(abi.CVAR), s.get(abi.CVAR))
+        assert np.array_equal(m.get(abi.PVAR), s.get(abi.PVAR))
+
+
+def test_batch_rejects_mixed_or_unsupported_members():
+    from fosite_b200.sim import Batch, FositeError, Simulation
+    c1, p1, _ = _khi(n=(24, 24))
+    c2, p2, _ = _khi(n=(24, 24), variables=abi.PRIMITIVE)
+    a, b = Simulation(c1), Simulation(c2)
+    for s, p in ((a, p1), (b, p2)):
+        s.set_state(abi.PVAR, p)
+    with pytest.raises(FositeError):
+        Batch([a])                       # before first_step
+    a.first_step()
+    b.first_step()
+    with pytest.raises(FositeError):
+        Batch([a, b])                    # conservative and primitive reconstruction
+    c3, p3, _ = _khi(n=(24, 24), method=abi.DORMAND_PRINCE, tdorder=5)
+    d = Simulation(c3)
+    d.set_state(abi.PVAR, p3)
+    d.first_step()
+    with pytest.raises(FositeError):
+        Batch([d])                       # embedded RK members are not batched
+
+
+def test_single_grid_autotune_keeps_results():
+    from fosite_b200.sim import Simulation
+    cfg, p, _ = _khi(n=(64, 48))
+    a, b = Simulation(cfg, exact=True), Simulation(cfg, exact=True)
+    for s in (a, b):
+        s.set_state(abi.PVAR, p)
+        s.first_step()
+    v = a.autotune(2)
+    assert v in (0, 1, 2, 3)
+    a.run(20)
+    b.run(20)
+    assert np.array_equal(a.get(abi.CVAR), b.get(abi.CVAR))

@@ -116,7 +116,7 @@ def test_steps_bitwise_exact_build(name):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["khi_ssprk3_vanleer_cons", "gauss3d_dopri_mc_prim", "disk_logcyl_pointmass",
-                                  "euler2d_absorbing", "iso3d_cashkarp_mixed_bc"])
+                                  "euler2d_absorbing", "iso3d_cashkarp_mixed_bc", "disk_fargo_logcyl"])
 def test_fast_build_tolerance(name):
     cfg, o, g = _pair(name, exact=False)
     o.first_step()
@@ -148,6 +148,29 @@ def test_run_graph_matches_single_steps():
         b.step()
     assert a.status().time == b.status().time
     assert np.array_equal(a.get(abi.CVAR), b.get(abi.CVAR))
+
+
+@pytest.mark.gpu
+def test_fargo_graph_run_matches_single_steps():
+    """FARGO: the first step after FirstStep runs outside the graph, later steps replay it."""
+    from fosite_b200.sim import Simulation
+    cfg, p, extra = CASES["disk_fargo_cyl_cons_reflect"]()
+    sims = []
+    for _ in range(2):
+        s = Simulation(cfg, exact=True)
+        shape = (cfg.knum, cfg.jnum + 4, cfg.inum + 4)
+        s.set_sound_speeds(np.broadcast_to(extra["bccsound"], shape), np.broadcast_to(extra["fcsound"], (4,) + shape))
+        s.set_state(abi.PVAR, p)
+        s.first_step()
+        sims.append(s)
+    a, b = sims
+    rc, done = a.run(35)
+    assert rc == 0 and done == 35
+    for _ in range(35):
+        assert b.step() == 0
+    assert a.status().time == b.status().time
+    assert np.array_equal(a.get(abi.CVAR), b.get(abi.CVAR))
+    assert np.array_equal(a.get(abi.PVAR), b.get(abi.PVAR))
 
 
 @pytest.mark.gpu
