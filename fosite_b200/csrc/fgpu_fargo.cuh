@@ -24,28 +24,47 @@ struct FargoWArgs {
 //   padded column i (the x-ghost columns come from the boundary fill).
 // pvar is the primitive state of the last ComputeRHS after its
 // SubtractBackgroundVelocityY and this routine's AddBackgroundVelocityY, i.e.
-// (vy - w_prev) + w_prev.  One thread per column; the sum runs in j order like
-// the reference loop so the result is bitwise reproducible.
-__global__ void __launch_bounds__(128) fargo_w_kernel(const __grid_constant__ FargoWArgs A) {
+// (vy - w_prev) + w_prev.  The sum runs in j order like the reference loop, so
+// the result is bitwise reproducible: a block owns WX columns; per chunk of WR
+// rows its threads evaluate the WR x WX terms in parallel into shared memory,
+// then one thread per column adds them in order.
+constexpr int FW_WX = 8, FW_WY = 32, FW_RPT = 4, FW_WR = FW_WY * FW_RPT;
+__global__ void __launch_bounds__(FW_WX* FW_WY) fargo_w_kernel(const __grid_constant__ FargoWArgs A) {
   using CE = Cells<2, false>;
+  __shared__ double terms[FW_WR][FW_WX + 1];
   if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
-  const int ip = blockIdx.x * blockDim.x + threadIdx.x;
   const Grid& g = A.g;
-  if (ip >= g.nx + 4) return;
+  const int tx = threadIdx.x % FW_WX, ty = threadIdx.x / FW_WX;
+  const int ip = blockIdx.x * FW_WX + tx;
+  const bool valid = ip < g.nx + 4;
   const int i = ip - 2;
   const bool ghost = i < 0 || i >= g.nx;
-  const double wf = A.wfac[ip];
-  const double wp = A.w_prev ? A.w_prev[ip] : 0.0;
+  const double wf = valid ? A.wfac[ip] : 0.0;
+  const double wp = (valid && A.w_prev) ? A.w_prev[ip] : 0.0;
   double wi = 0.0;
-  for (int j = 0; j < g.ny; ++j) {
-    double p[3];
-    if (ghost) CE::face_ghost_p(A.in, g, A.ph, A.mt, 0, i, j, 0, p);
-    else CE::interior_p(A.in, g, A.ph, i, j, 0, p);
-    double vy = p[2];
-    if (A.w_prev) vy = (vy - wp) + wp;
-    wi = wi + vy * wf;
+  for (int j0 = 0; j0 < g.ny; j0 += FW_WR) {
+#pragma unroll
+    for (int r = 0; r < FW_RPT; ++r) {
+      const int q = ty + FW_WY * r, j = j0 + q;
+      double t = 0.0;
+      if (valid && j < g.ny) {
+        double p[3];
+        if (ghost) CE::face_ghost_p(A.in, g, A.ph, A.mt, 0, i, j, 0, p);
+        else CE::interior_p(A.in, g, A.ph, i, j, 0, p);
+        double vy = p[2];
+        if (A.w_prev) vy = (vy - wp) + wp;
+        t = vy * wf;
+      }
+      terms[q][tx] = t;
+    }
+    __syncthreads();
+    if (ty == 0 && valid) {
+      const int nq = min(FW_WR, g.ny - j0);
+      for (int q = 0; q < nq; ++q) wi = wi + terms[q][tx];
+    }
+    __syncthreads();
   }
-  A.w_out[ip] = wi / (double)g.ny;
+  if (ty == 0 && valid) A.w_out[ip] = wi / (double)g.ny;
 }
 
 struct FargoAdvArgs {

@@ -529,8 +529,8 @@ int launch_fargo_w(fgpu_handle* h, const StateRef& in, const double* w_prev, dou
   F.w_out = w_out;
   F.ctl = h->d_ctl;
   return timed_launch(h, false, 0.0, [&] {
-    unsigned blocks = (unsigned)((h->g.nx + 4 + 127) / 128);
-    fargo_w_kernel<<<blocks, 128, 0, h->stream>>>(F);
+    unsigned blocks = (unsigned)((h->g.nx + 4 + FW_WX - 1) / FW_WX);
+    fargo_w_kernel<<<blocks, FW_WX * FW_WY, 0, h->stream>>>(F);
     CUDA_TRY(h, cudaGetLastError());
     return FGPU_OK;
   });
@@ -545,7 +545,7 @@ int launch_fargo_advect(fgpu_handle* h, const double* in, double* out, const dou
   X.out = out;
   X.ctl = h->d_ctl;
   X.checkdata = h->cfg.checkdata;
-  X.chunk = 16;
+  X.chunk = 8;
   return timed_launch(h, false, 0.0, [&] {
     constexpr int TX = 32, TY = 4;
     dim3 grid((h->g.nx + TX - 1) / TX, (h->g.ny + TY * X.chunk - 1) / (TY * X.chunk));
