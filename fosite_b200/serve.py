@@ -152,9 +152,10 @@ class Server:
         cl["members"] = keep
 
     def round(self):
-        """One scheduling round: admit, (re)batch, advance every class by chunk steps, retire."""
+        """One scheduling round: (re)batch and enqueue chunk steps of every class, admit
+        waiting requests while the GPU runs them (host-side set-up overlaps the
+        batched launches), then wait and retire finished requests."""
         from .sim import Batch
-        self._admit()
         active = []
         for key, cl in self.classes.items():
             if not cl["members"]:
@@ -171,6 +172,7 @@ class Server:
                 cl["dirty"] = False
             cl["batch"].enqueue(self.chunk)
             active.append(cl)
+        self._admit()
         for cl in active:
             cl["batch"].collect()
         for cl in active:
@@ -192,8 +194,9 @@ class Server:
             while i < len(pending) and pending[i].arrival <= t:
                 self.waiting.append(pending[i])
                 i += 1
-            n = self.round()
-            if n == 0 and not self.waiting and i < len(pending):
+            self.round()
+            running = any(cl["members"] for cl in self.classes.values())
+            if not running and not self.waiting and i < len(pending):
                 time.sleep(max(0.0, min(0.01, pending[i].arrival - self.now())))
         for cl in self.classes.values():
             if cl["batch"]:
