@@ -48,28 +48,29 @@ int bset_err(fgpu_batch* b, int code, const std::string& msg) {
   } while (0)
 
 template <class K>
-int persistent_grid(fgpu_batch* b, K kernel, int threads, int ntiles) {
+int persistent_grid(fgpu_batch* b, K kernel, int threads, size_t smem, int ntiles) {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
     per_sm = 1;
   return std::max(1, std::min(ntiles, per_sm * b->sms));
 }
 
+template <int ND, bool EU, bool PRIM, int MINB>
+void launch_batched_layout(fgpu_batch* b, const StageArgs* args) {
+  constexpr int TY = TileShapes<ND>::TY;
+  constexpr int T = 32 * TY;
+  constexpr size_t SM = TileLayout<ND, EU, PRIM, 32, TY, MINB>::SMEM;
+  auto k = batched_stage_kernel<ND, EU, PRIM, 32, TY, MINB>;
+  k<<<persistent_grid(b, k, T, SM, b->ntiles), T, SM, b->stream>>>(args, b->d_tiles, b->ntiles);
+}
+
+// batches keep the base tile height (their tile queue is built for it): layouts 0, 2, 3
 template <int ND, bool EU, bool PRIM>
 int launch_batched_stage_t(fgpu_batch* b, const StageArgs* args, int variant) {
-  constexpr int TY = ND == 2 ? 8 : 4;
-  constexpr int T = 32 * TY;
-  constexpr int M2 = ND == 2 ? 2 : 4, M3 = ND == 2 ? 3 : 6;
-  if (variant == 2) {
-    auto k = batched_stage_kernel<ND, EU, PRIM, 32, TY, M2>;
-    k<<<persistent_grid(b, k, T, b->ntiles), T, 0, b->stream>>>(args, b->d_tiles, b->ntiles);
-  } else if (variant == 3) {
-    auto k = batched_stage_kernel<ND, EU, PRIM, 32, TY, M3>;
-    k<<<persistent_grid(b, k, T, b->ntiles), T, 0, b->stream>>>(args, b->d_tiles, b->ntiles);
-  } else {
-    auto k = batched_stage_kernel<ND, EU, PRIM, 32, TY, 1>;
-    k<<<persistent_grid(b, k, T, b->ntiles), T, 0, b->stream>>>(args, b->d_tiles, b->ntiles);
-  }
+  using S = TileShapes<ND>;
+  if (variant == 2) launch_batched_layout<ND, EU, PRIM, S::M2>(b, args);
+  else if (variant == 3) launch_batched_layout<ND, EU, PRIM, S::M3>(b, args);
+  else launch_batched_layout<ND, EU, PRIM, 1>(b, args);
   BCUDA_TRY(b, cudaGetLastError());
   return FGPU_OK;
 }
@@ -169,7 +170,7 @@ int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
   cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, h0->device);
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
     return fail(FGPU_ECUDA, "stream");
-  b->variant = h0->variant == 1 ? 0 : h0->variant;
+  b->variant = (h0->variant == 1 || h0->variant == 4) ? 0 : h0->variant;
   // argument tables: step stages of every member, then the tuner's RHS probes
   std::vector<StageArgs> args((size_t)(b->order + 1) * n);
   std::vector<BndArgs> bnd(n);
@@ -326,7 +327,7 @@ int fgpu_autotune(fgpu_handle* h, int reps, int* variant) {
   A.out_mode = OUT_RHS;
   A.out = scratch;
   A.ctl = nullptr;
-  const int cand[4] = {0, 2, 3, 1};
+  const int cand[5] = {0, 2, 3, 4, 1};
   double best = 1e300;
   int bv = h->variant, keep = h->variant;
   for (int v : cand) {

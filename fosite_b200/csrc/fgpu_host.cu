@@ -147,7 +147,7 @@ struct fgpu_handle {
   // launch shape
   int tile_x = 32, tile_y = 8, kchunk = 16;
   int variant = 0;              // stage kernel layout: 0 shared-memory tile, 1 warp-shuffle window,
-                                // 2/3 tile with a register cap for more resident blocks
+                                // 2/3 tile with a register cap for more resident blocks, 4 taller tile
   // instrumentation
   cudaStream_t own_stream = nullptr;
   bool profiling = false;
@@ -300,28 +300,69 @@ int upload_metric(fgpu_handle* h) {
 }
 
 // ---------------------------------------------------------------- launchers
+// A shared-memory tile layout of the stage kernel: TX x TY cells per block,
+// MINB resident blocks per SM requested from the register allocator.
+template <int ND, bool EU, bool PRIM, int TX, int TY, int MINB>
+struct TileLayout {
+  static constexpr size_t SMEM = stage_smem_bytes<Phys<ND, EU>::V, TX, TY>();
+  // the tiles use more than the default 48 KB of dynamic shared memory: opt in (per device)
+  static void configure(bool batched) {
+    cudaFuncSetAttribute(stage_kernel<ND, EU, PRIM, TX, TY, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)SMEM);
+    if (batched)
+      cudaFuncSetAttribute(batched_stage_kernel<ND, EU, PRIM, TX, TY, MINB>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+  }
+  static void launch(const Grid& g, int kchunk, cudaStream_t s, const StageArgs& A) {
+    const int kz = ND == 3 ? (g.nz + kchunk - 1) / kchunk : 1;
+    dim3 grid((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, kz);
+    stage_kernel<ND, EU, PRIM, TX, TY, MINB><<<grid, TX * TY, SMEM, s>>>(A);
+  }
+};
+// Layouts by variant id: 0 the base tile (2D 32x8, 3D 32x4 marching in z), 2/3 the
+// base tile with a register cap for more resident blocks (2D 2/3, 3D 4/6 per SM),
+// 4 a taller tile (2D 32x16, 3D 32x8 with 2 blocks per SM) that halves the y halo;
+// 1 is the warp-shuffle kernel of fgpu_stage2.cuh.
+template <int ND> struct TileShapes;
+template <> struct TileShapes<2> { static constexpr int TY = 8, M2 = 2, M3 = 3, TY4 = 16, M4 = 1; };
+template <> struct TileShapes<3> { static constexpr int TY = 4, M2 = 4, M3 = 6, TY4 = 8, M4 = 2; };
+
+template <int ND, bool EU, bool PRIM>
+void configure_stage_kernels_t() {
+  using S = TileShapes<ND>;
+  TileLayout<ND, EU, PRIM, 32, S::TY, 1>::configure(true);
+  TileLayout<ND, EU, PRIM, 32, S::TY, S::M2>::configure(true);
+  TileLayout<ND, EU, PRIM, 32, S::TY, S::M3>::configure(true);
+  TileLayout<ND, EU, PRIM, 32, S::TY4, S::M4>::configure(false);
+}
+void configure_stage_kernels(int nd, bool e, bool p) {
+  if (nd == 2) {
+    if (e) p ? configure_stage_kernels_t<2, true, true>() : configure_stage_kernels_t<2, true, false>();
+    else p ? configure_stage_kernels_t<2, false, true>() : configure_stage_kernels_t<2, false, false>();
+  } else {
+    if (e) p ? configure_stage_kernels_t<3, true, true>() : configure_stage_kernels_t<3, true, false>();
+    else p ? configure_stage_kernels_t<3, false, true>() : configure_stage_kernels_t<3, false, false>();
+  }
+}
+
 template <int ND, bool EU, bool PRIM>
 int launch_stage_t(fgpu_handle* h, StageArgs& A) {
+  using S = TileShapes<ND>;
   A.kchunk = h->kchunk;
   const Grid& g = h->g;
   const int kz = ND == 3 ? (g.nz + h->kchunk - 1) / h->kchunk : 1;
-  if (h->variant == 1) {
-    // warp-shuffle layout: 32 x 8 points per block, 30 x 6 output cells
-    constexpr int NW = 8;
-    dim3 grid((g.nx + 29) / 30, (g.ny + NW - 3) / (NW - 2), kz);
-    stage2_kernel<ND, EU, PRIM, NW><<<grid, 32 * NW, 0, h->stream>>>(A);
-  } else if constexpr (ND == 2) {
-    // shared-memory tile 32 x 8; variants 2/3 cap registers for 2/3 resident blocks per SM
-    dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, 1);
-    if (h->variant == 2) stage_kernel<ND, EU, PRIM, 32, 8, 2><<<grid, 256, 0, h->stream>>>(A);
-    else if (h->variant == 3) stage_kernel<ND, EU, PRIM, 32, 8, 3><<<grid, 256, 0, h->stream>>>(A);
-    else stage_kernel<ND, EU, PRIM, 32, 8><<<grid, 256, 0, h->stream>>>(A);
-  } else {
-    // shared-memory tile 32 x 4 marching in z; variants 2/3 cap registers for 4/6 resident blocks per SM
-    dim3 grid((g.nx + 31) / 32, (g.ny + 3) / 4, kz);
-    if (h->variant == 2) stage_kernel<ND, EU, PRIM, 32, 4, 4><<<grid, 128, 0, h->stream>>>(A);
-    else if (h->variant == 3) stage_kernel<ND, EU, PRIM, 32, 4, 6><<<grid, 128, 0, h->stream>>>(A);
-    else stage_kernel<ND, EU, PRIM, 32, 4><<<grid, 128, 0, h->stream>>>(A);
+  switch (h->variant) {
+    case 1: {
+      // warp-shuffle layout: 32 x 8 points per block, 30 x 6 output cells
+      constexpr int NW = 8;
+      dim3 grid((g.nx + 29) / 30, (g.ny + NW - 3) / (NW - 2), kz);
+      stage2_kernel<ND, EU, PRIM, NW><<<grid, 32 * NW, 0, h->stream>>>(A);
+      break;
+    }
+    case 2: TileLayout<ND, EU, PRIM, 32, S::TY, S::M2>::launch(g, h->kchunk, h->stream, A); break;
+    case 3: TileLayout<ND, EU, PRIM, 32, S::TY, S::M3>::launch(g, h->kchunk, h->stream, A); break;
+    case 4: TileLayout<ND, EU, PRIM, 32, S::TY4, S::M4>::launch(g, h->kchunk, h->stream, A); break;
+    default: TileLayout<ND, EU, PRIM, 32, S::TY, 1>::launch(g, h->kchunk, h->stream, A); break;
   }
   CUDA_TRY(h, cudaGetLastError());
   return FGPU_OK;
@@ -884,9 +925,10 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
   }
   if (!rc) {
     // FGPU_STAGE_VARIANT / FGPU_KCHUNK force a stage-kernel layout and z chunk (the tuner's choice otherwise)
-    if (const char* e = std::getenv("FGPU_STAGE_VARIANT")) h->variant = std::max(0, std::min(3, std::atoi(e)));
+    if (const char* e = std::getenv("FGPU_STAGE_VARIANT")) h->variant = std::max(0, std::min(4, std::atoi(e)));
     if (const char* e = std::getenv("FGPU_KCHUNK")) { int v = std::atoi(e); if (v > 0) h->kchunk = v; }
   }
+  if (!rc) configure_stage_kernels(h->nd, h->euler, h->prim);
   if (!rc) rc = build_metric(h);
   if (!rc) {
     h->g.nx = cfg->inum; h->g.ny = cfg->jnum; h->g.nz = h->nd == 3 ? cfg->knum : 1;

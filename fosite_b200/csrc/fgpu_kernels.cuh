@@ -91,6 +91,15 @@ __device__ __forceinline__ void block_reduce_emit(double* vals, int nv, int flag
   }
 }
 
+// Shared memory of one stage tile (dynamic): reconstruction variables with the
+// cross halo, x and y slopes, x and y interface fluxes.
+template <int V, int TX, int TY>
+constexpr size_t stage_smem_bytes() {
+  return sizeof(double) * (size_t)V *
+         ((size_t)(TY + 4) * (TX + 4) + (size_t)TY * (TX + 2) + (size_t)(TY + 2) * TX + (size_t)TY * (TX + 1) +
+          (size_t)(TY + 1) * TX);
+}
+
 // One TX x TY tile (bx, by) of one grid, z chunk bz.  Shared by the single-grid
 // kernel (arguments in the parameter space) and the batched kernel (per-grid
 // arguments in global memory, tiles from a flattened queue).
@@ -101,11 +110,13 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
   constexpr int V = PH::V;
   constexpr int NT = TX * TY;
   constexpr int RW = TX + 4, RH = TY + 4;
-  constexpr int SW = TX + 2, SH = TY + 2;
-  constexpr int FW = TX + 1, FH = TY + 1;
-  __shared__ double Rs[V * RH * RW];
-  __shared__ double Ss[V * SH * SW];
-  __shared__ double Fs[V * FH * FW];
+  // dynamic shared memory, stage_smem_bytes<V, TX, TY>() bytes
+  extern __shared__ __align__(16) double stage_smem[];
+  double* const Rs = stage_smem;                    // [V][TY+4][TX+4]
+  double* const Sx = Rs + V * RH * RW;              // [V][TY][TX+2]   x slopes
+  double* const Sy = Sx + V * TY * (TX + 2);        // [V][TY+2][TX]   y slopes
+  double* const Fx = Sy + V * (TY + 2) * TX;        // [V][TY][TX+1]   x fluxes
+  double* const Fy = Fx + V * TY * (TX + 1);        // [V][TY+1][TX]   y fluxes
   __shared__ double sred[4 * ((NT + 31) / 32)];
 
   if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
@@ -125,8 +136,10 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
   if (ND == 3) { k0 = bz * A.kchunk; k1 = min(g.nz, k0 + A.kchunk); }
 
   auto RS = [&](int v, int ly, int lx) -> double& { return Rs[(v * RH + ly) * RW + lx]; };
-  auto SS = [&](int v, int r, int c) -> double& { return Ss[(v * SH + r) * SW + c]; };
-  auto FS = [&](int v, int r, int c) -> double& { return Fs[(v * FH + r) * FW + c]; };
+  auto SX = [&](int v, int r, int c) -> double& { return Sx[(v * TY + r) * (TX + 2) + c]; };
+  auto SY = [&](int v, int r, int c) -> double& { return Sy[(v * (TY + 2) + r) * TX + c]; };
+  auto FX = [&](int v, int r, int c) -> double& { return Fx[(v * TY + r) * (TX + 1) + c]; };
+  auto FY = [&](int v, int r, int c) -> double& { return Fy[(v * (TY + 1) + r) * TX + c]; };
 
   // reconstruction variables at a cross point (interior or face ghost)
   auto recon_at = [&](int gi, int gj, int gk, double* R) {
@@ -256,70 +269,70 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
     __syncthreads();
 
     double divX[V], divY[V];
-    // ---- x direction: slopes, interface fluxes, divergence
+    // ---- slopes of both directions in one phase (x: ey rows x ex+2 cells, y: ey+2 rows x ex cells)
+    const int nsx = (ex + 2) * ey, nsy = ex * (ey + 2);
     if (!A.constant_recon) {
-      for (int t = tid; t < (ex + 2) * ey; t += NT) {
-        int r = t / (ex + 2), c = t % (ex + 2) - 1;
+      for (int t = tid; t < nsx + nsy; t += NT) {
+        if (t < nsx) {
+          int r = t / (ex + 2), c = t % (ex + 2) - 1;
 #pragma unroll
-        for (int v = 0; v < V; ++v)
-          SS(v, r, c + 1) = slope(A.limiter, A.theta, A.invd[0], RS(v, r + 2, c + 1), RS(v, r + 2, c + 2), RS(v, r + 2, c + 3));
+          for (int v = 0; v < V; ++v)
+            SX(v, r, c + 1) = slope(A.limiter, A.theta, A.invd[0], RS(v, r + 2, c + 1), RS(v, r + 2, c + 2), RS(v, r + 2, c + 3));
+        } else {
+          int u = t - nsx;
+          int c = u % ex, r = u / ex - 1;
+#pragma unroll
+          for (int v = 0; v < V; ++v)
+            SY(v, r + 1, c) = slope(A.limiter, A.theta, A.invd[1], RS(v, r + 1, c + 2), RS(v, r + 2, c + 2), RS(v, r + 3, c + 2));
+        }
       }
       __syncthreads();
     }
-    for (int t = tid; t < (ex + 1) * ey; t += NT) {
-      int r = t / (ex + 1), f = t % (ex + 1);
-      int gl = i0 + f - 1 + 2;   // padded i of the left cell
+    // ---- interface fluxes of both directions in one phase
+    const int nfx = (ex + 1) * ey, nfy = ex * (ey + 1);
+    for (int t = tid; t < nfx + nfy; t += NT) {
       double RL[V], RR[V], F[V];
-      double oE = M.offxE[gl], oW = M.offxW[gl + 1];
+      if (t < nfx) {
+        int r = t / (ex + 1), f = t % (ex + 1);
+        int gl = i0 + f - 1 + 2;   // padded i of the left cell
+        double oE = M.offxE[gl], oW = M.offxW[gl + 1];
 #pragma unroll
-      for (int v = 0; v < V; ++v) {
-        RL[v] = A.constant_recon ? RS(v, r + 2, f + 1) : RS(v, r + 2, f + 1) + SS(v, r, f) * oE;
-        RR[v] = A.constant_recon ? RS(v, r + 2, f + 2) : RS(v, r + 2, f + 2) + SS(v, r, f + 1) * oW;
+        for (int v = 0; v < V; ++v) {
+          RL[v] = A.constant_recon ? RS(v, r + 2, f + 1) : RS(v, r + 2, f + 1) + SX(v, r, f) * oE;
+          RR[v] = A.constant_recon ? RS(v, r + 2, f + 2) : RS(v, r + 2, f + 2) + SX(v, r, f + 1) * oW;
+        }
+        kt_flux<ND, EU, PRIM>(0, RL, RR, EU ? 0.0 : M.cs[2 * M.nxp + gl], EU ? 0.0 : M.cs[1 * M.nxp + gl + 1],
+                              M.dAxW[gl + 1], P, F);
+#pragma unroll
+        for (int v = 0; v < V; ++v) FX(v, r, f) = F[v];
+      } else {
+        int u = t - nfx;
+        int c = u % ex, f = u / ex;
+        int gjl = j0 + f - 1 + 2;     // padded j of the lower cell
+        int gi = i0 + c + 2;          // padded i of the column
+        double oN = M.offyN[gjl], oS = M.offyS[gjl + 1];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          RL[v] = A.constant_recon ? RS(v, f + 1, c + 2) : RS(v, f + 1, c + 2) + SY(v, f, c) * oN;
+          RR[v] = A.constant_recon ? RS(v, f + 2, c + 2) : RS(v, f + 2, c + 2) + SY(v, f + 1, c) * oS;
+        }
+        kt_flux<ND, EU, PRIM>(1, RL, RR, EU ? 0.0 : M.cs[4 * M.nxp + gi], EU ? 0.0 : M.cs[3 * M.nxp + gi],
+                              M.dAyS[gi], P, F);
+#pragma unroll
+        for (int v = 0; v < V; ++v) FY(v, f, c) = F[v];
       }
-      kt_flux<ND, EU, PRIM>(0, RL, RR, EU ? 0.0 : M.cs[2 * M.nxp + gl], EU ? 0.0 : M.cs[1 * M.nxp + gl + 1],
-                            M.dAxW[gl + 1], P, F);
-#pragma unroll
-      for (int v = 0; v < V; ++v) FS(v, r, f) = F[v];
-    }
-    __syncthreads();
-    if (own) {
-      double dV = M.dydzdV[ip];
-#pragma unroll
-      for (int v = 0; v < V; ++v) divX[v] = dV * (FS(v, ty, tx + 1) - FS(v, ty, tx));
-    }
-    __syncthreads();
-    // ---- y direction
-    if (!A.constant_recon) {
-      for (int t = tid; t < ex * (ey + 2); t += NT) {
-        int c = t % ex, r = t / ex - 1;
-#pragma unroll
-        for (int v = 0; v < V; ++v)
-          SS(v, r + 1, c) = slope(A.limiter, A.theta, A.invd[1], RS(v, r + 1, c + 2), RS(v, r + 2, c + 2), RS(v, r + 3, c + 2));
-      }
-      __syncthreads();
-    }
-    for (int t = tid; t < ex * (ey + 1); t += NT) {
-      int c = t % ex, f = t / ex;
-      int gjl = j0 + f - 1 + 2;     // padded j of the lower cell
-      int gi = i0 + c + 2;          // padded i of the column
-      double RL[V], RR[V], F[V];
-      double oN = M.offyN[gjl], oS = M.offyS[gjl + 1];
-#pragma unroll
-      for (int v = 0; v < V; ++v) {
-        RL[v] = A.constant_recon ? RS(v, f + 1, c + 2) : RS(v, f + 1, c + 2) + SS(v, f, c) * oN;
-        RR[v] = A.constant_recon ? RS(v, f + 2, c + 2) : RS(v, f + 2, c + 2) + SS(v, f + 1, c) * oS;
-      }
-      kt_flux<ND, EU, PRIM>(1, RL, RR, EU ? 0.0 : M.cs[4 * M.nxp + gi], EU ? 0.0 : M.cs[3 * M.nxp + gi],
-                            M.dAyS[gi], P, F);
-#pragma unroll
-      for (int v = 0; v < V; ++v) FS(v, f, c) = F[v];
     }
     __syncthreads();
 
     if (own) {
+      {
+        double dV = M.dydzdV[ip];
+#pragma unroll
+        for (int v = 0; v < V; ++v) divX[v] = dV * (FX(v, ty, tx + 1) - FX(v, ty, tx));
+      }
       double dV = M.dzdxdV[ip];
 #pragma unroll
-      for (int v = 0; v < V; ++v) divY[v] = dV * (FS(v, ty + 1, tx) - FS(v, ty, tx));
+      for (int v = 0; v < V; ++v) divY[v] = dV * (FY(v, ty + 1, tx) - FY(v, ty, tx));
       const long long idx = CE::lin(g, i, j, k);
       // centre primitive / conservative state as ComputeRHS sees it
       double pc[V], cc[V];
@@ -479,7 +492,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
         }
       }
     }
-    __syncthreads();
+    // no barrier between the planes of one tile: a thread writes only its own cell and the
+    // halo of the next plane, and every reader of this plane has passed the flux barrier
   }
 
   if (A.ctl && (A.cfl_mode || A.last_stage)) {
@@ -489,6 +503,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
     if (nv) block_reduce_emit<NT>(vals, nv, flags, A.last_stage && !A.cfl_mode ? &A.ctl->err : A.ctl->invdt,
                                   &A.ctl->flags, sred);
   }
+  // the next tile of a persistent block may place its halo where this tile had cells
+  __syncthreads();
 }
 
 template <int ND, bool EU, bool PRIM, int TX, int TY, int MINB = 1>
