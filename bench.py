@@ -294,7 +294,9 @@ def run_own(args, world, rank, local):
         "achieved_gbps_step": value / world * bpc / 1e9,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "kernel": "stage_kernel (fused RHS + stage update)",
+                     "kernel": "RHS stage: stage_kernel (fused RHS + stage update), for Butcher stages with "
+                               "the form_kernel pass that forms its input state",
+                     "form_ms_per_launch": st.form_ms / max(1, st.stage_launches),
                      "peak_kind": peak_kind + " copy bandwidth (burst)",
                      "algorithmic_bytes_per_launch": st.stage_bytes / max(1, st.stage_launches),
                      "launch_ms_avg": st.stage_ms / max(1, st.stage_launches)},

@@ -74,7 +74,7 @@ class Stats(C.Structure):
     _fields_ = [
         ("launches", C.c_int64), ("stage_launches", C.c_int64), ("attempts", C.c_int64),
         ("cell_updates", C.c_int64), ("stage_ms", C.c_double), ("stage_bytes", C.c_double),
-        ("other_ms", C.c_double),
+        ("other_ms", C.c_double), ("form_ms", C.c_double),
     ]
 
 

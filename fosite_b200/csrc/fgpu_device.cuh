@@ -70,6 +70,8 @@ struct StateRef {
   // FARGO (2D isothermal): frame changes applied to the state before the
   // boundary fill, i.e. the real-frame cvar that CenterBoundary sees
   Chain pre;
+  // 1: base holds primitive variables already formed from a stage state (nk = 0)
+  int ready;
 };
 
 // apply a frame-change chain to the conservative state c of a cell in padded column ip
@@ -137,9 +139,18 @@ struct Phys {
 #endif
     }
   }
-  // GetSoundSpeed (physics_euler.f90:2682-2689)
+  // GetSoundSpeed (physics_euler.f90:2682-2689): sqrt(MAX(2 TINY, gamma*p/rho)).
+  // The product build evaluates sqrt(s/rho) as s*rsqrt(s*rho) with s = gamma*p (one
+  // reciprocal square root instead of a division and a square root; within a few ulp).
   static __device__ __forceinline__ double cs_of(const double* p, const PhysP& P) {
+#ifdef FGPU_EXACT
     return sqrt(dmax(P.tiny2, P.gamma * p[V - 1] / p[0]));
+#else
+    const double s = P.gamma * p[V - 1];
+    const double q = s * p[0];
+    if (s > P.tiny2 * p[0] && q > 1e-300 && q < 1e300) return s * rsqrt(q);
+    return sqrt(dmax(P.tiny2, s / p[0]));
+#endif
   }
 };
 
@@ -147,9 +158,16 @@ struct Phys {
 // reconstruction_linear.f90:645-733; returns the limited difference (times invd by caller)
 __device__ __forceinline__ double limit2(int lim, double theta, double a1, double a2) {
   switch (lim) {
-    case LIM_MINMOD:
+    case LIM_MINMOD: {
+#ifdef FGPU_EXACT
       if (fsign1(a1) * fsign1(a2) > 0) return fsign(dmin(fabs(a1), fabs(a2)), a1);
       return 0.;
+#else
+      // the same value for non-zero differences (see MONOCENT in slope)
+      const double lo = dmin(a1, a2), hi = dmax(a1, a2);
+      return lo > 0. ? lo : (hi < 0. ? hi : 0.);
+#endif
+    }
     case LIM_SWEBY:
     case LIM_SUPERBEE: {
       double p = lim == LIM_SWEBY ? theta : 2.0;
@@ -173,9 +191,17 @@ __device__ __forceinline__ double limit2(int lim, double theta, double a1, doubl
 __device__ __forceinline__ double slope(int lim, double theta, double invd, double qm, double q0, double qp) {
   if (lim == LIM_MC) {
     double a1 = theta * (q0 - qm), a2 = theta * (qp - q0), a3 = 0.5 * (qp - qm);
+#ifdef FGPU_EXACT
     double r = 0.;
     if (((fsign1(a1) * fsign1(a2)) > 0) && ((fsign1(a2) * fsign1(a3)) > 0))
       r = fsign(dmin(dmin(fabs(a1), fabs(a2)), fabs(a3)), a1);
+#else
+    // same value as the sign-test form for all non-zero slopes: the smallest of three
+    // positive differences, the largest of three negative ones, else zero (the sign of
+    // a zero result may differ)
+    const double lo = dmin(dmin(a1, a2), a3), hi = dmax(dmax(a1, a2), a3);
+    const double r = lo > 0. ? lo : (hi < 0. ? hi : 0.);
+#endif
     return invd * r;
   }
   return invd * limit2(lim, theta, q0 - qm, qp - q0);
@@ -216,6 +242,11 @@ struct Cells {
                                                     int i, int j, int k, double* p) {
     double u[V];
     state_at<V>(S, g.n, lin(g, i, j, k), u);
+    if (S.ready) {
+#pragma unroll
+      for (int l = 0; l < V; ++l) p[l] = u[l];
+      return;
+    }
     if (ND == 2 && !EU && S.pre.n) apply_chain(S.pre, u, i + 2);
     PH::c2p(u, p, P);
   }

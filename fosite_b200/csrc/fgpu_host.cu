@@ -146,6 +146,8 @@ struct fgpu_handle {
   int graph_steps = 0;
   // launch shape
   int tile_x = 32, tile_y = 8, kchunk = 16;
+  bool materialize = true;      // Butcher stages: form the stage's reconstruction variables once per cell
+  double* d_ready = nullptr;    // ... into this array (one state)
   int variant = 0;              // stage kernel layout: 0 shared-memory tile, 1 warp-shuffle window,
                                 // 2/3 tile with a register cap for more resident blocks, 4 taller tile
   // instrumentation
@@ -410,13 +412,14 @@ double stage_bytes(const fgpu_handle* h, const StageArgs& A) {
 }
 
 template <class F>
-int timed_launch(fgpu_handle* h, bool stage, double bytes, F&& fn) {
+// kind: 0 boundary/reduction/transfer kernels, 1 stage kernel, 2 stage-state formation
+int timed_launch(fgpu_handle* h, int kind, double bytes, F&& fn) {
   h->stats.launches += 1;
-  if (stage) h->stats.stage_launches += 1;
+  if (kind == 1) h->stats.stage_launches += 1;
   if (!h->profiling) return fn();
   fgpu_handle::Timed t;
   t.bytes = bytes;
-  t.stage = stage ? 1 : 0;
+  t.stage = kind;
   CUDA_TRY(h, cudaEventCreate(&t.a));
   CUDA_TRY(h, cudaEventCreate(&t.b));
   CUDA_TRY(h, cudaEventRecord(t.a, h->stream));
@@ -431,6 +434,19 @@ int launch_stage(fgpu_handle* h, StageArgs& A) {
 }
 int launch_misc(fgpu_handle* h, int which, BndArgs& B) {
   return timed_launch(h, false, 0.0, [&] { return launch_misc_raw(h, which, B); });
+}
+
+template <int ND, bool EU>
+void launch_form_t(fgpu_handle* h, const StateRef& S, double* out, unsigned blocks) {
+  if (h->prim) form_kernel<ND, EU, true><<<blocks, 256, 0, h->stream>>>(S, h->g, h->ph, out);
+  else form_kernel<ND, EU, false><<<blocks, 256, 0, h->stream>>>(S, h->g, h->ph, out);
+}
+int launch_form(fgpu_handle* h, const StateRef& S, double* out) {
+  unsigned blocks = (unsigned)std::min<long long>((h->g.n + 255) / 256, 148 * 8);
+  if (h->nd == 2) h->euler ? launch_form_t<2, true>(h, S, out, blocks) : launch_form_t<2, false>(h, S, out, blocks);
+  else h->euler ? launch_form_t<3, true>(h, S, out, blocks) : launch_form_t<3, false>(h, S, out, blocks);
+  CUDA_TRY(h, cudaGetLastError());
+  return FGPU_OK;
 }
 
 int launch_roundtrip(fgpu_handle* h, const double* in, double* out) {
@@ -732,6 +748,14 @@ int butcher_attempt(fgpu_handle* h, double dtv, double& err) {
       A.in.K[q] = h->buf[2 + q];
       A.in.coef[q] = T.A[(m - 1) * T.m + q] * dtv;
     }
+    if (h->materialize) {
+      // the stage state's reconstruction variables once per cell, read by the stencil
+      double* R = h->buf[2 + T.m];
+      StateRef S = A.in;
+      if (int rc = timed_launch(h, 2, 0.0, [&] { return launch_form(h, S, R); })) return rc;
+      A.rin = plain_state(R, false);
+      A.rin.ready = h->prim ? 1 : 0;
+    }
     A.out_mode = OUT_RHS;
     A.out = h->buf[2 + m - 1];
     if (m == T.m) {
@@ -927,6 +951,7 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
     // FGPU_STAGE_VARIANT / FGPU_KCHUNK force a stage-kernel layout and z chunk (the tuner's choice otherwise)
     if (const char* e = std::getenv("FGPU_STAGE_VARIANT")) h->variant = std::max(0, std::min(4, std::atoi(e)));
     if (const char* e = std::getenv("FGPU_KCHUNK")) { int v = std::atoi(e); if (v > 0) h->kchunk = v; }
+    if (const char* e = std::getenv("FGPU_MATERIALIZE")) h->materialize = std::atoi(e) != 0;
   }
   if (!rc) configure_stage_kernels(h->nd, h->euler, h->prim);
   if (!rc) rc = build_metric(h);
@@ -941,7 +966,7 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
   }
   if (!rc) rc = upload_metric(h);
   if (!rc) {
-    int nbuf = h->butcher ? 2 + h->T.m : 3;
+    int nbuf = h->butcher ? 2 + h->T.m + 1 : 3;   // Butcher: P, base, k1..km, formed stage state
     size_t bytes = sizeof(double) * h->V * h->g.n;
     for (int b = 0; b < nbuf && !rc; ++b) {
       double* p = nullptr;
@@ -1342,6 +1367,7 @@ int fgpu_get_stats(fgpu_handle* h, fgpu_stats* st) {
       CUDA_TRY(h, cudaEventElapsedTime(&ms, t.a, t.b));
       if (t.stage) { h->stats.stage_ms += ms; h->stats.stage_bytes += t.bytes; }
       else h->stats.other_ms += ms;
+      if (t.stage == 2) h->stats.form_ms += ms;
       cudaEventDestroy(t.a);
       cudaEventDestroy(t.b);
     }

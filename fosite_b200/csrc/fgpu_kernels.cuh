@@ -57,6 +57,11 @@ struct StageArgs {
   // sources) and the Shu-Osher base states as chains of frame changes of the stored states
   const double* w_sub;
   Chain yn_chain, y0_chain;
+  // optional: the stage's reconstruction variables formed once per cell by form_kernel
+  // (rin.ready = 1 for primitive reconstruction); the stencil then reads these instead of
+  // forming base - sum coef*K and converting at every stencil point.  in stays the
+  // stage state for the epilogues.
+  StateRef rin;
 };
 
 // block-wide max of up to 3 non-negative doubles + OR of flags, then one atomic per block
@@ -142,12 +147,18 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
   auto FY = [&](int v, int r, int c) -> double& { return Fy[(v * (TY + 1) + r) * TX + c]; };
 
   // reconstruction variables at a cross point (interior or face ghost)
+  const StateRef& SR = A.rin.base ? A.rin : A.in;
   auto recon_at = [&](int gi, int gj, int gk, double* R) {
     double p[V];
     bool inx = gi >= 0 && gi < g.nx, iny = gj >= 0 && gj < g.ny, inz = gk >= 0 && gk < g.nz;
     if (inx && iny && inz) {
       double u[V];
-      state_at<V>(A.in, g.n, CE::lin(g, gi, gj, gk), u);
+      state_at<V>(SR, g.n, CE::lin(g, gi, gj, gk), u);
+      if (PRIM && SR.ready) {
+#pragma unroll
+        for (int l = 0; l < V; ++l) R[l] = u[l];
+        return;
+      }
       if (FG && A.in.pre.n) apply_chain(A.in.pre, u, gi + 2);
       if (PRIM) {
         PH::c2p(u, p, P);
@@ -166,7 +177,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
       }
     } else {
       int d = !inx ? 0 : (!iny ? 1 : 2);
-      CE::face_ghost_p(A.in, g, P, M, d, gi, gj, gk, p);
+      CE::face_ghost_p(SR, g, P, M, d, gi, gj, gk, p);
       if (roundtrip) p[V - 1] = dmax(p[V - 1], P.pmin);
       if (PRIM) {
         if (FG && A.w_sub) p[2] = p[2] - A.w_sub[gi + 2];

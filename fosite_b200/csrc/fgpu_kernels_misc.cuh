@@ -240,6 +240,24 @@ __global__ void __launch_bounds__(256) unpack_kernel(const double* __restrict__ 
   }
 }
 
+// The reconstruction variables of a Butcher stage state, formed once per cell:
+// out = base - sum coef*K (the reference's accumulation order), converted with
+// Cons2Prim for primitive reconstruction.  Values are identical to what the
+// stage kernel forms at every stencil point.
+template <int ND, bool EU, bool PRIM>
+__global__ void __launch_bounds__(256) form_kernel(const __grid_constant__ StateRef in, Grid g, PhysP P,
+                                                   double* __restrict__ out) {
+  using PH = Phys<ND, EU>;
+  constexpr int V = PH::V;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < g.n; t += (long long)gridDim.x * blockDim.x) {
+    double u[V], p[V];
+    state_at<V>(in, g.n, t, u);
+    if (PRIM) PH::c2p(u, p, P);
+#pragma unroll
+    for (int v = 0; v < V; ++v) out[(long long)v * g.n + t] = PRIM ? p[v] : u[v];
+  }
+}
+
 // Apply the CHECK_PMIN round trip to a stored state: out = P2C(MAX(C2P(in),pmin)).
 template <int ND, bool EU>
 __global__ void __launch_bounds__(256) roundtrip_kernel(const double* __restrict__ in, double* __restrict__ out,

@@ -299,9 +299,11 @@ typedef struct fgpu_stats {
     int64_t stage_launches;   /* fused stage (RHS) kernels */
     int64_t attempts;         /* time-step attempts (accepted + rejected) */
     int64_t cell_updates;     /* interior cells x accepted steps */
-    double  stage_ms;         /* summed CUDA-event time of stage kernels (profiling on) */
-    double  stage_bytes;      /* algorithmic bytes of the timed stage kernels */
+    double  stage_ms;         /* summed CUDA-event time of the RHS stages (profiling on): stage
+                                 kernels plus the passes that form their input states */
+    double  stage_bytes;      /* algorithmic bytes of the timed stages */
     double  other_ms;         /* boundary / reduction kernels (profiling on) */
+    double  form_ms;          /* the stage-state formation part of stage_ms */
 } fgpu_stats;
 int fgpu_set_profiling(fgpu_handle* h, int on);
 int fgpu_get_stats(fgpu_handle* h, fgpu_stats* st);
