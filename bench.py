@@ -157,40 +157,24 @@ def cpu_baseline(name, budget_s=20.0):
 
 
 def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import torch.distributed as dist
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    return world, rank, local
+    from fosite_b200 import replicas
+    return replicas.init()
 
 
 def allmax(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from fosite_b200 import replicas
+    return replicas.allmax(x) if world > 1 else x
 
 
 def allsum(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    from fosite_b200 import replicas
+    return replicas.allsum(x) if world > 1 else x
 
 
 def barrier(world):
+    from fosite_b200 import replicas
     if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+        replicas.barrier()
 
 
 def run_reference(args, world, rank):
@@ -328,16 +312,22 @@ def ensemble_members(n=96, seed=4000):
     return out
 
 
-def run_ensemble(args):
-    """Batched ensemble against a loop of plain per-grid runs of the same members."""
-    from fosite_b200 import abi
+def run_ensemble(args, world=1, rank=0, local=0):
+    """Batched ensemble against a loop of plain per-grid runs of the same members.
+
+    With N ranks the members are dealt round-robin to the GPUs (no collective in the
+    step); the job time is the slowest rank's."""
+    import torch
+    from fosite_b200 import abi, replicas
     from fosite_b200.sim import Batch, Simulation
-    probs = ensemble_members(args.members)
+    torch.cuda.set_device(local)
+    all_probs = ensemble_members(args.members)
+    probs = replicas.partition(all_probs, rank, world)
 
     def make():
         sims = []
         for cfg, p, extra in probs:
-            s = Simulation(cfg)
+            s = Simulation(cfg, device=local)
             apply_extra(s, cfg, extra)
             s.set_state(abi.PVAR, p)
             s.first_step()
@@ -350,44 +340,75 @@ def run_ensemble(args):
     b.run(args.warmup)
     for s in plain:
         s.run(args.warmup)
-    clk = ClockSampler(0)
+    clk = ClockSampler(local)
     clk.start()
+    barrier(world)
     t0 = time.perf_counter()
-    b.run(args.steps)
+    b.run(args.steps)                      # returns after the device finished (status read back)
     t_batch = time.perf_counter() - t0
     clocks = clk.stop()
+    barrier(world)
     t0 = time.perf_counter()
     for s in plain:
         s.run(args.steps)
     t_plain = time.perf_counter() - t0
     same = all(np.array_equal(m.get(abi.CVAR), s.get(abi.CVAR)) for m, s in zip(members, plain))
-    value = cells * args.steps / t_batch
-    line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": 1,
+    value, cells_all, ms_batch = replicas.job_throughput(cells * args.steps, 1e3 * t_batch) if world > 1 else \
+        (cells * args.steps / t_batch, cells * args.steps, 1e3 * t_batch)
+    t_batch = ms_batch * 1e-3
+    t_plain = allmax(t_plain, world)
+    same = allsum(0.0 if same else 1.0, world) == 0.0
+    members_all = len(all_probs)
+    cells = int(allsum(cells, world))
+    if rank != 0:
+        b.close()
+        return
+    line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_batch / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)",
-            "config": {"workload": "ensemble", "description": ENSEMBLE_DESC, "members": len(probs),
-                       "cells": cells, "tiles": b.tiles, "variant": variant},
-            "member_steps_per_s": len(probs) * args.steps / t_batch,
+            "config": {"workload": "ensemble", "description": ENSEMBLE_DESC, "members": members_all,
+                       "cells": cells, "tiles_rank0": b.tiles, "variant": variant,
+                       "parallelism": "members dealt round-robin over %d GPU(s)" % world},
+            "member_steps_per_s": members_all * args.steps / t_batch,
             "plain_loop": {"value": cells * args.steps / t_plain, "ms_per_step": 1e3 * t_plain / args.steps},
             "speedup_vs_plain": t_plain / t_batch, "identical_to_plain": bool(same), "clocks": clocks}
     print(json.dumps(line), flush=True)
     b.close()
 
 
-def run_serve(args):
-    """Poisson request streams at swept rates through the continuous-batching server."""
+def run_serve(args, world=1, rank=0, local=0):
+    """Poisson request streams at swept rates through the continuous-batching server.
+
+    With N ranks each GPU serves the requests dealt to it round-robin (the stream's
+    arrival times are kept); latencies are gathered on rank 0."""
+    from fosite_b200 import replicas
     from fosite_b200.serve import Server, poisson_stream
     import torch
+    torch.cuda.set_device(local)
     free, total = torch.cuda.mem_get_info()
     out = []
     for rate in [float(r) for r in args.rates.split(",")]:
-        reqs = poisson_stream(rate, args.requests, seed=int(rate), t_scale=args.t_scale)
-        srv = Server(hbm_budget_bytes=int(0.8 * free), chunk=args.chunk, autotune=False)
+        reqs = replicas.partition(poisson_stream(rate, args.requests, seed=int(rate), t_scale=args.t_scale), rank, world)
+        srv = Server(hbm_budget_bytes=int(0.8 * free), device=local, chunk=args.chunk, autotune=False)
+        barrier(world)
         rep = srv.serve(reqs, timeout_s=900)
+        if world > 1:
+            import torch.distributed as dist
+            lat = [r.finished - r.arrival for r in srv.done]
+            parts = [None] * world
+            dist.all_gather_object(parts, (lat, rep["cell_updates"], rep["makespan_s"]))
+            lat = np.array([x for p in parts for x in p[0]])
+            span = max(p[2] for p in parts)
+            cu = sum(p[1] for p in parts)
+            rep = {"requests": int(lat.size), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                   "mean_s": float(lat.mean()), "makespan_s": span, "cell_updates": int(cu),
+                   "cell_updates_per_s": cu / span if span > 0 else None}
         rep["rate_req_s"] = rate
         out.append(rep)
-    line = {"metric": "p50/p99 time-to-solution, cell-updates/s", "unit": "s", "n_gpus": 1,
+    if rank != 0:
+        return
+    line = {"metric": "p50/p99 time-to-solution, cell-updates/s", "unit": "s", "n_gpus": world,
             "higher_is_better": False, "dtype": "f64", "data": "synthetic (seeded Poisson streams)",
             "config": {"workload": "serve", "requests_per_rate": args.requests, "t_scale": args.t_scale,
                        "chunk_steps": args.chunk,
@@ -415,16 +436,16 @@ def main():
     world, rank, local = dist_setup()
     try:
         if args.workload in ("ensemble", "serve"):
-            if rank == 0:
-                run_ensemble(args) if args.workload == "ensemble" else run_serve(args)
+            fn = run_ensemble if args.workload == "ensemble" else run_serve
+            fn(args, world, rank, local)
         elif args.impl == "reference":
             run_reference(args, world, rank)
         else:
             run_own(args, world, rank, local)
     finally:
         if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+            from fosite_b200 import replicas
+            replicas.finalize()
 
 
 if __name__ == "__main__":
