@@ -55,6 +55,7 @@ class Config(C.Structure):
         ("pm_mass", C.c_double),
         ("fargo_method", C.c_int32), ("fargo_direction", C.c_int32),
         ("tout", C.c_double),
+        ("pm_outbound", C.c_int32), ("pad_", C.c_int32),
     ]
 
 

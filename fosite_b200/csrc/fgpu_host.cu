@@ -164,6 +164,11 @@ struct fgpu_handle {
   bool fargo = false;
   double* d_w = nullptr;
   int fargo_phase = 0;
+  // point-mass accretion: d_acc = [bx (ny) | bxold (ny) | brow (ny) | mass, mdot]
+  bool accrete = false;
+  int acc_face = 0;             // 0 west, 1 east
+  double* d_acc = nullptr;
+  double dxyz[3] = {1.0, 1.0, 1.0};
 };
 
 namespace {
@@ -202,6 +207,7 @@ int build_metric(fgpu_handle* h) {
   if (dy < 2 * DBL_EPSILON) { if (ny == 1) { dy = 1.0; mdy = 0.0; } else return set_err(h, FGPU_EBADCFG, "JNUM > 1 conflicts with zero y-extent"); }
   if (dz < 2 * DBL_EPSILON) { if (nz == 1) { dz = 1.0; mdz = 0.0; } else return set_err(h, FGPU_EBADCFG, "KNUM > 1 conflicts with zero z-extent"); }
   h->invd[0] = 1. / dx; h->invd[1] = 1. / dy; h->invd[2] = 1. / dz;
+  h->dxyz[0] = dx; h->dxyz[1] = dy; h->dxyz[2] = dz;
   int nxp = nx + 4, nyp = ny + 4, nzp = nz + 4;
   h->nxp = nxp;
   // layout: M_NI arrays of nxp, then offyS, offyN (nyp), offzB, offzT (nzp)
@@ -353,7 +359,9 @@ int launch_stage_t(fgpu_handle* h, StageArgs& A) {
   A.kchunk = h->kchunk;
   const Grid& g = h->g;
   const int kz = ND == 3 ? (g.nz + h->kchunk - 1) / h->kchunk : 1;
-  switch (h->variant) {
+  // the warp-shuffle layout implements neither FARGO frame changes nor the accretion rows
+  const int variant = (h->variant == 1 && (h->fargo || h->accrete)) ? 0 : h->variant;
+  switch (variant) {
     case 1: {
       // warp-shuffle layout: 32 x 8 points per block, 30 x 6 output cells
       constexpr int NW = 8;
@@ -487,6 +495,11 @@ StageArgs base_args(fgpu_handle* h) {
   A.ctl = h->d_ctl;
   A.tol_rel = h->tol_rel;
   for (int v = 0; v < FGPU_MAXV; ++v) A.tol_abs[v] = h->tol_abs[v];
+  if (h->accrete) {
+    A.brow = h->d_acc + 2 * (size_t)h->g.ny;
+    A.brow_face = h->acc_face;
+    A.bdydz = h->dxyz[1] * h->dxyz[2];
+  }
   return A;
 }
 
@@ -545,10 +558,35 @@ StageArgs shu_osher_stage(fgpu_handle* h, int n) {
   return A;
 }
 
+// accretion bookkeeping after Shu-Osher stage n (no-op without accretion)
+int launch_accrete(fgpu_handle* h, int n) {
+  if (!h->accrete) return FGPU_OK;
+  AccArgs C;
+  std::memset(&C, 0, sizeof(C));
+  const size_t ny = (size_t)h->g.ny;
+  C.bx = h->d_acc;
+  C.bxold = h->d_acc + ny;
+  C.brow = h->d_acc + 2 * ny;
+  C.grav = h->d_acc + 3 * ny;
+  C.ny = h->g.ny;
+  C.eta = kEta[h->order - 1][n - 1];
+  C.dt = &h->d_ctl->dt;
+  C.last = n == h->order ? 1 : 0;
+  C.accel = h->d_metric + (size_t)M_accel0 * h->nxp;   // accel0 and accel1 are adjacent
+  C.naccel = 2 * h->nxp;
+  C.ctl = h->d_ctl;
+  return timed_launch(h, 0, 0.0, [&] {
+    accrete_kernel<<<1, 256, 0, h->stream>>>(C);
+    CUDA_TRY(h, cudaGetLastError());
+    return FGPU_OK;
+  });
+}
+
 int enqueue_shu_osher_step(fgpu_handle* h) {
   for (int n = 1; n <= h->order; ++n) {
     StageArgs A = shu_osher_stage(h, n);
     if (int rc = launch_stage(h, A)) return rc;
+    if (int rc = launch_accrete(h, n)) return rc;
   }
   if (h->order == 1)
     CUDA_TRY(h, cudaMemcpyAsync(h->buf[0], h->buf[1], sizeof(double) * h->V * h->g.n, cudaMemcpyDeviceToDevice,
@@ -655,6 +693,7 @@ int enqueue_fargo_step(fgpu_handle* h) {
     double* out = (n % 2 == 1) ? Abuf : Bbuf;
     A.out = out;
     if (int rc = launch_stage(h, A)) return rc;
+    if (int rc = launch_accrete(h, n)) return rc;
     in = out;
   }
   if (int rc = launch_fargo_advect(h, in, P, Wn)) return rc;
@@ -891,6 +930,14 @@ int validate(fgpu_handle* h) {
   if (c.tmin > 1.e-10 && (c.checkdata & FGPU_CHECK_TMIN) && h->euler)
     return set_err(h, FGPU_EUNSUPPORTED, "CHECK_TMIN with tmin > 1e-10 is not supported");
   h->roundtrip_cfg = h->euler && (c.checkdata & FGPU_CHECK_PMIN);
+  if (c.pm_outbound != 0) {
+    if (!c.pointmass) return set_err(h, FGPU_EBADCFG, "accretion needs the point mass");
+    if (c.pm_outbound != 1 && c.pm_outbound != 2)
+      return set_err(h, FGPU_EUNSUPPORTED, "accretion through the x boundaries only (outbound 1 or 2)");
+    if (h->butcher) return set_err(h, FGPU_EUNSUPPORTED, "accretion with the fixed-step modified Euler scheme only");
+    h->accrete = true;
+    h->acc_face = c.pm_outbound - 1;
+  }
   if (c.fargo_method != 0) {
     if (c.fargo_method != 1)
       return set_err(h, FGPU_EUNSUPPORTED, "fargo: only type 1 (background velocity computed every step) is supported");
@@ -976,6 +1023,15 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
       h->buf.push_back(p);
     }
   }
+  if (!rc && h->accrete) {
+    size_t na = 3 * (size_t)h->g.ny + 2;
+    if (cudaMalloc(&h->d_acc, sizeof(double) * na) != cudaSuccess) rc = set_err(h, FGPU_ENOMEM, "accretion arrays");
+    else {
+      std::vector<double> a(na, 0.0);
+      a[3 * (size_t)h->g.ny] = cfg->pm_mass;
+      cudaMemcpy(h->d_acc, a.data(), sizeof(double) * na, cudaMemcpyHostToDevice);
+    }
+  }
   if (!rc && h->fargo) {
     if (cudaMalloc(&h->d_w, sizeof(double) * 2 * h->nxp) != cudaSuccess) rc = set_err(h, FGPU_ENOMEM, "fargo arrays");
     else cudaMemsetAsync(h->d_w, 0, sizeof(double) * 2 * h->nxp, h->stream);
@@ -1009,6 +1065,7 @@ void fgpu_destroy(fgpu_handle* h) {
   if (h->d_pad) cudaFree(h->d_pad);
   if (h->d_metric) cudaFree(h->d_metric);
   if (h->d_w) cudaFree(h->d_w);
+  if (h->d_acc) cudaFree(h->d_acc);
   if (h->d_ctl) cudaFree(h->d_ctl);
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
   if (h->own_stream) h->stream = h->own_stream;
@@ -1335,6 +1392,17 @@ int fgpu_get_status(fgpu_handle* h, fgpu_status* st) {
   st->time = h->time; st->dt = h->dt; st->dtold = h->dtold; st->dtmin = h->dtmin; st->maxerr = h->last_err;
   st->iter = h->iter; st->n_adj = h->n_adj; st->dtcause = h->dtcause; st->brk = h->brk ? 1 : 0;
   st->checkflags = h->checkflags;
+  return FGPU_OK;
+}
+
+int fgpu_get_pointmass(fgpu_handle* h, double* mass, double* mdot) {
+  if (!h || !mass || !mdot) return FGPU_EARG;
+  if (!h->accrete) { *mass = h->cfg.pm_mass; *mdot = 0.0; return FGPU_OK; }
+  double g[2];
+  CUDA_TRY(h, cudaMemcpyAsync(g, h->d_acc + 3 * (size_t)h->g.ny, sizeof(g), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  *mass = g[0];
+  *mdot = g[1];
   return FGPU_OK;
 }
 

@@ -57,6 +57,11 @@ struct StageArgs {
   // sources) and the Shu-Osher base states as chains of frame changes of the stored states
   const double* w_sub;
   Chain yn_chain, y0_chain;
+  // point-mass accretion: the boundary row of this RHS through the outbound x face,
+  // (dy*dz)*xflux of the density (face 0 west) or -(dy*dz)*xflux (face 1 east), by j
+  double* brow;
+  int brow_face;
+  double bdydz;
   // optional: the stage's reconstruction variables formed once per cell by form_kernel
   // (rin.ready = 1 for primitive reconstruction); the stencil then reads these instead of
   // forming base - sum coef*K and converting at every stencil point.  in stays the
@@ -281,17 +286,21 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
 
     double divX[V], divY[V];
     // ---- slopes of both directions in one phase (x: ey rows x ex+2 cells, y: ey+2 rows x ex cells)
-    const int nsx = (ex + 2) * ey, nsy = ex * (ey + 2);
+    // work items are enumerated over the full tile shape (compile-time divisors) and the
+    // ones outside a partial edge tile are skipped
+    constexpr int NSX = TY * (TX + 2), NSY = (TY + 2) * TX;
     if (!A.constant_recon) {
-      for (int t = tid; t < nsx + nsy; t += NT) {
-        if (t < nsx) {
-          int r = t / (ex + 2), c = t % (ex + 2) - 1;
+      for (int t = tid; t < NSX + NSY; t += NT) {
+        if (t < NSX) {
+          int r = t / (TX + 2), c = t % (TX + 2) - 1;
+          if (r >= ey || c > ex) continue;
 #pragma unroll
           for (int v = 0; v < V; ++v)
             SX(v, r, c + 1) = slope(A.limiter, A.theta, A.invd[0], RS(v, r + 2, c + 1), RS(v, r + 2, c + 2), RS(v, r + 2, c + 3));
         } else {
-          int u = t - nsx;
-          int c = u % ex, r = u / ex - 1;
+          int u = t - NSX;
+          int c = u % TX, r = u / TX - 1;
+          if (c >= ex || r > ey) continue;
 #pragma unroll
           for (int v = 0; v < V; ++v)
             SY(v, r + 1, c) = slope(A.limiter, A.theta, A.invd[1], RS(v, r + 1, c + 2), RS(v, r + 2, c + 2), RS(v, r + 3, c + 2));
@@ -300,11 +309,12 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
       __syncthreads();
     }
     // ---- interface fluxes of both directions in one phase
-    const int nfx = (ex + 1) * ey, nfy = ex * (ey + 1);
-    for (int t = tid; t < nfx + nfy; t += NT) {
+    constexpr int NFX = TY * (TX + 1), NFY = (TY + 1) * TX;
+    for (int t = tid; t < NFX + NFY; t += NT) {
       double RL[V], RR[V], F[V];
-      if (t < nfx) {
-        int r = t / (ex + 1), f = t % (ex + 1);
+      if (t < NFX) {
+        int r = t / (TX + 1), f = t % (TX + 1);
+        if (r >= ey || f > ex) continue;
         int gl = i0 + f - 1 + 2;   // padded i of the left cell
         double oE = M.offxE[gl], oW = M.offxW[gl + 1];
 #pragma unroll
@@ -316,9 +326,13 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
                               M.dAxW[gl + 1], P, F);
 #pragma unroll
         for (int v = 0; v < V; ++v) FX(v, r, f) = F[v];
+        // boundary row of ComputeRHS (timedisc_base.f90:1224-1231) for the accretion bookkeeping
+        if (ND == 2 && A.brow && ((A.brow_face == 0 && i0 + f == 0) || (A.brow_face == 1 && i0 + f == g.nx)))
+          A.brow[j0 + r] = (A.brow_face == 0 ? A.bdydz : -A.bdydz) * F[0];
       } else {
-        int u = t - nfx;
-        int c = u % ex, f = u / ex;
+        int u = t - NFX;
+        int c = u % TX, f = u / TX;
+        if (c >= ex || f > ey) continue;
         int gjl = j0 + f - 1 + 2;     // padded j of the lower cell
         int gi = i0 + c + 2;          // padded i of the column
         double oN = M.offyN[gjl], oS = M.offyS[gjl + 1];
@@ -353,7 +367,10 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
       if (PRIM) {
 #pragma unroll
         for (int v = 0; v < V; ++v) pc[v] = R0[v];
-        PH::p2c(pc, cc, P);
+        // the sources read cvar itself (the stage state), which Prim2Cons(pvar) only
+        // reproduces to rounding; after the CHECK_PMIN round trip cvar is Prim2Cons(pvar)
+        if (!roundtrip && (M.curv || A.has_accel)) state_at<V>(A.in, g.n, idx, cc);
+        else PH::p2c(pc, cc, P);
       } else {
 #pragma unroll
         for (int v = 0; v < V; ++v) cc[v] = R0[v];

@@ -240,6 +240,53 @@ __global__ void __launch_bounds__(256) unpack_kernel(const double* __restrict__ 
   }
 }
 
+// Point-mass accretion after a Shu-Osher stage of a 2D grid: the boundary fluxes
+// follow the stage update of the state (timedisc_modeuler.f90:223-236, the same
+// update formula), then the next ComputeRHS's UpdateGravity
+// (gravity_pointmass.f90:383-428, acclimit and switch-on disabled): the face sum
+// of the accumulated mass flux in j order (fluxes_base.f90:220-270), the mass
+// change against the last sum, and the acceleration scaled in place by
+// new/old mass.  One block; grav = [mass, mdot].
+struct AccArgs {
+  double* bx;          // accumulated boundary mass flux, by j
+  double* bxold;       // value at the last accepted step
+  const double* brow;  // boundary row of the stage's RHS, by j
+  int ny;
+  double eta;
+  const double* dt;
+  int last;            // last stage: AcceptSolution's bxfold = bxflux
+  double* grav;
+  double* accel;       // point-mass acceleration, naccel values
+  int naccel;
+  Ctl* ctl;
+};
+__global__ void __launch_bounds__(256) accrete_kernel(const __grid_constant__ AccArgs A) {
+  __shared__ double s_fac;
+  if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
+  const double dt = *A.dt;
+  for (int j = threadIdx.x; j < A.ny; j += blockDim.x) {
+    const double y0 = A.bxold[j], yn = A.bx[j], r = A.brow[j];
+    const double y = yn - dt * r + A.eta * (y0 - yn + dt * r);
+    A.bx[j] = y;
+    if (A.last) A.bxold[j] = y;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sj = 0.0;
+    for (int j = 0; j < A.ny; ++j) sj = sj + A.bx[j];
+    const double bflux = 0.0 + sj;
+    const double oldmass = A.grav[0];
+    const double dmass = bflux - A.grav[1];
+    const double mass = oldmass + dmass;
+    A.grav[0] = mass;
+    A.grav[1] = bflux;
+    s_fac = mass / oldmass;
+  }
+  __syncthreads();
+  const double f = s_fac;
+  for (int q = threadIdx.x; q < A.naccel; q += blockDim.x) A.accel[q] = A.accel[q] * f;
+}
+
 // The reconstruction variables of a Butcher stage state, formed once per cell:
 // out = base - sum coef*K (the reference's accumulation order), converted with
 // Cons2Prim for primitive reconstruction.  Values are identical to what the

@@ -304,7 +304,9 @@ __global__ void __launch_bounds__(32 * NW, 2) stage2_kernel(const __grid_constan
       if (PRIM) {
 #pragma unroll
         for (int v = 0; v < V; ++v) pc[v] = Rc[v];
-        PH::p2c(pc, cc, P);
+        // the sources read cvar itself (see stage_tile)
+        if (!roundtrip && (M.curv || A.has_accel)) state_at<V>(A.in, g.n, idx, cc);
+        else PH::p2c(pc, cc, P);
       } else {
 #pragma unroll
         for (int v = 0; v < V; ++v) cc[v] = Rc[v];

@@ -42,10 +42,15 @@ class Request:
     result: np.ndarray = None
     status: int = 0
     rid: int = field(default=-1)
+    # the request's initial data (cfg, pvar, extra) when it arrives with it; otherwise the
+    # server generates it from kind/size/seed at admission
+    payload: tuple = None
 
 
 def build_problem(req):
     """(cfg, pvar, extra) of a request, with its stop time."""
+    if req.payload is not None:
+        return req.payload
     if req.kind == "khi":
         cfg, p, extra = problems.khi2d(n=req.size[0], seed=req.seed)
     elif req.kind == "disk":

@@ -56,6 +56,7 @@ def lib(exact=False):
     L.fgpu_get_stats.argtypes = [C.c_void_p, C.POINTER(abi.Stats)]
     L.fgpu_reset_stats.argtypes = [C.c_void_p]
     L.fgpu_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+    L.fgpu_get_pointmass.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.fgpu_batch_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]
     L.fgpu_batch_destroy.argtypes = [C.c_void_p]
     L.fgpu_batch_last_error.argtypes = [C.c_void_p, C.c_char_p, C.c_int]
@@ -165,6 +166,12 @@ class Simulation:
         st = abi.Status()
         self._check(self.L.fgpu_get_status(self.h, C.byref(st)))
         return st
+
+    def pointmass(self):
+        """(mass, mdot) of the central point mass; changes only with accretion."""
+        m, d = C.c_double(), C.c_double()
+        self._check(self.L.fgpu_get_pointmass(self.h, C.byref(m), C.byref(d)))
+        return m.value, d.value
 
     def synchronize(self):
         self._check(self.L.fgpu_synchronize(self.h))

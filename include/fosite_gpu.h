@@ -148,6 +148,12 @@ typedef struct fgpu_config {
     int32_t fargo_direction;       /* only 2 (transport along y) is supported */
     /* output clip time for AdjustTimestep (io/fileio_base.f90:604-621); 0 = stoptime */
     double  tout;
+    /* point-mass accretion (gravity_pointmass.f90:287-297, 383-428): the boundary whose
+     * accumulated mass flux feeds the point mass, in fosite's numbering 1 = WEST,
+     * 2 = EAST; 0 = off.  fosite defaults to WEST on cylindrical meshes, this struct
+     * to 0 (the caller passes the Dict value).  Fixed-step modified Euler only. */
+    int32_t pm_outbound;
+    int32_t pad_;
 } fgpu_config;
 
 /* Step bookkeeping returned to the caller (mirrors Timedisc%time/dt/...). */
@@ -281,6 +287,9 @@ int  fgpu_batch_autotune(fgpu_batch* b, int reps, int* variant);
  * array: calls that overlap on the GPU race. */
 int fgpu_calc_timestep_noalloc(const fgpu_config* cfg, const double* d_cvar, double* d_dt, void* stream);
 int fgpu_get_status(fgpu_handle* h, fgpu_status* st);
+/* The central point mass and the accumulated boundary mass flux of its last update
+ * (gravity_pointmass%mass, %mdot); the configured mass when accretion is off. */
+int fgpu_get_pointmass(fgpu_handle* h, double* mass, double* mdot);
 /* Block until all device work of h has finished. */
 int fgpu_synchronize(fgpu_handle* h);
 /* Enqueue all further work of h on a caller-owned CUDA stream (a cudaStream_t

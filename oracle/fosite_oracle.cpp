@@ -71,6 +71,11 @@ struct Oracle {
   std::vector<double> tmpw, tmpw1;           // NC
   std::vector<double> accel;                 // NC*VDIM
   bool have_accel = false;
+  // point-mass accretion: x-boundary fluxes (fluxes_base.f90:73-76 bxflux/bxfold, indexed
+  // [((l*2 + face)*KNUM + k)*JNUM + j]) and the point mass (gravity_pointmass.f90:383-428)
+  int outbound = 0;                          // fosite numbering: 1 WEST, 2 EAST
+  std::vector<double> bxf, bxo;
+  double pm_cur = 0.0, mdot = 0.0;
   // ---- timedisc ----
   int order, m_stages;
   bool butcher;
@@ -145,6 +150,17 @@ struct Oracle {
     if (int rc = setup_timedisc()) return rc;
     // sources
     if (cfg.pointmass) { if (int rc = setup_pointmass()) return rc; }
+    if (cfg.pm_outbound) {
+      if (!cfg.pointmass) { err = "accretion needs the point mass"; return FGPU_EBADCFG; }
+      if (cfg.pm_outbound != 1 && cfg.pm_outbound != 2) { err = "accretion through the x boundaries only"; return FGPU_EUNSUPPORTED; }
+      if (cfg.geometry != FGPU_CYLINDRICAL && cfg.geometry != FGPU_LOGCYLINDRICAL) { err = "geometry does not support accretion"; return FGPU_EUNSUPPORTED; }
+      if (butcher || tol_rel < 1.0) { err = "accretion with the fixed-step modified Euler scheme only"; return FGPU_EUNSUPPORTED; }
+      outbound = cfg.pm_outbound;
+      bxf.assign((size_t)VNUM * 2 * KNUM * JNUM, 0.0);
+      bxo = bxf;
+      pm_cur = cfg.pm_mass;
+      mdot = 0.0;
+    }
     // fargo (timedisc_base.f90:369-452)
     fargo = cfg.fargo_method;
     if (fargo) {
@@ -870,10 +886,46 @@ struct Oracle {
         if (g) s[id(i, j, k) + NC * l] = 0.0;
       }
   }
+  // ---------------------------------------------------------------- accretion
+  double& BX(std::vector<double>& a, int j, int k, int face, int l) {
+    return a[(((size_t)l * 2 + face) * KNUM + (k - KMIN)) * JNUM + (j - JMIN)];
+  }
+  // timedisc_modeuler.f90:223-236: boundary fluxes follow the stage update of the state,
+  // fed by the boundary rows of rhs (ComputeRHS :1224-1231)
+  void update_bflux(double e, double dtv) {
+    for (int l = 0; l < VNUM; ++l)
+      for (int k = KMIN; k <= KMAX; ++k) for (int j = JMIN; j <= JMAX; ++j) {
+        BX(bxf, j, k, 0, l) = update_me(e, dtv, BX(bxo, j, k, 0, l), BX(bxf, j, k, 0, l), rhs[id(IMIN - IP1, j, k) + NC * l]);
+        BX(bxf, j, k, 1, l) = update_me(e, dtv, BX(bxo, j, k, 1, l), BX(bxf, j, k, 1, l), rhs[id(IMAX + IP1, j, k) + NC * l]);
+      }
+  }
+  // fluxes_base.f90:220-270 GetBoundaryFlux (serial): SUM(SUM(bxflux(J,K,face,:),1),1), density
+  double boundary_mass_flux() {
+    int face = outbound == 1 ? 0 : 1;
+    double tot = 0.0;
+    for (int k = KMIN; k <= KMAX; ++k) {
+      double sj = 0.0;
+      for (int j = JMIN; j <= JMAX; ++j) sj = sj + BX(bxf, j, k, face, 0);
+      tot = tot + sj;
+    }
+    return tot;
+  }
+  // gravity_pointmass.f90:383-428 UpdateGravity_single (acclimit and switchon disabled)
+  void update_gravity() {
+    double bflux = boundary_mass_flux();
+    double oldmass = pm_cur;
+    double dmass = bflux - mdot;
+    pm_cur = pm_cur + dmass;
+    double massfac = pm_cur / oldmass;
+    for (size_t x = 0; x < accel.size(); ++x) accel[x] = accel[x] * massfac;
+    mdot = bflux;
+  }
+
   // sources_generic.f90:220-261 -> sources_gravity.f90:164-200 -> physics ExternalSources
   void external_sources(std::vector<double>& cv, std::vector<double>& s) {
     std::fill(s.begin(), s.end(), 0.0);
     if (!have_accel) return;
+    if (outbound) update_gravity();
     for (long x = 0; x < NC; ++x) {
       for (int n = 0; n < VDIM; ++n) s[x + NC * (1 + n)] = cv[x] * accel[x + NC * n];
       if (euler) {
@@ -1038,6 +1090,7 @@ struct Oracle {
         for (int n = 1; n <= order; ++n) {
           double e = eta[order - 1][n - 1];
           for (long x = 0; x < NS; ++x) cvar[x] = update_me(e, dtv, cold[x], cvar[x], rhs[x]);
+          if (outbound) update_bflux(e, dtv);
           if (n < order) compute_rhs(pvar, cvar, FGPU_CHECK_NOTHING, rhs);
         }
         errv = 0.0; dtv = HUGE_;
@@ -1103,11 +1156,13 @@ struct Oracle {
       else if (e >= 1.0) {   // RejectSolution
         cvar = cold;
         compute_rhs(pvar, cvar, FGPU_CHECK_NOTHING, rhs);
+        if (outbound) bxf = bxo;   // RejectSolution (timedisc_base.f90:980-1000)
         n_adj++; dtcause = FGPU_DTCAUSE_ERRADJ;
         if (d < dtmin) { dtmin = d; dtmincause = dtcause; }
       } else {               // AcceptSolution
         t = t + dtold_;
         if (t < time + dt) { compute_rhs(pvar, cvar, checkdatabm, rhs); cold = cvar; }
+        if (outbound) bxo = bxf;   // AcceptSolution (timedisc_base.f90:937-958)
         iter++;
       }
       if (d < dtlimit) brk = true;
@@ -1222,5 +1277,10 @@ int orc_get_status(orc_handle* h, fgpu_status* st) {
   return 0;
 }
 const char* orc_error(orc_handle* h) { return h ? h->o.err.c_str() : ""; }
+int orc_get_pointmass(orc_handle* h, double* mass, double* mdot) {
+  *mass = h->o.outbound ? h->o.pm_cur : h->o.cfg.pm_mass;
+  *mdot = h->o.mdot;
+  return 0;
+}
 
 }  // extern "C"

@@ -45,6 +45,7 @@ def lib():
         L.orc_get_status.argtypes = [C.c_void_p, C.POINTER(abi.Status)]
         L.orc_error.argtypes = [C.c_void_p]
         L.orc_error.restype = C.c_char_p
+        L.orc_get_pointmass.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         _lib = L
     return _lib
 
@@ -114,3 +115,9 @@ class Oracle:
         st = abi.Status()
         lib().orc_get_status(self.h, C.byref(st))
         return st
+
+    def pointmass(self):
+        """(mass, mdot) of the central point mass (accretion bookkeeping)."""
+        m, d = C.c_double(), C.c_double()
+        lib().orc_get_pointmass(self.h, C.byref(m), C.byref(d))
+        return m.value, d.value

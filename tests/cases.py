@@ -73,9 +73,14 @@ def _gauss3d(n=(20, 18, 16), variables=abi.PRIMITIVE, limiter=abi.MONOCENT, meth
     return c, p, {}
 
 
-def _disk(n=(32, 48), geometry=abi.LOGCYLINDRICAL, seed=31, hratio=0.05, variables=abi.PRIMITIVE):
-    c, p, extra = problems.disk2d(nr=n[0], nphi=n[1], seed=seed, hratio=hratio, geometry=geometry, fargo=0)
+def _disk(n=(32, 48), geometry=abi.LOGCYLINDRICAL, seed=31, hratio=0.05, variables=abi.PRIMITIVE, outbound=0,
+          bcs=None, fargo=0):
+    c, p, extra = problems.disk2d(nr=n[0], nphi=n[1], seed=seed, hratio=hratio, geometry=geometry, fargo=fargo)
     c.variables = variables
+    c.pm_outbound = outbound
+    if bcs:
+        for f, t in enumerate(bcs):
+            c.bc[f] = t
     rng = np.random.default_rng(seed + 1)
     p[1] = 0.01 * rng.uniform(-1, 1, p[1].shape)
     return c, p, extra
@@ -144,6 +149,10 @@ CASES = {
     "disk_logcyl_pointmass": lambda: _disk(),
     "disk_cyl_pointmass_cons": lambda: _disk(geometry=abi.CYLINDRICAL, n=(40, 32), variables=abi.CONSERVATIVE),
     "iso3d_cashkarp_mixed_bc": lambda: _iso3d(),
+    "disk_accretion_west_nograd": lambda: _disk(n=(36, 40), outbound=1,
+                                                bcs=[abi.NO_GRADIENTS, abi.REFLECTING, abi.PERIODIC, abi.PERIODIC]),
+    "disk_accretion_east_cyl_fargo": lambda: _disk(n=(30, 44), geometry=abi.CYLINDRICAL, outbound=2, fargo=1,
+                                                   bcs=[abi.REFLECTING, abi.NO_GRADIENTS, abi.PERIODIC, abi.PERIODIC]),
     "disk_fargo_logcyl": lambda: _disk_fargo(),
     "disk_fargo_cyl_cons_reflect": lambda: _disk_fargo(geometry=abi.CYLINDRICAL, n=(36, 40), variables=abi.CONSERVATIVE,
                                                        bcs=[abi.REFLECTING, abi.NO_GRADIENTS, abi.PERIODIC, abi.PERIODIC],

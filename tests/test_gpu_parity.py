@@ -106,6 +106,12 @@ def test_steps_bitwise_exact_build(name):
         if tol == 0.0:
             assert sg.time == so.time and sg.dt == so.dt, (s, sg.time, so.time, sg.dt, so.dt)
         _compare(cfg, o, g, tol, "step %d" % s)
+        if cfg.pm_outbound:
+            (mg, dg), (mo, do) = g.pointmass(), o.pointmass()
+            if tol == 0.0:
+                assert (mg, dg) == (mo, do), (s, mg, mo, dg, do)
+            else:
+                assert abs(mg - mo) <= 1e-13 * abs(mo) and abs(dg - do) <= 1e-11 * abs(mo)
     # full ghost-padded primitive state, ghost cells included (CenterBoundary + SetCornerEdges)
     pa, pb = g.get(abi.PVAR), o.get(abi.PVAR)
     if tol == 0.0:
