@@ -56,6 +56,7 @@ class Config(C.Structure):
         ("fargo_method", C.c_int32), ("fargo_direction", C.c_int32),
         ("tout", C.c_double),
         ("pm_outbound", C.c_int32), ("pad_", C.c_int32),
+        ("starttime", C.c_double),
     ]
 
 

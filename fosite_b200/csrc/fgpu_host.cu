@@ -1235,7 +1235,7 @@ int fgpu_first_step(fgpu_handle* h) {
   if (h->first_done) return set_err(h, FGPU_EBADCFG, "FirstStep should only be called once.");
   h->first_done = true;
   h->iter = 0;
-  h->time = 0.0;
+  h->time = h->cfg.starttime;
   if (h->butcher) {
     if (int rc = enqueue_k1(h, true, true)) return rc;
     double dtc;
@@ -1251,7 +1251,7 @@ int fgpu_first_step(fgpu_handle* h) {
   Ctl* c = h->h_ctl;
   std::memset(c, 0, sizeof(Ctl));
   c->stoptime = h->stoptime; c->tout = h->tout; c->cfl = h->cfl; c->dtlimit = h->dtlimit;
-  c->time = 0.0; c->dtmin = h->stoptime; c->iter = 0;
+  c->time = h->cfg.starttime; c->dtmin = h->stoptime; c->iter = 0;
   if (int rc = write_ctl(h)) return rc;
   BndArgs B = bnd_args(h, h->buf[0], h->roundtrip_cfg, FIN_FIRST);
   if (h->fargo) {

@@ -154,6 +154,9 @@ typedef struct fgpu_config {
      * to 0 (the caller passes the Dict value).  Fixed-step modified Euler only. */
     int32_t pm_outbound;
     int32_t pad_;
+    /* Timedisc%time at FirstStep ("starttime", timedisc_base.f90:295), e.g. the time of a
+     * restart file (examples/restart.f90); default 0 */
+    double  starttime;
 } fgpu_config;
 
 /* Step bookkeeping returned to the caller (mirrors Timedisc%time/dt/...). */

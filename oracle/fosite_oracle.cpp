@@ -143,7 +143,7 @@ struct Oracle {
     fprim.assign(NC * NFACES * VNUM, 0); fcons.assign(NC * NFACES * VNUM, 0); pfluxes.assign(NC * NFACES * VNUM, 0);
     minwav.assign(NC * NDIMS, 0); maxwav.assign(NC * NDIMS, 0); tmpw.assign(NC, 0); tmpw1.assign(NC, 0);
     // timedisc (timedisc_base.f90:285-350, timedisc_modeuler.f90:97-123)
-    time = 0.0; stoptime = cfg.stoptime; dt = stoptime; dtold = dt; dtmin = dt; dtmincause = -99;
+    time = cfg.starttime; stoptime = cfg.stoptime; dt = stoptime; dtold = dt; dtmin = dt; dtmincause = -99;
     cfl = cfg.cfl; dtlimit = cfg.dtlimit; tol_rel = cfg.tol_rel; beta = cfg.beta;
     tol_abs.assign(cfg.tol_abs, cfg.tol_abs + VNUM);
     checkdatabm = cfg.checkdata; maxerrold = 0.0; dtcause = 0;
