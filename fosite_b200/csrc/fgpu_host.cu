@@ -146,6 +146,7 @@ struct fgpu_handle {
   int graph_steps = 0;
   // launch shape
   int tile_x = 32, tile_y = 8, kchunk = 16;
+  bool adaptive_me = false;     // modified Euler with embedded error control (tol_rel < 1)
   bool materialize = true;      // Butcher stages: form the stage's reconstruction variables once per cell
   double* d_ready = nullptr;    // ... into this array (one state)
   int variant = 0;              // stage kernel layout: 0 shared-memory tile, 1 warp-shuffle window,
@@ -773,7 +774,60 @@ double adjust_timestep(fgpu_handle* h, double maxerr, double dtold_) {
   return dtnew;
 }
 
+// One attempt of the adaptive modified Euler scheme (timedisc_modeuler.f90:125-195,
+// tol_rel < 1).  At an attempt's start cvar = cold = base and rhs = k1:
+//   s1 = update(eta1, base, base, k1)                     (pointwise)
+//   order 3: s2 = update(eta2, base, s1, rhs(s1)), low = update(1/2, base, s1, rhs(s1))
+//            P  = update(eta3, base, s2, rhs(s2)),  err = ComputeError(P, low)
+//   order 2: P  = update(eta2, base, s1, rhs(s1)),  err = ComputeError(P, s1)
+int modeuler_attempt(fgpu_handle* h, double dtv, double& err) {
+  double* P = h->buf[0];
+  double* base = h->buf[1];
+  double* K1 = h->buf[2];
+  double* S1 = h->buf[3];
+  double* S2 = h->buf[4];
+  double* LO = h->buf[5];
+  const int ord = h->order;
+  h->stats.attempts += 1;
+  {
+    const long long n = (long long)h->V * h->g.n;
+    unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148 * 8);
+    const double e1 = kEta[ord - 1][0];
+    int rc = timed_launch(h, 0, 0.0, [&] {
+      shu_osher_update_kernel<<<blocks, 256, 0, h->stream>>>(base, base, K1, S1, n, e1, dtv);
+      CUDA_TRY(h, cudaGetLastError());
+      return FGPU_OK;
+    });
+    if (rc) return rc;
+  }
+  for (int n = 2; n <= ord; ++n) {
+    StageArgs A = base_args(h);
+    A.in = plain_state(n == 2 ? S1 : S2, false);
+    A.out_mode = OUT_SSPRK;
+    A.eta = kEta[ord - 1][n - 1];
+    A.y0 = base;
+    A.dt = dtv;
+    if (n == ord) {
+      A.out = P;
+      A.err_low = ord == 3 ? LO : S1;
+    } else {
+      A.out = S2;
+      A.out2 = LO;
+      A.eta2 = kEta[1][1];   // the second-order solution from the same RHS
+    }
+    if (int rc = launch_stage(h, A)) return rc;
+  }
+  if (int rc = read_ctl(h)) return rc;
+  double e;
+  std::memcpy(&e, &h->h_ctl->err, 8);
+  h->h_ctl->err = 0ULL;
+  CUDA_TRY(h, cudaMemsetAsync(&h->d_ctl->err, 0, sizeof(unsigned long long), h->stream));
+  err = e;
+  return FGPU_OK;
+}
+
 int butcher_attempt(fgpu_handle* h, double dtv, double& err) {
+  if (h->adaptive_me) return modeuler_attempt(h, dtv, err);
   const Tableau& T = h->T;
   double* P = h->buf[0];
   double* base = h->buf[1];
@@ -916,8 +970,15 @@ int validate(fgpu_handle* h) {
     h->order = c.tdorder ? c.tdorder : 3;
     if (h->order < 1 || h->order > 3) return set_err(h, FGPU_EBADCFG, "time order must be one of 1,2,3");
     if (h->order == 1) { h->tol_rel = 10.0; for (int v = 0; v < FGPU_MAXVAR; ++v) h->tol_abs[v] = 1.0; }
-    if (h->tol_rel < 1.0)
-      return set_err(h, FGPU_EUNSUPPORTED, "modified Euler with adaptive step control (tol_rel < 1) is not supported; use tol_rel >= 1 or an embedded RK method");
+    if (h->tol_rel < 1.0) {
+      // embedded error control (timedisc_modeuler.f90:163-192): the host-controlled attempt
+      // engine of the Butcher schemes with Shu-Osher attempts; buffers P, base, k1, the
+      // stage-1 state, the stage-2 state, the embedded solution and one spare
+      h->butcher = true;
+      h->adaptive_me = true;
+      h->T.m = 4;
+      h->T.order = h->order;
+    }
   } else {
     h->butcher = true;
     int ord = c.tdorder ? c.tdorder : 5;

@@ -57,6 +57,13 @@ struct StageArgs {
   // sources) and the Shu-Osher base states as chains of frame changes of the stored states
   const double* w_sub;
   Chain yn_chain, y0_chain;
+  // adaptive modified Euler: a second Shu-Osher result from the same RHS,
+  // out2 = yn - dt*rhs + eta2*(y0 - yn + dt*rhs) (the embedded lower-order solution,
+  // timedisc_modeuler.f90:163-192), and the error norm of the new state against
+  // err_low (ComputeError, timedisc_base.f90:1012-1053) reduced into ctl->err
+  double* out2;
+  double eta2;
+  const double* err_low;
   // point-mass accretion: the boundary row of this RHS through the outbound x face,
   // (dy*dz)*xflux of the density (face 0 west) or -(dy*dz)*xflux (face 1 east), by j
   double* brow;
@@ -463,6 +470,19 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
           y[v] = yn[v] - dt * rhs[v] + A.eta * (y0[v] - yn[v] + dt * rhs[v]);
           A.out[(long long)v * g.n + idx] = y[v];
         }
+        if (A.out2) {
+#pragma unroll
+          for (int v = 0; v < V; ++v)
+            A.out2[(long long)v * g.n + idx] = yn[v] - dt * rhs[v] + A.eta2 * (y0[v] - yn[v] + dt * rhs[v]);
+        }
+        if (A.err_low) {
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            const double l = __ldg(A.err_low + (long long)v * g.n + idx);
+            const double e = fabs(y[v] - l) / (A.tol_rel * fabs(y[v]) + A.tol_abs[v]);
+            errv = dmax(errv, e);
+          }
+        }
         if (A.cfl_mode == 1) {
           double p[V], c[V];
           PH::c2p(y, p, P);
@@ -524,11 +544,12 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
     // halo of the next plane, and every reader of this plane has passed the flux barrier
   }
 
-  if (A.ctl && (A.cfl_mode || A.last_stage)) {
+  const bool err_out = A.last_stage || A.err_low;
+  if (A.ctl && (A.cfl_mode || err_out)) {
     int nv = A.cfl_mode ? (ND == 3 ? 3 : 1) : 0;
     double vals[3] = {cflv[0], cflv[1], cflv[2]};
-    if (A.last_stage && !A.cfl_mode) { vals[0] = errv; nv = 1; }
-    if (nv) block_reduce_emit<NT>(vals, nv, flags, A.last_stage && !A.cfl_mode ? &A.ctl->err : A.ctl->invdt,
+    if (err_out && !A.cfl_mode) { vals[0] = errv; nv = 1; }
+    if (nv) block_reduce_emit<NT>(vals, nv, flags, err_out && !A.cfl_mode ? &A.ctl->err : A.ctl->invdt,
                                   &A.ctl->flags, sred);
   }
   // the next tile of a persistent block may place its halo where this tile had cells

@@ -287,6 +287,16 @@ __global__ void __launch_bounds__(256) accrete_kernel(const __grid_constant__ Ac
   for (int q = threadIdx.x; q < A.naccel; q += blockDim.x) A.accel[q] = A.accel[q] * f;
 }
 
+// Pointwise Shu-Osher update with a stored RHS (the first stage of the adaptive
+// modified Euler scheme, whose RHS is the step's k1): out = yn - dt*r + eta*(y0 - yn + dt*r)
+// (timedisc_modeuler.f90:279-291), over n values.
+__global__ void __launch_bounds__(256) shu_osher_update_kernel(const double* __restrict__ y0, const double* __restrict__ yn,
+                                                               const double* __restrict__ r, double* __restrict__ out,
+                                                               long long n, double eta, double dt) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    out[t] = yn[t] - dt * r[t] + eta * (y0[t] - yn[t] + dt * r[t]);
+}
+
 // The reconstruction variables of a Butcher stage state, formed once per cell:
 // out = base - sum coef*K (the reference's accumulation order), converted with
 // Cons2Prim for primitive reconstruction.  Values are identical to what the

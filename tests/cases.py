@@ -10,7 +10,7 @@ from fosite_b200 import abi, problems
 
 
 def _khi(n=(40, 36), limiter=abi.VANLEER, variables=abi.CONSERVATIVE, theta=1.0, order=abi.LINEAR,
-         method=abi.MODIFIED_EULER, tdorder=3, bcs=None, seed=11):
+         method=abi.MODIFIED_EULER, tdorder=3, bcs=None, seed=11, me_tol=None):
     c = abi.default_config()
     c.inum, c.jnum, c.knum = n[0], n[1], 1
     c.xmin, c.xmax, c.ymin, c.ymax = -0.5, 0.5, -0.5, 0.5
@@ -26,6 +26,10 @@ def _khi(n=(40, 36), limiter=abi.VANLEER, variables=abi.CONSERVATIVE, theta=1.0,
     if method != abi.MODIFIED_EULER:
         for v in range(abi.MAXVAR):
             c.tol_abs[v] = 1e-4
+    if me_tol is not None:      # modified Euler with embedded error control
+        c.tol_rel = me_tol
+        for v in range(abi.MAXVAR):
+            c.tol_abs[v] = me_tol
     c.cfl = 0.4
     c.stoptime = 1.0e3
     if bcs:
@@ -139,6 +143,9 @@ CASES = {
     "euler2d_reflect_nograd_ssprk5": lambda: _khi(bcs=[abi.REFLECTING, abi.REFLECTING, abi.NO_GRADIENTS, abi.NO_GRADIENTS],
                                                  method=abi.SSPRK, tdorder=5, n=(30, 26)),
     "euler2d_rkf45": lambda: _khi(method=abi.RK_FEHLBERG, tdorder=5, n=(28, 30)),
+    "khi_modeuler_adaptive3": lambda: _khi(me_tol=1e-3),
+    "khi_modeuler_adaptive2_mc_prim": lambda: _khi(tdorder=2, me_tol=1e-3, limiter=abi.MONOCENT,
+                                                  variables=abi.PRIMITIVE, n=(34, 30)),
     "gauss3d_dopri_mc_prim": lambda: _gauss3d(),
     "gauss3d_rkf3_minmod_cons": lambda: _gauss3d(variables=abi.CONSERVATIVE, limiter=abi.MINMOD, method=abi.RK_FEHLBERG,
                                                 tdorder=3, n=(17, 20, 14),
