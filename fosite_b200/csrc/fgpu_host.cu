@@ -665,9 +665,10 @@ int enqueue_fargo_step(fgpu_handle* h) {
   double* Abuf = h->buf[1];
   double* Bbuf = h->buf[2];
   const double* W = h->d_w;
-  double* Wn = h->d_w + h->nxp;
+  const bool dyn = h->cfg.fargo_method == 1;   // type 2 keeps the user's w: no recomputation
+  double* Wn = dyn ? h->d_w + h->nxp : h->d_w;
   const Chain pre = fargo_pre(h);
-  {
+  if (dyn) {
     StateRef S = plain_state(P, false);
     S.pre = pre;
     if (int rc = launch_fargo_w(h, S, W, Wn)) return rc;
@@ -680,7 +681,9 @@ int enqueue_fargo_step(fgpu_handle* h) {
     if (n == 1) {
       A.in.pre = pre;
       A.w_sub = W;
-      A.yn_chain = chain_add(chain_add(cold, W, 1.0), Wn, -1.0);
+      // type 1: CalcBackgroundVelocity adds w and the step subtracts w_new; type 2: cvar
+      // is already co-moving, the step's SubtractBackgroundVelocityY does nothing
+      A.yn_chain = dyn ? chain_add(chain_add(cold, W, 1.0), Wn, -1.0) : cold;
     } else {
       A.in.pre = chain_add(chain_none(), Wn, 1.0);
       A.w_sub = Wn;
@@ -702,7 +705,7 @@ int enqueue_fargo_step(fgpu_handle* h) {
   B.in.pre = chain_add(chain_none(), Wn, 1.0);
   B.w_sub = Wn;
   if (int rc = launch_misc(h, 0, B)) return rc;
-  CUDA_TRY(h, cudaMemcpyAsync(h->d_w, Wn, sizeof(double) * h->nxp, cudaMemcpyDeviceToDevice, h->stream));
+  if (dyn) CUDA_TRY(h, cudaMemcpyAsync(h->d_w, Wn, sizeof(double) * h->nxp, cudaMemcpyDeviceToDevice, h->stream));
   h->fargo_phase = 2;
   return FGPU_OK;
 }
@@ -1000,8 +1003,9 @@ int validate(fgpu_handle* h) {
     h->acc_face = c.pm_outbound - 1;
   }
   if (c.fargo_method != 0) {
-    if (c.fargo_method != 1)
-      return set_err(h, FGPU_EUNSUPPORTED, "fargo: only type 1 (background velocity computed every step) is supported");
+    if (c.fargo_method != 1 && c.fargo_method != 2)
+      return set_err(h, FGPU_EUNSUPPORTED, "fargo: types 1 (computed) and 2 (user-supplied) background velocity only; "
+                                           "type 3 needs the shearing-box sources");
     if (c.fargo_direction != 2) return set_err(h, FGPU_EUNSUPPORTED, "fargo: only transport along y (direction 2) is supported");
     if (h->nd != 2 || h->euler) return set_err(h, FGPU_EUNSUPPORTED, "fargo: 2D x-y meshes with isothermal physics only");
     if (h->butcher) return set_err(h, FGPU_EUNSUPPORTED, "fargo: fixed-step modified Euler (Shu-Osher) time stepping only");
@@ -1318,7 +1322,8 @@ int fgpu_first_step(fgpu_handle* h) {
   if (h->fargo) {
     // FirstStep's CenterBoundary + CalcBackgroundVelocity (fosite.f90:315-321), then the
     // CFL of its ComputeRHS on the co-moving state
-    if (int rc = launch_fargo_w(h, plain_state(h->buf[0], false), nullptr, h->d_w)) return rc;
+    if (h->cfg.fargo_method == 1)
+      if (int rc = launch_fargo_w(h, plain_state(h->buf[0], false), nullptr, h->d_w)) return rc;
     CUDA_TRY(h, cudaMemcpyAsync(h->d_w + h->nxp, h->d_w, sizeof(double) * h->nxp, cudaMemcpyDeviceToDevice, h->stream));
     B.w_sub = h->d_w;
     h->fargo_phase = 1;
@@ -1453,6 +1458,18 @@ int fgpu_get_status(fgpu_handle* h, fgpu_status* st) {
   st->time = h->time; st->dt = h->dt; st->dtold = h->dtold; st->dtmin = h->dtmin; st->maxerr = h->last_err;
   st->iter = h->iter; st->n_adj = h->n_adj; st->dtcause = h->dtcause; st->brk = h->brk ? 1 : 0;
   st->checkflags = h->checkflags;
+  return FGPU_OK;
+}
+
+int fgpu_set_fargo_velocity(fgpu_handle* h, const double* w, int64_t n) {
+  if (!h || !w) return FGPU_EARG;
+  if (!h->fargo || h->cfg.fargo_method != 2)
+    return set_err(h, FGPU_EBADCFG, "the background velocity is supplied for fargo type 2 only");
+  if (h->first_done) return set_err(h, FGPU_EBADCFG, "set the fargo background velocity before the first step");
+  if (n < h->nxp) return set_err(h, FGPU_EARG, "background velocity array too small (inum+4 values)");
+  CUDA_TRY(h, cudaMemcpyAsync(h->d_w, w, sizeof(double) * h->nxp, cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(h, cudaMemcpyAsync(h->d_w + h->nxp, w, sizeof(double) * h->nxp, cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return FGPU_OK;
 }
 

@@ -57,6 +57,7 @@ def lib(exact=False):
     L.fgpu_reset_stats.argtypes = [C.c_void_p]
     L.fgpu_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
     L.fgpu_get_pointmass.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.fgpu_set_fargo_velocity.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
     L.fgpu_batch_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]
     L.fgpu_batch_destroy.argtypes = [C.c_void_p]
     L.fgpu_batch_last_error.argtypes = [C.c_void_p, C.c_char_p, C.c_int]
@@ -166,6 +167,11 @@ class Simulation:
         st = abi.Status()
         self._check(self.L.fgpu_get_status(self.h, C.byref(st)))
         return st
+
+    def set_fargo_velocity(self, w):
+        """Background velocity of FARGO type 2, one value per padded i (inum+4)."""
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        self._check(self.L.fgpu_set_fargo_velocity(self.h, _ptr(w), w.size))
 
     def pointmass(self):
         """(mass, mdot) of the central point mass; changes only with accretion."""

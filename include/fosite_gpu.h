@@ -142,8 +142,9 @@ typedef struct fgpu_config {
     int32_t pointmass;
     double  pm_mass;               /* default 1.0 */
     /* fargo transport (timedisc_base.f90:369-452): method 0 off, 1 background velocity
-     * computed every step (the only type this backend runs; 2D x-y isothermal meshes with
-     * the fixed-step modified Euler scheme), 2 fixed user-supplied background velocity */
+     * computed every step, 2 fixed user-supplied background velocity
+     * (fgpu_set_fargo_velocity); 2D x-y isothermal meshes with the fixed-step modified
+     * Euler scheme.  Type 3 (shearing box) is not available. */
     int32_t fargo_method;
     int32_t fargo_direction;       /* only 2 (transport along y) is supported */
     /* output clip time for AdjustTimestep (io/fileio_base.f90:604-621); 0 = stoptime */
@@ -290,6 +291,10 @@ int  fgpu_batch_autotune(fgpu_batch* b, int reps, int* variant);
  * array: calls that overlap on the GPU race. */
 int fgpu_calc_timestep_noalloc(const fgpu_config* cfg, const double* d_cvar, double* d_dt, void* stream);
 int fgpu_get_status(fgpu_handle* h, fgpu_status* st);
+/* Timedisc%w for FARGO type 2 (a background velocity the user supplies, e.g. in
+ * InitData; timedisc_base.f90:414-424): one value per padded i (inum+4 values, the
+ * interior i starting at index 2); call before fgpu_first_step. */
+int fgpu_set_fargo_velocity(fgpu_handle* h, const double* w, int64_t n);
 /* The central point mass and the accumulated boundary mass flux of its last update
  * (gravity_pointmass%mass, %mdot); the configured mass when accretion is off. */
 int fgpu_get_pointmass(fgpu_handle* h, double* mass, double* mdot);

@@ -164,6 +164,9 @@ struct Oracle {
     // fargo (timedisc_base.f90:369-452)
     fargo = cfg.fargo_method;
     if (fargo) {
+      // types 1 (w computed every step) and 2 (w supplied by the user, fixed); type 3
+      // (shearing box) needs the shearing-box sources
+      if (fargo != 1 && fargo != 2) { err = "fargo: types 1 and 2 only"; return FGPU_EUNSUPPORTED; }
       if (cfg.fargo_direction != 2 || NDIMS < 2) { err = "fargo: only direction 2 supported"; return FGPU_EUNSUPPORTED; }
       if (euler) { err = "fargo: isothermal physics only"; return FGPU_EUNSUPPORTED; }
       if (NDIMS != 2 || dirs[0] != 0 || dirs[1] != 1) { err = "fargo: 2D x-y meshes only"; return FGPU_EUNSUPPORTED; }
@@ -1243,6 +1246,13 @@ int orc_set_sound_speeds(orc_handle* h, const double* bcc, const double* fcs) {
   Oracle& o = h->o;
   std::memcpy(o.bccsound.data(), bcc, sizeof(double) * o.NC);
   std::memcpy(o.fcsound.data(), fcs, sizeof(double) * o.NC * o.NFACES);
+  return 0;
+}
+// Timedisc%w of FARGO type 2 (user supplied, timedisc_base.f90:421-424), by padded i
+int orc_set_fargo_velocity(orc_handle* h, const double* w, int64_t n) {
+  Oracle& o = h->o;
+  if (o.fargo != 2 || n < (int64_t)o.w.size()) return FGPU_EARG;
+  std::memcpy(o.w.data(), w, sizeof(double) * o.w.size());
   return 0;
 }
 int orc_set_state(orc_handle* h, int which, const double* data) {

@@ -46,6 +46,7 @@ def lib():
         L.orc_error.argtypes = [C.c_void_p]
         L.orc_error.restype = C.c_char_p
         L.orc_get_pointmass.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.orc_set_fargo_velocity.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
         _lib = L
     return _lib
 
@@ -115,6 +116,12 @@ class Oracle:
         st = abi.Status()
         lib().orc_get_status(self.h, C.byref(st))
         return st
+
+    def set_fargo_velocity(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        rc = lib().orc_set_fargo_velocity(self.h, _ptr(w), w.size)
+        if rc:
+            raise RuntimeError("orc_set_fargo_velocity failed (%d)" % rc)
 
     def pointmass(self):
         """(mass, mdot) of the central point mass (accretion bookkeeping)."""

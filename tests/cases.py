@@ -105,6 +105,18 @@ def _disk_fargo(n=(32, 48), geometry=abi.LOGCYLINDRICAL, seed=51, variables=abi.
     return c, p, extra
 
 
+def _disk_fargo2(n=(32, 40), geometry=abi.CYLINDRICAL, seed=61):
+    """FARGO type 2: the user supplies w, here the Keplerian velocity at the cell centres."""
+    c, p, extra = _disk_fargo(n=n, geometry=geometry, seed=seed,
+                              bcs=[abi.NO_GRADIENTS, abi.REFLECTING, abi.PERIODIC, abi.PERIODIC])
+    c.fargo_method = 2
+    X, _, _, _ = problems.centers(c)
+    x = X[0, 0, :]
+    r = np.exp(x) if geometry == abi.LOGCYLINDRICAL else x
+    extra["fargo_w"] = np.sqrt(1.0 / r)
+    return c, p, extra
+
+
 def _iso3d(n=(18, 16, 20), seed=41):
     c = abi.default_config()
     c.inum, c.jnum, c.knum = n
@@ -164,6 +176,7 @@ CASES = {
     "disk_fargo_cyl_cons_reflect": lambda: _disk_fargo(geometry=abi.CYLINDRICAL, n=(36, 40), variables=abi.CONSERVATIVE,
                                                        bcs=[abi.REFLECTING, abi.NO_GRADIENTS, abi.PERIODIC, abi.PERIODIC],
                                                        limiter=abi.MONOCENT),
+    "disk_fargo2_user_w": lambda: _disk_fargo2(),
     "disk_fargo_order1_minmod": lambda: _disk_fargo(n=(30, 44), tdorder=1, limiter=abi.MINMOD,
                                                     bcs=[abi.REFLECTING, abi.REFLECTING, abi.PERIODIC, abi.PERIODIC]),
 }

@@ -29,6 +29,8 @@ def main():
         if "bccsound" in extra:
             o.set_sound_speeds(np.broadcast_to(extra["bccsound"], o.shape),
                                np.broadcast_to(extra["fcsound"], (4,) + o.shape))
+        if "fargo_w" in extra:
+            o.set_fargo_velocity(extra["fargo_w"])
         o.set_state(abi.PVAR, p)
         o.first_step()
         for _ in range(STEPS):

@@ -62,7 +62,7 @@ def _cfg(**kw):
     (dict(jnum=1), abi.EUNSUPPORTED),
     (dict(fluxtype=2), abi.EBADCFG),
     # FARGO: type 1 along y on 2D isothermal meshes with the fixed-step Shu-Osher scheme only
-    (dict(physics=abi.EULER_ISOTHERM, csiso=1.0, fargo_method=2, fargo_direction=2), abi.EUNSUPPORTED),
+    (dict(physics=abi.EULER_ISOTHERM, csiso=1.0, fargo_method=3, fargo_direction=2), abi.EUNSUPPORTED),
     (dict(physics=abi.EULER_ISOTHERM, csiso=1.0, fargo_method=1, fargo_direction=1), abi.EUNSUPPORTED),
     (dict(fargo_method=1, fargo_direction=2), abi.EUNSUPPORTED),
     (dict(physics=abi.EULER_ISOTHERM, csiso=1.0, fargo_method=1, fargo_direction=2, method=abi.DORMAND_PRINCE,

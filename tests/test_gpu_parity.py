@@ -50,6 +50,9 @@ def _pair(name, exact):
         fcs = np.broadcast_to(extra["fcsound"], (4,) + shape)
         o.set_sound_speeds(bcc, fcs)
         g.set_sound_speeds(bcc, fcs)
+    if "fargo_w" in extra:
+        o.set_fargo_velocity(extra["fargo_w"])
+        g.set_fargo_velocity(extra["fargo_w"])
     o.set_state(abi.PVAR, p)
     g.set_state(abi.PVAR, p)
     return cfg, o, g

@@ -23,6 +23,8 @@ def _run(cfg, p, steps, extra=None):
     if extra and "bccsound" in extra:
         o.set_sound_speeds(np.broadcast_to(extra["bccsound"], o.shape),
                            np.broadcast_to(extra["fcsound"], (4,) + o.shape))
+    if extra and "fargo_w" in extra:
+        o.set_fargo_velocity(extra["fargo_w"])
     o.set_state(abi.PVAR, p)
     assert o.first_step() == 0
     for _ in range(steps):
