@@ -165,6 +165,9 @@ int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
       return fail(FGPU_EBADCFG, "batch members differ in dimensionality, physics, reconstruction variables or order");
     if (h->device != h0->device) return fail(FGPU_EBADCFG, "batch members live on different devices");
     if (!h->first_done) return fail(FGPU_EBADCFG, "call fgpu_first_step on every member before batching");
+    if (h->pre_rt != h->roundtrip_cfg)
+      return fail(FGPU_EBADCFG, "an ideal-gas member whose checkdata lacks CHECK_PMIN must take its first step "
+                                "alone (FirstStep's CHECK_ALL round trip)");
     b->m.push_back(h);
   }
   cudaSetDevice(h0->device);

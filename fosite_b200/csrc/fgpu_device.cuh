@@ -54,6 +54,8 @@ struct Chain {
   int n;
   const double* w[4];   // background velocity by padded i
   double s[4];          // +1 add, -1 subtract
+  int rt;               // k > 0: the CHECK_PMIN round trip P2C(MAX(C2P(c),pmin)) before element k-1
+                        // (k = n+1: after the last); 0: none
 };
 
 // The stage input state at a cell: base - coef[0]*K[0] - coef[1]*K[1] - ...
@@ -74,9 +76,29 @@ struct StateRef {
   int ready;
 };
 
+// One frame change of a conservative 2D state c by s*w (s = +1 add, -1 subtract).  With
+// the energy (V = 4, ideal gas) the energy goes first, with the old momentum:
+// E + s*w*(m + s*rho*w/2), then m + s*rho*w (physics_euler.f90:2003-2047, 2159-2203);
+// multiplying by s = +-1 is exact, so both signs round like the reference's two forms.
+template <int V>
+__device__ __forceinline__ void frame_change(double* c, double s, double w) {
+  if (V == 4) c[3] = c[3] + s * (w * (c[2] + s * (0.5 * c[0] * w)));
+  c[2] = c[2] + s * (c[0] * w);
+}
 // apply a frame-change chain to the conservative state c of a cell in padded column ip
+// (rt_fn performs the round trip on c when the chain has one)
+template <int V, class RT>
+__device__ __forceinline__ void apply_chain(const Chain& C, double* c, int ip, RT&& rt_fn) {
+  for (int q = 0; q < C.n; ++q) {
+    if (C.rt == q + 1) rt_fn(c);
+    frame_change<V>(c, C.s[q], C.w[q][ip]);
+  }
+  if (C.rt == C.n + 1) rt_fn(c);
+}
+// chains without a round trip (the frame of a stage input)
+template <int V>
 __device__ __forceinline__ void apply_chain(const Chain& C, double* c, int ip) {
-  for (int q = 0; q < C.n; ++q) c[2] = c[2] + C.s[q] * (c[0] * C.w[q][ip]);
+  apply_chain<V>(C, c, ip, [](double*) {});
 }
 
 // Device control block for device-resident stepping.
@@ -247,7 +269,7 @@ struct Cells {
       for (int l = 0; l < V; ++l) p[l] = u[l];
       return;
     }
-    if (ND == 2 && !EU && S.pre.n) apply_chain(S.pre, u, i + 2);
+    if (ND == 2 && S.pre.n) apply_chain<V>(S.pre, u, i + 2);
     PH::c2p(u, p, P);
   }
 

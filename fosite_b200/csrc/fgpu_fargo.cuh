@@ -29,8 +29,9 @@ struct FargoWArgs {
 // rows its threads evaluate the WR x WX terms in parallel into shared memory,
 // then one thread per column adds them in order.
 constexpr int FW_WX = 8, FW_WY = 32, FW_RPT = 4, FW_WR = FW_WY * FW_RPT;
+template <bool EU>
 __global__ void __launch_bounds__(FW_WX* FW_WY) fargo_w_kernel(const __grid_constant__ FargoWArgs A) {
-  using CE = Cells<2, false>;
+  using CE = Cells<2, EU>;
   __shared__ double terms[FW_WR][FW_WX + 1];
   if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
   const Grid& g = A.g;
@@ -48,7 +49,7 @@ __global__ void __launch_bounds__(FW_WX* FW_WY) fargo_w_kernel(const __grid_cons
       const int q = ty + FW_WY * r, j = j0 + q;
       double t = 0.0;
       if (valid && j < g.ny) {
-        double p[3];
+        double p[Phys<2, EU>::V];
         if (ghost) CE::face_ghost_p(A.in, g, A.ph, A.mt, 0, i, j, 0, p);
         else CE::interior_p(A.in, g, A.ph, i, j, 0, p);
         double vy = p[2];
@@ -97,11 +98,11 @@ __device__ __forceinline__ double fargo_minmod(double a, double b) {
 // writes each result to its shifted row.  The same pass evaluates the closing
 // ComputeRHS's CheckData (real frame) and CalcTimestep's wave speeds
 // (co-moving frame) of the interior cells.
-template <int TX, int TY>
+template <bool EU, int TX, int TY>
 __global__ void __launch_bounds__(TX* TY) fargo_advect_kernel(const __grid_constant__ FargoAdvArgs A) {
-  using PH = Phys<2, false>;
-  using CE = Cells<2, false>;
-  constexpr int V = 3;
+  using PH = Phys<2, EU>;
+  using CE = Cells<2, EU>;
+  constexpr int V = PH::V;
   constexpr int NT = TX * TY;
   __shared__ double sred[4 * ((NT + 31) / 32)];
   if (A.ctl->stop | A.ctl->brk) return;
@@ -162,15 +163,17 @@ __global__ void __launch_bounds__(TX* TY) fargo_advect_kernel(const __grid_const
       double c[V], p[V];
 #pragma unroll
       for (int v = 0; v < V; ++v) c[v] = u[v];
-      c[2] = c[2] + c[0] * w;
+      frame_change<V>(c, 1.0, w);
       PH::c2p(c, p, P);
-      if ((A.checkdata & 0x01) && !(cs > 0.)) flags |= 0x01;
+      const double csc = EU ? PH::cs_of(p, P) : cs;
+      if ((A.checkdata & 0x01) && !(csc > 0.)) flags |= 0x01;
+      if (EU && (A.checkdata & 0x02) && p[V - 1] < P.pmin) flags |= 0x02;
       if ((A.checkdata & 0x04) && p[0] < P.rhomin) flags |= 0x04;
       if (A.checkdata & 0x08)
         for (int v = 0; v < V; ++v) if (!isfinite(p[v]) || !isfinite(c[v])) flags |= 0x08;
       p[2] = p[2] - w;
       double v3[3];
-      CE::cfl_cell(p, cs, M, ip, v3);
+      CE::cfl_cell(p, csc, M, ip, v3);
       cflv = dmax(cflv, v3[0]);
 #pragma unroll
       for (int r = 0; r < 4; ++r)

@@ -140,7 +140,8 @@ struct fgpu_handle {
   long long iter = -1, n_adj = 0;
   int checkflags = 0;
   bool first_done = false;
-  bool state_pre = false;       // buffer P holds a state whose fosite cvar is its CHECK_PMIN round trip
+  bool pre_rt = false;          // buffer P holds a state whose fosite cvar is its CHECK_PMIN round trip
+                                // (after FirstStep's CHECK_ALL, and after steps when checkdata has PMIN)
   // graph of G Shu-Osher steps
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
@@ -548,11 +549,11 @@ StageArgs shu_osher_stage(fgpu_handle* h, int n) {
   double* Bbuf = h->buf[2];
   const double* in = n == 1 ? P : ((n - 1) % 2 == 1 ? Abuf : Bbuf);
   StageArgs A = base_args(h);
-  A.in = plain_state(in, n == 1 && h->roundtrip_cfg);
+  A.in = plain_state(in, n == 1 && h->pre_rt);
   A.out_mode = OUT_SSPRK;
   A.eta = kEta[h->order - 1][n - 1];
   A.y0 = P;
-  A.y0_roundtrip = h->roundtrip_cfg ? 1 : 0;
+  A.y0_roundtrip = h->pre_rt ? 1 : 0;
   A.dt_dev = &h->d_ctl->dt;
   A.out = (n == h->order && h->order > 1) ? P : ((n % 2 == 1) ? Abuf : Bbuf);
   if (n == h->order) { A.cfl_mode = 1; A.cfl_roundtrip = h->roundtrip_cfg ? 1 : 0; }
@@ -593,6 +594,7 @@ int enqueue_shu_osher_step(fgpu_handle* h) {
     CUDA_TRY(h, cudaMemcpyAsync(h->buf[0], h->buf[1], sizeof(double) * h->V * h->g.n, cudaMemcpyDeviceToDevice,
                                 h->stream));
   BndArgs B = bnd_args(h, h->buf[0], h->roundtrip_cfg, FIN_STEP);
+  h->pre_rt = h->roundtrip_cfg;   // the end-of-step ComputeRHS uses the checkdata mask
   return launch_misc(h, 0, B);
 }
 
@@ -626,7 +628,8 @@ int launch_fargo_w(fgpu_handle* h, const StateRef& in, const double* w_prev, dou
   F.ctl = h->d_ctl;
   return timed_launch(h, false, 0.0, [&] {
     unsigned blocks = (unsigned)((h->g.nx + 4 + FW_WX - 1) / FW_WX);
-    fargo_w_kernel<<<blocks, FW_WX * FW_WY, 0, h->stream>>>(F);
+    if (h->euler) fargo_w_kernel<true><<<blocks, FW_WX * FW_WY, 0, h->stream>>>(F);
+    else fargo_w_kernel<false><<<blocks, FW_WX * FW_WY, 0, h->stream>>>(F);
     CUDA_TRY(h, cudaGetLastError());
     return FGPU_OK;
   });
@@ -645,7 +648,8 @@ int launch_fargo_advect(fgpu_handle* h, const double* in, double* out, const dou
   return timed_launch(h, false, 0.0, [&] {
     constexpr int TX = 32, TY = 4;
     dim3 grid((h->g.nx + TX - 1) / TX, (h->g.ny + TY * X.chunk - 1) / (TY * X.chunk));
-    fargo_advect_kernel<TX, TY><<<grid, TX * TY, 0, h->stream>>>(X);
+    if (h->euler) fargo_advect_kernel<true, TX, TY><<<grid, TX * TY, 0, h->stream>>>(X);
+    else fargo_advect_kernel<false, TX, TY><<<grid, TX * TY, 0, h->stream>>>(X);
     CUDA_TRY(h, cudaGetLastError());
     return FGPU_OK;
   });
@@ -673,11 +677,13 @@ int enqueue_fargo_step(fgpu_handle* h) {
     S.pre = pre;
     if (int rc = launch_fargo_w(h, S, W, Wn)) return rc;
   }
-  const Chain cold = chain_add(pre, W, -1.0);
+  // after FirstStep an ideal-gas cvar is the CHECK_ALL round trip of the stored state
+  Chain cold = chain_add(pre, W, -1.0);
+  if (h->pre_rt) cold.rt = 1;
   const double* in = P;
   for (int n = 1; n <= h->order; ++n) {
     StageArgs A = base_args(h);
-    A.in = plain_state(in, false);
+    A.in = plain_state(in, n == 1 && h->pre_rt);
     if (n == 1) {
       A.in.pre = pre;
       A.w_sub = W;
@@ -707,6 +713,7 @@ int enqueue_fargo_step(fgpu_handle* h) {
   if (int rc = launch_misc(h, 0, B)) return rc;
   if (dyn) CUDA_TRY(h, cudaMemcpyAsync(h->d_w, Wn, sizeof(double) * h->nxp, cudaMemcpyDeviceToDevice, h->stream));
   h->fargo_phase = 2;
+  h->pre_rt = h->roundtrip_cfg;
   return FGPU_OK;
 }
 
@@ -738,7 +745,7 @@ void sync_from_ctl(fgpu_handle* h) {
 }
 
 // ---------------------------------------------------------------- Butcher engine (host clock)
-int enqueue_k1(fgpu_handle* h, bool from_pre, bool cfl) {
+int enqueue_k1(fgpu_handle* h, bool from_pre, bool cfl, bool rt, int checkdata) {
   // ComputeRHS of the current state into K1.  from_pre: the stored state in P
   // gets the end-of-step CHECK_ALL treatment and its round trip goes to the
   // base buffer (cold = cvar); otherwise RejectSolution's CHECK_NOTHING RHS of base.
@@ -749,8 +756,9 @@ int enqueue_k1(fgpu_handle* h, bool from_pre, bool cfl) {
   A.out_mode = OUT_RHS;
   A.out = K1;
   if (from_pre) {
-    A.in = plain_state(P, h->roundtrip_cfg);
+    A.in = plain_state(P, rt);
     A.out_base = base;
+    A.checkdata = checkdata;
     if (cfl) A.cfl_mode = 2;
   } else {
     A.in = plain_state(base, false);
@@ -871,8 +879,9 @@ int butcher_attempt(fgpu_handle* h, double dtv, double& err) {
   return FGPU_OK;
 }
 
-int finish_cfl_host(fgpu_handle* h, const double* state, bool roundtrip, double& dtcfl) {
+int finish_cfl_host(fgpu_handle* h, const double* state, bool roundtrip, double& dtcfl, int checkdata) {
   BndArgs B = bnd_args(h, state, roundtrip, FIN_NONE);
+  B.checkdata = checkdata;
   if (int rc = launch_misc(h, 0, B)) return rc;
   if (int rc = read_ctl(h)) return rc;
   double invdt = ctl_invdt(h);
@@ -902,14 +911,14 @@ int butcher_integration_step(fgpu_handle* h) {
     if (e != e) h->brk = true;
     else if (e > DBL_MAX) h->brk = true;
     else if (e >= 1.0) {   // RejectSolution: cvar = cold, RHS with CHECK_NOTHING
-      if (int rc = enqueue_k1(h, false, false)) return rc;
+      if (int rc = enqueue_k1(h, false, false, false, h->cfg.checkdata)) return rc;
       h->n_adj++;
       h->dtcause = FGPU_DTCAUSE_ERRADJ;
       if (d < h->dtmin) h->dtmin = d;
     } else {               // AcceptSolution
       t = t + dtold_;
       if (t < h->time + h->dt) {
-        if (int rc = enqueue_k1(h, true, false)) return rc;
+        if (int rc = enqueue_k1(h, true, false, h->roundtrip_cfg, h->cfg.checkdata)) return rc;
         rhs_done_at_t = true;
       }
       h->iter++;
@@ -926,8 +935,8 @@ int butcher_integration_step(fgpu_handle* h) {
       CUDA_TRY(h, cudaMemcpyAsync(h->buf[0], h->buf[1], sizeof(double) * h->V * h->g.n, cudaMemcpyDeviceToDevice,
                                   h->stream));
     }
-    if (int rc = enqueue_k1(h, true, true)) return rc;
-    h->state_pre = true;
+    if (int rc = enqueue_k1(h, true, true, h->roundtrip_cfg, h->cfg.checkdata)) return rc;
+    h->pre_rt = h->roundtrip_cfg;
   }
   return FGPU_OK;
 }
@@ -1007,7 +1016,10 @@ int validate(fgpu_handle* h) {
       return set_err(h, FGPU_EUNSUPPORTED, "fargo: types 1 (computed) and 2 (user-supplied) background velocity only; "
                                            "type 3 needs the shearing-box sources");
     if (c.fargo_direction != 2) return set_err(h, FGPU_EUNSUPPORTED, "fargo: only transport along y (direction 2) is supported");
-    if (h->nd != 2 || h->euler) return set_err(h, FGPU_EUNSUPPORTED, "fargo: 2D x-y meshes with isothermal physics only");
+    if (h->nd != 2) return set_err(h, FGPU_EUNSUPPORTED, "fargo: 2D x-y meshes only");
+    if (h->roundtrip_cfg)
+      return set_err(h, FGPU_EUNSUPPORTED, "fargo with ideal-gas physics: checkdata without CHECK_PMIN "
+                                           "(its round trip sits between the frame changes)");
     if (h->butcher) return set_err(h, FGPU_EUNSUPPORTED, "fargo: fixed-step modified Euler (Shu-Osher) time stepping only");
     h->fargo = true;
   }
@@ -1237,7 +1249,7 @@ int fgpu_upload_state(fgpu_handle* h, int which, const double* data, int64_t n) 
   }
   CUDA_TRY(h, cudaGetLastError());
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-  h->state_pre = false;
+  h->pre_rt = false;
   // FARGO: after FirstStep an uploaded cvar is in the co-moving frame (what fgpu_download
   // returns); it takes the place of the transported state of the last step
   if (h->fargo && h->fargo_phase >= 1) h->fargo_phase = 2;
@@ -1280,7 +1292,7 @@ int fgpu_download(fgpu_handle* h, int which, double* out, int64_t n) {
   if (n < nc * h->V) return set_err(h, FGPU_EARG, "output too small");
   if (!h->d_pad) CUDA_TRY(h, cudaMalloc(&h->d_pad, sizeof(double) * 2 * nc * h->V));
   CUDA_TRY(h, cudaMemsetAsync(h->d_pad, 0, sizeof(double) * 2 * nc * h->V, h->stream));
-  bool rt = h->state_pre && h->roundtrip_cfg;
+  bool rt = h->pre_rt;
   BndArgs B = bnd_args(h, h->buf[0], rt, FIN_NONE);
   if (h->fargo) { B.in.pre = fargo_pre(h); B.w_sub = h->d_w; }
   B.ctl = nullptr;
@@ -1301,13 +1313,16 @@ int fgpu_first_step(fgpu_handle* h) {
   h->first_done = true;
   h->iter = 0;
   h->time = h->cfg.starttime;
+  // fosite%FirstStep's ComputeRHS checks with CHECK_ALL whatever the checkdata mask
+  // (fosite.f90:315-321): ideal-gas states get the CHECK_PMIN round trip here
+  const bool rt_first = h->euler;
   if (h->butcher) {
-    if (int rc = enqueue_k1(h, true, true)) return rc;
+    if (int rc = enqueue_k1(h, true, true, rt_first, FGPU_CHECK_ALL)) return rc;
     double dtc;
-    if (int rc = finish_cfl_host(h, h->buf[0], h->roundtrip_cfg, dtc)) return rc;
+    if (int rc = finish_cfl_host(h, h->buf[0], rt_first, dtc, FGPU_CHECK_ALL)) return rc;
     h->dt = dtc;
     h->dtcause = 0;
-    h->state_pre = true;
+    h->pre_rt = rt_first;
     if (h->brk) return set_err(h, FGPU_BREAK, "FirstStep: Initial data invalid!");
     // first fosite%Step clip happens in fgpu_step
     return FGPU_OK;
@@ -1318,7 +1333,8 @@ int fgpu_first_step(fgpu_handle* h) {
   c->stoptime = h->stoptime; c->tout = h->tout; c->cfl = h->cfl; c->dtlimit = h->dtlimit;
   c->time = h->cfg.starttime; c->dtmin = h->stoptime; c->iter = 0;
   if (int rc = write_ctl(h)) return rc;
-  BndArgs B = bnd_args(h, h->buf[0], h->roundtrip_cfg, FIN_FIRST);
+  BndArgs B = bnd_args(h, h->buf[0], rt_first, FIN_FIRST);
+  B.checkdata = FGPU_CHECK_ALL;
   if (h->fargo) {
     // FirstStep's CenterBoundary + CalcBackgroundVelocity (fosite.f90:315-321), then the
     // CFL of its ComputeRHS on the co-moving state
@@ -1332,7 +1348,7 @@ int fgpu_first_step(fgpu_handle* h) {
   if (int rc = launch_misc(h, 0, B)) return rc;
   if (int rc = read_ctl(h)) return rc;
   sync_from_ctl(h);
-  h->state_pre = true;
+  h->pre_rt = rt_first;
   if (h->brk) return set_err(h, FGPU_BREAK, "FirstStep: Initial data invalid!");
   return FGPU_OK;
 }
@@ -1345,7 +1361,7 @@ static int butcher_step(fgpu_handle* h) {
   if (int rc = butcher_integration_step(h)) return rc;
   if (h->brk) return FGPU_BREAK;
   double dtc;
-  if (int rc = finish_cfl_host(h, h->buf[0], h->roundtrip_cfg, dtc)) return rc;
+  if (int rc = finish_cfl_host(h, h->buf[0], h->roundtrip_cfg, dtc, h->cfg.checkdata)) return rc;
   if (h->brk) return FGPU_BREAK;
   h->dt = dtc;
   h->dtcause = 0;
@@ -1367,9 +1383,10 @@ int fgpu_run(fgpu_handle* h, int64_t n, int64_t* done) {
   }
   // device clock: graph of G steps, replayed
   long long it0 = h->iter;
-  if (h->fargo && h->fargo_phase < 2 && n > 0) {
-    // the first FARGO step after FirstStep has its own frame chains: direct launches
-    if (int rc = enqueue_fargo_step(h)) return rc;
+  if (n > 0 && ((h->fargo && h->fargo_phase < 2) || h->pre_rt != h->roundtrip_cfg)) {
+    // the first step after FirstStep has its own frame chains (FARGO) or round trip
+    // (FirstStep checks with CHECK_ALL): direct launches, the graph covers the rest
+    if (int rc = enqueue_step(h)) return rc;
     n -= 1;
   }
   const int G = 16;
@@ -1412,7 +1429,7 @@ int fgpu_compute_rhs(fgpu_handle* h) {
   // so between steps they are free scratch (m >= 3 for all tableaus)
   double* out = h->butcher ? h->buf[2 + h->T.m - 1] : h->buf[1];
   double* scratch = h->butcher ? h->buf[2 + h->T.m - 2] : h->buf[2];
-  if (h->state_pre && h->roundtrip_cfg) {
+  if (h->pre_rt) {
     if (int rc = launch_roundtrip(h, P, scratch)) return rc;
     src = scratch;
   }
@@ -1434,7 +1451,7 @@ int fgpu_compute_rhs(fgpu_handle* h) {
 
 int fgpu_calc_timestep(fgpu_handle* h, double* dt) {
   if (!h || !dt) return FGPU_EARG;
-  bool rt = h->state_pre && h->roundtrip_cfg;
+  bool rt = h->pre_rt;
   Ctl save = *h->h_ctl;
   if (int rc = read_ctl(h)) return rc;
   save = *h->h_ctl;

@@ -142,7 +142,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
   const MetricP& M = A.mt;
   const double dt = A.dt_dev ? *A.dt_dev : A.dt;
   const bool roundtrip = EU && A.in.roundtrip;
-  constexpr bool FG = ND == 2 && !EU;   // FARGO transforms are compiled for 2D isothermal physics only
+  constexpr bool FG = ND == 2;   // FARGO transforms are compiled for 2D meshes only
   const int tid = threadIdx.x;
   const int tx = tid % TX, ty = tid / TX;
   const int i0 = bx * TX, j0 = by * TY;
@@ -158,6 +158,13 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
   auto FX = [&](int v, int r, int c) -> double& { return Fx[(v * TY + r) * (TX + 1) + c]; };
   auto FY = [&](int v, int r, int c) -> double& { return Fy[(v * (TY + 1) + r) * TX + c]; };
 
+  // the CHECK_PMIN round trip of a conservative state, P2C(MAX(C2P(c),pmin))
+  auto rt_cons = [&](double* c) {
+    double q[V];
+    PH::c2p(c, q, P);
+    if (EU) q[V - 1] = dmax(q[V - 1], P.pmin);
+    PH::p2c(q, c, P);
+  };
   // reconstruction variables at a cross point (interior or face ghost)
   const StateRef& SR = A.rin.base ? A.rin : A.in;
   auto recon_at = [&](int gi, int gj, int gk, double* R) {
@@ -171,7 +178,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
         for (int l = 0; l < V; ++l) R[l] = u[l];
         return;
       }
-      if (FG && A.in.pre.n) apply_chain(A.in.pre, u, gi + 2);
+      if (FG && A.in.pre.n) apply_chain<V>(A.in.pre, u, gi + 2);
       if (PRIM) {
         PH::c2p(u, p, P);
         if (roundtrip) p[V - 1] = dmax(p[V - 1], P.pmin);
@@ -182,10 +189,11 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
         PH::c2p(u, p, P);
         p[V - 1] = dmax(p[V - 1], P.pmin);
         PH::p2c(p, R, P);
+        if (FG && A.w_sub) frame_change<V>(R, -1.0, A.w_sub[gi + 2]);
       } else {
 #pragma unroll
         for (int l = 0; l < V; ++l) R[l] = u[l];
-        if (FG && A.w_sub) R[2] = R[2] - R[0] * A.w_sub[gi + 2];
+        if (FG && A.w_sub) frame_change<V>(R, -1.0, A.w_sub[gi + 2]);
       }
     } else {
       int d = !inx ? 0 : (!iny ? 1 : 2);
@@ -197,7 +205,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
         for (int l = 0; l < V; ++l) R[l] = p[l];
       } else {
         PH::p2c(p, R, P);
-        if (FG && A.w_sub) R[2] = R[2] - R[0] * A.w_sub[gi + 2];
+        if (FG && A.w_sub) frame_change<V>(R, -1.0, A.w_sub[gi + 2]);
       }
     }
   };
@@ -376,7 +384,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
         for (int v = 0; v < V; ++v) pc[v] = R0[v];
         // the sources read cvar itself (the stage state), which Prim2Cons(pvar) only
         // reproduces to rounding; after the CHECK_PMIN round trip cvar is Prim2Cons(pvar)
-        if (!roundtrip && (M.curv || A.has_accel)) state_at<V>(A.in, g.n, idx, cc);
+        if (!roundtrip && (M.curv || A.has_accel || A.out_base)) state_at<V>(A.in, g.n, idx, cc);
         else PH::p2c(pc, cc, P);
       } else {
 #pragma unroll
@@ -398,22 +406,36 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
       const bool fsrc = FG && A.w_sub;
       if (fsrc) {
         state_at<V>(A.in, g.n, idx, cc);
-        if (A.in.pre.n) apply_chain(A.in.pre, cc, ip);
+        if (A.in.pre.n) apply_chain<V>(A.in.pre, cc, ip);
         PH::c2p(cc, pc, P);
+        if (roundtrip) {   // CHECK_PMIN of this ComputeRHS (FirstStep's CHECK_ALL)
+          pc[V - 1] = dmax(pc[V - 1], P.pmin);
+          PH::p2c(pc, cc, P);
+        }
       }
       // geometric sources (physics_euler.f90:1706-1847 / physics_eulerisotherm.f90:689-832)
       double geo2 = 0.0;
       if (M.curv && ND == 2 && fsrc) {
-        double Pp = pc[0] * (M.cs[ip] * M.cs[ip]);
+        double Pp = EU ? pc[V - 1] : pc[0] * (M.cs[ip] * M.cs[ip]);
         double vx = pc[1], vy = pc[2];
         double cxyx = M.cxyx[ip], cyxy = M.cyxy[ip], czxz = M.czxz[ip], czyz = M.czyz[ip];
         rhs[1] = rhs[1] - (cc[2] * (cyxy * vy - cxyx * vx) + (cyxy + czxz) * Pp);
         geo2 = cc[1] * (cxyx * vx - cyxy * vy) + (cxyx + czyz) * Pp;
       }
       if (fsrc) {
-        // AddFargoSourcesY (physics_eulerisotherm.f90:1531-1586) into the geometric source
-        geo2 = geo2 - cc[1] * 0.5 * (A.w_sub[ip + 1] - A.w_sub[ip - 1]) / M.dlx[ip];
+        // AddFargoSourcesY into the geometric source (isothermal
+        // physics_eulerisotherm.f90:1531-1586; Euler physics_euler.f90:2368-2455 adds the
+        // energy term -vy*(tmp + GetGeometricalSourceY(vz = P = mz = 0)))
+        const double tmp = cc[1] * 0.5 * (A.w_sub[ip + 1] - A.w_sub[ip - 1]) / M.dlx[ip];
+        geo2 = geo2 - tmp;
         rhs[2] = rhs[2] - geo2;
+        if (EU) {
+          const double vx = pc[1], vy = pc[2];
+          const double cxyx = M.cxyx[ip], cyxy = M.cyxy[ip], cyzy = M.cyzy[ip], czyz = M.czyz[ip];
+          const double gy = 0.0 * (czyz * 0.0 - cyzy * vy) + cc[1] * (cxyx * vx - cyxy * vy) + (cxyx + czyz) * 0.0;
+          const double geoE = 0.0 - vy * (tmp + gy);
+          rhs[V - 1] = rhs[V - 1] - geoE;
+        }
       } else if (M.curv) {
         double Pp = EU ? pc[V - 1] : pc[0] * (M.cs[ip] * M.cs[ip]);
         double vx = pc[1], vy = pc[2];
@@ -446,7 +468,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
         double yn[V], y0[V], y[V];
         if (FG && A.yn_chain.n) {
           state_at<V>(A.in, g.n, idx, yn);
-          apply_chain(A.yn_chain, yn, ip);
+          apply_chain<V>(A.yn_chain, yn, ip, rt_cons);
         } else if (!PRIM) {
 #pragma unroll
           for (int v = 0; v < V; ++v) yn[v] = cc[v];
@@ -458,7 +480,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
         }
 #pragma unroll
         for (int v = 0; v < V; ++v) y0[v] = __ldg(A.y0 + (long long)v * g.n + idx);
-        if (FG && A.y0_chain.n) apply_chain(A.y0_chain, y0, ip);
+        if (FG && A.y0_chain.n) apply_chain<V>(A.y0_chain, y0, ip, rt_cons);
         if (EU && A.y0_roundtrip) {
           double q[V];
           PH::c2p(y0, q, P);

@@ -29,10 +29,10 @@ struct BndArgs {
 // to the co-moving frame, SubtractBackgroundVelocityY (physics_eulerisotherm.f90:1336-1413)
 template <int ND, bool EU>
 __device__ __forceinline__ void to_comoving(const double* w_sub, int ip, double* p, double* c) {
-  if (ND == 2 && !EU && w_sub) {
+  if (ND == 2 && w_sub) {
     double w = w_sub[ip];
     p[2] = p[2] - w;
-    c[2] = c[2] - c[0] * w;
+    frame_change<Phys<ND, EU>::V>(c, -1.0, w);
   }
 }
 
@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(256) interior_cfl_kernel(const __grid_constant
     int i = (int)(t % A.g.nx);
     double u[V], p[V], c[V];
     state_at<V>(A.in, A.g.n, t, u);
-    if (ND == 2 && !EU && A.in.pre.n) apply_chain(A.in.pre, u, i + 2);
+    if (ND == 2 && A.in.pre.n) apply_chain<V>(A.in.pre, u, i + 2);
     PH::c2p(u, p, A.ph);
     if (EU && A.roundtrip) { p[V - 1] = dmax(p[V - 1], A.ph.pmin); PH::p2c(p, c, A.ph); }
     else { for (int v = 0; v < V; ++v) c[v] = u[v]; }
@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(256) pack_interior_kernel(const __grid_constan
     int j = (int)(r % A.g.ny), k = (int)(r / A.g.ny);
     double u[V], p[V], c[V];
     state_at<V>(A.in, A.g.n, t, u);
-    if (ND == 2 && !EU && A.in.pre.n) apply_chain(A.in.pre, u, i + 2);
+    if (ND == 2 && A.in.pre.n) apply_chain<V>(A.in.pre, u, i + 2);
     PH::c2p(u, p, A.ph);
     if (EU && A.roundtrip) { p[V - 1] = dmax(p[V - 1], A.ph.pmin); PH::p2c(p, c, A.ph); }
     else { for (int v = 0; v < V; ++v) c[v] = u[v]; }

@@ -305,7 +305,7 @@ __global__ void __launch_bounds__(32 * NW, 2) stage2_kernel(const __grid_constan
 #pragma unroll
         for (int v = 0; v < V; ++v) pc[v] = Rc[v];
         // the sources read cvar itself (see stage_tile)
-        if (!roundtrip && (M.curv || A.has_accel)) state_at<V>(A.in, g.n, idx, cc);
+        if (!roundtrip && (M.curv || A.has_accel || A.out_base)) state_at<V>(A.in, g.n, idx, cc);
         else PH::p2c(pc, cc, P);
       } else {
 #pragma unroll

@@ -167,8 +167,8 @@ struct Oracle {
       // types 1 (w computed every step) and 2 (w supplied by the user, fixed); type 3
       // (shearing box) needs the shearing-box sources
       if (fargo != 1 && fargo != 2) { err = "fargo: types 1 and 2 only"; return FGPU_EUNSUPPORTED; }
+      if (euler && (cfg.checkdata & FGPU_CHECK_PMIN)) { err = "fargo with ideal-gas physics: checkdata without CHECK_PMIN"; return FGPU_EUNSUPPORTED; }
       if (cfg.fargo_direction != 2 || NDIMS < 2) { err = "fargo: only direction 2 supported"; return FGPU_EUNSUPPORTED; }
-      if (euler) { err = "fargo: isothermal physics only"; return FGPU_EUNSUPPORTED; }
       if (NDIMS != 2 || dirs[0] != 0 || dirs[1] != 1) { err = "fargo: 2D x-y meshes only"; return FGPU_EUNSUPPORTED; }
       w.assign((long)NI * NK, 0.0); wfactor.assign((long)NI * NK, 0.0); delxy.assign((long)NI * NK, 0.0);
       shift.assign((long)NI * NK, 0);
@@ -645,7 +645,8 @@ struct Oracle {
   }
 
   // ---------------------------------------------------------------- fargo (direction 2)
-  // physics_eulerisotherm.f90:1263-1413 Add/SubtractBackgroundVelocityY
+  // Add/SubtractBackgroundVelocityY: isothermal physics_eulerisotherm.f90:1263-1413,
+  // Euler physics_euler.f90:2003-2047,2159-2203 (the energy first, with the old momentum)
   long widx(int i, int k) const { return (long)(i - IGMIN) + (long)NI * (k - KGMIN); }
   void add_bg(std::vector<double>& pv, std::vector<double>& cv) {
     if (!c_trans) return;
@@ -653,6 +654,7 @@ struct Oracle {
     int vi = 2;   // x-y plane: y velocity is component 2 (variable index 2)
     for (int k = KGMIN; k <= KGMAX; ++k) for (int j = JGMIN; j <= JGMAX; ++j) for (int i = IGMIN; i <= IGMAX; ++i) {
       long c = id(i, j, k); double wv = w[widx(i, k)];
+      if (euler) cv[c + NC * PRESSURE] = cv[c + NC * PRESSURE] + wv * (cv[c + NC * vi] + 0.5 * cv[c] * wv);
       pv[c + NC * vi] = pv[c + NC * vi] + wv;
       cv[c + NC * vi] = cv[c + NC * vi] + cv[c] * wv;
     }
@@ -664,6 +666,7 @@ struct Oracle {
     int vi = 2;
     for (int k = KGMIN; k <= KGMAX; ++k) for (int j = JGMIN; j <= JGMAX; ++j) for (int i = IGMIN; i <= IGMAX; ++i) {
       long c = id(i, j, k); double wv = w[widx(i, k)];
+      if (euler) cv[c + NC * PRESSURE] = cv[c + NC * PRESSURE] - wv * (cv[c + NC * vi] - 0.5 * cv[c] * wv);
       pv[c + NC * vi] = pv[c + NC * vi] - wv;
       cv[c + NC * vi] = cv[c + NC * vi] - cv[c] * wv;
     }
@@ -679,11 +682,22 @@ struct Oracle {
       w[widx(i, k)] = wi / JNUM;
     }
   }
-  // physics_eulerisotherm.f90:1531-1586 AddFargoSourcesY (x-y momentum)
-  void add_fargo_sources(std::vector<double>& cv, std::vector<double>& sterm) {
+  // AddFargoSourcesY (x-y momentum): isothermal physics_eulerisotherm.f90:1531-1586;
+  // Euler physics_euler.f90:2368-2455 adds the energy term -vy*(tmp + GetGeometricalSourceY
+  // with vz = P = mz = 0), physics_euler.f90:3139-3147
+  void add_fargo_sources(std::vector<double>& pv, std::vector<double>& cv, std::vector<double>& sterm) {
     for (int k = KMIN; k <= KMAX; ++k) for (int j = JMIN; j <= JMAX; ++j) for (int i = IMIN; i <= IMAX; ++i) {
       long c = id(i, j, k);
-      sterm[c + NC * 2] = sterm[c + NC * 2] - cv[c + NC * 1] * 0.5 * (w[widx(i + 1, k)] - w[widx(i - 1, k)]) / dlx[c];
+      if (!euler) {
+        sterm[c + NC * 2] = sterm[c + NC * 2] - cv[c + NC * 1] * 0.5 * (w[widx(i + 1, k)] - w[widx(i - 1, k)]) / dlx[c];
+      } else {
+        double tmp = cv[c + NC * 1] * 0.5 * (w[widx(i + 1, k)] - w[widx(i - 1, k)]) / dlx[c];
+        sterm[c + NC * 2] = sterm[c + NC * 2] - tmp;
+        double vx = pv[c + NC * 1], vy = pv[c + NC * 2], mx = cv[c + NC * 1];
+        double g = 0.0 * (czyz[c] * 0.0 - cyzy[c] * vy) + mx * (cxyx[c] * vx - cyxy[c] * vy) + (cxyx[c] + czyz[c]) * 0.0;
+        tmp = tmp + g;
+        sterm[c + NC * PRESSURE] = sterm[c + NC * PRESSURE] - vy * tmp;
+      }
     }
   }
   // timedisc_base.f90:1935-2069 FargoAdvectionY
@@ -957,7 +971,7 @@ struct Oracle {
     external_sources(cv, src);
     if (fargo) {
       if (cfg.geometry == FGPU_CARTESIAN) std::fill(geo_src.begin(), geo_src.end(), 0.0);
-      add_fargo_sources(cv, geo_src);
+      add_fargo_sources(pv, cv, geo_src);
       sub_bg(pv, cv);
     }
     calculate_fluxes(pv, cv);

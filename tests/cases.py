@@ -117,6 +117,39 @@ def _disk_fargo2(n=(32, 40), geometry=abi.CYLINDRICAL, seed=61):
     return c, p, extra
 
 
+def _euler_fargo(n=(36, 40), geometry=abi.CARTESIAN, variables=abi.CONSERVATIVE, fargo=1, seed=71):
+    """Ideal-gas FARGO: a sheared box (Cartesian) or an adiabatic disk around a point mass
+    (cylindrical); CHECK_PMIN off (its round trip sits between the frame changes)."""
+    if geometry == abi.CARTESIAN:
+        c, p, extra = _khi(n=n, variables=variables, seed=seed,
+                           bcs=[abi.REFLECTING, abi.NO_GRADIENTS, abi.PERIODIC, abi.PERIODIC])
+        X, Y, _, _ = problems.centers(c)
+        rng = np.random.default_rng(seed)
+        p[2] = 1.5 + 0.8 * X + 0.01 * rng.uniform(-1, 1, X.shape)
+        p[1] = 0.02 * rng.uniform(-1, 1, X.shape)
+    else:
+        c, p0, extra = problems.disk2d(nr=n[0], nphi=n[1], seed=seed, geometry=geometry, fargo=0)
+        c.physics = abi.EULER
+        c.gamma = 1.4
+        c.variables = variables
+        c.bc[abi.WEST] = abi.NO_GRADIENTS
+        c.bc[abi.EAST] = abi.REFLECTING
+        abi.finalize_config(c)
+        X, _, _, _ = problems.centers(c)
+        r = X
+        rng = np.random.default_rng(seed)
+        p = np.zeros((4,) + X.shape)
+        p[0] = p0[0]
+        p[1] = 0.01 * rng.uniform(-1, 1, X.shape)
+        p[2] = p0[2]
+        p[3] = p0[0] * (0.05 ** 2 / r)
+        extra = {}
+    c.fargo_method = fargo
+    c.fargo_direction = 2
+    c.checkdata = abi.CHECK_ALL & ~abi.CHECK_PMIN
+    return c, p, extra
+
+
 def _iso3d(n=(18, 16, 20), seed=41):
     c = abi.default_config()
     c.inum, c.jnum, c.knum = n
@@ -143,6 +176,13 @@ def _iso3d(n=(18, 16, 20), seed=41):
     return c, p, {}
 
 
+def _with(case, **kw):
+    c, p, extra = case
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c, p, extra
+
+
 CASES = {
     "khi_ssprk3_vanleer_cons": lambda: _khi(),
     "khi_ssprk3_mc_prim": lambda: _khi(limiter=abi.MONOCENT, variables=abi.PRIMITIVE, theta=1.2),
@@ -156,6 +196,9 @@ CASES = {
                                                  method=abi.SSPRK, tdorder=5, n=(30, 26)),
     "euler2d_rkf45": lambda: _khi(method=abi.RK_FEHLBERG, tdorder=5, n=(28, 30)),
     "khi_modeuler_adaptive3": lambda: _khi(me_tol=1e-3),
+    "khi_checkdata_no_pmin": lambda: _with(_khi(variables=abi.PRIMITIVE, n=(30, 28)),
+                                           checkdata=abi.CHECK_ALL & ~abi.CHECK_PMIN),
+    "gauss3d_dopri_no_pmin": lambda: _with(_gauss3d(n=(12, 14, 10)), checkdata=abi.CHECK_NOTHING),
     "khi_modeuler_adaptive2_mc_prim": lambda: _khi(tdorder=2, me_tol=1e-3, limiter=abi.MONOCENT,
                                                   variables=abi.PRIMITIVE, n=(34, 30)),
     "gauss3d_dopri_mc_prim": lambda: _gauss3d(),
@@ -177,6 +220,8 @@ CASES = {
                                                        bcs=[abi.REFLECTING, abi.NO_GRADIENTS, abi.PERIODIC, abi.PERIODIC],
                                                        limiter=abi.MONOCENT),
     "disk_fargo2_user_w": lambda: _disk_fargo2(),
+    "euler_fargo_shear_cons": lambda: _euler_fargo(),
+    "euler_fargo_disk_cyl_prim": lambda: _euler_fargo(n=(24, 160), geometry=abi.CYLINDRICAL, variables=abi.PRIMITIVE),
     "disk_fargo_order1_minmod": lambda: _disk_fargo(n=(30, 44), tdorder=1, limiter=abi.MINMOD,
                                                     bcs=[abi.REFLECTING, abi.REFLECTING, abi.PERIODIC, abi.PERIODIC]),
 }
