@@ -862,13 +862,44 @@ int butcher_attempt(fgpu_handle* h, double dtv, double& err) {
     }
     A.out_mode = OUT_RHS;
     A.out = h->buf[2 + m - 1];
-    if (m == T.m) {
+    const bool fused_end = m == T.m && !h->materialize;
+    if (fused_end) {
       A.last_stage = 1;
       A.nstage = T.m;
       for (int q = 0; q < T.m; ++q) { A.bh_dt[q] = T.bh[q] * dtv; A.bl_dt[q] = T.bl[q] * dtv; }
       A.out_high = P;
     }
     if (int rc = launch_stage(h, A)) return rc;
+    if (m == T.m && !fused_end) {
+      // the high/low combination and error norm as a streaming pass (the stencil kernel
+      // keeps its registers for the stencil)
+      CombineArgs Cb;
+      std::memset(&Cb, 0, sizeof(Cb));
+      Cb.base = base;
+      for (int q = 0; q < T.m; ++q) {
+        Cb.K[q] = h->buf[2 + q];
+        Cb.bh_dt[q] = T.bh[q] * dtv;
+        Cb.bl_dt[q] = T.bl[q] * dtv;
+      }
+      Cb.nstage = T.m;
+      Cb.out_high = P;
+      Cb.tol_rel = h->tol_rel;
+      for (int v = 0; v < FGPU_MAXV; ++v) Cb.tol_abs[v] = h->tol_abs[v];
+      Cb.n = h->g.n;
+      Cb.ctl = h->d_ctl;
+      const unsigned blocks = (unsigned)std::min<long long>((h->g.n + 255) / 256, 148 * 8);
+      // algorithmic bytes: the new state written (base and k reads are counted with the stage)
+      int rc = timed_launch(h, 2, (double)h->V * h->g.n * 8.0, [&] {
+        switch (h->V) {
+          case 3: combine_kernel<3><<<blocks, 256, 0, h->stream>>>(Cb); break;
+          case 4: combine_kernel<4><<<blocks, 256, 0, h->stream>>>(Cb); break;
+          default: combine_kernel<5><<<blocks, 256, 0, h->stream>>>(Cb); break;
+        }
+        CUDA_TRY(h, cudaGetLastError());
+        return FGPU_OK;
+      });
+      if (rc) return rc;
+    }
   }
   if (int rc = read_ctl(h)) return rc;
   double e;

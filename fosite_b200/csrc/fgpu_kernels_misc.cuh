@@ -287,6 +287,45 @@ __global__ void __launch_bounds__(256) accrete_kernel(const __grid_constant__ Ac
   for (int q = threadIdx.x; q < A.naccel; q += blockDim.x) A.accel[q] = A.accel[q] * f;
 }
 
+// The end of a Butcher attempt as a streaming pass (timedisc_rkfehlberg.f90:198-265 and
+// ComputeError, timedisc_base.f90:1012-1053): high and low order solutions
+// base - sum b_q dt k_q in the reference's order, the high one written as the new
+// state, max |h-l|/(tol_rel|h| + tol_abs) reduced into ctl->err.  Same arithmetic as
+// the fused last-stage epilogue of the stage kernel.
+struct CombineArgs {
+  const double* base;
+  const double* K[FGPU_MAXK];
+  double bh_dt[FGPU_MAXK], bl_dt[FGPU_MAXK];
+  int nstage;
+  double* out_high;
+  double tol_rel;
+  double tol_abs[FGPU_MAXV];
+  long long n;
+  Ctl* ctl;
+};
+template <int V>
+__global__ void __launch_bounds__(256) combine_kernel(const __grid_constant__ CombineArgs A) {
+  __shared__ double sred[4 * 8];
+  double errv = 0.0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < A.n; t += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const double b = __ldg(A.base + (long long)v * A.n + t);
+      double h = b, l = b;
+      for (int q = 0; q < A.nstage; ++q) {
+        const double kq = __ldg(A.K[q] + (long long)v * A.n + t);
+        l = l - A.bl_dt[q] * kq;
+        h = h - A.bh_dt[q] * kq;
+      }
+      A.out_high[(long long)v * A.n + t] = h;
+      const double e = fabs(h - l) / (A.tol_rel * fabs(h) + A.tol_abs[v]);
+      errv = dmax(errv, e);
+    }
+  }
+  double vals[3] = {errv, 0.0, 0.0};
+  block_reduce_emit<256>(vals, 1, 0, &A.ctl->err, nullptr, sred);
+}
+
 // Pointwise Shu-Osher update with a stored RHS (the first stage of the adaptive
 // modified Euler scheme, whose RHS is the step's k1): out = yn - dt*r + eta*(y0 - yn + dt*r)
 // (timedisc_modeuler.f90:279-291), over n values.
