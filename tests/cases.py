@@ -176,6 +176,60 @@ def _iso3d(n=(18, 16, 20), seed=41):
     return c, p, {}
 
 
+def khi3d(perm=(0, 1, 2), n=8, tsim=30.0, seed=17):
+    """tests/KHI3D.f90: a periodic 3D shear layer (flow along axis a, density and velocity
+    jump across axis b), Euler gamma 1.4, KT + MC(theta 1.2) on conservative variables,
+    SSPRK3 with CFL 0.4, no viscosity.  perm maps the base orientation (flow along x,
+    jump across y) to another axis order; the same seeded velocity noise is permuted
+    with it, so the six runs are images of each other.  Returns (cfg, pvar, perm)."""
+    c = abi.default_config()
+    c.inum = c.jnum = c.knum = n
+    c.xmin, c.xmax, c.ymin, c.ymax, c.zmin, c.zmax = -0.5, 0.5, -0.5, 0.5, -0.5, 0.5
+    for f in range(6):
+        c.bc[f] = abi.PERIODIC
+    c.physics = abi.EULER
+    c.gamma = 1.4
+    c.limiter = abi.MONOCENT
+    c.theta = 1.2
+    c.variables = abi.CONSERVATIVE
+    c.method = abi.MODIFIED_EULER
+    c.tdorder = 3
+    c.tol_rel = 10.0
+    c.cfl = 0.4
+    c.stoptime = tsim
+    c.dtlimit = 1e-10
+    abi.finalize_config(c)
+    X, Y, Z, _ = problems.centers(c)
+    rng = np.random.default_rng(seed)
+    dv = rng.uniform(0.0, 1.0, (3,) + X.shape)
+    # base orientation in [v, z, y, x] order: flow along x, jump across y
+    inner = ~((Y < -0.25) | (Y > 0.25))
+    base = np.zeros((5,) + X.shape)
+    base[0] = np.where(inner, 2.0, 1.0)
+    base[1] = np.where(inner, 0.5, -0.5)
+    base[4] = 2.5
+    base[1:4] = base[1:4] + (dv - 0.5) * 0.2
+    return c, permute_state(base, perm), perm
+
+
+def permute_state(p, perm):
+    """Relabel axes: new axis a carries old axis perm[a] (coordinates and velocity
+    components); arrays are [v, z, y, x]."""
+    spatial = [2 - perm[2 - d] for d in range(3)]       # array axis order (z, y, x)
+    q = p[:, :, :, :].transpose([0] + [1 + s for s in spatial])
+    out = q.copy()
+    for a in range(3):
+        out[1 + a] = q[1 + perm[a]]
+    return out
+
+
+def inverse_perm(perm):
+    inv = [0, 0, 0]
+    for a, b in enumerate(perm):
+        inv[b] = a
+    return tuple(inv)
+
+
 def _with(case, **kw):
     c, p, extra = case
     for k, v in kw.items():

@@ -201,3 +201,31 @@ def test_khi_transposition_symmetry():
     ra, rb = a.get(abi.PVAR), b.get(abi.PVAR)
     rbt = np.stack([rb[0].transpose(0, 2, 1), rb[2].transpose(0, 2, 1), rb[1].transpose(0, 2, 1), rb[3].transpose(0, 2, 1)])
     assert np.sqrt(np.mean((ra - rbt) ** 2)) < abi.TINY
+
+
+@pytest.mark.gpu
+def test_khi3d_orientation_symmetry_gpu():
+    """tests/KHI3D.f90:260-266 on the device: six orientations, TSIM = 30, RMS < 4 EPSILON
+    (the --fmad=false build; contraction of a*a + b*b is not symmetric in a, b), and the
+    base orientation equal to the oracle's run bit for bit."""
+    from fosite_b200.sim import Simulation
+    from cases import khi3d, permute_state, inverse_perm
+    runs = {}
+    for perm in [(0, 1, 2), (1, 0, 2), (2, 1, 0), (0, 2, 1), (1, 2, 0), (2, 0, 1)]:
+        cfg, p, _ = khi3d(perm)
+        g = Simulation(cfg, exact=True)
+        g.set_state(abi.PVAR, p)
+        g.first_step()
+        rc, done = g.run(100000)
+        assert rc == abi.STOPTIME and done > 900
+        runs[perm] = permute_state(g.get(abi.PVAR), inverse_perm(perm))
+    base = runs[(0, 1, 2)]
+    for perm, r in runs.items():
+        assert np.sqrt(np.mean((r - base) ** 2)) < 4 * np.finfo(float).eps, perm
+    cfg, p, _ = khi3d((0, 1, 2))
+    o = pyoracle.Oracle(cfg)
+    o.set_state(abi.PVAR, p)
+    o.first_step()
+    while o.step() == 0:
+        pass
+    assert np.array_equal(o.get(abi.PVAR), base)
