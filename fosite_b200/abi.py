@@ -22,6 +22,9 @@ CHECK_NOTHING, CHECK_CSOUND, CHECK_PMIN, CHECK_RHOMIN, CHECK_INVALID, CHECK_TMIN
 OK, BREAK, STOPTIME = 0, 1, 2
 EBADCFG, ENOMEM, ECUDA, ETIMEOUT, EUNSUPPORTED, EARG = -1, -2, -3, -4, -5, -6
 
+DTCAUSE_CFL, DTCAUSE_ERRADJ, DTCAUSE_SMALLERR, DTCAUSE_FILEIO, DTCAUSE_VISCOSITY = 0, -1, -2, -4, 3
+VIS_MOLECULAR, VIS_ALPHA, VIS_BETA, VIS_POWERLAW, VIS_ALPHA_ALT = 1, 2, 3, 4, 5
+
 CVAR, PVAR, RHS, BCCSOUND = 1, 2, 3, 4
 MESH_X, MESH_Y, MESH_Z, MESH_RADIUS = 10, 11, 12, 13
 
@@ -57,6 +60,9 @@ class Config(C.Structure):
         ("tout", C.c_double),
         ("pm_outbound", C.c_int32), ("pad_", C.c_int32),
         ("starttime", C.c_double),
+        ("vismodel", C.c_int32), ("pad2_", C.c_int32),
+        ("dynconst", C.c_double), ("bulkconst", C.c_double),
+        ("vis_exponent", C.c_double), ("cvis", C.c_double),
     ]
 
 
@@ -114,6 +120,11 @@ def default_config():
     c.fargo_method = 0
     c.fargo_direction = 0
     c.tout = 0.0
+    c.vismodel = 0
+    c.dynconst = 0.1
+    c.bulkconst = float("nan")   # fosite's default -2/3*dynconst
+    c.vis_exponent = 0.0
+    c.cvis = 0.5
     return c
 
 

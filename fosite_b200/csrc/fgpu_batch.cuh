@@ -160,6 +160,7 @@ int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
     if (h->butcher) return fail(FGPU_EUNSUPPORTED, "batch members use the fixed-step modified Euler scheme");
     if (h->fargo) return fail(FGPU_EUNSUPPORTED, "batch members without FARGO transport");
     if (h->accrete) return fail(FGPU_EUNSUPPORTED, "batch members without point-mass accretion");
+    if (h->vis) return fail(FGPU_EUNSUPPORTED, "batch members without the viscosity source");
     if (h->order < 2) return fail(FGPU_EUNSUPPORTED, "batch members of time order 2 or 3");
     if (h->nd != b->nd || h->euler != b->euler || h->prim != b->prim || h->order != b->order)
       return fail(FGPU_EBADCFG, "batch members differ in dimensionality, physics, reconstruction variables or order");
@@ -331,11 +332,12 @@ int fgpu_autotune(fgpu_handle* h, int reps, int* variant) {
   A.out_mode = OUT_RHS;
   A.out = scratch;
   A.ctl = nullptr;
+  A.visc = h->vis ? h->d_visc : nullptr;   // the stencil's read of the viscous source
   const int cand[5] = {0, 2, 3, 4, 1};
   double best = 1e300;
   int bv = h->variant, keep = h->variant;
   for (int v : cand) {
-    if (v == 1 && (h->fargo || h->accrete)) continue;   // layout 1 lacks these features
+    if (v == 1 && (h->fargo || h->accrete || h->vis)) continue;   // layout 1 lacks these features
     h->variant = v;
     int rc = FGPU_OK;
     double ms = time_launches(h->stream, reps, [&] { if (!rc) rc = launch_stage_raw(h, A); });

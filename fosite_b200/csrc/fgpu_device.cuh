@@ -40,8 +40,11 @@ struct MetricP {
   const double *offzB, *offzT;               // by padded k
   const double *accel;                       // [ndim][nx+4] point-mass acceleration or null
   const double *cs;                          // [7][nx+4] isothermal sound speed: C,W,E,S,N,B,T
+  const double *dAxE;                        // dAxdydz(i,E) (the N/S and T/B areas share the centre's x)
   int nxp;                                   // nx + 4
   int curv;                                  // geometric sources active
+  int vis;                                   // molecular viscosity: viscous time-step limit in cfl_cell
+  double vis_eta;                            // its constant dynamic viscosity
 };
 
 // A sequence of FARGO frame changes of the y momentum, m_y = m_y + s_q*(rho*w_q(i)),
@@ -103,13 +106,15 @@ __device__ __forceinline__ void apply_chain(const Chain& C, double* c, int ip) {
 
 // Device control block for device-resident stepping.
 struct Ctl {
-  unsigned long long invdt[3];   // CFL partial maxima (bits of non-negative doubles)
+  unsigned long long invdt[4];   // CFL partial maxima (bits of non-negative doubles); [3] viscous
   unsigned long long err;        // error-norm partial maximum
   int flags;                     // CheckData failures (FGPU_CHECK_* bits)
   unsigned int blocks_done;      // last-block detection of the boundary kernel
   double time, dt, dtold, dtmin, stoptime, tout, cfl, dtlimit;
   long long iter;
   int stop, brk, dtcause, pad;
+  double cvis;                   // viscous Courant number (vis = 1)
+  int vis, pad2;
 };
 
 enum { BC_NOGRAD = 0x01, BC_PERIODIC = 0x02, BC_REFLECTING = 0x03, BC_ABSORBING = 0x0D };
@@ -441,18 +446,29 @@ struct Cells {
 
   // CFL contribution of one cell (CalcWaveSpeeds_center + CalcTimestep,
   // physics_eulerisotherm.f90:530-552, timedisc_base.f90:860-893).
-  // ip = padded i; out[0] = 2D sum or x; out[1], out[2] for 3D.
+  // ip = padded i; out[0] = 2D sum or x; out[1], out[2] for 3D; out[3] the inverse
+  // viscous time step of sources_viscosity.f90:532-575, sum over the directions of
+  // (max wave speed + 2*kinvis/dl)/dl with kinvis = dynvis/density (0 without viscosity).
   static __device__ __forceinline__ void cfl_cell(const double* p, double cs, const MetricP& M, int ip, double* out) {
     double dl[3] = {M.dlx[ip], M.dly[ip], ND == 3 ? M.dlz[ip] : 1.0};
-    double a[3];
+    double w[3], a[3];
 #pragma unroll
     for (int m = 0; m < ND; ++m) {
       double v = p[1 + m];
       double mn = dmin(0., v - cs), mx = dmax(0., v + cs);
-      a[m] = dmax(mx, -mn) / dl[m];
+      w[m] = dmax(mx, -mn);
+      a[m] = w[m] / dl[m];
     }
     if (ND == 2) { out[0] = a[0] + a[1]; out[1] = 0.0; out[2] = 0.0; }
     else { out[0] = a[0]; out[1] = a[1]; out[2] = a[2]; }
+    out[3] = 0.0;
+    if (M.vis) {
+      const double kinvis = M.vis_eta / p[0];
+      double s = (w[0] + 2.0 * kinvis / dl[0]) / dl[0];
+#pragma unroll
+      for (int m = 1; m < ND; ++m) s = s + (w[m] + 2.0 * kinvis / dl[m]) / dl[m];
+      out[3] = s;
+    }
   }
 };
 

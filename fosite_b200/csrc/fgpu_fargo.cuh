@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(TX* TY) fargo_advect_kernel(const __grid_const
   using CE = Cells<2, EU>;
   constexpr int V = PH::V;
   constexpr int NT = TX * TY;
-  __shared__ double sred[4 * ((NT + 31) / 32)];
+  __shared__ double sred[RED_STRIDE * ((NT + 31) / 32)];
   if (A.ctl->stop | A.ctl->brk) return;
   const Grid& g = A.g;
   const PhysP& P = A.ph;
@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(TX* TY) fargo_advect_kernel(const __grid_const
   const int i = blockIdx.x * TX + tx;
   const int j0 = (blockIdx.y * TY + ty) * A.chunk;
   const int j1 = min(g.ny, j0 + A.chunk);
-  double cflv = 0.0;
+  double cflv = 0.0, cflvis = 0.0;
   int flags = 0;
   if (i < g.nx && j0 < g.ny) {
     const int ip = i + 2;
@@ -172,17 +172,18 @@ __global__ void __launch_bounds__(TX* TY) fargo_advect_kernel(const __grid_const
       if (A.checkdata & 0x08)
         for (int v = 0; v < V; ++v) if (!isfinite(p[v]) || !isfinite(c[v])) flags |= 0x08;
       p[2] = p[2] - w;
-      double v3[3];
+      double v3[4];
       CE::cfl_cell(p, csc, M, ip, v3);
       cflv = dmax(cflv, v3[0]);
+      cflvis = dmax(cflvis, v3[3]);
 #pragma unroll
       for (int r = 0; r < 4; ++r)
 #pragma unroll
         for (int v = 0; v < V; ++v) q[r][v] = q[r + 1][v];
     }
   }
-  double vals[3] = {cflv, 0.0, 0.0};
-  block_reduce_emit<NT>(vals, 1, flags, A.ctl->invdt, &A.ctl->flags, sred);
+  double vals[4] = {cflv, 0.0, 0.0, cflvis};
+  block_reduce_emit<NT>(vals, M.vis ? 4 : 1, flags, A.ctl->invdt, &A.ctl->flags, sred);
 }
 
 }  // namespace fgpu

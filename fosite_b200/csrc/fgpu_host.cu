@@ -23,6 +23,7 @@
 #include "fgpu_kernels_misc.cuh"
 #include "fgpu_stage2.cuh"
 #include "fgpu_fargo.cuh"
+#include "fgpu_visc.cuh"
 
 using namespace fgpu;
 
@@ -171,6 +172,10 @@ struct fgpu_handle {
   int acc_face = 0;             // 0 west, 1 east
   double* d_acc = nullptr;
   double dxyz[3] = {1.0, 1.0, 1.0};
+  // molecular viscosity: constants and the viscous source of the current stage state
+  bool vis = false;
+  double vis_eta = 0.0, vis_mub = 0.0, cvis = 0.5;
+  double* d_visc = nullptr;     // [nd (+1 energy)][n]
 };
 
 namespace {
@@ -197,7 +202,7 @@ void scale(int geo, double gp, double x, double& hx, double& hy, double& hz) {
 }
 
 enum { M_dAxW, M_dAyS, M_dAzB, M_dydzdV, M_dzdxdV, M_dxdydV, M_cxyx, M_cxzx, M_cyxy, M_cyzy, M_czxz, M_czyz,
-       M_dlx, M_dly, M_dlz, M_offxW, M_offxE, M_accel0, M_accel1, M_wfac, M_cs0, M_NI = M_cs0 + 7 };
+       M_dlx, M_dly, M_dlz, M_offxW, M_offxE, M_accel0, M_accel1, M_wfac, M_dAxE, M_cs0, M_NI = M_cs0 + 7 };
 
 int build_metric(fgpu_handle* h) {
   const fgpu_config& c = h->cfg;
@@ -237,6 +242,7 @@ int build_metric(fgpu_handle* h) {
     double dydzdV = dy * dz / (volume + DBL_MIN);
     double dzdxdV = dz * dx / (volume + DBL_MIN);
     A(M_dAxW, ip) = hyw * hzw;
+    A(M_dAxE, ip) = hye * hze;
     A(M_dAyS, ip) = hzc * hxc;
     A(M_dAzB, ip) = hxc * hyc;
     A(M_dydzdV, ip) = dydzdV;
@@ -304,8 +310,11 @@ int upload_metric(fgpu_handle* h) {
   M.offzB = b + base_y + 2 * nyp; M.offzT = b + base_y + 2 * nyp + nzp;
   M.accel = h->has_accel ? P(M_accel0) : nullptr;
   M.cs = P(M_cs0);
+  M.dAxE = P(M_dAxE);
   M.nxp = nxp;
   M.curv = h->curv ? 1 : 0;
+  M.vis = h->vis ? 1 : 0;
+  M.vis_eta = h->vis_eta;
   return FGPU_OK;
 }
 
@@ -361,8 +370,9 @@ int launch_stage_t(fgpu_handle* h, StageArgs& A) {
   A.kchunk = h->kchunk;
   const Grid& g = h->g;
   const int kz = ND == 3 ? (g.nz + h->kchunk - 1) / h->kchunk : 1;
-  // the warp-shuffle layout implements neither FARGO frame changes nor the accretion rows
-  const int variant = (h->variant == 1 && (h->fargo || h->accrete)) ? 0 : h->variant;
+  // the warp-shuffle layout implements neither FARGO frame changes, the accretion rows nor
+  // the viscous source
+  const int variant = (h->variant == 1 && (h->fargo || h->accrete || h->vis)) ? 0 : h->variant;
   switch (variant) {
     case 1: {
       // warp-shuffle layout: 32 x 8 points per block, 30 x 6 output cells
@@ -418,7 +428,9 @@ double stage_bytes(const fgpu_handle* h, const StageArgs& A) {
   arrays += 1;
   if (A.out_base) arrays += 1;
   if (A.last_stage && A.out_high) arrays += 1;
-  return (double)arrays * h->V * (double)h->g.n * 8.0;
+  double bytes = (double)arrays * h->V * (double)h->g.n * 8.0;
+  if (A.visc) bytes += (double)(h->nd + (h->euler ? 1 : 0)) * (double)h->g.n * 8.0;
+  return bytes;
 }
 
 template <class F>
@@ -439,7 +451,52 @@ int timed_launch(fgpu_handle* h, int kind, double bytes, F&& fn) {
   return rc;
 }
 
+// Viscous source of the stage state of A into h->d_visc (sources_viscosity.f90:484-507); the
+// stage kernel reads it.  Tiles: 2D 32 x 8, 3D 8 x 8 x 4.
+template <int ND> struct ViscShape;
+template <> struct ViscShape<2> { static constexpr int TX = 32, TY = 8, TZ = 1; };
+template <> struct ViscShape<3> { static constexpr int TX = 8, TY = 8, TZ = 4; };
+template <int ND, bool EU>
+void configure_visc_t() {
+  using S = ViscShape<ND>;
+  cudaFuncSetAttribute(visc_kernel<ND, EU, S::TX, S::TY, S::TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)ViscTile<ND, S::TX, S::TY, S::TZ>::SMEM);
+}
+void configure_visc(int nd, bool e) {
+  if (nd == 2) e ? configure_visc_t<2, true>() : configure_visc_t<2, false>();
+  else e ? configure_visc_t<3, true>() : configure_visc_t<3, false>();
+}
+template <int ND, bool EU>
+void launch_visc_t(fgpu_handle* h, const ViscArgs& V) {
+  using S = ViscShape<ND>;
+  const Grid& g = h->g;
+  dim3 grid((g.nx + S::TX - 1) / S::TX, (g.ny + S::TY - 1) / S::TY, ND == 3 ? (g.nz + S::TZ - 1) / S::TZ : 1);
+  visc_kernel<ND, EU, S::TX, S::TY, S::TZ>
+      <<<grid, S::TX * S::TY * S::TZ, ViscTile<ND, S::TX, S::TY, S::TZ>::SMEM, h->stream>>>(V);
+}
+int launch_visc(fgpu_handle* h, const StateRef& S) {
+  ViscArgs V;
+  std::memset(&V, 0, sizeof(V));
+  V.g = h->g; V.ph = h->ph; V.mt = h->mt;
+  V.in = S;
+  V.eta = h->vis_eta;
+  V.mub = h->vis_mub;
+  V.out = h->d_visc;
+  // algorithmic bytes: the state read once, the source written once
+  const double bytes = (double)(h->V + h->nd + (h->euler ? 1 : 0)) * (double)h->g.n * 8.0;
+  return timed_launch(h, 1, bytes, [&] {
+    if (h->nd == 2) h->euler ? launch_visc_t<2, true>(h, V) : launch_visc_t<2, false>(h, V);
+    else h->euler ? launch_visc_t<3, true>(h, V) : launch_visc_t<3, false>(h, V);
+    CUDA_TRY(h, cudaGetLastError());
+    return FGPU_OK;
+  });
+}
+
 int launch_stage(fgpu_handle* h, StageArgs& A) {
+  if (h->vis) {
+    if (int rc = launch_visc(h, A.rin.base ? A.rin : A.in)) return rc;
+    A.visc = h->d_visc;
+  }
   return timed_launch(h, true, stage_bytes(h, A), [&] { return launch_stage_raw(h, A); });
 }
 int launch_misc(fgpu_handle* h, int which, BndArgs& B) {
@@ -533,6 +590,21 @@ double ctl_invdt(const fgpu_handle* h) {
   if (h->nd == 2) return D(c->invdt[0]);
   double ix = D(c->invdt[0]), iy = D(c->invdt[1]), iz = D(c->invdt[2]);
   return std::max(std::max(iy, iz), ix);
+}
+// CalcTimestep's closing arithmetic on the host: the CFL step (timedisc_base.f90:885-900),
+// then the sources list (sources_generic.f90:264-293) with the viscous limit of
+// sources_viscosity.f90:576-580; *cause receives the dtcause
+double ctl_dt(const fgpu_handle* h, int* cause) {
+  double dt = h->cfl / ctl_invdt(h);
+  *cause = FGPU_DTCAUSE_CFL;
+  if (h->vis) {
+    double iv;
+    std::memcpy(&iv, &h->h_ctl->invdt[3], 8);
+    const double dtv = iv > DBL_MIN ? h->cvis / iv : DBL_MAX;
+    if (dtv < dt) *cause = FGPU_DTCAUSE_VISCOSITY;
+    dt = std::min(dt, dtv);
+  }
+  return dt;
 }
 
 // ---------------------------------------------------------------- Shu-Osher (device clock)
@@ -910,19 +982,18 @@ int butcher_attempt(fgpu_handle* h, double dtv, double& err) {
   return FGPU_OK;
 }
 
-int finish_cfl_host(fgpu_handle* h, const double* state, bool roundtrip, double& dtcfl, int checkdata) {
+int finish_cfl_host(fgpu_handle* h, const double* state, bool roundtrip, double& dtcfl, int checkdata, int& cause) {
   BndArgs B = bnd_args(h, state, roundtrip, FIN_NONE);
   B.checkdata = checkdata;
   if (int rc = launch_misc(h, 0, B)) return rc;
   if (int rc = read_ctl(h)) return rc;
-  double invdt = ctl_invdt(h);
+  dtcfl = ctl_dt(h, &cause);
   h->checkflags |= h->h_ctl->flags;
   if (h->h_ctl->flags) h->brk = true;
   h->h_ctl->flags = 0;
-  h->h_ctl->invdt[0] = h->h_ctl->invdt[1] = h->h_ctl->invdt[2] = 0ULL;
-  CUDA_TRY(h, cudaMemsetAsync(h->d_ctl, 0, sizeof(unsigned long long) * 3, h->stream));
+  h->h_ctl->invdt[0] = h->h_ctl->invdt[1] = h->h_ctl->invdt[2] = h->h_ctl->invdt[3] = 0ULL;
+  CUDA_TRY(h, cudaMemsetAsync(h->d_ctl, 0, sizeof(unsigned long long) * 4, h->stream));
   CUDA_TRY(h, cudaMemsetAsync(&h->d_ctl->flags, 0, sizeof(int), h->stream));
-  dtcfl = h->cfl / invdt;
   return FGPU_OK;
 }
 
@@ -1054,6 +1125,17 @@ int validate(fgpu_handle* h) {
     if (h->butcher) return set_err(h, FGPU_EUNSUPPORTED, "fargo: fixed-step modified Euler (Shu-Osher) time stepping only");
     h->fargo = true;
   }
+  if (c.vismodel != 0) {
+    // sources_viscosity.f90:132-266
+    if (c.vismodel < FGPU_VIS_MOLECULAR || c.vismodel > FGPU_VIS_ALPHA_ALT)
+      return set_err(h, FGPU_EBADCFG, "Viscosity prescription not supported.");
+    if (c.vismodel != FGPU_VIS_MOLECULAR)
+      return set_err(h, FGPU_EUNSUPPORTED, "viscosity: the MOLECULAR (constant) model only");
+    h->vis = true;
+    h->vis_eta = c.dynconst;
+    h->vis_mub = std::isnan(c.bulkconst) ? -2. / 3. * c.dynconst : c.bulkconst;
+    h->cvis = c.cvis;
+  }
   return FGPU_OK;
 }
 
@@ -1085,6 +1167,10 @@ void fgpu_config_init(fgpu_config* c) {
   c->checkdata = FGPU_CHECK_ALL;
   c->pmin = c->rhomin = c->tmin = DBL_MIN;
   c->pm_mass = 1.0;
+  // sources_viscosity.f90:150-166
+  c->dynconst = 0.1;
+  c->bulkconst = std::nan("");
+  c->cvis = 0.5;
 }
 
 int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
@@ -1109,6 +1195,7 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
     if (const char* e = std::getenv("FGPU_MATERIALIZE")) h->materialize = std::atoi(e) != 0;
   }
   if (!rc) configure_stage_kernels(h->nd, h->euler, h->prim);
+  if (!rc && h->vis) configure_visc(h->nd, h->euler);
   if (!rc) rc = build_metric(h);
   if (!rc) {
     h->g.nx = cfg->inum; h->g.ny = cfg->jnum; h->g.nz = h->nd == 3 ? cfg->knum : 1;
@@ -1140,6 +1227,11 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
       cudaMemcpy(h->d_acc, a.data(), sizeof(double) * na, cudaMemcpyHostToDevice);
     }
   }
+  if (!rc && h->vis) {
+    size_t bytes = sizeof(double) * (h->nd + (h->euler ? 1 : 0)) * h->g.n;
+    if (cudaMalloc(&h->d_visc, bytes) != cudaSuccess) rc = set_err(h, FGPU_ENOMEM, "viscous source array");
+    else cudaMemsetAsync(h->d_visc, 0, bytes, h->stream);
+  }
   if (!rc && h->fargo) {
     if (cudaMalloc(&h->d_w, sizeof(double) * 2 * h->nxp) != cudaSuccess) rc = set_err(h, FGPU_ENOMEM, "fargo arrays");
     else cudaMemsetAsync(h->d_w, 0, sizeof(double) * 2 * h->nxp, h->stream);
@@ -1153,6 +1245,7 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
     h->h_ctl->stoptime = h->stoptime; h->h_ctl->tout = h->tout; h->h_ctl->cfl = h->cfl;
     h->h_ctl->dtlimit = h->dtlimit; h->h_ctl->dt = h->stoptime; h->h_ctl->dtmin = h->stoptime;
     h->h_ctl->iter = -1;
+    h->h_ctl->vis = h->vis ? 1 : 0; h->h_ctl->cvis = h->cvis;
     rc = write_ctl(h);
     h->dt = h->stoptime; h->dtold = h->dt; h->dtmin = h->dt;
   }
@@ -1174,6 +1267,7 @@ void fgpu_destroy(fgpu_handle* h) {
   if (h->d_metric) cudaFree(h->d_metric);
   if (h->d_w) cudaFree(h->d_w);
   if (h->d_acc) cudaFree(h->d_acc);
+  if (h->d_visc) cudaFree(h->d_visc);
   if (h->d_ctl) cudaFree(h->d_ctl);
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
   if (h->own_stream) h->stream = h->own_stream;
@@ -1350,9 +1444,10 @@ int fgpu_first_step(fgpu_handle* h) {
   if (h->butcher) {
     if (int rc = enqueue_k1(h, true, true, rt_first, FGPU_CHECK_ALL)) return rc;
     double dtc;
-    if (int rc = finish_cfl_host(h, h->buf[0], rt_first, dtc, FGPU_CHECK_ALL)) return rc;
+    int cause = 0;
+    if (int rc = finish_cfl_host(h, h->buf[0], rt_first, dtc, FGPU_CHECK_ALL, cause)) return rc;
     h->dt = dtc;
-    h->dtcause = 0;
+    h->dtcause = cause;
     h->pre_rt = rt_first;
     if (h->brk) return set_err(h, FGPU_BREAK, "FirstStep: Initial data invalid!");
     // first fosite%Step clip happens in fgpu_step
@@ -1363,6 +1458,7 @@ int fgpu_first_step(fgpu_handle* h) {
   std::memset(c, 0, sizeof(Ctl));
   c->stoptime = h->stoptime; c->tout = h->tout; c->cfl = h->cfl; c->dtlimit = h->dtlimit;
   c->time = h->cfg.starttime; c->dtmin = h->stoptime; c->iter = 0;
+  c->vis = h->vis ? 1 : 0; c->cvis = h->cvis;
   if (int rc = write_ctl(h)) return rc;
   BndArgs B = bnd_args(h, h->buf[0], rt_first, FIN_FIRST);
   B.checkdata = FGPU_CHECK_ALL;
@@ -1392,10 +1488,11 @@ static int butcher_step(fgpu_handle* h) {
   if (int rc = butcher_integration_step(h)) return rc;
   if (h->brk) return FGPU_BREAK;
   double dtc;
-  if (int rc = finish_cfl_host(h, h->buf[0], h->roundtrip_cfg, dtc, h->cfg.checkdata)) return rc;
+  int cause = 0;
+  if (int rc = finish_cfl_host(h, h->buf[0], h->roundtrip_cfg, dtc, h->cfg.checkdata, cause)) return rc;
   if (h->brk) return FGPU_BREAK;
   h->dt = dtc;
-  h->dtcause = 0;
+  h->dtcause = cause;
   return FGPU_OK;
 }
 
@@ -1486,7 +1583,7 @@ int fgpu_calc_timestep(fgpu_handle* h, double* dt) {
   Ctl save = *h->h_ctl;
   if (int rc = read_ctl(h)) return rc;
   save = *h->h_ctl;
-  h->h_ctl->invdt[0] = h->h_ctl->invdt[1] = h->h_ctl->invdt[2] = 0ULL;
+  h->h_ctl->invdt[0] = h->h_ctl->invdt[1] = h->h_ctl->invdt[2] = h->h_ctl->invdt[3] = 0ULL;
   h->h_ctl->flags = 0;
   h->h_ctl->stop = 0; h->h_ctl->brk = 0;
   if (int rc = write_ctl(h)) return rc;
@@ -1495,7 +1592,8 @@ int fgpu_calc_timestep(fgpu_handle* h, double* dt) {
   if (int rc = launch_misc(h, 1, B)) return rc;
   if (int rc = launch_misc(h, 0, B)) return rc;
   if (int rc = read_ctl(h)) return rc;
-  *dt = h->cfl / ctl_invdt(h);
+  int cause = 0;
+  *dt = ctl_dt(h, &cause);
   *h->h_ctl = save;
   return write_ctl(h);
 }
@@ -1632,7 +1730,7 @@ void noalloc_launch(const BndArgs& B, long long n, cudaStream_t s, int nd, doubl
 extern "C" int fgpu_calc_timestep_noalloc(const fgpu_config* cfg, const double* d_cvar, double* d_dt, void* stream) {
   if (!cfg || !d_cvar || !d_dt) return FGPU_EARG;
   const fgpu_config& c = *cfg;
-  if (c.geometry != FGPU_CARTESIAN || c.pointmass || c.fargo_method) return FGPU_EUNSUPPORTED;
+  if (c.geometry != FGPU_CARTESIAN || c.pointmass || c.fargo_method || c.vismodel) return FGPU_EUNSUPPORTED;
   if (c.inum < 2 || c.jnum < 2 || c.knum < 1) return FGPU_EUNSUPPORTED;
   bool euler = c.physics == FGPU_EULER;
   if (!euler && !(c.physics == FGPU_EULER_ISOTHERM && c.csiso > 0.0)) return FGPU_EUNSUPPORTED;
@@ -1662,7 +1760,7 @@ extern "C" int fgpu_calc_timestep_noalloc(const fgpu_config* cfg, const double* 
   double volume = 1.0 * dx * dy * dz;
   double vals[M_NI];
   for (int q = 0; q < M_NI; ++q) vals[q] = 0.0;
-  vals[M_dAxW] = 1.0 * 1.0; vals[M_dAyS] = 1.0 * 1.0; vals[M_dAzB] = 1.0 * 1.0;
+  vals[M_dAxW] = 1.0 * 1.0; vals[M_dAxE] = 1.0 * 1.0; vals[M_dAyS] = 1.0 * 1.0; vals[M_dAzB] = 1.0 * 1.0;
   vals[M_dxdydV] = dx * dy / (volume + DBL_MIN);
   vals[M_dydzdV] = dy * dz / (volume + DBL_MIN);
   vals[M_dzdxdV] = dz * dx / (volume + DBL_MIN);

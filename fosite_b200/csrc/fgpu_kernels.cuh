@@ -74,9 +74,13 @@ struct StageArgs {
   // forming base - sum coef*K and converting at every stencil point.  in stays the
   // stage state for the epilogues.
   StateRef rin;
+  // optional: viscous source of the stage state, [ND momentum (+ energy)][n] (visc_kernel)
+  const double* visc;
 };
 
-// block-wide max of up to 3 non-negative doubles + OR of flags, then one atomic per block
+// block-wide max of up to 4 non-negative doubles + OR of flags, then one atomic per block;
+// sred holds RED_STRIDE doubles per warp
+constexpr int RED_STRIDE = 5;
 template <int NT>
 __device__ __forceinline__ void block_reduce_emit(double* vals, int nv, int flags, unsigned long long* dst,
                                                   int* dflags, double* sred) {
@@ -91,8 +95,8 @@ __device__ __forceinline__ void block_reduce_emit(double* vals, int nv, int flag
   for (int o = 16; o > 0; o >>= 1) flags |= __shfl_xor_sync(0xffffffffu, flags, o);
   __syncthreads();
   if (lane == 0) {
-    for (int q = 0; q < nv; ++q) sred[warp * 4 + q] = vals[q];
-    sred[warp * 4 + 3] = __longlong_as_double((long long)flags);
+    for (int q = 0; q < nv; ++q) sred[warp * RED_STRIDE + q] = vals[q];
+    sred[warp * RED_STRIDE + 4] = __longlong_as_double((long long)flags);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -100,10 +104,10 @@ __device__ __forceinline__ void block_reduce_emit(double* vals, int nv, int flag
     int f = 0;
     for (int q = 0; q < nv; ++q) {
       double m = 0.0;
-      for (int w = 0; w < NW; ++w) m = dmax(m, sred[w * 4 + q]);
+      for (int w = 0; w < NW; ++w) m = dmax(m, sred[w * RED_STRIDE + q]);
       if (dst) atomicMax(dst + q, (unsigned long long)__double_as_longlong(m));
     }
-    for (int w = 0; w < NW; ++w) f |= (int)__double_as_longlong(sred[w * 4 + 3]);
+    for (int w = 0; w < NW; ++w) f |= (int)__double_as_longlong(sred[w * RED_STRIDE + 4]);
     if (f && dflags) atomicOr(dflags, f);
   }
 }
@@ -134,7 +138,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
   double* const Sy = Sx + V * TY * (TX + 2);        // [V][TY+2][TX]   y slopes
   double* const Fx = Sy + V * (TY + 2) * TX;        // [V][TY][TX+1]   x fluxes
   double* const Fy = Fx + V * TY * (TX + 1);        // [V][TY+1][TX]   y fluxes
-  __shared__ double sred[4 * ((NT + 31) / 32)];
+  __shared__ double sred[RED_STRIDE * ((NT + 31) / 32)];
 
   if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
   const Grid& g = A.g;
@@ -211,7 +215,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
   };
 
   const int ip = i + 2;   // padded i of the own cell
-  double cflv[3] = {0.0, 0.0, 0.0};
+  double cflv[4] = {0.0, 0.0, 0.0, 0.0};
   double errv = 0.0;
   int flags = 0;
 
@@ -452,12 +456,31 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
           rhs[3] = rhs[3] - (mx * (cxzx * vx - czxz * vz) + my * (cyzy * vy - czyz * vz) + (cxzx + cyzy) * Pp);
         }
       }
-      // point-mass gravity (gravity_pointmass.f90:263-282, physics ExternalSources)
-      if (A.has_accel) {
-        double ax = M.accel[ip], ay = M.accel[M.nxp + ip];
-        rhs[1] = rhs[1] - cc[0] * ax;
-        rhs[2] = rhs[2] - cc[0] * ay;
-        if (EU) rhs[V - 1] = rhs[V - 1] - (cc[1] * ax + cc[2] * ay);
+      // external sources (sources_generic.f90:220-261): point-mass gravity (gravity_pointmass.f90:
+      // 263-282, physics ExternalSources) first in the list, then the viscous source of this
+      // stage state (precomputed by visc_kernel); rhs = ... - (gravity + viscosity)
+      if (A.has_accel || A.visc) {
+        double sm[ND] = {}, se = 0.0;
+        if (A.has_accel) {
+          const double ax = M.accel[ip], ay = M.accel[M.nxp + ip];
+          sm[0] = cc[0] * ax;
+          sm[1] = cc[0] * ay;
+          if (EU) se = cc[1] * ax + cc[2] * ay;
+        }
+        if (A.visc) {
+#pragma unroll
+          for (int m = 0; m < ND; ++m) {
+            const double sv = __ldg(A.visc + (long long)m * g.n + idx);
+            sm[m] = A.has_accel ? sm[m] + sv : sv;
+          }
+          if (EU) {
+            const double sv = __ldg(A.visc + (long long)ND * g.n + idx);
+            se = A.has_accel ? se + sv : sv;
+          }
+        }
+#pragma unroll
+        for (int m = 0; m < ND; ++m) rhs[1 + m] = rhs[1 + m] - sm[m];
+        if (EU) rhs[V - 1] = rhs[V - 1] - se;
       }
 
       if (A.out_mode == OUT_RHS) {
@@ -510,10 +533,10 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
           PH::c2p(y, p, P);
           if (EU && A.cfl_roundtrip) p[V - 1] = dmax(p[V - 1], P.pmin);
           double cs = EU ? PH::cs_of(p, P) : M.cs[ip];
-          double v3[3];
+          double v3[4];
           CE::cfl_cell(p, cs, M, ip, v3);
 #pragma unroll
-          for (int q = 0; q < 3; ++q) cflv[q] = dmax(cflv[q], v3[q]);
+          for (int q = 0; q < 4; ++q) cflv[q] = dmax(cflv[q], v3[q]);
           if (EU && A.cfl_roundtrip) PH::p2c(p, c, P);
           else { for (int v = 0; v < V; ++v) c[v] = y[v]; }
           if ((A.checkdata & 0x01) && !(cs > 0.)) flags |= 0x01;
@@ -529,10 +552,10 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
       }
       if (A.cfl_mode == 2) {
         double cs = EU ? PH::cs_of(pc, P) : M.cs[ip];
-        double v3[3];
+        double v3[4];
         CE::cfl_cell(pc, cs, M, ip, v3);
 #pragma unroll
-        for (int q = 0; q < 3; ++q) cflv[q] = dmax(cflv[q], v3[q]);
+        for (int q = 0; q < 4; ++q) cflv[q] = dmax(cflv[q], v3[q]);
         if ((A.checkdata & 0x01) && !(cs > 0.)) flags |= 0x01;
         if (EU && (A.checkdata & 0x02) && pc[V - 1] < P.pmin) flags |= 0x02;
         if ((A.checkdata & 0x04) && pc[0] < P.rhomin) flags |= 0x04;
@@ -568,8 +591,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
 
   const bool err_out = A.last_stage || A.err_low;
   if (A.ctl && (A.cfl_mode || err_out)) {
-    int nv = A.cfl_mode ? (ND == 3 ? 3 : 1) : 0;
-    double vals[3] = {cflv[0], cflv[1], cflv[2]};
+    int nv = A.cfl_mode ? (M.vis ? 4 : (ND == 3 ? 3 : 1)) : 0;
+    double vals[4] = {cflv[0], cflv[1], cflv[2], cflv[3]};
     if (err_out && !A.cfl_mode) { vals[0] = errv; nv = 1; }
     if (nv) block_reduce_emit<NT>(vals, nv, flags, err_out && !A.cfl_mode ? &A.ctl->err : A.ctl->invdt,
                                   &A.ctl->flags, sred);

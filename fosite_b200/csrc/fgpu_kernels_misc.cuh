@@ -81,10 +81,18 @@ __device__ void finalize_step(Ctl* c, int mode) {
     double iz = __longlong_as_double((long long)c->invdt[2]);
     invdt = dmax(dmax(iy, iz), ix);
   }
-  c->invdt[0] = c->invdt[1] = c->invdt[2] = 0ULL;
+  const double ivis = __longlong_as_double((long long)c->invdt[3]);
+  c->invdt[0] = c->invdt[1] = c->invdt[2] = c->invdt[3] = 0ULL;
   if (c->brk) { c->stop = 1; return; }
   double dt = c->cfl / invdt;
   int cause = 0;
+  if (c->vis) {
+    // sources list (sources_generic.f90:264-293): the viscous limit (sources_viscosity.f90:
+    // 576-580) replaces dt where smaller, with dtcause = VISCOSITY
+    const double dtv = ivis > DBL_MIN ? c->cvis / ivis : DBL_MAX;
+    if (dtv < dt) cause = 3;
+    dt = dmin(dt, dtv);
+  }
   if (fabs(c->stoptime - c->time) <= 1.0E-05 * c->stoptime) { c->stop = 1; c->dt = dt; c->dtcause = cause; return; }
   double tout = c->tout;
   if ((c->time + dt) / tout > 1.0) { dt = tout - c->time; cause = -4; }
@@ -100,11 +108,11 @@ __device__ __forceinline__ void boundary_block(const BndArgs& A, const int blk, 
   using PH = Phys<ND, EU>;
   using CE = Cells<ND, EU>;
   constexpr int V = PH::V;
-  __shared__ double sred[4 * 8];
+  __shared__ double sred[RED_STRIDE * 8];
   __shared__ bool is_last;
   if (A.ctl && A.finalize != FIN_FIRST && (A.ctl->stop | A.ctl->brk)) return;
   const MetricP& M = A.mt;
-  double cflv[3] = {0.0, 0.0, 0.0};
+  double cflv[4] = {0.0, 0.0, 0.0, 0.0};
   int flags = 0;
   for (long long t = blk * 256LL + threadIdx.x; t < A.nghost; t += nblk * 256LL) {
     int px, py, pz;
@@ -118,10 +126,10 @@ __device__ __forceinline__ void boundary_block(const BndArgs& A, const int blk, 
     if (A.checkdata & 0x08)
       for (int v = 0; v < V; ++v) if (!isfinite(p[v]) || !isfinite(c[v])) flags |= 0x08;
     to_comoving<ND, EU>(A.w_sub, px, p, c);
-    double v3[3];
+    double v3[4];
     CE::cfl_cell(p, cs, M, px, v3);
-    cflv[0] = dmax(cflv[0], v3[0]);
-    if (ND == 3) { cflv[1] = dmax(cflv[1], v3[1]); cflv[2] = dmax(cflv[2], v3[2]); }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) cflv[q] = dmax(cflv[q], v3[q]);
     if (A.out_p) {
       long long pi = px + (long long)(A.g.nx + 4) * (py + (long long)(A.g.ny + 4) * pz);
       for (int v = 0; v < V; ++v) {
@@ -131,7 +139,7 @@ __device__ __forceinline__ void boundary_block(const BndArgs& A, const int blk, 
     }
   }
   if (!A.ctl) return;
-  block_reduce_emit<256>(cflv, ND == 3 ? 3 : 1, flags, A.ctl->invdt, &A.ctl->flags, sred);
+  block_reduce_emit<256>(cflv, M.vis ? 4 : (ND == 3 ? 3 : 1), flags, A.ctl->invdt, &A.ctl->flags, sred);
   if (A.finalize == FIN_NONE) return;
   __threadfence();
   if (threadIdx.x == 0) {
@@ -165,9 +173,9 @@ __global__ void __launch_bounds__(256) interior_cfl_kernel(const __grid_constant
   using PH = Phys<ND, EU>;
   using CE = Cells<ND, EU>;
   constexpr int V = PH::V;
-  __shared__ double sred[4 * 8];
+  __shared__ double sred[RED_STRIDE * 8];
   const MetricP& M = A.mt;
-  double cflv[3] = {0.0, 0.0, 0.0};
+  double cflv[4] = {0.0, 0.0, 0.0, 0.0};
   int flags = 0;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < A.g.n;
        t += (long long)gridDim.x * blockDim.x) {
@@ -185,12 +193,12 @@ __global__ void __launch_bounds__(256) interior_cfl_kernel(const __grid_constant
     if (A.checkdata & 0x08)
       for (int v = 0; v < V; ++v) if (!isfinite(p[v]) || !isfinite(c[v])) flags |= 0x08;
     to_comoving<ND, EU>(A.w_sub, i + 2, p, c);
-    double v3[3];
+    double v3[4];
     CE::cfl_cell(p, cs, M, i + 2, v3);
-    cflv[0] = dmax(cflv[0], v3[0]);
-    if (ND == 3) { cflv[1] = dmax(cflv[1], v3[1]); cflv[2] = dmax(cflv[2], v3[2]); }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) cflv[q] = dmax(cflv[q], v3[q]);
   }
-  block_reduce_emit<256>(cflv, ND == 3 ? 3 : 1, flags, A.ctl->invdt, &A.ctl->flags, sred);
+  block_reduce_emit<256>(cflv, M.vis ? 4 : (ND == 3 ? 3 : 1), flags, A.ctl->invdt, &A.ctl->flags, sred);
 }
 
 // Interior cells of a stored state into padded primitive/conservative arrays.
@@ -305,7 +313,7 @@ struct CombineArgs {
 };
 template <int V>
 __global__ void __launch_bounds__(256) combine_kernel(const __grid_constant__ CombineArgs A) {
-  __shared__ double sred[4 * 8];
+  __shared__ double sred[RED_STRIDE * 8];
   double errv = 0.0;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < A.n; t += (long long)gridDim.x * blockDim.x) {
 #pragma unroll

@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(32 * NW, 2) stage2_kernel(const __grid_constan
   __shared__ double Rs[V * RH * RW];
   __shared__ double Fy[FD * NW * TXO];          // south-face data of rows -1..NW-2
   __shared__ double Gy[V * (NW - 1) * TXO];     // y fluxes of interfaces (r, r+1), r = -1..NW-3
-  __shared__ double sred[4 * NW];
+  __shared__ double sred[RED_STRIDE * NW];
 
   if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
   const Grid& g = A.g;
@@ -373,7 +373,7 @@ __global__ void __launch_bounds__(32 * NW, 2) stage2_kernel(const __grid_constan
           PH::c2p(y, p, P);
           if (EU && A.cfl_roundtrip) p[V - 1] = dmax(p[V - 1], P.pmin);
           double cs = EU ? PH::cs_of(p, P) : M.cs[ip];
-          double v3[3];
+          double v3[4];
           CE::cfl_cell(p, cs, M, ip, v3);
 #pragma unroll
           for (int q = 0; q < 3; ++q) cflv[q] = dmax(cflv[q], v3[q]);
@@ -395,7 +395,7 @@ __global__ void __launch_bounds__(32 * NW, 2) stage2_kernel(const __grid_constan
       }
       if (A.cfl_mode == 2) {
         double cs = EU ? PH::cs_of(pc, P) : M.cs[ip];
-        double v3[3];
+        double v3[4];
         CE::cfl_cell(pc, cs, M, ip, v3);
 #pragma unroll
         for (int q = 0; q < 3; ++q) cflv[q] = dmax(cflv[q], v3[q]);

@@ -85,6 +85,14 @@ extern "C" {
 #define FGPU_DTCAUSE_ERRADJ   -1
 #define FGPU_DTCAUSE_SMALLERR -2
 #define FGPU_DTCAUSE_FILEIO   -4
+/* dtcause of a source term is its source type: sources/sources_generic.f90:71-80 */
+#define FGPU_DTCAUSE_VISCOSITY 3
+/* viscosity models: sources/sources_viscosity.f90:72-76 */
+#define FGPU_VIS_MOLECULAR    1
+#define FGPU_VIS_ALPHA        2
+#define FGPU_VIS_BETA         3
+#define FGPU_VIS_POWERLAW     4
+#define FGPU_VIS_ALPHA_ALT    5
 
 /* ---- return codes ---- */
 #define FGPU_OK               0
@@ -158,6 +166,16 @@ typedef struct fgpu_config {
     /* Timedisc%time at FirstStep ("starttime", timedisc_base.f90:295), e.g. the time of a
      * restart file (examples/restart.f90); default 0 */
     double  starttime;
+    /* viscosity source (sources/sources_viscosity.f90, keys vismodel, dynconst,
+     * bulkconst, exponent, cvis): 0 = off.  FGPU_VIS_MOLECULAR (constant dynamic and
+     * bulk viscosity) on 2D x-y and 3D meshes.  bulkconst NaN (the fgpu_config_init
+     * value) takes fosite's default -2/3*dynconst. */
+    int32_t vismodel;
+    int32_t pad2_;
+    double  dynconst;              /* default 0.1 */
+    double  bulkconst;             /* default NaN = -2/3*dynconst */
+    double  vis_exponent;          /* POWERLAW exponent, default 0 */
+    double  cvis;                  /* viscous Courant number, default 0.5 */
 } fgpu_config;
 
 /* Step bookkeeping returned to the caller (mirrors Timedisc%time/dt/...). */

@@ -92,6 +92,11 @@ struct Oracle {
   std::vector<double> w, wfactor, delxy, fdq, fdql, fflux;
   std::vector<int> shift;
   bool c_trans = false, p_trans = false;     // fargo_transformation_applied flags
+  // ---- viscosity (sources_viscosity.f90, MOLECULAR) ----
+  int vismodel = 0;
+  double dynconst = 0.0, bulkconst = 0.0, cvis = 0.5;
+  std::vector<double> btxx, btxy, btxz, btyy, btyz, btzz;   // stress tensor (InitSources: zero)
+  std::vector<double> vtmp, vtmp1, vtmp2;                     // Physics%tmp, tmp1, tmp2
 
   long id(int i, int j, int k) const {
     return (long)(i - IGMIN) + (long)NI * ((long)(j - JGMIN) + (long)NJ * (long)(k - KGMIN));
@@ -160,6 +165,19 @@ struct Oracle {
       bxo = bxf;
       pm_cur = cfg.pm_mass;
       mdot = 0.0;
+    }
+    // viscosity (sources_viscosity.f90:132-266)
+    if (cfg.vismodel) {
+      if (VDIM < 2) { err = "viscosity is currently not supported in 1D physics"; return FGPU_EBADCFG; }
+      if (cfg.vismodel != FGPU_VIS_MOLECULAR) { err = "viscosity: the MOLECULAR model only"; return FGPU_EUNSUPPORTED; }
+      if (NDIMS == 2 && !(dirs[0] == 0 && dirs[1] == 1)) { err = "viscosity: 2D x-y and 3D meshes only"; return FGPU_EUNSUPPORTED; }
+      vismodel = cfg.vismodel;
+      dynconst = cfg.dynconst;
+      bulkconst = std::isnan(cfg.bulkconst) ? -2. / 3. * dynconst : cfg.bulkconst;
+      cvis = cfg.cvis;
+      btxx.assign(NC, 0.0); btxy.assign(NC, 0.0); btxz.assign(NC, 0.0);
+      btyy.assign(NC, 0.0); btyz.assign(NC, 0.0); btzz.assign(NC, 0.0);
+      vtmp.assign(NC, 0.0); vtmp1.assign(NC, 0.0); vtmp2.assign(NC, 0.0);
     }
     // fargo (timedisc_base.f90:369-452)
     fargo = cfg.fargo_method;
@@ -938,9 +956,145 @@ struct Oracle {
     mdot = bflux;
   }
 
-  // sources_generic.f90:220-261 -> sources_gravity.f90:164-200 -> physics ExternalSources
-  void external_sources(std::vector<double>& cv, std::vector<double>& s) {
+  // ---------------------------------------------------------------- viscosity
+  // mesh_midpoint.f90:586-630 Divergence3D, arguments in the reference's order
+  static double div3d(double aW, double aE, double aS, double aN, double aB, double aT,
+                      double dydzdV_, double dxdzdV_, double dxdydV_,
+                      double c_xyx, double c_xzx, double c_yxy, double c_zxz,
+                      double TxxW, double TxxE, double TxyS, double TxyN, double TxzB, double TxzT,
+                      double TyxC, double TzxC, double TyyC, double TzzC) {
+    return dydzdV_ * (aE * TxxE - aW * TxxW) + dxdzdV_ * (aN * TxyN - aS * TxyS)
+         + dxdydV_ * (aT * TxzT - aB * TxzB) + c_xyx * TyxC + c_xzx * TzxC - c_yxy * TyyC - c_zxz * TzzC;
+  }
+  // VectorDivergence2D_1 (x-y, mesh_midpoint.f90:156-183) / VectorDivergence3D (:474-502)
+  // of the cell-centred vector (ax, ay[, az]) at cell x
+  double vector_divergence(long x, const double* ax, const double* ay, const double* az) const {
+    const long sy = NI, sz = (long)NI * NJ;
+    if (NDIMS == 2)
+      return div3d(dAx[x * 2], dAx[x * 2 + 1], dAy[x * 2], dAy[x * 2 + 1], 0.0, 0.0,
+                   dydzdV[x], dzdxdV[x], 0.0, 0.0, 0.0, 0.0, 0.0,
+                   0.5 * (ax[x - 1] + ax[x]), 0.5 * (ax[x + 1] + ax[x]),
+                   0.5 * (ay[x - sy] + ay[x]), 0.5 * (ay[x + sy] + ay[x]),
+                   0.0, 0.0, 0.0, 0.0, 0.0, 0.0);
+    return div3d(dAx[x * 2], dAx[x * 2 + 1], dAy[x * 2], dAy[x * 2 + 1], dAz[x * 2], dAz[x * 2 + 1],
+                 dydzdV[x], dzdxdV[x], dxdydV[x], 0.0, 0.0, 0.0, 0.0,
+                 0.5 * (ax[x - 1] + ax[x]), 0.5 * (ax[x + 1] + ax[x]),
+                 0.5 * (ay[x - sy] + ay[x]), 0.5 * (ay[x + sy] + ay[x]),
+                 0.5 * (az[x - sz] + az[x]), 0.5 * (az[x + sz] + az[x]),
+                 0.0, 0.0, 0.0, 0.0);
+  }
+  // physics_eulerisotherm.f90:1023-1198 CalcStresses (x-y and x-y-z velocities) with the
+  // constant dynamic and bulk viscosity of the MOLECULAR model
+  void calc_stresses(std::vector<double>& pv) {
+    const double* vx = &pv[NC * 1];
+    const double* vy = &pv[NC * 2];
+    const double* vz = NDIMS == 3 ? &pv[NC * 3] : nullptr;
+    const long sy = NI, sz = (long)NI * NJ;
+    const double dynvis = dynconst, bulkvis = bulkconst;
+    for (int k = KGMIN + KP1; k <= KGMAX - KP1; ++k)
+      for (int j = JGMIN + JP1; j <= JGMAX - JP1; ++j)
+        for (int i = IGMIN + IP1; i <= IGMAX - IP1; ++i) {
+          long x = id(i, j, k);
+          vtmp[x] = bulkvis * vector_divergence(x, vx, vy, vz);
+        }
+    for (int k = KMIN - KP1; k <= KMAX + KP1; ++k)
+      for (int j = JMIN - JP1; j <= JMAX + JP1; ++j)
+        for (int i = IMIN - IP1; i <= IMAX + IP1; ++i) {
+          long x = id(i, j, k);
+          if (NDIMS == 2) {
+            btxx[x] = dynvis * ((vx[x + 1] - vx[x - 1]) / dlx[x] + 2.0 * cxyx[x] * vy[x]) + vtmp[x];
+            btyy[x] = dynvis * ((vy[x + sy] - vy[x - sy]) / dly[x] + 2.0 * cyxy[x] * vx[x]) + vtmp[x];
+            btxy[x] = dynvis * (0.5 * ((vy[x + 1] - vy[x - 1]) / dlx[x] + (vx[x + sy] - vx[x - sy]) / dly[x])
+                                - cxyx[x] * vx[x] - cyxy[x] * vy[x]);
+          } else {
+            btxx[x] = dynvis * ((vx[x + 1] - vx[x - 1]) / dlx[x] + 2.0 * cxyx[x] * vy[x] + 2.0 * cxzx[x] * vz[x])
+                      + vtmp[x];
+            btyy[x] = dynvis * ((vy[x + sy] - vy[x - sy]) / dly[x] + 2.0 * cyxy[x] * vx[x] + 2.0 * cyzy[x] * vz[x])
+                      + vtmp[x];
+            btzz[x] = dynvis * ((vz[x + sz] - vz[x - sz]) / dlz[x] + 2.0 * czxz[x] * vx[x] + 2.0 * czyz[x] * vy[x])
+                      + vtmp[x];
+            btxy[x] = dynvis * (0.5 * ((vy[x + 1] - vy[x - 1]) / dlx[x] + (vx[x + sy] - vx[x - sy]) / dly[x])
+                                - cxyx[x] * vx[x] - cyxy[x] * vy[x]);
+            btxz[x] = dynvis * (0.5 * ((vz[x + 1] - vz[x - 1]) / dlx[x] + (vx[x + sz] - vx[x - sz]) / dlz[x])
+                                - czxz[x] * vz[x] - cxzx[x] * vx[x]);
+            btyz[x] = dynvis * (0.5 * ((vy[x + sz] - vy[x - sz]) / dlz[x] + (vz[x + sy] - vz[x - sy]) / dly[x])
+                                - czyz[x] * vz[x] - cyzy[x] * vy[x]);
+          }
+        }
+  }
+  // sources_viscosity.f90:484-507 ExternalSources: CalcStresses, then ViscositySources
+  // (physics_eulerisotherm.f90:982-1017 tensor divergence with btyx = btxy etc., mesh_midpoint.f90:
+  // 283-323 / 508-580; physics_euler.f90:1887-1943 energy = div(v.T)), added to the list's sterm
+  void viscosity_sources(std::vector<double>& pv, std::vector<double>& s) {
+    calc_stresses(pv);
+    const double* vx = &pv[NC * 1];
+    const double* vy = &pv[NC * 2];
+    const double* vz = NDIMS == 3 ? &pv[NC * 3] : nullptr;
+    const long sy = NI, sz = (long)NI * NJ;
+    if (euler)   // v.T on the cells the divergence reads
+      for (int k = KMIN - KP1; k <= KMAX + KP1; ++k)
+        for (int j = JMIN - JP1; j <= JMAX + JP1; ++j)
+          for (int i = IMIN - IP1; i <= IMAX + IP1; ++i) {
+            long x = id(i, j, k);
+            if (NDIMS == 2) {
+              vtmp[x] = vx[x] * btxx[x] + vy[x] * btxy[x];
+              vtmp1[x] = vx[x] * btxy[x] + vy[x] * btyy[x];
+            } else {
+              vtmp[x] = vx[x] * btxx[x] + vy[x] * btxy[x] + vz[x] * btxz[x];
+              vtmp1[x] = vx[x] * btxy[x] + vy[x] * btyy[x] + vz[x] * btyz[x];
+              vtmp2[x] = vx[x] * btxz[x] + vy[x] * btyz[x] + vz[x] * btzz[x];
+            }
+          }
+    for (int k = KMIN; k <= KMAX; ++k) for (int j = JMIN; j <= JMAX; ++j) for (int i = IMIN; i <= IMAX; ++i) {
+      long x = id(i, j, k);
+      double sv[4];
+      if (NDIMS == 2) {
+        sv[0] = div3d(dAx[x * 2], dAx[x * 2 + 1], dAy[x * 2], dAy[x * 2 + 1], 0.0, 0.0,
+                      dydzdV[x], dzdxdV[x], 0.0, cxyx[x], 0.0, cyxy[x], 0.0,
+                      0.5 * (btxx[x - 1] + btxx[x]), 0.5 * (btxx[x + 1] + btxx[x]),
+                      0.5 * (btxy[x - sy] + btxy[x]), 0.5 * (btxy[x + sy] + btxy[x]), 0.0, 0.0,
+                      btxy[x], 0.0, btyy[x], 0.0);
+        sv[1] = div3d(dAx[x * 2], dAx[x * 2 + 1], dAy[x * 2], dAy[x * 2 + 1], 0.0, 0.0,
+                      dydzdV[x], dzdxdV[x], 0.0, -cxyx[x], 0.0, -cyxy[x], 0.0,
+                      0.5 * (btxy[x - 1] + btxy[x]), 0.5 * (btxy[x + 1] + btxy[x]),
+                      0.5 * (btyy[x - sy] + btyy[x]), 0.5 * (btyy[x + sy] + btyy[x]), 0.0, 0.0,
+                      btxx[x], 0.0, btxy[x], 0.0);
+        if (euler) sv[2] = vector_divergence(x, vtmp.data(), vtmp1.data(), nullptr);
+      } else {
+        const double aW = dAx[x * 2], aE = dAx[x * 2 + 1], aS = dAy[x * 2], aN = dAy[x * 2 + 1];
+        const double aB = dAz[x * 2], aT = dAz[x * 2 + 1];
+        sv[0] = div3d(aW, aE, aS, aN, aB, aT, dydzdV[x], dzdxdV[x], dxdydV[x], cxyx[x], cxzx[x], cyxy[x], czxz[x],
+                      0.5 * (btxx[x - 1] + btxx[x]), 0.5 * (btxx[x + 1] + btxx[x]),
+                      0.5 * (btxy[x - sy] + btxy[x]), 0.5 * (btxy[x + sy] + btxy[x]),
+                      0.5 * (btxz[x - sz] + btxz[x]), 0.5 * (btxz[x + sz] + btxz[x]),
+                      btxy[x], btxz[x], btyy[x], btzz[x]);
+        sv[1] = div3d(aW, aE, aS, aN, aB, aT, dydzdV[x], dzdxdV[x], dxdydV[x], -cxyx[x], cyzy[x], -cyxy[x], czyz[x],
+                      0.5 * (btxy[x - 1] + btxy[x]), 0.5 * (btxy[x + 1] + btxy[x]),
+                      0.5 * (btyy[x - sy] + btyy[x]), 0.5 * (btyy[x + sy] + btyy[x]),
+                      0.5 * (btyz[x - sz] + btyz[x]), 0.5 * (btyz[x + sz] + btyz[x]),
+                      btxx[x], btyz[x], btxy[x], btzz[x]);
+        sv[2] = div3d(aW, aE, aS, aN, aB, aT, dydzdV[x], dzdxdV[x], dxdydV[x], czyz[x], -cxzx[x], cyzy[x], -czxz[x],
+                      0.5 * (btxz[x - 1] + btxz[x]), 0.5 * (btxz[x + 1] + btxz[x]),
+                      0.5 * (btyz[x - sy] + btyz[x]), 0.5 * (btyz[x + sy] + btyz[x]),
+                      0.5 * (btzz[x - sz] + btzz[x]), 0.5 * (btzz[x + sz] + btzz[x]),
+                      btyz[x], btxx[x], btyy[x], btxz[x]);
+        if (euler) sv[3] = vector_divergence(x, vtmp.data(), vtmp1.data(), vtmp2.data());
+      }
+      s[x] = s[x] + 0.0;
+      for (int m = 0; m < VDIM; ++m) s[x + NC * (1 + m)] = s[x + NC * (1 + m)] + sv[m];
+      if (euler) s[x + NC * PRESSURE] = s[x + NC * PRESSURE] + sv[VDIM];
+    }
+  }
+
+  // sources_generic.f90:220-261 -> sources_gravity.f90:164-200 -> physics ExternalSources;
+  // the list holds gravity first (prepended last, sources_generic.f90:190-199), then viscosity
+  void external_sources(std::vector<double>& pv, std::vector<double>& cv, std::vector<double>& s) {
     std::fill(s.begin(), s.end(), 0.0);
+    external_gravity(cv, s);
+    if (vismodel) viscosity_sources(pv, s);
+    zero_ghosts(s);
+  }
+  void external_gravity(std::vector<double>& cv, std::vector<double>& s) {
     if (!have_accel) return;
     if (outbound) update_gravity();
     for (long x = 0; x < NC; ++x) {
@@ -953,7 +1107,6 @@ struct Oracle {
         s[x + NC * PRESSURE] = e;
       }
     }
-    zero_ghosts(s);
   }
 
   // timedisc_base.f90:1073-1271 ComputeRHS (rhstype 0)
@@ -968,7 +1121,7 @@ struct Oracle {
       for (long x = 0; x < NC; ++x) bccsound[x] = soundspeed(pvar[x], pvar[x + NC * PRESSURE]);
     if (checkbm != FGPU_CHECK_NOTHING) check_data(pv, cv, checkbm);
     geometrical_sources(pv, cv, geo_src);
-    external_sources(cv, src);
+    external_sources(pv, cv, src);
     if (fargo) {
       if (cfg.geometry == FGPU_CARTESIAN) std::fill(geo_src.begin(), geo_src.end(), 0.0);
       add_fargo_sources(pv, cv, geo_src);
@@ -1054,8 +1207,26 @@ struct Oracle {
     }
     double dt_cfl = cfl / invdt;
     dtcause = 0;
-    // point-mass sources do not limit dt (sources_c_accel.f90:113-126 -> HUGE)
-    return dt_cfl;
+    // sources_generic.f90:264-293: the point mass returns HUGE (sources_c_accel.f90:113-126),
+    // the viscosity its advection-diffusion limit (sources_viscosity.f90:511-581)
+    double dt = dt_cfl;
+    if (vismodel) {
+      double ivis = 0.0;
+      for (long x = 0; x < NC; ++x) {
+        const double kinvis = dynconst / pvar[x];
+        double v = 0.0;
+        for (int m = 0; m < NDIMS; ++m) {
+          const double dl = dls[dirs[m]][x];
+          const double t = (amax(x, m) + 2.0 * kinvis / dl) / dl;
+          v = m == 0 ? t : v + t;
+        }
+        ivis = x == 0 ? v : fmax2(ivis, v);
+      }
+      const double dt_new = ivis > TINY_ ? cvis / ivis : HUGE_;
+      if (dt_new < dt) dtcause = FGPU_DTCAUSE_VISCOSITY;
+      dt = fmin2(dt, dt_new);
+    }
+    return dt;
   }
 
   // timedisc_base.f90:1012-1053 ComputeError

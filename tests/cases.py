@@ -176,12 +176,13 @@ def _iso3d(n=(18, 16, 20), seed=41):
     return c, p, {}
 
 
-def khi3d(perm=(0, 1, 2), n=8, tsim=30.0, seed=17):
+def khi3d(perm=(0, 1, 2), n=8, tsim=30.0, seed=17, re=1.0e4):
     """tests/KHI3D.f90: a periodic 3D shear layer (flow along axis a, density and velocity
     jump across axis b), Euler gamma 1.4, KT + MC(theta 1.2) on conservative variables,
-    SSPRK3 with CFL 0.4, no viscosity.  perm maps the base orientation (flow along x,
-    jump across y) to another axis order; the same seeded velocity noise is permuted
-    with it, so the six runs are images of each other.  Returns (cfg, pvar, perm)."""
+    SSPRK3 with CFL 0.4 and the test's molecular viscosity for Reynolds number re
+    (None: inviscid).  perm maps the base orientation (flow along x, jump across y) to
+    another axis order; the same seeded velocity noise is permuted with it, so the six
+    runs are images of each other.  Returns (cfg, pvar, perm)."""
     c = abi.default_config()
     c.inum = c.jnum = c.knum = n
     c.xmin, c.xmax, c.ymin, c.ymax, c.zmin, c.zmax = -0.5, 0.5, -0.5, 0.5, -0.5, 0.5
@@ -198,6 +199,11 @@ def khi3d(perm=(0, 1, 2), n=8, tsim=30.0, seed=17):
     c.cfl = 0.4
     c.stoptime = tsim
     c.dtlimit = 1e-10
+    if re is not None:
+        eta = khi_reynolds(re)
+        c.vismodel = abi.VIS_MOLECULAR
+        c.dynconst = eta
+        c.bulkconst = -2. / 3. * eta
     abi.finalize_config(c)
     X, Y, Z, _ = problems.centers(c)
     rng = np.random.default_rng(seed)
@@ -228,6 +234,23 @@ def inverse_perm(perm):
     for a, b in enumerate(perm):
         inv[b] = a
     return tuple(inv)
+
+
+def _visc(case, dynconst, bulkconst=None, cvis=0.5):
+    """Add the MOLECULAR viscosity source (sources_viscosity.f90); bulkconst None keeps
+    fosite's default -2/3*dynconst."""
+    c, p, extra = case
+    c.vismodel = abi.VIS_MOLECULAR
+    c.dynconst = dynconst
+    if bulkconst is not None:
+        c.bulkconst = bulkconst
+    c.cvis = cvis
+    return c, p, extra
+
+
+def khi_reynolds(re=1.0e4, rho0=1.0, xyzlen=1.0, v0=-0.5, v1=0.5):
+    """Dynamic viscosity of tests/KHI2D.f90:236-239 and tests/KHI3D.f90:328-331."""
+    return abs(rho0 * xyzlen * (v0 - v1) / re)
 
 
 def _with(case, **kw):
@@ -278,6 +301,26 @@ CASES = {
     "euler_fargo_disk_cyl_prim": lambda: _euler_fargo(n=(24, 160), geometry=abi.CYLINDRICAL, variables=abi.PRIMITIVE),
     "disk_fargo_order1_minmod": lambda: _disk_fargo(n=(30, 44), tdorder=1, limiter=abi.MINMOD,
                                                     bcs=[abi.REFLECTING, abi.REFLECTING, abi.PERIODIC, abi.PERIODIC]),
+    # molecular viscosity (sources_viscosity.f90); the first is the KHI2D test's set-up
+    "khi_visc_re1e4_mc": lambda: _visc(_khi(limiter=abi.MONOCENT, theta=1.2, n=(32, 30)), khi_reynolds(),
+                                       bulkconst=-2. / 3. * khi_reynolds()),
+    "khi_visc_dominant_reflect_prim": lambda: _visc(_khi(variables=abi.PRIMITIVE, n=(30, 28),
+                                                         bcs=[abi.REFLECTING, abi.REFLECTING, abi.NO_GRADIENTS,
+                                                              abi.NO_GRADIENTS]), 0.05, cvis=0.4),
+    "khi_visc_rkf45_absorbing": lambda: _visc(_khi(method=abi.RK_FEHLBERG, tdorder=5, n=(26, 24),
+                                                   bcs=[abi.ABSORBING] * 4), 5e-3, bulkconst=1e-3),
+    "khi_visc_adaptive_me": lambda: _visc(_khi(me_tol=1e-3, n=(28, 26)), 2e-3),
+    "gauss3d_visc_dopri": lambda: _visc(_gauss3d(n=(14, 12, 10)), 2e-3),
+    "iso3d_visc_ssprk3_mixed_bc": lambda: _visc(_with(_iso3d(n=(14, 12, 16)), method=abi.MODIFIED_EULER, tdorder=3,
+                                                      tol_rel=10.0), 1e-2),
+    "disk_visc_logcyl_pointmass": lambda: _visc(_disk(bcs=[abi.NO_GRADIENTS, abi.REFLECTING, abi.PERIODIC,
+                                                           abi.PERIODIC]), 1e-3),
+    "disk_visc_fargo_cyl_cons": lambda: _visc(_disk_fargo(geometry=abi.CYLINDRICAL, n=(30, 36),
+                                                          variables=abi.CONSERVATIVE,
+                                                          bcs=[abi.REFLECTING, abi.NO_GRADIENTS, abi.PERIODIC,
+                                                               abi.PERIODIC]), 2e-3),
+    "euler_disk_cyl_visc_prim": lambda: _visc(_euler_fargo(n=(24, 40), geometry=abi.CYLINDRICAL,
+                                                           variables=abi.PRIMITIVE, fargo=0), 1e-3),
 }
 
 

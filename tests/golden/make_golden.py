@@ -21,9 +21,12 @@ import pyoracle  # noqa: E402
 STEPS = 3
 
 
-def main():
+def main(names=None):
+    """Regenerate the fixtures of the named cases (all cases without names)."""
     out = os.path.dirname(os.path.abspath(__file__))
     for name, build in sorted(CASES.items()):
+        if names and name not in names:
+            continue
         cfg, p, extra = build()
         o = pyoracle.Oracle(cfg)
         if "bccsound" in extra:
@@ -40,4 +43,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

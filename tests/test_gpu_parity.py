@@ -109,6 +109,7 @@ def test_steps_bitwise_exact_build(name):
         if tol == 0.0:
             assert sg.time == so.time and sg.dt == so.dt, (s, sg.time, so.time, sg.dt, so.dt)
         _compare(cfg, o, g, tol, "step %d" % s)
+        assert sg.dtcause == so.dtcause, (s, sg.dtcause, so.dtcause)
         if cfg.pm_outbound:
             (mg, dg), (mo, do) = g.pointmass(), o.pointmass()
             if tol == 0.0:
@@ -125,7 +126,8 @@ def test_steps_bitwise_exact_build(name):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["khi_ssprk3_vanleer_cons", "gauss3d_dopri_mc_prim", "disk_logcyl_pointmass",
-                                  "euler2d_absorbing", "iso3d_cashkarp_mixed_bc", "disk_fargo_logcyl"])
+                                  "euler2d_absorbing", "iso3d_cashkarp_mixed_bc", "disk_fargo_logcyl",
+                                  "khi_visc_re1e4_mc", "gauss3d_visc_dopri", "disk_visc_logcyl_pointmass"])
 def test_fast_build_tolerance(name):
     cfg, o, g = _pair(name, exact=False)
     o.first_step()
@@ -183,11 +185,15 @@ def test_fargo_graph_run_matches_single_steps():
 
 
 @pytest.mark.gpu
-def test_khi_transposition_symmetry():
-    """tests/KHI2D.f90:81-150: the x<->y transposed run agrees exactly (RMS < TINY)."""
+@pytest.mark.parametrize("visc", [False, True])
+def test_khi_transposition_symmetry(visc):
+    """tests/KHI2D.f90:81-150: the x<->y transposed run agrees exactly (RMS < TINY), also
+    with the test's molecular viscosity (RE = 1e4)."""
     from fosite_b200.sim import Simulation
-    from cases import _khi
+    from cases import _khi, _visc, khi_reynolds
     cfg, p, _ = _khi(n=(36, 36))
+    if visc:
+        cfg, p, _ = _visc((cfg, p, {}), khi_reynolds(), bulkconst=-2. / 3. * khi_reynolds())
     pt = np.stack([p[0].transpose(0, 2, 1), p[2].transpose(0, 2, 1), p[1].transpose(0, 2, 1), p[3].transpose(0, 2, 1)])
     # the --fmad=false build: FMA contraction of a*a + b*b is not symmetric in a, b
     a = Simulation(cfg, exact=True)
@@ -205,9 +211,10 @@ def test_khi_transposition_symmetry():
 
 @pytest.mark.gpu
 def test_khi3d_orientation_symmetry_gpu():
-    """tests/KHI3D.f90:260-266 on the device: six orientations, TSIM = 30, RMS < 4 EPSILON
-    (the --fmad=false build; contraction of a*a + b*b is not symmetric in a, b), and the
-    base orientation equal to the oracle's run bit for bit."""
+    """tests/KHI3D.f90:260-266 on the device, with the test's molecular viscosity: six
+    orientations, TSIM = 30, RMS < 4 EPSILON (the --fmad=false build; contraction of
+    a*a + b*b is not symmetric in a, b), and the base orientation equal to the oracle's
+    run bit for bit."""
     from fosite_b200.sim import Simulation
     from cases import khi3d, permute_state, inverse_perm
     runs = {}
