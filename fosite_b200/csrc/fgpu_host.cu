@@ -172,10 +172,28 @@ struct fgpu_handle {
   int acc_face = 0;             // 0 west, 1 east
   double* d_acc = nullptr;
   double dxyz[3] = {1.0, 1.0, 1.0};
-  // molecular viscosity: constants and the viscous source of the current stage state
+  // viscosity: model, constants and the viscous source of the current stage state; the
+  // ALPHA/BETA/POWERLAW models keep the dynamic viscosity by padded cell with the time of
+  // its last update (sources_viscosity.f90:359-453)
   bool vis = false;
-  double vis_eta = 0.0, vis_mub = 0.0, cvis = 0.5;
+  int vis_model = 0;
+  double vis_eta = 0.0, vis_mub = 0.0, cvis = 0.5, vis_power = 0.0;
   double* d_visc = nullptr;     // [nd (+1 energy)][n]
+  double* d_dynvis = nullptr;   // [npad]
+  double* d_ephir = nullptr;    // [nd][npad]
+  double* d_visrad = nullptr;   // [npad]
+  double* d_vistime = nullptr;  // 1 double, initially -1
+  long long npad_vis = 0;
+};
+
+// The time of a right-hand side evaluation, for the viscosity update: a host value, or on the
+// device clock the control block's time + zeta*dt
+struct RhsTime {
+  bool dev = false;
+  double t = 0.0;
+  double zeta = 0.0;
+  static RhsTime host(double t) { RhsTime r; r.t = t; return r; }
+  static RhsTime device(double zeta) { RhsTime r; r.dev = true; r.zeta = zeta; return r; }
 };
 
 namespace {
@@ -292,6 +310,63 @@ int build_metric(fgpu_handle* h) {
   return FGPU_OK;
 }
 
+// Cell geometry of the ALPHA/BETA/POWERLAW viscosities by padded cell: Mesh%radius at the
+// bary centres (geometry_*.f90 Radius) and ephi/r in curvilinear components
+// (sources_viscosity.f90:186-226: -y/r^2, x/r^2 from Convert2Cartesian of the bary centres,
+// geometry_cylindrical.f90:446-455 / geometry_logcylindrical.f90:344-356, converted back with
+// geometry_cylindrical.f90:485-494; Cartesian meshes use them as they are)
+int upload_visc_geometry(fgpu_handle* h) {
+  const fgpu_config& c = h->cfg;
+  const int nx = c.inum, ny = c.jnum, nz = c.knum, nd = h->nd;
+  const long long NXp = nx + 4, NYp = ny + 4, NZp = nd == 3 ? nz + 4 : 1;
+  const long long npad = NXp * NYp * NZp;
+  const double mdx = (c.xmax - c.xmin) / nx, mdy = (c.ymax - c.ymin) / ny;
+  double mdz = (c.zmax - c.zmin) / nz;
+  if (mdz < 2 * DBL_EPSILON && nz == 1) mdz = 0.0;
+  std::vector<double> eph((size_t)nd * npad), rad((size_t)npad);
+  for (long long kp = 0; kp < NZp; ++kp)
+    for (long long jp = 0; jp < NYp; ++jp)
+      for (long long ip = 0; ip < NXp; ++ip) {
+        const long long q = ip + NXp * (jp + NYp * kp);
+        const int I = (int)ip - 1, J = (int)jp - 1, K = nd == 3 ? (int)kp - 1 : 1;
+        const double x1 = c.xmin + ((double)(2 * I - 1) * 0.5) * mdx;
+        const double x2 = c.ymin + ((double)(2 * J - 1) * 0.5) * mdy;
+        const double x3 = c.zmin + ((double)(2 * K - 1) * 0.5) * mdz;
+        double X, Y, r;
+        if (c.geometry == FGPU_CYLINDRICAL) {
+          X = x1 * std::cos(x2); Y = x1 * std::sin(x2); r = std::sqrt(x1 * x1 + x3 * x3);
+        } else if (c.geometry == FGPU_LOGCYLINDRICAL) {
+          const double rr = c.gparam * std::exp(x1);
+          X = rr * std::cos(x2); Y = rr * std::sin(x2); r = std::sqrt(rr * rr + x3 * x3);
+        } else {
+          X = x1; Y = x2; r = std::sqrt(x1 * x1 + x2 * x2 + x3 * x3);
+        }
+        const double r2 = r * r;
+        const double ex = -Y / r2, ey = X / r2, ez = 0.0;
+        double e[3];
+        if (c.geometry == FGPU_CARTESIAN) { e[0] = ex; e[1] = ey; e[2] = ez; }
+        else {
+          e[0] = ex * std::cos(x2) + ey * std::sin(x2);
+          e[1] = -ex * std::sin(x2) + ey * std::cos(x2);
+          e[2] = ez;
+        }
+        for (int l = 0; l < nd; ++l) eph[(size_t)l * npad + q] = e[l];
+        rad[q] = r;
+      }
+  h->npad_vis = npad;
+  CUDA_TRY(h, cudaMalloc(&h->d_ephir, sizeof(double) * eph.size()));
+  CUDA_TRY(h, cudaMalloc(&h->d_visrad, sizeof(double) * rad.size()));
+  CUDA_TRY(h, cudaMalloc(&h->d_dynvis, sizeof(double) * npad));
+  CUDA_TRY(h, cudaMalloc(&h->d_vistime, sizeof(double)));
+  CUDA_TRY(h, cudaMemcpy(h->d_ephir, eph.data(), sizeof(double) * eph.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(h, cudaMemcpy(h->d_visrad, rad.data(), sizeof(double) * rad.size(), cudaMemcpyHostToDevice));
+  std::vector<double> dv((size_t)npad, c.dynconst);
+  CUDA_TRY(h, cudaMemcpy(h->d_dynvis, dv.data(), sizeof(double) * npad, cudaMemcpyHostToDevice));
+  const double t0 = -1.0;   // sources_viscosity.f90:256-258
+  CUDA_TRY(h, cudaMemcpy(h->d_vistime, &t0, sizeof(double), cudaMemcpyHostToDevice));
+  return FGPU_OK;
+}
+
 int upload_metric(fgpu_handle* h) {
   size_t bytes = h->h_metric.size() * sizeof(double);
   if (!h->d_metric) CUDA_TRY(h, cudaMalloc(&h->d_metric, bytes));
@@ -313,7 +388,9 @@ int upload_metric(fgpu_handle* h) {
   M.dAxE = P(M_dAxE);
   M.nxp = nxp;
   M.curv = h->curv ? 1 : 0;
-  M.vis = h->vis ? 1 : 0;
+  // the fused CFL epilogues add the viscous limit of the constant model; the other models
+  // evaluate it in visc_cfl_kernel after their end-of-step update
+  M.vis = h->vis && h->vis_model == FGPU_VIS_MOLECULAR ? 1 : 0;
   M.vis_eta = h->vis_eta;
   return FGPU_OK;
 }
@@ -474,6 +551,64 @@ void launch_visc_t(fgpu_handle* h, const ViscArgs& V) {
   visc_kernel<ND, EU, S::TX, S::TY, S::TZ>
       <<<grid, S::TX * S::TY * S::TZ, ViscTile<ND, S::TX, S::TY, S::TZ>::SMEM, h->stream>>>(V);
 }
+// UpdateViscosity of the state S at the time `when` (ALPHA/BETA/POWERLAW): the conditional
+// update of the cell viscosities, then the record of its time
+template <int ND, bool EU>
+void launch_visc_update_t(fgpu_handle* h, const VisUpdArgs& U) {
+  const unsigned blocks = (unsigned)std::min<long long>((U.npad + 255) / 256, 148 * 8);
+  visc_update_kernel<ND, EU><<<blocks, 256, 0, h->stream>>>(U);
+  visc_time_kernel<<<1, 1, 0, h->stream>>>(U, h->d_vistime);
+}
+int launch_visc_update(fgpu_handle* h, const StateRef& S, const RhsTime& when) {
+  if (!h->vis || h->vis_model == FGPU_VIS_MOLECULAR) return FGPU_OK;
+  VisUpdArgs U;
+  std::memset(&U, 0, sizeof(U));
+  U.g = h->g; U.ph = h->ph; U.mt = h->mt;
+  U.in = S;
+  U.model = h->vis_model;
+  U.dynconst = h->vis_eta;
+  U.power = h->vis_power;
+  U.ephir = h->d_ephir;
+  U.rad = h->d_visrad;
+  U.dynvis = h->d_dynvis;
+  U.vis_time = h->d_vistime;
+  U.t = when.t;
+  if (when.dev) { U.t_dev = &h->d_ctl->time; U.dt_dev = &h->d_ctl->dt; U.zeta = when.zeta; U.ctl = h->d_ctl; }
+  U.npad = h->npad_vis;
+  return timed_launch(h, 0, 0.0, [&] {
+    if (h->nd == 2) h->euler ? launch_visc_update_t<2, true>(h, U) : launch_visc_update_t<2, false>(h, U);
+    else h->euler ? launch_visc_update_t<3, true>(h, U) : launch_visc_update_t<3, false>(h, U);
+    CUDA_TRY(h, cudaGetLastError());
+    return FGPU_OK;
+  });
+}
+// CalcTimestep's viscous limit for ALPHA/BETA/POWERLAW: UpdateViscosity at the state's time,
+// then the reduction over the padded cells into ctl->invdt[3]
+int launch_visc_cfl(fgpu_handle* h, const StateRef& S, bool roundtrip, const RhsTime& when) {
+  if (!h->vis || h->vis_model == FGPU_VIS_MOLECULAR) return FGPU_OK;
+  if (int rc = launch_visc_update(h, S, when)) return rc;
+  VisCflArgs C;
+  std::memset(&C, 0, sizeof(C));
+  C.g = h->g; C.ph = h->ph; C.mt = h->mt;
+  C.in = S;
+  C.roundtrip = roundtrip ? 1 : 0;
+  C.dynvis = h->d_dynvis;
+  C.npad = h->npad_vis;
+  C.ctl = h->d_ctl;
+  const unsigned blocks = (unsigned)std::min<long long>((C.npad + 255) / 256, 148 * 8);
+  return timed_launch(h, 0, 0.0, [&] {
+    if (h->nd == 2) {
+      if (h->euler) visc_cfl_kernel<2, true><<<blocks, 256, 0, h->stream>>>(C);
+      else visc_cfl_kernel<2, false><<<blocks, 256, 0, h->stream>>>(C);
+    } else {
+      if (h->euler) visc_cfl_kernel<3, true><<<blocks, 256, 0, h->stream>>>(C);
+      else visc_cfl_kernel<3, false><<<blocks, 256, 0, h->stream>>>(C);
+    }
+    CUDA_TRY(h, cudaGetLastError());
+    return FGPU_OK;
+  });
+}
+
 int launch_visc(fgpu_handle* h, const StateRef& S) {
   ViscArgs V;
   std::memset(&V, 0, sizeof(V));
@@ -481,6 +616,7 @@ int launch_visc(fgpu_handle* h, const StateRef& S) {
   V.in = S;
   V.eta = h->vis_eta;
   V.mub = h->vis_mub;
+  V.dynvis = h->vis_model == FGPU_VIS_MOLECULAR ? nullptr : h->d_dynvis;
   V.out = h->d_visc;
   // algorithmic bytes: the state read once, the source written once
   const double bytes = (double)(h->V + h->nd + (h->euler ? 1 : 0)) * (double)h->g.n * 8.0;
@@ -492,9 +628,13 @@ int launch_visc(fgpu_handle* h, const StateRef& S) {
   });
 }
 
-int launch_stage(fgpu_handle* h, StageArgs& A) {
+// One right-hand side evaluation (stage kernel) at the time `when`, preceded by the viscous
+// source of its state when the viscosity is on
+int launch_stage(fgpu_handle* h, StageArgs& A, const RhsTime& when = RhsTime()) {
   if (h->vis) {
-    if (int rc = launch_visc(h, A.rin.base ? A.rin : A.in)) return rc;
+    const StateRef& S = A.rin.base ? A.rin : A.in;
+    if (int rc = launch_visc_update(h, S, when)) return rc;
+    if (int rc = launch_visc(h, S)) return rc;
     A.visc = h->d_visc;
   }
   return timed_launch(h, true, stage_bytes(h, A), [&] { return launch_stage_raw(h, A); });
@@ -608,8 +748,13 @@ double ctl_dt(const fgpu_handle* h, int* cause) {
 }
 
 // ---------------------------------------------------------------- Shu-Osher (device clock)
-// eta(n,order), timedisc_modeuler.f90:74-77
+// eta(n,order) and zeta(n,order), timedisc_modeuler.f90:74-77
 const double kEta[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.5, 0.0}, {0.0, 0.75, 1.0 / 3.0}};
+const double kZeta[3][3] = {{0.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {0.0, 1.0, 0.5}};
+// time of the right-hand side read by Shu-Osher stage n: the previous step's closing
+// ComputeRHS at time (n = 1), else the one after update n-1 at time + zeta(n-1)*dt
+// (timedisc_modeuler.f90:150-158)
+double stage_zeta(const fgpu_handle* h, int n) { return n == 1 ? 0.0 : kZeta[h->order - 1][n - 2]; }
 
 // Arguments of Shu-Osher stage n (1-based) of one grid: stage 1 reads the
 // stored state P (with the CHECK_PMIN round trip of the last ComputeRHS),
@@ -659,12 +804,16 @@ int launch_accrete(fgpu_handle* h, int n) {
 int enqueue_shu_osher_step(fgpu_handle* h) {
   for (int n = 1; n <= h->order; ++n) {
     StageArgs A = shu_osher_stage(h, n);
-    if (int rc = launch_stage(h, A)) return rc;
+    if (int rc = launch_stage(h, A, RhsTime::device(stage_zeta(h, n)))) return rc;
     if (int rc = launch_accrete(h, n)) return rc;
   }
   if (h->order == 1)
     CUDA_TRY(h, cudaMemcpyAsync(h->buf[0], h->buf[1], sizeof(double) * h->V * h->g.n, cudaMemcpyDeviceToDevice,
                                 h->stream));
+  // the closing ComputeRHS at time + dt (AcceptSolution) updates the viscosity that
+  // CalcTimestep then reads
+  if (int rc = launch_visc_cfl(h, plain_state(h->buf[0], h->roundtrip_cfg), h->roundtrip_cfg, RhsTime::device(1.0)))
+    return rc;
   BndArgs B = bnd_args(h, h->buf[0], h->roundtrip_cfg, FIN_STEP);
   h->pre_rt = h->roundtrip_cfg;   // the end-of-step ComputeRHS uses the checkdata mask
   return launch_misc(h, 0, B);
@@ -817,7 +966,7 @@ void sync_from_ctl(fgpu_handle* h) {
 }
 
 // ---------------------------------------------------------------- Butcher engine (host clock)
-int enqueue_k1(fgpu_handle* h, bool from_pre, bool cfl, bool rt, int checkdata) {
+int enqueue_k1(fgpu_handle* h, bool from_pre, bool cfl, bool rt, int checkdata, double t) {
   // ComputeRHS of the current state into K1.  from_pre: the stored state in P
   // gets the end-of-step CHECK_ALL treatment and its round trip goes to the
   // base buffer (cold = cvar); otherwise RejectSolution's CHECK_NOTHING RHS of base.
@@ -835,7 +984,7 @@ int enqueue_k1(fgpu_handle* h, bool from_pre, bool cfl, bool rt, int checkdata) 
   } else {
     A.in = plain_state(base, false);
   }
-  return launch_stage(h, A);
+  return launch_stage(h, A, RhsTime::host(t));
 }
 
 double adjust_timestep(fgpu_handle* h, double maxerr, double dtold_) {
@@ -863,7 +1012,7 @@ double adjust_timestep(fgpu_handle* h, double maxerr, double dtold_) {
 //   order 3: s2 = update(eta2, base, s1, rhs(s1)), low = update(1/2, base, s1, rhs(s1))
 //            P  = update(eta3, base, s2, rhs(s2)),  err = ComputeError(P, low)
 //   order 2: P  = update(eta2, base, s1, rhs(s1)),  err = ComputeError(P, s1)
-int modeuler_attempt(fgpu_handle* h, double dtv, double& err) {
+int modeuler_attempt(fgpu_handle* h, double t, double dtv, double& err) {
   double* P = h->buf[0];
   double* base = h->buf[1];
   double* K1 = h->buf[2];
@@ -898,7 +1047,7 @@ int modeuler_attempt(fgpu_handle* h, double dtv, double& err) {
       A.out2 = LO;
       A.eta2 = kEta[1][1];   // the second-order solution from the same RHS
     }
-    if (int rc = launch_stage(h, A)) return rc;
+    if (int rc = launch_stage(h, A, RhsTime::host(t + kZeta[ord - 1][n - 2] * dtv))) return rc;
   }
   if (int rc = read_ctl(h)) return rc;
   double e;
@@ -909,8 +1058,8 @@ int modeuler_attempt(fgpu_handle* h, double dtv, double& err) {
   return FGPU_OK;
 }
 
-int butcher_attempt(fgpu_handle* h, double dtv, double& err) {
-  if (h->adaptive_me) return modeuler_attempt(h, dtv, err);
+int butcher_attempt(fgpu_handle* h, double t, double dtv, double& err) {
+  if (h->adaptive_me) return modeuler_attempt(h, t, dtv, err);
   const Tableau& T = h->T;
   double* P = h->buf[0];
   double* base = h->buf[1];
@@ -941,7 +1090,8 @@ int butcher_attempt(fgpu_handle* h, double dtv, double& err) {
       for (int q = 0; q < T.m; ++q) { A.bh_dt[q] = T.bh[q] * dtv; A.bl_dt[q] = T.bl[q] * dtv; }
       A.out_high = P;
     }
-    if (int rc = launch_stage(h, A)) return rc;
+    // timedisc_rkfehlberg.f90:195: ComputeRHS at t + c(m)*dt
+    if (int rc = launch_stage(h, A, RhsTime::host(t + T.c[m - 1] * dtv))) return rc;
     if (m == T.m && !fused_end) {
       // the high/low combination and error norm as a streaming pass (the stencil kernel
       // keeps its registers for the stencil)
@@ -986,6 +1136,7 @@ int finish_cfl_host(fgpu_handle* h, const double* state, bool roundtrip, double&
   BndArgs B = bnd_args(h, state, roundtrip, FIN_NONE);
   B.checkdata = checkdata;
   if (int rc = launch_misc(h, 0, B)) return rc;
+  if (int rc = launch_visc_cfl(h, plain_state(state, roundtrip), roundtrip, RhsTime::host(h->time))) return rc;
   if (int rc = read_ctl(h)) return rc;
   dtcfl = ctl_dt(h, &cause);
   h->checkflags |= h->h_ctl->flags;
@@ -1006,21 +1157,21 @@ int butcher_integration_step(fgpu_handle* h) {
   while (!h->brk && t + d <= h->time + h->dt) {
     dtold_ = d;
     double e = 0.0;
-    if (int rc = butcher_attempt(h, d, e)) return rc;
+    if (int rc = butcher_attempt(h, t, d, e)) return rc;
     h->last_err = e;
     d = adjust_timestep(h, e, d);
     rhs_done_at_t = false;
     if (e != e) h->brk = true;
     else if (e > DBL_MAX) h->brk = true;
     else if (e >= 1.0) {   // RejectSolution: cvar = cold, RHS with CHECK_NOTHING
-      if (int rc = enqueue_k1(h, false, false, false, h->cfg.checkdata)) return rc;
+      if (int rc = enqueue_k1(h, false, false, false, h->cfg.checkdata, t)) return rc;
       h->n_adj++;
       h->dtcause = FGPU_DTCAUSE_ERRADJ;
       if (d < h->dtmin) h->dtmin = d;
     } else {               // AcceptSolution
       t = t + dtold_;
       if (t < h->time + h->dt) {
-        if (int rc = enqueue_k1(h, true, false, h->roundtrip_cfg, h->cfg.checkdata)) return rc;
+        if (int rc = enqueue_k1(h, true, false, h->roundtrip_cfg, h->cfg.checkdata, t)) return rc;
         rhs_done_at_t = true;
       }
       h->iter++;
@@ -1037,7 +1188,7 @@ int butcher_integration_step(fgpu_handle* h) {
       CUDA_TRY(h, cudaMemcpyAsync(h->buf[0], h->buf[1], sizeof(double) * h->V * h->g.n, cudaMemcpyDeviceToDevice,
                                   h->stream));
     }
-    if (int rc = enqueue_k1(h, true, true, h->roundtrip_cfg, h->cfg.checkdata)) return rc;
+    if (int rc = enqueue_k1(h, true, true, h->roundtrip_cfg, h->cfg.checkdata, h->time)) return rc;
     h->pre_rt = h->roundtrip_cfg;
   }
   return FGPU_OK;
@@ -1129,9 +1280,15 @@ int validate(fgpu_handle* h) {
     // sources_viscosity.f90:132-266
     if (c.vismodel < FGPU_VIS_MOLECULAR || c.vismodel > FGPU_VIS_ALPHA_ALT)
       return set_err(h, FGPU_EBADCFG, "Viscosity prescription not supported.");
-    if (c.vismodel != FGPU_VIS_MOLECULAR)
-      return set_err(h, FGPU_EUNSUPPORTED, "viscosity: the MOLECULAR (constant) model only");
+    if (c.vismodel == FGPU_VIS_ALPHA_ALT)
+      return set_err(h, FGPU_EUNSUPPORTED, "alternative alpha-viscosity currently not supported");
+    if (c.vismodel == FGPU_VIS_ALPHA && h->euler)
+      return set_err(h, FGPU_EUNSUPPORTED, "viscosity: ALPHA with isothermal physics only");
+    if (c.vismodel != FGPU_VIS_MOLECULAR && c.fargo_method != 0)
+      return set_err(h, FGPU_EUNSUPPORTED, "viscosity: ALPHA/BETA/POWERLAW without fargo");
     h->vis = true;
+    h->vis_model = c.vismodel;
+    h->vis_power = c.vis_exponent;
     h->vis_eta = c.dynconst;
     h->vis_mub = std::isnan(c.bulkconst) ? -2. / 3. * c.dynconst : c.bulkconst;
     h->cvis = c.cvis;
@@ -1231,6 +1388,7 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
     size_t bytes = sizeof(double) * (h->nd + (h->euler ? 1 : 0)) * h->g.n;
     if (cudaMalloc(&h->d_visc, bytes) != cudaSuccess) rc = set_err(h, FGPU_ENOMEM, "viscous source array");
     else cudaMemsetAsync(h->d_visc, 0, bytes, h->stream);
+    if (!rc && h->vis_model != FGPU_VIS_MOLECULAR) rc = upload_visc_geometry(h);
   }
   if (!rc && h->fargo) {
     if (cudaMalloc(&h->d_w, sizeof(double) * 2 * h->nxp) != cudaSuccess) rc = set_err(h, FGPU_ENOMEM, "fargo arrays");
@@ -1268,6 +1426,10 @@ void fgpu_destroy(fgpu_handle* h) {
   if (h->d_w) cudaFree(h->d_w);
   if (h->d_acc) cudaFree(h->d_acc);
   if (h->d_visc) cudaFree(h->d_visc);
+  if (h->d_dynvis) cudaFree(h->d_dynvis);
+  if (h->d_ephir) cudaFree(h->d_ephir);
+  if (h->d_visrad) cudaFree(h->d_visrad);
+  if (h->d_vistime) cudaFree(h->d_vistime);
   if (h->d_ctl) cudaFree(h->d_ctl);
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
   if (h->own_stream) h->stream = h->own_stream;
@@ -1442,7 +1604,7 @@ int fgpu_first_step(fgpu_handle* h) {
   // (fosite.f90:315-321): ideal-gas states get the CHECK_PMIN round trip here
   const bool rt_first = h->euler;
   if (h->butcher) {
-    if (int rc = enqueue_k1(h, true, true, rt_first, FGPU_CHECK_ALL)) return rc;
+    if (int rc = enqueue_k1(h, true, true, rt_first, FGPU_CHECK_ALL, h->time)) return rc;
     double dtc;
     int cause = 0;
     if (int rc = finish_cfl_host(h, h->buf[0], rt_first, dtc, FGPU_CHECK_ALL, cause)) return rc;
@@ -1472,6 +1634,7 @@ int fgpu_first_step(fgpu_handle* h) {
     h->fargo_phase = 1;
   }
   if (int rc = launch_misc(h, 1, B)) return rc;
+  if (int rc = launch_visc_cfl(h, plain_state(h->buf[0], rt_first), rt_first, RhsTime::host(h->time))) return rc;
   if (int rc = launch_misc(h, 0, B)) return rc;
   if (int rc = read_ctl(h)) return rc;
   sync_from_ctl(h);
@@ -1572,7 +1735,7 @@ int fgpu_compute_rhs(fgpu_handle* h) {
   A.out_mode = OUT_RHS;
   A.out = out;
   A.ctl = nullptr;
-  if (int rc = launch_stage(h, A)) return rc;
+  if (int rc = launch_stage(h, A, RhsTime::host(h->time))) return rc;
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return FGPU_OK;
 }
@@ -1591,6 +1754,7 @@ int fgpu_calc_timestep(fgpu_handle* h, double* dt) {
   if (h->fargo) { B.in.pre = fargo_pre(h); B.w_sub = h->d_w; }
   if (int rc = launch_misc(h, 1, B)) return rc;
   if (int rc = launch_misc(h, 0, B)) return rc;
+  if (int rc = launch_visc_cfl(h, plain_state(h->buf[0], rt), rt, RhsTime::host(h->time))) return rc;
   if (int rc = read_ctl(h)) return rc;
   int cause = 0;
   *dt = ctl_dt(h, &cause);

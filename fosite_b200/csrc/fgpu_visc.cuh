@@ -1,4 +1,4 @@
-// fgpu_visc.cuh -- viscous source of one stage state (MOLECULAR model).
+// fgpu_visc.cuh -- viscous source of one stage state (sources_viscosity.f90).
 //
 // sources_viscosity.f90:484-507 ExternalSources: CalcStresses
 // (physics_eulerisotherm.f90:1023-1198) builds the stress tensor
@@ -14,8 +14,13 @@
 // tile, the stress tensor within one step, then the divergences of its own
 // cells.  The result [ND momentum (+ energy)][n] is read by the stage kernel
 // of the same state, which subtracts it with the other external sources.
+//
+// MOLECULAR viscosity is constant; ALPHA, BETA and POWERLAW keep a dynamic
+// viscosity per padded cell that visc_update_kernel refreshes from the state
+// whenever a right-hand side (or CalcTimestep) comes at a new time, as
+// UpdateViscosity does, and visc_cfl_kernel evaluates their time-step limit.
 #pragma once
-#include "fgpu_device.cuh"
+#include "fgpu_kernels.cuh"
 
 namespace fgpu {
 
@@ -23,11 +28,18 @@ struct ViscArgs {
   Grid g;
   PhysP ph;
   MetricP mt;
-  StateRef in;      // the stage state as the stencil reads it (rin or in)
-  double eta;       // dynamic viscosity (dynconst)
-  double mub;       // bulk viscosity (bulkconst)
+  StateRef in;             // the stage state as the stencil reads it (rin or in)
+  double eta;              // MOLECULAR: dynamic viscosity (dynconst)
+  double mub;              // MOLECULAR: bulk viscosity (bulkconst)
+  const double* dynvis;    // other models: dynamic viscosity by padded cell (bulk = -2/3 of it)
   double* out;
 };
+
+// index of a cell of the ghost-padded grid (coordinates -2 .. n+1; 2D meshes have no z ghosts)
+template <int ND>
+__device__ __forceinline__ long long pad_index(const Grid& g, int i, int j, int k) {
+  return (long long)(i + 2) + (long long)(g.nx + 4) * ((long long)(j + 2) + (long long)(g.ny + 4) * (ND == 3 ? k + 2 : 0));
+}
 
 // mesh_midpoint.f90:586-630 Divergence3D, arguments in the reference's order,
 // evaluated left to right like the reference's expression
@@ -93,17 +105,22 @@ __global__ void __launch_bounds__(TX* TY* TZ) visc_kernel(const __grid_constant_
     const int ip = i0 + a + 2;
     const double dlx = M.dlx[ip], dly = M.dly[ip];
     const double cxyx = M.cxyx[ip], cyxy = M.cyxy[ip];
+    double eta = A.eta, mub = A.mub;
+    if (A.dynvis) {
+      eta = A.dynvis[pad_index<ND>(g, i0 + a, j0 + b, ND == 3 ? k0 + c : 0)];
+      mub = -2. / 3. * eta;
+    }
     const double vx = VV(0, a, b, c), vy = VV(1, a, b, c);
     const double vxW = VV(0, a - 1, b, c), vxE = VV(0, a + 1, b, c), vxS = VV(0, a, b - 1, c), vxN = VV(0, a, b + 1, c);
     const double vyW = VV(1, a - 1, b, c), vyE = VV(1, a + 1, b, c), vyS = VV(1, a, b - 1, c), vyN = VV(1, a, b + 1, c);
     if (ND == 2) {
       // VectorDivergence2D_1 of v (mesh_midpoint.f90:156-183) times the bulk viscosity
-      const double tb = A.mub * div3d(M.dAxW[ip], M.dAxE[ip], M.dAyS[ip], M.dAyS[ip], 0.0, 0.0, M.dydzdV[ip],
+      const double tb = mub * div3d(M.dAxW[ip], M.dAxE[ip], M.dAyS[ip], M.dAyS[ip], 0.0, 0.0, M.dydzdV[ip],
                                       M.dzdxdV[ip], 0.0, 0.0, 0.0, 0.0, 0.0, 0.5 * (vxW + vx), 0.5 * (vxE + vx),
                                       0.5 * (vyS + vy), 0.5 * (vyN + vy), 0.0, 0.0, 0.0, 0.0, 0.0, 0.0);
-      TT(0, a, b, c) = A.eta * ((vxE - vxW) / dlx + 2.0 * cxyx * vy) + tb;
-      TT(1, a, b, c) = A.eta * ((vyN - vyS) / dly + 2.0 * cyxy * vx) + tb;
-      TT(2, a, b, c) = A.eta * (0.5 * ((vyE - vyW) / dlx + (vxN - vxS) / dly) - cxyx * vx - cyxy * vy);
+      TT(0, a, b, c) = eta * ((vxE - vxW) / dlx + 2.0 * cxyx * vy) + tb;
+      TT(1, a, b, c) = eta * ((vyN - vyS) / dly + 2.0 * cyxy * vx) + tb;
+      TT(2, a, b, c) = eta * (0.5 * ((vyE - vyW) / dlx + (vxN - vxS) / dly) - cxyx * vx - cyxy * vy);
     } else {
       const double dlz = M.dlz[ip];
       const double cxzx = M.cxzx[ip], cyzy = M.cyzy[ip], czxz = M.czxz[ip], czyz = M.czyz[ip];
@@ -112,16 +129,16 @@ __global__ void __launch_bounds__(TX* TY* TZ) visc_kernel(const __grid_constant_
       const double vzW = VV(2, a - 1, b, c), vzE = VV(2, a + 1, b, c), vzS = VV(2, a, b - 1, c), vzN = VV(2, a, b + 1, c);
       const double vzB = VV(2, a, b, c - 1), vzT = VV(2, a, b, c + 1);
       // VectorDivergence3D (mesh_midpoint.f90:474-502)
-      const double tb = A.mub * div3d(M.dAxW[ip], M.dAxE[ip], M.dAyS[ip], M.dAyS[ip], M.dAzB[ip], M.dAzB[ip],
+      const double tb = mub * div3d(M.dAxW[ip], M.dAxE[ip], M.dAyS[ip], M.dAyS[ip], M.dAzB[ip], M.dAzB[ip],
                                       M.dydzdV[ip], M.dzdxdV[ip], M.dxdydV[ip], 0.0, 0.0, 0.0, 0.0,
                                       0.5 * (vxW + vx), 0.5 * (vxE + vx), 0.5 * (vyS + vy), 0.5 * (vyN + vy),
                                       0.5 * (vzB + vz), 0.5 * (vzT + vz), 0.0, 0.0, 0.0, 0.0);
-      TT(0, a, b, c) = A.eta * ((vxE - vxW) / dlx + 2.0 * cxyx * vy + 2.0 * cxzx * vz) + tb;
-      TT(1, a, b, c) = A.eta * ((vyN - vyS) / dly + 2.0 * cyxy * vx + 2.0 * cyzy * vz) + tb;
-      TT(2, a, b, c) = A.eta * ((vzT - vzB) / dlz + 2.0 * czxz * vx + 2.0 * czyz * vy) + tb;
-      TT(3, a, b, c) = A.eta * (0.5 * ((vyE - vyW) / dlx + (vxN - vxS) / dly) - cxyx * vx - cyxy * vy);
-      TT(4, a, b, c) = A.eta * (0.5 * ((vzE - vzW) / dlx + (vxT - vxB) / dlz) - czxz * vz - cxzx * vx);
-      TT(5, a, b, c) = A.eta * (0.5 * ((vyT - vyB) / dlz + (vzN - vzS) / dly) - czyz * vz - cyzy * vy);
+      TT(0, a, b, c) = eta * ((vxE - vxW) / dlx + 2.0 * cxyx * vy + 2.0 * cxzx * vz) + tb;
+      TT(1, a, b, c) = eta * ((vyN - vyS) / dly + 2.0 * cyxy * vx + 2.0 * cyzy * vz) + tb;
+      TT(2, a, b, c) = eta * ((vzT - vzB) / dlz + 2.0 * czxz * vx + 2.0 * czyz * vy) + tb;
+      TT(3, a, b, c) = eta * (0.5 * ((vyE - vyW) / dlx + (vxN - vxS) / dly) - cxyx * vx - cyxy * vy);
+      TT(4, a, b, c) = eta * (0.5 * ((vzE - vzW) / dlx + (vxT - vxB) / dlz) - czxz * vz - cxzx * vx);
+      TT(5, a, b, c) = eta * (0.5 * ((vyT - vyB) / dlz + (vzN - vzS) / dly) - czyz * vz - cyzy * vy);
     }
   }
   __syncthreads();
@@ -191,6 +208,115 @@ __global__ void __launch_bounds__(TX* TY* TZ) visc_kernel(const __grid_constant_
   }
 #pragma unroll
   for (int m = 0; m < ND + (EU ? 1 : 0); ++m) A.out[(long long)m * g.n + idx] = sv[m];
+}
+
+// ---------------------------------------------------------------- ALPHA / BETA / POWERLAW
+// sources_viscosity.f90:359-453 UpdateViscosity on the ghost-padded stage state: only when the
+// right-hand side's time differs from the last update's, or is 0.  The time is the host value t
+// or, on the device clock, *t_dev + zeta * *dt_dev (the reference's time + zeta*dt).
+struct VisUpdArgs {
+  Grid g;
+  PhysP ph;
+  MetricP mt;
+  StateRef in;
+  int model;                 // FGPU_VIS_ALPHA / _BETA / _POWERLAW
+  double dynconst, power;
+  const double* ephir;       // [ndim][npad] ephi/r in curvilinear components
+  const double* rad;         // [npad] Mesh%radius at the bary centres
+  double* dynvis;            // [npad]
+  const double* vis_time;    // time of the last update (initially -1)
+  double t;
+  const double* t_dev;
+  const double* dt_dev;
+  double zeta;
+  long long npad;
+  const Ctl* ctl;            // device clock: nothing to do once the run has stopped or broken
+};
+
+__device__ __forceinline__ double vis_rhs_time(const VisUpdArgs& A) {
+  return A.t_dev ? *A.t_dev + A.zeta * *A.dt_dev : A.t;
+}
+
+template <int ND, bool EU>
+__global__ void __launch_bounds__(256) visc_update_kernel(const __grid_constant__ VisUpdArgs A) {
+  using CE = Cells<ND, EU>;
+  constexpr int V = Phys<ND, EU>::V;
+  if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
+  const double t = vis_rhs_time(A);
+  if (!(t != *A.vis_time || t == 0.0)) return;
+  const int NXp = A.g.nx + 4, NYp = A.g.ny + 4;
+  for (long long q = blockIdx.x * 256LL + threadIdx.x; q < A.npad; q += (long long)gridDim.x * 256) {
+    const int px = (int)(q % NXp), py = (int)((q / NXp) % NYp), pz = (int)(q / ((long long)NXp * NYp));
+    double p[V];
+    CE::cell_p(A.in, A.g, A.ph, A.mt, px - 2, py - 2, ND == 3 ? pz - 2 : 0, p);
+    double om = A.ephir[q] * p[1];
+#pragma unroll
+    for (int l = 1; l < ND; ++l) om = om + A.ephir[(long long)l * A.npad + q] * p[1 + l];
+    om = om + 0.0;   // Mesh%Omega of a non-rotating frame
+    const double r = A.rad[q];
+    double eta;
+    if (A.model == 2) {
+      const double cs = A.mt.cs[px];
+      eta = A.dynconst * p[0] * (cs * cs) / fabs(om);
+    } else if (A.model == 3) {
+      eta = A.dynconst * p[0] * (r * r) * fabs(om);
+    } else {
+      eta = A.dynconst * p[0] * pow(r * r * fabs(om), A.power);
+    }
+    A.dynvis[q] = eta;
+  }
+}
+
+// records the update's time (after visc_update_kernel, whose blocks all read the old value)
+__global__ void visc_time_kernel(VisUpdArgs A, double* vis_time) {
+  if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
+  *vis_time = vis_rhs_time(A);
+}
+
+// The viscous time-step limit of sources_viscosity.f90:511-581 with the cell dynamic viscosity,
+// over every cell of the ghost-padded state (CalcTimestep's this%pvar): the maximum of
+// sum_d (max wave speed_d + 2 kinvis/dl_d)/dl_d goes to ctl->invdt[3]
+struct VisCflArgs {
+  Grid g;
+  PhysP ph;
+  MetricP mt;
+  StateRef in;
+  int roundtrip;             // the checked state gets the CHECK_PMIN clamp (ideal gas)
+  const double* dynvis;
+  long long npad;
+  Ctl* ctl;
+};
+
+template <int ND, bool EU>
+__global__ void __launch_bounds__(256) visc_cfl_kernel(const __grid_constant__ VisCflArgs A) {
+  using PH = Phys<ND, EU>;
+  using CE = Cells<ND, EU>;
+  constexpr int V = PH::V;
+  __shared__ double sred[RED_STRIDE * 8];
+  if (A.ctl->stop | A.ctl->brk) return;
+  const MetricP& M = A.mt;
+  const int NXp = A.g.nx + 4, NYp = A.g.ny + 4;
+  double mx = 0.0;
+  for (long long q = blockIdx.x * 256LL + threadIdx.x; q < A.npad; q += (long long)gridDim.x * 256) {
+    const int px = (int)(q % NXp), py = (int)((q / NXp) % NYp), pz = (int)(q / ((long long)NXp * NYp));
+    double p[V];
+    CE::cell_p(A.in, A.g, A.ph, M, px - 2, py - 2, ND == 3 ? pz - 2 : 0, p);
+    if (EU && A.roundtrip) p[V - 1] = dmax(p[V - 1], A.ph.pmin);
+    const double cs = EU ? PH::cs_of(p, A.ph) : M.cs[px];
+    const double dl[3] = {M.dlx[px], M.dly[px], ND == 3 ? M.dlz[px] : 1.0};
+    const double kinvis = A.dynvis[q] / p[0];
+    double s = 0.0;
+#pragma unroll
+    for (int m = 0; m < ND; ++m) {
+      const double v = p[1 + m];
+      const double w = dmax(dmax(0., v + cs), -dmin(0., v - cs));
+      const double term = (w + 2.0 * kinvis / dl[m]) / dl[m];
+      s = m == 0 ? term : s + term;
+    }
+    mx = dmax(mx, s);
+  }
+  double vals[4] = {0.0, 0.0, 0.0, mx};
+  block_reduce_emit<256>(vals, 4, 0, A.ctl->invdt, nullptr, sred);
 }
 
 }  // namespace fgpu

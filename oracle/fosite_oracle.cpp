@@ -92,9 +92,11 @@ struct Oracle {
   std::vector<double> w, wfactor, delxy, fdq, fdql, fflux;
   std::vector<int> shift;
   bool c_trans = false, p_trans = false;     // fargo_transformation_applied flags
-  // ---- viscosity (sources_viscosity.f90, MOLECULAR) ----
+  // ---- viscosity (sources_viscosity.f90) ----
   int vismodel = 0;
-  double dynconst = 0.0, bulkconst = 0.0, cvis = 0.5;
+  double dynconst = 0.0, bulkconst = 0.0, power = 0.0, cvis = 0.5;
+  double vis_time = -1.0;                                     // InitSources: time of the last update
+  std::vector<double> dynvis, bulkvis, kinvis, ephir;         // NC, NC, NC, NC*VDIM
   std::vector<double> btxx, btxy, btxz, btyy, btyz, btzz;   // stress tensor (InitSources: zero)
   std::vector<double> vtmp, vtmp1, vtmp2;                     // Physics%tmp, tmp1, tmp2
 
@@ -169,12 +171,18 @@ struct Oracle {
     // viscosity (sources_viscosity.f90:132-266)
     if (cfg.vismodel) {
       if (VDIM < 2) { err = "viscosity is currently not supported in 1D physics"; return FGPU_EBADCFG; }
-      if (cfg.vismodel != FGPU_VIS_MOLECULAR) { err = "viscosity: the MOLECULAR model only"; return FGPU_EUNSUPPORTED; }
+      if (cfg.vismodel < FGPU_VIS_MOLECULAR || cfg.vismodel > FGPU_VIS_ALPHA_ALT) { err = "Viscosity prescription not supported."; return FGPU_EBADCFG; }
+      if (cfg.vismodel == FGPU_VIS_ALPHA_ALT) { err = "alternative alpha-viscosity currently not supported"; return FGPU_EUNSUPPORTED; }
+      if (cfg.vismodel == FGPU_VIS_ALPHA && euler) { err = "viscosity: ALPHA with isothermal physics only"; return FGPU_EUNSUPPORTED; }
+      if (cfg.vismodel != FGPU_VIS_MOLECULAR && cfg.fargo_method) { err = "viscosity: ALPHA/BETA/POWERLAW without fargo"; return FGPU_EUNSUPPORTED; }
       if (NDIMS == 2 && !(dirs[0] == 0 && dirs[1] == 1)) { err = "viscosity: 2D x-y and 3D meshes only"; return FGPU_EUNSUPPORTED; }
       vismodel = cfg.vismodel;
       dynconst = cfg.dynconst;
       bulkconst = std::isnan(cfg.bulkconst) ? -2. / 3. * dynconst : cfg.bulkconst;
+      power = cfg.vis_exponent;
       cvis = cfg.cvis;
+      dynvis.assign(NC, dynconst); bulkvis.assign(NC, bulkconst); kinvis.assign(NC, 0.0);
+      if (vismodel != FGPU_VIS_MOLECULAR) build_ephir();
       btxx.assign(NC, 0.0); btxy.assign(NC, 0.0); btxz.assign(NC, 0.0);
       btyy.assign(NC, 0.0); btyz.assign(NC, 0.0); btzz.assign(NC, 0.0);
       vtmp.assign(NC, 0.0); vtmp1.assign(NC, 0.0); vtmp2.assign(NC, 0.0);
@@ -983,24 +991,73 @@ struct Oracle {
                  0.5 * (az[x - sz] + az[x]), 0.5 * (az[x + sz] + az[x]),
                  0.0, 0.0, 0.0, 0.0);
   }
+  // sources_viscosity.f90:186-226: ephi/r (azimuthal unit vector over the distance to the
+  // z-axis) from the Cartesian bary centres (Convert2Cartesian, geometry_cylindrical.f90:446-455,
+  // geometry_logcylindrical.f90:344-356), converted to curvilinear components
+  // (geometry_cylindrical.f90:485-494; identity for Cartesian meshes), the VDIM used ones
+  void build_ephir() {
+    ephir.assign(NC * VDIM, 0.0);
+    for (int k = KGMIN; k <= KGMAX; ++k) for (int j = JGMIN; j <= JGMAX; ++j) for (int i = IGMIN; i <= IGMAX; ++i) {
+      long c = id(i, j, k);
+      const double x1 = cx[i - IGMIN], x2 = cy[j - JGMIN], x3 = cz[k - KGMIN];
+      double X, Y;
+      if (cfg.geometry == FGPU_CYLINDRICAL) { X = x1 * std::cos(x2); Y = x1 * std::sin(x2); }
+      else if (cfg.geometry == FGPU_LOGCYLINDRICAL) { double r = cfg.gparam * std::exp(x1); X = r * std::cos(x2); Y = r * std::sin(x2); }
+      else { X = x1; Y = x2; }
+      (void)x3;
+      const double r2 = radius[c] * radius[c];
+      const double ex = -Y / r2, ey = X / r2, ez = 0.0;
+      double e[3];
+      if (cfg.geometry == FGPU_CARTESIAN) { e[0] = ex; e[1] = ey; e[2] = ez; }
+      else {
+        e[0] = ex * std::cos(x2) + ey * std::sin(x2);
+        e[1] = -ex * std::sin(x2) + ey * std::cos(x2);
+        e[2] = ez;
+      }
+      for (int l = 0; l < VDIM; ++l) ephir[c + NC * l] = e[dirs[l]];
+    }
+  }
+  // sources_viscosity.f90:359-453 UpdateViscosity: recomputed only when the time differs from
+  // the last update's (or is 0); the dynamic viscosity of ALPHA (alpha rho cs^2/|Omega|), BETA
+  // (beta rho r^2 |Omega|) and POWERLAW (beta rho (r^2 |Omega|)^q) with Omega = ephi/r . v
+  // (Mesh%Omega = 0), and the trace-free bulk viscosity -2/3 eta
+  void update_viscosity(double t, std::vector<double>& pv) {
+    if (!(t != vis_time || t == 0.0)) return;
+    if (vismodel != FGPU_VIS_MOLECULAR) {
+      for (long x = 0; x < NC; ++x) {
+        double om = ephir[x] * pv[x + NC * 1];
+        for (int l = 1; l < VDIM; ++l) om = om + ephir[x + NC * l] * pv[x + NC * (1 + l)];
+        om = om + 0.0;
+        const double rho = pv[x], r = radius[x];
+        double eta;
+        if (vismodel == FGPU_VIS_ALPHA) eta = dynconst * rho * (bccsound[x] * bccsound[x]) / std::fabs(om);
+        else if (vismodel == FGPU_VIS_BETA) eta = dynconst * rho * (r * r) * std::fabs(om);
+        else eta = dynconst * rho * std::pow(r * r * std::fabs(om), power);
+        dynvis[x] = eta;
+      }
+      for (long x = 0; x < NC; ++x) bulkvis[x] = -2. / 3. * dynvis[x];
+    }
+    vis_time = t;
+  }
+
   // physics_eulerisotherm.f90:1023-1198 CalcStresses (x-y and x-y-z velocities) with the
-  // constant dynamic and bulk viscosity of the MOLECULAR model
+  // cell values of the dynamic and bulk viscosity
   void calc_stresses(std::vector<double>& pv) {
     const double* vx = &pv[NC * 1];
     const double* vy = &pv[NC * 2];
     const double* vz = NDIMS == 3 ? &pv[NC * 3] : nullptr;
     const long sy = NI, sz = (long)NI * NJ;
-    const double dynvis = dynconst, bulkvis = bulkconst;
     for (int k = KGMIN + KP1; k <= KGMAX - KP1; ++k)
       for (int j = JGMIN + JP1; j <= JGMAX - JP1; ++j)
         for (int i = IGMIN + IP1; i <= IGMAX - IP1; ++i) {
           long x = id(i, j, k);
-          vtmp[x] = bulkvis * vector_divergence(x, vx, vy, vz);
+          vtmp[x] = bulkvis[x] * vector_divergence(x, vx, vy, vz);
         }
     for (int k = KMIN - KP1; k <= KMAX + KP1; ++k)
       for (int j = JMIN - JP1; j <= JMAX + JP1; ++j)
         for (int i = IMIN - IP1; i <= IMAX + IP1; ++i) {
           long x = id(i, j, k);
+          const double dynvis = this->dynvis[x];
           if (NDIMS == 2) {
             btxx[x] = dynvis * ((vx[x + 1] - vx[x - 1]) / dlx[x] + 2.0 * cxyx[x] * vy[x]) + vtmp[x];
             btyy[x] = dynvis * ((vy[x + sy] - vy[x - sy]) / dly[x] + 2.0 * cyxy[x] * vx[x]) + vtmp[x];
@@ -1025,7 +1082,8 @@ struct Oracle {
   // sources_viscosity.f90:484-507 ExternalSources: CalcStresses, then ViscositySources
   // (physics_eulerisotherm.f90:982-1017 tensor divergence with btyx = btxy etc., mesh_midpoint.f90:
   // 283-323 / 508-580; physics_euler.f90:1887-1943 energy = div(v.T)), added to the list's sterm
-  void viscosity_sources(std::vector<double>& pv, std::vector<double>& s) {
+  void viscosity_sources(double t, std::vector<double>& pv, std::vector<double>& s) {
+    update_viscosity(t, pv);
     calc_stresses(pv);
     const double* vx = &pv[NC * 1];
     const double* vy = &pv[NC * 2];
@@ -1088,10 +1146,10 @@ struct Oracle {
 
   // sources_generic.f90:220-261 -> sources_gravity.f90:164-200 -> physics ExternalSources;
   // the list holds gravity first (prepended last, sources_generic.f90:190-199), then viscosity
-  void external_sources(std::vector<double>& pv, std::vector<double>& cv, std::vector<double>& s) {
+  void external_sources(double t, std::vector<double>& pv, std::vector<double>& cv, std::vector<double>& s) {
     std::fill(s.begin(), s.end(), 0.0);
     external_gravity(cv, s);
-    if (vismodel) viscosity_sources(pv, s);
+    if (vismodel) viscosity_sources(t, pv, s);
     zero_ghosts(s);
   }
   void external_gravity(std::vector<double>& cv, std::vector<double>& s) {
@@ -1109,8 +1167,8 @@ struct Oracle {
     }
   }
 
-  // timedisc_base.f90:1073-1271 ComputeRHS (rhstype 0)
-  void compute_rhs(std::vector<double>& pv, std::vector<double>& cv, int checkbm, std::vector<double>& r) {
+  // timedisc_base.f90:1073-1271 ComputeRHS (rhstype 0) at time t
+  void compute_rhs(double t, std::vector<double>& pv, std::vector<double>& cv, int checkbm, std::vector<double>& r) {
     if (fargo) add_bg(pv, cv);
     center_boundary(pv, cv);
     if ((checkbm & FGPU_CHECK_PMIN) && euler) {
@@ -1121,7 +1179,7 @@ struct Oracle {
       for (long x = 0; x < NC; ++x) bccsound[x] = soundspeed(pvar[x], pvar[x + NC * PRESSURE]);
     if (checkbm != FGPU_CHECK_NOTHING) check_data(pv, cv, checkbm);
     geometrical_sources(pv, cv, geo_src);
-    external_sources(pv, cv, src);
+    external_sources(t, pv, cv, src);
     if (fargo) {
       if (cfg.geometry == FGPU_CARTESIAN) std::fill(geo_src.begin(), geo_src.end(), 0.0);
       add_fargo_sources(pv, cv, geo_src);
@@ -1211,9 +1269,11 @@ struct Oracle {
     // the viscosity its advection-diffusion limit (sources_viscosity.f90:511-581)
     double dt = dt_cfl;
     if (vismodel) {
+      update_viscosity(time, pvar);
+      for (long x = 0; x < NC; ++x) kinvis[x] = dynvis[x] / pvar[x];
       double ivis = 0.0;
       for (long x = 0; x < NC; ++x) {
-        const double kinvis = dynconst / pvar[x];
+        const double kinvis = this->kinvis[x];
         double v = 0.0;
         for (int m = 0; m < NDIMS; ++m) {
           const double dl = dls[dirs[m]][x];
@@ -1279,7 +1339,7 @@ struct Oracle {
           double e = eta[order - 1][n - 1];
           for (long x = 0; x < NS; ++x) cvar[x] = update_me(e, dtv, cold[x], cvar[x], rhs[x]);
           if (outbound) update_bflux(e, dtv);
-          if (n < order) compute_rhs(pvar, cvar, FGPU_CHECK_NOTHING, rhs);
+          if (n < order) compute_rhs(t0 + zeta[order - 1][n - 1] * dtv, pvar, cvar, FGPU_CHECK_NOTHING, rhs);
         }
         errv = 0.0; dtv = HUGE_;
       } else {
@@ -1291,12 +1351,12 @@ struct Oracle {
           for (long x = 0; x < NS; ++x) cout[x] = update_me(e, dtv, cold[x], cin[x], rhs[x]);
           if (n == 2 && order == 3)
             for (long x = 0; x < NS; ++x) ctmp[x] = update_me(eta[1][1], dtv, cold[x], ctmp[x], rhs[x]);
-          if (n < order) compute_rhs(*P[n], *C[n], FGPU_CHECK_NOTHING, rhs);
+          if (n < order) compute_rhs(t0 + zeta[order - 1][n - 1] * dtv, *P[n], *C[n], FGPU_CHECK_NOTHING, rhs);
         }
         errv = compute_error(cvar, ctmp);
         dtv = adjust_timestep(errv, dtv);
       }
-      (void)t0; (void)zeta;
+      (void)zeta;
       return;
     }
     // Butcher engine; coeff[0] is this%rhs
@@ -1310,7 +1370,7 @@ struct Oracle {
         double a = A[(m - 1) * m_stages + (mm - 1)];
         for (long x = 0; x < NS; ++x) ctmp[x] = ctmp[x] - a * dtv * (*K[mm - 1])[x];
       }
-      compute_rhs(ptmp, ctmp, FGPU_CHECK_NOTHING, *K[m - 1]);
+      compute_rhs(t0 + c_coef[m - 1] * dtv, ptmp, ctmp, FGPU_CHECK_NOTHING, *K[m - 1]);
     }
     ctmp = cvar;
     for (int m = 1; m <= m_stages; ++m) {
@@ -1343,13 +1403,13 @@ struct Oracle {
       else if (e > HUGE_) brk = true;
       else if (e >= 1.0) {   // RejectSolution
         cvar = cold;
-        compute_rhs(pvar, cvar, FGPU_CHECK_NOTHING, rhs);
+        compute_rhs(t, pvar, cvar, FGPU_CHECK_NOTHING, rhs);
         if (outbound) bxf = bxo;   // RejectSolution (timedisc_base.f90:980-1000)
         n_adj++; dtcause = FGPU_DTCAUSE_ERRADJ;
         if (d < dtmin) { dtmin = d; dtmincause = dtcause; }
       } else {               // AcceptSolution
         t = t + dtold_;
-        if (t < time + dt) { compute_rhs(pvar, cvar, checkdatabm, rhs); cold = cvar; }
+        if (t < time + dt) { compute_rhs(t, pvar, cvar, checkdatabm, rhs); cold = cvar; }
         if (outbound) bxo = bxf;   // AcceptSolution (timedisc_base.f90:937-958)
         iter++;
       }
@@ -1364,9 +1424,9 @@ struct Oracle {
         fargo_advection_y();
         c2p_range(cvar, pvar, IGMIN, IGMAX, JGMIN, JGMAX, KGMIN, KGMAX);
         p_trans = c_trans;
-        compute_rhs(pvar, cvar, checkdatabm, rhs);
+        compute_rhs(time, pvar, cvar, checkdatabm, rhs);
       } else {
-        compute_rhs(pvar, cvar, checkdatabm, rhs);
+        compute_rhs(time, pvar, cvar, checkdatabm, rhs);
       }
       cold = cvar;
     }
@@ -1376,7 +1436,7 @@ struct Oracle {
   void first_step() {
     iter = 0;
     if (fargo == 1) { center_boundary(pvar, cvar); calc_background_velocity(pvar, cvar); }
-    compute_rhs(pvar, cvar, FGPU_CHECK_ALL, rhs);
+    compute_rhs(time, pvar, cvar, FGPU_CHECK_ALL, rhs);
     dt = calc_timestep();
     cold = cvar;
   }
@@ -1462,7 +1522,7 @@ int orc_get(orc_handle* h, int which, double* out) {
 }
 int orc_first_step(orc_handle* h) { h->o.first_step(); return h->o.brk ? FGPU_BREAK : 0; }
 int orc_step(orc_handle* h) { return h->o.step(); }
-int orc_compute_rhs(orc_handle* h) { h->o.compute_rhs(h->o.pvar, h->o.cvar, FGPU_CHECK_NOTHING, h->o.rhs); return 0; }
+int orc_compute_rhs(orc_handle* h) { h->o.compute_rhs(h->o.time, h->o.pvar, h->o.cvar, FGPU_CHECK_NOTHING, h->o.rhs); return 0; }
 double orc_calc_timestep(orc_handle* h) { return h->o.calc_timestep(); }
 int orc_get_status(orc_handle* h, fgpu_status* st) {
   Oracle& o = h->o;

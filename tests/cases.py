@@ -248,6 +248,18 @@ def _visc(case, dynconst, bulkconst=None, cvis=0.5):
     return c, p, extra
 
 
+def _visc_model(case, model, dynconst, exponent=0.0, cvis=0.5, **kw):
+    """Add an ALPHA/BETA/POWERLAW viscosity (sources_viscosity.f90:359-453) and set other keys."""
+    c, p, extra = case
+    c.vismodel = model
+    c.dynconst = dynconst
+    c.vis_exponent = exponent
+    c.cvis = cvis
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c, p, extra
+
+
 def khi_reynolds(re=1.0e4, rho0=1.0, xyzlen=1.0, v0=-0.5, v1=0.5):
     """Dynamic viscosity of tests/KHI2D.f90:236-239 and tests/KHI3D.f90:328-331."""
     return abs(rho0 * xyzlen * (v0 - v1) / re)
@@ -321,6 +333,24 @@ CASES = {
                                                                abi.PERIODIC]), 2e-3),
     "euler_disk_cyl_visc_prim": lambda: _visc(_euler_fargo(n=(24, 40), geometry=abi.CYLINDRICAL,
                                                            variables=abi.PRIMITIVE, fargo=0), 1e-3),
+    # state-dependent viscosities with UpdateViscosity's time caching; the first is the
+    # set-up of tests/pringle.f90 (cylindrical disk, POWERLAW q = 0, SSPRK, tolerances)
+    "disk_powerlaw_pringle_ssprk5": lambda: _visc_model(
+        _disk(geometry=abi.CYLINDRICAL, n=(30, 36), bcs=[abi.NO_GRADIENTS, abi.REFLECTING, abi.PERIODIC, abi.PERIODIC]),
+        abi.VIS_POWERLAW, 1e-3, 0.0, cvis=0.3, method=abi.SSPRK, tdorder=5, tol_rel=0.01),
+    "disk_beta_logcyl_me3": lambda: _visc_model(
+        _disk(bcs=[abi.NO_GRADIENTS, abi.REFLECTING, abi.PERIODIC, abi.PERIODIC]), abi.VIS_BETA, 1e-3),
+    "disk_alpha_cyl_me2": lambda: _visc_model(
+        _disk(geometry=abi.CYLINDRICAL, n=(28, 40), bcs=[abi.REFLECTING, abi.NO_GRADIENTS, abi.PERIODIC, abi.PERIODIC]),
+        abi.VIS_ALPHA, 1e-2, tdorder=2),
+    "disk_powerlaw_q05_adaptive_me": lambda: _visc_model(
+        _disk(geometry=abi.CYLINDRICAL, n=(26, 32), bcs=[abi.REFLECTING, abi.REFLECTING, abi.PERIODIC, abi.PERIODIC]),
+        abi.VIS_POWERLAW, 2e-3, 0.5, tol_rel=1e-3),
+    "khi_powerlaw_me1": lambda: _visc_model(_khi(order=abi.CONSTANT, tdorder=1, n=(30, 26)), abi.VIS_POWERLAW, 1e-3, 0.0),
+    "iso3d_beta_dopri": lambda: _visc_model(
+        _with(_iso3d(n=(12, 14, 10)), method=abi.DORMAND_PRINCE,
+              bc=(abi.REFLECTING, abi.NO_GRADIENTS, abi.PERIODIC, abi.PERIODIC, abi.REFLECTING, abi.NO_GRADIENTS)),
+        abi.VIS_BETA, 1e-2),
 }
 
 
