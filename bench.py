@@ -30,6 +30,9 @@ WORKLOADS = {
     "khi2d": "2D Kelvin-Helmholtz 256^2, periodic, KT+van Leer(cons), SSPRK3 fixed CFL 0.4",
     "disk2d": "2D isothermal Keplerian disk, logcylindrical 512x1024, point mass GM=1, sigma~1/r, cs/vK=0.05, "
               "FARGO shift, KT+van Leer(prim), SSPRK3 fixed CFL 0.4, absorbing r / periodic phi",
+    "khi2d_visc": "khi2d with the KHI2D test's molecular viscosity at Reynolds number 1e4 (256^2)",
+    "khi3d_visc": "3D Kelvin-Helmholtz 128^3 (tests/KHI3D.f90 set-up), periodic, KT+MC 1.2(cons), SSPRK3 fixed "
+                  "CFL 0.4, molecular viscosity at Reynolds number 1e4",
 }
 
 
@@ -40,6 +43,10 @@ def make_problem(name, size):
     if name == "disk2d":
         nr = size or 512
         return problems.disk2d(nr=nr, nphi=2 * nr, fargo=1)
+    if name == "khi2d_visc":
+        return problems.khi2d(n=size or 256, re=1.0e4)
+    if name == "khi3d_visc":
+        return problems.khi3d(n=size or 128, re=1.0e4)
     return problems.khi2d(n=size or 256)
 
 
@@ -63,7 +70,12 @@ def algorithmic_bytes_per_cell_update(name, vnum):
     and the transport reads it and writes the state (2): 11 arrays.
     """
     arrays = {"gauss3d": 37, "disk2d": 11}.get(name, 8)
-    return arrays * vnum * 8.0
+    fields = arrays * vnum
+    if name.endswith("_visc"):
+        # per stage the viscous pass reads the state and writes ND momentum + energy sources,
+        # which the stage kernel reads: V + 2 (V - 1) more fields
+        fields += 3 * (vnum + 2 * (vnum - 1))
+    return fields * 8.0
 
 
 class ClockSampler:
@@ -135,7 +147,7 @@ def cpu_baseline(name, budget_s=20.0):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     from fosite_b200 import abi
-    size = {"gauss3d": 48, "disk2d": 128}.get(name, 256)
+    size = {"gauss3d": 48, "disk2d": 128, "khi3d_visc": 32}.get(name, 256)
     cfg, p, extra = make_problem(name, size)
     o = pyoracle.Oracle(cfg)
     apply_extra(o, cfg, extra)

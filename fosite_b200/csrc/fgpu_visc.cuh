@@ -41,6 +41,29 @@ __device__ __forceinline__ long long pad_index(const Grid& g, int i, int j, int 
   return (long long)(i + 2) + (long long)(g.nx + 4) * ((long long)(j + 2) + (long long)(g.ny + 4) * (ND == 3 ? k + 2 : 0));
 }
 
+// Density and velocity of an interior cell of a stage state, as Cells::interior_p gives them
+// (the FARGO frame chain without round trips, then Cons2Prim's m * (1/rho)), reading only the
+// density and momentum fields (the velocity of a formed primitive state directly)
+template <int ND>
+__device__ __forceinline__ void interior_rv(const StateRef& S, long long n, long long idx, int ip, double* rv) {
+  const double* b = S.base + idx;
+#pragma unroll
+  for (int v = 0; v <= ND; ++v) rv[v] = __ldg(b + (long long)v * n);
+#pragma unroll 1
+  for (int q = 0; q < S.nk; ++q) {
+    const double* kq = S.K[q] + idx;
+    const double a = S.coef[q];
+#pragma unroll
+    for (int v = 0; v <= ND; ++v) rv[v] = rv[v] - a * __ldg(kq + (long long)v * n);
+  }
+  if (S.ready) return;
+  if (ND == 2)
+    for (int q = 0; q < S.pre.n; ++q) rv[2] = rv[2] + S.pre.s[q] * (rv[0] * S.pre.w[q][ip]);
+  const double inv_rho = 1. / rv[0];
+#pragma unroll
+  for (int m = 1; m <= ND; ++m) rv[m] = rv[m] * inv_rho;
+}
+
 // mesh_midpoint.f90:586-630 Divergence3D, arguments in the reference's order,
 // evaluated left to right like the reference's expression
 __device__ __forceinline__ double div3d(double aW, double aE, double aS, double aN, double aB, double aT,
@@ -89,9 +112,14 @@ __global__ void __launch_bounds__(TX* TY* TZ) visc_kernel(const __grid_constant_
   for (int t = threadIdx.x; t < VX * VY * VZ; t += NT) {
     const int lx = t % VX, r = t / VX, ly = r % VY, lz = r / VY;
     const int a = lx - 2, b = ly - 2, c = lz - L::HZ;
-    if (outside(a, ex) + outside(b, ey) + (ND == 3 ? outside(c, ez) : 0) > 2) continue;
+    const int ox = outside(a, ex), oy = outside(b, ey), oz = ND == 3 ? outside(c, ez) : 0;
+    if (ox + oy + oz > 2) continue;
+    const int gi = i0 + a, gj = j0 + b, gk = ND == 3 ? k0 + c : 0;
     double p[V];
-    CE::cell_p(A.in, g, A.ph, M, i0 + a, j0 + b, ND == 3 ? k0 + c : 0, p);
+    if (gi >= 0 && gi < g.nx && gj >= 0 && gj < g.ny && gk >= 0 && gk < g.nz)
+      interior_rv<ND>(A.in, g.n, CE::lin(g, gi, gj, gk), gi + 2, p);
+    else
+      CE::cell_p(A.in, g, A.ph, M, gi, gj, gk, p);
 #pragma unroll
     for (int m = 0; m < ND; ++m) Vs[((m * VZ + lz) * VY + ly) * VX + lx] = p[1 + m];
   }
@@ -247,8 +275,12 @@ __global__ void __launch_bounds__(256) visc_update_kernel(const __grid_constant_
   const int NXp = A.g.nx + 4, NYp = A.g.ny + 4;
   for (long long q = blockIdx.x * 256LL + threadIdx.x; q < A.npad; q += (long long)gridDim.x * 256) {
     const int px = (int)(q % NXp), py = (int)((q / NXp) % NYp), pz = (int)(q / ((long long)NXp * NYp));
+    const int gi = px - 2, gj = py - 2, gk = ND == 3 ? pz - 2 : 0;
     double p[V];
-    CE::cell_p(A.in, A.g, A.ph, A.mt, px - 2, py - 2, ND == 3 ? pz - 2 : 0, p);
+    if (gi >= 0 && gi < A.g.nx && gj >= 0 && gj < A.g.ny && gk >= 0 && gk < A.g.nz)
+      interior_rv<ND>(A.in, A.g.n, CE::lin(A.g, gi, gj, gk), px, p);
+    else
+      CE::cell_p(A.in, A.g, A.ph, A.mt, gi, gj, gk, p);
     double om = A.ephir[q] * p[1];
 #pragma unroll
     for (int l = 1; l < ND; ++l) om = om + A.ephir[(long long)l * A.npad + q] * p[1 + l];

@@ -41,8 +41,19 @@ def _base(n, nd):
     return c
 
 
-def khi2d(n=256, seed=1000, steps=1000):
-    """2D Kelvin-Helmholtz, Euler gamma=1.4, periodic, KT + van Leer, SSPRK3 fixed CFL 0.4."""
+def with_viscosity(c, re, rho0=1.0, xyzlen=1.0, dv=1.0):
+    """The molecular viscosity of tests/KHI2D.f90:236-239 / tests/KHI3D.f90:328-331:
+    dynconst = |rho0 * L * (V0 - V1) / RE|, bulk viscosity -2/3 of it."""
+    eta = abs(rho0 * xyzlen * (-dv) / re)
+    c.vismodel = abi.VIS_MOLECULAR
+    c.dynconst = eta
+    c.bulkconst = -2. / 3. * eta
+    return c
+
+
+def khi2d(n=256, seed=1000, steps=1000, re=None):
+    """2D Kelvin-Helmholtz, Euler gamma=1.4, periodic, KT + van Leer, SSPRK3 fixed CFL 0.4;
+    re: Reynolds number of the molecular viscosity (None: inviscid)."""
     c = _base((n, n, 1), 2)
     c.xmin, c.xmax, c.ymin, c.ymax = -0.5, 0.5, -0.5, 0.5
     c.physics = abi.EULER
@@ -63,7 +74,42 @@ def khi2d(n=256, seed=1000, steps=1000):
     p[1] = np.where(band, 0.5, -0.5) + rng.uniform(-1e-3, 1e-3, X.shape)
     p[2] = 0.01 * np.sin(4 * np.pi * X) + rng.uniform(-1e-3, 1e-3, X.shape)
     p[3] = 2.5
+    if re is not None:
+        with_viscosity(c, re)
     return c, p, {"steps": steps}
+
+
+def khi3d(n=128, seed=1500, re=1.0e4):
+    """tests/KHI3D.f90: periodic 3D shear layer (flow along x, jump across y), Euler gamma 1.4,
+    KT + MC(theta 1.2) on conservative variables, SSPRK3 fixed CFL 0.4, the test's molecular
+    viscosity (RE = 1e4; None: inviscid) and seeded velocity noise of amplitude 0.1."""
+    c = _base((n, n, n), 3)
+    c.xmin, c.xmax, c.ymin, c.ymax, c.zmin, c.zmax = -0.5, 0.5, -0.5, 0.5, -0.5, 0.5
+    for f in range(6):
+        c.bc[f] = abi.PERIODIC
+    c.physics = abi.EULER
+    c.gamma = 1.4
+    c.limiter = abi.MONOCENT
+    c.theta = 1.2
+    c.variables = abi.CONSERVATIVE
+    c.method = abi.MODIFIED_EULER
+    c.tdorder = 3
+    c.tol_rel = 10.0
+    c.cfl = 0.4
+    c.stoptime = 1.0e3
+    if re is not None:
+        with_viscosity(c, re)
+    abi.finalize_config(c)
+    X, Y, Z, _ = centers(c)
+    rng = np.random.default_rng(seed)
+    inner = np.abs(Y) <= 0.25
+    p = np.zeros((5,) + X.shape)
+    p[0] = np.where(inner, 2.0, 1.0)
+    p[1] = np.where(inner, 0.5, -0.5) + (rng.uniform(0.0, 1.0, X.shape) - 0.5) * 0.2
+    p[2] = (rng.uniform(0.0, 1.0, X.shape) - 0.5) * 0.2
+    p[3] = (rng.uniform(0.0, 1.0, X.shape) - 0.5) * 0.2
+    p[4] = 2.5
+    return c, p, {}
 
 
 def gauss3d(n=256, seed=2000, mc_theta=1.0, method=None):
