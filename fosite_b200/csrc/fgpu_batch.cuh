@@ -321,10 +321,54 @@ int fgpu_batch_autotune(fgpu_batch* b, int reps, int* variant) {
   return FGPU_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// Tuning decisions of this process, by the key of what the stage kernel's cost depends on
+// (device, dimensionality, physics, reconstruction variables and limiter, geometry, mesh
+// size and the optional source/transport features): a grid with a known key reuses the
+// measured layout without probing.
+struct TuneKey {
+  int device, nd, euler, prim, order, limiter, geometry, nx, ny, nz, features;
+  bool operator<(const TuneKey& o) const {
+    return std::memcmp(this, &o, sizeof(TuneKey)) < 0;
+  }
+};
+std::mutex g_tune_mutex;
+std::map<TuneKey, int> g_tune_cache;
+TuneKey tune_key(const fgpu_handle* h) {
+  TuneKey k;
+  std::memset(&k, 0, sizeof(k));
+  k.device = h->device; k.nd = h->nd; k.euler = h->euler; k.prim = h->prim;
+  k.order = h->cfg.order; k.limiter = h->cfg.limiter; k.geometry = h->cfg.geometry;
+  k.nx = h->g.nx; k.ny = h->g.ny; k.nz = h->g.nz;
+  k.features = (h->fargo ? 1 : 0) | (h->accrete ? 2 : 0) | (h->vis ? 4 : 0) | (h->has_accel ? 8 : 0) |
+               (h->butcher ? 16 : 0) | (h->materialize ? 32 : 0);
+  return k;
+}
+}  // namespace
+
+extern "C" {
+
 // Measures each stage-kernel layout on this grid (RHS evaluations into a
-// scratch array, the state is not touched) and keeps the fastest.
+// scratch array, the state is not touched) and keeps the fastest; a grid whose
+// tuning key was measured before in this process takes the cached choice
+// (reps < 0 measures |reps| times regardless and refreshes the cache).
 int fgpu_autotune(fgpu_handle* h, int reps, int* variant) {
   if (!h) return FGPU_EARG;
+  const TuneKey key = tune_key(h);
+  if (reps >= 0) {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      if (h->variant != it->second && h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; h->graph_steps = 0; }
+      if (h->variant != it->second && h->bt_graph) { cudaGraphExecDestroy(h->bt_graph); h->bt_graph = nullptr; }
+      h->variant = it->second;
+      if (variant) *variant = it->second;
+      return FGPU_OK;
+    }
+  }
+  reps = reps < 0 ? -reps : reps;
   if (reps < 1) reps = 3;
   double* scratch = h->butcher ? h->buf[2 + h->T.m - 1] : h->buf[2];
   StageArgs A = base_args(h);
@@ -346,7 +390,12 @@ int fgpu_autotune(fgpu_handle* h, int reps, int* variant) {
   }
   h->variant = bv;
   if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; h->graph_steps = 0; }
+  if (h->bt_graph) { cudaGraphExecDestroy(h->bt_graph); h->bt_graph = nullptr; }
   if (variant) *variant = bv;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[key] = bv;
+  }
   return FGPU_OK;
 }
 

@@ -1,0 +1,133 @@
+// fgpu_bt.cuh -- the embedded Runge-Kutta step loop on the device clock.
+//
+// fosite's IntegrationStep (timedisc_base.f90:649-750) repeats attempts until
+// the sub-steps cover dt: reject (cvar = cold, RHS again), accept (advance t,
+// RHS at t while t < time + dt), then the closing RHS with CheckData and
+// CalcTimestep; the step size comes from AdjustTimestep's PI controller
+// (timedisc_base.f90:759-814).  Here that loop is a state machine in the
+// control block: every captured "slot" runs one attempt -- bt_begin_kernel opens
+// a fosite step when the previous one is done (stop test, output-time clip),
+// the stage kernels run with dt read on the device, bt_decide_kernel evaluates
+// the error norm, the controller and the accept/reject predicate, and the
+// slot's remaining kernels (the RHS of the restored or advanced state, the
+// closing RHS, the CFL reduction and bt_finish_kernel) run only when their
+// action bit is set.  The host replays slots without reading anything back
+// until it wants to know how far the run has come.
+#pragma once
+#include "fgpu_kernels_misc.cuh"
+#include "fgpu_ddmath.h"
+
+namespace fgpu {
+
+struct BtParams {
+  int order;        // the scheme's order (the controller's exponent)
+  double beta;      // PI controller parameter
+  double tol_rel;
+};
+
+// fosite%Step's opening (fosite.f90:367-388 stop test; io/fileio_base.f90:604-621
+// output-time clip) and IntegrationStep's loop head (timedisc_base.f90:649-676)
+// when the slot starts a step; then this slot's attempt.
+__global__ void bt_begin_kernel(Ctl* c) {
+  c->act = 0;
+  if (c->stop | c->brk) return;
+  if (c->phase == 0) {
+    if (c->steps_left <= 0) return;
+    if (fabs(c->stoptime - c->time) <= 1.0E-05 * c->stoptime) { c->stop = 1; return; }
+    if ((c->time + c->dt) / c->tout > 1.0) { c->dt = c->tout - c->time; c->dtcause = -4; }
+    else if ((c->time + 1.5 * c->dt) / c->tout > 1.0) { c->dt = 0.5 * (c->tout - c->time); c->dtcause = -4; }
+    c->t_loc = c->time;
+    c->d_att = c->dt;
+    if (c->d_att < c->dtmin && c->dtcause != -4) c->dtmin = c->d_att;
+    c->rhs_done = 0;
+    c->phase = 1;
+  }
+  c->dtold_att = c->d_att;
+  c->act = ACT_ATTEMPT;
+}
+
+// timedisc_base.f90:759-814 AdjustTimestep with correctly rounded exp/log
+__device__ double bt_adjust(Ctl* c, const BtParams& P, double maxerr, double dtold_) {
+  double dtnew, dttmp;
+  if (P.tol_rel >= 1.0) return DBL_MAX;
+  if (maxerr > 0.) dttmp = 0.9 * dtold_ * ddm::exp_cr(-ddm::log_cr(maxerr) / P.order);
+  else dttmp = 4. * dtold_;
+  if (c->maxerrold > 0.) dtnew = dttmp * ddm::exp_cr(-P.beta * ddm::log_cr(c->maxerrold / maxerr));
+  else dtnew = dttmp;
+  if (maxerr < 1.0) {
+    const double cap = 4. * dtold_;
+    dtnew = cap < dtnew ? cap : dtnew;
+    if (dtnew < dtold_) c->dtcause = -2;
+  } else {
+    if (dtnew > dtold_) dtnew = dttmp;
+    const double floor_ = 0.25 * dtold_;
+    dtnew = dtnew < floor_ ? floor_ : dtnew;
+  }
+  c->maxerrold = maxerr;
+  return dtnew;
+}
+
+// The body of IntegrationStep's loop after SolveODE (timedisc_base.f90:684-710): break on a
+// NaN/Inf error, RejectSolution or AcceptSolution (timedisc_base.f90:911-1009), the dtlimit
+// test, the loop condition, and the loop's closing (timedisc_base.f90:712-720).
+__global__ void bt_decide_kernel(Ctl* c, BtParams P) {
+  if (!(c->act & ACT_ATTEMPT) || (c->stop | c->brk)) { c->act = 0; return; }
+  const double e = __longlong_as_double((long long)c->err);
+  c->err = 0ULL;
+  c->last_err = e;
+  const double d = bt_adjust(c, P, e, c->dtold_att);
+  int act = 0;
+  c->rhs_done = 0;
+  if (e != e) c->brk = 1;
+  else if (e > DBL_MAX) c->brk = 1;
+  else if (e >= 1.0) {
+    act |= ACT_REJECT;
+    c->n_adj += 1;
+    c->dtcause = -1;
+    if (d < c->dtmin) c->dtmin = d;
+  } else {
+    c->t_loc = c->t_loc + c->dtold_att;
+    if (c->t_loc < c->time + c->dt) { act |= ACT_SUB; c->rhs_done = 1; }
+    c->iter += 1;
+  }
+  if (d < c->dtlimit) c->brk = 1;
+  c->d_att = d;
+  if (!c->brk && !(c->t_loc + d <= c->time + c->dt)) {
+    c->dt = c->t_loc - c->time;
+    c->time = c->t_loc;
+    c->dtold = d;
+    act |= ACT_END;
+    if (c->rhs_done) act |= ACT_COPY;
+  }
+  c->act = act;
+}
+
+// CalcTimestep's closing arithmetic after the step's closing RHS and ghost-cell pass
+// (timedisc_base.f90:885-909, the sources list's viscous limit), CheckData's break, and the
+// count of completed fosite steps.
+__global__ void bt_finish_kernel(Ctl* c, int nd) {
+  if ((c->stop | c->brk) || !(c->act & ACT_END)) return;
+  auto D = [](unsigned long long b) { return __longlong_as_double((long long)b); };
+  const double invdt = nd == 2 ? D(c->invdt[0]) : dmax(dmax(D(c->invdt[1]), D(c->invdt[2])), D(c->invdt[0]));
+  const double ivis = D(c->invdt[3]);
+  c->invdt[0] = c->invdt[1] = c->invdt[2] = c->invdt[3] = 0ULL;
+  if (c->flags) {
+    c->checkflags |= c->flags;
+    c->flags = 0;
+    c->brk = 1;
+    return;
+  }
+  double dt = c->cfl / invdt;
+  int cause = 0;
+  if (c->vis) {
+    const double dtv = ivis > DBL_MIN ? c->cvis / ivis : DBL_MAX;
+    if (dtv < dt) cause = 3;
+    dt = dtv < dt ? dtv : dt;
+  }
+  c->dt = dt;
+  c->dtcause = cause;
+  c->phase = 0;
+  c->steps_left -= 1;
+}
+
+}  // namespace fgpu

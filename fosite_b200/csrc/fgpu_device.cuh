@@ -77,6 +77,8 @@ struct StateRef {
   Chain pre;
   // 1: base holds primitive variables already formed from a stage state (nk = 0)
   int ready;
+  // device clock: coef[q] holds the tableau entry, multiplied by *dt_dev when read
+  const double* dt_dev;
 };
 
 // One frame change of a conservative 2D state c by s*w (s = +1 add, -1 subtract).  With
@@ -115,7 +117,26 @@ struct Ctl {
   int stop, brk, dtcause, pad;
   double cvis;                   // viscous Courant number (vis = 1)
   int vis, pad2;
+  // embedded Runge-Kutta schemes on the device clock: the IntegrationStep sub-step loop
+  // (timedisc_base.f90:649-750) as a state machine, one attempt per replayed slot
+  double t_loc;                  // the loop's time t
+  double d_att;                  // the attempt's dt (d)
+  double dtold_att;              // dt of the last attempt (dtold)
+  double maxerrold, last_err;    // AdjustTimestep's memory, the last error norm
+  long long n_adj;               // rejected attempts
+  long long steps_left;          // fosite steps still to run
+  int act;                       // this slot's actions (ACT_* bits)
+  int phase;                     // 0: next slot starts a fosite step, 1: inside IntegrationStep
+  int rhs_done;                  // AcceptSolution evaluated the RHS at t (rhs_done_at_t)
+  int checkflags;                // CheckData failures seen (FGPU_CHECK_* bits)
 };
+
+// actions of a device-clock attempt slot, decided by bt_decide_kernel
+enum { ACT_ATTEMPT = 1, ACT_REJECT = 2, ACT_SUB = 4, ACT_END = 8, ACT_COPY = 16 };
+// a kernel of a slot runs only if the slot's actions include one of its gate bits
+__device__ __forceinline__ bool gated_out(const Ctl* c, int gate) {
+  return gate && c && !(c->act & gate);
+}
 
 enum { BC_NOGRAD = 0x01, BC_PERIODIC = 0x02, BC_REFLECTING = 0x03, BC_ABSORBING = 0x0D };
 enum { LIM_MINMOD = 1, LIM_MC = 2, LIM_SWEBY = 3, LIM_SUPERBEE = 4, LIM_OSPRE = 5, LIM_VANLEER = 7, LIM_NOLIMIT = 8 };
@@ -245,7 +266,7 @@ __device__ __forceinline__ void state_at(const StateRef& S, long long n, long lo
 #pragma unroll 1
   for (int q = 0; q < S.nk; ++q) {
     const double* kq = S.K[q] + idx;
-    const double a = S.coef[q];
+    const double a = S.dt_dev ? S.coef[q] * *S.dt_dev : S.coef[q];
     double t[V];
 #pragma unroll
     for (int v = 0; v < V; ++v) t[v] = __ldg(kq + (long long)v * n);

@@ -17,6 +17,7 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <map>
 #include <mutex>
 #include <cstdlib>
 #include "../../include/fosite_gpu.h"
@@ -24,6 +25,8 @@
 #include "fgpu_stage2.cuh"
 #include "fgpu_fargo.cuh"
 #include "fgpu_visc.cuh"
+#include "fgpu_ddmath.h"
+#include "fgpu_bt.cuh"
 
 using namespace fgpu;
 
@@ -145,6 +148,9 @@ struct fgpu_handle {
                                 // (after FirstStep's CHECK_ALL, and after steps when checkdata has PMIN)
   // graph of G Shu-Osher steps
   cudaGraphExec_t graph = nullptr;
+  // device-clock embedded schemes: the captured attempt slot (fgpu_bt.cuh)
+  cudaGraphExec_t bt_graph = nullptr;
+  int kernels_per_slot = 0;
   int graph_steps = 0;
   // launch shape
   int tile_x = 32, tile_y = 8, kchunk = 16;
@@ -188,12 +194,16 @@ struct fgpu_handle {
 
 // The time of a right-hand side evaluation, for the viscosity update: a host value, or on the
 // device clock the control block's time + zeta*dt
+// device clock (time + zeta*dt), or on the attempt clock of the device-clock embedded
+// schemes (t + zeta*d of the IntegrationStep loop)
 struct RhsTime {
   bool dev = false;
+  bool attempt = false;
   double t = 0.0;
   double zeta = 0.0;
   static RhsTime host(double t) { RhsTime r; r.t = t; return r; }
   static RhsTime device(double zeta) { RhsTime r; r.dev = true; r.zeta = zeta; return r; }
+  static RhsTime att(double zeta) { RhsTime r; r.dev = true; r.attempt = true; r.zeta = zeta; return r; }
 };
 
 namespace {
@@ -447,9 +457,9 @@ int launch_stage_t(fgpu_handle* h, StageArgs& A) {
   A.kchunk = h->kchunk;
   const Grid& g = h->g;
   const int kz = ND == 3 ? (g.nz + h->kchunk - 1) / h->kchunk : 1;
-  // the warp-shuffle layout implements neither FARGO frame changes, the accretion rows nor
-  // the viscous source
-  const int variant = (h->variant == 1 && (h->fargo || h->accrete || h->vis)) ? 0 : h->variant;
+  // the warp-shuffle layout implements neither FARGO frame changes, the accretion rows, the
+  // viscous source nor the device-clock gates
+  const int variant = (h->variant == 1 && (h->fargo || h->accrete || h->vis || A.gate)) ? 0 : h->variant;
   switch (variant) {
     case 1: {
       // warp-shuffle layout: 32 x 8 points per block, 30 x 6 output cells
@@ -559,7 +569,7 @@ void launch_visc_update_t(fgpu_handle* h, const VisUpdArgs& U) {
   visc_update_kernel<ND, EU><<<blocks, 256, 0, h->stream>>>(U);
   visc_time_kernel<<<1, 1, 0, h->stream>>>(U, h->d_vistime);
 }
-int launch_visc_update(fgpu_handle* h, const StateRef& S, const RhsTime& when) {
+int launch_visc_update(fgpu_handle* h, const StateRef& S, const RhsTime& when, int gate = 0) {
   if (!h->vis || h->vis_model == FGPU_VIS_MOLECULAR) return FGPU_OK;
   VisUpdArgs U;
   std::memset(&U, 0, sizeof(U));
@@ -573,7 +583,13 @@ int launch_visc_update(fgpu_handle* h, const StateRef& S, const RhsTime& when) {
   U.dynvis = h->d_dynvis;
   U.vis_time = h->d_vistime;
   U.t = when.t;
-  if (when.dev) { U.t_dev = &h->d_ctl->time; U.dt_dev = &h->d_ctl->dt; U.zeta = when.zeta; U.ctl = h->d_ctl; }
+  if (when.dev) {
+    U.t_dev = when.attempt ? &h->d_ctl->t_loc : &h->d_ctl->time;
+    U.dt_dev = when.attempt ? &h->d_ctl->d_att : &h->d_ctl->dt;
+    U.zeta = when.zeta;
+    U.ctl = h->d_ctl;
+  }
+  U.gate = gate;
   U.npad = h->npad_vis;
   return timed_launch(h, 0, 0.0, [&] {
     if (h->nd == 2) h->euler ? launch_visc_update_t<2, true>(h, U) : launch_visc_update_t<2, false>(h, U);
@@ -584,9 +600,9 @@ int launch_visc_update(fgpu_handle* h, const StateRef& S, const RhsTime& when) {
 }
 // CalcTimestep's viscous limit for ALPHA/BETA/POWERLAW: UpdateViscosity at the state's time,
 // then the reduction over the padded cells into ctl->invdt[3]
-int launch_visc_cfl(fgpu_handle* h, const StateRef& S, bool roundtrip, const RhsTime& when) {
+int launch_visc_cfl(fgpu_handle* h, const StateRef& S, bool roundtrip, const RhsTime& when, int gate = 0) {
   if (!h->vis || h->vis_model == FGPU_VIS_MOLECULAR) return FGPU_OK;
-  if (int rc = launch_visc_update(h, S, when)) return rc;
+  if (int rc = launch_visc_update(h, S, when, gate)) return rc;
   VisCflArgs C;
   std::memset(&C, 0, sizeof(C));
   C.g = h->g; C.ph = h->ph; C.mt = h->mt;
@@ -595,6 +611,7 @@ int launch_visc_cfl(fgpu_handle* h, const StateRef& S, bool roundtrip, const Rhs
   C.dynvis = h->d_dynvis;
   C.npad = h->npad_vis;
   C.ctl = h->d_ctl;
+  C.gate = gate;
   const unsigned blocks = (unsigned)std::min<long long>((C.npad + 255) / 256, 148 * 8);
   return timed_launch(h, 0, 0.0, [&] {
     if (h->nd == 2) {
@@ -609,7 +626,7 @@ int launch_visc_cfl(fgpu_handle* h, const StateRef& S, bool roundtrip, const Rhs
   });
 }
 
-int launch_visc(fgpu_handle* h, const StateRef& S) {
+int launch_visc(fgpu_handle* h, const StateRef& S, int gate = 0) {
   ViscArgs V;
   std::memset(&V, 0, sizeof(V));
   V.g = h->g; V.ph = h->ph; V.mt = h->mt;
@@ -618,6 +635,8 @@ int launch_visc(fgpu_handle* h, const StateRef& S) {
   V.mub = h->vis_mub;
   V.dynvis = h->vis_model == FGPU_VIS_MOLECULAR ? nullptr : h->d_dynvis;
   V.out = h->d_visc;
+  V.ctl = h->d_ctl;
+  V.gate = gate;
   // algorithmic bytes: the state read once, the source written once
   const double bytes = (double)(h->V + h->nd + (h->euler ? 1 : 0)) * (double)h->g.n * 8.0;
   return timed_launch(h, 1, bytes, [&] {
@@ -633,8 +652,8 @@ int launch_visc(fgpu_handle* h, const StateRef& S) {
 int launch_stage(fgpu_handle* h, StageArgs& A, const RhsTime& when = RhsTime()) {
   if (h->vis) {
     const StateRef& S = A.rin.base ? A.rin : A.in;
-    if (int rc = launch_visc_update(h, S, when)) return rc;
-    if (int rc = launch_visc(h, S)) return rc;
+    if (int rc = launch_visc_update(h, S, when, A.gate)) return rc;
+    if (int rc = launch_visc(h, S, A.gate)) return rc;
     A.visc = h->d_visc;
   }
   return timed_launch(h, true, stage_bytes(h, A), [&] { return launch_stage_raw(h, A); });
@@ -644,14 +663,14 @@ int launch_misc(fgpu_handle* h, int which, BndArgs& B) {
 }
 
 template <int ND, bool EU>
-void launch_form_t(fgpu_handle* h, const StateRef& S, double* out, unsigned blocks) {
-  if (h->prim) form_kernel<ND, EU, true><<<blocks, 256, 0, h->stream>>>(S, h->g, h->ph, out);
-  else form_kernel<ND, EU, false><<<blocks, 256, 0, h->stream>>>(S, h->g, h->ph, out);
+void launch_form_t(fgpu_handle* h, const StateRef& S, double* out, unsigned blocks, int gate) {
+  if (h->prim) form_kernel<ND, EU, true><<<blocks, 256, 0, h->stream>>>(S, h->g, h->ph, out, h->d_ctl, gate);
+  else form_kernel<ND, EU, false><<<blocks, 256, 0, h->stream>>>(S, h->g, h->ph, out, h->d_ctl, gate);
 }
-int launch_form(fgpu_handle* h, const StateRef& S, double* out) {
+int launch_form(fgpu_handle* h, const StateRef& S, double* out, int gate = 0) {
   unsigned blocks = (unsigned)std::min<long long>((h->g.n + 255) / 256, 148 * 8);
-  if (h->nd == 2) h->euler ? launch_form_t<2, true>(h, S, out, blocks) : launch_form_t<2, false>(h, S, out, blocks);
-  else h->euler ? launch_form_t<3, true>(h, S, out, blocks) : launch_form_t<3, false>(h, S, out, blocks);
+  if (h->nd == 2) h->euler ? launch_form_t<2, true>(h, S, out, blocks, gate) : launch_form_t<2, false>(h, S, out, blocks, gate);
+  else h->euler ? launch_form_t<3, true>(h, S, out, blocks, gate) : launch_form_t<3, false>(h, S, out, blocks, gate);
   CUDA_TRY(h, cudaGetLastError());
   return FGPU_OK;
 }
@@ -991,9 +1010,10 @@ double adjust_timestep(fgpu_handle* h, double maxerr, double dtold_) {
   // timedisc_base.f90:759-814
   double dtnew, dttmp;
   if (h->tol_rel >= 1.0) return DBL_MAX;
-  if (maxerr > 0.) dttmp = 0.9 * dtold_ * std::exp(-std::log(maxerr) / h->T.order);
+  // correctly rounded exp/log (fgpu_ddmath.h): the device controller computes the same values
+  if (maxerr > 0.) dttmp = 0.9 * dtold_ * ddm::exp_cr(-ddm::log_cr(maxerr) / h->T.order);
   else dttmp = 4. * dtold_;
-  if (h->maxerrold > 0.) dtnew = dttmp * std::exp(-h->beta * std::log(h->maxerrold / maxerr));
+  if (h->maxerrold > 0.) dtnew = dttmp * ddm::exp_cr(-h->beta * ddm::log_cr(h->maxerrold / maxerr));
   else dtnew = dttmp;
   if (maxerr < 1.0) {
     dtnew = std::min(dtnew, 4. * dtold_);
@@ -1026,7 +1046,7 @@ int modeuler_attempt(fgpu_handle* h, double t, double dtv, double& err) {
     unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148 * 8);
     const double e1 = kEta[ord - 1][0];
     int rc = timed_launch(h, 0, 0.0, [&] {
-      shu_osher_update_kernel<<<blocks, 256, 0, h->stream>>>(base, base, K1, S1, n, e1, dtv);
+      shu_osher_update_kernel<<<blocks, 256, 0, h->stream>>>(base, base, K1, S1, n, e1, dtv, nullptr, nullptr, 0);
       CUDA_TRY(h, cudaGetLastError());
       return FGPU_OK;
     });
@@ -1420,6 +1440,7 @@ void fgpu_destroy(fgpu_handle* h) {
   if (!h) return;
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->graph) cudaGraphExecDestroy(h->graph);
+  if (h->bt_graph) cudaGraphExecDestroy(h->bt_graph);
   for (double* p : h->buf) cudaFree(p);
   if (h->d_pad) cudaFree(h->d_pad);
   if (h->d_metric) cudaFree(h->d_metric);
@@ -1643,6 +1664,221 @@ int fgpu_first_step(fgpu_handle* h) {
   return FGPU_OK;
 }
 
+// ---------------------------------------------------------------- embedded schemes (device clock)
+// One attempt slot (fgpu_bt.cuh): open a step if due, one attempt with dt read on the device,
+// the decision, then the RHS of the restored (reject) or advanced (accepted sub-step) state,
+// or the step's closing: cvar from AcceptSolution, the closing RHS with CheckData and the
+// CFL reduction, and CalcTimestep.  Every kernel after bt_begin runs only when its action
+// bit is set; the sequence is what butcher_integration_step and butcher_step enqueue.
+static int enqueue_bt_slot(fgpu_handle* h) {
+  const Tableau& T = h->T;
+  double* P = h->buf[0];
+  double* base = h->buf[1];
+  double* K1 = h->buf[2];
+  Ctl* c = h->d_ctl;
+  const double* d_att = &c->d_att;
+  auto one = [&](auto&& launch) {
+    return timed_launch(h, 0, 0.0, [&] {
+      launch();
+      CUDA_TRY(h, cudaGetLastError());
+      return FGPU_OK;
+    });
+  };
+  if (int rc = one([&] { bt_begin_kernel<<<1, 1, 0, h->stream>>>(c); })) return rc;
+  if (h->adaptive_me) {
+    double* S1 = h->buf[3];
+    double* S2 = h->buf[4];
+    double* LO = h->buf[5];
+    const int ord = h->order;
+    const long long n = (long long)h->V * h->g.n;
+    const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148 * 8);
+    const double e1 = kEta[ord - 1][0];
+    if (int rc = one([&] {
+          shu_osher_update_kernel<<<blocks, 256, 0, h->stream>>>(base, base, K1, S1, n, e1, 0.0, d_att, c, ACT_ATTEMPT);
+        }))
+      return rc;
+    for (int m = 2; m <= ord; ++m) {
+      StageArgs A = base_args(h);
+      A.in = plain_state(m == 2 ? S1 : S2, false);
+      A.out_mode = OUT_SSPRK;
+      A.eta = kEta[ord - 1][m - 1];
+      A.y0 = base;
+      A.dt_dev = d_att;
+      if (m == ord) {
+        A.out = P;
+        A.err_low = ord == 3 ? LO : S1;
+      } else {
+        A.out = S2;
+        A.out2 = LO;
+        A.eta2 = kEta[1][1];
+      }
+      A.gate = ACT_ATTEMPT;
+      if (int rc = launch_stage(h, A, RhsTime::att(kZeta[ord - 1][m - 2]))) return rc;
+    }
+  } else {
+    for (int m = 2; m <= T.m; ++m) {
+      StageArgs A = base_args(h);
+      A.in.base = base;
+      A.in.nk = m - 1;
+      A.in.roundtrip = 0;
+      for (int q = 0; q < m - 1; ++q) {
+        A.in.K[q] = h->buf[2 + q];
+        A.in.coef[q] = T.A[(m - 1) * T.m + q];
+      }
+      A.in.dt_dev = d_att;
+      double* R = h->buf[2 + T.m];
+      StateRef S = A.in;
+      if (int rc = timed_launch(h, 2, 0.0, [&] { return launch_form(h, S, R, ACT_ATTEMPT); })) return rc;
+      A.rin = plain_state(R, false);
+      A.rin.ready = h->prim ? 1 : 0;
+      A.out_mode = OUT_RHS;
+      A.out = h->buf[2 + m - 1];
+      A.gate = ACT_ATTEMPT;
+      if (int rc = launch_stage(h, A, RhsTime::att(T.c[m - 1]))) return rc;
+    }
+    CombineArgs Cb;
+    std::memset(&Cb, 0, sizeof(Cb));
+    Cb.base = base;
+    for (int q = 0; q < T.m; ++q) {
+      Cb.K[q] = h->buf[2 + q];
+      Cb.bh_dt[q] = T.bh[q];
+      Cb.bl_dt[q] = T.bl[q];
+    }
+    Cb.nstage = T.m;
+    Cb.out_high = P;
+    Cb.tol_rel = h->tol_rel;
+    for (int v = 0; v < FGPU_MAXV; ++v) Cb.tol_abs[v] = h->tol_abs[v];
+    Cb.n = h->g.n;
+    Cb.ctl = c;
+    Cb.dt_dev = d_att;
+    Cb.gate = ACT_ATTEMPT;
+    const unsigned blocks = (unsigned)std::min<long long>((h->g.n + 255) / 256, 148 * 8);
+    if (int rc = timed_launch(h, 2, (double)h->V * h->g.n * 8.0, [&] {
+          switch (h->V) {
+            case 3: combine_kernel<3><<<blocks, 256, 0, h->stream>>>(Cb); break;
+            case 4: combine_kernel<4><<<blocks, 256, 0, h->stream>>>(Cb); break;
+            default: combine_kernel<5><<<blocks, 256, 0, h->stream>>>(Cb); break;
+          }
+          CUDA_TRY(h, cudaGetLastError());
+          return FGPU_OK;
+        }))
+      return rc;
+  }
+  BtParams bp;
+  bp.order = T.order;
+  bp.beta = h->beta;
+  bp.tol_rel = h->tol_rel;
+  if (int rc = one([&] { bt_decide_kernel<<<1, 1, 0, h->stream>>>(c, bp); })) return rc;
+  {   // RejectSolution: the RHS of cold (CHECK_NOTHING)
+    StageArgs A = base_args(h);
+    A.out_mode = OUT_RHS;
+    A.out = K1;
+    A.in = plain_state(base, false);
+    A.gate = ACT_REJECT;
+    if (int rc = launch_stage(h, A, RhsTime::att(0.0))) return rc;
+  }
+  {   // AcceptSolution inside the step: the RHS at t with the checkdata mask, cold = cvar
+    StageArgs A = base_args(h);
+    A.out_mode = OUT_RHS;
+    A.out = K1;
+    A.in = plain_state(P, h->roundtrip_cfg);
+    A.out_base = base;
+    A.checkdata = h->cfg.checkdata;
+    A.gate = ACT_SUB;
+    if (int rc = launch_stage(h, A, RhsTime::att(0.0))) return rc;
+  }
+  {   // the closing: cvar as AcceptSolution's ComputeRHS left it, then IntegrationStep's RHS
+    const long long n = (long long)h->V * h->g.n;
+    const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148 * 8);
+    if (int rc = one([&] { gated_copy_kernel<<<blocks, 256, 0, h->stream>>>(base, P, n, c, ACT_COPY); })) return rc;
+    StageArgs A = base_args(h);
+    A.out_mode = OUT_RHS;
+    A.out = K1;
+    A.in = plain_state(P, h->roundtrip_cfg);
+    A.out_base = base;
+    A.checkdata = h->cfg.checkdata;
+    A.cfl_mode = 2;
+    A.gate = ACT_END;
+    if (int rc = launch_stage(h, A, RhsTime::att(0.0))) return rc;
+  }
+  BndArgs B = bnd_args(h, P, h->roundtrip_cfg, FIN_NONE);
+  B.checkdata = h->cfg.checkdata;
+  B.gate = ACT_END;
+  if (int rc = launch_misc(h, 0, B)) return rc;
+  if (int rc = launch_visc_cfl(h, plain_state(P, h->roundtrip_cfg), h->roundtrip_cfg, RhsTime::att(0.0), ACT_END))
+    return rc;
+  const int nd = h->nd;
+  return one([&] { bt_finish_kernel<<<1, 1, 0, h->stream>>>(c, nd); });
+}
+
+// n fosite steps of an embedded scheme on the device clock: the host state goes into the
+// control block, attempt slots are replayed (a captured graph) in chunks with one control-
+// block read per chunk, and the state comes back.  Results equal n calls of butcher_step.
+static int bt_run(fgpu_handle* h, int64_t n, int64_t* done) {
+  Ctl* c = h->h_ctl;
+  std::memset(c, 0, sizeof(Ctl));
+  c->time = h->time; c->dt = h->dt; c->dtold = h->dtold; c->dtmin = h->dtmin;
+  c->stoptime = h->stoptime; c->tout = h->tout; c->cfl = h->cfl; c->dtlimit = h->dtlimit;
+  c->iter = h->iter; c->brk = h->brk ? 1 : 0; c->dtcause = h->dtcause;
+  c->cvis = h->cvis; c->vis = h->vis ? 1 : 0;
+  c->maxerrold = h->maxerrold; c->last_err = h->last_err; c->n_adj = h->n_adj;
+  c->checkflags = h->checkflags;
+  c->steps_left = n;
+  if (int rc = write_ctl(h)) return rc;
+  if (!h->bt_graph && !h->profiling) {
+    cudaGraph_t gr;
+    fgpu_stats saved = h->stats;
+    CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_bt_slot(h);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &gr);
+    h->kernels_per_slot = (int)(h->stats.launches - saved.launches);
+    h->stats = saved;
+    if (rc) return rc;
+    if (e != cudaSuccess) return set_err(h, FGPU_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&h->bt_graph, gr, 0);
+    cudaGraphDestroy(gr);
+    if (e != cudaSuccess) return set_err(h, FGPU_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  }
+  const long long it0 = h->iter, adj0 = h->n_adj;
+  const int CH = 8;
+  long long slots = 0;
+  const long long cap = 64 * (long long)n + 64;   // every attempt either advances t or shrinks dt 4x
+  while (true) {
+    for (int k = 0; k < CH; ++k) {
+      if (h->profiling) {
+        if (int rc = enqueue_bt_slot(h)) return rc;
+      } else {
+        CUDA_TRY(h, cudaGraphLaunch(h->bt_graph, h->stream));
+        h->stats.launches += h->kernels_per_slot;
+      }
+    }
+    slots += CH;
+    if (int rc = read_ctl(h)) return rc;
+    if (c->steps_left <= 0 || c->stop || c->brk) break;
+    if (slots > cap) return set_err(h, FGPU_ETIMEOUT, "device-clock step loop: no progress");
+  }
+  h->time = c->time; h->dt = c->dt; h->dtold = c->dtold; h->dtmin = c->dtmin;
+  h->iter = c->iter; h->brk = c->brk != 0; h->dtcause = c->dtcause;
+  h->maxerrold = c->maxerrold; h->last_err = c->last_err; h->n_adj = c->n_adj;
+  h->checkflags = c->checkflags;
+  const int64_t steps = n - c->steps_left;
+  if (steps > 0) h->pre_rt = h->roundtrip_cfg;
+  h->stats.attempts += (h->iter - it0) + (h->n_adj - adj0);
+  h->stats.cell_updates += (h->iter - it0) * h->g.n;
+  if (done) *done = steps;
+  if (h->brk) return FGPU_BREAK;
+  if (c->stop) return FGPU_STOPTIME;
+  return FGPU_OK;
+}
+
+// the device clock serves embedded schemes whose stage states are formed by form_kernel;
+// FGPU_BUTCHER_HOST=1 keeps the host-controlled loop
+static bool bt_device(const fgpu_handle* h) {
+  if (!h->materialize) return false;
+  const char* e = std::getenv("FGPU_BUTCHER_HOST");
+  return !(e && std::atoi(e) != 0);
+}
+
 static int butcher_step(fgpu_handle* h) {
   // fosite%Step (fosite.f90:367-464) around the Butcher IntegrationStep
   if (std::fabs(h->stoptime - h->time) <= 1.0E-05 * h->stoptime) return FGPU_STOPTIME;
@@ -1664,6 +1900,7 @@ int fgpu_run(fgpu_handle* h, int64_t n, int64_t* done) {
   if (!h->first_done) { int rc = fgpu_first_step(h); if (rc) return rc; }
   int64_t k = 0;
   if (h->butcher) {
+    if (n > 0 && bt_device(h)) return bt_run(h, n, done);
     int rc = FGPU_OK;
     for (; k < n; ++k) {
       rc = butcher_step(h);

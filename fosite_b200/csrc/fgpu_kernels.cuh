@@ -76,6 +76,8 @@ struct StageArgs {
   StateRef rin;
   // optional: viscous source of the stage state, [ND momentum (+ energy)][n] (visc_kernel)
   const double* visc;
+  // device-clock attempt slots: run only if the slot's actions include a gate bit
+  int gate;
 };
 
 // block-wide max of up to 4 non-negative doubles + OR of flags, then one atomic per block;
@@ -141,6 +143,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
   __shared__ double sred[RED_STRIDE * ((NT + 31) / 32)];
 
   if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
+  if (gated_out(A.ctl, A.gate)) return;
   const Grid& g = A.g;
   const PhysP& P = A.ph;
   const MetricP& M = A.mt;

@@ -23,6 +23,7 @@ struct BndArgs {
   // FARGO: background velocity subtracted after the boundary fill (the co-moving
   // frame that CalcTimestep and the caller's cvar/pvar see); null = off
   const double* w_sub;
+  int gate;        // device-clock attempt slots (ACT_* bits)
 };
 
 // FARGO frame of a checked cell: the real-frame p/c computed from the state go
@@ -111,6 +112,7 @@ __device__ __forceinline__ void boundary_block(const BndArgs& A, const int blk, 
   __shared__ double sred[RED_STRIDE * 8];
   __shared__ bool is_last;
   if (A.ctl && A.finalize != FIN_FIRST && (A.ctl->stop | A.ctl->brk)) return;
+  if (gated_out(A.ctl, A.gate)) return;
   const MetricP& M = A.mt;
   double cflv[4] = {0.0, 0.0, 0.0, 0.0};
   int flags = 0;
@@ -310,10 +312,19 @@ struct CombineArgs {
   double tol_abs[FGPU_MAXV];
   long long n;
   Ctl* ctl;
+  const double* dt_dev;   // device clock: bh_dt/bl_dt hold the weights, times *dt_dev
+  int gate;
 };
 template <int V>
 __global__ void __launch_bounds__(256) combine_kernel(const __grid_constant__ CombineArgs A) {
   __shared__ double sred[RED_STRIDE * 8];
+  if (A.gate && (A.ctl->stop | A.ctl->brk)) return;
+  if (gated_out(A.ctl, A.gate)) return;
+  double bh[FGPU_MAXK], bl[FGPU_MAXK];
+  for (int q = 0; q < A.nstage; ++q) {
+    bh[q] = A.dt_dev ? A.bh_dt[q] * *A.dt_dev : A.bh_dt[q];
+    bl[q] = A.dt_dev ? A.bl_dt[q] * *A.dt_dev : A.bl_dt[q];
+  }
   double errv = 0.0;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < A.n; t += (long long)gridDim.x * blockDim.x) {
 #pragma unroll
@@ -322,8 +333,8 @@ __global__ void __launch_bounds__(256) combine_kernel(const __grid_constant__ Co
       double h = b, l = b;
       for (int q = 0; q < A.nstage; ++q) {
         const double kq = __ldg(A.K[q] + (long long)v * A.n + t);
-        l = l - A.bl_dt[q] * kq;
-        h = h - A.bh_dt[q] * kq;
+        l = l - bl[q] * kq;
+        h = h - bh[q] * kq;
       }
       A.out_high[(long long)v * A.n + t] = h;
       const double e = fabs(h - l) / (A.tol_rel * fabs(h) + A.tol_abs[v]);
@@ -339,9 +350,22 @@ __global__ void __launch_bounds__(256) combine_kernel(const __grid_constant__ Co
 // (timedisc_modeuler.f90:279-291), over n values.
 __global__ void __launch_bounds__(256) shu_osher_update_kernel(const double* __restrict__ y0, const double* __restrict__ yn,
                                                                const double* __restrict__ r, double* __restrict__ out,
-                                                               long long n, double eta, double dt) {
+                                                               long long n, double eta, double dt_host,
+                                                               const double* dt_dev, const Ctl* ctl, int gate) {
+  if (gate && (ctl->stop | ctl->brk)) return;
+  if (gated_out(ctl, gate)) return;
+  const double dt = dt_dev ? *dt_dev : dt_host;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
     out[t] = yn[t] - dt * r[t] + eta * (y0[t] - yn[t] + dt * r[t]);
+}
+
+// A gated copy of n doubles (AcceptSolution's state into cvar at the end of a device-clock step).
+__global__ void __launch_bounds__(256) gated_copy_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                                                         long long n, const Ctl* ctl, int gate) {
+  if (ctl->stop | ctl->brk) return;
+  if (gated_out(ctl, gate)) return;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    dst[t] = src[t];
 }
 
 // The reconstruction variables of a Butcher stage state, formed once per cell:
@@ -350,9 +374,11 @@ __global__ void __launch_bounds__(256) shu_osher_update_kernel(const double* __r
 // stage kernel forms at every stencil point.
 template <int ND, bool EU, bool PRIM>
 __global__ void __launch_bounds__(256) form_kernel(const __grid_constant__ StateRef in, Grid g, PhysP P,
-                                                   double* __restrict__ out) {
+                                                   double* __restrict__ out, const Ctl* ctl, int gate) {
   using PH = Phys<ND, EU>;
   constexpr int V = PH::V;
+  if (gate && (ctl->stop | ctl->brk)) return;
+  if (gated_out(ctl, gate)) return;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < g.n; t += (long long)gridDim.x * blockDim.x) {
     double u[V], p[V];
     state_at<V>(in, g.n, t, u);

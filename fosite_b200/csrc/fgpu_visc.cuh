@@ -33,6 +33,8 @@ struct ViscArgs {
   double mub;              // MOLECULAR: bulk viscosity (bulkconst)
   const double* dynvis;    // other models: dynamic viscosity by padded cell (bulk = -2/3 of it)
   double* out;
+  const Ctl* ctl;          // device-clock attempt slots: gate bits (0 = always run)
+  int gate;
 };
 
 // index of a cell of the ghost-padded grid (coordinates -2 .. n+1; 2D meshes have no z ghosts)
@@ -52,7 +54,7 @@ __device__ __forceinline__ void interior_rv(const StateRef& S, long long n, long
 #pragma unroll 1
   for (int q = 0; q < S.nk; ++q) {
     const double* kq = S.K[q] + idx;
-    const double a = S.coef[q];
+    const double a = S.dt_dev ? S.coef[q] * *S.dt_dev : S.coef[q];
 #pragma unroll
     for (int v = 0; v <= ND; ++v) rv[v] = rv[v] - a * __ldg(kq + (long long)v * n);
   }
@@ -95,6 +97,8 @@ __global__ void __launch_bounds__(TX* TY* TZ) visc_kernel(const __grid_constant_
   constexpr int NT = TX * TY * TZ;
   constexpr int VX = L::VX, VY = L::VY, VZ = L::VZ, BX = L::BX, BY = L::BY, BZ = L::BZ;
   extern __shared__ __align__(16) double visc_smem[];
+  if (A.gate && (A.ctl->stop | A.ctl->brk)) return;
+  if (gated_out(A.ctl, A.gate)) return;
   double* const Vs = visc_smem;                     // [ND][VZ][VY][VX]
   double* const Ts = Vs + ND * VX * VY * VZ;        // [NB][BZ][BY][BX]
   const Grid& g = A.g;
@@ -259,6 +263,7 @@ struct VisUpdArgs {
   double zeta;
   long long npad;
   const Ctl* ctl;            // device clock: nothing to do once the run has stopped or broken
+  int gate;                  // device-clock attempt slots (ACT_* bits)
 };
 
 __device__ __forceinline__ double vis_rhs_time(const VisUpdArgs& A) {
@@ -270,6 +275,7 @@ __global__ void __launch_bounds__(256) visc_update_kernel(const __grid_constant_
   using CE = Cells<ND, EU>;
   constexpr int V = Phys<ND, EU>::V;
   if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
+  if (gated_out(A.ctl, A.gate)) return;
   const double t = vis_rhs_time(A);
   if (!(t != *A.vis_time || t == 0.0)) return;
   const int NXp = A.g.nx + 4, NYp = A.g.ny + 4;
@@ -302,6 +308,7 @@ __global__ void __launch_bounds__(256) visc_update_kernel(const __grid_constant_
 // records the update's time (after visc_update_kernel, whose blocks all read the old value)
 __global__ void visc_time_kernel(VisUpdArgs A, double* vis_time) {
   if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
+  if (gated_out(A.ctl, A.gate)) return;
   *vis_time = vis_rhs_time(A);
 }
 
@@ -317,6 +324,7 @@ struct VisCflArgs {
   const double* dynvis;
   long long npad;
   Ctl* ctl;
+  int gate;
 };
 
 template <int ND, bool EU>
@@ -326,6 +334,7 @@ __global__ void __launch_bounds__(256) visc_cfl_kernel(const __grid_constant__ V
   constexpr int V = PH::V;
   __shared__ double sred[RED_STRIDE * 8];
   if (A.ctl->stop | A.ctl->brk) return;
+  if (gated_out(A.ctl, A.gate)) return;
   const MetricP& M = A.mt;
   const int NXp = A.g.nx + 4, NYp = A.g.ny + 4;
   double mx = 0.0;

@@ -261,7 +261,11 @@ int fgpu_compute_rhs(fgpu_handle* h);
 int fgpu_calc_timestep(fgpu_handle* h, double* dt);
 /* Measure every stage-kernel layout on this grid (reps RHS evaluations each into
  * a scratch array; the state is untouched) and keep the fastest for later
- * steps.  *variant receives the choice.  No counterpart in the reference. */
+ * steps.  *variant receives the choice.  Decisions are cached per process by
+ * (device, dimensionality, physics, reconstruction variables, limiter, geometry,
+ * mesh size, features): a grid with a known key takes the cached layout without
+ * probing; reps < 0 measures |reps| times anyway and refreshes the entry.  No
+ * counterpart in the reference. */
 int fgpu_autotune(fgpu_handle* h, int reps, int* variant);
 
 /* ---- batched ensembles (no counterpart in the reference, which integrates one
