@@ -334,8 +334,9 @@ struct TuneKey {
     return std::memcmp(this, &o, sizeof(TuneKey)) < 0;
   }
 };
+struct TuneChoice { int variant, kchunk; };
 std::mutex g_tune_mutex;
-std::map<TuneKey, int> g_tune_cache;
+std::map<TuneKey, TuneChoice> g_tune_cache;
 TuneKey tune_key(const fgpu_handle* h) {
   TuneKey k;
   std::memset(&k, 0, sizeof(k));
@@ -361,10 +362,13 @@ int fgpu_autotune(fgpu_handle* h, int reps, int* variant) {
     std::lock_guard<std::mutex> lock(g_tune_mutex);
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) {
-      if (h->variant != it->second && h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; h->graph_steps = 0; }
-      if (h->variant != it->second && h->bt_graph) { cudaGraphExecDestroy(h->bt_graph); h->bt_graph = nullptr; }
-      h->variant = it->second;
-      if (variant) *variant = it->second;
+      if (h->variant != it->second.variant || h->kchunk != it->second.kchunk) {
+        if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; h->graph_steps = 0; }
+        if (h->bt_graph) { cudaGraphExecDestroy(h->bt_graph); h->bt_graph = nullptr; }
+      }
+      h->variant = it->second.variant;
+      h->kchunk = it->second.kchunk;
+      if (variant) *variant = it->second.variant;
       return FGPU_OK;
     }
   }
@@ -378,23 +382,37 @@ int fgpu_autotune(fgpu_handle* h, int reps, int* variant) {
   A.ctl = nullptr;
   A.visc = h->vis ? h->d_visc : nullptr;   // the stencil's read of the viscous source
   const int cand[5] = {0, 2, 3, 4, 1};
+  // 3D: the z extent a block marches through (smaller chunks give small grids more blocks);
+  // FGPU_KCHUNK fixes it
+  std::vector<int> chunks;
+  if (h->nd == 3 && !std::getenv("FGPU_KCHUNK")) {
+    for (int kc : {4, 8, 16, 32})
+      if (kc <= std::max(4, h->g.nz)) chunks.push_back(kc);
+  } else {
+    chunks.push_back(h->kchunk);
+  }
   double best = 1e300;
-  int bv = h->variant, keep = h->variant;
+  int bv = h->variant, bk = h->kchunk;
+  const int keep = h->variant, keepk = h->kchunk;
   for (int v : cand) {
     if (v == 1 && (h->fargo || h->accrete || h->vis)) continue;   // layout 1 lacks these features
-    h->variant = v;
-    int rc = FGPU_OK;
-    double ms = time_launches(h->stream, reps, [&] { if (!rc) rc = launch_stage_raw(h, A); });
-    if (rc) { h->variant = keep; return rc; }
-    if (ms < best) { best = ms; bv = v; }
+    for (int kc : chunks) {
+      h->variant = v;
+      h->kchunk = kc;
+      int rc = FGPU_OK;
+      double ms = time_launches(h->stream, reps, [&] { if (!rc) rc = launch_stage_raw(h, A); });
+      if (rc) { h->variant = keep; h->kchunk = keepk; return rc; }
+      if (ms < best) { best = ms; bv = v; bk = kc; }
+    }
   }
   h->variant = bv;
+  h->kchunk = bk;
   if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; h->graph_steps = 0; }
   if (h->bt_graph) { cudaGraphExecDestroy(h->bt_graph); h->bt_graph = nullptr; }
   if (variant) *variant = bv;
   {
     std::lock_guard<std::mutex> lock(g_tune_mutex);
-    g_tune_cache[key] = bv;
+    g_tune_cache[key] = TuneChoice{bv, bk};
   }
   return FGPU_OK;
 }

@@ -1840,10 +1840,11 @@ static int bt_run(fgpu_handle* h, int64_t n, int64_t* done) {
     if (e != cudaSuccess) return set_err(h, FGPU_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
   }
   const long long it0 = h->iter, adj0 = h->n_adj;
-  const int CH = 8;
   long long slots = 0;
   const long long cap = 64 * (long long)n + 64;   // every attempt either advances t or shrinks dt 4x
   while (true) {
+    // as many slots as steps are left (most steps take one attempt), at most 8 per read
+    const int CH = (int)std::max<long long>(1, std::min<long long>(8, c->steps_left));
     for (int k = 0; k < CH; ++k) {
       if (h->profiling) {
         if (int rc = enqueue_bt_slot(h)) return rc;

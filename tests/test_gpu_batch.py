@@ -144,3 +144,26 @@ def test_single_grid_autotune_keeps_results():
     a.run(20)
     b.run(20)
     assert np.array_equal(a.get(abi.CVAR), b.get(abi.CVAR))
+
+
+@pytest.mark.gpu
+def test_autotune_3d_chunks_and_cache_keep_results():
+    """The tuner also picks the z chunk of 3D grids; a second grid with the same tuning key
+    takes the cached choice; neither changes any result."""
+    import time
+    from fosite_b200.sim import Simulation
+    from cases import _gauss3d
+    cfg, p, _ = _gauss3d(n=(24, 20, 18))
+    a, b, c = (Simulation(cfg, exact=True) for _ in range(3))
+    for s in (a, b, c):
+        s.set_state(abi.PVAR, p)
+        s.first_step()
+    va = a.autotune(2)
+    t0 = time.perf_counter()
+    vb = b.autotune(2)
+    assert vb == va
+    assert time.perf_counter() - t0 < 0.05          # cached: no probes
+    for s in (a, b, c):
+        assert s.run(6)[0] == 0
+    assert np.array_equal(a.get(abi.CVAR), c.get(abi.CVAR))
+    assert np.array_equal(b.get(abi.CVAR), c.get(abi.CVAR))
