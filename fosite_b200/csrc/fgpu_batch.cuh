@@ -31,6 +31,21 @@ struct fgpu_batch {
   int64_t pending_steps = 0;     // enqueued since the last collect
   std::vector<long long> it0;    // member iteration counts at the first enqueue
   std::string err;
+  // embedded Runge-Kutta members (fgpu_bt.cuh): one replayed attempt slot advances every
+  // member by one attempt; every member keeps its own controller, dt and error norm
+  bool embedded = false;
+  int stages = 0;                // tableau stages m
+  Ctl** d_ctlp = nullptr;        // [n] members' control blocks
+  BtParams* d_btp = nullptr;     // [n]
+  StageArgs* d_eargs = nullptr;  // [m-1] attempt stages, then reject, sub-step and closing RHS: [(m+2)][n]
+  FormArgs* d_fargs = nullptr;   // [m-1][n]
+  CombineArgs* d_cargs = nullptr;// [n]
+  CopyArgs* d_copy = nullptr;    // [n]
+  BndArgs* d_ebnd = nullptr;     // [n] closing ghost/CFL pass
+  int4* d_cblocks = nullptr;     // per-member cell blocks (member, block, blocks)
+  int ncblocks = 0;
+  cudaGraphExec_t slot_graph = nullptr;
+  std::vector<long long> adj0;
 };
 
 namespace {
@@ -142,6 +157,255 @@ double time_launches(cudaStream_t s, int reps, F&& fn) {
   return (double)ms / reps;
 }
 
+// ---- embedded-scheme batches
+template <class T>
+int upload_table(fgpu_batch* b, T** dst, const std::vector<T>& v) {
+  BCUDA_TRY(b, cudaMalloc(dst, sizeof(T) * std::max<size_t>(1, v.size())));
+  BCUDA_TRY(b, cudaMemcpyAsync(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, b->stream));
+  return FGPU_OK;
+}
+
+// The argument tables of the attempt slot: what enqueue_bt_slot launches for one grid,
+// for every member (the same arguments, member by member)
+int build_embedded_tables(fgpu_batch* b) {
+  const int n = (int)b->m.size();
+  const Tableau& T0 = b->m[0]->T;
+  const int M = T0.m;
+  b->stages = M;
+  std::vector<Ctl*> ctlp(n);
+  std::vector<BtParams> btp(n);
+  std::vector<StageArgs> eargs((size_t)(M + 2) * n);
+  std::vector<FormArgs> fargs((size_t)(M - 1) * n);
+  std::vector<CombineArgs> cargs(n);
+  std::vector<CopyArgs> copy(n);
+  std::vector<BndArgs> ebnd(n);
+  std::vector<int4> cblocks;
+  for (int i = 0; i < n; ++i) {
+    fgpu_handle* h = b->m[i];
+    const Tableau& T = h->T;
+    double* P = h->buf[0];
+    double* base = h->buf[1];
+    double* K1 = h->buf[2];
+    Ctl* c = h->d_ctl;
+    ctlp[i] = c;
+    btp[i].order = T.order; btp[i].beta = h->beta; btp[i].tol_rel = h->tol_rel;
+    for (int m = 2; m <= M; ++m) {
+      StageArgs A = base_args(h);
+      A.in.base = base;
+      A.in.nk = m - 1;
+      for (int q = 0; q < m - 1; ++q) { A.in.K[q] = h->buf[2 + q]; A.in.coef[q] = T.A[(m - 1) * T.m + q]; }
+      A.in.dt_dev = &c->d_att;
+      FormArgs F;
+      std::memset(&F, 0, sizeof(F));
+      F.in = A.in; F.g = h->g; F.ph = h->ph; F.out = h->buf[2 + T.m]; F.ctl = c; F.gate = ACT_ATTEMPT;
+      fargs[(size_t)(m - 2) * n + i] = F;
+      A.rin = plain_state(h->buf[2 + T.m], false);
+      A.rin.ready = h->prim ? 1 : 0;
+      A.out_mode = OUT_RHS;
+      A.out = h->buf[2 + m - 1];
+      A.gate = ACT_ATTEMPT;
+      A.kchunk = h->kchunk;
+      eargs[(size_t)(m - 2) * n + i] = A;
+    }
+    CombineArgs& Cb = cargs[i];
+    std::memset(&Cb, 0, sizeof(Cb));
+    Cb.base = base;
+    for (int q = 0; q < T.m; ++q) { Cb.K[q] = h->buf[2 + q]; Cb.bh_dt[q] = T.bh[q]; Cb.bl_dt[q] = T.bl[q]; }
+    Cb.nstage = T.m; Cb.out_high = P; Cb.tol_rel = h->tol_rel;
+    for (int v = 0; v < FGPU_MAXV; ++v) Cb.tol_abs[v] = h->tol_abs[v];
+    Cb.n = h->g.n; Cb.ctl = c; Cb.dt_dev = &c->d_att; Cb.gate = ACT_ATTEMPT;
+    {   // RejectSolution's RHS of cold
+      StageArgs A = base_args(h);
+      A.out_mode = OUT_RHS; A.out = K1; A.in = plain_state(base, false); A.gate = ACT_REJECT; A.kchunk = h->kchunk;
+      eargs[(size_t)(M - 1) * n + i] = A;
+    }
+    {   // AcceptSolution's RHS inside the step
+      StageArgs A = base_args(h);
+      A.out_mode = OUT_RHS; A.out = K1; A.in = plain_state(P, h->roundtrip_cfg); A.out_base = base;
+      A.checkdata = h->cfg.checkdata; A.gate = ACT_SUB; A.kchunk = h->kchunk;
+      eargs[(size_t)M * n + i] = A;
+    }
+    {   // the closing RHS with the CFL reduction
+      StageArgs A = base_args(h);
+      A.out_mode = OUT_RHS; A.out = K1; A.in = plain_state(P, h->roundtrip_cfg); A.out_base = base;
+      A.checkdata = h->cfg.checkdata; A.cfl_mode = 2; A.gate = ACT_END; A.kchunk = h->kchunk;
+      eargs[(size_t)(M + 1) * n + i] = A;
+    }
+    copy[i].src = base; copy[i].dst = P; copy[i].n = (long long)h->V * h->g.n; copy[i].ctl = c; copy[i].gate = ACT_COPY;
+    ebnd[i] = bnd_args(h, P, h->roundtrip_cfg, FIN_NONE);
+    ebnd[i].checkdata = h->cfg.checkdata;
+    ebnd[i].gate = ACT_END;
+    const long long nb = std::max<long long>(1, std::min<long long>((h->g.n + 255) / 256, 1024));
+    for (int q = 0; q < (int)nb; ++q) cblocks.push_back(make_int4(i, q, (int)nb, 0));
+  }
+  b->ncblocks = (int)cblocks.size();
+  if (int rc = upload_table(b, &b->d_ctlp, ctlp)) return rc;
+  if (int rc = upload_table(b, &b->d_btp, btp)) return rc;
+  if (int rc = upload_table(b, &b->d_eargs, eargs)) return rc;
+  if (int rc = upload_table(b, &b->d_fargs, fargs)) return rc;
+  if (int rc = upload_table(b, &b->d_cargs, cargs)) return rc;
+  if (int rc = upload_table(b, &b->d_copy, copy)) return rc;
+  if (int rc = upload_table(b, &b->d_ebnd, ebnd)) return rc;
+  if (int rc = upload_table(b, &b->d_cblocks, cblocks)) return rc;
+  BCUDA_TRY(b, cudaStreamSynchronize(b->stream));
+  return FGPU_OK;
+}
+
+template <int ND, bool EU, bool PRIM>
+void launch_batched_form_t(fgpu_batch* b, const FormArgs* a) {
+  batched_form_kernel<ND, EU, PRIM><<<b->ncblocks, 256, 0, b->stream>>>(a, b->d_cblocks);
+}
+int launch_batched_form(fgpu_batch* b, const FormArgs* a) {
+  if (b->nd == 2) {
+    if (b->euler) b->prim ? launch_batched_form_t<2, true, true>(b, a) : launch_batched_form_t<2, true, false>(b, a);
+    else b->prim ? launch_batched_form_t<2, false, true>(b, a) : launch_batched_form_t<2, false, false>(b, a);
+  } else {
+    if (b->euler) b->prim ? launch_batched_form_t<3, true, true>(b, a) : launch_batched_form_t<3, true, false>(b, a);
+    else b->prim ? launch_batched_form_t<3, false, true>(b, a) : launch_batched_form_t<3, false, false>(b, a);
+  }
+  BCUDA_TRY(b, cudaGetLastError());
+  return FGPU_OK;
+}
+
+// one attempt of every member (enqueue_bt_slot, batched)
+int enqueue_batch_slot(fgpu_batch* b) {
+  const int n = (int)b->m.size();
+  const int M = b->stages;
+  const unsigned mb = (unsigned)((n + 127) / 128);
+  bt_begin_batch_kernel<<<mb, 128, 0, b->stream>>>(b->d_ctlp, n);
+  BCUDA_TRY(b, cudaGetLastError());
+  for (int m = 2; m <= M; ++m) {
+    if (int rc = launch_batched_form(b, b->d_fargs + (size_t)(m - 2) * n)) return rc;
+    if (int rc = launch_batched_stage(b, b->d_eargs + (size_t)(m - 2) * n, b->variant)) return rc;
+  }
+  switch (b->m[0]->V) {
+    case 3: batched_combine_kernel<3><<<b->ncblocks, 256, 0, b->stream>>>(b->d_cargs, b->d_cblocks); break;
+    case 4: batched_combine_kernel<4><<<b->ncblocks, 256, 0, b->stream>>>(b->d_cargs, b->d_cblocks); break;
+    default: batched_combine_kernel<5><<<b->ncblocks, 256, 0, b->stream>>>(b->d_cargs, b->d_cblocks); break;
+  }
+  BCUDA_TRY(b, cudaGetLastError());
+  bt_decide_batch_kernel<<<mb, 128, 0, b->stream>>>(b->d_ctlp, b->d_btp, n);
+  BCUDA_TRY(b, cudaGetLastError());
+  if (int rc = launch_batched_stage(b, b->d_eargs + (size_t)(M - 1) * n, b->variant)) return rc;
+  if (int rc = launch_batched_stage(b, b->d_eargs + (size_t)M * n, b->variant)) return rc;
+  batched_copy_kernel<<<b->ncblocks, 256, 0, b->stream>>>(b->d_copy, b->d_cblocks);
+  BCUDA_TRY(b, cudaGetLastError());
+  if (int rc = launch_batched_stage(b, b->d_eargs + (size_t)(M + 1) * n, b->variant)) return rc;
+  if (b->nd == 2) {
+    if (b->euler) batched_boundary_kernel<2, true><<<b->nbblocks, 256, 0, b->stream>>>(b->d_ebnd, b->d_bblocks);
+    else batched_boundary_kernel<2, false><<<b->nbblocks, 256, 0, b->stream>>>(b->d_ebnd, b->d_bblocks);
+  } else {
+    if (b->euler) batched_boundary_kernel<3, true><<<b->nbblocks, 256, 0, b->stream>>>(b->d_ebnd, b->d_bblocks);
+    else batched_boundary_kernel<3, false><<<b->nbblocks, 256, 0, b->stream>>>(b->d_ebnd, b->d_bblocks);
+  }
+  BCUDA_TRY(b, cudaGetLastError());
+  bt_finish_batch_kernel<<<mb, 128, 0, b->stream>>>(b->d_ctlp, n, b->nd);
+  BCUDA_TRY(b, cudaGetLastError());
+  return FGPU_OK;
+}
+
+__global__ void add_steps_kernel(Ctl* const* ctls, int n, long long k) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) ctls[i]->steps_left += k;
+}
+
+int build_slot_graph(fgpu_batch* b, int slots);
+
+constexpr int kSlotGraph = 8;
+int launch_slots(fgpu_batch* b, long long slots) {
+  if (!b->slot_graph || b->graph_variant != b->variant) { if (int rc = build_slot_graph(b, kSlotGraph)) return rc; }
+  for (long long k = 0; k < (slots + kSlotGraph - 1) / kSlotGraph; ++k)
+    BCUDA_TRY(b, cudaGraphLaunch(b->slot_graph, b->stream));
+  const int n = (int)b->m.size();
+  for (int i = 0; i < n; ++i)
+    BCUDA_TRY(b, cudaMemcpyAsync(b->h_ctls + i, b->m[i]->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, b->stream));
+  return FGPU_OK;
+}
+
+// members' host state into their control blocks (as bt_run does), nsteps each, and a first
+// round of attempt slots (most steps take one attempt); collect_embedded runs the rest
+int enqueue_embedded(fgpu_batch* b, int64_t nsteps) {
+  const int n = (int)b->m.size();
+  if (b->pending_steps == 0) {
+    b->it0.resize(n);
+    b->adj0.resize(n);
+    for (int i = 0; i < n; ++i) {
+      fgpu_handle* h = b->m[i];
+      b->it0[i] = h->iter;
+      b->adj0[i] = h->n_adj;
+      Ctl& c = b->h_ctls[i];
+      std::memset(&c, 0, sizeof(Ctl));
+      c.time = h->time; c.dt = h->dt; c.dtold = h->dtold; c.dtmin = h->dtmin;
+      c.stoptime = h->stoptime; c.tout = h->tout; c.cfl = h->cfl; c.dtlimit = h->dtlimit;
+      c.iter = h->iter; c.brk = h->brk ? 1 : 0; c.dtcause = h->dtcause;
+      c.cvis = h->cvis; c.vis = h->vis ? 1 : 0;
+      c.maxerrold = h->maxerrold; c.last_err = h->last_err; c.n_adj = h->n_adj;
+      c.checkflags = h->checkflags;
+      c.steps_left = nsteps;
+      BCUDA_TRY(b, cudaMemcpyAsync(h->d_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, b->stream));
+    }
+  } else {
+    add_steps_kernel<<<(n + 127) / 128, 128, 0, b->stream>>>(b->d_ctlp, n, (long long)nsteps);
+    BCUDA_TRY(b, cudaGetLastError());
+  }
+  b->pending_steps += nsteps;
+  return launch_slots(b, nsteps + nsteps / 4 + 1);
+}
+
+int collect_embedded(fgpu_batch* b, int* active) {
+  const int n = (int)b->m.size();
+  const int64_t ns = b->pending_steps;
+  long long extra = 0;
+  const long long cap = 64 * (long long)ns + 64;
+  while (true) {
+    BCUDA_TRY(b, cudaStreamSynchronize(b->stream));
+    bool busy = false;
+    for (int i = 0; i < n; ++i) {
+      const Ctl& c = b->h_ctls[i];
+      if (c.steps_left > 0 && !c.stop && !c.brk) busy = true;
+    }
+    if (!busy || ns == 0) break;
+    if (extra > cap) return bset_err(b, FGPU_ETIMEOUT, "batched device-clock step loop: no progress");
+    if (int rc = launch_slots(b, kSlotGraph)) return rc;
+    extra += kSlotGraph;
+  }
+  int act = 0;
+  for (int i = 0; i < n; ++i) {
+    fgpu_handle* h = b->m[i];
+    const Ctl& c = b->h_ctls[i];
+    if (ns > 0) {
+      *h->h_ctl = c;
+      h->time = c.time; h->dt = c.dt; h->dtold = c.dtold; h->dtmin = c.dtmin;
+      h->iter = c.iter; h->brk = c.brk != 0; h->dtcause = c.dtcause;
+      h->maxerrold = c.maxerrold; h->last_err = c.last_err; h->n_adj = c.n_adj;
+      h->checkflags = c.checkflags;
+      if (h->iter > b->it0[i]) h->pre_rt = h->roundtrip_cfg;
+      h->stats.attempts += (h->iter - b->it0[i]) + (h->n_adj - b->adj0[i]);
+      h->stats.cell_updates += (h->iter - b->it0[i]) * h->g.n;
+    }
+    if (!c.stop && !c.brk) ++act;
+  }
+  b->pending_steps = 0;
+  if (active) *active = act;
+  return FGPU_OK;
+}
+
+int build_slot_graph(fgpu_batch* b, int slots) {
+  if (b->slot_graph) { cudaGraphExecDestroy(b->slot_graph); b->slot_graph = nullptr; }
+  cudaGraph_t gr;
+  BCUDA_TRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = 0;
+  for (int k = 0; k < slots && !rc; ++k) rc = enqueue_batch_slot(b);
+  cudaError_t e = cudaStreamEndCapture(b->stream, &gr);
+  if (rc) return rc;
+  if (e != cudaSuccess) return bset_err(b, FGPU_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&b->slot_graph, gr, 0);
+  cudaGraphDestroy(gr);
+  if (e != cudaSuccess) return bset_err(b, FGPU_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  b->graph_variant = b->variant;
+  return FGPU_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -154,14 +418,21 @@ int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
   const fgpu_handle* h0 = members[0];
   if (!h0) return fail(FGPU_EARG, "null member");
   b->nd = h0->nd; b->euler = h0->euler; b->prim = h0->prim; b->order = h0->order;
+  b->embedded = h0->butcher;
   for (int i = 0; i < n; ++i) {
     fgpu_handle* h = members[i];
     if (!h) return fail(FGPU_EARG, "null member");
-    if (h->butcher) return fail(FGPU_EUNSUPPORTED, "batch members use the fixed-step modified Euler scheme");
+    if (h->butcher != b->embedded) return fail(FGPU_EBADCFG, "batch members mix fixed-step and embedded schemes");
+    if (h->butcher) {
+      if (h->adaptive_me) return fail(FGPU_EUNSUPPORTED, "embedded batch members use a Butcher tableau (not the adaptive modified Euler scheme)");
+      if (!h->materialize) return fail(FGPU_EUNSUPPORTED, "embedded batch members need the formed stage states");
+      if (h->cfg.method != h0->cfg.method || h->T.m != h0->T.m || h->T.order != h0->T.order)
+        return fail(FGPU_EBADCFG, "embedded batch members differ in method or order");
+    }
     if (h->fargo) return fail(FGPU_EUNSUPPORTED, "batch members without FARGO transport");
     if (h->accrete) return fail(FGPU_EUNSUPPORTED, "batch members without point-mass accretion");
     if (h->vis) return fail(FGPU_EUNSUPPORTED, "batch members without the viscosity source");
-    if (h->order < 2) return fail(FGPU_EUNSUPPORTED, "batch members of time order 2 or 3");
+    if (!h->butcher && h->order < 2) return fail(FGPU_EUNSUPPORTED, "batch members of time order 2 or 3");
     if (h->nd != b->nd || h->euler != b->euler || h->prim != b->prim || h->order != b->order)
       return fail(FGPU_EBADCFG, "batch members differ in dimensionality, physics, reconstruction variables or order");
     if (h->device != h0->device) return fail(FGPU_EBADCFG, "batch members live on different devices");
@@ -176,6 +447,7 @@ int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
     return fail(FGPU_ECUDA, "stream");
   b->variant = (h0->variant == 1 || h0->variant == 4) ? 0 : h0->variant;
+  if (b->embedded) b->order = 0;   // no fixed stages: d_args holds the tuner's probes only
   // argument tables: step stages of every member, then the tuner's RHS probes
   std::vector<StageArgs> args((size_t)(b->order + 1) * n);
   std::vector<BndArgs> bnd(n);
@@ -191,7 +463,7 @@ int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
     StageArgs R = base_args(h);
     R.in = plain_state(h->buf[0], false);
     R.out_mode = OUT_RHS;
-    R.out = h->buf[2];
+    R.out = b->embedded ? h->buf[2 + h->T.m - 1] : h->buf[2];   // scratch between steps
     R.ctl = nullptr;
     R.kchunk = h->kchunk;
     args[(size_t)b->order * n + i] = R;
@@ -220,6 +492,7 @@ int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
   cudaMemcpyAsync(b->d_tiles, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice, b->stream);
   cudaMemcpyAsync(b->d_bblocks, bblocks.data(), sizeof(int4) * bblocks.size(), cudaMemcpyHostToDevice, b->stream);
   if (cudaStreamSynchronize(b->stream) != cudaSuccess) return fail(FGPU_ECUDA, "batch table upload");
+  if (b->embedded) { if (int rc = build_embedded_tables(b)) return fail(rc, b->err); }
   *out = b;
   return FGPU_OK;
 }
@@ -233,6 +506,10 @@ void fgpu_batch_destroy(fgpu_batch* b) {
   if (b->d_tiles) cudaFree(b->d_tiles);
   if (b->d_bblocks) cudaFree(b->d_bblocks);
   if (b->h_ctls) cudaFreeHost(b->h_ctls);
+  if (b->slot_graph) cudaGraphExecDestroy(b->slot_graph);
+  for (void* p : {(void*)b->d_ctlp, (void*)b->d_btp, (void*)b->d_eargs, (void*)b->d_fargs, (void*)b->d_cargs,
+                  (void*)b->d_copy, (void*)b->d_ebnd, (void*)b->d_cblocks})
+    if (p) cudaFree(p);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -256,6 +533,7 @@ int fgpu_batch_size(const fgpu_batch* b, int* members, int* tiles) {
 
 int fgpu_batch_enqueue(fgpu_batch* b, int64_t nsteps) {
   if (!b || nsteps < 0) return FGPU_EARG;
+  if (b->embedded) return enqueue_embedded(b, nsteps);
   if (b->pending_steps == 0) {
     b->it0.resize(b->m.size());
     for (size_t i = 0; i < b->m.size(); ++i) b->it0[i] = b->m[i]->iter;
@@ -276,6 +554,7 @@ int fgpu_batch_enqueue(fgpu_batch* b, int64_t nsteps) {
 
 int fgpu_batch_collect(fgpu_batch* b, int* active) {
   if (!b) return FGPU_EARG;
+  if (b->embedded) return collect_embedded(b, active);
   BCUDA_TRY(b, cudaStreamSynchronize(b->stream));
   const int n = (int)b->m.size();
   int act = 0;

@@ -28,7 +28,7 @@ struct BtParams {
 // fosite%Step's opening (fosite.f90:367-388 stop test; io/fileio_base.f90:604-621
 // output-time clip) and IntegrationStep's loop head (timedisc_base.f90:649-676)
 // when the slot starts a step; then this slot's attempt.
-__global__ void bt_begin_kernel(Ctl* c) {
+__device__ void bt_begin_body(Ctl* c) {
   c->act = 0;
   if (c->stop | c->brk) return;
   if (c->phase == 0) {
@@ -45,6 +45,7 @@ __global__ void bt_begin_kernel(Ctl* c) {
   c->dtold_att = c->d_att;
   c->act = ACT_ATTEMPT;
 }
+__global__ void bt_begin_kernel(Ctl* c) { bt_begin_body(c); }
 
 // timedisc_base.f90:759-814 AdjustTimestep with correctly rounded exp/log
 __device__ double bt_adjust(Ctl* c, const BtParams& P, double maxerr, double dtold_) {
@@ -70,7 +71,7 @@ __device__ double bt_adjust(Ctl* c, const BtParams& P, double maxerr, double dto
 // The body of IntegrationStep's loop after SolveODE (timedisc_base.f90:684-710): break on a
 // NaN/Inf error, RejectSolution or AcceptSolution (timedisc_base.f90:911-1009), the dtlimit
 // test, the loop condition, and the loop's closing (timedisc_base.f90:712-720).
-__global__ void bt_decide_kernel(Ctl* c, BtParams P) {
+__device__ void bt_decide_body(Ctl* c, const BtParams& P) {
   if (!(c->act & ACT_ATTEMPT) || (c->stop | c->brk)) { c->act = 0; return; }
   const double e = __longlong_as_double((long long)c->err);
   c->err = 0ULL;
@@ -101,11 +102,12 @@ __global__ void bt_decide_kernel(Ctl* c, BtParams P) {
   }
   c->act = act;
 }
+__global__ void bt_decide_kernel(Ctl* c, BtParams P) { bt_decide_body(c, P); }
 
 // CalcTimestep's closing arithmetic after the step's closing RHS and ghost-cell pass
 // (timedisc_base.f90:885-909, the sources list's viscous limit), CheckData's break, and the
 // count of completed fosite steps.
-__global__ void bt_finish_kernel(Ctl* c, int nd) {
+__device__ void bt_finish_body(Ctl* c, int nd) {
   if ((c->stop | c->brk) || !(c->act & ACT_END)) return;
   auto D = [](unsigned long long b) { return __longlong_as_double((long long)b); };
   const double invdt = nd == 2 ? D(c->invdt[0]) : dmax(dmax(D(c->invdt[1]), D(c->invdt[2])), D(c->invdt[0]));
@@ -128,6 +130,97 @@ __global__ void bt_finish_kernel(Ctl* c, int nd) {
   c->dtcause = cause;
   c->phase = 0;
   c->steps_left -= 1;
+}
+__global__ void bt_finish_kernel(Ctl* c, int nd) { bt_finish_body(c, nd); }
+
+// ---- batches of grids with embedded schemes: one thread per member for the scalar work,
+// block tables (member, block, blocks of the member) for the per-cell passes
+__global__ void bt_begin_batch_kernel(Ctl* const* ctls, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) bt_begin_body(ctls[i]);
+}
+__global__ void bt_decide_batch_kernel(Ctl* const* ctls, const BtParams* P, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) bt_decide_body(ctls[i], P[i]);
+}
+__global__ void bt_finish_batch_kernel(Ctl* const* ctls, int n, int nd) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) bt_finish_body(ctls[i], nd);
+}
+
+struct FormArgs {
+  StateRef in;
+  Grid g;
+  PhysP ph;
+  double* out;
+  const Ctl* ctl;
+  int gate;
+};
+template <int ND, bool EU, bool PRIM>
+__global__ void __launch_bounds__(256) batched_form_kernel(const FormArgs* __restrict__ args,
+                                                           const int4* __restrict__ blocks) {
+  using PH = Phys<ND, EU>;
+  constexpr int V = PH::V;
+  const int4 T = blocks[blockIdx.x];
+  const FormArgs& A = args[T.x];
+  if (A.ctl->stop | A.ctl->brk) return;
+  if (gated_out(A.ctl, A.gate)) return;
+  for (long long t = T.y * 256LL + threadIdx.x; t < A.g.n; t += T.z * 256LL) {
+    double u[V], p[V];
+    state_at<V>(A.in, A.g.n, t, u);
+    if (PRIM) PH::c2p(u, p, A.ph);
+#pragma unroll
+    for (int v = 0; v < V; ++v) A.out[(long long)v * A.g.n + t] = PRIM ? p[v] : u[v];
+  }
+}
+
+template <int V>
+__global__ void __launch_bounds__(256) batched_combine_kernel(const CombineArgs* __restrict__ args,
+                                                              const int4* __restrict__ blocks) {
+  __shared__ double sred[RED_STRIDE * 8];
+  const int4 T = blocks[blockIdx.x];
+  const CombineArgs& A = args[T.x];
+  if (A.ctl->stop | A.ctl->brk) return;
+  if (gated_out(A.ctl, A.gate)) return;
+  double bh[FGPU_MAXK], bl[FGPU_MAXK];
+  for (int q = 0; q < A.nstage; ++q) {
+    bh[q] = A.dt_dev ? A.bh_dt[q] * *A.dt_dev : A.bh_dt[q];
+    bl[q] = A.dt_dev ? A.bl_dt[q] * *A.dt_dev : A.bl_dt[q];
+  }
+  double errv = 0.0;
+  for (long long t = T.y * 256LL + threadIdx.x; t < A.n; t += T.z * 256LL) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const double b = __ldg(A.base + (long long)v * A.n + t);
+      double h = b, l = b;
+      for (int q = 0; q < A.nstage; ++q) {
+        const double kq = __ldg(A.K[q] + (long long)v * A.n + t);
+        l = l - bl[q] * kq;
+        h = h - bh[q] * kq;
+      }
+      A.out_high[(long long)v * A.n + t] = h;
+      const double e = fabs(h - l) / (A.tol_rel * fabs(h) + A.tol_abs[v]);
+      errv = dmax(errv, e);
+    }
+  }
+  double vals[3] = {errv, 0.0, 0.0};
+  block_reduce_emit<256>(vals, 1, 0, &A.ctl->err, nullptr, sred);
+}
+
+struct CopyArgs {
+  const double* src;
+  double* dst;
+  long long n;
+  const Ctl* ctl;
+  int gate;
+};
+__global__ void __launch_bounds__(256) batched_copy_kernel(const CopyArgs* __restrict__ args,
+                                                           const int4* __restrict__ blocks) {
+  const int4 T = blocks[blockIdx.x];
+  const CopyArgs& A = args[T.x];
+  if (A.ctl->stop | A.ctl->brk) return;
+  if (gated_out(A.ctl, A.gate)) return;
+  for (long long t = T.y * 256LL + threadIdx.x; t < A.n; t += T.z * 256LL) A.dst[t] = A.src[t];
 }
 
 }  // namespace fgpu

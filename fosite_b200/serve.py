@@ -10,9 +10,10 @@ disk or a 3D Gaussian pulse) integrated from its initial data to its stop time
   * keeps every admitted grid resident on the device from its upload to its
     final download;
   * groups the running grids by kernel class (dimensionality, physics,
-    reconstruction variables, time order) and advances each class as ONE
+    reconstruction variables, time integrator) and advances each class as ONE
     batch (``fgpu_batch_*``): one persistent stage launch per Runge-Kutta stage
-    over the tiles of all its grids.  Membership changes between scheduling
+    over the tiles of all its grids (embedded schemes: one replayed attempt slot
+    per round trip, every grid with its own step-size controller).  Membership changes between scheduling
     rounds (continuous batching): new grids join, finished ones leave;
   * records per request the arrival, admission and completion times.
 
@@ -61,7 +62,8 @@ def build_problem(req):
                                         geometry=abi.LOGCYLINDRICAL if req.seed % 2 else abi.CYLINDRICAL,
                                         fargo=0)
     elif req.kind == "pulse":
-        cfg, p, extra = problems.gauss3d(n=req.size[0], seed=req.seed, method=abi.MODIFIED_EULER)
+        # Dormand-Prince 5(4) with tolerance 1e-5: an embedded-scheme batch class
+        cfg, p, extra = problems.gauss3d(n=req.size[0], seed=req.seed)
     else:
         raise ValueError("unknown request kind %r" % req.kind)
     cfg.stoptime = float(req.t_end)
@@ -70,19 +72,30 @@ def build_problem(req):
     return cfg, p, extra
 
 
+STAGES = {abi.DORMAND_PRINCE: 7, abi.RK_FEHLBERG: 6, abi.CASH_KARP: 6, abi.SSPRK: 5}
+
+
 def footprint_bytes(cfg):
-    """Device bytes of one admitted grid: three state arrays (stored state and
-    two stage scratch arrays), the padded download scratch and the metric."""
+    """Device bytes of one admitted grid: its state arrays (stored state and two stage
+    scratch arrays for the fixed-step scheme; stored state, cold state, m k-arrays and the
+    formed stage state for an embedded scheme of m stages), the padded download scratch and
+    the metric."""
     nd = 3 if cfg.knum > 1 else 2
     vnum = 1 + nd + (1 if cfg.physics == abi.EULER else 0)
     n = cfg.inum * cfg.jnum * cfg.knum
     npad = (cfg.inum + 4) * (cfg.jnum + 4) * (cfg.knum + 4 if nd == 3 else 1)
-    return 8 * vnum * (3 * n + 2 * npad) + 8 * 40 * (cfg.inum + 4) + (1 << 16)
+    arrays = 3
+    if cfg.method != abi.MODIFIED_EULER:
+        m = STAGES.get(cfg.method, 7)
+        if cfg.method in (abi.RK_FEHLBERG, abi.SSPRK) and cfg.tdorder == 3:
+            m = 3
+        arrays = 3 + m
+    return 8 * vnum * (arrays * n + 2 * npad) + 8 * 40 * (cfg.inum + 4) + (1 << 16)
 
 
 def kernel_class(cfg):
     nd = 3 if cfg.knum > 1 else 2
-    return (nd, cfg.physics, cfg.variables, cfg.tdorder)
+    return (nd, cfg.physics, cfg.variables, cfg.method, cfg.tdorder)
 
 
 class Server:

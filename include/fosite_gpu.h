@@ -273,9 +273,12 @@ int fgpu_autotune(fgpu_handle* h, int reps, int* variant);
  * A batch advances many independent grids with one persistent launch per
  * Runge-Kutta stage over the flattened tile queue of all grids, plus one
  * ghost-cell / CFL / finalize launch.  Members are handles created, uploaded
- * and past fgpu_first_step, all with the fixed-step modified Euler scheme of
- * time order 2 or 3, the same dimensionality, physics and reconstruction
- * variables, no FARGO, on one device; mesh sizes, geometry, limiters,
+ * and past fgpu_first_step, all with either the fixed-step modified Euler
+ * scheme of time order 2 or 3 or the same embedded Butcher scheme (Dormand-
+ * Prince, Fehlberg, Cash-Karp, SSPRK; each member keeps its own tolerances,
+ * error norm and step-size controller, advanced attempt by attempt on the
+ * device), the same dimensionality, physics and reconstruction variables, no
+ * FARGO, accretion or viscosity, on one device; mesh sizes, geometry, limiters,
  * boundaries and physical parameters may differ.  Each member keeps its own
  * dt, time and stop state (a member that reached its stop time idles), and its
  * results are bitwise those of stepping it alone.  The handles stay owned by

@@ -129,7 +129,19 @@ def test_batch_rejects_mixed_or_unsupported_members():
     d.set_state(abi.PVAR, p3)
     d.first_step()
     with pytest.raises(FositeError):
-        Batch([d])                       # embedded RK members are not batched
+        Batch([a, d])                    # fixed-step and embedded members
+    c4, p4, _ = _khi(n=(24, 24), me_tol=1e-3)
+    e = Simulation(c4)
+    e.set_state(abi.PVAR, p4)
+    e.first_step()
+    with pytest.raises(FositeError):
+        Batch([e])                       # adaptive modified Euler members are not batched
+    c5, p5, _ = _khi(n=(24, 24), method=abi.CASH_KARP, tdorder=5)
+    f = Simulation(c5)
+    f.set_state(abi.PVAR, p5)
+    f.first_step()
+    with pytest.raises(FositeError):
+        Batch([d, f])                    # different tableaus
 
 
 def test_single_grid_autotune_keeps_results():
@@ -167,3 +179,46 @@ def test_autotune_3d_chunks_and_cache_keep_results():
         assert s.run(6)[0] == 0
     assert np.array_equal(a.get(abi.CVAR), c.get(abi.CVAR))
     assert np.array_equal(b.get(abi.CVAR), c.get(abi.CVAR))
+
+
+def test_embedded_batch_equals_lone_runs_and_oracle():
+    """Dormand-Prince members of different sizes and tolerances in one batch: one attempt slot
+    per replay advances every member with its own controller (rejections and sub-steps
+    included); each member equals its lone device-clock run and the oracle bit for bit."""
+    import pyoracle
+    from fosite_b200.sim import Batch, Simulation
+    specs = [((14, 12, 10), 1e-5), ((20, 18, 16), 1e-4), ((12, 16, 14), 3e-5)]
+
+    def make():
+        out = []
+        for n, tol in specs:
+            cfg, p, _ = _gauss3d(n=n, tol=tol)
+            s = Simulation(cfg, exact=True)
+            s.set_state(abi.PVAR, p)
+            s.first_step()
+            out.append(s)
+        return out
+    members, alone = make(), make()
+    b = Batch(members)
+    b.autotune(2)
+    assert b.run(7) == len(specs)
+    for s in alone:
+        assert s.run(7) == (0, 7)
+    for m, s in zip(members, alone):
+        sm, ss = m.status(), s.status()
+        assert (sm.time, sm.dt, sm.iter, sm.n_adj) == (ss.time, ss.dt, ss.iter, ss.n_adj)
+        assert np.array_equal(m.get(abi.CVAR), s.get(abi.CVAR))
+    cfg, p, _ = _gauss3d(n=specs[1][0], tol=specs[1][1])
+    o = pyoracle.Oracle(cfg)
+    o.set_state(abi.PVAR, p)
+    o.first_step()
+    for _ in range(7):
+        assert o.step() == 0
+    assert o.status().n_adj == members[1].status().n_adj and o.status().time == members[1].status().time
+    assert np.array_equal(o.get(abi.CVAR), members[1].get(abi.CVAR))
+    # a second round continues from the members' state
+    assert b.run(3) == len(specs)
+    for s in alone:
+        s.run(3)
+    for m, s in zip(members, alone):
+        assert np.array_equal(m.get(abi.CVAR), s.get(abi.CVAR))

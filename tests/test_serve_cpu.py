@@ -36,4 +36,4 @@ def test_kernel_classes_group_compatible_requests():
     k4 = kernel_class(build_problem(Request("pulse", (32, 32, 32), 0.1))[0])
     assert k1 == k2 and len({k1, k3, k4}) == 3
     cfg = build_problem(Request("pulse", (32, 32, 32), 0.25))[0]
-    assert cfg.method == abi.MODIFIED_EULER and cfg.stoptime == 0.25
+    assert cfg.method == abi.DORMAND_PRINCE and cfg.stoptime == 0.25   # configs: the pulse is DOPRI
