@@ -517,8 +517,12 @@ __device__ __forceinline__ void kt_flux(int d, const double* RL, const double* R
   }
   double csL = EU ? PH::cs_of(pL, P) : csL_iso;
   double csR = EU ? PH::cs_of(pR, P) : csR_iso;
-  int vn = 1 + d;
-  double uL = pL[vn], uR = pR[vn];
+  const int vn = 1 + d;
+  // the normal velocity by selection (d may be a run-time value: no indexed register arrays)
+  auto normal = [&](const double* q) {
+    return ND == 3 ? (vn == 1 ? q[1] : (vn == 2 ? q[2] : q[3])) : (vn == 1 ? q[1] : q[2]);
+  };
+  double uL = normal(pL), uR = normal(pR);
   double am = dmin(dmin(0.0, dmin(0., uR - csR)), dmin(0., uL - csL));
   double ap = dmax(dmax(0.0, dmax(0., uR + csR)), dmax(0., uL + csL));
   double fL[V], fR[V];

@@ -311,63 +311,83 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
     // work items are enumerated over the full tile shape (compile-time divisors) and the
     // ones outside a partial edge tile are skipped
     constexpr int NSX = TY * (TX + 2), NSY = (TY + 2) * TX;
+    constexpr int RHW = RH * RW;
     if (!A.constant_recon) {
+      // one code path for both directions (no divergence where a warp spans the x/y boundary)
       for (int t = tid; t < NSX + NSY; t += NT) {
+        int cidx, step, sidx, sstride;
+        double* Sout;
+        double invd;
         if (t < NSX) {
-          int r = t / (TX + 2), c = t % (TX + 2) - 1;
+          const int r = t / (TX + 2), c = t % (TX + 2) - 1;
           if (r >= ey || c > ex) continue;
-#pragma unroll
-          for (int v = 0; v < V; ++v)
-            SX(v, r, c + 1) = slope(A.limiter, A.theta, A.invd[0], RS(v, r + 2, c + 1), RS(v, r + 2, c + 2), RS(v, r + 2, c + 3));
+          cidx = (r + 2) * RW + (c + 2); step = 1;
+          Sout = Sx; sidx = r * (TX + 2) + (c + 1); sstride = TY * (TX + 2);
+          invd = A.invd[0];
         } else {
-          int u = t - NSX;
-          int c = u % TX, r = u / TX - 1;
+          const int u = t - NSX;
+          const int c = u % TX, r = u / TX - 1;
           if (c >= ex || r > ey) continue;
+          cidx = (r + 2) * RW + (c + 2); step = RW;
+          Sout = Sy; sidx = (r + 1) * TX + c; sstride = (TY + 2) * TX;
+          invd = A.invd[1];
+        }
 #pragma unroll
-          for (int v = 0; v < V; ++v)
-            SY(v, r + 1, c) = slope(A.limiter, A.theta, A.invd[1], RS(v, r + 1, c + 2), RS(v, r + 2, c + 2), RS(v, r + 3, c + 2));
+        for (int v = 0; v < V; ++v) {
+          const double* R = Rs + v * RHW + cidx;
+          Sout[v * sstride + sidx] = slope(A.limiter, A.theta, invd, R[-step], R[0], R[step]);
         }
       }
       __syncthreads();
     }
-    // ---- interface fluxes of both directions in one phase
+    // ---- interface fluxes of both directions in one phase, one code path
     constexpr int NFX = TY * (TX + 1), NFY = (TY + 1) * TX;
     for (int t = tid; t < NFX + NFY; t += NT) {
       double RL[V], RR[V], F[V];
-      if (t < NFX) {
-        int r = t / (TX + 1), f = t % (TX + 1);
+      int lidx, ridx, sL, sR, sstride, fstride, d;
+      const double* S;
+      double* Fout;
+      double oL, oR, csL, csR, dA;
+      const bool xf = t < NFX;
+      int xr = 0, xfc = 0;
+      if (xf) {
+        const int r = t / (TX + 1), f = t % (TX + 1);
         if (r >= ey || f > ex) continue;
-        int gl = i0 + f - 1 + 2;   // padded i of the left cell
-        double oE = M.offxE[gl], oW = M.offxW[gl + 1];
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-          RL[v] = A.constant_recon ? RS(v, r + 2, f + 1) : RS(v, r + 2, f + 1) + SX(v, r, f) * oE;
-          RR[v] = A.constant_recon ? RS(v, r + 2, f + 2) : RS(v, r + 2, f + 2) + SX(v, r, f + 1) * oW;
-        }
-        kt_flux<ND, EU, PRIM>(0, RL, RR, EU ? 0.0 : M.cs[2 * M.nxp + gl], EU ? 0.0 : M.cs[1 * M.nxp + gl + 1],
-                              M.dAxW[gl + 1], P, F);
-#pragma unroll
-        for (int v = 0; v < V; ++v) FX(v, r, f) = F[v];
-        // boundary row of ComputeRHS (timedisc_base.f90:1224-1231) for the accretion bookkeeping
-        if (ND == 2 && A.brow && ((A.brow_face == 0 && i0 + f == 0) || (A.brow_face == 1 && i0 + f == g.nx)))
-          A.brow[j0 + r] = (A.brow_face == 0 ? A.bdydz : -A.bdydz) * F[0];
+        const int gl = i0 + f - 1 + 2;   // padded i of the left cell
+        oL = M.offxE[gl]; oR = M.offxW[gl + 1];
+        lidx = (r + 2) * RW + (f + 1); ridx = lidx + 1;
+        S = Sx; sL = r * (TX + 2) + f; sR = sL + 1; sstride = TY * (TX + 2);
+        csL = EU ? 0.0 : M.cs[2 * M.nxp + gl]; csR = EU ? 0.0 : M.cs[1 * M.nxp + gl + 1];
+        dA = M.dAxW[gl + 1];
+        Fout = Fx + r * (TX + 1) + f; fstride = TY * (TX + 1);
+        d = 0;
+        xr = r; xfc = f;
       } else {
-        int u = t - NFX;
-        int c = u % TX, f = u / TX;
+        const int u = t - NFX;
+        const int c = u % TX, f = u / TX;
         if (c >= ex || f > ey) continue;
-        int gjl = j0 + f - 1 + 2;     // padded j of the lower cell
-        int gi = i0 + c + 2;          // padded i of the column
-        double oN = M.offyN[gjl], oS = M.offyS[gjl + 1];
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-          RL[v] = A.constant_recon ? RS(v, f + 1, c + 2) : RS(v, f + 1, c + 2) + SY(v, f, c) * oN;
-          RR[v] = A.constant_recon ? RS(v, f + 2, c + 2) : RS(v, f + 2, c + 2) + SY(v, f + 1, c) * oS;
-        }
-        kt_flux<ND, EU, PRIM>(1, RL, RR, EU ? 0.0 : M.cs[4 * M.nxp + gi], EU ? 0.0 : M.cs[3 * M.nxp + gi],
-                              M.dAyS[gi], P, F);
-#pragma unroll
-        for (int v = 0; v < V; ++v) FY(v, f, c) = F[v];
+        const int gjl = j0 + f - 1 + 2;     // padded j of the lower cell
+        const int gi = i0 + c + 2;          // padded i of the column
+        oL = M.offyN[gjl]; oR = M.offyS[gjl + 1];
+        lidx = (f + 1) * RW + (c + 2); ridx = lidx + RW;
+        S = Sy; sL = f * TX + c; sR = sL + TX; sstride = (TY + 2) * TX;
+        csL = EU ? 0.0 : M.cs[4 * M.nxp + gi]; csR = EU ? 0.0 : M.cs[3 * M.nxp + gi];
+        dA = M.dAyS[gi];
+        Fout = Fy + f * TX + c; fstride = (TY + 1) * TX;
+        d = 1;
       }
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const double rl = Rs[v * RHW + lidx], rr = Rs[v * RHW + ridx];
+        RL[v] = A.constant_recon ? rl : rl + S[v * sstride + sL] * oL;
+        RR[v] = A.constant_recon ? rr : rr + S[v * sstride + sR] * oR;
+      }
+      kt_flux<ND, EU, PRIM>(d, RL, RR, csL, csR, dA, P, F);
+#pragma unroll
+      for (int v = 0; v < V; ++v) Fout[v * fstride] = F[v];
+      // boundary row of ComputeRHS (timedisc_base.f90:1224-1231) for the accretion bookkeeping
+      if (ND == 2 && xf && A.brow && ((A.brow_face == 0 && i0 + xfc == 0) || (A.brow_face == 1 && i0 + xfc == g.nx)))
+        A.brow[j0 + xr] = (A.brow_face == 0 ? A.bdydz : -A.bdydz) * F[0];
     }
     __syncthreads();
 
