@@ -446,7 +446,7 @@ int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
   cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, h0->device);
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
     return fail(FGPU_ECUDA, "stream");
-  b->variant = (h0->variant == 1 || h0->variant == 4) ? 0 : h0->variant;
+  b->variant = (h0->variant == 1 || h0->variant >= 4) ? 0 : h0->variant;
   if (b->embedded) b->order = 0;   // no fixed stages: d_args holds the tuner's probes only
   // argument tables: step stages of every member, then the tuner's RHS probes
   std::vector<StageArgs> args((size_t)(b->order + 1) * n);
@@ -660,7 +660,7 @@ int fgpu_autotune(fgpu_handle* h, int reps, int* variant) {
   A.out = scratch;
   A.ctl = nullptr;
   A.visc = h->vis ? h->d_visc : nullptr;   // the stencil's read of the viscous source
-  const int cand[5] = {0, 2, 3, 4, 1};
+  const int cand[6] = {0, 2, 3, 4, 5, 1};
   // 3D: the z extent a block marches through (smaller chunks give small grids more blocks);
   // FGPU_KCHUNK fixes it
   std::vector<int> chunks;

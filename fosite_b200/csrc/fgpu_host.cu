@@ -430,8 +430,8 @@ struct TileLayout {
 // 4 a taller tile (2D 32x16, 3D 32x8 with 2 blocks per SM) that halves the y halo;
 // 1 is the warp-shuffle kernel of fgpu_stage2.cuh.
 template <int ND> struct TileShapes;
-template <> struct TileShapes<2> { static constexpr int TY = 8, M2 = 2, M3 = 3, TY4 = 16, M4 = 1; };
-template <> struct TileShapes<3> { static constexpr int TY = 4, M2 = 4, M3 = 6, TY4 = 8, M4 = 2; };
+template <> struct TileShapes<2> { static constexpr int TY = 8, M2 = 2, M3 = 3, TY4 = 16, M4 = 1, M5 = 1; };
+template <> struct TileShapes<3> { static constexpr int TY = 4, M2 = 4, M3 = 6, TY4 = 8, M4 = 2, M5 = 3; };
 
 template <int ND, bool EU, bool PRIM>
 void configure_stage_kernels_t() {
@@ -440,6 +440,7 @@ void configure_stage_kernels_t() {
   TileLayout<ND, EU, PRIM, 32, S::TY, S::M2>::configure(true);
   TileLayout<ND, EU, PRIM, 32, S::TY, S::M3>::configure(true);
   TileLayout<ND, EU, PRIM, 32, S::TY4, S::M4>::configure(false);
+  TileLayout<ND, EU, PRIM, 32, S::TY4, S::M5>::configure(false);
 }
 void configure_stage_kernels(int nd, bool e, bool p) {
   if (nd == 2) {
@@ -471,6 +472,7 @@ int launch_stage_t(fgpu_handle* h, StageArgs& A) {
     case 2: TileLayout<ND, EU, PRIM, 32, S::TY, S::M2>::launch(g, h->kchunk, h->stream, A); break;
     case 3: TileLayout<ND, EU, PRIM, 32, S::TY, S::M3>::launch(g, h->kchunk, h->stream, A); break;
     case 4: TileLayout<ND, EU, PRIM, 32, S::TY4, S::M4>::launch(g, h->kchunk, h->stream, A); break;
+    case 5: TileLayout<ND, EU, PRIM, 32, S::TY4, S::M5>::launch(g, h->kchunk, h->stream, A); break;
     default: TileLayout<ND, EU, PRIM, 32, S::TY, 1>::launch(g, h->kchunk, h->stream, A); break;
   }
   CUDA_TRY(h, cudaGetLastError());
@@ -1367,7 +1369,7 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
   }
   if (!rc) {
     // FGPU_STAGE_VARIANT / FGPU_KCHUNK force a stage-kernel layout and z chunk (the tuner's choice otherwise)
-    if (const char* e = std::getenv("FGPU_STAGE_VARIANT")) h->variant = std::max(0, std::min(4, std::atoi(e)));
+    if (const char* e = std::getenv("FGPU_STAGE_VARIANT")) h->variant = std::max(0, std::min(5, std::atoi(e)));
     if (const char* e = std::getenv("FGPU_KCHUNK")) { int v = std::atoi(e); if (v > 0) h->kchunk = v; }
     if (const char* e = std::getenv("FGPU_MATERIALIZE")) h->materialize = std::atoi(e) != 0;
   }
