@@ -293,12 +293,13 @@ def run_own(args, world, rank, local):
                    "grid": [cfg.inum, cfg.jnum, cfg.knum], "parallelism": "replicas x%d" % world,
                    "l2": "inputs larger than L2: each state array is %.0f MB" % (n_cells * sim.vnum * 8 / 1e6),
                    "accepted_steps_per_rank": int(st.cell_updates // n_cells), "attempts": int(st.attempts),
-                   "stage_variant": variant, "stage_variant_source": "forced" if forced is not None else "autotuned"},
+                   "stage_variant": variant, "stage_kchunk": sim.stage_layout()[1] if cfg.knum > 1 else None,
+                   "stage_variant_source": "forced" if forced is not None else "autotuned"},
         "achieved_gbps_step": value / world * bpc / 1e9,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "kernel": "RHS stage: stage_kernel (fused RHS + stage update), for Butcher stages with "
-                               "the form_kernel pass that forms its input state",
+                     "kernel": "RHS stage: stage_kernel (fused RHS + stage update; a Butcher stage's epilogue "
+                               "forms the next stage's input state, the form_kernel pass only stage 2's)",
                      "form_ms_per_launch": stp.form_ms / max(1, stp.stage_launches),
                      "peak_kind": peak_kind + " copy bandwidth (burst)",
                      "algorithmic_bytes_per_launch": stp.stage_bytes / max(1, stp.stage_launches),

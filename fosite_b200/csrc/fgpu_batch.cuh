@@ -197,12 +197,13 @@ int build_embedded_tables(fgpu_batch* b) {
       A.in.dt_dev = &c->d_att;
       FormArgs F;
       std::memset(&F, 0, sizeof(F));
-      F.in = A.in; F.g = h->g; F.ph = h->ph; F.out = h->buf[2 + T.m]; F.ctl = c; F.gate = ACT_ATTEMPT;
+      F.in = A.in; F.g = h->g; F.ph = h->ph; F.out = stage_rbuf(h, m); F.ctl = c; F.gate = ACT_ATTEMPT;
       fargs[(size_t)(m - 2) * n + i] = F;
-      A.rin = plain_state(h->buf[2 + T.m], false);
+      A.rin = plain_state(stage_rbuf(h, m), false);
       A.rin.ready = h->prim ? 1 : 0;
       A.out_mode = OUT_RHS;
       A.out = h->buf[2 + m - 1];
+      set_fnext(h, A, m, 0.0, &c->d_att);
       A.gate = ACT_ATTEMPT;
       A.kchunk = h->kchunk;
       eargs[(size_t)(m - 2) * n + i] = A;
@@ -275,7 +276,8 @@ int enqueue_batch_slot(fgpu_batch* b) {
   bt_begin_batch_kernel<<<mb, 128, 0, b->stream>>>(b->d_ctlp, n);
   BCUDA_TRY(b, cudaGetLastError());
   for (int m = 2; m <= M; ++m) {
-    if (int rc = launch_batched_form(b, b->d_fargs + (size_t)(m - 2) * n)) return rc;
+    if (m == 2 || !b->m[0]->fuse_form)
+      if (int rc = launch_batched_form(b, b->d_fargs + (size_t)(m - 2) * n)) return rc;
     if (int rc = launch_batched_stage(b, b->d_eargs + (size_t)(m - 2) * n, b->variant)) return rc;
   }
   switch (b->m[0]->V) {
@@ -426,6 +428,7 @@ int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
     if (h->butcher) {
       if (h->adaptive_me) return fail(FGPU_EUNSUPPORTED, "embedded batch members use a Butcher tableau (not the adaptive modified Euler scheme)");
       if (!h->materialize) return fail(FGPU_EUNSUPPORTED, "embedded batch members need the formed stage states");
+      if (h->fuse_form != h0->fuse_form) return fail(FGPU_EBADCFG, "embedded batch members differ in stage-state formation");
       if (h->cfg.method != h0->cfg.method || h->T.m != h0->T.m || h->T.order != h0->T.order)
         return fail(FGPU_EBADCFG, "embedded batch members differ in method or order");
     }
@@ -693,6 +696,13 @@ int fgpu_autotune(fgpu_handle* h, int reps, int* variant) {
     std::lock_guard<std::mutex> lock(g_tune_mutex);
     g_tune_cache[key] = TuneChoice{bv, bk};
   }
+  return FGPU_OK;
+}
+
+int fgpu_stage_layout(const fgpu_handle* h, int* variant, int* kchunk) {
+  if (!h) return FGPU_EARG;
+  if (variant) *variant = h->variant;
+  if (kchunk) *kchunk = h->kchunk;
   return FGPU_OK;
 }
 

@@ -156,6 +156,7 @@ struct fgpu_handle {
   int tile_x = 32, tile_y = 8, kchunk = 16;
   bool adaptive_me = false;     // modified Euler with embedded error control (tol_rel < 1)
   bool materialize = true;      // Butcher stages: form the stage's reconstruction variables once per cell
+  bool fuse_form = true;        // ... stage m's kernel forms stage m+1's (buffers alternate), only stage 2 by form_kernel
   double* d_ready = nullptr;    // ... into this array (one state)
   int variant = 0;              // stage kernel layout: 0 shared-memory tile, 1 warp-shuffle window,
                                 // 2/3 tile with a register cap for more resident blocks, 4 taller tile
@@ -723,6 +724,28 @@ StageArgs base_args(fgpu_handle* h) {
   return A;
 }
 
+// Butcher stage m's formed input (reconstruction variables), alternating between two buffers
+// when the stage kernels form the next stage's state (fuse_form)
+double* stage_rbuf(const fgpu_handle* h, int m) {
+  return h->buf[2 + h->T.m + (h->fuse_form ? (m % 2) : 0)];
+}
+// let stage m (< M) form stage m+1's state: base - sum_{q<=m} (a_{m+1,q} dt) k_q into its buffer;
+// coefficients times dt on the host (dt_dev null) or, on the device clock, times *dt_dev
+void set_fnext(const fgpu_handle* h, StageArgs& A, int m, double dtv, const double* dt_dev) {
+  const Tableau& T = h->T;
+  if (!h->fuse_form || m >= T.m) return;
+  StateRef& S = A.fnext;
+  std::memset(&S, 0, sizeof(S));
+  S.base = h->buf[1];
+  S.nk = m;
+  for (int q = 0; q < m; ++q) {
+    S.K[q] = h->buf[2 + q];
+    S.coef[q] = dt_dev ? T.A[m * T.m + q] : T.A[m * T.m + q] * dtv;
+  }
+  S.dt_dev = dt_dev;
+  A.fnext_out = stage_rbuf(h, m + 1);
+}
+
 BndArgs bnd_args(fgpu_handle* h, const double* state, bool roundtrip, int finalize) {
   BndArgs B;
   std::memset(&B, 0, sizeof(B));
@@ -1097,14 +1120,17 @@ int butcher_attempt(fgpu_handle* h, double t, double dtv, double& err) {
     }
     if (h->materialize) {
       // the stage state's reconstruction variables once per cell, read by the stencil
-      double* R = h->buf[2 + T.m];
+      // (formed by the previous stage's kernel when fuse_form, else by form_kernel)
+      double* R = stage_rbuf(h, m);
       StateRef S = A.in;
-      if (int rc = timed_launch(h, 2, 0.0, [&] { return launch_form(h, S, R); })) return rc;
+      if (m == 2 || !h->fuse_form)
+        if (int rc = timed_launch(h, 2, 0.0, [&] { return launch_form(h, S, R); })) return rc;
       A.rin = plain_state(R, false);
       A.rin.ready = h->prim ? 1 : 0;
     }
     A.out_mode = OUT_RHS;
     A.out = h->buf[2 + m - 1];
+    set_fnext(h, A, m, dtv, nullptr);
     const bool fused_end = m == T.m && !h->materialize;
     if (fused_end) {
       A.last_stage = 1;
@@ -1372,6 +1398,8 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
     if (const char* e = std::getenv("FGPU_STAGE_VARIANT")) h->variant = std::max(0, std::min(5, std::atoi(e)));
     if (const char* e = std::getenv("FGPU_KCHUNK")) { int v = std::atoi(e); if (v > 0) h->kchunk = v; }
     if (const char* e = std::getenv("FGPU_MATERIALIZE")) h->materialize = std::atoi(e) != 0;
+    if (const char* e = std::getenv("FGPU_FUSE_FORM")) h->fuse_form = std::atoi(e) != 0;
+    h->fuse_form = h->fuse_form && h->materialize;
   }
   if (!rc) configure_stage_kernels(h->nd, h->euler, h->prim);
   if (!rc && h->vis) configure_visc(h->nd, h->euler);
@@ -1387,7 +1415,8 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
   }
   if (!rc) rc = upload_metric(h);
   if (!rc) {
-    int nbuf = h->butcher ? 2 + h->T.m + 1 : 3;   // Butcher: P, base, k1..km, formed stage state
+    // Butcher: P, base, k1..km, formed stage state(s)
+    int nbuf = h->butcher ? 2 + h->T.m + 1 + (h->fuse_form ? 1 : 0) : 3;
     size_t bytes = sizeof(double) * h->V * h->g.n;
     for (int b = 0; b < nbuf && !rc; ++b) {
       double* p = nullptr;
@@ -1728,13 +1757,15 @@ static int enqueue_bt_slot(fgpu_handle* h) {
         A.in.coef[q] = T.A[(m - 1) * T.m + q];
       }
       A.in.dt_dev = d_att;
-      double* R = h->buf[2 + T.m];
+      double* R = stage_rbuf(h, m);
       StateRef S = A.in;
-      if (int rc = timed_launch(h, 2, 0.0, [&] { return launch_form(h, S, R, ACT_ATTEMPT); })) return rc;
+      if (m == 2 || !h->fuse_form)
+        if (int rc = timed_launch(h, 2, 0.0, [&] { return launch_form(h, S, R, ACT_ATTEMPT); })) return rc;
       A.rin = plain_state(R, false);
       A.rin.ready = h->prim ? 1 : 0;
       A.out_mode = OUT_RHS;
       A.out = h->buf[2 + m - 1];
+      set_fnext(h, A, m, 0.0, d_att);
       A.gate = ACT_ATTEMPT;
       if (int rc = launch_stage(h, A, RhsTime::att(T.c[m - 1]))) return rc;
     }

@@ -78,6 +78,10 @@ struct StageArgs {
   const double* visc;
   // device-clock attempt slots: run only if the slot's actions include a gate bit
   int gate;
+  // optional (Butcher stage m < M, OUT_RHS): the next stage's state (base and k_1..k_m, the
+  // last being this stage's output) formed into fnext_out as its reconstruction variables
+  StateRef fnext;
+  double* fnext_out;
 };
 
 // block-wide max of up to 4 non-negative doubles + OR of flags, then one atomic per block;
@@ -126,6 +130,10 @@ constexpr size_t stage_smem_bytes() {
 // One TX x TY tile (bx, by) of one grid, z chunk bz.  Shared by the single-grid
 // kernel (arguments in the parameter space) and the batched kernel (per-grid
 // arguments in global memory, tiles from a flattened queue).
+__device__ __forceinline__ void prefetch_l2(const double* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 template <int ND, bool EU, bool PRIM, int TX, int TY>
 __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, const int by, const int bz) {
   using PH = Phys<ND, EU>;
@@ -249,6 +257,18 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
 
   for (int k = k0; k < k1; ++k) {
     double divZ[V];
+    if (A.fnext_out && own) {
+      // the stream the epilogue forms the next stage's state from (base and the earlier
+      // stages' k of this cell), fetched into L2 while the plane's stencil runs
+      const long long pidx = CE::lin(g, i, j, k);
+      const StateRef& S = A.fnext;
+#pragma unroll
+      for (int v = 0; v < V; ++v) prefetch_l2(S.base + (long long)v * g.n + pidx);
+#pragma unroll 1
+      for (int q = 0; q + 1 < S.nk; ++q)
+#pragma unroll
+        for (int v = 0; v < V; ++v) prefetch_l2(S.K[q] + (long long)v * g.n + pidx);
+    }
     // ---- own cell: plane k into shared memory; z-flux at k+1/2
     if (own) {
       double Rc[V];
@@ -509,6 +529,38 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
       if (A.out_mode == OUT_RHS) {
 #pragma unroll
         for (int v = 0; v < V; ++v) A.out[(long long)v * g.n + idx] = rhs[v];
+        if (A.fnext_out) {
+          // the next Butcher stage's state base - sum_q (a dt) k_q in the reference's order
+          // (timedisc_rkfehlberg.f90:277-302), this stage's k from the registers, formed as
+          // form_kernel would form it
+          const StateRef& S = A.fnext;
+          double u[V];
+#pragma unroll
+          for (int v = 0; v < V; ++v) u[v] = __ldg(S.base + (long long)v * g.n + idx);
+          // the earlier stages' k (unrolled to the tableau limit, so all loads issue together)
+#pragma unroll
+          for (int q = 0; q < FGPU_MAXK - 1; ++q) {
+            if (q + 1 < S.nk) {
+              const double a = S.dt_dev ? S.coef[q] * *S.dt_dev : S.coef[q];
+#pragma unroll
+              for (int v = 0; v < V; ++v) u[v] = u[v] - a * __ldg(S.K[q] + (long long)v * g.n + idx);
+            }
+          }
+          {
+            const double a = S.dt_dev ? S.coef[S.nk - 1] * *S.dt_dev : S.coef[S.nk - 1];
+#pragma unroll
+            for (int v = 0; v < V; ++v) u[v] = u[v] - a * rhs[v];
+          }
+          if (PRIM) {
+            double p[V];
+            PH::c2p(u, p, P);
+#pragma unroll
+            for (int v = 0; v < V; ++v) A.fnext_out[(long long)v * g.n + idx] = p[v];
+          } else {
+#pragma unroll
+            for (int v = 0; v < V; ++v) A.fnext_out[(long long)v * g.n + idx] = u[v];
+          }
+        }
       } else {
         // Shu-Osher update y = yn - dt*rhs + eta*(y0 - yn + dt*rhs) (timedisc_modeuler.f90:289)
         double yn[V], y0[V], y[V];

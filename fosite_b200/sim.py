@@ -56,6 +56,7 @@ def lib(exact=False):
     L.fgpu_get_stats.argtypes = [C.c_void_p, C.POINTER(abi.Stats)]
     L.fgpu_reset_stats.argtypes = [C.c_void_p]
     L.fgpu_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+    L.fgpu_stage_layout.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.fgpu_get_pointmass.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.fgpu_set_fargo_velocity.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
     L.fgpu_batch_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]
@@ -202,6 +203,12 @@ class Simulation:
         v = C.c_int(0)
         self._check(self.L.fgpu_autotune(self.h, int(reps), C.byref(v)))
         return int(v.value)
+
+    def stage_layout(self):
+        """(layout id, z chunk) of the stage kernel later steps launch."""
+        v, k = C.c_int(0), C.c_int(0)
+        self._check(self.L.fgpu_stage_layout(self.h, C.byref(v), C.byref(k)))
+        return int(v.value), int(k.value)
 
 
 class Batch:

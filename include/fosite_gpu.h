@@ -267,6 +267,10 @@ int fgpu_calc_timestep(fgpu_handle* h, double* dt);
  * probing; reps < 0 measures |reps| times anyway and refreshes the entry.  No
  * counterpart in the reference. */
 int fgpu_autotune(fgpu_handle* h, int reps, int* variant);
+/* The stage-kernel layout later steps use (the tuner's choice, FGPU_STAGE_VARIANT, or
+ * the default 0) and, for 3D grids, the z extent one block marches through.  Either
+ * pointer may be NULL.  No counterpart in the reference. */
+int fgpu_stage_layout(const fgpu_handle* h, int* variant, int* kchunk);
 
 /* ---- batched ensembles (no counterpart in the reference, which integrates one
  * grid per process) ---------------------------------------------------------

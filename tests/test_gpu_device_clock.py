@@ -94,3 +94,27 @@ def test_device_clock_stops_at_stoptime():
     assert np.array_equal(o.get(abi.CVAR), g.get(abi.CVAR))
     rc, done = g.run(5)
     assert rc == abi.STOPTIME and done == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("host", [False, True])
+@pytest.mark.parametrize("name", ["gauss3d_dopri_mc_prim", "gauss3d_rkf3_minmod_cons", "iso3d_beta_dopri",
+                                  "euler2d_rkf45", "disk_powerlaw_pringle_ssprk5", "gauss3d_visc_dopri"])
+def test_fused_stage_state_equals_form_pass(name, host, monkeypatch):
+    """Butcher stage states formed in the previous stage kernel's epilogue (the default)
+    equal the ones a separate form pass writes (FGPU_FUSE_FORM=0), bit for bit, on the
+    device clock and on the host-controlled loop (FGPU_BUTCHER_HOST=1)."""
+    if host:
+        monkeypatch.setenv("FGPU_BUTCHER_HOST", "1")
+    sims = []
+    for fuse in ("1", "0"):
+        monkeypatch.setenv("FGPU_FUSE_FORM", fuse)
+        _, _, g = _pair(name, exact=True)
+        assert g.first_step() == 0
+        rc, done = g.run(5)
+        assert rc == 0 and done == 5
+        sims.append(g)
+    a, b = sims
+    sa, sb = a.status(), b.status()
+    assert (sa.time, sa.dt, sa.iter, sa.n_adj) == (sb.time, sb.dt, sb.iter, sb.n_adj)
+    assert np.array_equal(a.get(abi.CVAR), b.get(abi.CVAR))
