@@ -204,6 +204,7 @@ int build_embedded_tables(fgpu_batch* b) {
       A.out_mode = OUT_RHS;
       A.out = h->buf[2 + m - 1];
       set_fnext(h, A, m, 0.0, &c->d_att);
+      if (m == M && h->fuse_end) set_last_stage(h, A, P, 0.0);
       A.gate = ACT_ATTEMPT;
       A.kchunk = h->kchunk;
       eargs[(size_t)(m - 2) * n + i] = A;
@@ -280,12 +281,14 @@ int enqueue_batch_slot(fgpu_batch* b) {
       if (int rc = launch_batched_form(b, b->d_fargs + (size_t)(m - 2) * n)) return rc;
     if (int rc = launch_batched_stage(b, b->d_eargs + (size_t)(m - 2) * n, b->variant)) return rc;
   }
-  switch (b->m[0]->V) {
-    case 3: batched_combine_kernel<3><<<b->ncblocks, 256, 0, b->stream>>>(b->d_cargs, b->d_cblocks); break;
-    case 4: batched_combine_kernel<4><<<b->ncblocks, 256, 0, b->stream>>>(b->d_cargs, b->d_cblocks); break;
-    default: batched_combine_kernel<5><<<b->ncblocks, 256, 0, b->stream>>>(b->d_cargs, b->d_cblocks); break;
+  if (!b->m[0]->fuse_end) {
+    switch (b->m[0]->V) {
+      case 3: batched_combine_kernel<3><<<b->ncblocks, 256, 0, b->stream>>>(b->d_cargs, b->d_cblocks); break;
+      case 4: batched_combine_kernel<4><<<b->ncblocks, 256, 0, b->stream>>>(b->d_cargs, b->d_cblocks); break;
+      default: batched_combine_kernel<5><<<b->ncblocks, 256, 0, b->stream>>>(b->d_cargs, b->d_cblocks); break;
+    }
+    BCUDA_TRY(b, cudaGetLastError());
   }
-  BCUDA_TRY(b, cudaGetLastError());
   bt_decide_batch_kernel<<<mb, 128, 0, b->stream>>>(b->d_ctlp, b->d_btp, n);
   BCUDA_TRY(b, cudaGetLastError());
   if (int rc = launch_batched_stage(b, b->d_eargs + (size_t)(M - 1) * n, b->variant)) return rc;
@@ -428,7 +431,8 @@ int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
     if (h->butcher) {
       if (h->adaptive_me) return fail(FGPU_EUNSUPPORTED, "embedded batch members use a Butcher tableau (not the adaptive modified Euler scheme)");
       if (!h->materialize) return fail(FGPU_EUNSUPPORTED, "embedded batch members need the formed stage states");
-      if (h->fuse_form != h0->fuse_form) return fail(FGPU_EBADCFG, "embedded batch members differ in stage-state formation");
+      if (h->fuse_form != h0->fuse_form || h->fuse_end != h0->fuse_end)
+        return fail(FGPU_EBADCFG, "embedded batch members differ in stage-state formation");
       if (h->cfg.method != h0->cfg.method || h->T.m != h0->T.m || h->T.order != h0->T.order)
         return fail(FGPU_EBADCFG, "embedded batch members differ in method or order");
     }
@@ -677,7 +681,8 @@ int fgpu_autotune(fgpu_handle* h, int reps, int* variant) {
   int bv = h->variant, bk = h->kchunk;
   const int keep = h->variant, keepk = h->kchunk;
   for (int v : cand) {
-    if (v == 1 && (h->fargo || h->accrete || h->vis)) continue;   // layout 1 lacks these features
+    // layout 1 lacks these features (Butcher steps gate their stages or form the next stage's state)
+    if (v == 1 && (h->fargo || h->accrete || h->vis || h->butcher)) continue;
     for (int kc : chunks) {
       h->variant = v;
       h->kchunk = kc;

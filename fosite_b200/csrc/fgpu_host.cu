@@ -157,6 +157,7 @@ struct fgpu_handle {
   bool adaptive_me = false;     // modified Euler with embedded error control (tol_rel < 1)
   bool materialize = true;      // Butcher stages: form the stage's reconstruction variables once per cell
   bool fuse_form = true;        // ... stage m's kernel forms stage m+1's (buffers alternate), only stage 2 by form_kernel
+  bool fuse_end = true;         // the last stage's kernel also forms the high/low-order solutions and the error norm
   double* d_ready = nullptr;    // ... into this array (one state)
   int variant = 0;              // stage kernel layout: 0 shared-memory tile, 1 warp-shuffle window,
                                 // 2/3 tile with a register cap for more resident blocks, 4 taller tile
@@ -460,8 +461,9 @@ int launch_stage_t(fgpu_handle* h, StageArgs& A) {
   const Grid& g = h->g;
   const int kz = ND == 3 ? (g.nz + h->kchunk - 1) / h->kchunk : 1;
   // the warp-shuffle layout implements neither FARGO frame changes, the accretion rows, the
-  // viscous source nor the device-clock gates
-  const int variant = (h->variant == 1 && (h->fargo || h->accrete || h->vis || A.gate)) ? 0 : h->variant;
+  // viscous source, the device-clock gates nor the next Butcher stage's state formation
+  const int variant =
+      (h->variant == 1 && (h->fargo || h->accrete || h->vis || A.gate || A.fnext_out)) ? 0 : h->variant;
   switch (variant) {
     case 1: {
       // warp-shuffle layout: 32 x 8 points per block, 30 x 6 output cells
@@ -744,6 +746,20 @@ void set_fnext(const fgpu_handle* h, StageArgs& A, int m, double dtv, const doub
   }
   S.dt_dev = dt_dev;
   A.fnext_out = stage_rbuf(h, m + 1);
+}
+
+// the last Butcher stage's epilogue: high/low-order solutions (the high one into out_high) and
+// the error norm; weights times dt on the host, or (dtv = 0, device clock) the bare weights
+// that the kernel multiplies by *in.dt_dev
+void set_last_stage(const fgpu_handle* h, StageArgs& A, double* out_high, double dtv) {
+  const Tableau& T = h->T;
+  A.last_stage = 1;
+  A.nstage = T.m;
+  for (int q = 0; q < T.m; ++q) {
+    A.bh_dt[q] = A.in.dt_dev ? T.bh[q] : T.bh[q] * dtv;
+    A.bl_dt[q] = A.in.dt_dev ? T.bl[q] : T.bl[q] * dtv;
+  }
+  A.out_high = out_high;
 }
 
 BndArgs bnd_args(fgpu_handle* h, const double* state, bool roundtrip, int finalize) {
@@ -1131,13 +1147,8 @@ int butcher_attempt(fgpu_handle* h, double t, double dtv, double& err) {
     A.out_mode = OUT_RHS;
     A.out = h->buf[2 + m - 1];
     set_fnext(h, A, m, dtv, nullptr);
-    const bool fused_end = m == T.m && !h->materialize;
-    if (fused_end) {
-      A.last_stage = 1;
-      A.nstage = T.m;
-      for (int q = 0; q < T.m; ++q) { A.bh_dt[q] = T.bh[q] * dtv; A.bl_dt[q] = T.bl[q] * dtv; }
-      A.out_high = P;
-    }
+    const bool fused_end = m == T.m && (!h->materialize || h->fuse_end);
+    if (fused_end) set_last_stage(h, A, P, dtv);
     // timedisc_rkfehlberg.f90:195: ComputeRHS at t + c(m)*dt
     if (int rc = launch_stage(h, A, RhsTime::host(t + T.c[m - 1] * dtv))) return rc;
     if (m == T.m && !fused_end) {
@@ -1399,6 +1410,7 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
     if (const char* e = std::getenv("FGPU_KCHUNK")) { int v = std::atoi(e); if (v > 0) h->kchunk = v; }
     if (const char* e = std::getenv("FGPU_MATERIALIZE")) h->materialize = std::atoi(e) != 0;
     if (const char* e = std::getenv("FGPU_FUSE_FORM")) h->fuse_form = std::atoi(e) != 0;
+    if (const char* e = std::getenv("FGPU_FUSE_END")) h->fuse_end = std::atoi(e) != 0;
     h->fuse_form = h->fuse_form && h->materialize;
   }
   if (!rc) configure_stage_kernels(h->nd, h->euler, h->prim);
@@ -1766,9 +1778,12 @@ static int enqueue_bt_slot(fgpu_handle* h) {
       A.out_mode = OUT_RHS;
       A.out = h->buf[2 + m - 1];
       set_fnext(h, A, m, 0.0, d_att);
+      if (m == T.m && h->fuse_end) set_last_stage(h, A, P, 0.0);
       A.gate = ACT_ATTEMPT;
       if (int rc = launch_stage(h, A, RhsTime::att(T.c[m - 1]))) return rc;
     }
+  }
+  if (h->butcher && !h->fuse_end) {
     CombineArgs Cb;
     std::memset(&Cb, 0, sizeof(Cb));
     Cb.base = base;

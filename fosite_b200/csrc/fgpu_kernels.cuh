@@ -257,15 +257,17 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
 
   for (int k = k0; k < k1; ++k) {
     double divZ[V];
-    if (A.fnext_out && own) {
-      // the stream the epilogue forms the next stage's state from (base and the earlier
-      // stages' k of this cell), fetched into L2 while the plane's stencil runs
+    if ((A.fnext_out || A.last_stage) && own) {
+      // the stream the epilogue combines (base and the earlier stages' k of this cell, for the
+      // next stage's state or the high/low-order solutions), fetched into L2 while the
+      // plane's stencil runs
       const long long pidx = CE::lin(g, i, j, k);
-      const StateRef& S = A.fnext;
+      const StateRef& S = A.fnext_out ? A.fnext : A.in;
+      const int nq = A.fnext_out ? S.nk - 1 : A.nstage - 1;
 #pragma unroll
       for (int v = 0; v < V; ++v) prefetch_l2(S.base + (long long)v * g.n + pidx);
 #pragma unroll 1
-      for (int q = 0; q + 1 < S.nk; ++q)
+      for (int q = 0; q < nq; ++q)
 #pragma unroll
         for (int v = 0; v < V; ++v) prefetch_l2(S.K[q] + (long long)v * g.n + pidx);
     }
@@ -639,23 +641,40 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
       }
       if (A.last_stage) {
         // high/low order solutions and ComputeError (timedisc_rkfehlberg.f90:198-265,
-        // timedisc_base.f90:1012-1053)
+        // timedisc_base.f90:1012-1053); base and the earlier k unrolled to the tableau limit
+        // so that their loads issue together, this stage's k from the registers.  On the
+        // device clock (in.dt_dev) bh_dt/bl_dt hold the weights, multiplied by *dt_dev here.
+        const double* dtd = A.in.dt_dev;
         double hi[V], lo[V];
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-          double b = __ldg(A.in.base + (long long)v * g.n + idx);
-          double h = b, l = b;
-          for (int q = 0; q < A.nstage - 1; ++q) {
-            double kq = __ldg(A.in.K[q] + (long long)v * g.n + idx);
-            l = l - A.bl_dt[q] * kq;
-            h = h - A.bh_dt[q] * kq;
+        for (int v = 0; v < V; ++v) hi[v] = lo[v] = __ldg(A.in.base + (long long)v * g.n + idx);
+#pragma unroll
+        for (int q = 0; q < FGPU_MAXK - 1; ++q) {
+          if (q + 1 < A.nstage) {
+            const double bh = dtd ? A.bh_dt[q] * *dtd : A.bh_dt[q];
+            const double bl = dtd ? A.bl_dt[q] * *dtd : A.bl_dt[q];
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+              const double kq = __ldg(A.in.K[q] + (long long)v * g.n + idx);
+              lo[v] = lo[v] - bl * kq;
+              hi[v] = hi[v] - bh * kq;
+            }
           }
-          l = l - A.bl_dt[A.nstage - 1] * rhs[v];
-          h = h - A.bh_dt[A.nstage - 1] * rhs[v];
-          hi[v] = h;
-          lo[v] = l;
-          A.out_high[(long long)v * g.n + idx] = h;
-          double e = fabs(h - l) / (A.tol_rel * fabs(h) + A.tol_abs[v]);
+        }
+        {
+          const int q = A.nstage - 1;
+          const double bh = dtd ? A.bh_dt[q] * *dtd : A.bh_dt[q];
+          const double bl = dtd ? A.bl_dt[q] * *dtd : A.bl_dt[q];
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            lo[v] = lo[v] - bl * rhs[v];
+            hi[v] = hi[v] - bh * rhs[v];
+          }
+        }
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          A.out_high[(long long)v * g.n + idx] = hi[v];
+          const double e = fabs(hi[v] - lo[v]) / (A.tol_rel * fabs(hi[v]) + A.tol_abs[v]);
           errv = dmax(errv, e);
         }
       }

@@ -118,3 +118,22 @@ def test_fused_stage_state_equals_form_pass(name, host, monkeypatch):
     sa, sb = a.status(), b.status()
     assert (sa.time, sa.dt, sa.iter, sa.n_adj) == (sb.time, sb.dt, sb.iter, sb.n_adj)
     assert np.array_equal(a.get(abi.CVAR), b.get(abi.CVAR))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("host", [False, True])
+def test_butcher_steps_with_shuffle_layout_forced(host, monkeypatch):
+    """With the warp-shuffle stage layout forced (FGPU_STAGE_VARIANT=1), the stages that it
+    cannot run (gated device-clock stages, stages forming the next stage's state) take the
+    base tile: results still equal the oracle's bit for bit."""
+    monkeypatch.setenv("FGPU_STAGE_VARIANT", "1")
+    if host:
+        monkeypatch.setenv("FGPU_BUTCHER_HOST", "1")
+    cfg, o, g = _pair("gauss3d_dopri_mc_prim", exact=True)
+    assert o.first_step() == 0 and g.first_step() == 0
+    for _ in range(4):
+        assert o.step() == 0
+    rc, done = g.run(4)
+    assert rc == 0 and done == 4
+    assert g.status().time == o.status().time
+    assert np.array_equal(g.get(abi.CVAR), o.get(abi.CVAR))
