@@ -92,8 +92,8 @@ struct Oracle {
   int64_t iter = -1, n_adj = 0;
   double last_err = 0;
   int checkflags = 0;
-  // ---- fargo (direction 2) ----
-  int fargo = 0;
+  // ---- fargo (direction 1: transport along x, w by (j,k); direction 2: along y, w by (i,k)) ----
+  int fargo = 0, fdir = 2;
   std::vector<double> w, wfactor, delxy, fdq, fdql, fflux;
   std::vector<int> shift;
   bool c_trans = false, p_trans = false;     // fargo_transformation_applied flags
@@ -199,19 +199,32 @@ struct Oracle {
       // (shearing box) needs the shearing-box sources
       if (fargo != 1 && fargo != 2) { err = "fargo: types 1 and 2 only"; return FGPU_EUNSUPPORTED; }
       if (euler && (cfg.checkdata & FGPU_CHECK_PMIN)) { err = "fargo with ideal-gas physics: checkdata without CHECK_PMIN"; return FGPU_EUNSUPPORTED; }
-      if (cfg.fargo_direction != 2 || NDIMS < 2) { err = "fargo: only direction 2 supported"; return FGPU_EUNSUPPORTED; }
+      if ((cfg.fargo_direction != 1 && cfg.fargo_direction != 2) || NDIMS < 2) { err = "fargo: directions 1 and 2 only"; return FGPU_EUNSUPPORTED; }
       if (NDIMS != 2 || dirs[0] != 0 || dirs[1] != 1) { err = "fargo: 2D x-y meshes only"; return FGPU_EUNSUPPORTED; }
-      w.assign((long)NI * NK, 0.0); wfactor.assign((long)NI * NK, 0.0); delxy.assign((long)NI * NK, 0.0);
-      shift.assign((long)NI * NK, 0);
+      fdir = cfg.fargo_direction;
+      if (fdir == 1 && outbound) { err = "fargo along x with point-mass accretion"; return FGPU_EUNSUPPORTED; }
+      const long nw = (long)(fdir == 1 ? NJ : NI) * NK;   // timedisc_base.f90:377-403
+      w.assign(nw, 0.0); wfactor.assign(nw, 0.0); delxy.assign(nw, 0.0);
+      shift.assign(nw, 0);
       fdq.assign(NC, 0.0); fdql.assign(NC, 0.0); fflux.assign(NC, 0.0);
-      if (fargo == 1) {
-        for (int k = KGMIN; k <= KGMAX; ++k)
-          for (int i = IGMIN; i <= IGMAX; ++i) {
-            long c0 = id(i, JMIN, k);
-            double a = fmin2(hfy[c0 * 6 + 0], hfy[c0 * 6 + 1]);
-            double b = fmin2(hfy[c0 * 6 + 4], hfy[c0 * 6 + 5]);
-            wfactor[(i - IGMIN) + (long)NI * (k - KGMIN)] = fmin2(a, b) / hcy[c0];
-          }
+      if (fargo == 1) {   // timedisc_base.f90:428-452
+        if (fdir == 1) {
+          for (int k = KGMIN; k <= KGMAX; ++k)
+            for (int j = JGMIN; j <= JGMAX; ++j) {
+              long c0 = id(IMIN, j, k);
+              double a = fmin2(hfx[c0 * 6 + 2], hfx[c0 * 6 + 3]);
+              double b = fmin2(hfx[c0 * 6 + 4], hfx[c0 * 6 + 5]);
+              wfactor[widx(j, k)] = fmin2(a, b) / hcx[c0];
+            }
+        } else {
+          for (int k = KGMIN; k <= KGMAX; ++k)
+            for (int i = IGMIN; i <= IGMAX; ++i) {
+              long c0 = id(i, JMIN, k);
+              double a = fmin2(hfy[c0 * 6 + 0], hfy[c0 * 6 + 1]);
+              double b = fmin2(hfy[c0 * 6 + 4], hfy[c0 * 6 + 5]);
+              wfactor[widx(i, k)] = fmin2(a, b) / hcy[c0];
+            }
+        }
       }
     }
     return FGPU_OK;
@@ -675,16 +688,20 @@ struct Oracle {
     }
   }
 
-  // ---------------------------------------------------------------- fargo (direction 2)
-  // Add/SubtractBackgroundVelocityY: isothermal physics_eulerisotherm.f90:1263-1413,
-  // Euler physics_euler.f90:2003-2047,2159-2203 (the energy first, with the old momentum)
-  long widx(int i, int k) const { return (long)(i - IGMIN) + (long)NI * (k - KGMIN); }
+  // ---------------------------------------------------------------- fargo
+  // Add/SubtractBackgroundVelocityX/Y: isothermal physics_eulerisotherm.f90:1229-1413,
+  // Euler physics_euler.f90:1955-2047,2109-2203 (the energy first, with the old momentum)
+  // w index of a (j,k) row (direction 1) or an (i,k) column (direction 2)
+  long widx(int a, int k) const {
+    return fdir == 1 ? (long)(a - JGMIN) + (long)NJ * (k - KGMIN) : (long)(a - IGMIN) + (long)NI * (k - KGMIN);
+  }
+  double wof(int i, int j, int k) const { return w[widx(fdir == 1 ? j : i, k)]; }
   void add_bg(std::vector<double>& pv, std::vector<double>& cv) {
     if (!c_trans) return;
     if (!p_trans) return;
-    int vi = 2;   // x-y plane: y velocity is component 2 (variable index 2)
+    const int vi = fdir;   // the velocity component along the transport
     for (int k = KGMIN; k <= KGMAX; ++k) for (int j = JGMIN; j <= JGMAX; ++j) for (int i = IGMIN; i <= IGMAX; ++i) {
-      long c = id(i, j, k); double wv = w[widx(i, k)];
+      long c = id(i, j, k); double wv = wof(i, j, k);
       if (euler) cv[c + NC * PRESSURE] = cv[c + NC * PRESSURE] + wv * (cv[c + NC * vi] + 0.5 * cv[c] * wv);
       pv[c + NC * vi] = pv[c + NC * vi] + wv;
       cv[c + NC * vi] = cv[c + NC * vi] + cv[c] * wv;
@@ -694,18 +711,27 @@ struct Oracle {
   void sub_bg(std::vector<double>& pv, std::vector<double>& cv) {
     if (c_trans) return;
     if (p_trans) return;
-    int vi = 2;
+    const int vi = fdir;
     for (int k = KGMIN; k <= KGMAX; ++k) for (int j = JGMIN; j <= JGMAX; ++j) for (int i = IGMIN; i <= IGMAX; ++i) {
-      long c = id(i, j, k); double wv = w[widx(i, k)];
+      long c = id(i, j, k); double wv = wof(i, j, k);
       if (euler) cv[c + NC * PRESSURE] = cv[c + NC * PRESSURE] - wv * (cv[c + NC * vi] - 0.5 * cv[c] * wv);
       pv[c + NC * vi] = pv[c + NC * vi] - wv;
       cv[c + NC * vi] = cv[c + NC * vi] - cv[c] * wv;
     }
     c_trans = true; p_trans = true;
   }
-  // timedisc_base.f90:2243-2326 CalcBackgroundVelocity (direction 2)
+  // timedisc_base.f90:2243-2326 CalcBackgroundVelocity
   void calc_background_velocity(std::vector<double>& pv, std::vector<double>& cv) {
     add_bg(pv, cv);
+    if (fdir == 1) {
+      for (int k = KGMIN; k <= KGMAX; ++k) for (int j = JGMIN; j <= JGMAX; ++j) {
+        double wf = wfactor[widx(j, k)];
+        double wi = 0.0;
+        for (int i = IMIN; i <= IMAX; ++i) wi = wi + pv[id(i, j, k) + NC * 1] * wf;
+        w[widx(j, k)] = wi / INUM;
+      }
+      return;
+    }
     for (int k = KGMIN; k <= KGMAX; ++k) for (int i = IGMIN; i <= IGMAX; ++i) {
       double wf = wfactor[widx(i, k)];
       double wi = 0.0;
@@ -713,13 +739,24 @@ struct Oracle {
       w[widx(i, k)] = wi / JNUM;
     }
   }
-  // AddFargoSourcesY (x-y momentum): isothermal physics_eulerisotherm.f90:1531-1586;
-  // Euler physics_euler.f90:2368-2455 adds the energy term -vy*(tmp + GetGeometricalSourceY
-  // with vz = P = mz = 0), physics_euler.f90:3139-3147
+  // AddFargoSourcesX/Y (x-y momentum): isothermal physics_eulerisotherm.f90:1462-1518,1531-1586;
+  // Euler physics_euler.f90:2267-2355,2368-2455 add the energy term -v*(tmp + GetGeometricalSource
+  // with vz = P = mz = 0), physics_euler.f90:3128-3147
   void add_fargo_sources(std::vector<double>& pv, std::vector<double>& cv, std::vector<double>& sterm) {
     for (int k = KMIN; k <= KMAX; ++k) for (int j = JMIN; j <= JMAX; ++j) for (int i = IMIN; i <= IMAX; ++i) {
       long c = id(i, j, k);
-      if (!euler) {
+      if (fdir == 1) {
+        if (!euler) {
+          sterm[c + NC * 1] = sterm[c + NC * 1] - cv[c + NC * 2] * 0.5 * (w[widx(j + 1, k)] - w[widx(j - 1, k)]) / dly[c];
+        } else {
+          double tmp = cv[c + NC * 2] * 0.5 * (w[widx(j + 1, k)] - w[widx(j - 1, k)]) / dly[c];
+          sterm[c + NC * 1] = sterm[c + NC * 1] - tmp;
+          double vx = pv[c + NC * 1], vy = pv[c + NC * 2], my = cv[c + NC * 2];
+          double g = my * (cyxy[c] * vy - cxyx[c] * vx) + 0.0 * (czxz[c] * 0.0 - cxzx[c] * vx) + (cyxy[c] + czxz[c]) * 0.0;
+          tmp = tmp + g;
+          sterm[c + NC * PRESSURE] = sterm[c + NC * PRESSURE] - vx * tmp;
+        }
+      } else if (!euler) {
         sterm[c + NC * 2] = sterm[c + NC * 2] - cv[c + NC * 1] * 0.5 * (w[widx(i + 1, k)] - w[widx(i - 1, k)]) / dlx[c];
       } else {
         double tmp = cv[c + NC * 1] * 0.5 * (w[widx(i + 1, k)] - w[widx(i - 1, k)]) / dlx[c];
@@ -730,6 +767,47 @@ struct Oracle {
         sterm[c + NC * PRESSURE] = sterm[c + NC * PRESSURE] - vy * tmp;
       }
     }
+  }
+  // timedisc_base.f90:1779-1914 FargoAdvectionX
+  void fargo_advection_x() {
+    for (int k = KGMIN; k <= KGMAX; ++k) for (int j = JGMIN; j <= JGMAX; ++j)
+      delxy[widx(j, k)] = w[widx(j, k)] * dt / dlx[id(IMIN, j, k)];
+    for (int k = KGMIN; k <= KGMAX; ++k) for (int j = JGMIN; j <= JGMAX; ++j) {
+      double d = delxy[widx(j, k)];
+      int s = (int)std::lround(d);   // NINT: round half away from zero
+      shift[widx(j, k)] = s;
+      delxy[widx(j, k)] = d - (double)s;
+    }
+    for (int l = 0; l < VNUM; ++l) {
+      for (int k = KGMIN; k <= KGMAX; ++k) for (int j = JGMIN; j <= JGMAX; ++j)
+        fdq[id(IGMIN, j, k)] = cvar[id(IGMIN + 1, j, k) + NC * l] - cvar[id(IGMIN, j, k) + NC * l];
+      for (int i = IGMIN + 1; i <= IGMAX - 1; ++i)
+        for (int k = KGMIN; k <= KGMAX; ++k) for (int j = JGMIN; j <= JGMAX; ++j) {
+          fdq[id(i, j, k)] = cvar[id(i + 1, j, k) + NC * l] - cvar[id(i, j, k) + NC * l];
+          double a = fdq[id(i - 1, j, k)], b = fdq[id(i, j, k)];
+          if (fsign(1.0, a) * fsign(1.0, b) > 0.) fdql[id(i, j, k)] = fsign(fmin2(std::fabs(a), std::fabs(b)), a);
+          else fdql[id(i, j, k)] = 0.;
+        }
+      for (int i = IMIN - 1; i <= IMAX; ++i)
+        for (int k = KGMIN; k <= KGMAX; ++k) for (int j = JGMIN; j <= JGMAX; ++j) {
+          double d = delxy[widx(j, k)];
+          long c = id(i, j, k);
+          if (d > 0.) fflux[c] = cvar[c + NC * l] + .5 * fdql[c] * (1. - d);
+          else fflux[c] = cvar[id(i + 1, j, k) + NC * l] - .5 * fdql[id(i + 1, j, k)] * (1. + d);
+          cvar[c + NC * l] = cvar[c + NC * l] - d * (fflux[c] - fflux[id(i - 1, j, k)]);
+        }
+    }
+    std::vector<double> row(INUM);
+    for (int l = 0; l < VNUM; ++l)
+      for (int k = KGMIN; k <= KGMAX; ++k) for (int j = JGMIN; j <= JGMAX; ++j) {
+        int s = shift[widx(j, k)];
+        for (int i = 0; i < INUM; ++i) row[i] = cvar[id(IMIN + i, j, k) + NC * l];
+        for (int i = 0; i < INUM; ++i) {
+          // CSHIFT(a, -s): result(i) = a(i - s) (circular)
+          int src = ((i - s) % INUM + INUM) % INUM;
+          cvar[id(IMIN + i, j, k) + NC * l] = row[src];
+        }
+      }
   }
   // timedisc_base.f90:1935-2069 FargoAdvectionY
   void fargo_advection_y() {
@@ -1432,7 +1510,8 @@ struct Oracle {
       dtold = d;
       if (fargo) {
         center_boundary(pvar, cvar);
-        fargo_advection_y();
+        if (fdir == 1) fargo_advection_x();
+        else fargo_advection_y();
         c2p_range(cvar, pvar, IGMIN, IGMAX, JGMIN, JGMAX, KGMIN, KGMAX);
         p_trans = c_trans;
         compute_rhs(time, pvar, cvar, checkdatabm, rhs);
@@ -1505,6 +1584,7 @@ int orc_set_sound_speeds(orc_handle* h, const double* bcc, const double* fcs) {
   return 0;
 }
 // Timedisc%w of FARGO type 2 (user supplied, timedisc_base.f90:421-424), by padded i
+// (direction 2) or padded j (direction 1)
 int orc_set_fargo_velocity(orc_handle* h, const double* w, int64_t n) {
   Oracle& o = h->o;
   if (o.fargo != 2 || n < (int64_t)o.w.size()) return FGPU_EARG;

@@ -265,6 +265,35 @@ def khi_reynolds(re=1.0e4, rho0=1.0, xyzlen=1.0, v0=-0.5, v1=0.5):
     return abs(rho0 * xyzlen * (v0 - v1) / re)
 
 
+def khi_fargo(fargo, direction=1, n=(24, 24), visc=False, seed=11):
+    """tests/KHI2D.f90's FARGO legs (:81-150, config :168-245, InitData :300-360): ideal-gas KHI,
+    KT + MONOCENT (theta 1.2) on conservative variables, periodic box, FARGO type 1 or 2 along
+    x (direction 1: shear layer along x, bands in y) or, for the transposed run, along y
+    (direction 2: everything transposed), optionally with the test's molecular viscosity.
+    Type 2 takes the band velocity as background velocity (InitData :323-331); CHECK_PMIN off
+    (its round trip sits between the frame changes)."""
+    cfg, p, extra = _khi(n=n, limiter=abi.MONOCENT, theta=1.2, seed=seed)
+    cfg.fargo_method = fargo
+    cfg.fargo_direction = 1
+    cfg.checkdata = abi.CHECK_ALL & ~abi.CHECK_PMIN
+    if visc:
+        eta = khi_reynolds()
+        cfg, p, extra = _visc((cfg, p, extra), eta, bulkconst=-2. / 3. * eta)
+    # background velocity by padded j: the band velocity at the padded cell centres
+    dy = (cfg.ymax - cfg.ymin) / cfg.jnum
+    y = cfg.ymin + (np.arange(cfg.jnum + 4) - 1.5) * dy
+    w = np.where(np.abs(y) < 0.25, 0.5, -0.5)
+    if fargo == 2:
+        extra = dict(extra, fargo_w=w)
+    if direction == 2:
+        cfg.inum, cfg.jnum = cfg.jnum, cfg.inum
+        cfg.xmin, cfg.xmax, cfg.ymin, cfg.ymax = cfg.ymin, cfg.ymax, cfg.xmin, cfg.xmax
+        cfg.fargo_direction = 2
+        abi.finalize_config(cfg)
+        p = np.stack([p[0], p[2], p[1], p[3]]).transpose(0, 1, 3, 2).copy()
+    return cfg, p, extra
+
+
 def _with(case, **kw):
     c, p, extra = case
     for k, v in kw.items():

@@ -47,6 +47,21 @@ def test_khi_transposition_symmetry_exact():
     assert a.status().dt == b.status().dt
 
 
+@pytest.mark.parametrize("visc", [False, True])
+@pytest.mark.parametrize("fargo", [1, 2])
+def test_khi_fargo_transposition_symmetry_exact(fargo, visc):
+    """tests/KHI2D.f90:81-150, the FARGO legs: FARGO type 1 or 2 along x and the transposed
+    run with FARGO along y agree to TINY (with and without the test's viscosity)."""
+    from cases import khi_fargo
+    ca, pa, ea = khi_fargo(fargo, direction=1, visc=visc)
+    cb, pb, eb = khi_fargo(fargo, direction=2, visc=visc)
+    a = _run(ca, pa, 15, ea)
+    b = _run(cb, pb, 15, eb)
+    ra, rb = a.get(abi.PVAR), _swap_xy(b.get(abi.PVAR))
+    assert np.sqrt(np.mean((ra - rb) ** 2)) < abi.TINY
+    assert a.status().dt == b.status().dt and a.status().time == b.status().time
+
+
 def test_khi_conservation_periodic():
     cfg, p, _ = _khi(n=(32, 28))
     o = pyoracle.Oracle(cfg)
