@@ -28,7 +28,12 @@ struct Grid {
   int nx, ny, nz;      // interior cells (nz = 1 in 2D)
   long long n;         // nx*ny*nz
   int bc[6];           // boundary type per face (W,E,S,N,B,T)
+  int fdir;            // FARGO transport direction: 1 along x (w by padded j), 2 along y (w by padded i)
 };
+
+// FARGO: index of a cell's background velocity (padded j for transport along x, padded i
+// along y); the transported momentum is component fdir of the state (1 x, 2 y)
+__device__ __forceinline__ int fargo_ix(const Grid& g, int i, int j) { return (g.fdir == 1 ? j : i) + 2; }
 
 struct MetricP {
   const double *dAxW, *dAyS, *dAzB;          // face area factors (dAxdydz(i,W) ...)
@@ -47,15 +52,16 @@ struct MetricP {
   double vis_eta;                            // its constant dynamic viscosity
 };
 
-// A sequence of FARGO frame changes of the y momentum, m_y = m_y + s_q*(rho*w_q(i)),
-// applied in order.  It reproduces the in-place Add/SubtractBackgroundVelocityY
-// calls (physics_eulerisotherm.f90:1263-1413) that IntegrationStep and ComputeRHS
-// make on cvar (timedisc_base.f90:662-674, 1096-1110, 1190-1208): every stored
-// state is kept untransformed and the transforms are replayed pointwise where
-// the state is read, so the rounding of each in-place update is reproduced.
+// A sequence of FARGO frame changes of the momentum along the transport,
+// m = m + s_q*(rho*w_q), applied in order.  It reproduces the in-place
+// Add/SubtractBackgroundVelocityX/Y calls (physics_eulerisotherm.f90:1229-1413)
+// that IntegrationStep and ComputeRHS make on cvar (timedisc_base.f90:662-674,
+// 1096-1121, 1190-1208): every stored state is kept untransformed and the
+// transforms are replayed pointwise where the state is read, so the rounding of
+// each in-place update is reproduced.
 struct Chain {
   int n;
-  const double* w[4];   // background velocity by padded i
+  const double* w[4];   // background velocity by fargo_ix
   double s[4];          // +1 add, -1 subtract
   int rt;               // k > 0: the CHECK_PMIN round trip P2C(MAX(C2P(c),pmin)) before element k-1
                         // (k = n+1: after the last); 0: none
@@ -85,25 +91,35 @@ struct StateRef {
 // the energy (V = 4, ideal gas) the energy goes first, with the old momentum:
 // E + s*w*(m + s*rho*w/2), then m + s*rho*w (physics_euler.f90:2003-2047, 2159-2203);
 // multiplying by s = +-1 is exact, so both signs round like the reference's two forms.
+// The momentum component is fdir (1 x, 2 y), selected without indexing the array.
 template <int V>
-__device__ __forceinline__ void frame_change(double* c, double s, double w) {
-  if (V == 4) c[3] = c[3] + s * (w * (c[2] + s * (0.5 * c[0] * w)));
-  c[2] = c[2] + s * (c[0] * w);
+__device__ __forceinline__ void frame_change(double* c, double s, double w, int fdir) {
+  const double m = fdir == 1 ? c[1] : c[2];
+  if (V == 4) c[3] = c[3] + s * (w * (m + s * (0.5 * c[0] * w)));
+  const double mn = m + s * (c[0] * w);
+  if (fdir == 1) c[1] = mn;
+  else c[2] = mn;
 }
-// apply a frame-change chain to the conservative state c of a cell in padded column ip
-// (rt_fn performs the round trip on c when the chain has one)
+// the velocity component along the transport of a primitive state, minus w
+__device__ __forceinline__ void sub_velocity(double* p, double w, int fdir) {
+  if (fdir == 1) p[1] = p[1] - w;
+  else p[2] = p[2] - w;
+}
+// apply a frame-change chain to the conservative state c of cell (i, j) (0-based interior
+// coordinates; rt_fn performs the round trip on c when the chain has one)
 template <int V, class RT>
-__device__ __forceinline__ void apply_chain(const Chain& C, double* c, int ip, RT&& rt_fn) {
+__device__ __forceinline__ void apply_chain(const Chain& C, double* c, const Grid& g, int i, int j, RT&& rt_fn) {
+  const int ix = fargo_ix(g, i, j);
   for (int q = 0; q < C.n; ++q) {
     if (C.rt == q + 1) rt_fn(c);
-    frame_change<V>(c, C.s[q], C.w[q][ip]);
+    frame_change<V>(c, C.s[q], C.w[q][ix], g.fdir);
   }
   if (C.rt == C.n + 1) rt_fn(c);
 }
 // chains without a round trip (the frame of a stage input)
 template <int V>
-__device__ __forceinline__ void apply_chain(const Chain& C, double* c, int ip) {
-  apply_chain<V>(C, c, ip, [](double*) {});
+__device__ __forceinline__ void apply_chain(const Chain& C, double* c, const Grid& g, int i, int j) {
+  apply_chain<V>(C, c, g, i, j, [](double*) {});
 }
 
 // Device control block for device-resident stepping.
@@ -295,7 +311,7 @@ struct Cells {
       for (int l = 0; l < V; ++l) p[l] = u[l];
       return;
     }
-    if (ND == 2 && S.pre.n) apply_chain<V>(S.pre, u, i + 2);
+    if (ND == 2 && S.pre.n) apply_chain<V>(S.pre, u, g, i, j);
     PH::c2p(u, p, P);
   }
 

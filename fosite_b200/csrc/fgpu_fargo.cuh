@@ -1,8 +1,8 @@
-// fgpu_fargo.cuh -- FARGO transport along y (fosite fargo type 1, 2D x-y
-// meshes, isothermal physics): the background velocity w(i) of
+// fgpu_fargo.cuh -- FARGO transport (fosite fargo types 1 and 2, 2D x-y meshes)
+// along y (direction 2) or x (direction 1): the background velocity of
 // CalcBackgroundVelocity and the shift + upwind residual advection of
-// FargoAdvectionY, with the CFL / CheckData pass of the step's closing
-// ComputeRHS + CalcTimestep fused into the advection.
+// FargoAdvectionY / FargoAdvectionX, with the CFL / CheckData pass of the
+// step's closing ComputeRHS + CalcTimestep fused into the advection.
 #pragma once
 #include "fgpu_kernels.cuh"
 
@@ -14,8 +14,8 @@ struct FargoWArgs {
   MetricP mt;
   StateRef in;            // state whose real frame is in + in.pre
   const double* w_prev;   // background velocity of the last ComputeRHS (pvar round trip), or null
-  const double* wfac;     // wfactor(i), by padded i
-  double* w_out;          // new background velocity, by padded i
+  const double* wfac;     // wfactor, by padded i (direction 2) or padded j (direction 1)
+  double* w_out;          // new background velocity, indexed like wfac
   Ctl* ctl;
 };
 
@@ -68,12 +68,55 @@ __global__ void __launch_bounds__(FW_WX* FW_WY) fargo_w_kernel(const __grid_cons
   if (ty == 0 && valid) A.w_out[ip] = wi / (double)g.ny;
 }
 
+// CalcBackgroundVelocity for direction 1 (timedisc_base.f90:2262-2282):
+//   w(j) = SUM_i pvar(i,j,vx)*wfactor(j) / INUM over the interior i, for every padded row j
+// (the y-ghost rows come from the boundary fill), with vx = (vx - w_prev) + w_prev as for
+// direction 2.  A block owns FX_WY rows; per chunk of FX_WX columns its threads evaluate the
+// terms in parallel into shared memory (coalesced along x), then one thread per row adds
+// them in i order, so the sum rounds like the reference loop.
+constexpr int FX_WX = 32, FX_WY = 8;
+template <bool EU>
+__global__ void __launch_bounds__(FX_WX* FX_WY) fargo_w_x_kernel(const __grid_constant__ FargoWArgs A) {
+  using CE = Cells<2, EU>;
+  __shared__ double terms[FX_WY][FX_WX + 1];
+  if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
+  const Grid& g = A.g;
+  const int tx = threadIdx.x % FX_WX, ty = threadIdx.x / FX_WX;
+  const int jp = blockIdx.x * FX_WY + ty;
+  const bool valid = jp < g.ny + 4;
+  const int j = jp - 2;
+  const bool ghost = j < 0 || j >= g.ny;
+  const double wf = valid ? A.wfac[jp] : 0.0;
+  const double wp = (valid && A.w_prev) ? A.w_prev[jp] : 0.0;
+  double wi = 0.0;
+  for (int i0 = 0; i0 < g.nx; i0 += FX_WX) {
+    const int i = i0 + tx;
+    double t = 0.0;
+    if (valid && i < g.nx) {
+      double p[Phys<2, EU>::V];
+      if (ghost) CE::face_ghost_p(A.in, g, A.ph, A.mt, 1, i, j, 0, p);
+      else CE::interior_p(A.in, g, A.ph, i, j, 0, p);
+      double vx = p[1];
+      if (A.w_prev) vx = (vx - wp) + wp;
+      t = vx * wf;
+    }
+    terms[ty][tx] = t;
+    __syncthreads();
+    if (tx == 0 && valid) {
+      const int nq = min(FX_WX, g.nx - i0);
+      for (int q = 0; q < nq; ++q) wi = wi + terms[ty][q];
+    }
+    __syncthreads();
+  }
+  if (tx == 0 && valid) A.w_out[jp] = wi / (double)g.nx;
+}
+
 struct FargoAdvArgs {
   Grid g;
   PhysP ph;
   MetricP mt;
   StateRef in;           // co-moving state after the last stage (no frame changes)
-  const double* w;       // background velocity, by padded i
+  const double* w;       // background velocity, by padded i (direction 2) or padded j (direction 1)
   double* out;           // advected state (must not alias in.base)
   Ctl* ctl;              // dt/time source and CFL / CheckData sink
   int checkdata;
@@ -163,7 +206,7 @@ __global__ void __launch_bounds__(TX* TY) fargo_advect_kernel(const __grid_const
       double c[V], p[V];
 #pragma unroll
       for (int v = 0; v < V; ++v) c[v] = u[v];
-      frame_change<V>(c, 1.0, w);
+      frame_change<V>(c, 1.0, w, 2);
       PH::c2p(c, p, P);
       const double csc = EU ? PH::cs_of(p, P) : cs;
       if ((A.checkdata & 0x01) && !(csc > 0.)) flags |= 0x01;
@@ -184,6 +227,90 @@ __global__ void __launch_bounds__(TX* TY) fargo_advect_kernel(const __grid_const
   }
   double vals[4] = {cflv, 0.0, 0.0, cflvis};
   block_reduce_emit<NT>(vals, M.vis ? 4 : 1, flags, A.ctl->invdt, &A.ctl->flags, sred);
+}
+
+// FargoAdvectionX (timedisc_base.f90:1779-1914) for the interior cells, the same transport
+// along x with w(j): delxy = w*dt/dlx(IMIN), shift = NINT(delxy), delxy -= shift; the
+// minmod-limited upwind residual step over i, then CSHIFT(q, -shift) over the interior
+// columns.  The x ghosts of the input come from the boundary fill of the co-moving state.
+// One thread per cell reads its five-cell window along x (adjacent threads, adjacent i) and
+// writes the result to its shifted column; the closing ComputeRHS's CheckData and
+// CalcTimestep see that cell at the shifted column (its metric and sound speed).
+template <bool EU>
+__global__ void __launch_bounds__(256) fargo_advect_x_kernel(const __grid_constant__ FargoAdvArgs A) {
+  using PH = Phys<2, EU>;
+  using CE = Cells<2, EU>;
+  constexpr int V = PH::V;
+  __shared__ double sred[RED_STRIDE * 8];
+  if (A.ctl->stop | A.ctl->brk) return;
+  const Grid& g = A.g;
+  const PhysP& P = A.ph;
+  const MetricP& M = A.mt;
+  double cflv = 0.0, cflvis = 0.0;
+  int flags = 0;
+  const double dte = (A.ctl->time + A.ctl->dt) - A.ctl->time;
+  const double dlx0 = M.dlx[2];   // dlx(IMIN, j): the metric depends on i only
+  for (long long t = blockIdx.x * 256LL + threadIdx.x; t < g.n; t += (long long)gridDim.x * 256) {
+    const int i = (int)(t % g.nx), j = (int)(t / g.nx);
+    const double w = A.w[j + 2];
+    double d = w * dte / dlx0;
+    const double sh = round(d);   // NINT: half away from zero
+    const int s = (int)sh;
+    d = d - (double)s;
+    auto load = [&](int ii, double* c) {
+      if (ii >= 0 && ii < g.nx) {
+        state_at<V>(A.in, g.n, CE::lin(g, ii, j, 0), c);
+      } else {
+        double p[V];
+        CE::face_ghost_p(A.in, g, P, M, 0, ii, j, 0, p);
+        PH::p2c(p, c, P);
+      }
+    };
+    double q[5][V];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) load(i - 2 + r, q[r]);
+    double u[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      double a0 = q[1][v] - q[0][v], a1 = q[2][v] - q[1][v];
+      double a2 = q[3][v] - q[2][v], a3 = q[4][v] - q[3][v];
+      double fl, fr;   // flux(i-1), flux(i)
+      if (d > 0.) {
+        fl = q[1][v] + .5 * fargo_minmod(a0, a1) * (1. - d);
+        fr = q[2][v] + .5 * fargo_minmod(a1, a2) * (1. - d);
+      } else {
+        fl = q[2][v] - .5 * fargo_minmod(a1, a2) * (1. + d);
+        fr = q[3][v] - .5 * fargo_minmod(a2, a3) * (1. + d);
+      }
+      u[v] = q[2][v] - d * (fr - fl);
+    }
+    int id = (i + s) % g.nx;
+    if (id < 0) id += g.nx;
+    const long long o = CE::lin(g, id, j, 0);
+#pragma unroll
+    for (int v = 0; v < V; ++v) A.out[(long long)v * g.n + o] = u[v];
+    // closing ComputeRHS: AddBackgroundVelocityX, CenterBoundary's Cons2Prim, CheckData;
+    // CalcTimestep on the co-moving primitive state, at the cell's new column
+    const int ipd = id + 2;
+    double c[V], p[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) c[v] = u[v];
+    frame_change<V>(c, 1.0, w, 1);
+    PH::c2p(c, p, P);
+    const double csc = EU ? PH::cs_of(p, P) : M.cs[ipd];
+    if ((A.checkdata & 0x01) && !(csc > 0.)) flags |= 0x01;
+    if (EU && (A.checkdata & 0x02) && p[V - 1] < P.pmin) flags |= 0x02;
+    if ((A.checkdata & 0x04) && p[0] < P.rhomin) flags |= 0x04;
+    if (A.checkdata & 0x08)
+      for (int v = 0; v < V; ++v) if (!isfinite(p[v]) || !isfinite(c[v])) flags |= 0x08;
+    p[1] = p[1] - w;
+    double v3[4];
+    CE::cfl_cell(p, csc, M, ipd, v3);
+    cflv = dmax(cflv, v3[0]);
+    cflvis = dmax(cflvis, v3[3]);
+  }
+  double vals[4] = {cflv, 0.0, 0.0, cflvis};
+  block_reduce_emit<256>(vals, M.vis ? 4 : 1, flags, A.ctl->invdt, &A.ctl->flags, sred);
 }
 
 }  // namespace fgpu

@@ -173,7 +173,9 @@ struct fgpu_handle {
   // FirstStep's real-frame cvar); 2: after a step (the stored state is the
   // transported state, w the background velocity of its closing ComputeRHS)
   bool fargo = false;
-  double* d_w = nullptr;
+  int fdir = 2;                 // transport along x (1, w by padded j) or y (2, w by padded i)
+  int nw = 0;                   // padded length of w along the other direction
+  double* d_w = nullptr;        // [w | w_new | wfactor of direction 1]
   int fargo_phase = 0;
   // point-mass accretion: d_acc = [bx (ny) | bxold (ny) | brow (ny) | mass, mdot]
   bool accrete = false;
@@ -896,7 +898,9 @@ Chain chain_none() {
 Chain fargo_pre(const fgpu_handle* h) {
   return h->fargo_phase == 2 ? chain_add(chain_none(), h->d_w, 1.0) : chain_none();
 }
-const double* fargo_wfac(const fgpu_handle* h) { return h->d_metric + (size_t)M_wfac * h->nxp; }
+const double* fargo_wfac(const fgpu_handle* h) {
+  return h->fdir == 1 ? h->d_w + 2 * (size_t)h->nw : h->d_metric + (size_t)M_wfac * h->nxp;
+}
 
 int launch_fargo_w(fgpu_handle* h, const StateRef& in, const double* w_prev, double* w_out) {
   FargoWArgs F;
@@ -908,9 +912,15 @@ int launch_fargo_w(fgpu_handle* h, const StateRef& in, const double* w_prev, dou
   F.w_out = w_out;
   F.ctl = h->d_ctl;
   return timed_launch(h, false, 0.0, [&] {
-    unsigned blocks = (unsigned)((h->g.nx + 4 + FW_WX - 1) / FW_WX);
-    if (h->euler) fargo_w_kernel<true><<<blocks, FW_WX * FW_WY, 0, h->stream>>>(F);
-    else fargo_w_kernel<false><<<blocks, FW_WX * FW_WY, 0, h->stream>>>(F);
+    if (h->fdir == 1) {
+      unsigned blocks = (unsigned)((h->g.ny + 4 + FX_WY - 1) / FX_WY);
+      if (h->euler) fargo_w_x_kernel<true><<<blocks, FX_WX * FX_WY, 0, h->stream>>>(F);
+      else fargo_w_x_kernel<false><<<blocks, FX_WX * FX_WY, 0, h->stream>>>(F);
+    } else {
+      unsigned blocks = (unsigned)((h->g.nx + 4 + FW_WX - 1) / FW_WX);
+      if (h->euler) fargo_w_kernel<true><<<blocks, FW_WX * FW_WY, 0, h->stream>>>(F);
+      else fargo_w_kernel<false><<<blocks, FW_WX * FW_WY, 0, h->stream>>>(F);
+    }
     CUDA_TRY(h, cudaGetLastError());
     return FGPU_OK;
   });
@@ -927,10 +937,16 @@ int launch_fargo_advect(fgpu_handle* h, const double* in, double* out, const dou
   X.checkdata = h->cfg.checkdata;
   X.chunk = 8;
   return timed_launch(h, false, 0.0, [&] {
-    constexpr int TX = 32, TY = 4;
-    dim3 grid((h->g.nx + TX - 1) / TX, (h->g.ny + TY * X.chunk - 1) / (TY * X.chunk));
-    if (h->euler) fargo_advect_kernel<true, TX, TY><<<grid, TX * TY, 0, h->stream>>>(X);
-    else fargo_advect_kernel<false, TX, TY><<<grid, TX * TY, 0, h->stream>>>(X);
+    if (h->fdir == 1) {
+      const unsigned blocks = (unsigned)std::min<long long>((h->g.n + 255) / 256, 148 * 8);
+      if (h->euler) fargo_advect_x_kernel<true><<<blocks, 256, 0, h->stream>>>(X);
+      else fargo_advect_x_kernel<false><<<blocks, 256, 0, h->stream>>>(X);
+    } else {
+      constexpr int TX = 32, TY = 4;
+      dim3 grid((h->g.nx + TX - 1) / TX, (h->g.ny + TY * X.chunk - 1) / (TY * X.chunk));
+      if (h->euler) fargo_advect_kernel<true, TX, TY><<<grid, TX * TY, 0, h->stream>>>(X);
+      else fargo_advect_kernel<false, TX, TY><<<grid, TX * TY, 0, h->stream>>>(X);
+    }
     CUDA_TRY(h, cudaGetLastError());
     return FGPU_OK;
   });
@@ -951,7 +967,7 @@ int enqueue_fargo_step(fgpu_handle* h) {
   double* Bbuf = h->buf[2];
   const double* W = h->d_w;
   const bool dyn = h->cfg.fargo_method == 1;   // type 2 keeps the user's w: no recomputation
-  double* Wn = dyn ? h->d_w + h->nxp : h->d_w;
+  double* Wn = dyn ? h->d_w + h->nw : h->d_w;
   const Chain pre = fargo_pre(h);
   if (dyn) {
     StateRef S = plain_state(P, false);
@@ -992,7 +1008,7 @@ int enqueue_fargo_step(fgpu_handle* h) {
   B.in.pre = chain_add(chain_none(), Wn, 1.0);
   B.w_sub = Wn;
   if (int rc = launch_misc(h, 0, B)) return rc;
-  if (dyn) CUDA_TRY(h, cudaMemcpyAsync(h->d_w, Wn, sizeof(double) * h->nxp, cudaMemcpyDeviceToDevice, h->stream));
+  if (dyn) CUDA_TRY(h, cudaMemcpyAsync(h->d_w, Wn, sizeof(double) * h->nw, cudaMemcpyDeviceToDevice, h->stream));
   h->fargo_phase = 2;
   h->pre_rt = h->roundtrip_cfg;
   return FGPU_OK;
@@ -1327,8 +1343,12 @@ int validate(fgpu_handle* h) {
     if (c.fargo_method != 1 && c.fargo_method != 2)
       return set_err(h, FGPU_EUNSUPPORTED, "fargo: types 1 (computed) and 2 (user-supplied) background velocity only; "
                                            "type 3 needs the shearing-box sources");
-    if (c.fargo_direction != 2) return set_err(h, FGPU_EUNSUPPORTED, "fargo: only transport along y (direction 2) is supported");
+    if (c.fargo_direction != 1 && c.fargo_direction != 2)
+      return set_err(h, FGPU_EUNSUPPORTED, "fargo: transport along x (direction 1) or y (direction 2) only");
     if (h->nd != 2) return set_err(h, FGPU_EUNSUPPORTED, "fargo: 2D x-y meshes only");
+    if (c.fargo_direction == 1 && h->accrete)
+      return set_err(h, FGPU_EUNSUPPORTED, "fargo along x with point-mass accretion through the x boundaries");
+    h->fdir = c.fargo_direction;
     if (h->roundtrip_cfg)
       return set_err(h, FGPU_EUNSUPPORTED, "fargo with ideal-gas physics: checkdata without CHECK_PMIN "
                                            "(its round trip sits between the frame changes)");
@@ -1420,6 +1440,7 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
     h->g.nx = cfg->inum; h->g.ny = cfg->jnum; h->g.nz = h->nd == 3 ? cfg->knum : 1;
     h->g.n = (long long)h->g.nx * h->g.ny * h->g.nz;
     for (int f = 0; f < 6; ++f) h->g.bc[f] = cfg->bc[f];
+    h->g.fdir = h->fdir;
     h->ph.gamma = cfg->gamma; h->ph.gm1 = cfg->gamma - 1.; h->ph.pmin = cfg->pmin; h->ph.rhomin = cfg->rhomin;
     h->ph.tiny2 = 2.0 * DBL_MIN;
     h->ph.inv_gm1 = 1.0 / h->ph.gm1;
@@ -1454,8 +1475,24 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
     if (!rc && h->vis_model != FGPU_VIS_MOLECULAR) rc = upload_visc_geometry(h);
   }
   if (!rc && h->fargo) {
-    if (cudaMalloc(&h->d_w, sizeof(double) * 2 * h->nxp) != cudaSuccess) rc = set_err(h, FGPU_ENOMEM, "fargo arrays");
-    else cudaMemsetAsync(h->d_w, 0, sizeof(double) * 2 * h->nxp, h->stream);
+    h->nw = h->fdir == 1 ? h->g.ny + 4 : h->nxp;
+    if (cudaMalloc(&h->d_w, sizeof(double) * 3 * h->nw) != cudaSuccess) rc = set_err(h, FGPU_ENOMEM, "fargo arrays");
+    else cudaMemsetAsync(h->d_w, 0, sizeof(double) * 3 * h->nw, h->stream);
+    if (!rc && h->fdir == 1) {
+      // wfactor(j) (timedisc_base.f90:435-441): the narrowest x-width of the first interior
+      // column over its S/N and B/T faces relative to the width through the centre; those
+      // faces share the centre's x, and the scale factors depend on x only
+      const fgpu_config& c = h->cfg;
+      const double x = c.xmin + ((double)(2 * 1 - 1) * 0.5) * ((c.xmax - c.xmin) / c.inum);
+      double hxc, hyc, hzc;
+      scale(c.geometry, c.gparam, x, hxc, hyc, hzc);
+      auto mn = [](double a, double b) { return b < a ? b : a; };
+      std::vector<double> wf((size_t)h->nw, mn(mn(hxc, hxc), mn(hxc, hxc)) / hxc);
+      // on the handle's stream, after its memset (a pageable source is staged before the call returns)
+      if (cudaMemcpyAsync(h->d_w + 2 * (size_t)h->nw, wf.data(), sizeof(double) * wf.size(), cudaMemcpyHostToDevice,
+                          h->stream) != cudaSuccess)
+        rc = set_err(h, FGPU_ECUDA, "fargo wfactor upload");
+    }
   }
   if (!rc) {
     if (cudaMalloc(&h->d_ctl, sizeof(Ctl)) != cudaSuccess) rc = set_err(h, FGPU_ENOMEM, "control block");
@@ -1693,7 +1730,7 @@ int fgpu_first_step(fgpu_handle* h) {
     // CFL of its ComputeRHS on the co-moving state
     if (h->cfg.fargo_method == 1)
       if (int rc = launch_fargo_w(h, plain_state(h->buf[0], false), nullptr, h->d_w)) return rc;
-    CUDA_TRY(h, cudaMemcpyAsync(h->d_w + h->nxp, h->d_w, sizeof(double) * h->nxp, cudaMemcpyDeviceToDevice, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->d_w + h->nw, h->d_w, sizeof(double) * h->nw, cudaMemcpyDeviceToDevice, h->stream));
     B.w_sub = h->d_w;
     h->fargo_phase = 1;
   }
@@ -2062,9 +2099,10 @@ int fgpu_set_fargo_velocity(fgpu_handle* h, const double* w, int64_t n) {
   if (!h->fargo || h->cfg.fargo_method != 2)
     return set_err(h, FGPU_EBADCFG, "the background velocity is supplied for fargo type 2 only");
   if (h->first_done) return set_err(h, FGPU_EBADCFG, "set the fargo background velocity before the first step");
-  if (n < h->nxp) return set_err(h, FGPU_EARG, "background velocity array too small (inum+4 values)");
-  CUDA_TRY(h, cudaMemcpyAsync(h->d_w, w, sizeof(double) * h->nxp, cudaMemcpyHostToDevice, h->stream));
-  CUDA_TRY(h, cudaMemcpyAsync(h->d_w + h->nxp, w, sizeof(double) * h->nxp, cudaMemcpyHostToDevice, h->stream));
+  if (n < h->nw)
+    return set_err(h, FGPU_EARG, "background velocity array too small (inum+4 values along y, jnum+4 along x)");
+  CUDA_TRY(h, cudaMemcpyAsync(h->d_w, w, sizeof(double) * h->nw, cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(h, cudaMemcpyAsync(h->d_w + h->nw, w, sizeof(double) * h->nw, cudaMemcpyHostToDevice, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return FGPU_OK;
 }

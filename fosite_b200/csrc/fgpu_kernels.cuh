@@ -193,34 +193,34 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
         for (int l = 0; l < V; ++l) R[l] = u[l];
         return;
       }
-      if (FG && A.in.pre.n) apply_chain<V>(A.in.pre, u, gi + 2);
+      if (FG && A.in.pre.n) apply_chain<V>(A.in.pre, u, g, gi, gj);
       if (PRIM) {
         PH::c2p(u, p, P);
         if (roundtrip) p[V - 1] = dmax(p[V - 1], P.pmin);
-        if (FG && A.w_sub) p[2] = p[2] - A.w_sub[gi + 2];
+        if (FG && A.w_sub) sub_velocity(p, A.w_sub[fargo_ix(g, gi, gj)], g.fdir);
 #pragma unroll
         for (int l = 0; l < V; ++l) R[l] = p[l];
       } else if (roundtrip) {
         PH::c2p(u, p, P);
         p[V - 1] = dmax(p[V - 1], P.pmin);
         PH::p2c(p, R, P);
-        if (FG && A.w_sub) frame_change<V>(R, -1.0, A.w_sub[gi + 2]);
+        if (FG && A.w_sub) frame_change<V>(R, -1.0, A.w_sub[fargo_ix(g, gi, gj)], g.fdir);
       } else {
 #pragma unroll
         for (int l = 0; l < V; ++l) R[l] = u[l];
-        if (FG && A.w_sub) frame_change<V>(R, -1.0, A.w_sub[gi + 2]);
+        if (FG && A.w_sub) frame_change<V>(R, -1.0, A.w_sub[fargo_ix(g, gi, gj)], g.fdir);
       }
     } else {
       int d = !inx ? 0 : (!iny ? 1 : 2);
       CE::face_ghost_p(SR, g, P, M, d, gi, gj, gk, p);
       if (roundtrip) p[V - 1] = dmax(p[V - 1], P.pmin);
       if (PRIM) {
-        if (FG && A.w_sub) p[2] = p[2] - A.w_sub[gi + 2];
+        if (FG && A.w_sub) sub_velocity(p, A.w_sub[fargo_ix(g, gi, gj)], g.fdir);
 #pragma unroll
         for (int l = 0; l < V; ++l) R[l] = p[l];
       } else {
         PH::p2c(p, R, P);
-        if (FG && A.w_sub) frame_change<V>(R, -1.0, A.w_sub[gi + 2]);
+        if (FG && A.w_sub) frame_change<V>(R, -1.0, A.w_sub[fargo_ix(g, gi, gj)], g.fdir);
       }
     }
   };
@@ -455,7 +455,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
       const bool fsrc = FG && A.w_sub;
       if (fsrc) {
         state_at<V>(A.in, g.n, idx, cc);
-        if (A.in.pre.n) apply_chain<V>(A.in.pre, cc, ip);
+        if (A.in.pre.n) apply_chain<V>(A.in.pre, cc, g, i, j);
         PH::c2p(cc, pc, P);
         if (roundtrip) {   // CHECK_PMIN of this ComputeRHS (FirstStep's CHECK_ALL)
           pc[V - 1] = dmax(pc[V - 1], P.pmin);
@@ -464,14 +464,36 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
       }
       // geometric sources (physics_euler.f90:1706-1847 / physics_eulerisotherm.f90:689-832)
       double geo2 = 0.0;
-      if (M.curv && ND == 2 && fsrc) {
+      if (fsrc && g.fdir == 1) {
+        // transport along x: geometric sources of the real frame, AddFargoSourcesX into the x
+        // one (isothermal physics_eulerisotherm.f90:1462-1518; Euler physics_euler.f90:2267-2355
+        // adds the energy term -vx*(tmp + GetGeometricalSourceX(vz = P = mz = 0)))
+        const double vx = pc[1], vy = pc[2];
+        const double cxyx = M.cxyx[ip], cyxy = M.cyxy[ip], czxz = M.czxz[ip], czyz = M.czyz[ip];
+        double geo1 = 0.0;
+        if (M.curv) {
+          const double Pp = EU ? pc[V - 1] : pc[0] * (M.cs[ip] * M.cs[ip]);
+          geo1 = cc[2] * (cyxy * vy - cxyx * vx) + (cyxy + czxz) * Pp;
+          rhs[2] = rhs[2] - (cc[1] * (cxyx * vx - cyxy * vy) + (cxyx + czyz) * Pp);
+        }
+        const int jp = j + 2;
+        const double tmp = cc[2] * 0.5 * (A.w_sub[jp + 1] - A.w_sub[jp - 1]) / M.dly[ip];
+        geo1 = geo1 - tmp;
+        rhs[1] = rhs[1] - geo1;
+        if (EU) {
+          const double cxzx = M.cxzx[ip];
+          const double gx = cc[2] * (cyxy * vy - cxyx * vx) + 0.0 * (czxz * 0.0 - cxzx * vx) + (cyxy + czxz) * 0.0;
+          const double geoE = 0.0 - vx * (tmp + gx);
+          rhs[V - 1] = rhs[V - 1] - geoE;
+        }
+      } else if (M.curv && ND == 2 && fsrc) {
         double Pp = EU ? pc[V - 1] : pc[0] * (M.cs[ip] * M.cs[ip]);
         double vx = pc[1], vy = pc[2];
         double cxyx = M.cxyx[ip], cyxy = M.cyxy[ip], czxz = M.czxz[ip], czyz = M.czyz[ip];
         rhs[1] = rhs[1] - (cc[2] * (cyxy * vy - cxyx * vx) + (cyxy + czxz) * Pp);
         geo2 = cc[1] * (cxyx * vx - cyxy * vy) + (cxyx + czyz) * Pp;
       }
-      if (fsrc) {
+      if (fsrc && g.fdir != 1) {
         // AddFargoSourcesY into the geometric source (isothermal
         // physics_eulerisotherm.f90:1531-1586; Euler physics_euler.f90:2368-2455 adds the
         // energy term -vy*(tmp + GetGeometricalSourceY(vz = P = mz = 0)))
@@ -485,7 +507,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
           const double geoE = 0.0 - vy * (tmp + gy);
           rhs[V - 1] = rhs[V - 1] - geoE;
         }
-      } else if (M.curv) {
+      } else if (!fsrc && M.curv) {
         double Pp = EU ? pc[V - 1] : pc[0] * (M.cs[ip] * M.cs[ip]);
         double vx = pc[1], vy = pc[2];
         double cxyx = M.cxyx[ip], cyxy = M.cyxy[ip], czxz = M.czxz[ip], czyz = M.czyz[ip];
@@ -568,7 +590,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
         double yn[V], y0[V], y[V];
         if (FG && A.yn_chain.n) {
           state_at<V>(A.in, g.n, idx, yn);
-          apply_chain<V>(A.yn_chain, yn, ip, rt_cons);
+          apply_chain<V>(A.yn_chain, yn, g, i, j, rt_cons);
         } else if (!PRIM) {
 #pragma unroll
           for (int v = 0; v < V; ++v) yn[v] = cc[v];
@@ -580,7 +602,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
         }
 #pragma unroll
         for (int v = 0; v < V; ++v) y0[v] = __ldg(A.y0 + (long long)v * g.n + idx);
-        if (FG && A.y0_chain.n) apply_chain<V>(A.y0_chain, y0, ip, rt_cons);
+        if (FG && A.y0_chain.n) apply_chain<V>(A.y0_chain, y0, g, i, j, rt_cons);
         if (EU && A.y0_roundtrip) {
           double q[V];
           PH::c2p(y0, q, P);

@@ -26,14 +26,14 @@ struct BndArgs {
   int gate;        // device-clock attempt slots (ACT_* bits)
 };
 
-// FARGO frame of a checked cell: the real-frame p/c computed from the state go
-// to the co-moving frame, SubtractBackgroundVelocityY (physics_eulerisotherm.f90:1336-1413)
+// FARGO frame of a checked cell (i, j): the real-frame p/c computed from the state go to
+// the co-moving frame, SubtractBackgroundVelocityX/Y (physics_eulerisotherm.f90:1339-1413)
 template <int ND, bool EU>
-__device__ __forceinline__ void to_comoving(const double* w_sub, int ip, double* p, double* c) {
+__device__ __forceinline__ void to_comoving(const double* w_sub, const Grid& g, int i, int j, double* p, double* c) {
   if (ND == 2 && w_sub) {
-    double w = w_sub[ip];
-    p[2] = p[2] - w;
-    frame_change<Phys<ND, EU>::V>(c, -1.0, w);
+    double w = w_sub[fargo_ix(g, i, j)];
+    sub_velocity(p, w, g.fdir);
+    frame_change<Phys<ND, EU>::V>(c, -1.0, w, g.fdir);
   }
 }
 
@@ -127,7 +127,7 @@ __device__ __forceinline__ void boundary_block(const BndArgs& A, const int blk, 
     if ((A.checkdata & 0x01) && !(cs > 0.)) flags |= 0x01;
     if (A.checkdata & 0x08)
       for (int v = 0; v < V; ++v) if (!isfinite(p[v]) || !isfinite(c[v])) flags |= 0x08;
-    to_comoving<ND, EU>(A.w_sub, px, p, c);
+    to_comoving<ND, EU>(A.w_sub, A.g, px - 2, py - 2, p, c);
     double v3[4];
     CE::cfl_cell(p, cs, M, px, v3);
 #pragma unroll
@@ -182,9 +182,10 @@ __global__ void __launch_bounds__(256) interior_cfl_kernel(const __grid_constant
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < A.g.n;
        t += (long long)gridDim.x * blockDim.x) {
     int i = (int)(t % A.g.nx);
+    const int j = (int)((t / A.g.nx) % A.g.ny);
     double u[V], p[V], c[V];
     state_at<V>(A.in, A.g.n, t, u);
-    if (ND == 2 && A.in.pre.n) apply_chain<V>(A.in.pre, u, i + 2);
+    if (ND == 2 && A.in.pre.n) apply_chain<V>(A.in.pre, u, A.g, i, j);
     PH::c2p(u, p, A.ph);
     if (EU && A.roundtrip) { p[V - 1] = dmax(p[V - 1], A.ph.pmin); PH::p2c(p, c, A.ph); }
     else { for (int v = 0; v < V; ++v) c[v] = u[v]; }
@@ -194,7 +195,7 @@ __global__ void __launch_bounds__(256) interior_cfl_kernel(const __grid_constant
     if ((A.checkdata & 0x04) && p[0] < A.ph.rhomin) flags |= 0x04;
     if (A.checkdata & 0x08)
       for (int v = 0; v < V; ++v) if (!isfinite(p[v]) || !isfinite(c[v])) flags |= 0x08;
-    to_comoving<ND, EU>(A.w_sub, i + 2, p, c);
+    to_comoving<ND, EU>(A.w_sub, A.g, i, j, p, c);
     double v3[4];
     CE::cfl_cell(p, cs, M, i + 2, v3);
 #pragma unroll
@@ -215,11 +216,11 @@ __global__ void __launch_bounds__(256) pack_interior_kernel(const __grid_constan
     int j = (int)(r % A.g.ny), k = (int)(r / A.g.ny);
     double u[V], p[V], c[V];
     state_at<V>(A.in, A.g.n, t, u);
-    if (ND == 2 && A.in.pre.n) apply_chain<V>(A.in.pre, u, i + 2);
+    if (ND == 2 && A.in.pre.n) apply_chain<V>(A.in.pre, u, A.g, i, j);
     PH::c2p(u, p, A.ph);
     if (EU && A.roundtrip) { p[V - 1] = dmax(p[V - 1], A.ph.pmin); PH::p2c(p, c, A.ph); }
     else { for (int v = 0; v < V; ++v) c[v] = u[v]; }
-    to_comoving<ND, EU>(A.w_sub, i + 2, p, c);
+    to_comoving<ND, EU>(A.w_sub, A.g, i, j, p, c);
     int kk = ND == 3 ? k + 2 : 0;
     long long pi = (i + 2) + (long long)(A.g.nx + 4) * ((j + 2) + (long long)(A.g.ny + 4) * kk);
     for (int v = 0; v < V; ++v) {

@@ -47,7 +47,8 @@ __device__ __forceinline__ long long pad_index(const Grid& g, int i, int j, int 
 // (the FARGO frame chain without round trips, then Cons2Prim's m * (1/rho)), reading only the
 // density and momentum fields (the velocity of a formed primitive state directly)
 template <int ND>
-__device__ __forceinline__ void interior_rv(const StateRef& S, long long n, long long idx, int ip, double* rv) {
+__device__ __forceinline__ void interior_rv(const StateRef& S, const Grid& g, long long idx, int i, int j, double* rv) {
+  const long long n = g.n;
   const double* b = S.base + idx;
 #pragma unroll
   for (int v = 0; v <= ND; ++v) rv[v] = __ldg(b + (long long)v * n);
@@ -59,8 +60,14 @@ __device__ __forceinline__ void interior_rv(const StateRef& S, long long n, long
     for (int v = 0; v <= ND; ++v) rv[v] = rv[v] - a * __ldg(kq + (long long)v * n);
   }
   if (S.ready) return;
-  if (ND == 2)
-    for (int q = 0; q < S.pre.n; ++q) rv[2] = rv[2] + S.pre.s[q] * (rv[0] * S.pre.w[q][ip]);
+  if (ND == 2 && S.pre.n) {
+    // the frame changes of the momentum along the transport (the energy is not read)
+    const int ix = fargo_ix(g, i, j);
+    double m = g.fdir == 1 ? rv[1] : rv[2];
+    for (int q = 0; q < S.pre.n; ++q) m = m + S.pre.s[q] * (rv[0] * S.pre.w[q][ix]);
+    if (g.fdir == 1) rv[1] = m;
+    else rv[2] = m;
+  }
   const double inv_rho = 1. / rv[0];
 #pragma unroll
   for (int m = 1; m <= ND; ++m) rv[m] = rv[m] * inv_rho;
@@ -121,7 +128,7 @@ __global__ void __launch_bounds__(TX* TY* TZ) visc_kernel(const __grid_constant_
     const int gi = i0 + a, gj = j0 + b, gk = ND == 3 ? k0 + c : 0;
     double p[V];
     if (gi >= 0 && gi < g.nx && gj >= 0 && gj < g.ny && gk >= 0 && gk < g.nz)
-      interior_rv<ND>(A.in, g.n, CE::lin(g, gi, gj, gk), gi + 2, p);
+      interior_rv<ND>(A.in, g, CE::lin(g, gi, gj, gk), gi, gj, p);
     else
       CE::cell_p(A.in, g, A.ph, M, gi, gj, gk, p);
 #pragma unroll
@@ -284,7 +291,7 @@ __global__ void __launch_bounds__(256) visc_update_kernel(const __grid_constant_
     const int gi = px - 2, gj = py - 2, gk = ND == 3 ? pz - 2 : 0;
     double p[V];
     if (gi >= 0 && gi < A.g.nx && gj >= 0 && gj < A.g.ny && gk >= 0 && gk < A.g.nz)
-      interior_rv<ND>(A.in, A.g.n, CE::lin(A.g, gi, gj, gk), px, p);
+      interior_rv<ND>(A.in, A.g, CE::lin(A.g, gi, gj, gk), gi, gj, p);
     else
       CE::cell_p(A.in, A.g, A.ph, A.mt, gi, gj, gk, p);
     double om = A.ephir[q] * p[1];

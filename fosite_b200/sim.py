@@ -170,7 +170,8 @@ class Simulation:
         return st
 
     def set_fargo_velocity(self, w):
-        """Background velocity of FARGO type 2, one value per padded i (inum+4)."""
+        """Background velocity of FARGO type 2: one value per padded i (inum+4) for transport
+        along y, per padded j (jnum+4) along x."""
         w = np.ascontiguousarray(w, dtype=np.float64)
         self._check(self.L.fgpu_set_fargo_velocity(self.h, _ptr(w), w.size))
 

@@ -151,10 +151,10 @@ typedef struct fgpu_config {
     double  pm_mass;               /* default 1.0 */
     /* fargo transport (timedisc_base.f90:369-452): method 0 off, 1 background velocity
      * computed every step, 2 fixed user-supplied background velocity
-     * (fgpu_set_fargo_velocity); 2D x-y isothermal meshes with the fixed-step modified
-     * Euler scheme.  Type 3 (shearing box) is not available. */
+     * (fgpu_set_fargo_velocity); 2D x-y meshes (isothermal or ideal gas without CHECK_PMIN)
+     * with the fixed-step modified Euler scheme.  Type 3 (shearing box) is not available. */
     int32_t fargo_method;
-    int32_t fargo_direction;       /* only 2 (transport along y) is supported */
+    int32_t fargo_direction;       /* 1 transport along x, 2 along y */
     /* output clip time for AdjustTimestep (io/fileio_base.f90:604-621); 0 = stoptime */
     double  tout;
     /* point-mass accretion (gravity_pointmass.f90:287-297, 383-428): the boundary whose
@@ -321,8 +321,9 @@ int  fgpu_batch_autotune(fgpu_batch* b, int reps, int* variant);
 int fgpu_calc_timestep_noalloc(const fgpu_config* cfg, const double* d_cvar, double* d_dt, void* stream);
 int fgpu_get_status(fgpu_handle* h, fgpu_status* st);
 /* Timedisc%w for FARGO type 2 (a background velocity the user supplies, e.g. in
- * InitData; timedisc_base.f90:414-424): one value per padded i (inum+4 values, the
- * interior i starting at index 2); call before fgpu_first_step. */
+ * InitData; timedisc_base.f90:414-424): transport along y, one value per padded i
+ * (inum+4 values, the interior i starting at index 2); along x, one per padded j
+ * (jnum+4 values); call before fgpu_first_step. */
 int fgpu_set_fargo_velocity(fgpu_handle* h, const double* w, int64_t n);
 /* The central point mass and the accumulated boundary mass flux of its last update
  * (gravity_pointmass%mass, %mdot); the configured mass when accretion is off. */

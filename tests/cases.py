@@ -265,6 +265,34 @@ def khi_reynolds(re=1.0e4, rho0=1.0, xyzlen=1.0, v0=-0.5, v1=0.5):
     return abs(rho0 * xyzlen * (v0 - v1) / re)
 
 
+def _iso_fargo_x(n=(40, 30), fargo=1, seed=83):
+    """Isothermal shear flow along x with FARGO transport along x (direction 1): periodic in
+    x, reflecting in y, v_x = 1 + 0.8 y plus noise (a sheared background that FARGO follows)."""
+    c = abi.default_config()
+    c.inum, c.jnum, c.knum = n[0], n[1], 1
+    c.xmin, c.xmax, c.ymin, c.ymax = 0.0, 2.0, -0.5, 0.5
+    c.physics = abi.EULER_ISOTHERM
+    c.csiso = 0.6
+    c.limiter = abi.VANLEER
+    c.variables = abi.PRIMITIVE
+    c.method = abi.MODIFIED_EULER
+    c.tdorder = 3
+    c.tol_rel = 10.0
+    c.cfl = 0.4
+    c.stoptime = 1.0e3
+    c.bc[:4] = [abi.PERIODIC, abi.PERIODIC, abi.REFLECTING, abi.REFLECTING]
+    c.fargo_method = fargo
+    c.fargo_direction = 1
+    abi.finalize_config(c)
+    X, Y, _, _ = problems.centers(c)
+    rng = np.random.default_rng(seed)
+    p = np.zeros((3,) + X.shape)
+    p[0] = 1.0 + 0.1 * np.sin(np.pi * X) + 0.01 * rng.uniform(-1, 1, X.shape)
+    p[1] = 1.0 + 0.8 * Y + 0.02 * rng.uniform(-1, 1, X.shape)
+    p[2] = 0.02 * rng.uniform(-1, 1, X.shape)
+    return c, p, {}
+
+
 def khi_fargo(fargo, direction=1, n=(24, 24), visc=False, seed=11):
     """tests/KHI2D.f90's FARGO legs (:81-150, config :168-245, InitData :300-360): ideal-gas KHI,
     KT + MONOCENT (theta 1.2) on conservative variables, periodic box, FARGO type 1 or 2 along
@@ -339,6 +367,10 @@ CASES = {
                                                        limiter=abi.MONOCENT),
     "disk_fargo2_user_w": lambda: _disk_fargo2(),
     "euler_fargo_shear_cons": lambda: _euler_fargo(),
+    "khi_fargo1_x": lambda: khi_fargo(1, n=(28, 24)),
+    "khi_fargo2_x_visc": lambda: khi_fargo(2, n=(24, 26), visc=True),
+    "iso_fargo1_x_shear": lambda: _iso_fargo_x(),
+    "euler_fargo1_x_disk_cyl": lambda: _with(_euler_fargo(n=(24, 40), geometry=abi.CYLINDRICAL), fargo_direction=1),
     "euler_fargo_disk_cyl_prim": lambda: _euler_fargo(n=(24, 160), geometry=abi.CYLINDRICAL, variables=abi.PRIMITIVE),
     "disk_fargo_order1_minmod": lambda: _disk_fargo(n=(30, 44), tdorder=1, limiter=abi.MINMOD,
                                                     bcs=[abi.REFLECTING, abi.REFLECTING, abi.PERIODIC, abi.PERIODIC]),

@@ -134,7 +134,8 @@ def test_steps_bitwise_exact_build(name):
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["khi_ssprk3_vanleer_cons", "gauss3d_dopri_mc_prim", "disk_logcyl_pointmass",
                                   "euler2d_absorbing", "iso3d_cashkarp_mixed_bc", "disk_fargo_logcyl",
-                                  "khi_visc_re1e4_mc", "gauss3d_visc_dopri", "disk_visc_logcyl_pointmass"])
+                                  "khi_visc_re1e4_mc", "gauss3d_visc_dopri", "disk_visc_logcyl_pointmass",
+                                  "khi_fargo2_x_visc", "iso_fargo1_x_shear"])
 def test_fast_build_tolerance(name):
     cfg, o, g = _pair(name, exact=False)
     o.first_step()
@@ -167,16 +168,13 @@ def test_run_graph_matches_single_steps(name):
 
 
 @pytest.mark.gpu
-def test_fargo_graph_run_matches_single_steps():
-    """FARGO: the first step after FirstStep runs outside the graph, later steps replay it."""
-    from fosite_b200.sim import Simulation
-    cfg, p, extra = CASES["disk_fargo_cyl_cons_reflect"]()
+@pytest.mark.parametrize("name", ["disk_fargo_cyl_cons_reflect", "khi_fargo1_x", "iso_fargo1_x_shear"])
+def test_fargo_graph_run_matches_single_steps(name):
+    """FARGO (along y and along x): the first step after FirstStep runs outside the graph,
+    later steps replay it."""
     sims = []
     for _ in range(2):
-        s = Simulation(cfg, exact=True)
-        shape = (cfg.knum, cfg.jnum + 4, cfg.inum + 4)
-        s.set_sound_speeds(np.broadcast_to(extra["bccsound"], shape), np.broadcast_to(extra["fcsound"], (4,) + shape))
-        s.set_state(abi.PVAR, p)
+        _, _, s = _pair(name, exact=True)
         s.first_step()
         sims.append(s)
     a, b = sims
@@ -212,6 +210,41 @@ def test_khi_transposition_symmetry(visc):
     ra, rb = a.get(abi.PVAR), b.get(abi.PVAR)
     rbt = np.stack([rb[0].transpose(0, 2, 1), rb[2].transpose(0, 2, 1), rb[1].transpose(0, 2, 1), rb[3].transpose(0, 2, 1)])
     assert np.sqrt(np.mean((ra - rbt) ** 2)) < abi.TINY
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("visc", [False, True])
+@pytest.mark.parametrize("fargo", [1, 2])
+def test_khi_fargo_transposition_symmetry(fargo, visc):
+    """tests/KHI2D.f90:81-150, the FARGO legs on the device: FARGO type 1 or 2 along x and
+    the transposed run with FARGO along y agree to TINY (RMS), with and without the test's
+    molecular viscosity, and the run along x equals the oracle's bit for bit."""
+    from fosite_b200.sim import Simulation
+    from cases import khi_fargo
+    runs = []
+    for direction in (1, 2):
+        cfg, p, extra = khi_fargo(fargo, direction=direction, visc=visc)
+        g = Simulation(cfg, exact=True)
+        if "fargo_w" in extra:
+            g.set_fargo_velocity(extra["fargo_w"])
+        g.set_state(abi.PVAR, p)
+        g.first_step()
+        rc, done = g.run(20)
+        assert rc == 0 and done == 20
+        runs.append((g, cfg, p, extra))
+    (a, ca, pa, ea), (b, _, _, _) = runs
+    rb = b.get(abi.PVAR)
+    rbt = np.stack([rb[0], rb[2], rb[1], rb[3]]).transpose(0, 1, 3, 2)
+    assert np.sqrt(np.mean((a.get(abi.PVAR) - rbt) ** 2)) < abi.TINY
+    assert a.status().time == b.status().time
+    o = pyoracle.Oracle(ca)
+    if "fargo_w" in ea:
+        o.set_fargo_velocity(ea["fargo_w"])
+    o.set_state(abi.PVAR, pa)
+    o.first_step()
+    for _ in range(20):
+        assert o.step() == 0
+    assert np.array_equal(o.get(abi.PVAR), a.get(abi.PVAR))
 
 
 @pytest.mark.gpu
