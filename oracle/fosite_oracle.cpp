@@ -96,7 +96,12 @@ struct Oracle {
   int fargo = 0, fdir = 2;
   std::vector<double> w, wfactor, delxy, fdq, fdql, fflux;
   std::vector<int> shift;
-  bool c_trans = false, p_trans = false;     // fargo_transformation_applied flags
+  // fargo_transformation_applied flags of each state vector (physics_eulerisotherm.f90:124):
+  // cvar/pvar and the Butcher stage vectors ctmp/ptmp; assignments between state vectors copy
+  // data only (marray_compound.f90:118-229), Convert2Primitive copies c's flag to p (:338)
+  bool c_trans = false, p_trans = false, ct_trans = false, pt_trans = false;
+  bool& cflag(const std::vector<double>& cv) { return &cv == &ctmp ? ct_trans : c_trans; }
+  bool& pflag(const std::vector<double>& pv) { return &pv == &ptmp ? pt_trans : p_trans; }
   // ---- viscosity (sources_viscosity.f90) ----
   int vismodel = 0;
   double dynconst = 0.0, bulkconst = 0.0, power = 0.0, cvis = 0.5;
@@ -457,7 +462,7 @@ struct Oracle {
   // boundary_generic.f90:287-418 CenterBoundary
   void center_boundary(std::vector<double>& pv, std::vector<double>& cv) {
     c2p_range(cv, pv, IMIN, IMAX, JMIN, JMAX, KMIN, KMAX);
-    p_trans = c_trans;
+    pflag(pv) = cflag(cv);
     if (INUM > 1) { set_bc(FGPU_WEST, pv); set_bc(FGPU_EAST, pv); }
     if (JNUM > 1) { set_bc(FGPU_SOUTH, pv); set_bc(FGPU_NORTH, pv); }
     if (KNUM > 1) { set_bc(FGPU_BOTTOM, pv); set_bc(FGPU_TOP, pv); }
@@ -697,8 +702,9 @@ struct Oracle {
   }
   double wof(int i, int j, int k) const { return w[widx(fdir == 1 ? j : i, k)]; }
   void add_bg(std::vector<double>& pv, std::vector<double>& cv) {
-    if (!c_trans) return;
-    if (!p_trans) return;
+    bool &c_tr = cflag(cv), &p_tr = pflag(pv);
+    if (!c_tr) return;
+    if (!p_tr) return;
     const int vi = fdir;   // the velocity component along the transport
     for (int k = KGMIN; k <= KGMAX; ++k) for (int j = JGMIN; j <= JGMAX; ++j) for (int i = IGMIN; i <= IGMAX; ++i) {
       long c = id(i, j, k); double wv = wof(i, j, k);
@@ -706,11 +712,12 @@ struct Oracle {
       pv[c + NC * vi] = pv[c + NC * vi] + wv;
       cv[c + NC * vi] = cv[c + NC * vi] + cv[c] * wv;
     }
-    c_trans = false; p_trans = false;
+    c_tr = false; p_tr = false;
   }
   void sub_bg(std::vector<double>& pv, std::vector<double>& cv) {
-    if (c_trans) return;
-    if (p_trans) return;
+    bool &c_tr = cflag(cv), &p_tr = pflag(pv);
+    if (c_tr) return;
+    if (p_tr) return;
     const int vi = fdir;
     for (int k = KGMIN; k <= KGMAX; ++k) for (int j = JGMIN; j <= JGMAX; ++j) for (int i = IGMIN; i <= IGMAX; ++i) {
       long c = id(i, j, k); double wv = wof(i, j, k);
@@ -718,7 +725,7 @@ struct Oracle {
       pv[c + NC * vi] = pv[c + NC * vi] - wv;
       cv[c + NC * vi] = cv[c + NC * vi] - cv[c] * wv;
     }
-    c_trans = true; p_trans = true;
+    c_tr = true; p_tr = true;
   }
   // timedisc_base.f90:2243-2326 CalcBackgroundVelocity
   void calc_background_velocity(std::vector<double>& pv, std::vector<double>& cv) {

@@ -105,6 +105,18 @@ def _disk_fargo(n=(32, 48), geometry=abi.LOGCYLINDRICAL, seed=51, variables=abi.
     return c, p, extra
 
 
+def _butcher(case, method, tdorder, tol=1e-3):
+    """Switch a case to an embedded Butcher scheme (timedisc_rkfehlberg.f90 and its tableaus)
+    with relative and absolute tolerance tol."""
+    c, p, extra = case
+    c.method = method
+    c.tdorder = tdorder
+    c.tol_rel = tol
+    for v in range(abi.MAXVAR):
+        c.tol_abs[v] = tol
+    return c, p, extra
+
+
 def _disk_fargo2(n=(32, 40), geometry=abi.CYLINDRICAL, seed=61):
     """FARGO type 2: the user supplies w, here the Keplerian velocity at the cell centres."""
     c, p, extra = _disk_fargo(n=n, geometry=geometry, seed=seed,
@@ -368,6 +380,10 @@ CASES = {
     "disk_fargo2_user_w": lambda: _disk_fargo2(),
     "euler_fargo_shear_cons": lambda: _euler_fargo(),
     "khi_fargo1_x": lambda: khi_fargo(1, n=(28, 24)),
+    "disk_fargo_ssprk5_logcyl": lambda: _butcher(_disk_fargo(), abi.SSPRK, 5),
+    "disk_fargo2_dopri_cyl": lambda: _butcher(_disk_fargo2(), abi.DORMAND_PRINCE, 5, 1e-4),
+    "euler_fargo_rkf5_shear": lambda: _butcher(_euler_fargo(), abi.RK_FEHLBERG, 5, 1e-4),
+    "khi_fargo1_x_cashkarp": lambda: _butcher(khi_fargo(1, n=(24, 26)), abi.CASH_KARP, 5, 1e-4),
     "khi_fargo2_x_visc": lambda: khi_fargo(2, n=(24, 26), visc=True),
     "iso_fargo1_x_shear": lambda: _iso_fargo_x(),
     "euler_fargo1_x_disk_cyl": lambda: _with(_euler_fargo(n=(24, 40), geometry=abi.CYLINDRICAL), fargo_direction=1),
