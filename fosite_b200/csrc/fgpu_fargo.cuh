@@ -121,6 +121,7 @@ struct FargoAdvArgs {
   Ctl* ctl;              // dt/time source and CFL / CheckData sink
   int checkdata;
   int chunk;             // rows of one thread
+  double dt_host;        // > 0: the transport's dt (IntegrationStep's this%dt); else (time+dt)-time of ctl
 };
 
 __device__ __forceinline__ double fargo_minmod(double a, double b) {
@@ -161,7 +162,7 @@ __global__ void __launch_bounds__(TX* TY) fargo_advect_kernel(const __grid_const
   if (i < g.nx && j0 < g.ny) {
     const int ip = i + 2;
     const double w = A.w[ip];
-    const double dte = (A.ctl->time + A.ctl->dt) - A.ctl->time;
+    const double dte = A.dt_host > 0. ? A.dt_host : (A.ctl->time + A.ctl->dt) - A.ctl->time;
     double d = w * dte / M.dly[ip];
     const double sh = round(d);   // NINT: half away from zero
     const int s = (int)sh;
@@ -248,7 +249,7 @@ __global__ void __launch_bounds__(256) fargo_advect_x_kernel(const __grid_consta
   const MetricP& M = A.mt;
   double cflv = 0.0, cflvis = 0.0;
   int flags = 0;
-  const double dte = (A.ctl->time + A.ctl->dt) - A.ctl->time;
+  const double dte = A.dt_host > 0. ? A.dt_host : (A.ctl->time + A.ctl->dt) - A.ctl->time;
   const double dlx0 = M.dlx[2];   // dlx(IMIN, j): the metric depends on i only
   for (long long t = blockIdx.x * 256LL + threadIdx.x; t < g.n; t += (long long)gridDim.x * 256) {
     const int i = (int)(t % g.nx), j = (int)(t / g.nx);
@@ -311,6 +312,22 @@ __global__ void __launch_bounds__(256) fargo_advect_x_kernel(const __grid_consta
   }
   double vals[4] = {cflv, 0.0, 0.0, cflvis};
   block_reduce_emit<256>(vals, M.vis ? 4 : 1, flags, A.ctl->invdt, &A.ctl->flags, sred);
+}
+
+// out = the frame-change chain C applied to every interior cell of the conservative state in
+// (2D): the in-place Add/SubtractBackgroundVelocity calls that IntegrationStep makes on cvar
+template <int V>
+__global__ void __launch_bounds__(256) fargo_chain_copy_kernel(const double* __restrict__ in, double* __restrict__ out,
+                                                               Grid g, Chain C) {
+  for (long long t = blockIdx.x * 256LL + threadIdx.x; t < g.n; t += (long long)gridDim.x * 256) {
+    const int i = (int)(t % g.nx), j = (int)(t / g.nx);
+    double c[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) c[v] = in[(long long)v * g.n + t];
+    apply_chain<V>(C, c, g, i, j);
+#pragma unroll
+    for (int v = 0; v < V; ++v) out[(long long)v * g.n + t] = c[v];
+  }
 }
 
 }  // namespace fgpu

@@ -177,6 +177,7 @@ struct fgpu_handle {
   int nw = 0;                   // padded length of w along the other direction
   double* d_w = nullptr;        // [w | w_new | wfactor of direction 1]
   int fargo_phase = 0;
+  bool fargo_tmp_fresh = true;  // Butcher + FARGO: the stage vectors' frame flags are still unset
   // point-mass accretion: d_acc = [bx (ny) | bxold (ny) | brow (ny) | mass, mdot]
   bool accrete = false;
   int acc_face = 0;             // 0 west, 1 east
@@ -926,16 +927,7 @@ int launch_fargo_w(fgpu_handle* h, const StateRef& in, const double* w_prev, dou
   });
 }
 
-int launch_fargo_advect(fgpu_handle* h, const double* in, double* out, const double* w) {
-  FargoAdvArgs X;
-  std::memset(&X, 0, sizeof(X));
-  X.g = h->g; X.ph = h->ph; X.mt = h->mt;
-  X.in = plain_state(in, false);
-  X.w = w;
-  X.out = out;
-  X.ctl = h->d_ctl;
-  X.checkdata = h->cfg.checkdata;
-  X.chunk = 8;
+int launch_fargo_advect_args(fgpu_handle* h, const FargoAdvArgs& X) {
   return timed_launch(h, false, 0.0, [&] {
     if (h->fdir == 1) {
       const unsigned blocks = (unsigned)std::min<long long>((h->g.n + 255) / 256, 148 * 8);
@@ -950,6 +942,18 @@ int launch_fargo_advect(fgpu_handle* h, const double* in, double* out, const dou
     CUDA_TRY(h, cudaGetLastError());
     return FGPU_OK;
   });
+}
+int launch_fargo_advect(fgpu_handle* h, const double* in, double* out, const double* w) {
+  FargoAdvArgs X;
+  std::memset(&X, 0, sizeof(X));
+  X.g = h->g; X.ph = h->ph; X.mt = h->mt;
+  X.in = plain_state(in, false);
+  X.w = w;
+  X.out = out;
+  X.ctl = h->d_ctl;
+  X.checkdata = h->cfg.checkdata;
+  X.chunk = 8;
+  return launch_fargo_advect_args(h, X);
 }
 
 // One fosite%Step with FARGO transport (timedisc_base.f90:649-750 with the
@@ -1135,11 +1139,45 @@ int modeuler_attempt(fgpu_handle* h, double t, double dtv, double& err) {
   return FGPU_OK;
 }
 
+// FARGO with a Butcher scheme: the background velocity of the step (w_new for type 1) and the
+// attempt base cvar, which differs from cold once a ComputeRHS has framed it (the spare
+// formed-state buffer; cold stays in buf[1])
+const double* fargo_wn(const fgpu_handle* h) { return h->cfg.fargo_method == 1 ? h->d_w + h->nw : h->d_w; }
+double* bt_cvar(const fgpu_handle* h) { return h->fargo ? h->buf[2 + h->T.m] : h->buf[1]; }
+
+int launch_fargo_chain_copy(fgpu_handle* h, const double* in, double* out, const Chain& C) {
+  const unsigned blocks = (unsigned)std::min<long long>((h->g.n + 255) / 256, 148 * 8);
+  return timed_launch(h, false, 0.0, [&] {
+    switch (h->V) {
+      case 3: fargo_chain_copy_kernel<3><<<blocks, 256, 0, h->stream>>>(in, out, h->g, C); break;
+      default: fargo_chain_copy_kernel<4><<<blocks, 256, 0, h->stream>>>(in, out, h->g, C); break;
+    }
+    CUDA_TRY(h, cudaGetLastError());
+    return FGPU_OK;
+  });
+}
+
+// ComputeRHS of a FARGO state vector into k1 (timedisc_base.f90:1096-1121,1190-1208): in gets
+// AddBackgroundVelocity (pre) before the boundary fill and SubtractBackgroundVelocity(w) after
+// the sources; cvar after the call (co-moving) goes to out_base
+int enqueue_k1_fargo(fgpu_handle* h, const double* in, const Chain& pre, bool rt, int checkdata, double* out_base,
+                     double t) {
+  StageArgs A = base_args(h);
+  A.out_mode = OUT_RHS;
+  A.out = h->buf[2];
+  A.in = plain_state(in, rt);
+  A.in.pre = pre;
+  A.w_sub = fargo_wn(h);
+  A.out_base = out_base;
+  A.checkdata = checkdata;
+  return launch_stage(h, A, RhsTime::host(t));
+}
+
 int butcher_attempt(fgpu_handle* h, double t, double dtv, double& err) {
   if (h->adaptive_me) return modeuler_attempt(h, t, dtv, err);
   const Tableau& T = h->T;
   double* P = h->buf[0];
-  double* base = h->buf[1];
+  double* base = bt_cvar(h);
   h->stats.attempts += 1;
   for (int m = 2; m <= T.m; ++m) {
     StageArgs A = base_args(h);
@@ -1149,6 +1187,14 @@ int butcher_attempt(fgpu_handle* h, double t, double dtv, double& err) {
     for (int q = 0; q < m - 1; ++q) {
       A.in.K[q] = h->buf[2 + q];
       A.in.coef[q] = T.A[(m - 1) * T.m + q] * dtv;
+    }
+    if (h->fargo) {
+      // ComputeRHS(ptmp, ctmp): AddBackgroundVelocity(w) acts only once the stage vectors carry
+      // the frame flag, i.e. not on the first ComputeRHS of the run (physics_eulerisotherm.f90:
+      // 1279-1299); SubtractBackgroundVelocity(w) always
+      A.in.pre = h->fargo_tmp_fresh ? chain_none() : chain_add(chain_none(), fargo_wn(h), 1.0);
+      A.w_sub = fargo_wn(h);
+      h->fargo_tmp_fresh = false;
     }
     if (h->materialize) {
       // the stage state's reconstruction variables once per cell, read by the stencil
@@ -1207,9 +1253,14 @@ int butcher_attempt(fgpu_handle* h, double t, double dtv, double& err) {
   return FGPU_OK;
 }
 
-int finish_cfl_host(fgpu_handle* h, const double* state, bool roundtrip, double& dtcfl, int checkdata, int& cause) {
+int finish_cfl_host(fgpu_handle* h, const double* state, bool roundtrip, double& dtcfl, int checkdata, int& cause,
+                    bool interior = false) {
   BndArgs B = bnd_args(h, state, roundtrip, FIN_NONE);
   B.checkdata = checkdata;
+  if (h->fargo) { B.in.pre = fargo_pre(h); B.w_sub = h->d_w; }
+  // interior cells too (the stage kernels' CFL epilogue sees the real frame only)
+  if (interior)
+    if (int rc = launch_misc(h, 1, B)) return rc;
   if (int rc = launch_misc(h, 0, B)) return rc;
   if (int rc = launch_visc_cfl(h, plain_state(state, roundtrip), roundtrip, RhsTime::host(h->time))) return rc;
   if (int rc = read_ctl(h)) return rc;
@@ -1225,6 +1276,23 @@ int finish_cfl_host(fgpu_handle* h, const double* state, bool roundtrip, double&
 
 int butcher_integration_step(fgpu_handle* h) {
   // timedisc_base.f90:649-750 IntegrationStep
+  if (h->fargo) {
+    // CalcBackgroundVelocity (type 1: w_new from the real-frame state of the last ComputeRHS)
+    // adds w to cvar, SubtractBackgroundVelocity(w_new) takes it to the new co-moving frame;
+    // cold is not touched (timedisc_base.f90:661-674)
+    double* W = h->d_w;
+    const double* Wn = fargo_wn(h);
+    if (h->cfg.fargo_method == 1) {
+      StateRef S = plain_state(h->buf[0], false);
+      S.pre = fargo_pre(h);
+      if (int rc = launch_fargo_w(h, S, W, h->d_w + h->nw)) return rc;
+      if (int rc = launch_fargo_chain_copy(h, h->buf[1], bt_cvar(h), chain_add(chain_add(chain_none(), W, 1.0), Wn, -1.0)))
+        return rc;
+    } else {
+      CUDA_TRY(h, cudaMemcpyAsync(bt_cvar(h), h->buf[1], sizeof(double) * h->V * h->g.n, cudaMemcpyDeviceToDevice,
+                                  h->stream));
+    }
+  }
   double t = h->time, d = h->dt;
   if (d < h->dtmin && h->dtcause != FGPU_DTCAUSE_FILEIO) h->dtmin = d;
   double dtold_ = 0.0;
@@ -1239,20 +1307,66 @@ int butcher_integration_step(fgpu_handle* h) {
     if (e != e) h->brk = true;
     else if (e > DBL_MAX) h->brk = true;
     else if (e >= 1.0) {   // RejectSolution: cvar = cold, RHS with CHECK_NOTHING
-      if (int rc = enqueue_k1(h, false, false, false, h->cfg.checkdata, t)) return rc;
+      if (h->fargo) {
+        // the RHS frames cvar (cold + w_new - w_new), cold keeps its data
+        const Chain pre = chain_add(chain_none(), fargo_wn(h), 1.0);
+        if (int rc = enqueue_k1_fargo(h, h->buf[1], pre, false, FGPU_CHECK_NOTHING, bt_cvar(h), t)) return rc;
+      } else if (int rc = enqueue_k1(h, false, false, false, h->cfg.checkdata, t)) {
+        return rc;
+      }
       h->n_adj++;
       h->dtcause = FGPU_DTCAUSE_ERRADJ;
       if (d < h->dtmin) h->dtmin = d;
     } else {               // AcceptSolution
       t = t + dtold_;
       if (t < h->time + h->dt) {
-        if (int rc = enqueue_k1(h, true, false, h->roundtrip_cfg, h->cfg.checkdata, t)) return rc;
+        if (h->fargo) {
+          // cold = cvar = the accepted state framed by this ComputeRHS
+          const Chain pre = chain_add(chain_none(), fargo_wn(h), 1.0);
+          if (int rc = enqueue_k1_fargo(h, h->buf[0], pre, h->roundtrip_cfg, h->cfg.checkdata, h->buf[1], t)) return rc;
+          CUDA_TRY(h, cudaMemcpyAsync(bt_cvar(h), h->buf[1], sizeof(double) * h->V * h->g.n, cudaMemcpyDeviceToDevice,
+                                      h->stream));
+        } else if (int rc = enqueue_k1(h, true, false, h->roundtrip_cfg, h->cfg.checkdata, t)) {
+          return rc;
+        }
         rhs_done_at_t = true;
       }
       h->iter++;
       h->stats.cell_updates += h->g.n;
     }
     if (d < h->dtlimit) h->brk = true;
+  }
+  if (!h->brk && h->fargo) {
+    const double dt_step = t - h->time;
+    h->dt = dt_step;
+    h->time = t;
+    h->dtold = d;
+    // CenterBoundary + FargoAdvection of cvar (the accepted state, or its framed copy in cold
+    // when AcceptSolution already evaluated the RHS), Convert2Primitive and the closing
+    // ComputeRHS (timedisc_base.f90:727-744); the advection pass also reduces the interior
+    // CFL (co-moving) and CheckData (real frame) of the closing ComputeRHS
+    const double* Wn = fargo_wn(h);
+    double* src = rhs_done_at_t ? h->buf[1] : h->buf[0];
+    double* dst = rhs_done_at_t ? h->buf[0] : bt_cvar(h);
+    FargoAdvArgs X;
+    std::memset(&X, 0, sizeof(X));
+    X.g = h->g; X.ph = h->ph; X.mt = h->mt;
+    X.in = plain_state(src, false);
+    X.w = Wn;
+    X.out = dst;
+    X.ctl = h->d_ctl;
+    X.checkdata = h->cfg.checkdata;
+    X.chunk = 8;
+    X.dt_host = dt_step;
+    if (int rc = launch_fargo_advect_args(h, X)) return rc;
+    if (!rhs_done_at_t) std::swap(h->buf[0], h->buf[2 + h->T.m]);   // the advected state is the stored one
+    const Chain pre = chain_add(chain_none(), Wn, 1.0);
+    if (int rc = enqueue_k1_fargo(h, h->buf[0], pre, false, h->cfg.checkdata, h->buf[1], h->time)) return rc;
+    if (h->cfg.fargo_method == 1)
+      CUDA_TRY(h, cudaMemcpyAsync(h->d_w, Wn, sizeof(double) * h->nw, cudaMemcpyDeviceToDevice, h->stream));
+    h->fargo_phase = 2;
+    h->pre_rt = false;
+    return FGPU_OK;
   }
   if (!h->brk) {
     h->dt = t - h->time;
@@ -1352,7 +1466,8 @@ int validate(fgpu_handle* h) {
     if (h->roundtrip_cfg)
       return set_err(h, FGPU_EUNSUPPORTED, "fargo with ideal-gas physics: checkdata without CHECK_PMIN "
                                            "(its round trip sits between the frame changes)");
-    if (h->butcher) return set_err(h, FGPU_EUNSUPPORTED, "fargo: fixed-step modified Euler (Shu-Osher) time stepping only");
+    if (h->adaptive_me)
+      return set_err(h, FGPU_EUNSUPPORTED, "fargo: modified Euler with embedded error control not supported");
     h->fargo = true;
   }
   if (c.vismodel != 0) {
@@ -1431,6 +1546,8 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
     if (const char* e = std::getenv("FGPU_MATERIALIZE")) h->materialize = std::atoi(e) != 0;
     if (const char* e = std::getenv("FGPU_FUSE_FORM")) h->fuse_form = std::atoi(e) != 0;
     if (const char* e = std::getenv("FGPU_FUSE_END")) h->fuse_end = std::atoi(e) != 0;
+    // FARGO with a Butcher scheme: the stencil forms each stage state with its frame changes
+    if (h->fargo && h->butcher) h->materialize = false;
     h->fuse_form = h->fuse_form && h->materialize;
   }
   if (!rc) configure_stage_kernels(h->nd, h->euler, h->prim);
@@ -1705,10 +1822,22 @@ int fgpu_first_step(fgpu_handle* h) {
   // (fosite.f90:315-321): ideal-gas states get the CHECK_PMIN round trip here
   const bool rt_first = h->euler;
   if (h->butcher) {
-    if (int rc = enqueue_k1(h, true, true, rt_first, FGPU_CHECK_ALL, h->time)) return rc;
     double dtc;
     int cause = 0;
-    if (int rc = finish_cfl_host(h, h->buf[0], rt_first, dtc, FGPU_CHECK_ALL, cause)) return rc;
+    if (h->fargo) {
+      // FirstStep's CenterBoundary + CalcBackgroundVelocity (the state carries no frame yet),
+      // then its ComputeRHS: no AddBackgroundVelocity, SubtractBackgroundVelocity(w) after the
+      // sources; cold = that co-moving cvar; CalcTimestep on the co-moving state
+      if (h->cfg.fargo_method == 1)
+        if (int rc = launch_fargo_w(h, plain_state(h->buf[0], false), nullptr, h->d_w)) return rc;
+      CUDA_TRY(h, cudaMemcpyAsync(h->d_w + h->nw, h->d_w, sizeof(double) * h->nw, cudaMemcpyDeviceToDevice, h->stream));
+      h->fargo_phase = 1;
+      if (int rc = enqueue_k1_fargo(h, h->buf[0], chain_none(), rt_first, FGPU_CHECK_ALL, h->buf[1], h->time)) return rc;
+      if (int rc = finish_cfl_host(h, h->buf[0], rt_first, dtc, FGPU_CHECK_ALL, cause, true)) return rc;
+    } else {
+      if (int rc = enqueue_k1(h, true, true, rt_first, FGPU_CHECK_ALL, h->time)) return rc;
+      if (int rc = finish_cfl_host(h, h->buf[0], rt_first, dtc, FGPU_CHECK_ALL, cause)) return rc;
+    }
     h->dt = dtc;
     h->dtcause = cause;
     h->pre_rt = rt_first;

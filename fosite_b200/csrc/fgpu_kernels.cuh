@@ -648,6 +648,15 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
       if (A.out_base) {
 #pragma unroll
         for (int v = 0; v < V; ++v) A.out_base[(long long)v * g.n + idx] = cc[v];
+        if (fsrc) {
+          // FARGO: cvar after this ComputeRHS is co-moving (its SubtractBackgroundVelocity)
+          double o[V];
+#pragma unroll
+          for (int v = 0; v < V; ++v) o[v] = cc[v];
+          frame_change<V>(o, -1.0, A.w_sub[fargo_ix(g, i, j)], g.fdir);
+#pragma unroll
+          for (int v = 0; v < V; ++v) A.out_base[(long long)v * g.n + idx] = o[v];
+        }
       }
       if (A.cfl_mode == 2) {
         double cs = EU ? PH::cs_of(pc, P) : M.cs[ip];

@@ -135,7 +135,7 @@ def test_steps_bitwise_exact_build(name):
 @pytest.mark.parametrize("name", ["khi_ssprk3_vanleer_cons", "gauss3d_dopri_mc_prim", "disk_logcyl_pointmass",
                                   "euler2d_absorbing", "iso3d_cashkarp_mixed_bc", "disk_fargo_logcyl",
                                   "khi_visc_re1e4_mc", "gauss3d_visc_dopri", "disk_visc_logcyl_pointmass",
-                                  "khi_fargo2_x_visc", "iso_fargo1_x_shear"])
+                                  "khi_fargo2_x_visc", "iso_fargo1_x_shear", "disk_fargo_ssprk5_logcyl"])
 def test_fast_build_tolerance(name):
     cfg, o, g = _pair(name, exact=False)
     o.first_step()
