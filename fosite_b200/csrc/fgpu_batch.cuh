@@ -224,7 +224,7 @@ int build_embedded_tables(fgpu_batch* b) {
     {   // AcceptSolution's RHS inside the step
       StageArgs A = base_args(h);
       A.out_mode = OUT_RHS; A.out = K1; A.in = plain_state(P, h->roundtrip_cfg); A.out_base = base;
-      A.checkdata = h->cfg.checkdata; A.gate = ACT_SUB; A.kchunk = h->kchunk;
+      A.checkdata = h->cfg.checkdata; A.cfl_mode = h->cfg.checkdata ? 3 : 0; A.gate = ACT_SUB; A.kchunk = h->kchunk;
       eargs[(size_t)M * n + i] = A;
     }
     {   // the closing RHS with the CFL reduction
@@ -293,6 +293,8 @@ int enqueue_batch_slot(fgpu_batch* b) {
   BCUDA_TRY(b, cudaGetLastError());
   if (int rc = launch_batched_stage(b, b->d_eargs + (size_t)(M - 1) * n, b->variant)) return rc;
   if (int rc = launch_batched_stage(b, b->d_eargs + (size_t)M * n, b->variant)) return rc;
+  bt_subcheck_batch_kernel<<<mb, 128, 0, b->stream>>>(b->d_ctlp, n);
+  BCUDA_TRY(b, cudaGetLastError());
   batched_copy_kernel<<<b->ncblocks, 256, 0, b->stream>>>(b->d_copy, b->d_cblocks);
   BCUDA_TRY(b, cudaGetLastError());
   if (int rc = launch_batched_stage(b, b->d_eargs + (size_t)(M + 1) * n, b->variant)) return rc;

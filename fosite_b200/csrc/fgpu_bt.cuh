@@ -94,6 +94,9 @@ __device__ void bt_decide_body(Ctl* c, const BtParams& P) {
   if (d < c->dtlimit) c->brk = 1;
   c->d_att = d;
   if (!c->brk && !(c->t_loc + d <= c->time + c->dt)) {
+    c->time_prev = c->time;
+    c->dt_prev = c->dt;
+    c->dtold_prev = c->dtold;
     c->dt = c->t_loc - c->time;
     c->time = c->t_loc;
     c->dtold = d;
@@ -104,11 +107,36 @@ __device__ void bt_decide_body(Ctl* c, const BtParams& P) {
 }
 __global__ void bt_decide_kernel(Ctl* c, BtParams P) { bt_decide_body(c, P); }
 
+// CheckData of AcceptSolution's ComputeRHS inside the step (timedisc_base.f90:926-931): a
+// failure breaks IntegrationStep's loop; the step then ends without its closing (time, dt and
+// dtold stay those of the step's start).  The stored state keeps the accepted solution, whose
+// CHECK_PMIN round trip gives cvar as that ComputeRHS left it; bt_finish breaks and the
+// slot's closing kernels do nothing.
+__device__ void bt_subcheck_body(Ctl* c) {
+  if (!(c->act & ACT_SUB) || (c->stop | c->brk)) return;
+  if (c->flags) {
+    c->checkflags |= c->flags;
+    c->flags = 0;
+    if (c->act & ACT_END) {
+      c->time = c->time_prev;
+      c->dt = c->dt_prev;
+      c->dtold = c->dtold_prev;
+    }
+    c->act = ACT_BRK;
+  }
+}
+__global__ void bt_subcheck_kernel(Ctl* c) { bt_subcheck_body(c); }
+
 // CalcTimestep's closing arithmetic after the step's closing RHS and ghost-cell pass
 // (timedisc_base.f90:885-909, the sources list's viscous limit), CheckData's break, and the
 // count of completed fosite steps.
 __device__ void bt_finish_body(Ctl* c, int nd) {
-  if ((c->stop | c->brk) || !(c->act & ACT_END)) return;
+  if (c->stop | c->brk) return;
+  if (c->act & ACT_BRK) {
+    c->brk = 1;
+    return;
+  }
+  if (!(c->act & ACT_END)) return;
   auto D = [](unsigned long long b) { return __longlong_as_double((long long)b); };
   const double invdt = nd == 2 ? D(c->invdt[0]) : dmax(dmax(D(c->invdt[1]), D(c->invdt[2])), D(c->invdt[0]));
   const double ivis = D(c->invdt[3]);
@@ -135,6 +163,10 @@ __global__ void bt_finish_kernel(Ctl* c, int nd) { bt_finish_body(c, nd); }
 
 // ---- batches of grids with embedded schemes: one thread per member for the scalar work,
 // block tables (member, block, blocks of the member) for the per-cell passes
+__global__ void bt_subcheck_batch_kernel(Ctl* const* ctls, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) bt_subcheck_body(ctls[i]);
+}
 __global__ void bt_begin_batch_kernel(Ctl* const* ctls, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) bt_begin_body(ctls[i]);

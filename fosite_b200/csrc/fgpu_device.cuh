@@ -31,6 +31,10 @@ struct Grid {
   int fdir;            // FARGO transport direction: 1 along x (w by padded j), 2 along y (w by padded i)
 };
 
+// CheckData's CHECK_INVALID test of one value (timedisc_base.f90:1716-1725): NaN or above
+// HUGE (negative infinity passes, as in the reference)
+__device__ __forceinline__ bool invalid_value(double x) { return x != x || x > DBL_MAX; }
+
 // FARGO: index of a cell's background velocity (padded j for transport along x, padded i
 // along y); the transported momentum is component fdir of the state (1 x, 2 y)
 __device__ __forceinline__ int fargo_ix(const Grid& g, int i, int j) { return (g.fdir == 1 ? j : i) + 2; }
@@ -145,10 +149,12 @@ struct Ctl {
   int phase;                     // 0: next slot starts a fosite step, 1: inside IntegrationStep
   int rhs_done;                  // AcceptSolution evaluated the RHS at t (rhs_done_at_t)
   int checkflags;                // CheckData failures seen (FGPU_CHECK_* bits)
+  double time_prev, dt_prev, dtold_prev;   // the step's time, dt, dtold before a slot closed it
 };
 
 // actions of a device-clock attempt slot, decided by bt_decide_kernel
-enum { ACT_ATTEMPT = 1, ACT_REJECT = 2, ACT_SUB = 4, ACT_END = 8, ACT_COPY = 16 };
+// (ACT_BRK: CheckData failed inside the step; the slot ends with a break)
+enum { ACT_ATTEMPT = 1, ACT_REJECT = 2, ACT_SUB = 4, ACT_END = 8, ACT_COPY = 16, ACT_BRK = 32 };
 // a kernel of a slot runs only if the slot's actions include one of its gate bits
 __device__ __forceinline__ bool gated_out(const Ctl* c, int gate) {
   return gate && c && !(c->act & gate);

@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(TX* TY) fargo_advect_kernel(const __grid_const
       if (EU && (A.checkdata & 0x02) && p[V - 1] < P.pmin) flags |= 0x02;
       if ((A.checkdata & 0x04) && p[0] < P.rhomin) flags |= 0x04;
       if (A.checkdata & 0x08)
-        for (int v = 0; v < V; ++v) if (!isfinite(p[v]) || !isfinite(c[v])) flags |= 0x08;
+        for (int v = 0; v < V; ++v) if (invalid_value(p[v]) || invalid_value(c[v])) flags |= 0x08;
       p[2] = p[2] - w;
       double v3[4];
       CE::cfl_cell(p, csc, M, ip, v3);
@@ -303,7 +303,7 @@ __global__ void __launch_bounds__(256) fargo_advect_x_kernel(const __grid_consta
     if (EU && (A.checkdata & 0x02) && p[V - 1] < P.pmin) flags |= 0x02;
     if ((A.checkdata & 0x04) && p[0] < P.rhomin) flags |= 0x04;
     if (A.checkdata & 0x08)
-      for (int v = 0; v < V; ++v) if (!isfinite(p[v]) || !isfinite(c[v])) flags |= 0x08;
+      for (int v = 0; v < V; ++v) if (invalid_value(p[v]) || invalid_value(c[v])) flags |= 0x08;
     p[1] = p[1] - w;
     double v3[4];
     CE::cfl_cell(p, csc, M, ipd, v3);

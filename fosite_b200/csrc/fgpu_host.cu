@@ -464,9 +464,11 @@ int launch_stage_t(fgpu_handle* h, StageArgs& A) {
   const Grid& g = h->g;
   const int kz = ND == 3 ? (g.nz + h->kchunk - 1) / h->kchunk : 1;
   // the warp-shuffle layout implements neither FARGO frame changes, the accretion rows, the
-  // viscous source, the device-clock gates nor the next Butcher stage's state formation
+  // viscous source, the device-clock gates, the next Butcher stage's state formation nor the
+  // CheckData-only epilogue
   const int variant =
-      (h->variant == 1 && (h->fargo || h->accrete || h->vis || A.gate || A.fnext_out)) ? 0 : h->variant;
+      (h->variant == 1 && (h->fargo || h->accrete || h->vis || A.gate || A.fnext_out || A.cfl_mode == 3))
+          ? 0 : h->variant;
   switch (variant) {
     case 1: {
       // warp-shuffle layout: 32 x 8 points per block, 30 x 6 output cells
@@ -1061,6 +1063,7 @@ int enqueue_k1(fgpu_handle* h, bool from_pre, bool cfl, bool rt, int checkdata, 
     A.out_base = base;
     A.checkdata = checkdata;
     if (cfl) A.cfl_mode = 2;
+    else if (checkdata) A.cfl_mode = 3;   // AcceptSolution's ComputeRHS inside the step
   } else {
     A.in = plain_state(base, false);
   }
@@ -1161,7 +1164,7 @@ int launch_fargo_chain_copy(fgpu_handle* h, const double* in, double* out, const
 // AddBackgroundVelocity (pre) before the boundary fill and SubtractBackgroundVelocity(w) after
 // the sources; cvar after the call (co-moving) goes to out_base
 int enqueue_k1_fargo(fgpu_handle* h, const double* in, const Chain& pre, bool rt, int checkdata, double* out_base,
-                     double t) {
+                     double t, bool check = false) {
   StageArgs A = base_args(h);
   A.out_mode = OUT_RHS;
   A.out = h->buf[2];
@@ -1170,7 +1173,22 @@ int enqueue_k1_fargo(fgpu_handle* h, const double* in, const Chain& pre, bool rt
   A.w_sub = fargo_wn(h);
   A.out_base = out_base;
   A.checkdata = checkdata;
+  if (check && checkdata) A.cfl_mode = 3;
   return launch_stage(h, A, RhsTime::host(t));
+}
+
+// CheckData of AcceptSolution's ComputeRHS inside a step: a failure breaks the step's loop
+// before the next attempt (timedisc_base.f90:676,926-931)
+int read_substep_check(fgpu_handle* h) {
+  if (!h->cfg.checkdata) return FGPU_OK;
+  if (int rc = read_ctl(h)) return rc;
+  if (h->h_ctl->flags) {
+    h->checkflags |= h->h_ctl->flags;
+    h->brk = true;
+    h->h_ctl->flags = 0;
+    CUDA_TRY(h, cudaMemsetAsync(&h->d_ctl->flags, 0, sizeof(int), h->stream));
+  }
+  return FGPU_OK;
 }
 
 int butcher_attempt(fgpu_handle* h, double t, double dtv, double& err) {
@@ -1323,12 +1341,17 @@ int butcher_integration_step(fgpu_handle* h) {
         if (h->fargo) {
           // cold = cvar = the accepted state framed by this ComputeRHS
           const Chain pre = chain_add(chain_none(), fargo_wn(h), 1.0);
-          if (int rc = enqueue_k1_fargo(h, h->buf[0], pre, h->roundtrip_cfg, h->cfg.checkdata, h->buf[1], t)) return rc;
+          if (int rc = enqueue_k1_fargo(h, h->buf[0], pre, h->roundtrip_cfg, h->cfg.checkdata, h->buf[1], t, true))
+            return rc;
           CUDA_TRY(h, cudaMemcpyAsync(bt_cvar(h), h->buf[1], sizeof(double) * h->V * h->g.n, cudaMemcpyDeviceToDevice,
                                       h->stream));
         } else if (int rc = enqueue_k1(h, true, false, h->roundtrip_cfg, h->cfg.checkdata, t)) {
           return rc;
         }
+        if (int rc = read_substep_check(h)) return rc;
+        // on a break the stored state is the accepted solution; with this ComputeRHS's round
+        // trip it gives cvar and pvar as fosite leaves them
+        if (h->brk) h->pre_rt = h->roundtrip_cfg;
         rhs_done_at_t = true;
       }
       h->iter++;
@@ -1998,8 +2021,11 @@ static int enqueue_bt_slot(fgpu_handle* h) {
     A.in = plain_state(P, h->roundtrip_cfg);
     A.out_base = base;
     A.checkdata = h->cfg.checkdata;
+    if (h->cfg.checkdata) A.cfl_mode = 3;
     A.gate = ACT_SUB;
     if (int rc = launch_stage(h, A, RhsTime::att(0.0))) return rc;
+    if (h->cfg.checkdata)
+      if (int rc = one([&] { bt_subcheck_kernel<<<1, 1, 0, h->stream>>>(c); })) return rc;
   }
   {   // the closing: cvar as AcceptSolution's ComputeRHS left it, then IntegrationStep's RHS
     const long long n = (long long)h->V * h->g.n;
@@ -2077,7 +2103,9 @@ static int bt_run(fgpu_handle* h, int64_t n, int64_t* done) {
   h->maxerrold = c->maxerrold; h->last_err = c->last_err; h->n_adj = c->n_adj;
   h->checkflags = c->checkflags;
   const int64_t steps = n - c->steps_left;
-  if (steps > 0) h->pre_rt = h->roundtrip_cfg;
+  // after a completed step, or a break inside one (the stored state then went through that
+  // step's ComputeRHS with the configured checks)
+  if (steps > 0 || h->brk) h->pre_rt = h->roundtrip_cfg;
   h->stats.attempts += (h->iter - it0) + (h->n_adj - adj0);
   h->stats.cell_updates += (h->iter - it0) * h->g.n;
   if (done) *done = steps;

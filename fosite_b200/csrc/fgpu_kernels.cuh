@@ -47,7 +47,8 @@ struct StageArgs {
   double* out_high;
   double tol_rel;
   double tol_abs[FGPU_MAXV];
-  // CFL/CheckData epilogue: 0 none, 1 on the OUT_SSPRK result, 2 on the input state
+  // CFL/CheckData epilogue: 0 none, 1 on the OUT_SSPRK result, 2 on the input state, 3 CheckData
+  // of the input state only (AcceptSolution's ComputeRHS inside a step)
   int cfl_mode;
   int cfl_roundtrip;       // the checked state gets the CHECK_PMIN round trip
   int checkdata;
@@ -642,7 +643,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
           if (EU && (A.checkdata & 0x02) && p[V - 1] < P.pmin) flags |= 0x02;
           if ((A.checkdata & 0x04) && p[0] < P.rhomin) flags |= 0x04;
           if (A.checkdata & 0x08)
-            for (int v = 0; v < V; ++v) if (!isfinite(p[v]) || !isfinite(c[v])) flags |= 0x08;
+            for (int v = 0; v < V; ++v) if (invalid_value(p[v]) || invalid_value(c[v])) flags |= 0x08;
         }
       }
       if (A.out_base) {
@@ -658,17 +659,19 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
           for (int v = 0; v < V; ++v) A.out_base[(long long)v * g.n + idx] = o[v];
         }
       }
-      if (A.cfl_mode == 2) {
+      if (A.cfl_mode >= 2) {
         double cs = EU ? PH::cs_of(pc, P) : M.cs[ip];
-        double v3[4];
-        CE::cfl_cell(pc, cs, M, ip, v3);
+        if (A.cfl_mode == 2) {
+          double v3[4];
+          CE::cfl_cell(pc, cs, M, ip, v3);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) cflv[q] = dmax(cflv[q], v3[q]);
+          for (int q = 0; q < 4; ++q) cflv[q] = dmax(cflv[q], v3[q]);
+        }
         if ((A.checkdata & 0x01) && !(cs > 0.)) flags |= 0x01;
         if (EU && (A.checkdata & 0x02) && pc[V - 1] < P.pmin) flags |= 0x02;
         if ((A.checkdata & 0x04) && pc[0] < P.rhomin) flags |= 0x04;
         if (A.checkdata & 0x08)
-          for (int v = 0; v < V; ++v) if (!isfinite(pc[v]) || !isfinite(cc[v])) flags |= 0x08;
+          for (int v = 0; v < V; ++v) if (invalid_value(pc[v]) || invalid_value(cc[v])) flags |= 0x08;
       }
       if (A.last_stage) {
         // high/low order solutions and ComputeError (timedisc_rkfehlberg.f90:198-265,

@@ -126,7 +126,7 @@ __device__ __forceinline__ void boundary_block(const BndArgs& A, const int blk, 
     double cs = EU ? PH::cs_of(p, A.ph) : M.cs[px];
     if ((A.checkdata & 0x01) && !(cs > 0.)) flags |= 0x01;
     if (A.checkdata & 0x08)
-      for (int v = 0; v < V; ++v) if (!isfinite(p[v]) || !isfinite(c[v])) flags |= 0x08;
+      for (int v = 0; v < V; ++v) if (invalid_value(p[v]) || invalid_value(c[v])) flags |= 0x08;
     to_comoving<ND, EU>(A.w_sub, A.g, px - 2, py - 2, p, c);
     double v3[4];
     CE::cfl_cell(p, cs, M, px, v3);
@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(256) interior_cfl_kernel(const __grid_constant
     if (EU && (A.checkdata & 0x02) && p[V - 1] < A.ph.pmin) flags |= 0x02;
     if ((A.checkdata & 0x04) && p[0] < A.ph.rhomin) flags |= 0x04;
     if (A.checkdata & 0x08)
-      for (int v = 0; v < V; ++v) if (!isfinite(p[v]) || !isfinite(c[v])) flags |= 0x08;
+      for (int v = 0; v < V; ++v) if (invalid_value(p[v]) || invalid_value(c[v])) flags |= 0x08;
     to_comoving<ND, EU>(A.w_sub, A.g, i, j, p, c);
     double v3[4];
     CE::cfl_cell(p, cs, M, i + 2, v3);

@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(32 * NW, 2) stage2_kernel(const __grid_constan
           if (EU && (A.checkdata & 0x02) && p[V - 1] < P.pmin) flags |= 0x02;
           if ((A.checkdata & 0x04) && p[0] < P.rhomin) flags |= 0x04;
           if (A.checkdata & 0x08)
-            for (int v = 0; v < V; ++v) if (!isfinite(p[v]) || !isfinite(cv[v])) flags |= 0x08;
+            for (int v = 0; v < V; ++v) if (invalid_value(p[v]) || invalid_value(cv[v])) flags |= 0x08;
         }
       }
       if (A.out_base) {
@@ -403,7 +403,7 @@ __global__ void __launch_bounds__(32 * NW, 2) stage2_kernel(const __grid_constan
         if (EU && (A.checkdata & 0x02) && pc[V - 1] < P.pmin) flags |= 0x02;
         if ((A.checkdata & 0x04) && pc[0] < P.rhomin) flags |= 0x04;
         if (A.checkdata & 0x08)
-          for (int v = 0; v < V; ++v) if (!isfinite(pc[v]) || !isfinite(cc[v])) flags |= 0x08;
+          for (int v = 0; v < V; ++v) if (invalid_value(pc[v]) || invalid_value(cc[v])) flags |= 0x08;
       }
       if (A.last_stage) {
 #pragma unroll

@@ -1321,7 +1321,8 @@ struct Oracle {
     }
     if ((bm & FGPU_CHECK_INVALID)) {
       for (long x = 0; x < NC * VNUM; ++x)
-        if (!std::isfinite(cv[x]) || !std::isfinite(pv[x])) { f |= FGPU_CHECK_INVALID; break; }
+        // timedisc_base.f90:1716-1725: NaN (x /= x) or above HUGE; negative infinity passes
+        if (cv[x] != cv[x] || pv[x] != pv[x] || cv[x] > HUGE_ || pv[x] > HUGE_) { f |= FGPU_CHECK_INVALID; break; }
     }
     if (f) { brk = true; checkflags |= f; }
   }

@@ -137,3 +137,39 @@ def test_butcher_steps_with_shuffle_layout_forced(host, monkeypatch):
     assert rc == 0 and done == 4
     assert g.status().time == o.status().time
     assert np.array_equal(g.get(abi.CVAR), o.get(abi.CVAR))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("host", [False, True])
+@pytest.mark.parametrize("name,frac", [("gauss3d_dopri_mc_prim", 0.999), ("gauss3d_dopri_mc_prim", 0.99),
+                                       ("khi_modeuler_adaptive2_mc_prim", 0.999), ("euler2d_rkf45", 0.999)])
+def test_checkdata_break_matches_oracle(name, frac, host, monkeypatch):
+    """CheckData breaks the step where fosite does: inside the step, at AcceptSolution's
+    ComputeRHS (timedisc_base.f90:926-931; the step then ends without its closing, time and dt
+    unchanged), or at the closing ComputeRHS.  CHECK_RHOMIN with rhomin just below the initial
+    minimum density provokes either; the break step, the bookkeeping and the state equal the
+    oracle's, on the device clock (fgpu_run) and on the host-controlled loop."""
+    if host:
+        monkeypatch.setenv("FGPU_BUTCHER_HOST", "1")
+    from fosite_b200.sim import Simulation
+    cfg, p, extra = CASES[name]()
+    cfg.rhomin = float(p[0].min()) * frac
+    o = pyoracle.Oracle(cfg)
+    o.set_state(abi.PVAR, p)
+    g = Simulation(cfg, exact=True)
+    g.set_state(abi.PVAR, p)
+    assert o.first_step() == 0 and g.first_step() == 0
+    for s in range(12):
+        ro = o.step()
+        rc, done = g.run(1)
+        assert rc == ro, (s, rc, ro)
+        assert done == (1 if ro == 0 else 0)
+        so, sg = o.status(), g.status()
+        assert (sg.time, sg.dt, sg.iter, sg.n_adj) == (so.time, so.dt, so.iter, so.n_adj), s
+        assert sg.checkflags == so.checkflags and sg.brk == so.brk
+        if ro != 0:
+            assert ro == abi.BREAK
+            assert np.array_equal(g.get(abi.CVAR), o.get(abi.CVAR))
+            break
+    else:
+        pytest.fail("no CheckData break")
