@@ -46,6 +46,12 @@ struct fgpu_batch {
   int ncblocks = 0;
   cudaGraphExec_t slot_graph = nullptr;
   std::vector<long long> adj0;
+  // FARGO members (fixed-step Shu-Osher): per-step background velocity (type 1), advection
+  // and the copy of w_new into w, over per-member tables and block tables
+  int fdir = 0;                  // the FARGO members' common transport direction, 0 = none
+  FargoWArgs* d_fw = nullptr;    int4* d_fwb = nullptr;  int nfwb = 0;
+  FargoAdvArgs* d_fa = nullptr;  int4* d_fab = nullptr;  int nfab = 0;
+  CopyArgs* d_fwc = nullptr;     int4* d_fwcb = nullptr; int nfwcb = 0;
 };
 
 namespace {
@@ -115,11 +121,37 @@ int launch_batched_boundary(fgpu_batch* b) {
   return FGPU_OK;
 }
 
+template <bool EU>
+void launch_batched_fargo_t(fgpu_batch* b, bool w) {
+  if (w) {
+    if (b->fdir == 1) batched_fargo_w_kernel<EU, 1><<<b->nfwb, 256, 0, b->stream>>>(b->d_fw, b->d_fwb);
+    else batched_fargo_w_kernel<EU, 2><<<b->nfwb, 256, 0, b->stream>>>(b->d_fw, b->d_fwb);
+  } else {
+    if (b->fdir == 1) batched_fargo_advect_kernel<EU, 1><<<b->nfab, 256, 0, b->stream>>>(b->d_fa, b->d_fab);
+    else batched_fargo_advect_kernel<EU, 2><<<b->nfab, FA_TX * FA_TY, 0, b->stream>>>(b->d_fa, b->d_fab);
+  }
+}
+
 int enqueue_batch_step(fgpu_batch* b) {
   const int n = (int)b->m.size();
+  // FARGO members: CalcBackgroundVelocity (type 1) before the stages, FargoAdvection and the
+  // closing pass after them, then w = w_new (the single-grid FARGO step's order)
+  if (b->nfwb) {
+    b->euler ? launch_batched_fargo_t<true>(b, true) : launch_batched_fargo_t<false>(b, true);
+    BCUDA_TRY(b, cudaGetLastError());
+  }
   for (int s = 0; s < b->order; ++s)
     if (int rc = launch_batched_stage(b, b->d_args + (size_t)s * n, b->variant)) return rc;
-  return launch_batched_boundary(b);
+  if (b->nfab) {
+    b->euler ? launch_batched_fargo_t<true>(b, false) : launch_batched_fargo_t<false>(b, false);
+    BCUDA_TRY(b, cudaGetLastError());
+  }
+  if (int rc = launch_batched_boundary(b)) return rc;
+  if (b->nfwcb) {
+    batched_copy_kernel<<<b->nfwcb, 256, 0, b->stream>>>(b->d_fwc, b->d_fwcb);
+    BCUDA_TRY(b, cudaGetLastError());
+  }
+  return FGPU_OK;
 }
 
 int build_batch_graph(fgpu_batch* b, int steps) {
@@ -438,7 +470,13 @@ int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
       if (h->cfg.method != h0->cfg.method || h->T.m != h0->T.m || h->T.order != h0->T.order)
         return fail(FGPU_EBADCFG, "embedded batch members differ in method or order");
     }
-    if (h->fargo) return fail(FGPU_EUNSUPPORTED, "batch members without FARGO transport");
+    if (h->fargo) {
+      if (h->butcher) return fail(FGPU_EUNSUPPORTED, "FARGO batch members with the fixed-step modified Euler scheme");
+      if (h->fargo_phase != 2)
+        return fail(FGPU_EBADCFG, "a FARGO member must take its first step alone (that step has its own frame changes)");
+      if (b->fdir && h->fdir != b->fdir) return fail(FGPU_EBADCFG, "FARGO batch members differ in transport direction");
+      b->fdir = h->fdir;
+    }
     if (h->accrete) return fail(FGPU_EUNSUPPORTED, "batch members without point-mass accretion");
     if (h->vis) return fail(FGPU_EUNSUPPORTED, "batch members without the viscosity source");
     if (!h->butcher && h->order < 2) return fail(FGPU_EUNSUPPORTED, "batch members of time order 2 or 3");
@@ -461,13 +499,43 @@ int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
   std::vector<StageArgs> args((size_t)(b->order + 1) * n);
   std::vector<BndArgs> bnd(n);
   std::vector<int4> tiles, bblocks;
+  std::vector<FargoWArgs> fw;
+  std::vector<FargoAdvArgs> fa;
+  std::vector<CopyArgs> fwc;
+  std::vector<int4> fwb, fab, fwcb;
   for (int i = 0; i < n; ++i) {
     fgpu_handle* h = b->m[i];
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) return fail(FGPU_ECUDA, "member stream");
+    const FargoStep F = h->fargo ? fargo_step_of(h) : FargoStep{};
     for (int s = 1; s <= b->order; ++s) {
-      StageArgs A = shu_osher_stage(h, s);
+      StageArgs A = h->fargo ? fargo_stage_args(h, F, s) : shu_osher_stage(h, s);
       A.kchunk = h->kchunk;
       args[(size_t)(s - 1) * n + i] = A;
+    }
+    if (h->fargo) {
+      const Grid& g = h->g;
+      if (F.dyn) {
+        const int k = (int)fw.size();
+        fw.push_back(fargo_w_args(h, F));
+        const int nb = h->fdir == 1 ? (g.ny + 4 + FX_WY - 1) / FX_WY : (g.nx + 4 + FW_WX - 1) / FW_WX;
+        for (int q = 0; q < nb; ++q) fwb.push_back(make_int4(k, q, 0, 0));
+        CopyArgs C;
+        C.src = F.Wn; C.dst = h->d_w; C.n = h->nw; C.ctl = h->d_ctl; C.gate = 0;
+        const int kc = (int)fwc.size();
+        fwc.push_back(C);
+        fwcb.push_back(make_int4(kc, 0, 1, 0));
+      }
+      const int ka = (int)fa.size();
+      fa.push_back(fargo_adv_args(h, F));
+      if (h->fdir == 1) {
+        const int nb = (int)std::max<long long>(1, std::min<long long>((g.n + 255) / 256, 148 * 8));
+        for (int q = 0; q < nb; ++q) fab.push_back(make_int4(ka, q, nb, 0));
+      } else {
+        const int chunk = fa.back().chunk;
+        const int gx = (g.nx + FA_TX - 1) / FA_TX, gy = (g.ny + FA_TY * chunk - 1) / (FA_TY * chunk);
+        for (int y = 0; y < gy; ++y)
+          for (int x = 0; x < gx; ++x) fab.push_back(make_int4(ka, x, y, 0));
+      }
     }
     StageArgs R = base_args(h);
     R.in = plain_state(h->buf[0], false);
@@ -476,7 +544,7 @@ int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
     R.ctl = nullptr;
     R.kchunk = h->kchunk;
     args[(size_t)b->order * n + i] = R;
-    bnd[i] = bnd_args(h, h->buf[0], h->roundtrip_cfg, FIN_STEP);
+    bnd[i] = h->fargo ? fargo_closing_bnd(h, F) : bnd_args(h, h->buf[0], h->roundtrip_cfg, FIN_STEP);
     const Grid& g = h->g;
     const int TY = b->nd == 2 ? 8 : 4;
     const int tx = (g.nx + 31) / 32, ty = (g.ny + TY - 1) / TY;
@@ -501,6 +569,20 @@ int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
   cudaMemcpyAsync(b->d_tiles, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice, b->stream);
   cudaMemcpyAsync(b->d_bblocks, bblocks.data(), sizeof(int4) * bblocks.size(), cudaMemcpyHostToDevice, b->stream);
   if (cudaStreamSynchronize(b->stream) != cudaSuccess) return fail(FGPU_ECUDA, "batch table upload");
+  if (!fa.empty()) {
+    auto up = [&](auto** dst, const auto& v) {
+      using T = typename std::decay_t<decltype(v)>::value_type;
+      if (v.empty()) return true;
+      if (cudaMalloc(dst, sizeof(T) * v.size()) != cudaSuccess) return false;
+      return cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+    };
+    if (!up(&b->d_fw, fw) || !up(&b->d_fwb, fwb) || !up(&b->d_fa, fa) || !up(&b->d_fab, fab) || !up(&b->d_fwc, fwc) ||
+        !up(&b->d_fwcb, fwcb))
+      return fail(FGPU_ENOMEM, "batch fargo tables");
+    b->nfwb = (int)fwb.size();
+    b->nfab = (int)fab.size();
+    b->nfwcb = (int)fwcb.size();
+  }
   if (b->embedded) { if (int rc = build_embedded_tables(b)) return fail(rc, b->err); }
   *out = b;
   return FGPU_OK;
@@ -517,7 +599,8 @@ void fgpu_batch_destroy(fgpu_batch* b) {
   if (b->h_ctls) cudaFreeHost(b->h_ctls);
   if (b->slot_graph) cudaGraphExecDestroy(b->slot_graph);
   for (void* p : {(void*)b->d_ctlp, (void*)b->d_btp, (void*)b->d_eargs, (void*)b->d_fargs, (void*)b->d_cargs,
-                  (void*)b->d_copy, (void*)b->d_ebnd, (void*)b->d_cblocks})
+                  (void*)b->d_copy, (void*)b->d_ebnd, (void*)b->d_cblocks, (void*)b->d_fw, (void*)b->d_fwb,
+                  (void*)b->d_fa, (void*)b->d_fab, (void*)b->d_fwc, (void*)b->d_fwcb})
     if (p) cudaFree(p);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;

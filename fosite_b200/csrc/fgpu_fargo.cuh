@@ -30,13 +30,13 @@ struct FargoWArgs {
 // then one thread per column adds them in order.
 constexpr int FW_WX = 8, FW_WY = 32, FW_RPT = 4, FW_WR = FW_WY * FW_RPT;
 template <bool EU>
-__global__ void __launch_bounds__(FW_WX* FW_WY) fargo_w_kernel(const __grid_constant__ FargoWArgs A) {
+__device__ __forceinline__ void fargo_w_body(const FargoWArgs& A, const int bx) {
   using CE = Cells<2, EU>;
   __shared__ double terms[FW_WR][FW_WX + 1];
   if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
   const Grid& g = A.g;
   const int tx = threadIdx.x % FW_WX, ty = threadIdx.x / FW_WX;
-  const int ip = blockIdx.x * FW_WX + tx;
+  const int ip = bx * FW_WX + tx;
   const bool valid = ip < g.nx + 4;
   const int i = ip - 2;
   const bool ghost = i < 0 || i >= g.nx;
@@ -67,6 +67,10 @@ __global__ void __launch_bounds__(FW_WX* FW_WY) fargo_w_kernel(const __grid_cons
   }
   if (ty == 0 && valid) A.w_out[ip] = wi / (double)g.ny;
 }
+template <bool EU>
+__global__ void __launch_bounds__(FW_WX* FW_WY) fargo_w_kernel(const __grid_constant__ FargoWArgs A) {
+  fargo_w_body<EU>(A, blockIdx.x);
+}
 
 // CalcBackgroundVelocity for direction 1 (timedisc_base.f90:2262-2282):
 //   w(j) = SUM_i pvar(i,j,vx)*wfactor(j) / INUM over the interior i, for every padded row j
@@ -76,13 +80,13 @@ __global__ void __launch_bounds__(FW_WX* FW_WY) fargo_w_kernel(const __grid_cons
 // them in i order, so the sum rounds like the reference loop.
 constexpr int FX_WX = 32, FX_WY = 8;
 template <bool EU>
-__global__ void __launch_bounds__(FX_WX* FX_WY) fargo_w_x_kernel(const __grid_constant__ FargoWArgs A) {
+__device__ __forceinline__ void fargo_w_x_body(const FargoWArgs& A, const int bx) {
   using CE = Cells<2, EU>;
   __shared__ double terms[FX_WY][FX_WX + 1];
   if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
   const Grid& g = A.g;
   const int tx = threadIdx.x % FX_WX, ty = threadIdx.x / FX_WX;
-  const int jp = blockIdx.x * FX_WY + ty;
+  const int jp = bx * FX_WY + ty;
   const bool valid = jp < g.ny + 4;
   const int j = jp - 2;
   const bool ghost = j < 0 || j >= g.ny;
@@ -109,6 +113,10 @@ __global__ void __launch_bounds__(FX_WX* FX_WY) fargo_w_x_kernel(const __grid_co
     __syncthreads();
   }
   if (tx == 0 && valid) A.w_out[jp] = wi / (double)g.nx;
+}
+template <bool EU>
+__global__ void __launch_bounds__(FX_WX* FX_WY) fargo_w_x_kernel(const __grid_constant__ FargoWArgs A) {
+  fargo_w_x_body<EU>(A, blockIdx.x);
 }
 
 struct FargoAdvArgs {
@@ -143,7 +151,7 @@ __device__ __forceinline__ double fargo_minmod(double a, double b) {
 // ComputeRHS's CheckData (real frame) and CalcTimestep's wave speeds
 // (co-moving frame) of the interior cells.
 template <bool EU, int TX, int TY>
-__global__ void __launch_bounds__(TX* TY) fargo_advect_kernel(const __grid_constant__ FargoAdvArgs A) {
+__device__ __forceinline__ void fargo_advect_body(const FargoAdvArgs& A, const int bx, const int by) {
   using PH = Phys<2, EU>;
   using CE = Cells<2, EU>;
   constexpr int V = PH::V;
@@ -154,8 +162,8 @@ __global__ void __launch_bounds__(TX* TY) fargo_advect_kernel(const __grid_const
   const PhysP& P = A.ph;
   const MetricP& M = A.mt;
   const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
-  const int i = blockIdx.x * TX + tx;
-  const int j0 = (blockIdx.y * TY + ty) * A.chunk;
+  const int i = bx * TX + tx;
+  const int j0 = (by * TY + ty) * A.chunk;
   const int j1 = min(g.ny, j0 + A.chunk);
   double cflv = 0.0, cflvis = 0.0;
   int flags = 0;
@@ -229,6 +237,10 @@ __global__ void __launch_bounds__(TX* TY) fargo_advect_kernel(const __grid_const
   double vals[4] = {cflv, 0.0, 0.0, cflvis};
   block_reduce_emit<NT>(vals, M.vis ? 4 : 1, flags, A.ctl->invdt, &A.ctl->flags, sred);
 }
+template <bool EU, int TX, int TY>
+__global__ void __launch_bounds__(TX* TY) fargo_advect_kernel(const __grid_constant__ FargoAdvArgs A) {
+  fargo_advect_body<EU, TX, TY>(A, blockIdx.x, blockIdx.y);
+}
 
 // FargoAdvectionX (timedisc_base.f90:1779-1914) for the interior cells, the same transport
 // along x with w(j): delxy = w*dt/dlx(IMIN), shift = NINT(delxy), delxy -= shift; the
@@ -238,7 +250,7 @@ __global__ void __launch_bounds__(TX* TY) fargo_advect_kernel(const __grid_const
 // writes the result to its shifted column; the closing ComputeRHS's CheckData and
 // CalcTimestep see that cell at the shifted column (its metric and sound speed).
 template <bool EU>
-__global__ void __launch_bounds__(256) fargo_advect_x_kernel(const __grid_constant__ FargoAdvArgs A) {
+__device__ __forceinline__ void fargo_advect_x_body(const FargoAdvArgs& A, const int b, const int nb) {
   using PH = Phys<2, EU>;
   using CE = Cells<2, EU>;
   constexpr int V = PH::V;
@@ -251,7 +263,7 @@ __global__ void __launch_bounds__(256) fargo_advect_x_kernel(const __grid_consta
   int flags = 0;
   const double dte = A.dt_host > 0. ? A.dt_host : (A.ctl->time + A.ctl->dt) - A.ctl->time;
   const double dlx0 = M.dlx[2];   // dlx(IMIN, j): the metric depends on i only
-  for (long long t = blockIdx.x * 256LL + threadIdx.x; t < g.n; t += (long long)gridDim.x * 256) {
+  for (long long t = b * 256LL + threadIdx.x; t < g.n; t += (long long)nb * 256) {
     const int i = (int)(t % g.nx), j = (int)(t / g.nx);
     const double w = A.w[j + 2];
     double d = w * dte / dlx0;
@@ -312,6 +324,30 @@ __global__ void __launch_bounds__(256) fargo_advect_x_kernel(const __grid_consta
   }
   double vals[4] = {cflv, 0.0, 0.0, cflvis};
   block_reduce_emit<256>(vals, M.vis ? 4 : 1, flags, A.ctl->invdt, &A.ctl->flags, sred);
+}
+template <bool EU>
+__global__ void __launch_bounds__(256) fargo_advect_x_kernel(const __grid_constant__ FargoAdvArgs A) {
+  fargo_advect_x_body<EU>(A, blockIdx.x, gridDim.x);
+}
+
+// Batches of FARGO grids: the same passes over per-member argument tables, one block per
+// (member, block) entry of a block table (x: member, y/z: block coordinates or, along x, the
+// block and the member's block count); every FARGO member of a batch transports along the
+// same direction (DIR)
+template <bool EU, int DIR>
+__global__ void __launch_bounds__(256) batched_fargo_w_kernel(const FargoWArgs* __restrict__ args,
+                                                              const int4* __restrict__ blocks) {
+  const int4 T = blocks[blockIdx.x];
+  if constexpr (DIR == 1) fargo_w_x_body<EU>(args[T.x], T.y);
+  else fargo_w_body<EU>(args[T.x], T.y);
+}
+constexpr int FA_TX = 32, FA_TY = 4;   // the along-y transport's block of a batch
+template <bool EU, int DIR>
+__global__ void __launch_bounds__(DIR == 1 ? 256 : FA_TX* FA_TY) batched_fargo_advect_kernel(
+    const FargoAdvArgs* __restrict__ args, const int4* __restrict__ blocks) {
+  const int4 T = blocks[blockIdx.x];
+  if constexpr (DIR == 1) fargo_advect_x_body<EU>(args[T.x], T.y, T.z);
+  else fargo_advect_body<EU, FA_TX, FA_TY>(args[T.x], T.y, T.z);
 }
 
 // out = the frame-change chain C applied to every interior cell of the conservative state in

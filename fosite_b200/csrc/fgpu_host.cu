@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <map>
 #include <mutex>
+#include <type_traits>
 #include <cstdlib>
 #include "../../include/fosite_gpu.h"
 #include "fgpu_kernels_misc.cuh"
@@ -945,76 +946,111 @@ int launch_fargo_advect_args(fgpu_handle* h, const FargoAdvArgs& X) {
     return FGPU_OK;
   });
 }
-int launch_fargo_advect(fgpu_handle* h, const double* in, double* out, const double* w) {
+
+// The arguments of one FARGO step's passes (shared by the single-grid step and batches):
+// the background velocity of the step, stage n of the Shu-Osher update, the advection and the
+// closing ghost-cell pass.  W is the background velocity of the last ComputeRHS, Wn the step's.
+struct FargoStep {
+  double* P;
+  const double* W;
+  double* Wn;
+  bool dyn;        // type 1: w_new computed from the state; type 2: the user's w stays
+  Chain pre;       // the stored state's frame (the last ComputeRHS's AddBackgroundVelocity)
+};
+FargoStep fargo_step_of(fgpu_handle* h) {
+  FargoStep F;
+  F.P = h->buf[0];
+  F.W = h->d_w;
+  F.dyn = h->cfg.fargo_method == 1;
+  F.Wn = F.dyn ? h->d_w + h->nw : h->d_w;
+  F.pre = fargo_pre(h);
+  return F;
+}
+FargoWArgs fargo_w_args(fgpu_handle* h, const FargoStep& F) {
+  FargoWArgs X;
+  std::memset(&X, 0, sizeof(X));
+  X.g = h->g; X.ph = h->ph; X.mt = h->mt;
+  X.in = plain_state(F.P, false);
+  X.in.pre = F.pre;
+  X.w_prev = F.W;
+  X.wfac = fargo_wfac(h);
+  X.w_out = F.Wn;
+  X.ctl = h->d_ctl;
+  return X;
+}
+StageArgs fargo_stage_args(fgpu_handle* h, const FargoStep& F, int n) {
+  double* Abuf = h->buf[1];
+  double* Bbuf = h->buf[2];
+  // after FirstStep an ideal-gas cvar is the CHECK_ALL round trip of the stored state
+  Chain cold = chain_add(F.pre, F.W, -1.0);
+  if (h->pre_rt) cold.rt = 1;
+  const double* in = n == 1 ? F.P : ((n - 1) % 2 == 1 ? Abuf : Bbuf);
+  StageArgs A = base_args(h);
+  A.in = plain_state(in, n == 1 && h->pre_rt);
+  if (n == 1) {
+    A.in.pre = F.pre;
+    A.w_sub = F.W;
+    // type 1: CalcBackgroundVelocity adds w and the step subtracts w_new; type 2: cvar
+    // is already co-moving, the step's SubtractBackgroundVelocity does nothing
+    A.yn_chain = F.dyn ? chain_add(chain_add(cold, F.W, 1.0), F.Wn, -1.0) : cold;
+  } else {
+    A.in.pre = chain_add(chain_none(), F.Wn, 1.0);
+    A.w_sub = F.Wn;
+    A.yn_chain = chain_add(A.in.pre, F.Wn, -1.0);
+  }
+  A.out_mode = OUT_SSPRK;
+  A.eta = kEta[h->order - 1][n - 1];
+  A.y0 = F.P;
+  A.y0_chain = cold;
+  A.dt_dev = &h->d_ctl->dt;
+  A.out = (n % 2 == 1) ? Abuf : Bbuf;
+  return A;
+}
+// the last stage's result, which the advection transports into P
+const double* fargo_last_stage_out(const fgpu_handle* h) { return (h->order % 2 == 1) ? h->buf[1] : h->buf[2]; }
+FargoAdvArgs fargo_adv_args(fgpu_handle* h, const FargoStep& F) {
   FargoAdvArgs X;
   std::memset(&X, 0, sizeof(X));
   X.g = h->g; X.ph = h->ph; X.mt = h->mt;
-  X.in = plain_state(in, false);
-  X.w = w;
-  X.out = out;
+  X.in = plain_state(fargo_last_stage_out(h), false);
+  X.w = F.Wn;
+  X.out = F.P;
   X.ctl = h->d_ctl;
   X.checkdata = h->cfg.checkdata;
   X.chunk = 8;
-  return launch_fargo_advect_args(h, X);
+  return X;
+}
+BndArgs fargo_closing_bnd(fgpu_handle* h, const FargoStep& F) {
+  BndArgs B = bnd_args(h, F.P, false, FIN_STEP);
+  B.in.pre = chain_add(chain_none(), F.Wn, 1.0);
+  B.w_sub = F.Wn;
+  return B;
 }
 
 // One fosite%Step with FARGO transport (timedisc_base.f90:649-750 with the
 // modified-Euler SolveODE, timedisc_modeuler.f90:279-291):
 //   CalcBackgroundVelocity -> w_new; the Shu-Osher stages on the co-moving
-//   state; FargoAdvectionY; the closing ComputeRHS's CheckData and
+//   state; FargoAdvection; the closing ComputeRHS's CheckData and
 //   CalcTimestep.  The in-place frame changes of cvar are carried as chains:
 //   fosite's cvar at stage 1 is pre + [-w, +w, -w_new] applied to the stored
 //   state, cold is pre + [-w], later stages read the previous stage's result
-//   with [+w_new] (ComputeRHS's AddBackgroundVelocityY) and their Shu-Osher
+//   with [+w_new] (ComputeRHS's AddBackgroundVelocity) and their Shu-Osher
 //   base is [+w_new, -w_new].
 int enqueue_fargo_step(fgpu_handle* h) {
-  double* P = h->buf[0];
-  double* Abuf = h->buf[1];
-  double* Bbuf = h->buf[2];
-  const double* W = h->d_w;
-  const bool dyn = h->cfg.fargo_method == 1;   // type 2 keeps the user's w: no recomputation
-  double* Wn = dyn ? h->d_w + h->nw : h->d_w;
-  const Chain pre = fargo_pre(h);
-  if (dyn) {
-    StateRef S = plain_state(P, false);
-    S.pre = pre;
-    if (int rc = launch_fargo_w(h, S, W, Wn)) return rc;
+  const FargoStep F = fargo_step_of(h);
+  if (F.dyn) {
+    const FargoWArgs X = fargo_w_args(h, F);
+    if (int rc = launch_fargo_w(h, X.in, X.w_prev, X.w_out)) return rc;
   }
-  // after FirstStep an ideal-gas cvar is the CHECK_ALL round trip of the stored state
-  Chain cold = chain_add(pre, W, -1.0);
-  if (h->pre_rt) cold.rt = 1;
-  const double* in = P;
   for (int n = 1; n <= h->order; ++n) {
-    StageArgs A = base_args(h);
-    A.in = plain_state(in, n == 1 && h->pre_rt);
-    if (n == 1) {
-      A.in.pre = pre;
-      A.w_sub = W;
-      // type 1: CalcBackgroundVelocity adds w and the step subtracts w_new; type 2: cvar
-      // is already co-moving, the step's SubtractBackgroundVelocityY does nothing
-      A.yn_chain = dyn ? chain_add(chain_add(cold, W, 1.0), Wn, -1.0) : cold;
-    } else {
-      A.in.pre = chain_add(chain_none(), Wn, 1.0);
-      A.w_sub = Wn;
-      A.yn_chain = chain_add(A.in.pre, Wn, -1.0);
-    }
-    A.out_mode = OUT_SSPRK;
-    A.eta = kEta[h->order - 1][n - 1];
-    A.y0 = P;
-    A.y0_chain = cold;
-    A.dt_dev = &h->d_ctl->dt;
-    double* out = (n % 2 == 1) ? Abuf : Bbuf;
-    A.out = out;
+    StageArgs A = fargo_stage_args(h, F, n);
     if (int rc = launch_stage(h, A)) return rc;
     if (int rc = launch_accrete(h, n)) return rc;
-    in = out;
   }
-  if (int rc = launch_fargo_advect(h, in, P, Wn)) return rc;
-  BndArgs B = bnd_args(h, P, false, FIN_STEP);
-  B.in.pre = chain_add(chain_none(), Wn, 1.0);
-  B.w_sub = Wn;
+  if (int rc = launch_fargo_advect_args(h, fargo_adv_args(h, F))) return rc;
+  BndArgs B = fargo_closing_bnd(h, F);
   if (int rc = launch_misc(h, 0, B)) return rc;
-  if (dyn) CUDA_TRY(h, cudaMemcpyAsync(h->d_w, Wn, sizeof(double) * h->nw, cudaMemcpyDeviceToDevice, h->stream));
+  if (F.dyn) CUDA_TRY(h, cudaMemcpyAsync(h->d_w, F.Wn, sizeof(double) * h->nw, cudaMemcpyDeviceToDevice, h->stream));
   h->fargo_phase = 2;
   h->pre_rt = h->roundtrip_cfg;
   return FGPU_OK;

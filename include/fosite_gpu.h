@@ -283,7 +283,9 @@ int fgpu_stage_layout(const fgpu_handle* h, int* variant, int* kchunk);
  * Prince, Fehlberg, Cash-Karp, SSPRK; each member keeps its own tolerances,
  * error norm and step-size controller, advanced attempt by attempt on the
  * device), the same dimensionality, physics and reconstruction variables, no
- * FARGO, accretion or viscosity, on one device; mesh sizes, geometry, limiters,
+ * accretion or viscosity, on one device; fixed-step members may use FARGO (one
+ * transport direction per batch; such a member takes its first step after
+ * fgpu_first_step alone, as that step has its own frame changes); mesh sizes, geometry, limiters,
  * boundaries and physical parameters may differ.  Each member keeps its own
  * dt, time and stop state (a member that reached its stop time idles), and its
  * results are bitwise those of stepping it alone.  The handles stay owned by

@@ -222,3 +222,78 @@ def test_embedded_batch_equals_lone_runs_and_oracle():
         s.run(3)
     for m, s in zip(members, alone):
         assert np.array_equal(m.get(abi.CVAR), s.get(abi.CVAR))
+
+
+def _fargo_member(sp, fargo, exact):
+    """A disk with FARGO transport (type 1, or type 2 with the Keplerian w) after FirstStep and
+    one step alone (the first step after FirstStep has its own frame changes)."""
+    from fosite_b200.sim import Simulation
+    nr, nphi, geometry, hratio, sigma, seed = sp
+    cfg, p, extra = problems.disk2d(nr=nr, nphi=nphi, seed=seed, hratio=hratio, sigma_index=sigma,
+                                    geometry=geometry, fargo=fargo)
+    s = Simulation(cfg, exact=exact)
+    shape = (1, nphi + 4, nr + 4)
+    s.set_sound_speeds(np.broadcast_to(extra["bccsound"], shape), np.broadcast_to(extra["fcsound"], (4,) + shape))
+    if fargo == 2:
+        X, _, _, _ = problems.centers(cfg)
+        x = X[0, 0, :]
+        r = np.exp(x) if geometry == abi.LOGCYLINDRICAL else x
+        s.set_fargo_velocity(np.sqrt(1.0 / r))
+    s.set_state(abi.PVAR, p)
+    assert s.first_step() == 0
+    assert s.step() == 0
+    return s
+
+
+@pytest.mark.parametrize("exact", [True, False])
+def test_fargo_disk_batch_matches_single_grids(exact):
+    """FARGO members (types 1 and 2, cylindrical and logcylindrical, mixed with a member
+    without FARGO): background velocity, advection and w update over the batch's tables give
+    every member exactly its lone run."""
+    from fosite_b200.sim import Batch
+    specs = _disk_specs(6, seed=13)
+    kinds = [1, 1, 2, 1, 0, 2]
+    members = [_fargo_member(sp, f, exact) for sp, f in zip(specs, kinds)]
+    alone = [_fargo_member(sp, f, exact) for sp, f in zip(specs, kinds)]
+    b = Batch(members)
+    assert b.run(21) == len(members)
+    for s in alone:
+        rc, done = s.run(21)
+        assert rc == 0 and done == 21
+    for m, s in zip(members, alone):
+        assert (m.status().iter, m.status().time, m.status().dt) == (s.status().iter, s.status().time, s.status().dt)
+        assert np.array_equal(m.get(abi.CVAR), s.get(abi.CVAR))
+        assert np.array_equal(m.get(abi.PVAR), s.get(abi.PVAR))
+    b.close()
+
+
+def test_fargo_x_batch_and_rejections():
+    """FARGO along x (the reference's KHI2D legs, ideal gas) in a batch equals the lone runs;
+    members must have stepped once alone and share the transport direction."""
+    from fosite_b200.sim import Batch, FositeError, Simulation
+    from cases import khi_fargo
+
+    def member(fargo, direction, step=True):
+        cfg, p, extra = khi_fargo(fargo, direction=direction, n=(24, 26))
+        s = Simulation(cfg, exact=True)
+        if "fargo_w" in extra:
+            s.set_fargo_velocity(extra["fargo_w"])
+        s.set_state(abi.PVAR, p)
+        assert s.first_step() == 0
+        if step:
+            assert s.step() == 0
+        return s
+
+    members = [member(1, 1), member(2, 1)]
+    alone = [member(1, 1), member(2, 1)]
+    b = Batch(members)
+    assert b.run(19) == 2
+    for m, s in zip(members, alone):
+        assert s.run(19) == (0, 19)
+        assert m.status().time == s.status().time
+        assert np.array_equal(m.get(abi.CVAR), s.get(abi.CVAR))
+    b.close()
+    with pytest.raises(FositeError):
+        Batch([member(1, 1, step=False)])        # first step after FirstStep not taken alone
+    with pytest.raises(FositeError):
+        Batch([member(1, 1), member(1, 2)])      # different transport directions
