@@ -178,15 +178,28 @@ double time_launches(cudaStream_t s, int reps, F&& fn) {
   cudaEventCreate(&a);
   cudaEventCreate(&z);
   fn();   // warm-up (first-touch, instruction cache)
-  cudaEventRecord(a, s);
-  for (int r = 0; r < reps; ++r) fn();
-  cudaEventRecord(z, s);
-  cudaEventSynchronize(z);
-  float ms = 0.f;
-  cudaEventElapsedTime(&ms, a, z);
+  auto run = [&](int n) {
+    cudaEventRecord(a, s);
+    for (int r = 0; r < n; ++r) fn();
+    cudaEventRecord(z, s);
+    cudaEventSynchronize(z);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, z);
+    return (double)ms;
+  };
+  double total = run(reps);
+  // short launches (small grids): repeat until the timed run lasts about 2 ms, so that the
+  // layouts' differences are not lost in event and launch jitter
+  if (total > 0.0 && total < 2.0) {
+    const int more = std::min(400, (int)std::ceil(2.0 / (total / reps)));
+    if (more > reps) {
+      reps = more;
+      total = run(reps);
+    }
+  }
   cudaEventDestroy(a);
   cudaEventDestroy(z);
-  return (double)ms / reps;
+  return total / reps;
 }
 
 // ---- embedded-scheme batches
