@@ -288,7 +288,7 @@ def run_own(args, world, rank, local):
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded, BASELINE config shapes)",
+        "data": "synthetic (seeded inputs of the workload's shapes and value distributions)",
         "config": {"workload": args.workload, "description": WORKLOADS[args.workload],
                    "grid": [cfg.inum, cfg.jnum, cfg.knum], "parallelism": "replicas x%d" % world,
                    "l2": "inputs larger than L2: each state array is %.0f MB" % (n_cells * sim.vnum * 8 / 1e6),
