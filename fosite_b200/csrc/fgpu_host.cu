@@ -1132,9 +1132,17 @@ double adjust_timestep(fgpu_handle* h, double maxerr, double dtold_) {
 //   order 3: s2 = update(eta2, base, s1, rhs(s1)), low = update(1/2, base, s1, rhs(s1))
 //            P  = update(eta3, base, s2, rhs(s2)),  err = ComputeError(P, low)
 //   order 2: P  = update(eta2, base, s1, rhs(s1)),  err = ComputeError(P, s1)
+const double* fargo_wn(const fgpu_handle* h);
+double* bt_cvar(const fgpu_handle* h);
+
 int modeuler_attempt(fgpu_handle* h, double t, double dtv, double& err) {
+  // timedisc_modeuler.f90:125-195 with tol_rel < 1: cvar -> ctmp (stage 1), the RHS of ctmp,
+  // cvar and the embedded solution from it, the RHS of cvar, cvar (stage 3); with FARGO each
+  // ComputeRHS frames its state vector in place (AddBackgroundVelocity only once the vector
+  // carries the frame flag) and the updates read the framed vectors
   double* P = h->buf[0];
-  double* base = h->buf[1];
+  double* base = h->buf[1];      // cold
+  double* cv = bt_cvar(h);       // cvar (cold itself without FARGO)
   double* K1 = h->buf[2];
   double* S1 = h->buf[3];
   double* S2 = h->buf[4];
@@ -1146,7 +1154,7 @@ int modeuler_attempt(fgpu_handle* h, double t, double dtv, double& err) {
     unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148 * 8);
     const double e1 = kEta[ord - 1][0];
     int rc = timed_launch(h, 0, 0.0, [&] {
-      shu_osher_update_kernel<<<blocks, 256, 0, h->stream>>>(base, base, K1, S1, n, e1, dtv, nullptr, nullptr, 0);
+      shu_osher_update_kernel<<<blocks, 256, 0, h->stream>>>(base, cv, K1, S1, n, e1, dtv, nullptr, nullptr, 0);
       CUDA_TRY(h, cudaGetLastError());
       return FGPU_OK;
     });
@@ -1155,6 +1163,14 @@ int modeuler_attempt(fgpu_handle* h, double t, double dtv, double& err) {
   for (int n = 2; n <= ord; ++n) {
     StageArgs A = base_args(h);
     A.in = plain_state(n == 2 ? S1 : S2, false);
+    if (h->fargo) {
+      // n = 2 reads ctmp (its own frame flag), n = 3 cvar
+      const Chain pre = (n == 2 && h->fargo_tmp_fresh) ? chain_none() : chain_add(chain_none(), fargo_wn(h), 1.0);
+      A.in.pre = pre;
+      A.w_sub = fargo_wn(h);
+      A.yn_chain = chain_add(pre, fargo_wn(h), -1.0);
+      if (n == 2) h->fargo_tmp_fresh = false;
+    }
     A.out_mode = OUT_SSPRK;
     A.eta = kEta[ord - 1][n - 1];
     A.y0 = base;
@@ -1525,8 +1541,8 @@ int validate(fgpu_handle* h) {
     if (h->roundtrip_cfg)
       return set_err(h, FGPU_EUNSUPPORTED, "fargo with ideal-gas physics: checkdata without CHECK_PMIN "
                                            "(its round trip sits between the frame changes)");
-    if (h->adaptive_me)
-      return set_err(h, FGPU_EUNSUPPORTED, "fargo: modified Euler with embedded error control not supported");
+    if (h->adaptive_me && h->order != 3)
+      return set_err(h, FGPU_EUNSUPPORTED, "fargo: modified Euler with embedded error control of order 3 only");
     h->fargo = true;
   }
   if (c.vismodel != 0) {
