@@ -1169,6 +1169,8 @@ int modeuler_attempt(fgpu_handle* h, double t, double dtv, double& err) {
       A.in.pre = pre;
       A.w_sub = fargo_wn(h);
       A.yn_chain = chain_add(pre, fargo_wn(h), -1.0);
+      // order 2 compares with ctmp itself, which this stage's ComputeRHS framed
+      if (n == ord && ord == 2) A.err_chain = A.yn_chain;
       if (n == 2) h->fargo_tmp_fresh = false;
     }
     A.out_mode = OUT_SSPRK;
@@ -1541,8 +1543,6 @@ int validate(fgpu_handle* h) {
     if (h->roundtrip_cfg)
       return set_err(h, FGPU_EUNSUPPORTED, "fargo with ideal-gas physics: checkdata without CHECK_PMIN "
                                            "(its round trip sits between the frame changes)");
-    if (h->adaptive_me && h->order != 3)
-      return set_err(h, FGPU_EUNSUPPORTED, "fargo: modified Euler with embedded error control of order 3 only");
     h->fargo = true;
   }
   if (c.vismodel != 0) {

@@ -65,6 +65,7 @@ struct StageArgs {
   double* out2;
   double eta2;
   const double* err_low;
+  Chain err_chain;         // FARGO: frame changes of err_low before the comparison
   // point-mass accretion: the boundary row of this RHS through the outbound x face,
   // (dy*dz)*xflux of the density (face 0 west) or -(dy*dz)*xflux (face 1 east), by j
   double* brow;
@@ -621,10 +622,14 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
             A.out2[(long long)v * g.n + idx] = yn[v] - dt * rhs[v] + A.eta2 * (y0[v] - yn[v] + dt * rhs[v]);
         }
         if (A.err_low) {
+          double l[V];
+#pragma unroll
+          for (int v = 0; v < V; ++v) l[v] = __ldg(A.err_low + (long long)v * g.n + idx);
+          // FARGO: the low-order solution as its ComputeRHS framed it in place
+          if (FG && A.err_chain.n) apply_chain<V>(A.err_chain, l, g, i, j);
 #pragma unroll
           for (int v = 0; v < V; ++v) {
-            const double l = __ldg(A.err_low + (long long)v * g.n + idx);
-            const double e = fabs(y[v] - l) / (A.tol_rel * fabs(y[v]) + A.tol_abs[v]);
+            const double e = fabs(y[v] - l[v]) / (A.tol_rel * fabs(y[v]) + A.tol_abs[v]);
             errv = dmax(errv, e);
           }
         }

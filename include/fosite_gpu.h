@@ -152,8 +152,8 @@ typedef struct fgpu_config {
     /* fargo transport (timedisc_base.f90:369-452): method 0 off, 1 background velocity
      * computed every step, 2 fixed user-supplied background velocity
      * (fgpu_set_fargo_velocity); 2D x-y meshes (isothermal or ideal gas without CHECK_PMIN)
-     * with the fixed-step modified Euler scheme, an embedded Butcher scheme or the embedded
-     * modified Euler scheme of order 3.  Type 3 (shearing box) is not available. */
+     * with the fixed-step or embedded modified Euler scheme or an embedded Butcher scheme.
+     * Type 3 (shearing box) is not available. */
     int32_t fargo_method;
     int32_t fargo_direction;       /* 1 transport along x, 2 along y */
     /* output clip time for AdjustTimestep (io/fileio_base.f90:604-621); 0 = stoptime */

@@ -386,6 +386,7 @@ CASES = {
     "khi_fargo1_x_cashkarp": lambda: _butcher(khi_fargo(1, n=(24, 26)), abi.CASH_KARP, 5, 1e-4),
     "disk_fargo_me3_adaptive": lambda: _butcher(_disk_fargo(n=(30, 40)), abi.MODIFIED_EULER, 3, 1e-3),
     "khi_fargo2_x_me3_adaptive": lambda: _butcher(khi_fargo(2, n=(26, 24)), abi.MODIFIED_EULER, 3, 1e-4),
+    "disk_fargo2_me2_adaptive": lambda: _butcher(_disk_fargo2(), abi.MODIFIED_EULER, 2, 1e-3),
     "khi_fargo2_x_visc": lambda: khi_fargo(2, n=(24, 26), visc=True),
     "iso_fargo1_x_shear": lambda: _iso_fargo_x(),
     "euler_fargo1_x_disk_cyl": lambda: _with(_euler_fargo(n=(24, 40), geometry=abi.CYLINDRICAL), fargo_direction=1),

@@ -61,14 +61,12 @@ def _cfg(**kw):
     (dict(method=9), abi.EBADCFG),
     (dict(jnum=1), abi.EUNSUPPORTED),
     (dict(fluxtype=2), abi.EBADCFG),
-    # FARGO: types 1 and 2 along x or y on 2D meshes; the embedded modified Euler scheme of order 3 only
+    # FARGO: types 1 and 2 along x or y on 2D meshes
     (dict(physics=abi.EULER_ISOTHERM, csiso=1.0, fargo_method=3, fargo_direction=2), abi.EUNSUPPORTED),
     (dict(physics=abi.EULER_ISOTHERM, csiso=1.0, fargo_method=1, fargo_direction=3), abi.EUNSUPPORTED),
     (dict(physics=abi.EULER_ISOTHERM, csiso=1.0, fargo_method=1, fargo_direction=1, pointmass=1, pm_outbound=1,
           geometry=abi.CYLINDRICAL, xmin=0.5, xmax=1.5), abi.EUNSUPPORTED),
     (dict(fargo_method=1, fargo_direction=2), abi.EUNSUPPORTED),
-    (dict(physics=abi.EULER_ISOTHERM, csiso=1.0, fargo_method=1, fargo_direction=2, method=abi.MODIFIED_EULER,
-          tdorder=2, tol_rel=1e-3), abi.EUNSUPPORTED),
 ])
 def test_bad_configs_rejected(kw, code):
     from fosite_b200.sim import lib_path
