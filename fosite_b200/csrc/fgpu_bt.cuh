@@ -31,7 +31,9 @@ struct BtParams {
 __device__ void bt_begin_body(Ctl* c) {
   c->act = 0;
   if (c->stop | c->brk) return;
+  int open = 0;
   if (c->phase == 0) {
+    open = ACT_OPEN;
     if (c->steps_left <= 0) return;
     if (fabs(c->stoptime - c->time) <= 1.0E-05 * c->stoptime) { c->stop = 1; return; }
     if ((c->time + c->dt) / c->tout > 1.0) { c->dt = c->tout - c->time; c->dtcause = -4; }
@@ -43,7 +45,7 @@ __device__ void bt_begin_body(Ctl* c) {
     c->phase = 1;
   }
   c->dtold_att = c->d_att;
-  c->act = ACT_ATTEMPT;
+  c->act = ACT_ATTEMPT | open;
 }
 __global__ void bt_begin_kernel(Ctl* c) { bt_begin_body(c); }
 
@@ -101,7 +103,7 @@ __device__ void bt_decide_body(Ctl* c, const BtParams& P) {
     c->time = c->t_loc;
     c->dtold = d;
     act |= ACT_END;
-    if (c->rhs_done) act |= ACT_COPY;
+    act |= c->rhs_done ? ACT_COPY : ACT_ENDNC;
   }
   c->act = act;
 }

@@ -153,8 +153,10 @@ struct Ctl {
 };
 
 // actions of a device-clock attempt slot, decided by bt_decide_kernel
-// (ACT_BRK: CheckData failed inside the step; the slot ends with a break)
-enum { ACT_ATTEMPT = 1, ACT_REJECT = 2, ACT_SUB = 4, ACT_END = 8, ACT_COPY = 16, ACT_BRK = 32 };
+// (ACT_BRK: CheckData failed inside the step; the slot ends with a break; ACT_OPEN: the slot
+// opens a fosite step; ACT_ENDNC: the step closes without AcceptSolution's RHS at its end)
+enum { ACT_ATTEMPT = 1, ACT_REJECT = 2, ACT_SUB = 4, ACT_END = 8, ACT_COPY = 16, ACT_BRK = 32, ACT_OPEN = 64,
+       ACT_ENDNC = 128 };
 // a kernel of a slot runs only if the slot's actions include one of its gate bits
 __device__ __forceinline__ bool gated_out(const Ctl* c, int gate) {
   return gate && c && !(c->act & gate);

@@ -17,6 +17,7 @@ struct FargoWArgs {
   const double* wfac;     // wfactor, by padded i (direction 2) or padded j (direction 1)
   double* w_out;          // new background velocity, indexed like wfac
   Ctl* ctl;
+  int gate;               // device-clock attempt slots: run only with one of these action bits
 };
 
 // CalcBackgroundVelocity for direction 2 (timedisc_base.f90:2243-2326):
@@ -34,6 +35,7 @@ __device__ __forceinline__ void fargo_w_body(const FargoWArgs& A, const int bx) 
   using CE = Cells<2, EU>;
   __shared__ double terms[FW_WR][FW_WX + 1];
   if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
+  if (gated_out(A.ctl, A.gate)) return;
   const Grid& g = A.g;
   const int tx = threadIdx.x % FW_WX, ty = threadIdx.x / FW_WX;
   const int ip = bx * FW_WX + tx;
@@ -84,6 +86,7 @@ __device__ __forceinline__ void fargo_w_x_body(const FargoWArgs& A, const int bx
   using CE = Cells<2, EU>;
   __shared__ double terms[FX_WY][FX_WX + 1];
   if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
+  if (gated_out(A.ctl, A.gate)) return;
   const Grid& g = A.g;
   const int tx = threadIdx.x % FX_WX, ty = threadIdx.x / FX_WX;
   const int jp = bx * FX_WY + ty;
@@ -130,6 +133,8 @@ struct FargoAdvArgs {
   int checkdata;
   int chunk;             // rows of one thread
   double dt_host;        // > 0: the transport's dt (IntegrationStep's this%dt); else (time+dt)-time of ctl
+  int dt_ctl;            // 1: the transport's dt is ctl->dt (an embedded scheme's closed step)
+  int gate;              // device-clock attempt slots: run only with one of these action bits
 };
 
 __device__ __forceinline__ double fargo_minmod(double a, double b) {
@@ -158,6 +163,7 @@ __device__ __forceinline__ void fargo_advect_body(const FargoAdvArgs& A, const i
   constexpr int NT = TX * TY;
   __shared__ double sred[RED_STRIDE * ((NT + 31) / 32)];
   if (A.ctl->stop | A.ctl->brk) return;
+  if (gated_out(A.ctl, A.gate)) return;
   const Grid& g = A.g;
   const PhysP& P = A.ph;
   const MetricP& M = A.mt;
@@ -170,7 +176,7 @@ __device__ __forceinline__ void fargo_advect_body(const FargoAdvArgs& A, const i
   if (i < g.nx && j0 < g.ny) {
     const int ip = i + 2;
     const double w = A.w[ip];
-    const double dte = A.dt_host > 0. ? A.dt_host : (A.ctl->time + A.ctl->dt) - A.ctl->time;
+    const double dte = A.dt_ctl ? A.ctl->dt : (A.dt_host > 0. ? A.dt_host : (A.ctl->time + A.ctl->dt) - A.ctl->time);
     double d = w * dte / M.dly[ip];
     const double sh = round(d);   // NINT: half away from zero
     const int s = (int)sh;
@@ -256,12 +262,13 @@ __device__ __forceinline__ void fargo_advect_x_body(const FargoAdvArgs& A, const
   constexpr int V = PH::V;
   __shared__ double sred[RED_STRIDE * 8];
   if (A.ctl->stop | A.ctl->brk) return;
+  if (gated_out(A.ctl, A.gate)) return;
   const Grid& g = A.g;
   const PhysP& P = A.ph;
   const MetricP& M = A.mt;
   double cflv = 0.0, cflvis = 0.0;
   int flags = 0;
-  const double dte = A.dt_host > 0. ? A.dt_host : (A.ctl->time + A.ctl->dt) - A.ctl->time;
+  const double dte = A.dt_ctl ? A.ctl->dt : (A.dt_host > 0. ? A.dt_host : (A.ctl->time + A.ctl->dt) - A.ctl->time);
   const double dlx0 = M.dlx[2];   // dlx(IMIN, j): the metric depends on i only
   for (long long t = b * 256LL + threadIdx.x; t < g.n; t += (long long)nb * 256) {
     const int i = (int)(t % g.nx), j = (int)(t / g.nx);
@@ -354,7 +361,9 @@ __global__ void __launch_bounds__(DIR == 1 ? 256 : FA_TX* FA_TY) batched_fargo_a
 // (2D): the in-place Add/SubtractBackgroundVelocity calls that IntegrationStep makes on cvar
 template <int V>
 __global__ void __launch_bounds__(256) fargo_chain_copy_kernel(const double* __restrict__ in, double* __restrict__ out,
-                                                               Grid g, Chain C) {
+                                                               Grid g, Chain C, const Ctl* ctl, int gate) {
+  if (ctl && gate && (ctl->stop | ctl->brk)) return;
+  if (gated_out(ctl, gate)) return;
   for (long long t = blockIdx.x * 256LL + threadIdx.x; t < g.n; t += (long long)gridDim.x * 256) {
     const int i = (int)(t % g.nx), j = (int)(t / g.nx);
     double c[V];

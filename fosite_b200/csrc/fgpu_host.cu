@@ -906,9 +906,10 @@ const double* fargo_wfac(const fgpu_handle* h) {
   return h->fdir == 1 ? h->d_w + 2 * (size_t)h->nw : h->d_metric + (size_t)M_wfac * h->nxp;
 }
 
-int launch_fargo_w(fgpu_handle* h, const StateRef& in, const double* w_prev, double* w_out) {
+int launch_fargo_w(fgpu_handle* h, const StateRef& in, const double* w_prev, double* w_out, int gate = 0) {
   FargoWArgs F;
   std::memset(&F, 0, sizeof(F));
+  F.gate = gate;
   F.g = h->g; F.ph = h->ph; F.mt = h->mt;
   F.in = in;
   F.w_prev = w_prev;
@@ -1202,12 +1203,13 @@ int modeuler_attempt(fgpu_handle* h, double t, double dtv, double& err) {
 const double* fargo_wn(const fgpu_handle* h) { return h->cfg.fargo_method == 1 ? h->d_w + h->nw : h->d_w; }
 double* bt_cvar(const fgpu_handle* h) { return h->fargo ? h->buf[2 + h->T.m] : h->buf[1]; }
 
-int launch_fargo_chain_copy(fgpu_handle* h, const double* in, double* out, const Chain& C) {
+int launch_fargo_chain_copy(fgpu_handle* h, const double* in, double* out, const Chain& C, int gate = 0) {
   const unsigned blocks = (unsigned)std::min<long long>((h->g.n + 255) / 256, 148 * 8);
+  const Ctl* ctl = gate ? h->d_ctl : nullptr;
   return timed_launch(h, false, 0.0, [&] {
     switch (h->V) {
-      case 3: fargo_chain_copy_kernel<3><<<blocks, 256, 0, h->stream>>>(in, out, h->g, C); break;
-      default: fargo_chain_copy_kernel<4><<<blocks, 256, 0, h->stream>>>(in, out, h->g, C); break;
+      case 3: fargo_chain_copy_kernel<3><<<blocks, 256, 0, h->stream>>>(in, out, h->g, C, ctl, gate); break;
+      default: fargo_chain_copy_kernel<4><<<blocks, 256, 0, h->stream>>>(in, out, h->g, C, ctl, gate); break;
     }
     CUDA_TRY(h, cudaGetLastError());
     return FGPU_OK;
@@ -1424,7 +1426,7 @@ int butcher_integration_step(fgpu_handle* h) {
     // CFL (co-moving) and CheckData (real frame) of the closing ComputeRHS
     const double* Wn = fargo_wn(h);
     double* src = rhs_done_at_t ? h->buf[1] : h->buf[0];
-    double* dst = rhs_done_at_t ? h->buf[0] : bt_cvar(h);
+    double* dst = rhs_done_at_t ? h->buf[0] : bt_cvar(h);   // then copied into P (fixed buffers)
     FargoAdvArgs X;
     std::memset(&X, 0, sizeof(X));
     X.g = h->g; X.ph = h->ph; X.mt = h->mt;
@@ -1436,7 +1438,8 @@ int butcher_integration_step(fgpu_handle* h) {
     X.chunk = 8;
     X.dt_host = dt_step;
     if (int rc = launch_fargo_advect_args(h, X)) return rc;
-    if (!rhs_done_at_t) std::swap(h->buf[0], h->buf[2 + h->T.m]);   // the advected state is the stored one
+    if (!rhs_done_at_t)
+      CUDA_TRY(h, cudaMemcpyAsync(h->buf[0], dst, sizeof(double) * h->V * h->g.n, cudaMemcpyDeviceToDevice, h->stream));
     const Chain pre = chain_add(chain_none(), Wn, 1.0);
     if (int rc = enqueue_k1_fargo(h, h->buf[0], pre, false, h->cfg.checkdata, h->buf[1], h->time)) return rc;
     if (h->cfg.fargo_method == 1)
@@ -1969,6 +1972,25 @@ static int enqueue_bt_slot(fgpu_handle* h) {
     });
   };
   if (int rc = one([&] { bt_begin_kernel<<<1, 1, 0, h->stream>>>(c); })) return rc;
+  // FARGO (after the run's first step, which the host loop takes): cvar of the attempts lives
+  // apart from cold; every ComputeRHS adds and subtracts the step's background velocity
+  const bool fg = h->fargo;
+  double* CV = bt_cvar(h);
+  const double* Wn = fg ? fargo_wn(h) : nullptr;
+  const Chain addWn = fg ? chain_add(chain_none(), Wn, 1.0) : chain_none();
+  const bool dyn = fg && h->cfg.fargo_method == 1;
+  if (fg) {
+    // IntegrationStep's opening: CalcBackgroundVelocity (type 1) and cvar = cold + w - w_new
+    if (dyn) {
+      const FargoStep F = fargo_step_of(h);
+      if (int rc = launch_fargo_w(h, fargo_w_args(h, F).in, F.W, F.Wn, ACT_OPEN)) return rc;
+      if (int rc = launch_fargo_chain_copy(h, base, CV, chain_add(chain_add(chain_none(), h->d_w, 1.0), Wn, -1.0),
+                                           ACT_OPEN))
+        return rc;
+    } else if (int rc = launch_fargo_chain_copy(h, base, CV, chain_none(), ACT_OPEN)) {
+      return rc;
+    }
+  }
   if (h->adaptive_me) {
     double* S1 = h->buf[3];
     double* S2 = h->buf[4];
@@ -1999,6 +2021,27 @@ static int enqueue_bt_slot(fgpu_handle* h) {
       A.gate = ACT_ATTEMPT;
       if (int rc = launch_stage(h, A, RhsTime::att(kZeta[ord - 1][m - 2]))) return rc;
     }
+  } else if (fg) {
+    // stage states formed in the stencil from cvar with their frame chain; the last stage
+    // forms the high/low-order solutions and the error norm
+    for (int m = 2; m <= T.m; ++m) {
+      StageArgs A = base_args(h);
+      A.in.base = CV;
+      A.in.nk = m - 1;
+      A.in.roundtrip = 0;
+      for (int q = 0; q < m - 1; ++q) {
+        A.in.K[q] = h->buf[2 + q];
+        A.in.coef[q] = T.A[(m - 1) * T.m + q];
+      }
+      A.in.dt_dev = d_att;
+      A.in.pre = addWn;
+      A.w_sub = Wn;
+      A.out_mode = OUT_RHS;
+      A.out = h->buf[2 + m - 1];
+      if (m == T.m) set_last_stage(h, A, P, 0.0);
+      A.gate = ACT_ATTEMPT;
+      if (int rc = launch_stage(h, A, RhsTime::att(T.c[m - 1]))) return rc;
+    }
   } else {
     for (int m = 2; m <= T.m; ++m) {
       StageArgs A = base_args(h);
@@ -2024,7 +2067,7 @@ static int enqueue_bt_slot(fgpu_handle* h) {
       if (int rc = launch_stage(h, A, RhsTime::att(T.c[m - 1]))) return rc;
     }
   }
-  if (h->butcher && !h->fuse_end) {
+  if (h->butcher && !h->fuse_end && !fg) {
     CombineArgs Cb;
     std::memset(&Cb, 0, sizeof(Cb));
     Cb.base = base;
@@ -2058,11 +2101,12 @@ static int enqueue_bt_slot(fgpu_handle* h) {
   bp.beta = h->beta;
   bp.tol_rel = h->tol_rel;
   if (int rc = one([&] { bt_decide_kernel<<<1, 1, 0, h->stream>>>(c, bp); })) return rc;
-  {   // RejectSolution: the RHS of cold (CHECK_NOTHING)
+  {   // RejectSolution: the RHS of cold (CHECK_NOTHING); with FARGO it frames cvar
     StageArgs A = base_args(h);
     A.out_mode = OUT_RHS;
     A.out = K1;
     A.in = plain_state(base, false);
+    if (fg) { A.in.pre = addWn; A.w_sub = Wn; A.out_base = CV; }
     A.gate = ACT_REJECT;
     if (int rc = launch_stage(h, A, RhsTime::att(0.0))) return rc;
   }
@@ -2074,10 +2118,55 @@ static int enqueue_bt_slot(fgpu_handle* h) {
     A.out_base = base;
     A.checkdata = h->cfg.checkdata;
     if (h->cfg.checkdata) A.cfl_mode = 3;
+    if (fg) { A.in.pre = addWn; A.w_sub = Wn; }
     A.gate = ACT_SUB;
     if (int rc = launch_stage(h, A, RhsTime::att(0.0))) return rc;
     if (h->cfg.checkdata)
       if (int rc = one([&] { bt_subcheck_kernel<<<1, 1, 0, h->stream>>>(c); })) return rc;
+    if (fg) {   // cvar = cold
+      const long long n = (long long)h->V * h->g.n;
+      const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148 * 8);
+      if (int rc = one([&] { gated_copy_kernel<<<blocks, 256, 0, h->stream>>>(base, CV, n, c, ACT_SUB); })) return rc;
+    }
+  }
+  if (fg) {
+    // the closing (timedisc_base.f90:727-744): FargoAdvection of cvar (AcceptSolution's framed
+    // copy in cold when it evaluated the RHS at the step's end, else the accepted state), the
+    // closing ComputeRHS (its CheckData and the interior CFL come from the advection pass),
+    // the ghost cells' CFL, w = w_new and CalcTimestep
+    const long long n = (long long)h->V * h->g.n;
+    const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148 * 8);
+    const FargoStep F = fargo_step_of(h);
+    FargoAdvArgs X = fargo_adv_args(h, F);
+    X.w = Wn;
+    X.dt_ctl = 1;
+    X.in = plain_state(base, false); X.out = P; X.gate = ACT_COPY;
+    if (int rc = launch_fargo_advect_args(h, X)) return rc;
+    X.in = plain_state(P, false); X.out = CV; X.gate = ACT_ENDNC;
+    if (int rc = launch_fargo_advect_args(h, X)) return rc;
+    if (int rc = one([&] { gated_copy_kernel<<<blocks, 256, 0, h->stream>>>(CV, P, n, c, ACT_ENDNC); })) return rc;
+    StageArgs A = base_args(h);
+    A.out_mode = OUT_RHS;
+    A.out = K1;
+    A.in = plain_state(P, false);
+    A.in.pre = addWn;
+    A.w_sub = Wn;
+    A.out_base = base;
+    A.gate = ACT_END;
+    if (int rc = launch_stage(h, A, RhsTime::att(0.0))) return rc;
+    BndArgs B = bnd_args(h, P, false, FIN_NONE);
+    B.in.pre = addWn;
+    B.w_sub = Wn;
+    B.checkdata = h->cfg.checkdata;
+    B.gate = ACT_END;
+    if (int rc = launch_misc(h, 0, B)) return rc;
+    if (dyn) {
+      const long long nw = h->nw;
+      double* W = h->d_w;
+      if (int rc = one([&] { gated_copy_kernel<<<1, 256, 0, h->stream>>>(Wn, W, nw, c, ACT_END); })) return rc;
+    }
+    const int nd = h->nd;
+    return one([&] { bt_finish_kernel<<<1, 1, 0, h->stream>>>(c, nd); });
   }
   {   // the closing: cvar as AcceptSolution's ComputeRHS left it, then IntegrationStep's RHS
     const long long n = (long long)h->V * h->g.n;
@@ -2169,7 +2258,8 @@ static int bt_run(fgpu_handle* h, int64_t n, int64_t* done) {
 // the device clock serves embedded schemes whose stage states are formed by form_kernel;
 // FGPU_BUTCHER_HOST=1 keeps the host-controlled loop
 static bool bt_device(const fgpu_handle* h) {
-  if (!h->materialize) return false;
+  // (FARGO with a Butcher scheme forms its stage states in the stencil)
+  if (!h->materialize && !(h->fargo && !h->adaptive_me)) return false;
   const char* e = std::getenv("FGPU_BUTCHER_HOST");
   return !(e && std::atoi(e) != 0);
 }
@@ -2195,6 +2285,15 @@ int fgpu_run(fgpu_handle* h, int64_t n, int64_t* done) {
   if (!h->first_done) { int rc = fgpu_first_step(h); if (rc) return rc; }
   int64_t k = 0;
   if (h->butcher) {
+    if (n > 0 && bt_device(h) && h->fargo && (h->fargo_tmp_fresh || h->fargo_phase < 2)) {
+      // the run's first FARGO step (its stage vectors' first frame flag, the frame of the
+      // state FirstStep left) on the host loop, the rest on the device clock
+      if (int rc = butcher_step(h)) { if (done) *done = 0; return rc; }
+      int64_t d2 = 0;
+      const int rc = n > 1 ? bt_run(h, n - 1, &d2) : FGPU_OK;
+      if (done) *done = 1 + d2;
+      return rc;
+    }
     if (n > 0 && bt_device(h)) return bt_run(h, n, done);
     int rc = FGPU_OK;
     for (; k < n; ++k) {

@@ -47,7 +47,8 @@ def test_device_clock_matches_oracle(name):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["gauss3d_dopri_mc_prim", "gauss3d_rkf3_minmod_cons", "khi_modeuler_adaptive2_mc_prim",
-                                  "iso3d_cashkarp_mixed_bc", "disk_powerlaw_pringle_ssprk5"])
+                                  "iso3d_cashkarp_mixed_bc", "disk_powerlaw_pringle_ssprk5", "disk_fargo_ssprk5_logcyl",
+                                  "khi_fargo1_x_cashkarp"])
 def test_device_clock_equals_host_steps(name):
     """fgpu_run (device clock) and repeated fgpu_step (host-controlled loop) agree bitwise,
     also when the device run is continued by host steps and vice versa."""
