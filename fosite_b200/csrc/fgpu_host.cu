@@ -2000,12 +2000,19 @@ static int enqueue_bt_slot(fgpu_handle* h) {
     const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148 * 8);
     const double e1 = kEta[ord - 1][0];
     if (int rc = one([&] {
-          shu_osher_update_kernel<<<blocks, 256, 0, h->stream>>>(base, base, K1, S1, n, e1, 0.0, d_att, c, ACT_ATTEMPT);
+          shu_osher_update_kernel<<<blocks, 256, 0, h->stream>>>(base, CV, K1, S1, n, e1, 0.0, d_att, c, ACT_ATTEMPT);
         }))
       return rc;
     for (int m = 2; m <= ord; ++m) {
       StageArgs A = base_args(h);
       A.in = plain_state(m == 2 ? S1 : S2, false);
+      if (fg) {
+        // every ComputeRHS frames its vector in place; the updates read the framed vectors
+        A.in.pre = addWn;
+        A.w_sub = Wn;
+        A.yn_chain = chain_add(addWn, Wn, -1.0);
+        if (m == ord && ord == 2) A.err_chain = A.yn_chain;
+      }
       A.out_mode = OUT_SSPRK;
       A.eta = kEta[ord - 1][m - 1];
       A.y0 = base;
@@ -2258,8 +2265,8 @@ static int bt_run(fgpu_handle* h, int64_t n, int64_t* done) {
 // the device clock serves embedded schemes whose stage states are formed by form_kernel;
 // FGPU_BUTCHER_HOST=1 keeps the host-controlled loop
 static bool bt_device(const fgpu_handle* h) {
-  // (FARGO with a Butcher scheme forms its stage states in the stencil)
-  if (!h->materialize && !(h->fargo && !h->adaptive_me)) return false;
+  // (FARGO with an embedded scheme forms its stage states in the stencil)
+  if (!h->materialize && !h->fargo) return false;
   const char* e = std::getenv("FGPU_BUTCHER_HOST");
   return !(e && std::atoi(e) != 0);
 }

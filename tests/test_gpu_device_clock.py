@@ -48,7 +48,7 @@ def test_device_clock_matches_oracle(name):
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["gauss3d_dopri_mc_prim", "gauss3d_rkf3_minmod_cons", "khi_modeuler_adaptive2_mc_prim",
                                   "iso3d_cashkarp_mixed_bc", "disk_powerlaw_pringle_ssprk5", "disk_fargo_ssprk5_logcyl",
-                                  "khi_fargo1_x_cashkarp"])
+                                  "khi_fargo1_x_cashkarp", "disk_fargo_me3_adaptive", "disk_fargo2_me2_adaptive"])
 def test_device_clock_equals_host_steps(name):
     """fgpu_run (device clock) and repeated fgpu_step (host-controlled loop) agree bitwise,
     also when the device run is continued by host steps and vice versa."""
