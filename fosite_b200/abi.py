@@ -14,6 +14,7 @@ CONSTANT, LINEAR = 1, 2
 PRIMITIVE, CONSERVATIVE = 1, 2
 MINMOD, MONOCENT, SWEBY, SUPERBEE, OSPRE, PP, VANLEER, NOLIMIT = 1, 2, 3, 4, 5, 6, 7, 8
 NO_GRADIENTS, PERIODIC, REFLECTING, ABSORBING = 0x01, 0x02, 0x03, 0x0D
+AXIS = 0x04
 WEST, EAST, SOUTH, NORTH, BOTTOM, TOP = 0, 1, 2, 3, 4, 5
 MODIFIED_EULER, RK_FEHLBERG, CASH_KARP, DORMAND_PRINCE, SSPRK = 1, 2, 3, 4, 5
 CHECK_NOTHING, CHECK_CSOUND, CHECK_PMIN, CHECK_RHOMIN, CHECK_INVALID, CHECK_TMIN, CHECK_ALL = \

@@ -162,7 +162,7 @@ __device__ __forceinline__ bool gated_out(const Ctl* c, int gate) {
   return gate && c && !(c->act & gate);
 }
 
-enum { BC_NOGRAD = 0x01, BC_PERIODIC = 0x02, BC_REFLECTING = 0x03, BC_ABSORBING = 0x0D };
+enum { BC_NOGRAD = 0x01, BC_PERIODIC = 0x02, BC_REFLECTING = 0x03, BC_AXIS = 0x04, BC_ABSORBING = 0x0D };
 enum { LIM_MINMOD = 1, LIM_MC = 2, LIM_SWEBY = 3, LIM_SUPERBEE = 4, LIM_OSPRE = 5, LIM_VANLEER = 7, LIM_NOLIMIT = 8 };
 
 __device__ __forceinline__ double fsign1(double b) { return signbit(b) ? -1.0 : 1.0; }
@@ -339,10 +339,14 @@ struct Cells {
     if (type == BC_PERIODIC) {
       ijk[d] = lo ? nd - s : s - 1;
       interior_p(S, g, P, ijk[0], ijk[1], ijk[2], p);
-    } else if (type == BC_REFLECTING) {
+    } else if (type == BC_REFLECTING || type == BC_AXIS) {
       ijk[d] = lo ? s - 1 : nd - s;
       interior_p(S, g, P, ijk[0], ijk[1], ijk[2], p);
       p[vn] = -p[vn];
+      // AXIS (boundary_axis.f90, physics_eulerisotherm.f90:1701-1760 AxisMasks): on the
+      // curvilinear meshes here the azimuth is the second coordinate, whose velocity is
+      // reflected too at the x faces
+      if (type == BC_AXIS && d == 0 && M.curv) p[2] = -p[2];
     } else if (type == BC_NOGRAD) {
       ijk[d] = lo ? 0 : nd - 1;
       interior_p(S, g, P, ijk[0], ijk[1], ijk[2], p);

@@ -1481,8 +1481,9 @@ int validate(fgpu_handle* h) {
   for (int f = 0; f < 6; ++f) {
     if (h->nd == 2 && f >= 4) continue;
     int t = c.bc[f];
-    if (t != FGPU_PERIODIC && t != FGPU_REFLECTING && t != FGPU_ABSORBING && t != FGPU_NO_GRADIENTS)
-      return set_err(h, FGPU_EUNSUPPORTED, "boundary condition not supported (periodic, reflecting, absorbing, no_gradients)");
+    if (t != FGPU_PERIODIC && t != FGPU_REFLECTING && t != FGPU_ABSORBING && t != FGPU_NO_GRADIENTS &&
+        t != FGPU_AXIS)
+      return set_err(h, FGPU_EUNSUPPORTED, "boundary condition not supported (periodic, reflecting, axis, absorbing, no_gradients)");
   }
   for (int d = 0; d < h->nd; ++d)
     if ((c.bc[2 * d] == FGPU_PERIODIC) != (c.bc[2 * d + 1] == FGPU_PERIODIC))
@@ -2540,7 +2541,8 @@ extern "C" int fgpu_calc_timestep_noalloc(const fgpu_config* cfg, const double* 
   int nd = c.knum > 1 ? 3 : 2;
   for (int f = 0; f < 2 * nd; ++f) {
     int t = c.bc[f];
-    if (t != FGPU_PERIODIC && t != FGPU_REFLECTING && t != FGPU_ABSORBING && t != FGPU_NO_GRADIENTS)
+    if (t != FGPU_PERIODIC && t != FGPU_REFLECTING && t != FGPU_ABSORBING && t != FGPU_NO_GRADIENTS &&
+        t != FGPU_AXIS)
       return FGPU_EUNSUPPORTED;
   }
   int nxp = c.inum + 4, nyp = c.jnum + 4, nzp = c.knum + 4;

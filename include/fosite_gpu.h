@@ -58,6 +58,7 @@ extern "C" {
 #define FGPU_NO_GRADIENTS     0x01
 #define FGPU_PERIODIC         0x02
 #define FGPU_REFLECTING       0x03
+#define FGPU_AXIS             0x04   /* reflecting, with the azimuthal velocity reflected too (boundary_axis.f90) */
 #define FGPU_ABSORBING        0x0D
 /* boundary orientation: mesh/mesh_base.f90:102-107 (1-based there, 0-based here) */
 #define FGPU_WEST   0

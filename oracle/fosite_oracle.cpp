@@ -513,8 +513,10 @@ struct Oracle {
           }
         break;
       case FGPU_REFLECTING:   // boundary_reflecting.f90:89-204
+      case FGPU_AXIS:         // boundary_axis.f90: reflecting with AxisMasks (physics_eulerisotherm.f90:1701-1760)
         for (int l = 0; l < VNUM; ++l) {
-          bool refl = (l == vn);
+          // the azimuthal velocity (second coordinate of the curvilinear meshes) is reflected too
+          bool refl = (l == vn) || (type == FGPU_AXIS && d == 0 && cfg.geometry != FGPU_CARTESIAN && l == vel(1));
           for (int s = 1; s <= g; ++s)
             for (int b = t2lo; b <= t2hi; ++b) for (int a = t1lo; a <= t1hi; ++a) {
               double v = lo ? pv[at(nmin + s - 1, a, b) + NC * l] : pv[at(nmax - s + 1, a, b) + NC * l];

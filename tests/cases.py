@@ -305,6 +305,36 @@ def _iso_fargo_x(n=(40, 30), fargo=1, seed=83):
     return c, p, {}
 
 
+def _axis_disk(n=(28, 36), euler=False, seed=91):
+    """A rotating gas on a cylindrical mesh reaching the axis: r in [0, 1] with the AXIS
+    boundary at r = 0 (boundary_axis.f90), reflecting at r = 1, periodic in phi; no point mass."""
+    c = abi.default_config()
+    c.inum, c.jnum, c.knum = n[0], n[1], 1
+    c.geometry = abi.CYLINDRICAL
+    c.xmin, c.xmax, c.ymin, c.ymax = 0.0, 1.0, -np.pi, np.pi
+    c.physics = abi.EULER if euler else abi.EULER_ISOTHERM
+    c.gamma = 1.4
+    c.csiso = 0.0 if euler else 0.5
+    c.limiter = abi.VANLEER
+    c.variables = abi.PRIMITIVE
+    c.method = abi.MODIFIED_EULER
+    c.tdorder = 3
+    c.tol_rel = 10.0
+    c.cfl = 0.4
+    c.stoptime = 1.0e3
+    c.bc[:4] = [abi.AXIS, abi.REFLECTING, abi.PERIODIC, abi.PERIODIC]
+    abi.finalize_config(c)
+    X, Y, _, _ = problems.centers(c)
+    rng = np.random.default_rng(seed)
+    p = np.zeros((4 if euler else 3,) + X.shape)
+    p[0] = 1.0 + 0.3 * np.exp(-((X - 0.4) ** 2) / 0.02) * (1 + np.cos(Y)) + 0.01 * rng.uniform(-1, 1, X.shape)
+    p[1] = 0.05 * rng.uniform(-1, 1, X.shape)
+    p[2] = 0.5 * X * np.exp(-X ** 2) + 0.02 * rng.uniform(-1, 1, X.shape)
+    if euler:
+        p[3] = 1.0 + 0.2 * np.exp(-((X - 0.5) ** 2) / 0.01)
+    return c, p, {}
+
+
 def khi_fargo(fargo, direction=1, n=(24, 24), visc=False, seed=11):
     """tests/KHI2D.f90's FARGO legs (:81-150, config :168-245, InitData :300-360): ideal-gas KHI,
     KT + MONOCENT (theta 1.2) on conservative variables, periodic box, FARGO type 1 or 2 along
@@ -380,6 +410,8 @@ CASES = {
     "disk_fargo2_user_w": lambda: _disk_fargo2(),
     "euler_fargo_shear_cons": lambda: _euler_fargo(),
     "khi_fargo1_x": lambda: khi_fargo(1, n=(28, 24)),
+    "iso_axis_cyl": lambda: _axis_disk(),
+    "euler_axis_cyl_dopri": lambda: _butcher(_axis_disk(n=(24, 32), euler=True), abi.DORMAND_PRINCE, 5, 1e-4),
     "disk_fargo_ssprk5_logcyl": lambda: _butcher(_disk_fargo(), abi.SSPRK, 5),
     "disk_fargo2_dopri_cyl": lambda: _butcher(_disk_fargo2(), abi.DORMAND_PRINCE, 5, 1e-4),
     "euler_fargo_rkf5_shear": lambda: _butcher(_euler_fargo(), abi.RK_FEHLBERG, 5, 1e-4),
