@@ -42,6 +42,9 @@ struct fgpu_batch {
   CombineArgs* d_cargs = nullptr;// [n]
   CopyArgs* d_copy = nullptr;    // [n]
   BndArgs* d_ebnd = nullptr;     // [n] closing ghost/CFL pass
+  bool adaptive_me = false;      // embedded modified Euler members: stage 1 by d_upd, no forms
+  int me_order = 0;
+  UpdArgs* d_upd = nullptr;      // [n]
   int4* d_cblocks = nullptr;     // per-member cell blocks (member, block, blocks)
   int ncblocks = 0;
   cudaGraphExec_t slot_graph = nullptr;
@@ -224,6 +227,7 @@ int build_embedded_tables(fgpu_batch* b) {
   std::vector<CombineArgs> cargs(n);
   std::vector<CopyArgs> copy(n);
   std::vector<BndArgs> ebnd(n);
+  std::vector<UpdArgs> upd(b->adaptive_me ? n : 0);
   std::vector<int4> cblocks;
   for (int i = 0; i < n; ++i) {
     fgpu_handle* h = b->m[i];
@@ -234,7 +238,37 @@ int build_embedded_tables(fgpu_batch* b) {
     Ctl* c = h->d_ctl;
     ctlp[i] = c;
     btp[i].order = T.order; btp[i].beta = h->beta; btp[i].tol_rel = h->tol_rel;
-    for (int m = 2; m <= M; ++m) {
+    if (b->adaptive_me) {
+      // timedisc_modeuler.f90:163-192: stage 1 pointwise, stages 2..order with the embedded
+      // solution and the error norm (modeuler_attempt's launches per member)
+      const int ord = h->order;
+      double* S1 = h->buf[3];
+      double* S2 = h->buf[4];
+      double* LO = h->buf[5];
+      UpdArgs& U = upd[i];
+      U.y0 = base; U.yn = base; U.r = K1; U.out = S1; U.n = (long long)h->V * h->g.n;
+      U.eta = kEta[ord - 1][0]; U.dt_dev = &c->d_att; U.ctl = c; U.gate = ACT_ATTEMPT;
+      for (int m = 2; m <= ord; ++m) {
+        StageArgs A = base_args(h);
+        A.in = plain_state(m == 2 ? S1 : S2, false);
+        A.out_mode = OUT_SSPRK;
+        A.eta = kEta[ord - 1][m - 1];
+        A.y0 = base;
+        A.dt_dev = &c->d_att;
+        if (m == ord) {
+          A.out = P;
+          A.err_low = ord == 3 ? LO : S1;
+        } else {
+          A.out = S2;
+          A.out2 = LO;
+          A.eta2 = kEta[1][1];
+        }
+        A.gate = ACT_ATTEMPT;
+        A.kchunk = h->kchunk;
+        eargs[(size_t)(m - 2) * n + i] = A;
+      }
+    }
+    for (int m = 2; m <= M && !b->adaptive_me; ++m) {
       StageArgs A = base_args(h);
       A.in.base = base;
       A.in.nk = m - 1;
@@ -257,7 +291,9 @@ int build_embedded_tables(fgpu_batch* b) {
     CombineArgs& Cb = cargs[i];
     std::memset(&Cb, 0, sizeof(Cb));
     Cb.base = base;
-    for (int q = 0; q < T.m; ++q) { Cb.K[q] = h->buf[2 + q]; Cb.bh_dt[q] = T.bh[q]; Cb.bl_dt[q] = T.bl[q]; }
+    // (the embedded modified Euler scheme has no weights: its combination is the last stage's)
+    if (!b->adaptive_me)
+      for (int q = 0; q < T.m; ++q) { Cb.K[q] = h->buf[2 + q]; Cb.bh_dt[q] = T.bh[q]; Cb.bl_dt[q] = T.bl[q]; }
     Cb.nstage = T.m; Cb.out_high = P; Cb.tol_rel = h->tol_rel;
     for (int v = 0; v < FGPU_MAXV; ++v) Cb.tol_abs[v] = h->tol_abs[v];
     Cb.n = h->g.n; Cb.ctl = c; Cb.dt_dev = &c->d_att; Cb.gate = ACT_ATTEMPT;
@@ -294,6 +330,8 @@ int build_embedded_tables(fgpu_batch* b) {
   if (int rc = upload_table(b, &b->d_copy, copy)) return rc;
   if (int rc = upload_table(b, &b->d_ebnd, ebnd)) return rc;
   if (int rc = upload_table(b, &b->d_cblocks, cblocks)) return rc;
+  if (b->adaptive_me)
+    if (int rc = upload_table(b, &b->d_upd, upd)) return rc;
   BCUDA_TRY(b, cudaStreamSynchronize(b->stream));
   return FGPU_OK;
 }
@@ -321,12 +359,18 @@ int enqueue_batch_slot(fgpu_batch* b) {
   const unsigned mb = (unsigned)((n + 127) / 128);
   bt_begin_batch_kernel<<<mb, 128, 0, b->stream>>>(b->d_ctlp, n);
   BCUDA_TRY(b, cudaGetLastError());
-  for (int m = 2; m <= M; ++m) {
+  if (b->adaptive_me) {
+    batched_update_kernel<<<b->ncblocks, 256, 0, b->stream>>>(b->d_upd, b->d_cblocks);
+    BCUDA_TRY(b, cudaGetLastError());
+    for (int m = 2; m <= b->me_order; ++m)
+      if (int rc = launch_batched_stage(b, b->d_eargs + (size_t)(m - 2) * n, b->variant)) return rc;
+  }
+  for (int m = 2; m <= M && !b->adaptive_me; ++m) {
     if (m == 2 || !b->m[0]->fuse_form)
       if (int rc = launch_batched_form(b, b->d_fargs + (size_t)(m - 2) * n)) return rc;
     if (int rc = launch_batched_stage(b, b->d_eargs + (size_t)(m - 2) * n, b->variant)) return rc;
   }
-  if (!b->m[0]->fuse_end) {
+  if (!b->m[0]->fuse_end && !b->adaptive_me) {
     switch (b->m[0]->V) {
       case 3: batched_combine_kernel<3><<<b->ncblocks, 256, 0, b->stream>>>(b->d_cargs, b->d_cblocks); break;
       case 4: batched_combine_kernel<4><<<b->ncblocks, 256, 0, b->stream>>>(b->d_cargs, b->d_cblocks); break;
@@ -476,7 +520,10 @@ int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
     if (!h) return fail(FGPU_EARG, "null member");
     if (h->butcher != b->embedded) return fail(FGPU_EBADCFG, "batch members mix fixed-step and embedded schemes");
     if (h->butcher) {
-      if (h->adaptive_me) return fail(FGPU_EUNSUPPORTED, "embedded batch members use a Butcher tableau (not the adaptive modified Euler scheme)");
+      if (h->adaptive_me != h0->adaptive_me || (h->adaptive_me && h->order != h0->order))
+        return fail(FGPU_EBADCFG, "embedded batch members mix modified Euler and Butcher schemes or orders");
+      b->adaptive_me = h->adaptive_me;
+      b->me_order = h->order;
       if (!h->materialize) return fail(FGPU_EUNSUPPORTED, "embedded batch members need the formed stage states");
       if (h->fuse_form != h0->fuse_form || h->fuse_end != h0->fuse_end)
         return fail(FGPU_EBADCFG, "embedded batch members differ in stage-state formation");
@@ -613,7 +660,7 @@ void fgpu_batch_destroy(fgpu_batch* b) {
   if (b->slot_graph) cudaGraphExecDestroy(b->slot_graph);
   for (void* p : {(void*)b->d_ctlp, (void*)b->d_btp, (void*)b->d_eargs, (void*)b->d_fargs, (void*)b->d_cargs,
                   (void*)b->d_copy, (void*)b->d_ebnd, (void*)b->d_cblocks, (void*)b->d_fw, (void*)b->d_fwb,
-                  (void*)b->d_fa, (void*)b->d_fab, (void*)b->d_fwc, (void*)b->d_fwcb})
+                  (void*)b->d_fa, (void*)b->d_fab, (void*)b->d_fwc, (void*)b->d_fwcb, (void*)b->d_upd})
     if (p) cudaFree(p);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;

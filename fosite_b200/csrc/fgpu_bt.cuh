@@ -248,6 +248,30 @@ struct CopyArgs {
   const Ctl* ctl;
   int gate;
 };
+// The first stage of the embedded modified Euler scheme for a batch: out = yn - dt*r +
+// eta*(y0 - yn + dt*r) with the member's attempt dt (shu_osher_update_kernel per member)
+struct UpdArgs {
+  const double* y0;
+  const double* yn;
+  const double* r;
+  double* out;
+  long long n;
+  double eta;
+  const double* dt_dev;
+  const Ctl* ctl;
+  int gate;
+};
+__global__ void __launch_bounds__(256) batched_update_kernel(const UpdArgs* __restrict__ args,
+                                                             const int4* __restrict__ blocks) {
+  const int4 T = blocks[blockIdx.x];
+  const UpdArgs& A = args[T.x];
+  if (A.ctl->stop | A.ctl->brk) return;
+  if (gated_out(A.ctl, A.gate)) return;
+  const double dt = *A.dt_dev;
+  for (long long t = T.y * 256LL + threadIdx.x; t < A.n; t += T.z * 256LL)
+    A.out[t] = A.yn[t] - dt * A.r[t] + A.eta * (A.y0[t] - A.yn[t] + dt * A.r[t]);
+}
+
 __global__ void __launch_bounds__(256) batched_copy_kernel(const CopyArgs* __restrict__ args,
                                                            const int4* __restrict__ blocks) {
   const int4 T = blocks[blockIdx.x];

@@ -280,7 +280,8 @@ int fgpu_stage_layout(const fgpu_handle* h, int* variant, int* kchunk);
  * Runge-Kutta stage over the flattened tile queue of all grids, plus one
  * ghost-cell / CFL / finalize launch.  Members are handles created, uploaded
  * and past fgpu_first_step, all with either the fixed-step modified Euler
- * scheme of time order 2 or 3 or the same embedded Butcher scheme (Dormand-
+ * scheme of time order 2 or 3, the embedded modified Euler scheme of one order,
+ * or the same embedded Butcher scheme (Dormand-
  * Prince, Fehlberg, Cash-Karp, SSPRK; each member keeps its own tolerances,
  * error norm and step-size controller, advanced attempt by attempt on the
  * device), the same dimensionality, physics and reconstruction variables, no

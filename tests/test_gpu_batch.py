@@ -135,7 +135,7 @@ def test_batch_rejects_mixed_or_unsupported_members():
     e.set_state(abi.PVAR, p4)
     e.first_step()
     with pytest.raises(FositeError):
-        Batch([e])                       # adaptive modified Euler members are not batched
+        Batch([e, d])                    # embedded modified Euler and Butcher members
     c5, p5, _ = _khi(n=(24, 24), method=abi.CASH_KARP, tdorder=5)
     f = Simulation(c5)
     f.set_state(abi.PVAR, p5)
@@ -297,3 +297,43 @@ def test_fargo_x_batch_and_rejections():
         Batch([member(1, 1, step=False)])        # first step after FirstStep not taken alone
     with pytest.raises(FositeError):
         Batch([member(1, 1), member(1, 2)])      # different transport directions
+
+
+@pytest.mark.parametrize("order", [2, 3])
+def test_adaptive_modified_euler_batch_equals_lone_runs(order):
+    """Members with the embedded modified Euler scheme (fosite's default tol_rel < 1) of
+    different sizes and tolerances in one batch: the per-member first-stage update, the stages
+    with the embedded solution and each member's controller give every member exactly its
+    lone device-clock run (rejections and sub-steps included) and the oracle's steps."""
+    import pyoracle
+    from fosite_b200.sim import Batch, Simulation
+    specs = [((30, 28), 1e-3), ((24, 36), 3e-4), ((40, 20), 1e-3)]
+
+    def make():
+        out = []
+        for n, tol in specs:
+            cfg, p, _ = _khi(n=n, tdorder=order, me_tol=tol, limiter=abi.MONOCENT, variables=abi.PRIMITIVE)
+            s = Simulation(cfg, exact=True)
+            s.set_state(abi.PVAR, p)
+            s.first_step()
+            out.append(s)
+        return out
+    members, alone = make(), make()
+    b = Batch(members)
+    assert b.run(9) == len(specs)
+    for s in alone:
+        assert s.run(9) == (0, 9)
+    for m, s in zip(members, alone):
+        sm, ss = m.status(), s.status()
+        assert (sm.time, sm.dt, sm.iter, sm.n_adj) == (ss.time, ss.dt, ss.iter, ss.n_adj)
+        assert np.array_equal(m.get(abi.CVAR), s.get(abi.CVAR))
+    assert sum(m.status().n_adj for m in members) > 0
+    cfg, p, _ = _khi(n=specs[1][0], tdorder=order, me_tol=specs[1][1], limiter=abi.MONOCENT, variables=abi.PRIMITIVE)
+    o = pyoracle.Oracle(cfg)
+    o.set_state(abi.PVAR, p)
+    o.first_step()
+    for _ in range(9):
+        assert o.step() == 0
+    assert o.status().time == members[1].status().time
+    assert np.array_equal(o.get(abi.CVAR), members[1].get(abi.CVAR))
+    b.close()
