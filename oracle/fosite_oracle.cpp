@@ -31,6 +31,20 @@
 #include <quadmath.h>
 #include "../include/fosite_gpu.h"
 
+// Data-parallel loops (every iteration writes its own elements, no reductions) run on the
+// host's cores when built with OpenMP; the arithmetic of each element is unchanged, so the
+// results are the same bit for bit at any thread count.  Reductions stay serial.
+#ifdef _OPENMP
+#include <omp.h>
+#define PAR_FOR _Pragma("omp parallel for schedule(static)")
+#define PAR_FOR2 _Pragma("omp parallel for collapse(2) schedule(static)")
+#define PAR_FOR3 _Pragma("omp parallel for collapse(3) schedule(static)")
+#else
+#define PAR_FOR
+#define PAR_FOR2
+#define PAR_FOR3
+#endif
+
 namespace {
 
 const double TINY_ = DBL_MIN;     // Fortran TINY(1.0) for REAL(8)
@@ -440,8 +454,9 @@ struct Oracle {
     return std::sqrt(fmax2(2.0 * TINY_, cfg.gamma * P / rho));
   }
   void c2p_range(std::vector<double>& cv, std::vector<double>& pv, int i1, int i2, int j1, int j2, int k1, int k2) {
-    double c[FGPU_MAXVAR], p[FGPU_MAXVAR];
+    PAR_FOR2
     for (int k = k1; k <= k2; ++k) for (int j = j1; j <= j2; ++j) for (int i = i1; i <= i2; ++i) {
+      double c[FGPU_MAXVAR], p[FGPU_MAXVAR];
       long id0 = id(i, j, k);
       for (int l = 0; l < VNUM; ++l) c[l] = cv[id0 + NC * l];
       cons2prim(c, p);
@@ -449,8 +464,9 @@ struct Oracle {
     }
   }
   void p2c_range(std::vector<double>& pv, std::vector<double>& cv, int i1, int i2, int j1, int j2, int k1, int k2) {
-    double c[FGPU_MAXVAR], p[FGPU_MAXVAR];
+    PAR_FOR2
     for (int k = k1; k <= k2; ++k) for (int j = j1; j <= j2; ++j) for (int i = i1; i <= i2; ++i) {
+      double c[FGPU_MAXVAR], p[FGPU_MAXVAR];
       long id0 = id(i, j, k);
       for (int l = 0; l < VNUM; ++l) p[l] = pv[id0 + NC * l];
       prim2cons(p, c);
@@ -893,6 +909,7 @@ struct Oracle {
   // reconstruction_linear.f90:215-630
   void calculate_states(std::vector<double>& rv, std::vector<double>& rst) {
     if (cfg.order == FGPU_CONSTANT) {   // reconstruction_constant.f90:74-93
+      PAR_FOR3
       for (int l = 0; l < VNUM; ++l) for (int n = 0; n < NFACES; ++n)
         for (long c = 0; c < NC; ++c) rst[c + NC * (n + (long)NFACES * l)] = rv[c + NC * l];
       return;
@@ -905,6 +922,7 @@ struct Oracle {
       if (d == 0) { lo_i = IGMIN + IP1; hi_i = IGMAX + IM1; }
       if (d == 1) { lo_j = JGMIN + 1; hi_j = JGMAX - 1; }
       if (d == 2) { lo_k = KGMIN + 1; hi_k = KGMAX - 1; }
+      PAR_FOR2
       for (int l = 0; l < VNUM; ++l)
         for (int k = lo_k; k <= hi_k; ++k) for (int j = lo_j; j <= hi_j; ++j) for (int i = lo_i; i <= hi_i; ++i) {
           long c = id(i, j, k);
@@ -913,6 +931,7 @@ struct Oracle {
           slopes[c + NC * ((long)m + (long)NDIMS * l)] = s;
         }
     }
+    PAR_FOR3
     for (int l = 0; l < VNUM; ++l) for (int n = 0; n < NFACES; ++n)
       for (long c = 0; c < NC; ++c)
         rst[c + NC * (n + (long)NFACES * l)] = rv[c + NC * l] + slopes[c + NC * ((long)(n / 2) + (long)NDIMS * l)] * rdx[c + NC * n];
@@ -920,31 +939,37 @@ struct Oracle {
 
   // fluxes_base.f90:368-397 CalculateFaceData + fluxes_kt.f90:109-208
   void calculate_fluxes(std::vector<double>& pv, std::vector<double>& cv) {
-    double c[FGPU_MAXVAR], p[FGPU_MAXVAR];
     bool prim_recon = (cfg.variables == FGPU_PRIMITIVE);
     if (prim_recon) {
       calculate_states(pv, fprim);
+      PAR_FOR2
       for (int n = 0; n < NFACES; ++n) for (long x = 0; x < NC; ++x) {
+        double c[FGPU_MAXVAR], p[FGPU_MAXVAR];
         for (int l = 0; l < VNUM; ++l) p[l] = fprim[x + NC * (n + (long)NFACES * l)];
         prim2cons(p, c);
         for (int l = 0; l < VNUM; ++l) fcons[x + NC * (n + (long)NFACES * l)] = c[l];
       }
     } else {
       calculate_states(cv, fcons);
+      PAR_FOR2
       for (int n = 0; n < NFACES; ++n) for (long x = 0; x < NC; ++x) {
+        double c[FGPU_MAXVAR], p[FGPU_MAXVAR];
         for (int l = 0; l < VNUM; ++l) c[l] = fcons[x + NC * (n + (long)NFACES * l)];
         cons2prim(c, p);
         for (int l = 0; l < VNUM; ++l) fprim[x + NC * (n + (long)NFACES * l)] = p[l];
       }
     }
-    if (euler)   // UpdateSoundSpeed on faces (physics_euler.f90:2555-2574)
+    if (euler) {  // UpdateSoundSpeed on faces (physics_euler.f90:2555-2574)
+      PAR_FOR2
       for (int n = 0; n < NFACES; ++n) for (long x = 0; x < NC; ++x)
         fcsound[x + NC * n] = soundspeed(fprim[x + NC * (n + (long)NFACES * 0)], fprim[x + NC * (n + (long)NFACES * PRESSURE)]);
+    }
     // CalcWaveSpeeds_faces (physics_eulerisotherm.f90:555-686)
     for (int m = 0; m < NDIMS; ++m) {
       int d = dirs[m]; int vi = vel(m);
       long str = d == 0 ? 1 : d == 1 ? NI : (long)NI * NJ;
       int fw = 2 * m, fe = 2 * m + 1;
+      PAR_FOR
       for (long x = 0; x < NC; ++x) {
         double cs = fcsound[x + NC * fw], v = fprim[x + NC * (fw + (long)NFACES * vi)];
         tmpw[x] = fmin2(0., v - cs); tmpw1[x] = fmax2(0., v + cs);
@@ -955,12 +980,14 @@ struct Oracle {
       if (d == 0) { lo_i = IMIN + IM1; hi_i = IMAX; }
       if (d == 1) { lo_j = JMIN + JM1; hi_j = JMAX; }
       if (d == 2) { lo_k = KMIN + KM1; hi_k = KMAX; }
+      PAR_FOR2
       for (int k = lo_k; k <= hi_k; ++k) for (int j = lo_j; j <= hi_j; ++j) for (int i = lo_i; i <= hi_i; ++i) {
         long x = id(i, j, k);
         minwav[x + NC * m] = fmin2(fmin2(0.0, tmpw[x + str]), minwav[x + NC * m]);
         maxwav[x + NC * m] = fmax2(fmax2(0.0, tmpw1[x + str]), maxwav[x + NC * m]);
       }
       // physical fluxes on both faces of direction m (CalcFluxes{X,Y,Z})
+      PAR_FOR2
       for (int n = fw; n <= fe; ++n) for (long x = 0; x < NC; ++x) {
         auto P = [&](int l) { return fprim[x + NC * (n + (long)NFACES * l)]; };
         auto C = [&](int l) { return fcons[x + NC * (n + (long)NFACES * l)]; };
@@ -980,6 +1007,7 @@ struct Oracle {
       // KT (fluxes_kt.f90:126-207)
       std::vector<double>& out = d == 0 ? xflux : d == 1 ? yflux : zflux;
       std::vector<double>& dA = d == 0 ? dAx : d == 1 ? dAy : dAz;
+      PAR_FOR2
       for (int l = 0; l < VNUM; ++l)
         for (int k = lo_k; k <= hi_k; ++k) for (int j = lo_j; j <= hi_j; ++j) for (int i = lo_i; i <= hi_i; ++i) {
           long x = id(i, j, k);
@@ -995,6 +1023,7 @@ struct Oracle {
   void geometrical_sources(std::vector<double>& pv, std::vector<double>& cv, std::vector<double>& s) {
     if (cfg.geometry == FGPU_CARTESIAN) return;
     if (!(NDIMS == 2 && dirs[0] == 0 && dirs[1] == 1) && NDIMS != 3) return;
+    PAR_FOR
     for (long x = 0; x < NC; ++x) {
       double P = euler ? pv[x + NC * PRESSURE] : pv[x] * (bccsound[x] * bccsound[x]);
       double vx = pv[x + NC * 1], vy = pv[x + NC * 2];
@@ -1264,11 +1293,14 @@ struct Oracle {
     if (fargo) add_bg(pv, cv);
     center_boundary(pv, cv);
     if ((checkbm & FGPU_CHECK_PMIN) && euler) {
+      PAR_FOR
       for (long x = 0; x < NC; ++x) pv[x + NC * PRESSURE] = fmax2(pv[x + NC * PRESSURE], cfg.pmin);
       p2c_range(pv, cv, IGMIN, IGMAX, JGMIN, JGMAX, KGMIN, KGMAX);
     }
-    if (euler)   // UpdateSoundSpeed(this%pvar) (always_update_bccsound)
+    if (euler) {  // UpdateSoundSpeed(this%pvar) (always_update_bccsound)
+      PAR_FOR
       for (long x = 0; x < NC; ++x) bccsound[x] = soundspeed(pvar[x], pvar[x + NC * PRESSURE]);
+    }
     if (checkbm != FGPU_CHECK_NOTHING) check_data(pv, cv, checkbm);
     geometrical_sources(pv, cv, geo_src);
     external_sources(t, pv, cv, src);
@@ -1292,6 +1324,7 @@ struct Oracle {
         r[id(i, j, KMAX + KP1) + NC * l] = -dx * dy * zflux[id(i, j, KMAX) + NC * l];
       }
     }
+    PAR_FOR2
     for (int l = 0; l < VNUM; ++l)
       for (int k = KMIN; k <= KMAX; ++k) for (int j = JMIN; j <= JMAX; ++j) for (int i = IMIN; i <= IMAX; ++i) {
         long x = id(i, j, k), o = NC * l;
@@ -1387,6 +1420,7 @@ struct Oracle {
     double maxerr = 0.0;
     for (int l = 0; l < VNUM; ++l) {
       double rel = -HUGE_;
+      PAR_FOR
       for (long x = 0; x < NC; ++x) {
         double v = hi[x + NC * l];
         cerr[x + NC * l] = std::fabs(v - lo[x + NC * l]) / (tol_rel * std::fabs(v) + tol_abs[l]);
@@ -1436,6 +1470,7 @@ struct Oracle {
       if (tol_rel >= 1.0) {
         for (int n = 1; n <= order; ++n) {
           double e = eta[order - 1][n - 1];
+          PAR_FOR
           for (long x = 0; x < NS; ++x) cvar[x] = update_me(e, dtv, cold[x], cvar[x], rhs[x]);
           if (outbound) update_bflux(e, dtv);
           if (n < order) compute_rhs(t0 + zeta[order - 1][n - 1] * dtv, pvar, cvar, FGPU_CHECK_NOTHING, rhs);
@@ -1447,6 +1482,7 @@ struct Oracle {
         for (int n = 1; n <= order; ++n) {
           double e = eta[order - 1][n - 1];
           std::vector<double>& cin = *C[n - 1]; std::vector<double>& cout = *C[n];
+          PAR_FOR
           for (long x = 0; x < NS; ++x) cout[x] = update_me(e, dtv, cold[x], cin[x], rhs[x]);
           if (n == 2 && order == 3)
             for (long x = 0; x < NS; ++x) ctmp[x] = update_me(eta[1][1], dtv, cold[x], ctmp[x], rhs[x]);
@@ -1464,9 +1500,11 @@ struct Oracle {
     for (int m = 1; m < m_stages; ++m) K[m] = &coeff[m];
     for (int m = 2; m <= m_stages; ++m) {
       double a1 = A[(m - 1) * m_stages + 0];
+      PAR_FOR
       for (long x = 0; x < NS; ++x) ctmp[x] = cvar[x] - a1 * dtv * (*K[0])[x];
       for (int mm = 2; mm <= m - 1; ++mm) {
         double a = A[(m - 1) * m_stages + (mm - 1)];
+        PAR_FOR
         for (long x = 0; x < NS; ++x) ctmp[x] = ctmp[x] - a * dtv * (*K[mm - 1])[x];
       }
       compute_rhs(t0 + c_coef[m - 1] * dtv, ptmp, ctmp, FGPU_CHECK_NOTHING, *K[m - 1]);
@@ -1475,6 +1513,7 @@ struct Oracle {
     for (int m = 1; m <= m_stages; ++m) {
       double bl = b_low[m - 1], bh = b_high[m - 1];
       std::vector<double>& k = *K[m - 1];
+      PAR_FOR
       for (long x = 0; x < NS; ++x) {
         ctmp[x] = ctmp[x] - bl * dtv * k[x];
         cvar[x] = cvar[x] - bh * dtv * k[x];
@@ -1569,6 +1608,16 @@ int orc_create(const fgpu_config* cfg, orc_handle** out) {
   return 0;
 }
 void orc_destroy(orc_handle* h) { delete h; }
+// host threads of the data-parallel loops (1 = the serial restatement); returns the count in use
+int orc_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+#else
+  (void)n;
+  return 1;
+#endif
+}
 int64_t orc_cell_count(orc_handle* h) { return h->o.NC; }
 int orc_vnum(orc_handle* h) { return h->o.VNUM; }
 int orc_nfaces(orc_handle* h) { return h->o.NFACES; }

@@ -47,8 +47,17 @@ def lib():
         L.orc_error.restype = C.c_char_p
         L.orc_get_pointmass.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.orc_set_fargo_velocity.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
+        L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_set_threads.restype = C.c_int
         _lib = L
     return _lib
+
+
+def set_threads(n=0):
+    """Host threads of the oracle's data-parallel loops (n <= 0: keep the current count).
+
+    Returns the number in use.  Results do not depend on it."""
+    return int(lib().orc_set_threads(int(n)))
 
 
 def _ptr(a):
