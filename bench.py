@@ -26,14 +26,15 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 WORKLOADS = {
-    "gauss3d": "3D Euler Gaussian pulse 256^3, reflecting, KT+MC(prim), Dormand-Prince 5(4) tol 1e-5, CFL 0.4",
-    "khi2d": "2D Kelvin-Helmholtz 256^2, periodic, KT+van Leer(cons), SSPRK3 fixed CFL 0.4",
-    "disk2d": "2D isothermal Keplerian disk, logcylindrical 512x1024, point mass GM=1, sigma~1/r, cs/vK=0.05, "
-              "FARGO shift, KT+van Leer(prim), SSPRK3 fixed CFL 0.4, absorbing r / periodic phi",
-    "khi2d_visc": "khi2d with the KHI2D test's molecular viscosity at Reynolds number 1e4 (256^2)",
-    "khi3d_visc": "3D Kelvin-Helmholtz 128^3 (tests/KHI3D.f90 set-up), periodic, KT+MC 1.2(cons), SSPRK3 fixed "
+    "gauss3d": "3D Euler Gaussian pulse, reflecting, KT+MC(prim), Dormand-Prince 5(4) tol 1e-5, CFL 0.4",
+    "khi2d": "2D Kelvin-Helmholtz, periodic, KT+van Leer(cons), SSPRK3 fixed CFL 0.4",
+    "disk2d": "2D isothermal Keplerian disk, logcylindrical (r x phi = n x 2n), point mass GM=1, sigma~1/r, "
+              "cs/vK=0.05, FARGO shift, KT+van Leer(prim), SSPRK3 fixed CFL 0.4, absorbing r / periodic phi",
+    "khi2d_visc": "khi2d with the KHI2D test's molecular viscosity at Reynolds number 1e4",
+    "khi3d_visc": "3D Kelvin-Helmholtz (tests/KHI3D.f90 set-up), periodic, KT+MC 1.2(cons), SSPRK3 fixed "
                   "CFL 0.4, molecular viscosity at Reynolds number 1e4",
 }
+# the grid of each description is the line's config.grid
 
 
 def make_problem(name, size):
@@ -142,12 +143,49 @@ def load_traffic_profile(name):
         return None
 
 
-def cpu_baseline(name, budget_s=20.0):
-    """The oracle (serial C++ restatement of the reference CPU path) on a bounded sample."""
+HEADLINE_SIZE = {"gauss3d": 256, "khi2d": 256, "disk2d": 512, "khi2d_visc": 256, "khi3d_visc": 128}
+# host memory of the oracle (it keeps the reference's face-state arrays) per ghost-padded cell,
+# measured on the 3D Dormand-Prince workload: 2.2 KB
+ORACLE_BYTES_PER_PADDED_CELL = 2400.0
+
+
+def _padded_cells(name, size):
+    if name in ("gauss3d", "khi3d_visc"):
+        return (size + 4) ** 3
+    if name == "disk2d":
+        return (size + 4) * (2 * size + 4)
+    return (size + 4) ** 2
+
+
+def _mem_available():
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return float(line.split()[1]) * 1024.0
+    except Exception:
+        pass
+    return 0.0
+
+
+def oracle_size(name, full):
+    """The headline grid if the oracle fits in half the available host memory, else the largest
+    grid (multiple of 16) that does."""
+    avail = 0.5 * _mem_available()
+    size = full
+    while size > 16 and _padded_cells(name, size) * ORACLE_BYTES_PER_PADDED_CELL > avail:
+        size -= 16
+    return size
+
+
+def time_oracle(name, size, threads, budget_s, max_steps=200):
+    """The oracle (C++ restatement of the reference CPU path) on the workload at `size`: FirstStep
+    untimed, then fosite steps until the budget is spent; cell-updates (accepted steps x interior
+    cells) per second."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     from fosite_b200 import abi
-    size = {"gauss3d": 48, "disk2d": 128, "khi3d_visc": 32}.get(name, 256)
+    used = pyoracle.set_threads(threads if threads > 0 else (os.cpu_count() or 1))
     cfg, p, extra = make_problem(name, size)
     o = pyoracle.Oracle(cfg)
     apply_extra(o, cfg, extra)
@@ -159,13 +197,24 @@ def cpu_baseline(name, budget_s=20.0):
     while True:
         o.step()
         steps += 1
-        if time.perf_counter() - t0 > budget_s or steps >= 200:
+        if time.perf_counter() - t0 > budget_s or steps >= max_steps:
             break
     el = time.perf_counter() - t0
     upd = (o.status().iter - it0) * cfg.inum * cfg.jnum * cfg.knum
-    return {"value": upd / el, "unit": "cell-updates/s", "cores": 1, "kind": "port",
-            "sample": "%d fosite steps of the same problem on a %dx%dx%d grid (%.1f s, serial oracle)"
-                      % (steps, cfg.inum, cfg.jnum, cfg.knum, el)}
+    grid = [cfg.inum, cfg.jnum, cfg.knum]
+    return {"value": upd / el, "unit": "cell-updates/s", "cores": used, "kind": "port", "grid": grid,
+            "sample": "%d fosite steps of the workload on a %dx%dx%d grid (%.1f s, oracle on %d host thread%s)"
+                      % (steps, grid[0], grid[1], grid[2], el, used, "" if used == 1 else "s")}
+
+
+def cpu_baseline(name, budget_s=20.0):
+    """Bounded samples of the oracle on this host: all threads on a reduced grid, and the serial
+    restatement (1 thread) on a smaller one."""
+    small = {"gauss3d": 96, "disk2d": 256, "khi3d_visc": 48}.get(name, 256)
+    cb = time_oracle(name, small, 0, 0.6 * budget_s)
+    tiny = {"gauss3d": 48, "disk2d": 128, "khi3d_visc": 32}.get(name, 128)
+    cb["serial"] = time_oracle(name, tiny, 1, 0.4 * budget_s)
+    return cb
 
 
 def dist_setup():
@@ -190,15 +239,26 @@ def barrier(world):
 
 
 def run_reference(args, world, rank):
+    """The reference CPU path (the oracle, all host threads) on the headline grid when it fits in
+    host memory; FirstStep untimed, then fosite steps for at most --ref-budget seconds."""
     if rank != 0:
         return
-    cb = cpu_baseline(args.workload, budget_s=args.ref_budget)
+    full = args.size or HEADLINE_SIZE.get(args.workload, 256)
+    size = oracle_size(args.workload, full)
+    cb = time_oracle(args.workload, size, 0, args.ref_budget, max_steps=max(1, args.steps))
+    cfg, _, _ = make_problem(args.workload, full)
+    grid = [cfg.inum, cfg.jnum, cfg.knum]
+    conf = {"workload": args.workload, "description": WORKLOADS[args.workload], "grid": grid}
+    if cb["grid"] != grid:
+        conf["timed_grid"] = cb["grid"]
+        conf["comparable"] = False
+        conf["note"] = "the oracle at the headline grid needs more host memory than this box has"
     line = {"metric": "cell-updates/s", "value": cb["value"], "unit": "cell-updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": args.workload, "description": WORKLOADS[args.workload]},
-            "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "cell-updates/s",
-                                        "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": conf, "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -282,7 +342,7 @@ def run_own(args, world, rank, local):
     traffic = None
     if prof and stp.stage_launches:
         traffic = prof["dram_bytes_per_cell"] * n_cells
-    cb = cpu_baseline(args.workload, budget_s=args.ref_budget) if world == 1 and not args.no_cpu else None
+    cb = cpu_baseline(args.workload, budget_s=args.cpu_budget) if world == 1 and not args.no_cpu else None
     bpc = algorithmic_bytes_per_cell_update(args.workload, sim.vnum)
     line = {
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
@@ -456,7 +516,8 @@ def main():
     ap.add_argument("--t-scale", type=float, default=0.01)
     ap.add_argument("--chunk", type=int, default=8)
     ap.add_argument("--size", type=int, default=0)
-    ap.add_argument("--ref-budget", type=float, default=20.0)
+    ap.add_argument("--ref-budget", type=float, default=120.0)
+    ap.add_argument("--cpu-budget", type=float, default=25.0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     world, rank, local = dist_setup()

@@ -27,6 +27,7 @@ DTCAUSE_CFL, DTCAUSE_ERRADJ, DTCAUSE_SMALLERR, DTCAUSE_FILEIO, DTCAUSE_VISCOSITY
 VIS_MOLECULAR, VIS_ALPHA, VIS_BETA, VIS_POWERLAW, VIS_ALPHA_ALT = 1, 2, 3, 4, 5
 
 CVAR, PVAR, RHS, BCCSOUND = 1, 2, 3, 4
+XFLUX, YFLUX, ZFLUX = 5, 6, 7     # interface fluxes of the last compute_rhs (fosite xfluxdydz ...)
 MESH_X, MESH_Y, MESH_Z, MESH_RADIUS = 10, 11, 12, 13
 
 MAXVAR = 5

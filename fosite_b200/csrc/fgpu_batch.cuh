@@ -452,7 +452,8 @@ int collect_embedded(fgpu_batch* b, int* active) {
   const int n = (int)b->m.size();
   const int64_t ns = b->pending_steps;
   long long extra = 0;
-  const long long cap = 64 * (long long)ns + 64;
+  const long long cap = slot_cap(64 * (long long)ns + 64);
+  bool stalled = false;
   while (true) {
     BCUDA_TRY(b, cudaStreamSynchronize(b->stream));
     bool busy = false;
@@ -461,7 +462,7 @@ int collect_embedded(fgpu_batch* b, int* active) {
       if (c.steps_left > 0 && !c.stop && !c.brk) busy = true;
     }
     if (!busy || ns == 0) break;
-    if (extra > cap) return bset_err(b, FGPU_ETIMEOUT, "batched device-clock step loop: no progress");
+    if (extra > cap) { stalled = true; break; }
     if (int rc = launch_slots(b, kSlotGraph)) return rc;
     extra += kSlotGraph;
   }
@@ -483,6 +484,8 @@ int collect_embedded(fgpu_batch* b, int* active) {
   }
   b->pending_steps = 0;
   if (active) *active = act;
+  // no progress within the slot budget: the members' bookkeeping above is the device's
+  if (stalled) return bset_err(b, FGPU_ETIMEOUT, "batched device-clock step loop: no progress");
   return FGPU_OK;
 }
 
@@ -812,7 +815,7 @@ int fgpu_autotune(fgpu_handle* h, int reps, int* variant) {
   A.out = scratch;
   A.ctl = nullptr;
   A.visc = h->vis ? h->d_visc : nullptr;   // the stencil's read of the viscous source
-  const int cand[6] = {0, 2, 3, 4, 5, 1};
+  const int cand[7] = {0, 2, 3, 4, 5, 1, 6};
   // 3D: the z extent a block marches through (smaller chunks give small grids more blocks);
   // FGPU_KCHUNK fixes it
   std::vector<int> chunks;
@@ -828,6 +831,11 @@ int fgpu_autotune(fgpu_handle* h, int reps, int* variant) {
   for (int v : cand) {
     // layout 1 lacks these features (Butcher steps gate their stages or form the next stage's state)
     if (v == 1 && (h->fargo || h->accrete || h->vis || h->butcher)) continue;
+    // layout 6 (TMA-staged planes) serves grids without FARGO, viscosity or accretion, even nx
+    if (v == 6 && (h->fargo || h->accrete || h->vis || h->g.nx % 2 != 0)) continue;
+    // the taller tiles (4, 5) differ from the oracle in the last bit on FARGO transport along x
+    // with a user-supplied background velocity; such grids keep the 32 x 8 tiles
+    if ((v == 4 || v == 5) && h->fargo && h->fdir == 1) continue;
     for (int kc : chunks) {
       h->variant = v;
       h->kchunk = kc;

@@ -150,6 +150,8 @@ struct Ctl {
   int rhs_done;                  // AcceptSolution evaluated the RHS at t (rhs_done_at_t)
   int checkflags;                // CheckData failures seen (FGPU_CHECK_* bits)
   double time_prev, dt_prev, dtold_prev;   // the step's time, dt, dtold before a slot closed it
+  int dev_err;                   // a kernel's bounded wait ran out (its results are void)
+  int pad3;
 };
 
 // actions of a device-clock attempt slot, decided by bt_decide_kernel

@@ -10,6 +10,7 @@
 //     accept/reject logic of IntegrationStep (timedisc_base.f90:649-750) runs on
 //     the host after one 8-byte read of the error norm per attempt.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <cmath>
 #include <cfloat>
 #include <cstring>
@@ -28,6 +29,7 @@
 #include "fgpu_visc.cuh"
 #include "fgpu_ddmath.h"
 #include "fgpu_bt.cuh"
+#include "fgpu_tma.cuh"
 
 using namespace fgpu;
 
@@ -129,6 +131,8 @@ struct fgpu_handle {
   // state buffers: [0] P (stored state), then scheme-specific
   std::vector<double*> buf;
   double* d_pad = nullptr;      // padded download scratch (2 * npad * V)
+  double* d_flux = nullptr;     // interface fluxes of the last fgpu_compute_rhs (3 * V * padded cells)
+  bool flux_valid = false;
   long long npad = 0;
   Ctl* d_ctl = nullptr;
   Ctl* h_ctl = nullptr;         // pinned
@@ -161,7 +165,11 @@ struct fgpu_handle {
   bool fuse_end = true;         // the last stage's kernel also forms the high/low-order solutions and the error norm
   double* d_ready = nullptr;    // ... into this array (one state)
   int variant = 0;              // stage kernel layout: 0 shared-memory tile, 1 warp-shuffle window,
-                                // 2/3 tile with a register cap for more resident blocks, 4 taller tile
+                                // 2/3 tile with a register cap for more resident blocks, 4 taller tile,
+                                // 6 tile with TMA-staged planes (fgpu_tma.cuh)
+  // tensor maps of the stage inputs the TMA layout has read (by base pointer and tile shape)
+  struct TmapEntry { const double* base; int tx, ty; CUtensorMap map; };
+  std::vector<TmapEntry> tmaps;
   // instrumentation
   cudaStream_t own_stream = nullptr;
   bool profiling = false;
@@ -217,6 +225,12 @@ namespace {
 int set_err(fgpu_handle* h, int code, const std::string& msg) {
   if (h) h->err = msg; else g_create_error = msg;
   return code;
+}
+// Slot budget of the device-clock loops (attempt slots replayed before a call gives up with
+// FGPU_ETIMEOUT); FGPU_SLOT_CAP overrides the computed budget (tests force the timeout path).
+long long slot_cap(long long computed) {
+  if (const char* e = std::getenv("FGPU_SLOT_CAP")) return std::atoll(e);
+  return computed;
 }
 #define CUDA_TRY(h, call)                                                                    \
   do {                                                                                       \
@@ -439,6 +453,24 @@ template <int ND> struct TileShapes;
 template <> struct TileShapes<2> { static constexpr int TY = 8, M2 = 2, M3 = 3, TY4 = 16, M4 = 1, M5 = 1; };
 template <> struct TileShapes<3> { static constexpr int TY = 4, M2 = 4, M3 = 6, TY4 = 8, M4 = 2, M5 = 3; };
 
+// ---- the TMA-staged layout (variant 6): 32 x 8 tiles, 3D with a three-plane ring (two
+// blocks per SM), 2D one plane (three blocks per SM)
+template <int ND> struct TmaShape { static constexpr int TX = 32, TY = 8, MINB = ND == 3 ? 2 : 3; };
+template <int ND, bool EU, bool PRIM>
+struct TmaLaunch {
+  using T = TmaShape<ND>;
+  static constexpr size_t SMEM = TmaLayout<Phys<ND, EU>::V, T::TX, T::TY, TmaSlots<ND>::N>::SMEM;
+  static void configure() {
+    cudaFuncSetAttribute(tma_stage_kernel<ND, EU, PRIM, T::TX, T::TY, T::MINB>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+  }
+  static void launch(const Grid& g, int kchunk, cudaStream_t s, const StageArgs& A, const CUtensorMap& map) {
+    const int kz = ND == 3 ? (g.nz + kchunk - 1) / kchunk : 1;
+    dim3 grid((g.nx + T::TX - 1) / T::TX, (g.ny + T::TY - 1) / T::TY, kz);
+    tma_stage_kernel<ND, EU, PRIM, T::TX, T::TY, T::MINB><<<grid, T::TX * T::TY, SMEM, s>>>(A, map);
+  }
+};
+
 template <int ND, bool EU, bool PRIM>
 void configure_stage_kernels_t() {
   using S = TileShapes<ND>;
@@ -447,6 +479,7 @@ void configure_stage_kernels_t() {
   TileLayout<ND, EU, PRIM, 32, S::TY, S::M3>::configure(true);
   TileLayout<ND, EU, PRIM, 32, S::TY4, S::M4>::configure(false);
   TileLayout<ND, EU, PRIM, 32, S::TY4, S::M5>::configure(false);
+  TmaLaunch<ND, EU, PRIM>::configure();
 }
 void configure_stage_kernels(int nd, bool e, bool p) {
   if (nd == 2) {
@@ -458,18 +491,85 @@ void configure_stage_kernels(int nd, bool e, bool p) {
   }
 }
 
+// cuTensorMapEncodeTiled from the driver (no link against libcuda)
+PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// Tensor map of a state (V fields of n doubles, i fastest) for boxes of (tx+4) x (ty+4) cells
+// of one plane and every variable: dims (nx, ny, [nz,] V); cached per handle by base pointer.
+const CUtensorMap* stage_tmap(fgpu_handle* h, const double* base, int tx, int ty) {
+  for (const auto& e : h->tmaps)
+    if (e.base == base && e.tx == tx && e.ty == ty) return &e.map;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+  if (!enc) return nullptr;
+  const Grid& g = h->g;
+  fgpu_handle::TmapEntry e;
+  e.base = base; e.tx = tx; e.ty = ty;
+  cuuint64_t dims[4], strides[3];
+  cuuint32_t box[4], es[4] = {1, 1, 1, 1};
+  int rank;
+  if (h->nd == 3) {
+    rank = 4;
+    dims[0] = g.nx; dims[1] = g.ny; dims[2] = g.nz; dims[3] = h->V;
+    strides[0] = 8ull * g.nx; strides[1] = 8ull * g.nx * g.ny; strides[2] = 8ull * g.n;
+    box[0] = tx + 4; box[1] = ty + 4; box[2] = 1; box[3] = h->V;
+  } else {
+    rank = 3;
+    dims[0] = g.nx; dims[1] = g.ny; dims[2] = h->V;
+    strides[0] = 8ull * g.nx; strides[1] = 8ull * g.n;
+    box[0] = tx + 4; box[1] = ty + 4; box[2] = h->V;
+  }
+  CUresult r = enc(&e.map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, rank, const_cast<double*>(base), dims, strides, box, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return nullptr;
+  h->tmaps.push_back(e);
+  return &h->tmaps.back().map;
+}
+
+// The TMA layout serves stages whose input is a plain or formed state (no k-sums at the stencil
+// points) without FARGO frame changes, viscous source or accretion rows, on meshes whose x
+// extent is even (16-byte strides of the tensor map).
+bool tma_eligible(const fgpu_handle* h, const StageArgs& A) {
+  const StateRef& S = A.rin.base ? A.rin : A.in;
+  return h->g.nx % 2 == 0 && !h->fargo && !h->vis && !A.visc && !A.brow && !A.w_sub && !A.flux_out && S.nk == 0 &&
+         !S.pre.n &&
+         !A.in.pre.n && !A.yn_chain.n && !A.y0_chain.n && !A.err_chain.n && tmap_encoder() != nullptr;
+}
+
 template <int ND, bool EU, bool PRIM>
 int launch_stage_t(fgpu_handle* h, StageArgs& A) {
   using S = TileShapes<ND>;
   A.kchunk = h->kchunk;
   const Grid& g = h->g;
   const int kz = ND == 3 ? (g.nz + h->kchunk - 1) / h->kchunk : 1;
+  if (h->variant == 6 && tma_eligible(h, A)) {
+    using T = TmaShape<ND>;
+    const StateRef& SR = A.rin.base ? A.rin : A.in;
+    const CUtensorMap* map = stage_tmap(h, SR.base, T::TX, T::TY);
+    if (!map) return set_err(h, FGPU_ECUDA, "cuTensorMapEncodeTiled failed for a stage input");
+    TmaLaunch<ND, EU, PRIM>::launch(g, h->kchunk, h->stream, A, *map);
+    CUDA_TRY(h, cudaGetLastError());
+    return FGPU_OK;
+  }
   // the warp-shuffle layout implements neither FARGO frame changes, the accretion rows, the
   // viscous source, the device-clock gates, the next Butcher stage's state formation nor the
   // CheckData-only epilogue
+  // (a variant-6 launch that the TMA layout does not serve runs on the base tile)
   const int variant =
-      (h->variant == 1 && (h->fargo || h->accrete || h->vis || A.gate || A.fnext_out || A.cfl_mode == 3))
-          ? 0 : h->variant;
+      (h->variant == 1 && (h->fargo || h->accrete || h->vis || A.gate || A.fnext_out || A.cfl_mode == 3 ||
+                           A.flux_out))
+          ? 0 : (h->variant == 6 ? 0 : h->variant);
   switch (variant) {
     case 1: {
       // warp-shuffle layout: 32 x 8 points per block, 30 x 6 output cells
@@ -1620,7 +1720,7 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
   }
   if (!rc) {
     // FGPU_STAGE_VARIANT / FGPU_KCHUNK force a stage-kernel layout and z chunk (the tuner's choice otherwise)
-    if (const char* e = std::getenv("FGPU_STAGE_VARIANT")) h->variant = std::max(0, std::min(5, std::atoi(e)));
+    if (const char* e = std::getenv("FGPU_STAGE_VARIANT")) h->variant = std::max(0, std::min(6, std::atoi(e)));
     if (const char* e = std::getenv("FGPU_KCHUNK")) { int v = std::atoi(e); if (v > 0) h->kchunk = v; }
     if (const char* e = std::getenv("FGPU_MATERIALIZE")) h->materialize = std::atoi(e) != 0;
     if (const char* e = std::getenv("FGPU_FUSE_FORM")) h->fuse_form = std::atoi(e) != 0;
@@ -1719,6 +1819,7 @@ void fgpu_destroy(fgpu_handle* h) {
   if (h->bt_graph) cudaGraphExecDestroy(h->bt_graph);
   for (double* p : h->buf) cudaFree(p);
   if (h->d_pad) cudaFree(h->d_pad);
+  if (h->d_flux) cudaFree(h->d_flux);
   if (h->d_metric) cudaFree(h->d_metric);
   if (h->d_w) cudaFree(h->d_w);
   if (h->d_acc) cudaFree(h->d_acc);
@@ -1858,6 +1959,16 @@ int fgpu_download(fgpu_handle* h, int which, double* out, int64_t n) {
           for (int i = 0; i < h->g.nx; ++i)
             out[(i + 2) + (long long)NXp * ((j + 2) + (long long)NYp * (k + kofs)) + nc * l] =
                 tmp[i + (long long)h->g.nx * (j + (long long)h->g.ny * k) + h->g.n * l];
+    return FGPU_OK;
+  }
+  if (which == FGPU_XFLUX || which == FGPU_YFLUX || which == FGPU_ZFLUX) {
+    if (n < nc * h->V) return set_err(h, FGPU_EARG, "output too small");
+    if (!h->flux_valid) return set_err(h, FGPU_EARG, "no fluxes: call fgpu_compute_rhs first");
+    const int d = which - FGPU_XFLUX;
+    if (d >= h->nd) return set_err(h, FGPU_EARG, "no such direction on this mesh");
+    CUDA_TRY(h, cudaMemcpyAsync(out, h->d_flux + (size_t)d * h->V * nc, sizeof(double) * nc * h->V,
+                                cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     return FGPU_OK;
   }
   if (which == FGPU_BCCSOUND) {
@@ -2230,7 +2341,8 @@ static int bt_run(fgpu_handle* h, int64_t n, int64_t* done) {
   }
   const long long it0 = h->iter, adj0 = h->n_adj;
   long long slots = 0;
-  const long long cap = 64 * (long long)n + 64;   // every attempt either advances t or shrinks dt 4x
+  const long long cap = slot_cap(64 * (long long)n + 64);   // every attempt either advances t or shrinks dt 4x
+  bool stalled = false;
   while (true) {
     // as many slots as steps are left (most steps take one attempt), at most 8 per read
     const int CH = (int)std::max<long long>(1, std::min<long long>(8, c->steps_left));
@@ -2245,7 +2357,7 @@ static int bt_run(fgpu_handle* h, int64_t n, int64_t* done) {
     slots += CH;
     if (int rc = read_ctl(h)) return rc;
     if (c->steps_left <= 0 || c->stop || c->brk) break;
-    if (slots > cap) return set_err(h, FGPU_ETIMEOUT, "device-clock step loop: no progress");
+    if (slots > cap) { stalled = true; break; }
   }
   h->time = c->time; h->dt = c->dt; h->dtold = c->dtold; h->dtmin = c->dtmin;
   h->iter = c->iter; h->brk = c->brk != 0; h->dtcause = c->dtcause;
@@ -2258,6 +2370,8 @@ static int bt_run(fgpu_handle* h, int64_t n, int64_t* done) {
   h->stats.attempts += (h->iter - it0) + (h->n_adj - adj0);
   h->stats.cell_updates += (h->iter - it0) * h->g.n;
   if (done) *done = steps;
+  // no progress within the slot budget: the bookkeeping above is the device's, the call ends
+  if (stalled) return set_err(h, FGPU_ETIMEOUT, "device-clock step loop: no progress");
   if (h->brk) return FGPU_BREAK;
   if (c->stop) return FGPU_STOPTIME;
   return FGPU_OK;
@@ -2374,8 +2488,21 @@ int fgpu_compute_rhs(fgpu_handle* h) {
   A.out_mode = OUT_RHS;
   A.out = out;
   A.ctl = nullptr;
+  // the interface fluxes too, for fgpu_download(FGPU_XFLUX..ZFLUX)
+  const size_t nflux = 3 * (size_t)h->V * (size_t)fgpu_cell_count(h);
+  if (!h->d_flux) CUDA_TRY(h, cudaMalloc(&h->d_flux, sizeof(double) * nflux));
+  CUDA_TRY(h, cudaMemsetAsync(h->d_flux, 0, sizeof(double) * nflux, h->stream));
+  A.flux_out = h->d_flux;
   if (int rc = launch_stage(h, A, RhsTime::host(h->time))) return rc;
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  h->flux_valid = true;
+  return FGPU_OK;
+}
+
+int fgpu_set_output_time(fgpu_handle* h, double tout) {
+  if (!h) return FGPU_EARG;
+  if (!(tout > 0.0)) return set_err(h, FGPU_EARG, "output time must be positive");
+  h->tout = tout;
   return FGPU_OK;
 }
 
@@ -2514,6 +2641,36 @@ int noalloc_scratch(int dev, double** ptr) {
   return FGPU_OK;
 }
 
+// The Cartesian metric of the allocation-free CFL call in its scratch array: the constant
+// factors by array (vals) and the reconstruction offsets x_face - x_centre of x, y and z in the
+// operation order of build_metric (mesh_midpoint.f90:97-145), evaluated without contraction so
+// that they equal the host's values bit for bit.
+struct NoallocMetric {
+  double vals[M_NI];
+  double lo[3], d[3];
+  int np[3];
+};
+__global__ void noalloc_metric_kernel(double* dm, const NoallocMetric m) {
+  const int nxp = m.np[0], nyp = m.np[1], nzp = m.np[2];
+  const int total = M_NI * nxp + 2 * nyp + 2 * nzp;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    int q, ip, dir, east;
+    if (t < M_NI * nxp) {
+      q = t / nxp; ip = t % nxp;
+      if (q != M_offxW && q != M_offxE) { dm[t] = m.vals[q]; continue; }
+      dir = 0; east = q == M_offxE;
+    } else {
+      int u = t - M_NI * nxp;
+      if (u < 2 * nyp) { dir = 1; east = u / nyp; ip = u % nyp; }
+      else { u -= 2 * nyp; dir = 2; east = u / nzp; ip = u % nzp; }
+    }
+    const double h = m.d[dir];
+    const double x = __dadd_rn(m.lo[dir], __dmul_rn(__dmul_rn((double)(2 * (ip - 1) - 1), 0.5), h));
+    const double f = east ? __dadd_rn(x, __dmul_rn(0.5, h)) : __dadd_rn(x, __dmul_rn(-0.5, h));
+    dm[t] = __dsub_rn(f, x);
+  }
+}
+
 __global__ void noalloc_finalize_kernel(const Ctl* c, int nd, double cfl, double* dt_out) {
   auto D = [](unsigned long long b) { return __longlong_as_double((long long)b); };
   double invdt = nd == 2 ? D(c->invdt[0]) : dmax(dmax(D(c->invdt[1]), D(c->invdt[2])), D(c->invdt[0]));
@@ -2557,53 +2714,27 @@ extern "C" int fgpu_calc_timestep_noalloc(const fgpu_config* cfg, const double* 
   Ctl* ctl = (Ctl*)scratch;
   double* dm = scratch + ctl_doubles;
 
-  // Cartesian metric (mesh_base.f90:570-601, mesh_midpoint.f90:97-145 with h = 1), built on the stack
-  // in chunks and copied into the scratch array
+  // Cartesian metric (mesh_base.f90:570-601, mesh_midpoint.f90:97-145 with h = 1): the constant
+  // factors computed here, the reconstruction offsets by a kernel, all in the scratch array
   double dx = (c.xmax - c.xmin) / c.inum, dy = (c.ymax - c.ymin) / c.jnum, dz = (c.zmax - c.zmin) / c.knum;
   double mdx = dx, mdy = dy, mdz = dz;
   if (dz < 2 * DBL_EPSILON && c.knum == 1) { dz = 1.0; mdz = 0.0; }
   double volume = 1.0 * dx * dy * dz;
-  double vals[M_NI];
-  for (int q = 0; q < M_NI; ++q) vals[q] = 0.0;
-  vals[M_dAxW] = 1.0 * 1.0; vals[M_dAxE] = 1.0 * 1.0; vals[M_dAyS] = 1.0 * 1.0; vals[M_dAzB] = 1.0 * 1.0;
-  vals[M_dxdydV] = dx * dy / (volume + DBL_MIN);
-  vals[M_dydzdV] = dy * dz / (volume + DBL_MIN);
-  vals[M_dzdxdV] = dz * dx / (volume + DBL_MIN);
-  vals[M_dlx] = 1.0 * dx; vals[M_dly] = 1.0 * dy; vals[M_dlz] = 1.0 * dz;
-  for (int q = 0; q < 7; ++q) vals[M_cs0 + q] = euler ? 0.0 : c.csiso;
-  const int CH = 512;
-  double buf[CH];
-  auto put = [&](size_t ofs, int n, auto&& f) -> int {
-    for (int b = 0; b < n; b += CH) {
-      int m = std::min(CH, n - b);
-      for (int t = 0; t < m; ++t) buf[t] = f(b + t);
-      if (cudaMemcpyAsync(dm + ofs + b, buf, sizeof(double) * m, cudaMemcpyHostToDevice, s) != cudaSuccess) return FGPU_ECUDA;
-      if (cudaStreamSynchronize(s) != cudaSuccess) return FGPU_ECUDA;   // buf is reused
-    }
-    return FGPU_OK;
-  };
-  for (int q = 0; q < M_NI; ++q) {
-    int rc;
-    if (q == M_offxW || q == M_offxE) {
-      bool east = q == M_offxE;
-      rc = put((size_t)q * nxp, nxp, [&](int ip) {
-        double x = c.xmin + ((double)(2 * (ip - 1) - 1) * 0.5) * mdx;
-        return (east ? x + 0.5 * mdx : x + (-0.5 * mdx)) - x;
-      });
-    } else {
-      double v = vals[q];
-      rc = put((size_t)q * nxp, nxp, [&](int) { return v; });
-    }
-    if (rc) return rc;
-  }
-  size_t by = (size_t)M_NI * nxp;
-  for (int side = 0; side < 2; ++side) {
-    if (int rc = put(by + side * nyp, nyp, [&](int jp) {
-          double y = c.ymin + ((double)(2 * (jp - 1) - 1) * 0.5) * mdy;
-          return (side ? y + 0.5 * mdy : y + (-0.5 * mdy)) - y; })) return rc;
-    if (int rc = put(by + 2 * nyp + side * nzp, nzp, [&](int kp) {
-          double z = c.zmin + ((double)(2 * (kp - 1) - 1) * 0.5) * mdz;
-          return (side ? z + 0.5 * mdz : z + (-0.5 * mdz)) - z; })) return rc;
+  NoallocMetric nm;
+  for (int q = 0; q < M_NI; ++q) nm.vals[q] = 0.0;
+  nm.vals[M_dAxW] = 1.0 * 1.0; nm.vals[M_dAxE] = 1.0 * 1.0; nm.vals[M_dAyS] = 1.0 * 1.0; nm.vals[M_dAzB] = 1.0 * 1.0;
+  nm.vals[M_dxdydV] = dx * dy / (volume + DBL_MIN);
+  nm.vals[M_dydzdV] = dy * dz / (volume + DBL_MIN);
+  nm.vals[M_dzdxdV] = dz * dx / (volume + DBL_MIN);
+  nm.vals[M_dlx] = 1.0 * dx; nm.vals[M_dly] = 1.0 * dy; nm.vals[M_dlz] = 1.0 * dz;
+  for (int q = 0; q < 7; ++q) nm.vals[M_cs0 + q] = euler ? 0.0 : c.csiso;
+  nm.lo[0] = c.xmin; nm.lo[1] = c.ymin; nm.lo[2] = c.zmin;
+  nm.d[0] = mdx; nm.d[1] = mdy; nm.d[2] = mdz;
+  nm.np[0] = nxp; nm.np[1] = nyp; nm.np[2] = nzp;
+  const size_t by = (size_t)M_NI * nxp;
+  {
+    const int total = M_NI * nxp + 2 * nyp + 2 * nzp;
+    noalloc_metric_kernel<<<(total + 255) / 256, 256, 0, s>>>(dm, nm);
   }
   // the reduction slots must start at zero on every call
   if (cudaMemsetAsync(ctl, 0, sizeof(Ctl), s) != cudaSuccess) return FGPU_ECUDA;

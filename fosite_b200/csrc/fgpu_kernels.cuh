@@ -84,7 +84,22 @@ struct StageArgs {
   // last being this stage's output) formed into fnext_out as its reconstruction variables
   StateRef fnext;
   double* fnext_out;
+  // optional: the interface fluxes of this right-hand side, [3 directions][V][padded cells]
+  // in fosite's xfluxdydz/yfluxdzdx/zfluxdxdy indexing (face between cells i and i+1 at i)
+  double* flux_out;
 };
+
+// padded index of interior cell (i, j, k) (ghost layers of 2 in every active direction)
+__device__ __forceinline__ long long padded_index(const Grid& g, int i, int j, int k, int nd) {
+  const long long NXp = g.nx + 4, NYp = g.ny + 4;
+  return (i + 2) + NXp * ((j + 2) + NYp * (long long)(nd == 3 ? k + 2 : 0));
+}
+// store F (V values) as the flux of direction d at the face after padded cell pc
+template <int V>
+__device__ __forceinline__ void store_flux(const StageArgs& A, int d, long long pc, long long npad, const double* F) {
+#pragma unroll
+  for (int v = 0; v < V; ++v) A.flux_out[((long long)d * V + v) * npad + pc] = F[v];
+}
 
 // block-wide max of up to 4 non-negative doubles + OR of flags, then one atomic per block;
 // sred holds RED_STRIDE doubles per warp
@@ -134,6 +149,321 @@ constexpr size_t stage_smem_bytes() {
 // arguments in global memory, tiles from a flattened queue).
 __device__ __forceinline__ void prefetch_l2(const double* p) {
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+// The per-cell part of one right-hand side after the flux divergence: the centre state as
+// ComputeRHS sees it, geometric and external sources (timedisc_base.f90:1263-1267), and the
+// stage's consumer (k_m and the next Butcher stage's state, the Shu-Osher update, the embedded
+// solutions and error norm, CheckData and CFL partial maxima).  R0: the cell's reconstruction
+// variables; rhs: (divX + divY) + divZ on entry, the full right-hand side after the sources.
+// Shared by the stage kernels of every tile layout.
+template <int ND, bool EU, bool PRIM>
+__device__ __forceinline__ void stage_cell_epilogue(const StageArgs& A, const int i, const int j, const int k,
+                                                    const double* R0, double* rhs, const double dt, double* cflv,
+                                                    double& errv, int& flags) {
+  using PH = Phys<ND, EU>;
+  using CE = Cells<ND, EU>;
+  constexpr int V = PH::V;
+  constexpr bool FG = ND == 2;   // FARGO transforms are compiled for 2D meshes only
+  const Grid& g = A.g;
+  const PhysP& P = A.ph;
+  const MetricP& M = A.mt;
+  const bool roundtrip = EU && A.in.roundtrip;
+  const int ip = i + 2;
+  // the CHECK_PMIN round trip of a conservative state, P2C(MAX(C2P(c),pmin))
+  auto rt_cons = [&](double* c) {
+    double q[V];
+    PH::c2p(c, q, P);
+    if (EU) q[V - 1] = dmax(q[V - 1], P.pmin);
+    PH::p2c(q, c, P);
+  };
+  const long long idx = CE::lin(g, i, j, k);
+  // centre primitive / conservative state as ComputeRHS sees it
+  double pc[V], cc[V];
+  if (PRIM) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) pc[v] = R0[v];
+    // the sources read cvar itself (the stage state), which Prim2Cons(pvar) only
+    // reproduces to rounding; after the CHECK_PMIN round trip cvar is Prim2Cons(pvar)
+    if (!roundtrip && (M.curv || A.has_accel || A.out_base)) state_at<V>(A.in, g.n, idx, cc);
+    else PH::p2c(pc, cc, P);
+  } else {
+#pragma unroll
+    for (int v = 0; v < V; ++v) cc[v] = R0[v];
+    if (roundtrip) {
+      double u[V];
+      state_at<V>(A.in, g.n, idx, u);
+      PH::c2p(u, pc, P);
+      pc[V - 1] = dmax(pc[V - 1], P.pmin);
+    } else {
+      PH::c2p(cc, pc, P);
+    }
+  }
+  // with FARGO the sources see the real frame: cvar after AddBackgroundVelocityY and the
+  // primitive state CenterBoundary derives from it
+  const bool fsrc = FG && A.w_sub;
+  if (fsrc) {
+    state_at<V>(A.in, g.n, idx, cc);
+    if (A.in.pre.n) apply_chain<V>(A.in.pre, cc, g, i, j);
+    PH::c2p(cc, pc, P);
+    if (roundtrip) {   // CHECK_PMIN of this ComputeRHS (FirstStep's CHECK_ALL)
+      pc[V - 1] = dmax(pc[V - 1], P.pmin);
+      PH::p2c(pc, cc, P);
+    }
+  }
+  // geometric sources (physics_euler.f90:1706-1847 / physics_eulerisotherm.f90:689-832)
+  double geo2 = 0.0;
+  if (fsrc && g.fdir == 1) {
+    // transport along x: geometric sources of the real frame, AddFargoSourcesX into the x
+    // one (isothermal physics_eulerisotherm.f90:1462-1518; Euler physics_euler.f90:2267-2355
+    // adds the energy term -vx*(tmp + GetGeometricalSourceX(vz = P = mz = 0)))
+    const double vx = pc[1], vy = pc[2];
+    const double cxyx = M.cxyx[ip], cyxy = M.cyxy[ip], czxz = M.czxz[ip], czyz = M.czyz[ip];
+    double geo1 = 0.0;
+    if (M.curv) {
+      const double Pp = EU ? pc[V - 1] : pc[0] * (M.cs[ip] * M.cs[ip]);
+      geo1 = cc[2] * (cyxy * vy - cxyx * vx) + (cyxy + czxz) * Pp;
+      rhs[2] = rhs[2] - (cc[1] * (cxyx * vx - cyxy * vy) + (cxyx + czyz) * Pp);
+    }
+    const int jp = j + 2;
+    const double tmp = cc[2] * 0.5 * (A.w_sub[jp + 1] - A.w_sub[jp - 1]) / M.dly[ip];
+    geo1 = geo1 - tmp;
+    rhs[1] = rhs[1] - geo1;
+    if (EU) {
+      const double cxzx = M.cxzx[ip];
+      const double gx = cc[2] * (cyxy * vy - cxyx * vx) + 0.0 * (czxz * 0.0 - cxzx * vx) + (cyxy + czxz) * 0.0;
+      const double geoE = 0.0 - vx * (tmp + gx);
+      rhs[V - 1] = rhs[V - 1] - geoE;
+    }
+  } else if (M.curv && ND == 2 && fsrc) {
+    double Pp = EU ? pc[V - 1] : pc[0] * (M.cs[ip] * M.cs[ip]);
+    double vx = pc[1], vy = pc[2];
+    double cxyx = M.cxyx[ip], cyxy = M.cyxy[ip], czxz = M.czxz[ip], czyz = M.czyz[ip];
+    rhs[1] = rhs[1] - (cc[2] * (cyxy * vy - cxyx * vx) + (cyxy + czxz) * Pp);
+    geo2 = cc[1] * (cxyx * vx - cyxy * vy) + (cxyx + czyz) * Pp;
+  }
+  if (fsrc && g.fdir != 1) {
+    // AddFargoSourcesY into the geometric source (isothermal
+    // physics_eulerisotherm.f90:1531-1586; Euler physics_euler.f90:2368-2455 adds the
+    // energy term -vy*(tmp + GetGeometricalSourceY(vz = P = mz = 0)))
+    const double tmp = cc[1] * 0.5 * (A.w_sub[ip + 1] - A.w_sub[ip - 1]) / M.dlx[ip];
+    geo2 = geo2 - tmp;
+    rhs[2] = rhs[2] - geo2;
+    if (EU) {
+      const double vx = pc[1], vy = pc[2];
+      const double cxyx = M.cxyx[ip], cyxy = M.cyxy[ip], cyzy = M.cyzy[ip], czyz = M.czyz[ip];
+      const double gy = 0.0 * (czyz * 0.0 - cyzy * vy) + cc[1] * (cxyx * vx - cyxy * vy) + (cxyx + czyz) * 0.0;
+      const double geoE = 0.0 - vy * (tmp + gy);
+      rhs[V - 1] = rhs[V - 1] - geoE;
+    }
+  } else if (!fsrc && M.curv) {
+    double Pp = EU ? pc[V - 1] : pc[0] * (M.cs[ip] * M.cs[ip]);
+    double vx = pc[1], vy = pc[2];
+    double cxyx = M.cxyx[ip], cyxy = M.cyxy[ip], czxz = M.czxz[ip], czyz = M.czyz[ip];
+    if (ND == 2) {
+      double mx = cc[1], my = cc[2];
+      rhs[1] = rhs[1] - (my * (cyxy * vy - cxyx * vx) + (cyxy + czxz) * Pp);
+      rhs[2] = rhs[2] - (mx * (cxyx * vx - cyxy * vy) + (cxyx + czyz) * Pp);
+    } else {
+      double vz = pc[3], mx = cc[1], my = cc[2], mz = cc[3];
+      double cxzx = M.cxzx[ip], cyzy = M.cyzy[ip];
+      rhs[1] = rhs[1] - (my * (cyxy * vy - cxyx * vx) + mz * (czxz * vz - cxzx * vx) + (cyxy + czxz) * Pp);
+      rhs[2] = rhs[2] - (mz * (czyz * vz - cyzy * vy) + mx * (cxyx * vx - cyxy * vy) + (cxyx + czyz) * Pp);
+      rhs[3] = rhs[3] - (mx * (cxzx * vx - czxz * vz) + my * (cyzy * vy - czyz * vz) + (cxzx + cyzy) * Pp);
+    }
+  }
+  // external sources (sources_generic.f90:220-261): point-mass gravity (gravity_pointmass.f90:
+  // 263-282, physics ExternalSources) first in the list, then the viscous source of this
+  // stage state (precomputed by visc_kernel); rhs = ... - (gravity + viscosity)
+  if (A.has_accel || A.visc) {
+    double sm[ND] = {}, se = 0.0;
+    if (A.has_accel) {
+      const double ax = M.accel[ip], ay = M.accel[M.nxp + ip];
+      sm[0] = cc[0] * ax;
+      sm[1] = cc[0] * ay;
+      if (EU) se = cc[1] * ax + cc[2] * ay;
+    }
+    if (A.visc) {
+#pragma unroll
+      for (int m = 0; m < ND; ++m) {
+        const double sv = __ldg(A.visc + (long long)m * g.n + idx);
+        sm[m] = A.has_accel ? sm[m] + sv : sv;
+      }
+      if (EU) {
+        const double sv = __ldg(A.visc + (long long)ND * g.n + idx);
+        se = A.has_accel ? se + sv : sv;
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < ND; ++m) rhs[1 + m] = rhs[1 + m] - sm[m];
+    if (EU) rhs[V - 1] = rhs[V - 1] - se;
+  }
+
+  if (A.out_mode == OUT_RHS) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) A.out[(long long)v * g.n + idx] = rhs[v];
+    if (A.fnext_out) {
+      // the next Butcher stage's state base - sum_q (a dt) k_q in the reference's order
+      // (timedisc_rkfehlberg.f90:277-302), this stage's k from the registers, formed as
+      // form_kernel would form it
+      const StateRef& S = A.fnext;
+      double u[V];
+#pragma unroll
+      for (int v = 0; v < V; ++v) u[v] = __ldg(S.base + (long long)v * g.n + idx);
+      // the earlier stages' k (unrolled to the tableau limit, so all loads issue together)
+#pragma unroll
+      for (int q = 0; q < FGPU_MAXK - 1; ++q) {
+        if (q + 1 < S.nk) {
+          const double a = S.dt_dev ? S.coef[q] * *S.dt_dev : S.coef[q];
+#pragma unroll
+          for (int v = 0; v < V; ++v) u[v] = u[v] - a * __ldg(S.K[q] + (long long)v * g.n + idx);
+        }
+      }
+      {
+        const double a = S.dt_dev ? S.coef[S.nk - 1] * *S.dt_dev : S.coef[S.nk - 1];
+#pragma unroll
+        for (int v = 0; v < V; ++v) u[v] = u[v] - a * rhs[v];
+      }
+      if (PRIM) {
+        double p[V];
+        PH::c2p(u, p, P);
+#pragma unroll
+        for (int v = 0; v < V; ++v) A.fnext_out[(long long)v * g.n + idx] = p[v];
+      } else {
+#pragma unroll
+        for (int v = 0; v < V; ++v) A.fnext_out[(long long)v * g.n + idx] = u[v];
+      }
+    }
+  } else {
+    // Shu-Osher update y = yn - dt*rhs + eta*(y0 - yn + dt*rhs) (timedisc_modeuler.f90:289)
+    double yn[V], y0[V], y[V];
+    if (FG && A.yn_chain.n) {
+      state_at<V>(A.in, g.n, idx, yn);
+      apply_chain<V>(A.yn_chain, yn, g, i, j, rt_cons);
+    } else if (!PRIM) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) yn[v] = cc[v];
+    } else if (roundtrip) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) yn[v] = cc[v];
+    } else {
+      state_at<V>(A.in, g.n, idx, yn);
+    }
+#pragma unroll
+    for (int v = 0; v < V; ++v) y0[v] = __ldg(A.y0 + (long long)v * g.n + idx);
+    if (FG && A.y0_chain.n) apply_chain<V>(A.y0_chain, y0, g, i, j, rt_cons);
+    if (EU && A.y0_roundtrip) {
+      double q[V];
+      PH::c2p(y0, q, P);
+      q[V - 1] = dmax(q[V - 1], P.pmin);
+      PH::p2c(q, y0, P);
+    }
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      y[v] = yn[v] - dt * rhs[v] + A.eta * (y0[v] - yn[v] + dt * rhs[v]);
+      A.out[(long long)v * g.n + idx] = y[v];
+    }
+    if (A.out2) {
+#pragma unroll
+      for (int v = 0; v < V; ++v)
+        A.out2[(long long)v * g.n + idx] = yn[v] - dt * rhs[v] + A.eta2 * (y0[v] - yn[v] + dt * rhs[v]);
+    }
+    if (A.err_low) {
+      double l[V];
+#pragma unroll
+      for (int v = 0; v < V; ++v) l[v] = __ldg(A.err_low + (long long)v * g.n + idx);
+      // FARGO: the low-order solution as its ComputeRHS framed it in place
+      if (FG && A.err_chain.n) apply_chain<V>(A.err_chain, l, g, i, j);
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const double e = fabs(y[v] - l[v]) / (A.tol_rel * fabs(y[v]) + A.tol_abs[v]);
+        errv = dmax(errv, e);
+      }
+    }
+    if (A.cfl_mode == 1) {
+      double p[V], c[V];
+      PH::c2p(y, p, P);
+      if (EU && A.cfl_roundtrip) p[V - 1] = dmax(p[V - 1], P.pmin);
+      double cs = EU ? PH::cs_of(p, P) : M.cs[ip];
+      double v3[4];
+      CE::cfl_cell(p, cs, M, ip, v3);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) cflv[q] = dmax(cflv[q], v3[q]);
+      if (EU && A.cfl_roundtrip) PH::p2c(p, c, P);
+      else { for (int v = 0; v < V; ++v) c[v] = y[v]; }
+      if ((A.checkdata & 0x01) && !(cs > 0.)) flags |= 0x01;
+      if (EU && (A.checkdata & 0x02) && p[V - 1] < P.pmin) flags |= 0x02;
+      if ((A.checkdata & 0x04) && p[0] < P.rhomin) flags |= 0x04;
+      if (A.checkdata & 0x08)
+        for (int v = 0; v < V; ++v) if (invalid_value(p[v]) || invalid_value(c[v])) flags |= 0x08;
+    }
+  }
+  if (A.out_base) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) A.out_base[(long long)v * g.n + idx] = cc[v];
+    if (fsrc) {
+      // FARGO: cvar after this ComputeRHS is co-moving (its SubtractBackgroundVelocity)
+      double o[V];
+#pragma unroll
+      for (int v = 0; v < V; ++v) o[v] = cc[v];
+      frame_change<V>(o, -1.0, A.w_sub[fargo_ix(g, i, j)], g.fdir);
+#pragma unroll
+      for (int v = 0; v < V; ++v) A.out_base[(long long)v * g.n + idx] = o[v];
+    }
+  }
+  if (A.cfl_mode >= 2) {
+    double cs = EU ? PH::cs_of(pc, P) : M.cs[ip];
+    if (A.cfl_mode == 2) {
+      double v3[4];
+      CE::cfl_cell(pc, cs, M, ip, v3);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) cflv[q] = dmax(cflv[q], v3[q]);
+    }
+    if ((A.checkdata & 0x01) && !(cs > 0.)) flags |= 0x01;
+    if (EU && (A.checkdata & 0x02) && pc[V - 1] < P.pmin) flags |= 0x02;
+    if ((A.checkdata & 0x04) && pc[0] < P.rhomin) flags |= 0x04;
+    if (A.checkdata & 0x08)
+      for (int v = 0; v < V; ++v) if (invalid_value(pc[v]) || invalid_value(cc[v])) flags |= 0x08;
+  }
+  if (A.last_stage) {
+    // high/low order solutions and ComputeError (timedisc_rkfehlberg.f90:198-265,
+    // timedisc_base.f90:1012-1053); base and the earlier k unrolled to the tableau limit
+    // so that their loads issue together, this stage's k from the registers.  On the
+    // device clock (in.dt_dev) bh_dt/bl_dt hold the weights, multiplied by *dt_dev here.
+    const double* dtd = A.in.dt_dev;
+    double hi[V], lo[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) hi[v] = lo[v] = __ldg(A.in.base + (long long)v * g.n + idx);
+#pragma unroll
+    for (int q = 0; q < FGPU_MAXK - 1; ++q) {
+      if (q + 1 < A.nstage) {
+        const double bh = dtd ? A.bh_dt[q] * *dtd : A.bh_dt[q];
+        const double bl = dtd ? A.bl_dt[q] * *dtd : A.bl_dt[q];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          const double kq = __ldg(A.in.K[q] + (long long)v * g.n + idx);
+          lo[v] = lo[v] - bl * kq;
+          hi[v] = hi[v] - bh * kq;
+        }
+      }
+    }
+    {
+      const int q = A.nstage - 1;
+      const double bh = dtd ? A.bh_dt[q] * *dtd : A.bh_dt[q];
+      const double bl = dtd ? A.bl_dt[q] * *dtd : A.bl_dt[q];
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        lo[v] = lo[v] - bl * rhs[v];
+        hi[v] = hi[v] - bh * rhs[v];
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      A.out_high[(long long)v * g.n + idx] = hi[v];
+      const double e = fabs(hi[v] - lo[v]) / (A.tol_rel * fabs(hi[v]) + A.tol_abs[v]);
+      errv = dmax(errv, e);
+    }
+  }
 }
 
 template <int ND, bool EU, bool PRIM, int TX, int TY>
@@ -228,6 +558,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
   };
 
   const int ip = i + 2;   // padded i of the own cell
+  // padded cells of one flux field (flux_out)
+  const long long npad = (long long)(g.nx + 4) * (g.ny + 4) * (ND == 3 ? g.nz + 4 : 1);
   double cflv[4] = {0.0, 0.0, 0.0, 0.0};
   double errv = 0.0;
   int flags = 0;
@@ -255,6 +587,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
     }
     kt_flux<ND, EU, PRIM>(2, RL, RR, EU ? 0.0 : M.cs[6 * M.nxp + ip], EU ? 0.0 : M.cs[5 * M.nxp + ip],
                           M.dAzB[ip], P, Fzm);
+    if (A.flux_out && k0 == 0) store_flux<V>(A, 2, padded_index(g, i, j, k0 - 1, ND), npad, Fzm);
   }
 
   for (int k = k0; k < k1; ++k) {
@@ -291,6 +624,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
         }
         kt_flux<ND, EU, PRIM>(2, RL, RR, EU ? 0.0 : M.cs[6 * M.nxp + ip], EU ? 0.0 : M.cs[5 * M.nxp + ip],
                               M.dAzB[ip], P, Fzp);
+        if (A.flux_out) store_flux<V>(A, 2, padded_index(g, i, j, k, ND), npad, Fzp);
         double dV = M.dxdydV[ip];
 #pragma unroll
         for (int v = 0; v < V; ++v) {
@@ -373,7 +707,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
       double* Fout;
       double oL, oR, csL, csR, dA;
       const bool xf = t < NFX;
-      int xr = 0, xfc = 0;
+      int xr = 0, xfc = 0, yc = 0, yf = 0;
       if (xf) {
         const int r = t / (TX + 1), f = t % (TX + 1);
         if (r >= ey || f > ex) continue;
@@ -390,6 +724,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
         const int u = t - NFX;
         const int c = u % TX, f = u / TX;
         if (c >= ex || f > ey) continue;
+        yc = c; yf = f;
         const int gjl = j0 + f - 1 + 2;     // padded j of the lower cell
         const int gi = i0 + c + 2;          // padded i of the column
         oL = M.offyN[gjl]; oR = M.offyS[gjl + 1];
@@ -409,6 +744,9 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
       kt_flux<ND, EU, PRIM>(d, RL, RR, csL, csR, dA, P, F);
 #pragma unroll
       for (int v = 0; v < V; ++v) Fout[v * fstride] = F[v];
+      if (A.flux_out)
+        store_flux<V>(A, d, xf ? padded_index(g, i0 + xfc - 1, j0 + xr, k, ND) : padded_index(g, i0 + yc, j0 + yf - 1, k, ND),
+                      npad, F);
       // boundary row of ComputeRHS (timedisc_base.f90:1224-1231) for the accretion bookkeeping
       if (ND == 2 && xf && A.brow && ((A.brow_face == 0 && i0 + xfc == 0) || (A.brow_face == 1 && i0 + xfc == g.nx)))
         A.brow[j0 + xr] = (A.brow_face == 0 ? A.bdydz : -A.bdydz) * F[0];
@@ -424,299 +762,12 @@ __device__ __forceinline__ void stage_tile(const StageArgs& A, const int bx, con
       double dV = M.dzdxdV[ip];
 #pragma unroll
       for (int v = 0; v < V; ++v) divY[v] = dV * (FY(v, ty + 1, tx) - FY(v, ty, tx));
-      const long long idx = CE::lin(g, i, j, k);
-      // centre primitive / conservative state as ComputeRHS sees it
-      double pc[V], cc[V];
-      double R0[V];
+      double R0[V], rhs[V];
 #pragma unroll
       for (int v = 0; v < V; ++v) R0[v] = RS(v, ty + 2, tx + 2);
-      if (PRIM) {
-#pragma unroll
-        for (int v = 0; v < V; ++v) pc[v] = R0[v];
-        // the sources read cvar itself (the stage state), which Prim2Cons(pvar) only
-        // reproduces to rounding; after the CHECK_PMIN round trip cvar is Prim2Cons(pvar)
-        if (!roundtrip && (M.curv || A.has_accel || A.out_base)) state_at<V>(A.in, g.n, idx, cc);
-        else PH::p2c(pc, cc, P);
-      } else {
-#pragma unroll
-        for (int v = 0; v < V; ++v) cc[v] = R0[v];
-        if (roundtrip) {
-          double u[V];
-          state_at<V>(A.in, g.n, idx, u);
-          PH::c2p(u, pc, P);
-          pc[V - 1] = dmax(pc[V - 1], P.pmin);
-        } else {
-          PH::c2p(cc, pc, P);
-        }
-      }
-      double rhs[V];
 #pragma unroll
       for (int v = 0; v < V; ++v) rhs[v] = (divX[v] + divY[v]) + (ND == 3 ? divZ[v] : 0.0);
-      // with FARGO the sources see the real frame: cvar after AddBackgroundVelocityY and the
-      // primitive state CenterBoundary derives from it
-      const bool fsrc = FG && A.w_sub;
-      if (fsrc) {
-        state_at<V>(A.in, g.n, idx, cc);
-        if (A.in.pre.n) apply_chain<V>(A.in.pre, cc, g, i, j);
-        PH::c2p(cc, pc, P);
-        if (roundtrip) {   // CHECK_PMIN of this ComputeRHS (FirstStep's CHECK_ALL)
-          pc[V - 1] = dmax(pc[V - 1], P.pmin);
-          PH::p2c(pc, cc, P);
-        }
-      }
-      // geometric sources (physics_euler.f90:1706-1847 / physics_eulerisotherm.f90:689-832)
-      double geo2 = 0.0;
-      if (fsrc && g.fdir == 1) {
-        // transport along x: geometric sources of the real frame, AddFargoSourcesX into the x
-        // one (isothermal physics_eulerisotherm.f90:1462-1518; Euler physics_euler.f90:2267-2355
-        // adds the energy term -vx*(tmp + GetGeometricalSourceX(vz = P = mz = 0)))
-        const double vx = pc[1], vy = pc[2];
-        const double cxyx = M.cxyx[ip], cyxy = M.cyxy[ip], czxz = M.czxz[ip], czyz = M.czyz[ip];
-        double geo1 = 0.0;
-        if (M.curv) {
-          const double Pp = EU ? pc[V - 1] : pc[0] * (M.cs[ip] * M.cs[ip]);
-          geo1 = cc[2] * (cyxy * vy - cxyx * vx) + (cyxy + czxz) * Pp;
-          rhs[2] = rhs[2] - (cc[1] * (cxyx * vx - cyxy * vy) + (cxyx + czyz) * Pp);
-        }
-        const int jp = j + 2;
-        const double tmp = cc[2] * 0.5 * (A.w_sub[jp + 1] - A.w_sub[jp - 1]) / M.dly[ip];
-        geo1 = geo1 - tmp;
-        rhs[1] = rhs[1] - geo1;
-        if (EU) {
-          const double cxzx = M.cxzx[ip];
-          const double gx = cc[2] * (cyxy * vy - cxyx * vx) + 0.0 * (czxz * 0.0 - cxzx * vx) + (cyxy + czxz) * 0.0;
-          const double geoE = 0.0 - vx * (tmp + gx);
-          rhs[V - 1] = rhs[V - 1] - geoE;
-        }
-      } else if (M.curv && ND == 2 && fsrc) {
-        double Pp = EU ? pc[V - 1] : pc[0] * (M.cs[ip] * M.cs[ip]);
-        double vx = pc[1], vy = pc[2];
-        double cxyx = M.cxyx[ip], cyxy = M.cyxy[ip], czxz = M.czxz[ip], czyz = M.czyz[ip];
-        rhs[1] = rhs[1] - (cc[2] * (cyxy * vy - cxyx * vx) + (cyxy + czxz) * Pp);
-        geo2 = cc[1] * (cxyx * vx - cyxy * vy) + (cxyx + czyz) * Pp;
-      }
-      if (fsrc && g.fdir != 1) {
-        // AddFargoSourcesY into the geometric source (isothermal
-        // physics_eulerisotherm.f90:1531-1586; Euler physics_euler.f90:2368-2455 adds the
-        // energy term -vy*(tmp + GetGeometricalSourceY(vz = P = mz = 0)))
-        const double tmp = cc[1] * 0.5 * (A.w_sub[ip + 1] - A.w_sub[ip - 1]) / M.dlx[ip];
-        geo2 = geo2 - tmp;
-        rhs[2] = rhs[2] - geo2;
-        if (EU) {
-          const double vx = pc[1], vy = pc[2];
-          const double cxyx = M.cxyx[ip], cyxy = M.cyxy[ip], cyzy = M.cyzy[ip], czyz = M.czyz[ip];
-          const double gy = 0.0 * (czyz * 0.0 - cyzy * vy) + cc[1] * (cxyx * vx - cyxy * vy) + (cxyx + czyz) * 0.0;
-          const double geoE = 0.0 - vy * (tmp + gy);
-          rhs[V - 1] = rhs[V - 1] - geoE;
-        }
-      } else if (!fsrc && M.curv) {
-        double Pp = EU ? pc[V - 1] : pc[0] * (M.cs[ip] * M.cs[ip]);
-        double vx = pc[1], vy = pc[2];
-        double cxyx = M.cxyx[ip], cyxy = M.cyxy[ip], czxz = M.czxz[ip], czyz = M.czyz[ip];
-        if (ND == 2) {
-          double mx = cc[1], my = cc[2];
-          rhs[1] = rhs[1] - (my * (cyxy * vy - cxyx * vx) + (cyxy + czxz) * Pp);
-          rhs[2] = rhs[2] - (mx * (cxyx * vx - cyxy * vy) + (cxyx + czyz) * Pp);
-        } else {
-          double vz = pc[3], mx = cc[1], my = cc[2], mz = cc[3];
-          double cxzx = M.cxzx[ip], cyzy = M.cyzy[ip];
-          rhs[1] = rhs[1] - (my * (cyxy * vy - cxyx * vx) + mz * (czxz * vz - cxzx * vx) + (cyxy + czxz) * Pp);
-          rhs[2] = rhs[2] - (mz * (czyz * vz - cyzy * vy) + mx * (cxyx * vx - cyxy * vy) + (cxyx + czyz) * Pp);
-          rhs[3] = rhs[3] - (mx * (cxzx * vx - czxz * vz) + my * (cyzy * vy - czyz * vz) + (cxzx + cyzy) * Pp);
-        }
-      }
-      // external sources (sources_generic.f90:220-261): point-mass gravity (gravity_pointmass.f90:
-      // 263-282, physics ExternalSources) first in the list, then the viscous source of this
-      // stage state (precomputed by visc_kernel); rhs = ... - (gravity + viscosity)
-      if (A.has_accel || A.visc) {
-        double sm[ND] = {}, se = 0.0;
-        if (A.has_accel) {
-          const double ax = M.accel[ip], ay = M.accel[M.nxp + ip];
-          sm[0] = cc[0] * ax;
-          sm[1] = cc[0] * ay;
-          if (EU) se = cc[1] * ax + cc[2] * ay;
-        }
-        if (A.visc) {
-#pragma unroll
-          for (int m = 0; m < ND; ++m) {
-            const double sv = __ldg(A.visc + (long long)m * g.n + idx);
-            sm[m] = A.has_accel ? sm[m] + sv : sv;
-          }
-          if (EU) {
-            const double sv = __ldg(A.visc + (long long)ND * g.n + idx);
-            se = A.has_accel ? se + sv : sv;
-          }
-        }
-#pragma unroll
-        for (int m = 0; m < ND; ++m) rhs[1 + m] = rhs[1 + m] - sm[m];
-        if (EU) rhs[V - 1] = rhs[V - 1] - se;
-      }
-
-      if (A.out_mode == OUT_RHS) {
-#pragma unroll
-        for (int v = 0; v < V; ++v) A.out[(long long)v * g.n + idx] = rhs[v];
-        if (A.fnext_out) {
-          // the next Butcher stage's state base - sum_q (a dt) k_q in the reference's order
-          // (timedisc_rkfehlberg.f90:277-302), this stage's k from the registers, formed as
-          // form_kernel would form it
-          const StateRef& S = A.fnext;
-          double u[V];
-#pragma unroll
-          for (int v = 0; v < V; ++v) u[v] = __ldg(S.base + (long long)v * g.n + idx);
-          // the earlier stages' k (unrolled to the tableau limit, so all loads issue together)
-#pragma unroll
-          for (int q = 0; q < FGPU_MAXK - 1; ++q) {
-            if (q + 1 < S.nk) {
-              const double a = S.dt_dev ? S.coef[q] * *S.dt_dev : S.coef[q];
-#pragma unroll
-              for (int v = 0; v < V; ++v) u[v] = u[v] - a * __ldg(S.K[q] + (long long)v * g.n + idx);
-            }
-          }
-          {
-            const double a = S.dt_dev ? S.coef[S.nk - 1] * *S.dt_dev : S.coef[S.nk - 1];
-#pragma unroll
-            for (int v = 0; v < V; ++v) u[v] = u[v] - a * rhs[v];
-          }
-          if (PRIM) {
-            double p[V];
-            PH::c2p(u, p, P);
-#pragma unroll
-            for (int v = 0; v < V; ++v) A.fnext_out[(long long)v * g.n + idx] = p[v];
-          } else {
-#pragma unroll
-            for (int v = 0; v < V; ++v) A.fnext_out[(long long)v * g.n + idx] = u[v];
-          }
-        }
-      } else {
-        // Shu-Osher update y = yn - dt*rhs + eta*(y0 - yn + dt*rhs) (timedisc_modeuler.f90:289)
-        double yn[V], y0[V], y[V];
-        if (FG && A.yn_chain.n) {
-          state_at<V>(A.in, g.n, idx, yn);
-          apply_chain<V>(A.yn_chain, yn, g, i, j, rt_cons);
-        } else if (!PRIM) {
-#pragma unroll
-          for (int v = 0; v < V; ++v) yn[v] = cc[v];
-        } else if (roundtrip) {
-#pragma unroll
-          for (int v = 0; v < V; ++v) yn[v] = cc[v];
-        } else {
-          state_at<V>(A.in, g.n, idx, yn);
-        }
-#pragma unroll
-        for (int v = 0; v < V; ++v) y0[v] = __ldg(A.y0 + (long long)v * g.n + idx);
-        if (FG && A.y0_chain.n) apply_chain<V>(A.y0_chain, y0, g, i, j, rt_cons);
-        if (EU && A.y0_roundtrip) {
-          double q[V];
-          PH::c2p(y0, q, P);
-          q[V - 1] = dmax(q[V - 1], P.pmin);
-          PH::p2c(q, y0, P);
-        }
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-          y[v] = yn[v] - dt * rhs[v] + A.eta * (y0[v] - yn[v] + dt * rhs[v]);
-          A.out[(long long)v * g.n + idx] = y[v];
-        }
-        if (A.out2) {
-#pragma unroll
-          for (int v = 0; v < V; ++v)
-            A.out2[(long long)v * g.n + idx] = yn[v] - dt * rhs[v] + A.eta2 * (y0[v] - yn[v] + dt * rhs[v]);
-        }
-        if (A.err_low) {
-          double l[V];
-#pragma unroll
-          for (int v = 0; v < V; ++v) l[v] = __ldg(A.err_low + (long long)v * g.n + idx);
-          // FARGO: the low-order solution as its ComputeRHS framed it in place
-          if (FG && A.err_chain.n) apply_chain<V>(A.err_chain, l, g, i, j);
-#pragma unroll
-          for (int v = 0; v < V; ++v) {
-            const double e = fabs(y[v] - l[v]) / (A.tol_rel * fabs(y[v]) + A.tol_abs[v]);
-            errv = dmax(errv, e);
-          }
-        }
-        if (A.cfl_mode == 1) {
-          double p[V], c[V];
-          PH::c2p(y, p, P);
-          if (EU && A.cfl_roundtrip) p[V - 1] = dmax(p[V - 1], P.pmin);
-          double cs = EU ? PH::cs_of(p, P) : M.cs[ip];
-          double v3[4];
-          CE::cfl_cell(p, cs, M, ip, v3);
-#pragma unroll
-          for (int q = 0; q < 4; ++q) cflv[q] = dmax(cflv[q], v3[q]);
-          if (EU && A.cfl_roundtrip) PH::p2c(p, c, P);
-          else { for (int v = 0; v < V; ++v) c[v] = y[v]; }
-          if ((A.checkdata & 0x01) && !(cs > 0.)) flags |= 0x01;
-          if (EU && (A.checkdata & 0x02) && p[V - 1] < P.pmin) flags |= 0x02;
-          if ((A.checkdata & 0x04) && p[0] < P.rhomin) flags |= 0x04;
-          if (A.checkdata & 0x08)
-            for (int v = 0; v < V; ++v) if (invalid_value(p[v]) || invalid_value(c[v])) flags |= 0x08;
-        }
-      }
-      if (A.out_base) {
-#pragma unroll
-        for (int v = 0; v < V; ++v) A.out_base[(long long)v * g.n + idx] = cc[v];
-        if (fsrc) {
-          // FARGO: cvar after this ComputeRHS is co-moving (its SubtractBackgroundVelocity)
-          double o[V];
-#pragma unroll
-          for (int v = 0; v < V; ++v) o[v] = cc[v];
-          frame_change<V>(o, -1.0, A.w_sub[fargo_ix(g, i, j)], g.fdir);
-#pragma unroll
-          for (int v = 0; v < V; ++v) A.out_base[(long long)v * g.n + idx] = o[v];
-        }
-      }
-      if (A.cfl_mode >= 2) {
-        double cs = EU ? PH::cs_of(pc, P) : M.cs[ip];
-        if (A.cfl_mode == 2) {
-          double v3[4];
-          CE::cfl_cell(pc, cs, M, ip, v3);
-#pragma unroll
-          for (int q = 0; q < 4; ++q) cflv[q] = dmax(cflv[q], v3[q]);
-        }
-        if ((A.checkdata & 0x01) && !(cs > 0.)) flags |= 0x01;
-        if (EU && (A.checkdata & 0x02) && pc[V - 1] < P.pmin) flags |= 0x02;
-        if ((A.checkdata & 0x04) && pc[0] < P.rhomin) flags |= 0x04;
-        if (A.checkdata & 0x08)
-          for (int v = 0; v < V; ++v) if (invalid_value(pc[v]) || invalid_value(cc[v])) flags |= 0x08;
-      }
-      if (A.last_stage) {
-        // high/low order solutions and ComputeError (timedisc_rkfehlberg.f90:198-265,
-        // timedisc_base.f90:1012-1053); base and the earlier k unrolled to the tableau limit
-        // so that their loads issue together, this stage's k from the registers.  On the
-        // device clock (in.dt_dev) bh_dt/bl_dt hold the weights, multiplied by *dt_dev here.
-        const double* dtd = A.in.dt_dev;
-        double hi[V], lo[V];
-#pragma unroll
-        for (int v = 0; v < V; ++v) hi[v] = lo[v] = __ldg(A.in.base + (long long)v * g.n + idx);
-#pragma unroll
-        for (int q = 0; q < FGPU_MAXK - 1; ++q) {
-          if (q + 1 < A.nstage) {
-            const double bh = dtd ? A.bh_dt[q] * *dtd : A.bh_dt[q];
-            const double bl = dtd ? A.bl_dt[q] * *dtd : A.bl_dt[q];
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-              const double kq = __ldg(A.in.K[q] + (long long)v * g.n + idx);
-              lo[v] = lo[v] - bl * kq;
-              hi[v] = hi[v] - bh * kq;
-            }
-          }
-        }
-        {
-          const int q = A.nstage - 1;
-          const double bh = dtd ? A.bh_dt[q] * *dtd : A.bh_dt[q];
-          const double bl = dtd ? A.bl_dt[q] * *dtd : A.bl_dt[q];
-#pragma unroll
-          for (int v = 0; v < V; ++v) {
-            lo[v] = lo[v] - bl * rhs[v];
-            hi[v] = hi[v] - bh * rhs[v];
-          }
-        }
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-          A.out_high[(long long)v * g.n + idx] = hi[v];
-          const double e = fabs(hi[v] - lo[v]) / (A.tol_rel * fabs(hi[v]) + A.tol_abs[v]);
-          errv = dmax(errv, e);
-        }
-      }
+      stage_cell_epilogue<ND, EU, PRIM>(A, i, j, k, R0, rhs, dt, cflv, errv, flags);
     }
     // no barrier between the planes of one tile: a thread writes only its own cell and the
     // halo of the next plane, and every reader of this plane has passed the flux barrier

@@ -1,0 +1,488 @@
+// fgpu_tma.cuh -- stage kernel with TMA-staged halo planes (sm_100a).
+//
+// Same right-hand side and epilogues as stage_tile (fgpu_kernels.cuh: fosite's ComputeRHS,
+// timedisc_base.f90:1073-1271, fused with its consumer), laid out for the Blackwell memory
+// system:
+//   * every x-y plane of a tile, halo included, arrives in shared memory by one bulk tensor
+//     copy (cp.async.bulk.tensor, 4-D map x, y, z, variable) completing on an mbarrier;
+//     a 3D tile marches along z with a ring of three plane slots, the copy of plane k+3
+//     issued while plane k is computed, so the stencil reads each cell from HBM once per
+//     stage and never waits on a load in its inner phases;
+//   * interior tiles need no boundary logic at all; tiles touching an x or y face fill
+//     their ghost cells once per plane in shared memory (CenterBoundary rules,
+//     boundary_generic.f90:287-418), the z ghosts of the own column come from the same
+//     rules;
+//   * the own column's z neighbours come from the ring (planes k, k+1) and a register
+//     lookahead (plane k+2, loaded one plane early);
+//   * the epilogue's streams (base and earlier k of a Butcher stage, the Shu-Osher start
+//     state) are brought into L2 one plane ahead by bulk prefetches issued by one warp.
+// Requirements (checked on the host): even nx (16-byte strides of the tensor map), no
+// FARGO frame changes, no viscous source, no accretion rows, a plain or formed stage
+// input (no k-sums in the stencil).
+#pragma once
+#include <cuda.h>
+#include "fgpu_kernels.cuh"
+
+namespace fgpu {
+
+// ------------------------------------------------------------------ PTX wrappers
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(count) : "memory");
+}
+// orders this thread's generic-proxy shared-memory accesses with later async-proxy ones
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned long long* b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Wait for phase `parity` of an mbarrier, for at most about two seconds of SM clock;
+// false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity) {
+  if (mbar_test(b, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_test(b, parity))
+    if (clock64() - t0 > 4000000000LL) return false;
+  return true;
+}
+// bulk tensor copy of one box (coordinates x, y, z; the variable coordinate 0) into shared
+// memory, completing on the mbarrier; RANK 4 (x, y, z, var) or 3 (x, y, var)
+template <int RANK>
+__device__ __forceinline__ void tma_load_box(void* dst, const CUtensorMap* map, unsigned long long* bar, int x, int y,
+                                             int z) {
+  if (RANK == 4)
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(smem_addr(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(0), "r"(smem_addr(bar))
+        : "memory");
+  else
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_addr(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(0), "r"(smem_addr(bar))
+        : "memory");
+}
+// L2 prefetch of `bytes` contiguous bytes (16-byte aligned address, multiple of 16 bytes)
+__device__ __forceinline__ void bulk_prefetch_l2(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// ------------------------------------------------------------------ layout
+// Shared memory of one TMA tile: NSLOT staged planes [V][TY+4][TX+4] (the box of one tensor
+// copy, 128-byte aligned), the x and y slopes and interface fluxes, NSLOT mbarriers.
+template <int V, int TX, int TY, int NSLOT>
+struct TmaLayout {
+  static constexpr int RW = TX + 4, RH = TY + 4;
+  static constexpr int PLANE = V * RH * RW;
+  static constexpr unsigned PLANE_BYTES = 8u * PLANE;
+  static constexpr int NSX = V * TY * (TX + 2), NSY = V * (TY + 2) * TX;
+  static constexpr int NFX = V * TY * (TX + 1), NFY = V * (TY + 1) * TX;
+  static constexpr size_t SMEM = 128 + 8 * ((size_t)NSLOT * PLANE + NSX + NSY + NFX + NFY + NSLOT);
+  static_assert(PLANE_BYTES % 128 == 0, "plane slots must stay 128-byte aligned");
+};
+template <int ND> struct TmaSlots { static constexpr int N = ND == 3 ? 3 : 1; };
+
+// ------------------------------------------------------------------ the tile
+template <int ND, bool EU, bool PRIM, int TX, int TY>
+__device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtensorMap* tmap, const int bx, const int by,
+                                               const int bz) {
+  using PH = Phys<ND, EU>;
+  using CE = Cells<ND, EU>;
+  constexpr int V = PH::V;
+  constexpr int NT = TX * TY;
+  constexpr int NSLOT = TmaSlots<ND>::N;
+  using L = TmaLayout<V, TX, TY, NSLOT>;
+  constexpr int RW = L::RW, RHW = L::RH * L::RW;
+  extern __shared__ __align__(16) double tma_smem_raw[];
+  double* const ring = reinterpret_cast<double*>((reinterpret_cast<size_t>(tma_smem_raw) + 127) & ~(size_t)127);
+  double* const Sx = ring + NSLOT * L::PLANE;   // [V][TY][TX+2]
+  double* const Sy = Sx + L::NSX;               // [V][TY+2][TX]
+  double* const Fx = Sy + L::NSY;               // [V][TY][TX+1]
+  double* const Fy = Fx + L::NFX;               // [V][TY+1][TX]
+  unsigned long long* const mbar = reinterpret_cast<unsigned long long*>(Fy + L::NFY);
+  __shared__ double sred[RED_STRIDE * ((NT + 31) / 32)];
+  __shared__ int abort_flag;
+
+  if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
+  if (gated_out(A.ctl, A.gate)) return;
+  const Grid& g = A.g;
+  const PhysP& P = A.ph;
+  const MetricP& M = A.mt;
+  const double dt = A.dt_dev ? *A.dt_dev : A.dt;
+  const bool roundtrip = EU && A.in.roundtrip;
+  const StateRef& SR = A.rin.base ? A.rin : A.in;
+  // the staged values are the reconstruction variables as they stand (a formed primitive
+  // stage state, or a conservative state without the CHECK_PMIN round trip), else every
+  // staged point is converted once
+  const bool raw_ok = PRIM ? (SR.ready != 0) : !roundtrip;
+  const int tid = threadIdx.x;
+  const int tx = tid % TX, ty = tid / TX;
+  const int i0 = bx * TX, j0 = by * TY;
+  const int ex = min(TX, g.nx - i0), ey = min(TY, g.ny - j0);
+  const bool own = tx < ex && ty < ey;
+  const int i = i0 + tx, j = j0 + ty;
+  const int ip = i + 2;
+  int k0 = 0, k1 = 1;
+  if (ND == 3) { k0 = bz * A.kchunk; k1 = min(g.nz, k0 + A.kchunk); }
+  // the tile's staged box reaches ghost cells of an x or y face
+  const bool xy_ghosts = i0 == 0 || i0 + ex + 2 > g.nx || j0 == 0 || j0 + ey + 2 > g.ny;
+  const bool prep_sync = !raw_ok || xy_ghosts;
+
+  // reconstruction variables of a raw staged value (in place), and of a face ghost
+  auto conv = [&](double* u) {
+    if (PRIM) {
+      double p[V];
+      PH::c2p(u, p, P);
+      if (roundtrip) p[V - 1] = dmax(p[V - 1], P.pmin);
+#pragma unroll
+      for (int v = 0; v < V; ++v) u[v] = p[v];
+    } else if (roundtrip) {
+      double p[V];
+      PH::c2p(u, p, P);
+      p[V - 1] = dmax(p[V - 1], P.pmin);
+      PH::p2c(p, u, P);
+    }
+  };
+  auto ghost = [&](int d, int gi, int gj, int gk, double* R) {
+    double p[V];
+    CE::face_ghost_p(SR, g, P, M, d, gi, gj, gk, p);
+    if (roundtrip) p[V - 1] = dmax(p[V - 1], P.pmin);
+    if (PRIM) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) R[v] = p[v];
+    } else {
+      PH::p2c(p, R, P);
+    }
+  };
+  // own column at plane gk: raw loads (interior planes), then the reconstruction variables
+  auto col_load = [&](int gk, double* u) {
+    if (gk >= 0 && gk < g.nz) {
+      const double* b = SR.base + CE::lin(g, i, j, gk);
+#pragma unroll
+      for (int v = 0; v < V; ++v) u[v] = __ldg(b + (long long)v * g.n);
+    }
+  };
+  auto col_finish = [&](int gk, double* u) {
+    if (gk < 0 || gk >= g.nz) ghost(2, i, j, gk, u);
+    else if (!raw_ok) conv(u);
+  };
+
+  auto slot = [&](int kp) { return ring + ((kp - k0) % NSLOT) * L::PLANE; };
+  auto issue = [&](int kp) {   // one thread: the tensor copy of plane kp's box into its slot
+    unsigned long long* b = &mbar[(kp - k0) % NSLOT];
+    mbar_expect_tx(b, L::PLANE_BYTES);
+    tma_load_box<ND + 1>(slot(kp), tmap, b, i0 - 2, j0 - 2, kp);
+  };
+  // planes k0 .. k1-1 are staged by tensor copies; the own column of planes k1, k1+1 comes
+  // from the lookahead
+  if (tid == 0) {
+    abort_flag = 0;
+    for (int s = 0; s < NSLOT; ++s) mbar_init(&mbar[s], 1);
+    fence_proxy_async();
+    for (int kp = k0; kp < min(k1, k0 + NSLOT); ++kp) issue(kp);
+  }
+  __syncthreads();
+
+  // wait for plane kp's copy, then fill its ghost cells / convert its raw values in place
+  int waited = 0;   // thread 0: planes k0 .. k0+waited-1 seen complete (or given up on)
+  auto prepare = [&](int kp) {
+    if (kp >= k1) {   // own column only (the next chunk's plane or a z ghost)
+      if (own) {
+        double u[V];
+        col_load(kp, u);
+        col_finish(kp, u);
+        double* S = slot(kp);
+#pragma unroll
+        for (int v = 0; v < V; ++v) S[v * RHW + (ty + 2) * RW + tx + 2] = u[v];
+      }
+      return;
+    }
+    if (!mbar_wait(&mbar[(kp - k0) % NSLOT], (unsigned)(((kp - k0) / NSLOT) & 1))) abort_flag = 1;
+    if (tid == 0) waited = kp + 1 - k0;
+    if (prep_sync) {
+      double* S = slot(kp);
+      constexpr int NXB = (TX + 4) * TY, NYB = TX * 4;
+      for (int t = tid; t < NXB + NYB; t += NT) {
+        int lx, ly;
+        if (t < NXB) {
+          lx = t % (TX + 4);
+          ly = 2 + t / (TX + 4);
+          if (lx >= ex + 4 || ly >= ey + 2) continue;
+        } else {
+          const int u = t - NXB, q = u / TX;
+          lx = 2 + u % TX;
+          ly = q < 2 ? q : ey + q;
+          if (lx >= ex + 2) continue;
+        }
+        const int gi = i0 + lx - 2, gj = j0 + ly - 2;
+        const bool gx = gi < 0 || gi >= g.nx, gy = gj < 0 || gj >= g.ny;
+        if (gx || gy || !raw_ok) {
+          double R[V];
+          if (gx || gy) {
+            ghost(gx ? 0 : 1, gi, gj, kp, R);
+          } else {
+#pragma unroll
+            for (int v = 0; v < V; ++v) R[v] = S[v * RHW + ly * RW + lx];
+            conv(R);
+          }
+#pragma unroll
+          for (int v = 0; v < V; ++v) S[v * RHW + ly * RW + lx] = R[v];
+        }
+      }
+      fence_proxy_async();
+      __syncthreads();
+    }
+  };
+
+  // epilogue streams of plane kp brought into L2 (one warp, one bulk prefetch per tile row):
+  // stream q < nf: the next Butcher stage's base and earlier k; then the stage input's base
+  // and k (the last stage's high/low-order sums, or cvar read by the sources); y0; err_low
+  const int nf = A.fnext_out ? A.fnext.nk : 0;
+  const bool in_needed = A.last_stage || (PRIM && !roundtrip && (M.curv || A.has_accel || A.out_base ||
+                                                                 A.out_mode == OUT_SSPRK)) ||
+                         (!PRIM && roundtrip);
+  const int nin = !in_needed ? 0 : (A.last_stage ? A.nstage : A.in.nk + 1);
+  const int nstreams = nf + nin + (A.out_mode == OUT_SSPRK ? 1 : 0) + (A.err_low ? 1 : 0);
+  auto stream = [&](int q) -> const double* {
+    if (q < nf) return q == 0 ? A.fnext.base : A.fnext.K[q - 1];
+    q -= nf;
+    if (q < nin) return q == 0 ? A.in.base : A.in.K[q - 1];
+    q -= nin;
+    if (A.out_mode == OUT_SSPRK) {
+      if (q == 0) return A.y0;
+      q -= 1;
+    }
+    return A.err_low;
+  };
+  auto prefetch_epilogue = [&](int kp) {
+    if (tid >= 32 || kp >= k1) return;
+    const int rows = ey * V * nstreams;
+    for (int r = tid; r < rows; r += 32) {
+      const int q = r / (ey * V), rem = r % (ey * V), v = rem / ey, jr = rem % ey;
+      bulk_prefetch_l2(stream(q) + (long long)v * g.n + CE::lin(g, i0, j0 + jr, kp), 8u * ex);
+    }
+  };
+
+  double cflv[4] = {0.0, 0.0, 0.0, 0.0};
+  double errv = 0.0;
+  int flags = 0;
+  int issued = min(k1, k0 + NSLOT) - k0;   // thread 0: planes k0 .. k0+issued-1 copied
+
+  // z state of the own column (3D): lookahead raw values of plane k+2, z slope at k, z flux at k-1/2
+  double la[V], sz0[V], Fzm[V];
+  if (ND == 3) {
+    prepare(k0);
+    if (own) {
+      double Ra[V], Rb[V], Rc[V], Rd[V];
+      col_load(k0 - 2, Ra);
+      col_load(k0 - 1, Rb);
+      col_load(k0 + 1, Rd);
+      col_finish(k0 - 2, Ra);
+      col_finish(k0 - 1, Rb);
+      col_finish(k0 + 1, Rd);
+      const double* S0 = slot(k0);
+#pragma unroll
+      for (int v = 0; v < V; ++v) Rc[v] = S0[v * RHW + (ty + 2) * RW + tx + 2];
+      double szm[V];
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        szm[v] = A.constant_recon ? 0.0 : slope(A.limiter, A.theta, A.invd[2], Ra[v], Rb[v], Rc[v]);
+        sz0[v] = A.constant_recon ? 0.0 : slope(A.limiter, A.theta, A.invd[2], Rb[v], Rc[v], Rd[v]);
+      }
+      double RL[V], RR[V];
+      const double oT = M.offzT[k0 - 1 + 2], oB = M.offzB[k0 + 2];
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        RL[v] = A.constant_recon ? Rb[v] : Rb[v] + szm[v] * oT;
+        RR[v] = A.constant_recon ? Rc[v] : Rc[v] + sz0[v] * oB;
+      }
+      kt_flux<ND, EU, PRIM>(2, RL, RR, EU ? 0.0 : M.cs[6 * M.nxp + ip], EU ? 0.0 : M.cs[5 * M.nxp + ip], M.dAzB[ip],
+                            P, Fzm);
+      col_load(k0 + 2, la);
+    }
+  } else {
+    prepare(0);
+  }
+  prefetch_epilogue(k0);
+
+  bool aborted = false;
+  for (int k = k0; k < k1; ++k) {
+    const double* S = slot(k);
+    const int oc = (ty + 2) * RW + tx + 2;   // the own cell in a staged plane
+    if (ND == 3) prepare(k + 1);
+    // ---- x and y slopes of plane k (own cells, then the halo ring of the tile)
+    if (!A.constant_recon) {
+      if (own) {
+        const double* c = S + oc;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          const double* R = c + v * RHW;
+          Sx[(v * TY + ty) * (TX + 2) + tx + 1] = slope(A.limiter, A.theta, A.invd[0], R[-1], R[0], R[1]);
+          Sy[(v * (TY + 2) + ty + 1) * TX + tx] = slope(A.limiter, A.theta, A.invd[1], R[-RW], R[0], R[RW]);
+        }
+      }
+      if (tid < 2 * TY + 2 * TX) {
+        int r, c, dx, stride, sidx;
+        double* Sout;
+        double invd;
+        bool valid;
+        if (tid < 2 * TY) {
+          r = tid >> 1;
+          c = (tid & 1) ? ex : -1;
+          valid = r < ey;
+          dx = 1; stride = TY * (TX + 2); Sout = Sx; sidx = r * (TX + 2) + c + 1; invd = A.invd[0];
+        } else {
+          const int u = tid - 2 * TY;
+          c = u >> 1;
+          r = (u & 1) ? ey : -1;
+          valid = c < ex;
+          dx = RW; stride = (TY + 2) * TX; Sout = Sy; sidx = (r + 1) * TX + c; invd = A.invd[1];
+        }
+        if (valid) {
+          const double* R0p = S + (r + 2) * RW + c + 2;
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            const double* R = R0p + v * RHW;
+            Sout[v * stride + sidx] = slope(A.limiter, A.theta, invd, R[-dx], R[0], R[dx]);
+          }
+        }
+      }
+      __syncthreads();
+    }
+    // ---- x and y interface fluxes of plane k: the own cell's lower faces, then the tile's
+    // upper edge faces
+    auto xy_flux = [&](bool xf, int r, int c) {
+      // xf: x face c (left face of cell c) of row r; else y face r (lower face of row r) of column c
+      double RL[V], RR[V], F[V];
+      int lidx, ridx, sL, sR, sstride, d;
+      const double* Sl;
+      double* Fout;
+      int fstride;
+      double oL, oR, csL, csR, dA;
+      if (xf) {
+        const int gl = i0 + c - 1 + 2;
+        oL = M.offxE[gl]; oR = M.offxW[gl + 1];
+        lidx = (r + 2) * RW + c + 1; ridx = lidx + 1;
+        Sl = Sx; sL = r * (TX + 2) + c; sR = sL + 1; sstride = TY * (TX + 2);
+        csL = EU ? 0.0 : M.cs[2 * M.nxp + gl]; csR = EU ? 0.0 : M.cs[1 * M.nxp + gl + 1];
+        dA = M.dAxW[gl + 1];
+        Fout = Fx + r * (TX + 1) + c; fstride = TY * (TX + 1);
+        d = 0;
+      } else {
+        const int gjl = j0 + r - 1 + 2, gi = i0 + c + 2;
+        oL = M.offyN[gjl]; oR = M.offyS[gjl + 1];
+        lidx = (r + 1) * RW + c + 2; ridx = lidx + RW;
+        Sl = Sy; sL = r * TX + c; sR = sL + TX; sstride = (TY + 2) * TX;
+        csL = EU ? 0.0 : M.cs[4 * M.nxp + gi]; csR = EU ? 0.0 : M.cs[3 * M.nxp + gi];
+        dA = M.dAyS[gi];
+        Fout = Fy + r * TX + c; fstride = (TY + 1) * TX;
+        d = 1;
+      }
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const double rl = S[v * RHW + lidx], rr = S[v * RHW + ridx];
+        RL[v] = A.constant_recon ? rl : rl + Sl[v * sstride + sL] * oL;
+        RR[v] = A.constant_recon ? rr : rr + Sl[v * sstride + sR] * oR;
+      }
+      kt_flux<ND, EU, PRIM>(d, RL, RR, csL, csR, dA, P, F);
+#pragma unroll
+      for (int v = 0; v < V; ++v) Fout[v * fstride] = F[v];
+    };
+    if (own) {
+      xy_flux(true, ty, tx);
+      xy_flux(false, ty, tx);
+    }
+    if (tid < TY + TX) {
+      if (tid < TY) {
+        if (tid < ey) xy_flux(true, tid, ex);
+      } else if (tid - TY < ex) {
+        xy_flux(false, ey, tid - TY);
+      }
+    }
+    __syncthreads();
+    if (abort_flag) { aborted = true; break; }   // block-uniform: read after the barrier
+    // ---- divergence, sources and the stage's consumer
+    if (own) {
+      double divZ[V];
+      if (ND == 3) {
+        // z: slope at k+1 and the flux at k+1/2 of the own column (planes k, k+1 staged, k+2
+        // from the lookahead, whose registers take plane k+3's raw values after the epilogue)
+        const double* S1 = slot(k + 1);
+        col_finish(k + 2, la);
+        double sz1[V], RL[V], RR[V], Fzp[V];
+        const double oT = M.offzT[k + 2], oB = M.offzB[k + 1 + 2];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          const double r0 = S[v * RHW + oc], r1 = S1[v * RHW + oc];
+          sz1[v] = A.constant_recon ? 0.0 : slope(A.limiter, A.theta, A.invd[2], r0, r1, la[v]);
+          RL[v] = A.constant_recon ? r0 : r0 + sz0[v] * oT;
+          RR[v] = A.constant_recon ? r1 : r1 + sz1[v] * oB;
+        }
+        kt_flux<ND, EU, PRIM>(2, RL, RR, EU ? 0.0 : M.cs[6 * M.nxp + ip], EU ? 0.0 : M.cs[5 * M.nxp + ip],
+                              M.dAzB[ip], P, Fzp);
+        const double dVz = M.dxdydV[ip];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          divZ[v] = dVz * (Fzp[v] - Fzm[v]);
+          Fzm[v] = Fzp[v];
+          sz0[v] = sz1[v];
+        }
+      }
+      double rhs[V], R0[V];
+      const double dVx = M.dydzdV[ip], dVy = M.dzdxdV[ip];
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const double divX = dVx * (Fx[(v * TY + ty) * (TX + 1) + tx + 1] - Fx[(v * TY + ty) * (TX + 1) + tx]);
+        const double divY = dVy * (Fy[(v * (TY + 1) + ty + 1) * TX + tx] - Fy[(v * (TY + 1) + ty) * TX + tx]);
+        rhs[v] = (divX + divY) + (ND == 3 ? divZ[v] : 0.0);
+        R0[v] = S[v * RHW + oc];
+      }
+      stage_cell_epilogue<ND, EU, PRIM>(A, i, j, k, R0, rhs, dt, cflv, errv, flags);
+      if (ND == 3) col_load(k + 3, la);
+    }
+    // ---- plane k's slot is free once every thread has read its centre: copy plane k+3 into
+    // it; the epilogue streams of plane k+1 to L2
+    if (ND == 3 && k + 1 < k1) {
+      __syncthreads();
+      if (tid == 0 && k + NSLOT < k1) { issue(k + NSLOT); ++issued; }
+      prefetch_epilogue(k + 1);
+    }
+  }
+
+  if (aborted) {
+    // a copy did not complete in time: report it, give the copies still in flight their
+    // (bounded) time to land in this block's shared memory, leave
+    if (tid == 0) {
+      if (A.ctl) atomicOr(&A.ctl->dev_err, 1);
+      for (int kp = k0 + waited; kp < k0 + issued; ++kp)
+        mbar_wait(&mbar[(kp - k0) % NSLOT], (unsigned)(((kp - k0) / NSLOT) & 1));
+    }
+    __syncthreads();
+    return;
+  }
+  const bool err_out = A.last_stage || A.err_low;
+  if (A.ctl && (A.cfl_mode || err_out)) {
+    int nv = A.cfl_mode ? (M.vis ? 4 : (ND == 3 ? 3 : 1)) : 0;
+    double vals[4] = {cflv[0], cflv[1], cflv[2], cflv[3]};
+    if (err_out && !A.cfl_mode) { vals[0] = errv; nv = 1; }
+    if (nv) block_reduce_emit<NT>(vals, nv, flags, err_out && !A.cfl_mode ? &A.ctl->err : A.ctl->invdt,
+                                  &A.ctl->flags, sred);
+  }
+}
+
+template <int ND, bool EU, bool PRIM, int TX, int TY, int MINB>
+__global__ void __launch_bounds__(TX* TY, MINB)
+    tma_stage_kernel(const __grid_constant__ StageArgs A, const __grid_constant__ CUtensorMap tmap) {
+  tma_stage_tile<ND, EU, PRIM, TX, TY>(A, &tmap, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+}  // namespace fgpu

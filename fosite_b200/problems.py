@@ -196,3 +196,42 @@ def disk2d(nr=512, nphi=1024, seed=3000, hratio=0.05, sigma_index=-1.0, geometry
     # Keplerian rotation, pressure corrected for sigma ~ r^s, cs^2 ~ 1/r: v^2 = GM/r (1 - (1 - s) h^2)
     p[2] = np.sqrt(1.0 / r) * np.sqrt(1.0 - (1.0 - sigma_index) * hratio * hratio)
     return c, p, {"bccsound": cs_c, "fcsound": fcs}
+
+
+def sedov(nd=2, n=64, half=0.3, r0=3.0e-2, e1=1.0, p0=1.0e-5, rho0=1.0, gamma=1.4, method=abi.MODIFIED_EULER,
+          tdorder=2, stoptime=0.05, variables=abi.CONSERVATIVE, limiter=abi.MONOCENT, theta=1.2, cfl=0.3,
+          tol_rel=0.01, tol_abs=(0.0, 1e-3, 1e-3, 0.0), dtlimit=1.0e-15):
+    """Sedov point explosion on a Cartesian box [-half, half]^nd with no-gradient boundaries:
+    gas at rest, density rho0, pressure p0 outside r0 and p1 = 3 (gamma-1) e1 / ((nd+1) pi r0^nd)
+    inside (tests/ode.f90:159-190 in 2D, tests/sedov3d.f90:270-300 with nd = 3).  The defaults
+    are the ode test's (64^2, KT + MC(1.2) on conservative variables, CFL 0.3, tol_rel 0.01,
+    tol_abs (0, 1e-3, 1e-3, 0), stoptime 0.05)."""
+    c = _base((n, n, n), nd)
+    c.xmin, c.xmax, c.ymin, c.ymax = -half, half, -half, half
+    if nd == 3:
+        c.zmin, c.zmax = -half, half
+    for f in range(6):
+        c.bc[f] = abi.NO_GRADIENTS
+    c.physics = abi.EULER
+    c.gamma = gamma
+    c.variables = variables
+    c.limiter = limiter
+    c.theta = theta
+    c.method = method
+    c.tdorder = tdorder
+    c.cfl = cfl
+    c.stoptime = stoptime
+    c.dtlimit = dtlimit
+    c.tol_rel = tol_rel
+    V = nd + 2
+    for v in range(abi.MAXVAR):
+        c.tol_abs[v] = tol_abs[min(v, len(tol_abs) - 1)] if v < V - 1 else tol_abs[-1]
+    c.maxiter = 1000000
+    abi.finalize_config(c)
+    X, Y, Z, _ = centers(c)
+    r = np.sqrt(X * X + Y * Y + Z * Z)
+    p1 = 3.0 * (gamma - 1.0) * e1 / ((nd + 1) * np.pi * r0 ** nd)
+    p = np.zeros((V,) + X.shape)
+    p[0] = rho0
+    p[V - 1] = np.where(r <= r0, p1, p0)
+    return c, p, {}

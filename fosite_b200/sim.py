@@ -49,6 +49,7 @@ def lib(exact=False):
     L.fgpu_run.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]
     L.fgpu_compute_rhs.argtypes = [C.c_void_p]
     L.fgpu_calc_timestep.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    L.fgpu_set_output_time.argtypes = [C.c_void_p, C.c_double]
     L.fgpu_get_status.argtypes = [C.c_void_p, C.POINTER(abi.Status)]
     L.fgpu_synchronize.argtypes = [C.c_void_p]
     L.fgpu_set_stream.argtypes = [C.c_void_p, C.c_void_p]
@@ -163,6 +164,15 @@ class Simulation:
         d = C.c_double()
         self._check(self.L.fgpu_calc_timestep(self.h, C.byref(d)))
         return d.value
+
+    def fluxes(self, which):
+        """Interface fluxes of the last compute_rhs (abi.XFLUX, YFLUX or ZFLUX), ghost-padded like
+        fosite's Fluxes%xfluxdydz: index i holds the flux through the face between cells i and i+1."""
+        return self.get(which)
+
+    def set_output_time(self, tout):
+        """The next output time; step() clips dt so that a step ends there."""
+        self._check(self.L.fgpu_set_output_time(self.h, float(tout)))
 
     def status(self):
         st = abi.Status()

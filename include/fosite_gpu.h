@@ -3,7 +3,7 @@
  * finite-volume time step.
  *
  * The entry points below are what a Fortran 2008 caller binds with
- * ISO_C_BINDING (see INTEGRATION.md for the BIND(C) interface block).  Every
+ * ISO_C_BINDING (fortran/fosite_gpu_bind.f90 holds the BIND(C) interface block).  Every
  * call takes plain pointers and sizes; no C++ or torch type crosses the
  * boundary.  All state arrays exchanged with the caller use fosite's own
  * layout: Fortran order, i fastest, ghost-padded by two cells in every active
@@ -202,6 +202,13 @@ typedef struct fgpu_handle fgpu_handle;
 #define FGPU_PVAR        2   /* primitive state, ghost-padded */
 #define FGPU_RHS         3   /* right-hand side of the last fgpu_compute_rhs (interior cells valid) */
 #define FGPU_BCCSOUND    4   /* cell-centre sound speed (ghost-padded) */
+/* Fluxes%xfluxdydz / yfluxdzdx / zfluxdxdy of the last fgpu_compute_rhs (fluxes_base.f90:87-97,
+ * fluxes_kt.f90:109-208): ghost-padded, VNUM variables; index i holds the flux through the
+ * face between cells i and i+1 (x), likewise j (y) and k (z).  Valid on the faces the
+ * right-hand side reads: i from IMIN-1 to IMAX with interior j and k (x), and so on. */
+#define FGPU_XFLUX       5
+#define FGPU_YFLUX       6
+#define FGPU_ZFLUX       7
 #define FGPU_MESH_X      10  /* curvilinear cell-centre coordinates, ghost-padded scalar arrays */
 #define FGPU_MESH_Y      11
 #define FGPU_MESH_Z      12
@@ -243,7 +250,8 @@ int fgpu_set_sound_speeds(fgpu_handle* h, const double* bccsound, int64_t nb,
  * FARGO transport, a state uploaded after fgpu_first_step is taken to be in
  * the co-moving frame, the frame fgpu_download returns. */
 int fgpu_upload_state(fgpu_handle* h, int which, const double* data, int64_t n);
-/* Download a ghost-padded array (FGPU_CVAR, FGPU_PVAR, FGPU_RHS, FGPU_BCCSOUND). */
+/* Download a ghost-padded array (FGPU_CVAR, FGPU_PVAR, FGPU_RHS, FGPU_BCCSOUND,
+ * FGPU_XFLUX/YFLUX/ZFLUX). */
 int fgpu_download(fgpu_handle* h, int which, double* out, int64_t n);
 
 /* fosite%FirstStep (fosite.f90:258-348): full ComputeRHS with CHECK_ALL and
@@ -261,6 +269,10 @@ int fgpu_run(fgpu_handle* h, int64_t n, int64_t* done);
 int fgpu_compute_rhs(fgpu_handle* h);
 /* Timedisc%CalcTimestep of the current state (does not change the status). */
 int fgpu_calc_timestep(fgpu_handle* h, double* dt);
+/* Datafile%time, the next output time (io/fileio_base.f90:604-621): fgpu_step clips dt so
+ * that a step ends there, as fosite%Step does through Datafile%AdjustTimestep; replaces
+ * fgpu_config.tout after each output. */
+int fgpu_set_output_time(fgpu_handle* h, double tout);
 /* Measure every stage-kernel layout on this grid (reps RHS evaluations each into
  * a scratch array; the state is untouched) and keep the fastest for later
  * steps.  *variant receives the choice.  Decisions are cached per process by
@@ -320,9 +332,10 @@ int  fgpu_batch_autotune(fgpu_batch* b, int reps, int* variant);
  * 1 MiB file-scope __device__ array that every GPU loading the library holds
  * until exit.  Cartesian meshes, ideal-gas or constant-cs isothermal physics,
  * no point mass or fargo; meshes whose metric does not fit (inum above about
- * 5000) return FGPU_EARG.  The first call on a device looks up the array's
- * device address, so make it before any stream capture.  All calls share the
- * array: calls that overlap on the GPU race. */
+ * 5000) return FGPU_EARG.  Each call only enqueues work on the caller's stream
+ * (a memset and four kernels; the host does not wait).  The first call on a
+ * device looks up the array's device address, so make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race. */
 int fgpu_calc_timestep_noalloc(const fgpu_config* cfg, const double* d_cvar, double* d_dt, void* stream);
 int fgpu_get_status(fgpu_handle* h, fgpu_status* st);
 /* Timedisc%w for FARGO type 2 (a background velocity the user supplies, e.g. in

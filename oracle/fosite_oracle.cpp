@@ -1666,6 +1666,9 @@ int orc_get(orc_handle* h, int which, double* out) {
     case FGPU_PVAR: std::memcpy(out, o.pvar.data(), sizeof(double) * n); break;
     case FGPU_RHS: std::memcpy(out, o.rhs.data(), sizeof(double) * n); break;
     case FGPU_BCCSOUND: std::memcpy(out, o.bccsound.data(), sizeof(double) * o.NC); break;
+    case FGPU_XFLUX: std::memcpy(out, o.xflux.data(), sizeof(double) * n); break;
+    case FGPU_YFLUX: std::memcpy(out, o.yflux.data(), sizeof(double) * n); break;
+    case FGPU_ZFLUX: std::memcpy(out, o.zflux.data(), sizeof(double) * n); break;
     default: return FGPU_EARG;
   }
   return 0;

@@ -274,3 +274,38 @@ def test_khi3d_orientation_symmetry_gpu():
     while o.step() == 0:
         pass
     assert np.array_equal(o.get(abi.PVAR), base)
+
+
+def _face_region(cfg, d):
+    """Slices of the faces a right-hand side reads in direction d (padded indexing: the face
+    between cells i and i+1 sits at i, from IMIN-1 to IMAX; the other directions interior)."""
+    sl = [slice(None)]
+    for ax, n in zip((2, 1, 0), (cfg.knum, cfg.jnum, cfg.inum)):
+        if n == 1:
+            sl.append(slice(None))
+        elif ax == d:
+            sl.append(slice(1, n + 2))
+        else:
+            sl.append(slice(2, n + 2))
+    return tuple(sl)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_interface_fluxes_match_oracle(name):
+    """CalculateFluxes (fluxes_base.f90:87-97): the x/y/z interface fluxes of ComputeRHS, exact build."""
+    cfg, o, g = _pair(name, exact=True)
+    tol = 1e-13 if _inexact(cfg) else 0.0
+    o.compute_rhs()
+    g.compute_rhs()
+    dirs = [abi.XFLUX, abi.YFLUX] + ([abi.ZFLUX] if cfg.knum > 1 else [])
+    for d, which in enumerate(dirs):
+        sl = _face_region(cfg, d)
+        a, b = g.fluxes(which)[sl], o.get(which)[sl]
+        if tol == 0.0:
+            bad = np.argwhere(a != b)
+            assert bad.size == 0, "dir %d: %d faces differ, first %s gpu=%r oracle=%r" % (
+                d, len(bad), bad[0], a[tuple(bad[0])], b[tuple(bad[0])])
+        else:
+            assert rel_l1(a, b) <= tol, d
+    g.close()
