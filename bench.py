@@ -335,6 +335,9 @@ def run_own(args, world, rank, local):
     e2e_value = allsum(float(st2.cell_updates), world) / (ems_max * 1e-3)
 
     if rank != 0:
+        sim.close()
+        if not args.no_extras:
+            run_ensemble(args, world, rank, local, emit=False)   # same collective steps as rank 0
         return
     peak, peak_kind = peak_hbm()
     achieved = stp.stage_bytes / (stp.stage_ms * 1e-3) / 1e9 if stp.stage_ms > 0 else None
@@ -372,8 +375,14 @@ def run_own(args, world, rank, local):
         "gpu_launches": int(st.launches),
         "clocks": clocks,
     }
-    print(json.dumps(line), flush=True)
     sim.close()
+    if not args.no_extras:
+        # the batched ensemble against the loop of plain per-grid runs (96 disks), same steps
+        ens = run_ensemble(args, world, rank, local, emit=False)
+        line["ensemble"] = {k: ens[k] for k in ("value", "unit", "ms_per_step", "speedup_vs_plain",
+                                                  "identical_to_plain", "plain_loop", "member_steps_per_s")}
+        line["ensemble"]["config"] = {k: ens["config"][k] for k in ("description", "members", "cells")}
+    print(json.dumps(line), flush=True)
 
 
 ENSEMBLE_DESC = ("96 independent 2D isothermal disks, Nr in [64,384], Nphi in [128,768] (multiples of 32), "
@@ -394,11 +403,12 @@ def ensemble_members(n=96, seed=4000):
     return out
 
 
-def run_ensemble(args, world=1, rank=0, local=0):
+def run_ensemble(args, world=1, rank=0, local=0, emit=True):
     """Batched ensemble against a loop of plain per-grid runs of the same members.
 
     With N ranks the members are dealt round-robin to the GPUs (no collective in the
-    step); the job time is the slowest rank's."""
+    step); the job time is the slowest rank's.  emit=False returns rank 0's line instead
+    of printing it (None on the other ranks)."""
     import torch
     from fosite_b200 import abi, replicas
     from fosite_b200.sim import Batch, Simulation
@@ -444,7 +454,7 @@ def run_ensemble(args, world=1, rank=0, local=0):
     cells = int(allsum(cells, world))
     if rank != 0:
         b.close()
-        return
+        return None
     line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_batch / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -455,8 +465,10 @@ def run_ensemble(args, world=1, rank=0, local=0):
             "member_steps_per_s": members_all * args.steps / t_batch,
             "plain_loop": {"value": cells * args.steps / t_plain, "ms_per_step": 1e3 * t_plain / args.steps},
             "speedup_vs_plain": t_plain / t_batch, "identical_to_plain": bool(same), "clocks": clocks}
-    print(json.dumps(line), flush=True)
     b.close()
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 def run_serve(args, world=1, rank=0, local=0):
@@ -519,6 +531,7 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=120.0)
     ap.add_argument("--cpu-budget", type=float, default=25.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the ensemble comparison of the default line")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:

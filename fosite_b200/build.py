@@ -5,6 +5,9 @@ Two variants are built from the same sources:
   lib/libfosite_gpu_exact.so  --fmad=false: every operation rounded as in the
                               reference's CPU build; used to prove bit-level
                               agreement with the CPU oracle
+Each variant links three translation units compiled in parallel: fgpu_host.cu (the C ABI,
+host drivers and the shared-memory stage kernels) and the TMA-staged stage kernels of 2D and
+3D meshes (fgpu_tma_2d.cu, fgpu_tma_3d.cu).
 """
 import os
 import subprocess
@@ -13,7 +16,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
+BUILDDIR = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+UNITS = ["fgpu_host.cu", "fgpu_tma_2d.cu", "fgpu_tma_3d.cu"]
 
 
 def nvcc():
@@ -23,38 +28,51 @@ def nvcc():
     return "nvcc"
 
 
+def _flags(var, verbose):
+    f = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-lineinfo", "--expt-relaxed-constexpr", *ARCH]
+    if var == "exact":
+        f = ["--fmad=false", "-DFGPU_EXACT"] + f
+    if verbose:
+        f = ["-Xptxas=-v"] + f
+    return f
+
+
+def _obj(unit, var):
+    return os.path.join(BUILDDIR, "%s_%s.o" % (os.path.splitext(unit)[0], var))
+
+
 def build(verbose=False, variants=("fast", "exact")):
     os.makedirs(LIBDIR, exist_ok=True)
-    src = os.path.join(CSRC, "fgpu_host.cu")
+    os.makedirs(BUILDDIR, exist_ok=True)
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(HERE, "..", "include", "fosite_gpu.h")]
     newest = max(os.path.getmtime(d) for d in deps)
-    outs, procs = [], []
+    todo = []
     for var in variants:
         name = "libfosite_gpu.so" if var == "fast" else "libfosite_gpu_exact.so"
         out = os.path.join(LIBDIR, name)
-        outs.append(out)
         if os.path.exists(out) and os.path.getmtime(out) >= newest:
             continue
-        cmd = [nvcc(), "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC", "-lineinfo",
-               "--expt-relaxed-constexpr", *ARCH, "-o", out + ".tmp", src]
-        if var == "exact":
-            cmd[1:1] = ["--fmad=false", "-DFGPU_EXACT"]
-        if verbose:
-            cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd), file=sys.stderr)
-        procs.append((subprocess.Popen(cmd), out))   # the two variants compile concurrently
-    failed = []
-    for p, out in procs:
-        if p.wait() != 0:
-            failed.append(out)
-        else:
-            os.replace(out + ".tmp", out)
-            # stamp the library with the sources' time, so that a source edited while
-            # nvcc ran still counts as newer than the library
-            os.utime(out, (newest, newest))
+        todo.append((var, out))
+    # every translation unit of every variant compiles concurrently
+    procs = []
+    for var, out in todo:
+        for u in UNITS:
+            cmd = [nvcc(), *_flags(var, verbose), "-c", "-o", _obj(u, var), os.path.join(CSRC, u)]
+            print(" ".join(cmd), file=sys.stderr)
+            procs.append((subprocess.Popen(cmd), _obj(u, var)))
+    failed = [obj for p, obj in procs if p.wait() != 0]
     if failed:
         raise RuntimeError("nvcc failed for " + ", ".join(failed))
-    return outs
+    for var, out in todo:
+        cmd = [nvcc(), "-shared", *ARCH, "-o", out + ".tmp", *[_obj(u, var) for u in UNITS]]
+        print(" ".join(cmd), file=sys.stderr)
+        if subprocess.call(cmd) != 0:
+            raise RuntimeError("link failed for " + out)
+        os.replace(out + ".tmp", out)
+        # stamp the library with the sources' time, so that a source edited while nvcc ran
+        # still counts as newer than the library
+        os.utime(out, (newest, newest))
+    return [os.path.join(LIBDIR, n) for n in ("libfosite_gpu.so", "libfosite_gpu_exact.so")]
 
 
 if __name__ == "__main__":

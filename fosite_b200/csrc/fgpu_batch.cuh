@@ -815,7 +815,30 @@ int fgpu_autotune(fgpu_handle* h, int reps, int* variant) {
   A.out = scratch;
   A.ctl = nullptr;
   A.visc = h->vis ? h->d_visc : nullptr;   // the stencil's read of the viscous source
-  const int cand[7] = {0, 2, 3, 4, 5, 1, 6};
+  if (!h->fargo && !h->vis && !h->accrete) {
+    if (h->butcher && !h->adaptive_me && h->materialize && h->fuse_form && h->T.m >= 3) {
+      // a late Butcher stage as the steps launch it: the formed input state, this stage's k and
+      // the next stage's state formed from base and the earlier k (the heaviest epilogue
+      // stream); only scratch buffers are written (k_{M-1}, a formed-state buffer)
+      const int m = h->T.m - 1;
+      A.rin = plain_state(stage_rbuf(h, m), false);
+      A.rin.ready = h->prim ? 1 : 0;
+      A.in.base = h->buf[1];
+      A.in.nk = m - 1;
+      for (int q = 0; q < m - 1; ++q) {
+        A.in.K[q] = h->buf[2 + q];
+        A.in.coef[q] = h->T.A[(m - 1) * h->T.m + q] * h->dt;
+      }
+      A.out = h->buf[2 + m - 1];
+      set_fnext(h, A, m, h->dt, nullptr);
+    } else if (!h->butcher && !h->adaptive_me && h->order >= 3) {
+      // a middle Shu-Osher stage: scratch state in, scratch state out, the stored state as y0
+      A = shu_osher_stage(h, 2);
+      A.ctl = nullptr;
+      A.cfl_mode = 0;
+    }
+  }
+  const int cand[8] = {0, 2, 3, 4, 5, 1, 6, 7};
   // 3D: the z extent a block marches through (smaller chunks give small grids more blocks);
   // FGPU_KCHUNK fixes it
   std::vector<int> chunks;
@@ -831,8 +854,9 @@ int fgpu_autotune(fgpu_handle* h, int reps, int* variant) {
   for (int v : cand) {
     // layout 1 lacks these features (Butcher steps gate their stages or form the next stage's state)
     if (v == 1 && (h->fargo || h->accrete || h->vis || h->butcher)) continue;
-    // layout 6 (TMA-staged planes) serves grids without FARGO, viscosity or accretion, even nx
-    if (v == 6 && (h->fargo || h->accrete || h->vis || h->g.nx % 2 != 0)) continue;
+    // layouts 6, 7 (TMA-staged planes) serve grids without FARGO, viscosity or accretion, even nx
+    if (v >= 6 && (h->fargo || h->accrete || h->vis || h->g.nx % 2 != 0)) continue;
+    if (v == 7 && h->nd == 3) continue;   // the 32 x 4 TMA tile is built for 2D meshes
     // the taller tiles (4, 5) differ from the oracle in the last bit on FARGO transport along x
     // with a user-supplied background velocity; such grids keep the 32 x 8 tiles
     if ((v == 4 || v == 5) && h->fargo && h->fdir == 1) continue;

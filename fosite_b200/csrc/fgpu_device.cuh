@@ -166,6 +166,8 @@ __device__ __forceinline__ bool gated_out(const Ctl* c, int gate) {
 
 enum { BC_NOGRAD = 0x01, BC_PERIODIC = 0x02, BC_REFLECTING = 0x03, BC_AXIS = 0x04, BC_ABSORBING = 0x0D };
 enum { LIM_MINMOD = 1, LIM_MC = 2, LIM_SWEBY = 3, LIM_SUPERBEE = 4, LIM_OSPRE = 5, LIM_VANLEER = 7, LIM_NOLIMIT = 8 };
+// kernel-internal code: MC with theta = 1 (the products theta*difference are exact and skipped)
+enum { LIM_MC1 = 102 };
 
 __device__ __forceinline__ double fsign1(double b) { return signbit(b) ? -1.0 : 1.0; }
 __device__ __forceinline__ double fsign(double a, double b) { return signbit(b) ? -fabs(a) : fabs(a); }
@@ -263,8 +265,9 @@ __device__ __forceinline__ double limit2(int lim, double theta, double a1, doubl
 }
 // slope of q0 with neighbours qm, qp (MONOCENT uses minmod3 of three differences)
 __device__ __forceinline__ double slope(int lim, double theta, double invd, double qm, double q0, double qp) {
-  if (lim == LIM_MC) {
-    double a1 = theta * (q0 - qm), a2 = theta * (qp - q0), a3 = 0.5 * (qp - qm);
+  if (lim == LIM_MC || lim == LIM_MC1) {
+    double a1 = lim == LIM_MC1 ? q0 - qm : theta * (q0 - qm), a2 = lim == LIM_MC1 ? qp - q0 : theta * (qp - q0);
+    double a3 = 0.5 * (qp - qm);
 #ifdef FGPU_EXACT
     double r = 0.;
     if (((fsign1(a1) * fsign1(a2)) > 0) && ((fsign1(a2) * fsign1(a3)) > 0))
@@ -528,11 +531,13 @@ struct Cells {
 // 555-686) and CalcFluxes{X,Y,Z}/SetFlux (physics_euler.f90:492-742,
 // physics_eulerisotherm.f90:835-979).  RL: reconstructed variables on the
 // plus face of the left cell, RR: on the minus face of the right cell.
-template <int ND, bool EU, bool PRIM>
-__device__ __forceinline__ void kt_flux(int d, const double* RL, const double* RR, double csL_iso, double csR_iso,
+// DC >= 0: the direction is DC, known at compile time (d_rt is ignored).
+template <int ND, bool EU, bool PRIM, int DC = -1>
+__device__ __forceinline__ void kt_flux(int d_rt, const double* RL, const double* RR, double csL_iso, double csR_iso,
                                         double dA, const PhysP& P, double* F) {
   using PH = Phys<ND, EU>;
   constexpr int V = PH::V;
+  const int d = DC >= 0 ? DC : d_rt;
   double pL[V], cL[V], pR[V], cR[V];
   if (PRIM) {
 #pragma unroll

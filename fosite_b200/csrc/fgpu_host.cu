@@ -29,7 +29,7 @@
 #include "fgpu_visc.cuh"
 #include "fgpu_ddmath.h"
 #include "fgpu_bt.cuh"
-#include "fgpu_tma.cuh"
+#include "fgpu_tma_launch.h"
 
 using namespace fgpu;
 
@@ -166,7 +166,7 @@ struct fgpu_handle {
   double* d_ready = nullptr;    // ... into this array (one state)
   int variant = 0;              // stage kernel layout: 0 shared-memory tile, 1 warp-shuffle window,
                                 // 2/3 tile with a register cap for more resident blocks, 4 taller tile,
-                                // 6 tile with TMA-staged planes (fgpu_tma.cuh)
+                                // 6 tile with TMA-staged planes (fgpu_tma.cuh), 7 its 32 x 4 form (2D)
   // tensor maps of the stage inputs the TMA layout has read (by base pointer and tile shape)
   struct TmapEntry { const double* base; int tx, ty; CUtensorMap map; };
   std::vector<TmapEntry> tmaps;
@@ -453,24 +453,6 @@ template <int ND> struct TileShapes;
 template <> struct TileShapes<2> { static constexpr int TY = 8, M2 = 2, M3 = 3, TY4 = 16, M4 = 1, M5 = 1; };
 template <> struct TileShapes<3> { static constexpr int TY = 4, M2 = 4, M3 = 6, TY4 = 8, M4 = 2, M5 = 3; };
 
-// ---- the TMA-staged layout (variant 6): 32 x 8 tiles, 3D with a three-plane ring (two
-// blocks per SM), 2D one plane (three blocks per SM)
-template <int ND> struct TmaShape { static constexpr int TX = 32, TY = 8, MINB = ND == 3 ? 2 : 3; };
-template <int ND, bool EU, bool PRIM>
-struct TmaLaunch {
-  using T = TmaShape<ND>;
-  static constexpr size_t SMEM = TmaLayout<Phys<ND, EU>::V, T::TX, T::TY, TmaSlots<ND>::N>::SMEM;
-  static void configure() {
-    cudaFuncSetAttribute(tma_stage_kernel<ND, EU, PRIM, T::TX, T::TY, T::MINB>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
-  }
-  static void launch(const Grid& g, int kchunk, cudaStream_t s, const StageArgs& A, const CUtensorMap& map) {
-    const int kz = ND == 3 ? (g.nz + kchunk - 1) / kchunk : 1;
-    dim3 grid((g.nx + T::TX - 1) / T::TX, (g.ny + T::TY - 1) / T::TY, kz);
-    tma_stage_kernel<ND, EU, PRIM, T::TX, T::TY, T::MINB><<<grid, T::TX * T::TY, SMEM, s>>>(A, map);
-  }
-};
-
 template <int ND, bool EU, bool PRIM>
 void configure_stage_kernels_t() {
   using S = TileShapes<ND>;
@@ -479,7 +461,8 @@ void configure_stage_kernels_t() {
   TileLayout<ND, EU, PRIM, 32, S::TY, S::M3>::configure(true);
   TileLayout<ND, EU, PRIM, 32, S::TY4, S::M4>::configure(false);
   TileLayout<ND, EU, PRIM, 32, S::TY4, S::M5>::configure(false);
-  TmaLaunch<ND, EU, PRIM>::configure();
+  if (ND == 3) tma_stage_configure_3d(EU, PRIM);
+  else tma_stage_configure_2d(EU, PRIM);
 }
 void configure_stage_kernels(int nd, bool e, bool p) {
   if (nd == 2) {
@@ -553,13 +536,14 @@ int launch_stage_t(fgpu_handle* h, StageArgs& A) {
   A.kchunk = h->kchunk;
   const Grid& g = h->g;
   const int kz = ND == 3 ? (g.nz + h->kchunk - 1) / h->kchunk : 1;
-  if (h->variant == 6 && tma_eligible(h, A)) {
-    using T = TmaShape<ND>;
+  if ((h->variant == 6 || (h->variant == 7 && ND == 2)) && tma_eligible(h, A)) {
     const StateRef& SR = A.rin.base ? A.rin : A.in;
-    const CUtensorMap* map = stage_tmap(h, SR.base, T::TX, T::TY);
+    const int ty = h->variant == 7 ? 4 : kTmaTY;
+    const CUtensorMap* map = stage_tmap(h, SR.base, kTmaTX, ty);
     if (!map) return set_err(h, FGPU_ECUDA, "cuTensorMapEncodeTiled failed for a stage input");
-    TmaLaunch<ND, EU, PRIM>::launch(g, h->kchunk, h->stream, A, *map);
-    CUDA_TRY(h, cudaGetLastError());
+    const bool crec = A.constant_recon != 0;
+    if (ND == 3) CUDA_TRY(h, tma_stage_launch_3d(EU, PRIM, A.limiter, crec, g, h->kchunk, h->stream, A, *map));
+    else CUDA_TRY(h, tma_stage_launch_2d(EU, PRIM, A.limiter, crec, ty, g, h->stream, A, *map));
     return FGPU_OK;
   }
   // the warp-shuffle layout implements neither FARGO frame changes, the accretion rows, the
@@ -569,7 +553,7 @@ int launch_stage_t(fgpu_handle* h, StageArgs& A) {
   const int variant =
       (h->variant == 1 && (h->fargo || h->accrete || h->vis || A.gate || A.fnext_out || A.cfl_mode == 3 ||
                            A.flux_out))
-          ? 0 : (h->variant == 6 ? 0 : h->variant);
+          ? 0 : (h->variant >= 6 ? 0 : h->variant);
   switch (variant) {
     case 1: {
       // warp-shuffle layout: 32 x 8 points per block, 30 x 6 output cells
@@ -1720,7 +1704,7 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
   }
   if (!rc) {
     // FGPU_STAGE_VARIANT / FGPU_KCHUNK force a stage-kernel layout and z chunk (the tuner's choice otherwise)
-    if (const char* e = std::getenv("FGPU_STAGE_VARIANT")) h->variant = std::max(0, std::min(6, std::atoi(e)));
+    if (const char* e = std::getenv("FGPU_STAGE_VARIANT")) h->variant = std::max(0, std::min(7, std::atoi(e)));
     if (const char* e = std::getenv("FGPU_KCHUNK")) { int v = std::atoi(e); if (v > 0) h->kchunk = v; }
     if (const char* e = std::getenv("FGPU_MATERIALIZE")) h->materialize = std::atoi(e) != 0;
     if (const char* e = std::getenv("FGPU_FUSE_FORM")) h->fuse_form = std::atoi(e) != 0;

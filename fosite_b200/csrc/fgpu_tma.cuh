@@ -15,12 +15,16 @@
 //   * the own column's z neighbours come from the ring (planes k, k+1) and a register
 //     lookahead (plane k+2, loaded one plane early);
 //   * the epilogue's streams (base and earlier k of a Butcher stage, the Shu-Osher start
-//     state) are brought into L2 one plane ahead by bulk prefetches issued by one warp.
+//     state) are brought into L2 one plane ahead by bulk prefetches, one tile row per thread;
+//   * the x and y interface fluxes run in warp-sized chunks of one direction each, so that
+//     the flux code is specialised for its direction; the common limiters (minmod, MC with
+//     theta = 1, van Leer) are compiled in.
 // Requirements (checked on the host): even nx (16-byte strides of the tensor map), no
 // FARGO frame changes, no viscous source, no accretion rows, a plain or formed stage
 // input (no k-sums in the stencil).
 #pragma once
 #include <cuda.h>
+#include <type_traits>
 #include "fgpu_kernels.cuh"
 
 namespace fgpu {
@@ -86,13 +90,15 @@ struct TmaLayout {
   static constexpr unsigned PLANE_BYTES = 8u * PLANE;
   static constexpr int NSX = V * TY * (TX + 2), NSY = V * (TY + 2) * TX;
   static constexpr int NFX = V * TY * (TX + 1), NFY = V * (TY + 1) * TX;
-  static constexpr size_t SMEM = 128 + 8 * ((size_t)NSLOT * PLANE + NSX + NSY + NFX + NFY + NSLOT);
+  static constexpr size_t SMEM = 8 * ((size_t)NSLOT * PLANE + NSX + NSY + NFX + NFY + NSLOT);
   static_assert(PLANE_BYTES % 128 == 0, "plane slots must stay 128-byte aligned");
 };
 template <int ND> struct TmaSlots { static constexpr int N = ND == 3 ? 3 : 1; };
 
 // ------------------------------------------------------------------ the tile
-template <int ND, bool EU, bool PRIM, int TX, int TY>
+// LIM > 0: the limiter is compiled in (linear reconstruction with that limiter); LIM = 0: the
+// limiter and the reconstruction order are read from the arguments
+template <int ND, bool EU, bool PRIM, int TX, int TY, int LIM>
 __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtensorMap* tmap, const int bx, const int by,
                                                const int bz) {
   using PH = Phys<ND, EU>;
@@ -102,8 +108,10 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
   constexpr int NSLOT = TmaSlots<ND>::N;
   using L = TmaLayout<V, TX, TY, NSLOT>;
   constexpr int RW = L::RW, RHW = L::RH * L::RW;
-  extern __shared__ __align__(16) double tma_smem_raw[];
-  double* const ring = reinterpret_cast<double*>((reinterpret_cast<size_t>(tma_smem_raw) + 127) & ~(size_t)127);
+  // dynamic shared memory, 128-byte aligned (the plane slots are tensor-copy destinations);
+  // every pointer below is an offset from the shared array, so accesses stay shared-space
+  extern __shared__ __align__(128) double tma_smem_raw[];
+  double* const ring = tma_smem_raw;
   double* const Sx = ring + NSLOT * L::PLANE;   // [V][TY][TX+2]
   double* const Sy = Sx + L::NSX;               // [V][TY+2][TX]
   double* const Fx = Sy + L::NSY;               // [V][TY][TX+1]
@@ -120,6 +128,8 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
   const double dt = A.dt_dev ? *A.dt_dev : A.dt;
   const bool roundtrip = EU && A.in.roundtrip;
   const StateRef& SR = A.rin.base ? A.rin : A.in;
+  const int lim = LIM > 0 ? LIM : A.limiter;
+  const bool crec = LIM > 0 ? false : A.constant_recon != 0;   // constant reconstruction (no slopes)
   // the staged values are the reconstruction variables as they stand (a formed primitive
   // stage state, or a conservative state without the CHECK_PMIN round trip), else every
   // staged point is converted once
@@ -163,6 +173,46 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
       PH::p2c(p, R, P);
     }
   };
+  // A face ghost of a staged plane from its mirror cell in the same box, for the boundaries
+  // whose ghosts copy an interior cell (reflecting, axis, no gradients; boundary_reflecting.f90:
+  // 89-204, boundary_axis.f90, boundary_nogradients.f90:75-125) while the staged values are the
+  // reconstruction variables: the arithmetic of face_ghost_p on the same values, no global
+  // load.  False when the face has another rule or the mirror cell lies outside the box.
+  auto box_ghost = [&](const double* S, int d, int lx, int ly, int gi, int gj, double* R) -> bool {
+    if (!raw_ok) return false;
+    const int x = d == 0 ? gi : gj, nd = d == 0 ? g.nx : g.ny;
+    const bool lo = x < 0;
+    const int type = g.bc[2 * d + (lo ? 0 : 1)];
+    if (type != BC_REFLECTING && type != BC_AXIS && type != BC_NOGRAD) return false;
+    const int sdep = lo ? -x : x - (nd - 1);
+    const int mirror = type == BC_NOGRAD ? (lo ? 0 : nd - 1) : (lo ? sdep - 1 : nd - sdep);
+    const int lm = mirror - (d == 0 ? i0 : j0) + 2;   // the mirror's box coordinate along d
+    if (lm < 2 || lm > (d == 0 ? ex : ey) + 1) return false;
+    const double* src = S + (d == 0 ? ly * RW + lm : lm * RW + lx);
+    double p[V];
+    if (PRIM) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) p[v] = src[v * RHW];
+    } else {
+      double u[V];
+#pragma unroll
+      for (int v = 0; v < V; ++v) u[v] = src[v * RHW];
+      PH::c2p(u, p, P);
+    }
+    if (type != BC_NOGRAD) {
+      if (d == 0) p[1] = -p[1];
+      else p[2] = -p[2];
+      if (type == BC_AXIS && d == 0 && M.curv) p[2] = -p[2];
+    }
+    if (roundtrip) p[V - 1] = dmax(p[V - 1], P.pmin);
+    if (PRIM) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) R[v] = p[v];
+    } else {
+      PH::p2c(p, R, P);
+    }
+    return true;
+  };
   // own column at plane gk: raw loads (interior planes), then the reconstruction variables
   auto col_load = [&](int gk, double* u) {
     if (gk >= 0 && gk < g.nz) {
@@ -182,8 +232,8 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
     mbar_expect_tx(b, L::PLANE_BYTES);
     tma_load_box<ND + 1>(slot(kp), tmap, b, i0 - 2, j0 - 2, kp);
   };
-  // planes k0 .. k1-1 are staged by tensor copies; the own column of planes k1, k1+1 comes
-  // from the lookahead
+  // planes k0 .. k1-1 are staged by tensor copies (k0 .. k0+2 now, then plane k+2 once every
+  // thread is past plane k-1); the own column of planes k1, k1+1 comes from the lookahead
   if (tid == 0) {
     abort_flag = 0;
     for (int s = 0; s < NSLOT; ++s) mbar_init(&mbar[s], 1);
@@ -228,7 +278,7 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
         if (gx || gy || !raw_ok) {
           double R[V];
           if (gx || gy) {
-            ghost(gx ? 0 : 1, gi, gj, kp, R);
+            if (!box_ghost(S, gx ? 0 : 1, lx, ly, gi, gj, R)) ghost(gx ? 0 : 1, gi, gj, kp, R);
           } else {
 #pragma unroll
             for (int v = 0; v < V; ++v) R[v] = S[v * RHW + ly * RW + lx];
@@ -243,9 +293,10 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
     }
   };
 
-  // epilogue streams of plane kp brought into L2 (one warp, one bulk prefetch per tile row):
-  // stream q < nf: the next Butcher stage's base and earlier k; then the stage input's base
-  // and k (the last stage's high/low-order sums, or cvar read by the sources); y0; err_low
+  // epilogue streams of plane kp brought into L2 (one bulk prefetch per tile row, spread over
+  // the block): stream q < nf: the next Butcher stage's base and earlier k; then the stage
+  // input's base and k (the last stage's high/low-order sums, or cvar read by the sources);
+  // y0; err_low
   const int nf = A.fnext_out ? A.fnext.nk : 0;
   const bool in_needed = A.last_stage || (PRIM && !roundtrip && (M.curv || A.has_accel || A.out_base ||
                                                                  A.out_mode == OUT_SSPRK)) ||
@@ -264,11 +315,11 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
     return A.err_low;
   };
   auto prefetch_epilogue = [&](int kp) {
-    if (tid >= 32 || kp >= k1) return;
-    const int rows = ey * V * nstreams;
-    for (int r = tid; r < rows; r += 32) {
-      const int q = r / (ey * V), rem = r % (ey * V), v = rem / ey, jr = rem % ey;
-      bulk_prefetch_l2(stream(q) + (long long)v * g.n + CE::lin(g, i0, j0 + jr, kp), 8u * ex);
+    if (kp >= k1) return;
+    const int rows = TY * V * nstreams;
+    for (int r = tid; r < rows; r += NT) {
+      const int jr = r % TY, vq = r / TY, v = vq % V, q = vq / V;
+      if (jr < ey) bulk_prefetch_l2(stream(q) + (long long)v * g.n + CE::lin(g, i0, j0 + jr, kp), 8u * ex);
     }
   };
 
@@ -295,18 +346,18 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
       double szm[V];
 #pragma unroll
       for (int v = 0; v < V; ++v) {
-        szm[v] = A.constant_recon ? 0.0 : slope(A.limiter, A.theta, A.invd[2], Ra[v], Rb[v], Rc[v]);
-        sz0[v] = A.constant_recon ? 0.0 : slope(A.limiter, A.theta, A.invd[2], Rb[v], Rc[v], Rd[v]);
+        szm[v] = crec ? 0.0 : slope(lim, A.theta, A.invd[2], Ra[v], Rb[v], Rc[v]);
+        sz0[v] = crec ? 0.0 : slope(lim, A.theta, A.invd[2], Rb[v], Rc[v], Rd[v]);
       }
       double RL[V], RR[V];
       const double oT = M.offzT[k0 - 1 + 2], oB = M.offzB[k0 + 2];
 #pragma unroll
       for (int v = 0; v < V; ++v) {
-        RL[v] = A.constant_recon ? Rb[v] : Rb[v] + szm[v] * oT;
-        RR[v] = A.constant_recon ? Rc[v] : Rc[v] + sz0[v] * oB;
+        RL[v] = crec ? Rb[v] : Rb[v] + szm[v] * oT;
+        RR[v] = crec ? Rc[v] : Rc[v] + sz0[v] * oB;
       }
-      kt_flux<ND, EU, PRIM>(2, RL, RR, EU ? 0.0 : M.cs[6 * M.nxp + ip], EU ? 0.0 : M.cs[5 * M.nxp + ip], M.dAzB[ip],
-                            P, Fzm);
+      kt_flux<ND, EU, PRIM, 2>(2, RL, RR, EU ? 0.0 : M.cs[6 * M.nxp + ip], EU ? 0.0 : M.cs[5 * M.nxp + ip],
+                               M.dAzB[ip], P, Fzm);
       col_load(k0 + 2, la);
     }
   } else {
@@ -315,128 +366,129 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
   prefetch_epilogue(k0);
 
   bool aborted = false;
+  constexpr int NSXI = TY * (TX + 2), NSYI = (TY + 2) * TX;   // slope items (x, y)
+  constexpr int NFXI = TY * (TX + 1), NFYI = (TY + 1) * TX;   // interface-flux items (x, y)
   for (int k = k0; k < k1; ++k) {
     const double* S = slot(k);
     const int oc = (ty + 2) * RW + tx + 2;   // the own cell in a staged plane
     if (ND == 3) prepare(k + 1);
-    // ---- x and y slopes of plane k (own cells, then the halo ring of the tile)
-    if (!A.constant_recon) {
-      if (own) {
-        const double* c = S + oc;
+    // ---- z: slope at k+1 and the flux at k+1/2 of the own column (planes k, k+1 staged, k+2
+    // from the lookahead, whose registers then take plane k+3's raw values)
+    double divZ[V];
+    if (ND == 3 && own) {
+      const double* S1 = slot(k + 1);
+      col_finish(k + 2, la);
+      double sz1[V], RL[V], RR[V], Fzp[V];
+      const double oT = M.offzT[k + 2], oB = M.offzB[k + 1 + 2];
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-          const double* R = c + v * RHW;
-          Sx[(v * TY + ty) * (TX + 2) + tx + 1] = slope(A.limiter, A.theta, A.invd[0], R[-1], R[0], R[1]);
-          Sy[(v * (TY + 2) + ty + 1) * TX + tx] = slope(A.limiter, A.theta, A.invd[1], R[-RW], R[0], R[RW]);
-        }
+      for (int v = 0; v < V; ++v) {
+        const double r0 = S[v * RHW + oc], r1 = S1[v * RHW + oc];
+        sz1[v] = crec ? 0.0 : slope(lim, A.theta, A.invd[2], r0, r1, la[v]);
+        RL[v] = crec ? r0 : r0 + sz0[v] * oT;
+        RR[v] = crec ? r1 : r1 + sz1[v] * oB;
       }
-      if (tid < 2 * TY + 2 * TX) {
-        int r, c, dx, stride, sidx;
+      col_load(k + 3, la);
+      kt_flux<ND, EU, PRIM, 2>(2, RL, RR, EU ? 0.0 : M.cs[6 * M.nxp + ip], EU ? 0.0 : M.cs[5 * M.nxp + ip],
+                               M.dAzB[ip], P, Fzp);
+      const double dVz = M.dxdydV[ip];
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        divZ[v] = dVz * (Fzp[v] - Fzm[v]);
+        Fzm[v] = Fzp[v];
+        sz0[v] = sz1[v];
+      }
+    }
+    // ---- x and y slopes of plane k: items over the full tile shape (ey rows x ex+2 cells for x,
+    // ey+2 rows x ex cells for y), one code path for both directions, the ones outside a
+    // partial edge tile skipped
+    if (!crec) {
+      for (int t = tid; t < NSXI + NSYI; t += NT) {
+        int cidx, step, sidx, sstride;
         double* Sout;
         double invd;
-        bool valid;
-        if (tid < 2 * TY) {
-          r = tid >> 1;
-          c = (tid & 1) ? ex : -1;
-          valid = r < ey;
-          dx = 1; stride = TY * (TX + 2); Sout = Sx; sidx = r * (TX + 2) + c + 1; invd = A.invd[0];
+        if (t < NSXI) {
+          const int r = t / (TX + 2), c = t % (TX + 2) - 1;
+          if (r >= ey || c > ex) continue;
+          cidx = (r + 2) * RW + (c + 2); step = 1;
+          Sout = Sx; sidx = r * (TX + 2) + (c + 1); sstride = TY * (TX + 2);
+          invd = A.invd[0];
         } else {
-          const int u = tid - 2 * TY;
-          c = u >> 1;
-          r = (u & 1) ? ey : -1;
-          valid = c < ex;
-          dx = RW; stride = (TY + 2) * TX; Sout = Sy; sidx = (r + 1) * TX + c; invd = A.invd[1];
+          const int u = t - NSXI;
+          const int c = u % TX, r = u / TX - 1;
+          if (c >= ex || r > ey) continue;
+          cidx = (r + 2) * RW + (c + 2); step = RW;
+          Sout = Sy; sidx = (r + 1) * TX + c; sstride = (TY + 2) * TX;
+          invd = A.invd[1];
         }
-        if (valid) {
-          const double* R0p = S + (r + 2) * RW + c + 2;
 #pragma unroll
-          for (int v = 0; v < V; ++v) {
-            const double* R = R0p + v * RHW;
-            Sout[v * stride + sidx] = slope(A.limiter, A.theta, invd, R[-dx], R[0], R[dx]);
-          }
+        for (int v = 0; v < V; ++v) {
+          const double* R = S + v * RHW + cidx;
+          Sout[v * sstride + sidx] = slope(lim, A.theta, invd, R[-step], R[0], R[step]);
         }
       }
-      __syncthreads();
     }
-    // ---- x and y interface fluxes of plane k: the own cell's lower faces, then the tile's
-    // upper edge faces
-    auto xy_flux = [&](bool xf, int r, int c) {
-      // xf: x face c (left face of cell c) of row r; else y face r (lower face of row r) of column c
+    __syncthreads();
+    // every thread is past plane k-1's epilogue: its slot takes plane k+2
+    if (ND == 3 && tid == 0 && k >= k0 + 1 && k + 2 < k1) { issue(k + 2); ++issued; }
+    // ---- x and y interface fluxes of plane k: warp-sized chunks of items, each chunk of one
+    // direction, so that the direction is a compile-time constant of the flux code
+    auto xy_flux = [&](auto dir, int t) {
+      constexpr int D = decltype(dir)::value;
       double RL[V], RR[V], F[V];
-      int lidx, ridx, sL, sR, sstride, d;
+      int lidx, ridx, sL, sR, sstride, fstride;
       const double* Sl;
       double* Fout;
-      int fstride;
       double oL, oR, csL, csR, dA;
-      if (xf) {
-        const int gl = i0 + c - 1 + 2;
+      if (D == 0) {
+        const int r = t / (TX + 1), f = t % (TX + 1);
+        if (r >= ey || f > ex) return;
+        const int gl = i0 + f - 1 + 2;   // padded i of the left cell
         oL = M.offxE[gl]; oR = M.offxW[gl + 1];
-        lidx = (r + 2) * RW + c + 1; ridx = lidx + 1;
-        Sl = Sx; sL = r * (TX + 2) + c; sR = sL + 1; sstride = TY * (TX + 2);
+        lidx = (r + 2) * RW + (f + 1); ridx = lidx + 1;
+        Sl = Sx; sL = r * (TX + 2) + f; sR = sL + 1; sstride = TY * (TX + 2);
         csL = EU ? 0.0 : M.cs[2 * M.nxp + gl]; csR = EU ? 0.0 : M.cs[1 * M.nxp + gl + 1];
         dA = M.dAxW[gl + 1];
-        Fout = Fx + r * (TX + 1) + c; fstride = TY * (TX + 1);
-        d = 0;
+        Fout = Fx + r * (TX + 1) + f; fstride = TY * (TX + 1);
       } else {
-        const int gjl = j0 + r - 1 + 2, gi = i0 + c + 2;
+        const int c = t % TX, f = t / TX;
+        if (c >= ex || f > ey) return;
+        const int gjl = j0 + f - 1 + 2, gi = i0 + c + 2;
         oL = M.offyN[gjl]; oR = M.offyS[gjl + 1];
-        lidx = (r + 1) * RW + c + 2; ridx = lidx + RW;
-        Sl = Sy; sL = r * TX + c; sR = sL + TX; sstride = (TY + 2) * TX;
+        lidx = (f + 1) * RW + (c + 2); ridx = lidx + RW;
+        Sl = Sy; sL = f * TX + c; sR = sL + TX; sstride = (TY + 2) * TX;
         csL = EU ? 0.0 : M.cs[4 * M.nxp + gi]; csR = EU ? 0.0 : M.cs[3 * M.nxp + gi];
         dA = M.dAyS[gi];
-        Fout = Fy + r * TX + c; fstride = (TY + 1) * TX;
-        d = 1;
+        Fout = Fy + f * TX + c; fstride = (TY + 1) * TX;
       }
 #pragma unroll
       for (int v = 0; v < V; ++v) {
         const double rl = S[v * RHW + lidx], rr = S[v * RHW + ridx];
-        RL[v] = A.constant_recon ? rl : rl + Sl[v * sstride + sL] * oL;
-        RR[v] = A.constant_recon ? rr : rr + Sl[v * sstride + sR] * oR;
+        RL[v] = crec ? rl : rl + Sl[v * sstride + sL] * oL;
+        RR[v] = crec ? rr : rr + Sl[v * sstride + sR] * oR;
       }
-      kt_flux<ND, EU, PRIM>(d, RL, RR, csL, csR, dA, P, F);
+      kt_flux<ND, EU, PRIM, D>(D, RL, RR, csL, csR, dA, P, F);
 #pragma unroll
       for (int v = 0; v < V; ++v) Fout[v * fstride] = F[v];
     };
-    if (own) {
-      xy_flux(true, ty, tx);
-      xy_flux(false, ty, tx);
-    }
-    if (tid < TY + TX) {
-      if (tid < TY) {
-        if (tid < ey) xy_flux(true, tid, ex);
-      } else if (tid - TY < ex) {
-        xy_flux(false, ey, tid - TY);
+    {
+      constexpr int CX = (NFXI + 31) / 32, CY = (NFYI + 31) / 32;
+      const int warp = tid >> 5, lane = tid & 31;
+      for (int c = warp; c < CX + CY; c += NT / 32) {
+        if (c < CX) {
+          const int t = c * 32 + lane;
+          if (t < NFXI) xy_flux(std::integral_constant<int, 0>(), t);
+        } else {
+          const int t = (c - CX) * 32 + lane;
+          if (t < NFYI) xy_flux(std::integral_constant<int, 1>(), t);
+        }
       }
     }
     __syncthreads();
     if (abort_flag) { aborted = true; break; }   // block-uniform: read after the barrier
-    // ---- divergence, sources and the stage's consumer
+    if (ND == 3) prefetch_epilogue(k + 1);
+    // ---- divergence, sources and the stage's consumer (no barrier after it: the slot of
+    // plane k is next written after the following plane's slope barrier)
     if (own) {
-      double divZ[V];
-      if (ND == 3) {
-        // z: slope at k+1 and the flux at k+1/2 of the own column (planes k, k+1 staged, k+2
-        // from the lookahead, whose registers take plane k+3's raw values after the epilogue)
-        const double* S1 = slot(k + 1);
-        col_finish(k + 2, la);
-        double sz1[V], RL[V], RR[V], Fzp[V];
-        const double oT = M.offzT[k + 2], oB = M.offzB[k + 1 + 2];
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-          const double r0 = S[v * RHW + oc], r1 = S1[v * RHW + oc];
-          sz1[v] = A.constant_recon ? 0.0 : slope(A.limiter, A.theta, A.invd[2], r0, r1, la[v]);
-          RL[v] = A.constant_recon ? r0 : r0 + sz0[v] * oT;
-          RR[v] = A.constant_recon ? r1 : r1 + sz1[v] * oB;
-        }
-        kt_flux<ND, EU, PRIM>(2, RL, RR, EU ? 0.0 : M.cs[6 * M.nxp + ip], EU ? 0.0 : M.cs[5 * M.nxp + ip],
-                              M.dAzB[ip], P, Fzp);
-        const double dVz = M.dxdydV[ip];
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-          divZ[v] = dVz * (Fzp[v] - Fzm[v]);
-          Fzm[v] = Fzp[v];
-          sz0[v] = sz1[v];
-        }
-      }
       double rhs[V], R0[V];
       const double dVx = M.dydzdV[ip], dVy = M.dzdxdV[ip];
 #pragma unroll
@@ -447,14 +499,6 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
         R0[v] = S[v * RHW + oc];
       }
       stage_cell_epilogue<ND, EU, PRIM>(A, i, j, k, R0, rhs, dt, cflv, errv, flags);
-      if (ND == 3) col_load(k + 3, la);
-    }
-    // ---- plane k's slot is free once every thread has read its centre: copy plane k+3 into
-    // it; the epilogue streams of plane k+1 to L2
-    if (ND == 3 && k + 1 < k1) {
-      __syncthreads();
-      if (tid == 0 && k + NSLOT < k1) { issue(k + NSLOT); ++issued; }
-      prefetch_epilogue(k + 1);
     }
   }
 
@@ -479,10 +523,10 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
   }
 }
 
-template <int ND, bool EU, bool PRIM, int TX, int TY, int MINB>
+template <int ND, bool EU, bool PRIM, int TX, int TY, int MINB, int LIM>
 __global__ void __launch_bounds__(TX* TY, MINB)
     tma_stage_kernel(const __grid_constant__ StageArgs A, const __grid_constant__ CUtensorMap tmap) {
-  tma_stage_tile<ND, EU, PRIM, TX, TY>(A, &tmap, blockIdx.x, blockIdx.y, blockIdx.z);
+  tma_stage_tile<ND, EU, PRIM, TX, TY, LIM>(A, &tmap, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 }  // namespace fgpu

@@ -1,0 +1,14 @@
+// fgpu_tma_2d.cu -- the TMA-staged stage kernels of 2D meshes (fgpu_tma.cuh).
+#include "fgpu_tma_nd.cuh"
+
+namespace fgpu {
+cudaError_t tma_stage_launch_2d(bool euler, bool prim, int limiter, bool constant_recon, int ty, const Grid& g,
+                                cudaStream_t s, const StageArgs& A, const CUtensorMap& map) {
+  if (ty == 4) return launch_nd<2, 4>(euler, prim, limiter, constant_recon, g, 1, s, A, map);
+  return launch_nd<2, kTmaTY>(euler, prim, limiter, constant_recon, g, 1, s, A, map);
+}
+void tma_stage_configure_2d(bool euler, bool prim) {
+  configure_nd<2, kTmaTY>(euler, prim);
+  configure_nd<2, 4>(euler, prim);
+}
+}  // namespace fgpu

@@ -1,0 +1,28 @@
+// fgpu_tma_launch.h -- host entry of the TMA-staged stage kernel (fgpu_tma.cuh).
+//
+// The kernel instantiations live in their own translation units (fgpu_tma_2d.cu,
+// fgpu_tma_3d.cu) so that they compile in parallel with the rest of the library.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include "fgpu_kernels.cuh"
+
+namespace fgpu {
+
+// tile shapes of the TMA layouts: 32 x 8 cells (layout 6; 3D: a three-plane ring, two blocks
+// per SM; 2D: one plane, three blocks per SM) and, for 2D meshes, 32 x 4 cells (layout 7, six
+// blocks per SM: twice the blocks on small grids)
+constexpr int kTmaTX = 32, kTmaTY = 8;
+
+// Launch one stage on the TMA layout.  limiter / constant_recon are the config's: the
+// minmod, MC (theta = 1) and van Leer limiters of linear reconstruction have kernels with the
+// limiter compiled in, every other case the kernel that reads it from the arguments.
+cudaError_t tma_stage_launch_2d(bool euler, bool prim, int limiter, bool constant_recon, int ty, const Grid& g,
+                                cudaStream_t s, const StageArgs& A, const CUtensorMap& map);
+cudaError_t tma_stage_launch_3d(bool euler, bool prim, int limiter, bool constant_recon, const Grid& g, int kchunk,
+                                cudaStream_t s, const StageArgs& A, const CUtensorMap& map);
+// opt the kernels into their dynamic shared memory (once per device)
+void tma_stage_configure_2d(bool euler, bool prim);
+void tma_stage_configure_3d(bool euler, bool prim);
+
+}  // namespace fgpu

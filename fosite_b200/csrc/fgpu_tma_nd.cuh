@@ -1,0 +1,70 @@
+// fgpu_tma_nd.cuh -- instantiations of the TMA-staged stage kernel for one dimensionality
+// (included by fgpu_tma_2d.cu and fgpu_tma_3d.cu).
+#pragma once
+#include "fgpu_tma.cuh"
+#include "fgpu_tma_launch.h"
+
+namespace fgpu {
+namespace {
+
+// resident blocks per SM requested from the register allocator: the 32 x 8 tile two (3D) or
+// three (2D), the 32 x 4 tile (2D) six
+template <int ND, int TY> struct TmaMinBlocks { static constexpr int N = ND == 3 ? 2 : (TY == 4 ? 6 : 3); };
+
+template <int ND, bool EU, bool PRIM, int TY, int LIM>
+struct TmaKernel {
+  static constexpr int MINB = TmaMinBlocks<ND, TY>::N;
+  static constexpr size_t SMEM = TmaLayout<Phys<ND, EU>::V, kTmaTX, TY, TmaSlots<ND>::N>::SMEM;
+  static void configure() {
+    cudaFuncSetAttribute(tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+  }
+  static void launch(const Grid& g, int kchunk, cudaStream_t s, const StageArgs& A, const CUtensorMap& map) {
+    const int kz = ND == 3 ? (g.nz + kchunk - 1) / kchunk : 1;
+    dim3 grid((g.nx + kTmaTX - 1) / kTmaTX, (g.ny + TY - 1) / TY, kz);
+    tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM><<<grid, kTmaTX * TY, SMEM, s>>>(A, map);
+  }
+};
+
+template <int ND, bool EU, bool PRIM, int TY>
+void configure_all() {
+  TmaKernel<ND, EU, PRIM, TY, 0>::configure();
+  TmaKernel<ND, EU, PRIM, TY, LIM_MINMOD>::configure();
+  TmaKernel<ND, EU, PRIM, TY, LIM_MC1>::configure();
+  TmaKernel<ND, EU, PRIM, TY, LIM_VANLEER>::configure();
+}
+
+template <int ND, bool EU, bool PRIM, int TY>
+void launch_lim(int limiter, bool constant_recon, const Grid& g, int kchunk, cudaStream_t s, const StageArgs& A,
+                const CUtensorMap& map) {
+  // MC with theta = 1 has its own kernel; MC with another theta reads it from the arguments
+  const int lim = constant_recon ? 0 : (limiter == LIM_MC ? (A.theta == 1.0 ? LIM_MC1 : 0) : limiter);
+  switch (lim) {
+    case LIM_MINMOD: TmaKernel<ND, EU, PRIM, TY, LIM_MINMOD>::launch(g, kchunk, s, A, map); break;
+    case LIM_MC1: TmaKernel<ND, EU, PRIM, TY, LIM_MC1>::launch(g, kchunk, s, A, map); break;
+    case LIM_VANLEER: TmaKernel<ND, EU, PRIM, TY, LIM_VANLEER>::launch(g, kchunk, s, A, map); break;
+    default: TmaKernel<ND, EU, PRIM, TY, 0>::launch(g, kchunk, s, A, map); break;
+  }
+}
+
+template <int ND, int TY>
+cudaError_t launch_nd(bool euler, bool prim, int limiter, bool constant_recon, const Grid& g, int kchunk,
+                      cudaStream_t s, const StageArgs& A, const CUtensorMap& map) {
+  if (euler) {
+    if (prim) launch_lim<ND, true, true, TY>(limiter, constant_recon, g, kchunk, s, A, map);
+    else launch_lim<ND, true, false, TY>(limiter, constant_recon, g, kchunk, s, A, map);
+  } else {
+    if (prim) launch_lim<ND, false, true, TY>(limiter, constant_recon, g, kchunk, s, A, map);
+    else launch_lim<ND, false, false, TY>(limiter, constant_recon, g, kchunk, s, A, map);
+  }
+  return cudaGetLastError();
+}
+
+template <int ND, int TY>
+void configure_nd(bool euler, bool prim) {
+  if (euler) prim ? configure_all<ND, true, true, TY>() : configure_all<ND, true, false, TY>();
+  else prim ? configure_all<ND, false, true, TY>() : configure_all<ND, false, false, TY>();
+}
+
+}  // namespace
+}  // namespace fgpu

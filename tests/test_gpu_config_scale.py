@@ -130,7 +130,8 @@ def test_disk512_fargo(exact):
     assert np.all(np.abs(sums - pin["s2000_sum"]) <= 1e-9 * pin["s2000_abssum"]), (sums, pin["s2000_sum"])
     st = g.status()
     assert st.iter == int(pin["s2000_iter"])
-    assert abs(st.time - float(pin["s2000_time"])) <= 1e-12 * float(pin["s2000_time"])
+    # dt follows the state: within the state's bar (the exact build's exp/log differ by an ulp)
+    assert abs(st.time - float(pin["s2000_time"])) <= 1e-10 * float(pin["s2000_time"])
     g.close()
 
 

@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 from fosite_b200 import abi
-from cases import CASES, _gauss3d
+from cases import _gauss3d
 from test_gpu_parity import _interior
 
 pyoracle = pytest.importorskip("pyoracle")
@@ -20,7 +20,8 @@ pyoracle = pytest.importorskip("pyoracle")
 @pytest.mark.gpu
 def test_single_grid_timeout_then_resume(monkeypatch):
     from fosite_b200.sim import FositeError, Simulation
-    cfg, p, _ = CASES["gauss3d_dopri_mc_prim"]()
+    # Dormand-Prince with tolerance 1e-2: every step of this run is one attempt
+    cfg, p, _ = _gauss3d(tol=1e-2)
     o = pyoracle.Oracle(cfg)
     o.set_state(abi.PVAR, p)
     o.first_step()

@@ -11,7 +11,7 @@
   Dormand-Prince, KT and van Leer on primitive variables, CFL 0.4, tol_rel 0.01.  The reference
   runs it on a spherical mesh (200 radial cells to radius 2 at t = 1, about 100 cells per blast
   radius); spherical meshes are outside this backend, so the explosion runs on a Cartesian
-  256^3 box [-0.5, 0.5]^3 to t = 0.1, where the blast radius (0.41) spans about 105 cells too.
+  256^3 box [-0.5, 0.5]^3 to t = 0.14, where the blast radius (0.47) spans about 120 cells.
   The solution is evaluated at t + T0, T0 the time at which the blast radius equals the radius
   r0 of the initial energy deposit, as the reference does.
 """
@@ -88,7 +88,7 @@ def test_ode_gpu_matches_oracle(name, method, order):
 @pytest.mark.gpu
 def test_sedov3d_l1_envelopes():
     from fosite_b200.sim import Simulation
-    r0, tend = 0.05, 0.1
+    r0, tend = 0.05, 0.14
     cfg, p, _ = problems.sedov(nd=3, n=256, half=0.5, r0=r0, method=abi.DORMAND_PRINCE, tdorder=5,
                                variables=abi.PRIMITIVE, limiter=abi.VANLEER, theta=1.0, cfl=0.4, tol_rel=0.01,
                                tol_abs=(1e-3,), dtlimit=1e-13, stoptime=tend)
