@@ -387,7 +387,8 @@ def run_own(args, world, rank, local):
 
 ENSEMBLE_DESC = ("96 independent 2D isothermal disks, Nr in [64,384], Nphi in [128,768] (multiples of 32), "
                  "cs/vK in [0.03,0.1], sigma index in [-1.5,-0.5], mixed cylindrical/logcylindrical, SSPRK3, "
-                 "point mass, one persistent launch per stage, CUDA-graph captured, autotuned")
+                 "point mass, one launch per stage over every member's tiles, CUDA-graph captured, autotuned; "
+                 "the plain loop steps each member alone, each member's stage layout autotuned")
 
 
 def ensemble_members(n=96, seed=4000):
@@ -430,7 +431,10 @@ def run_ensemble(args, world=1, rank=0, local=0, emit=True):
     b = Batch(members)
     variant = b.autotune(3)
     b.run(args.warmup)
+    plain_layouts = {}
     for s in plain:
+        v = s.autotune(3)
+        plain_layouts[v] = plain_layouts.get(v, 0) + 1
         s.run(args.warmup)
     clk = ClockSampler(local)
     clk.start()
@@ -463,7 +467,8 @@ def run_ensemble(args, world=1, rank=0, local=0, emit=True):
                        "cells": cells, "tiles_rank0": b.tiles, "variant": variant,
                        "parallelism": "members dealt round-robin over %d GPU(s)" % world},
             "member_steps_per_s": members_all * args.steps / t_batch,
-            "plain_loop": {"value": cells * args.steps / t_plain, "ms_per_step": 1e3 * t_plain / args.steps},
+            "plain_loop": {"value": cells * args.steps / t_plain, "ms_per_step": 1e3 * t_plain / args.steps,
+                           "layouts_rank0": {str(k): v for k, v in sorted(plain_layouts.items())}},
             "speedup_vs_plain": t_plain / t_batch, "identical_to_plain": bool(same), "clocks": clocks}
     b.close()
     if emit:

@@ -16,8 +16,10 @@ struct fgpu_batch {
   int nd = 2, order = 3;
   bool euler = false, prim = false;
   cudaStream_t stream = nullptr;
-  int variant = 0;
+  int variant = 0;               // stage layout: 0/2/3 shared-memory tiles, 6 TMA-staged tiles (2D)
   StageArgs* d_args = nullptr;   // [order][n] step stages, then [n] RHS probes of the tuner
+  CUtensorMap* d_maps = nullptr; // [order + 1][n] tensor maps of the stage inputs of d_args (layout 6)
+  int tma_lim = -1;              // compiled-in limiter of layout 6, -1 when the batch cannot use it
   BndArgs* d_bnd = nullptr;      // [n]
   int4* d_tiles = nullptr;
   int ntiles = 0;
@@ -100,6 +102,13 @@ int launch_batched_stage_t(fgpu_batch* b, const StageArgs* args, int variant) {
 }
 
 int launch_batched_stage(fgpu_batch* b, const StageArgs* args, int variant) {
+  if (variant == 6) {   // TMA-staged tiles: tensor maps parallel to the step and probe tables
+    if (!b->d_maps || args < b->d_args || args >= b->d_args + (size_t)(b->order + 1) * b->m.size())
+      return bset_err(b, FGPU_EUNSUPPORTED, "the TMA layout serves fixed-step 2D batches only");
+    BCUDA_TRY(b, tma_batched_launch_2d(b->euler, b->prim, b->tma_lim, args, b->d_maps + (args - b->d_args),
+                                       b->d_tiles, b->ntiles, b->stream));
+    return FGPU_OK;
+  }
   if (b->nd == 2) {
     if (b->euler) return b->prim ? launch_batched_stage_t<2, true, true>(b, args, variant)
                                  : launch_batched_stage_t<2, true, false>(b, args, variant);
@@ -646,6 +655,32 @@ int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
     b->nfab = (int)fab.size();
     b->nfwcb = (int)fwcb.size();
   }
+  // tensor maps of every stage input for the TMA layout: fixed-step 2D members whose stages
+  // it serves (the same conditions as a lone grid's), the limiter compiled in when shared
+  if (b->nd == 2 && !b->embedded && !b->fdir) {
+    std::vector<CUtensorMap> maps(args.size());
+    bool ok = true;
+    int lim = -2;
+    for (size_t q = 0; q < args.size() && ok; ++q) {
+      fgpu_handle* h = b->m[q % n];
+      const StageArgs& A = args[q];
+      ok = tma_eligible(h, A);
+      if (!ok) break;
+      const StateRef& SR = A.rin.base ? A.rin : A.in;
+      const CUtensorMap* mp = stage_tmap(h, SR.base, kTmaTX, kTmaTY);
+      ok = mp != nullptr;
+      if (ok) maps[q] = *mp;
+      const int l = compiled_limiter(A.limiter, A.constant_recon != 0, A.theta);
+      lim = lim == -2 ? l : (lim == l ? lim : 0);
+    }
+    if (ok && !args.empty()) {
+      if (cudaMalloc(&b->d_maps, sizeof(CUtensorMap) * maps.size()) != cudaSuccess ||
+          cudaMemcpy(b->d_maps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(FGPU_ENOMEM, "batch tensor maps");
+      b->tma_lim = lim;
+      if (h0->variant >= 6) b->variant = 6;
+    }
+  }
   if (b->embedded) { if (int rc = build_embedded_tables(b)) return fail(rc, b->err); }
   *out = b;
   return FGPU_OK;
@@ -656,6 +691,7 @@ void fgpu_batch_destroy(fgpu_batch* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->d_args) cudaFree(b->d_args);
+  if (b->d_maps) cudaFree(b->d_maps);
   if (b->d_bnd) cudaFree(b->d_bnd);
   if (b->d_tiles) cudaFree(b->d_tiles);
   if (b->d_bblocks) cudaFree(b->d_bblocks);
@@ -683,6 +719,12 @@ int fgpu_batch_size(const fgpu_batch* b, int* members, int* tiles) {
   if (!b) return FGPU_EARG;
   if (members) *members = (int)b->m.size();
   if (tiles) *tiles = b->ntiles;
+  return FGPU_OK;
+}
+
+int fgpu_batch_layout(const fgpu_batch* b, int* variant) {
+  if (!b || !variant) return FGPU_EARG;
+  *variant = b->variant;
   return FGPU_OK;
 }
 
@@ -740,7 +782,8 @@ int fgpu_batch_autotune(fgpu_batch* b, int reps, int* variant) {
   if (!b) return FGPU_EARG;
   if (reps < 1) reps = 3;
   const StageArgs* probe = b->d_args + (size_t)b->order * b->m.size();
-  const int cand[3] = {0, 2, 3};
+  std::vector<int> cand = {0, 2, 3};
+  if (b->d_maps) cand.push_back(6);
   double best = 1e300;
   int bv = b->variant;
   for (int v : cand) {

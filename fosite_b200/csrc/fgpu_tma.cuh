@@ -529,4 +529,19 @@ __global__ void __launch_bounds__(TX* TY, MINB)
   tma_stage_tile<ND, EU, PRIM, TX, TY, LIM>(A, &tmap, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
+// Batched ensemble on the TMA layout: one block per tile of the flattened tile queue of many
+// independent grids, tile t = (grid, bx, by, bz); args[grid] are the grid's stage arguments and
+// maps[grid] the tensor map of its stage input (global memory, 64-byte aligned, written by the
+// host before the launch).
+template <int ND, bool EU, bool PRIM, int TX, int TY, int MINB, int LIM>
+__global__ void __launch_bounds__(TX* TY, MINB)
+    batched_tma_stage_kernel(const StageArgs* __restrict__ args, const CUtensorMap* __restrict__ maps,
+                             const int4* __restrict__ tiles) {
+  const int4 T = tiles[blockIdx.x];
+  const CUtensorMap* map = maps + T.x;
+  if (threadIdx.x == 0)
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
+  tma_stage_tile<ND, EU, PRIM, TX, TY, LIM>(args[T.x], map, T.y, T.z, T.w);
+}
+
 }  // namespace fgpu

@@ -7,6 +7,17 @@ cudaError_t tma_stage_launch_2d(bool euler, bool prim, int limiter, bool constan
   if (ty == 4) return launch_nd<2, 4>(euler, prim, limiter, constant_recon, g, 1, s, A, map);
   return launch_nd<2, kTmaTY>(euler, prim, limiter, constant_recon, g, 1, s, A, map);
 }
+cudaError_t tma_batched_launch_2d(bool euler, bool prim, int lim, const StageArgs* args, const CUtensorMap* maps,
+                                  const int4* tiles, int ntiles, cudaStream_t s) {
+  if (euler) {
+    if (prim) launch_batched_lim<2, true, true>(lim, args, maps, tiles, ntiles, s);
+    else launch_batched_lim<2, true, false>(lim, args, maps, tiles, ntiles, s);
+  } else {
+    if (prim) launch_batched_lim<2, false, true>(lim, args, maps, tiles, ntiles, s);
+    else launch_batched_lim<2, false, false>(lim, args, maps, tiles, ntiles, s);
+  }
+  return cudaGetLastError();
+}
 void tma_stage_configure_2d(bool euler, bool prim) {
   configure_nd<2, kTmaTY>(euler, prim);
   configure_nd<2, 4>(euler, prim);

@@ -21,6 +21,19 @@ cudaError_t tma_stage_launch_2d(bool euler, bool prim, int limiter, bool constan
                                 cudaStream_t s, const StageArgs& A, const CUtensorMap& map);
 cudaError_t tma_stage_launch_3d(bool euler, bool prim, int limiter, bool constant_recon, const Grid& g, int kchunk,
                                 cudaStream_t s, const StageArgs& A, const CUtensorMap& map);
+// Batched ensembles of 2D grids on the 32 x 8 TMA layout: one block per tile of the tile queue
+// (grid, bx, by, 0); args[grid] and maps[grid] (device arrays) the stage arguments and the
+// tensor map of the stage input of each grid; lim the compiled-in limiter shared by every grid
+// (compiled_limiter), 0 when the grids differ or read it from their arguments.
+cudaError_t tma_batched_launch_2d(bool euler, bool prim, int lim, const StageArgs* args, const CUtensorMap* maps,
+                                  const int4* tiles, int ntiles, cudaStream_t s);
+// the limiter code a stage's TMA kernel is compiled for: minmod, MC with theta = 1 (LIM_MC1),
+// van Leer; 0 when the kernel reads limiter, theta and reconstruction order from the arguments
+inline int compiled_limiter(int limiter, bool constant_recon, double theta) {
+  if (constant_recon) return 0;
+  if (limiter == LIM_MC) return theta == 1.0 ? LIM_MC1 : 0;
+  return (limiter == LIM_MINMOD || limiter == LIM_VANLEER) ? limiter : 0;
+}
 // opt the kernels into their dynamic shared memory (once per device)
 void tma_stage_configure_2d(bool euler, bool prim);
 void tma_stage_configure_3d(bool euler, bool prim);

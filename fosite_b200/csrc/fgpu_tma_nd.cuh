@@ -18,6 +18,13 @@ struct TmaKernel {
   static void configure() {
     cudaFuncSetAttribute(tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    if (ND == 2 && TY == kTmaTY)
+      cudaFuncSetAttribute(batched_tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+  }
+  static void launch_batched(const StageArgs* args, const CUtensorMap* maps, const int4* tiles, int ntiles,
+                             cudaStream_t s) {
+    batched_tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM><<<ntiles, kTmaTX * TY, SMEM, s>>>(args, maps, tiles);
   }
   static void launch(const Grid& g, int kchunk, cudaStream_t s, const StageArgs& A, const CUtensorMap& map) {
     const int kz = ND == 3 ? (g.nz + kchunk - 1) / kchunk : 1;
@@ -38,7 +45,7 @@ template <int ND, bool EU, bool PRIM, int TY>
 void launch_lim(int limiter, bool constant_recon, const Grid& g, int kchunk, cudaStream_t s, const StageArgs& A,
                 const CUtensorMap& map) {
   // MC with theta = 1 has its own kernel; MC with another theta reads it from the arguments
-  const int lim = constant_recon ? 0 : (limiter == LIM_MC ? (A.theta == 1.0 ? LIM_MC1 : 0) : limiter);
+  const int lim = compiled_limiter(limiter, constant_recon, A.theta);
   switch (lim) {
     case LIM_MINMOD: TmaKernel<ND, EU, PRIM, TY, LIM_MINMOD>::launch(g, kchunk, s, A, map); break;
     case LIM_MC1: TmaKernel<ND, EU, PRIM, TY, LIM_MC1>::launch(g, kchunk, s, A, map); break;
@@ -58,6 +65,17 @@ cudaError_t launch_nd(bool euler, bool prim, int limiter, bool constant_recon, c
     else launch_lim<ND, false, false, TY>(limiter, constant_recon, g, kchunk, s, A, map);
   }
   return cudaGetLastError();
+}
+
+template <int ND, bool EU, bool PRIM>
+void launch_batched_lim(int lim, const StageArgs* args, const CUtensorMap* maps, const int4* tiles, int ntiles,
+                        cudaStream_t s) {
+  switch (lim) {
+    case LIM_MINMOD: TmaKernel<ND, EU, PRIM, kTmaTY, LIM_MINMOD>::launch_batched(args, maps, tiles, ntiles, s); break;
+    case LIM_MC1: TmaKernel<ND, EU, PRIM, kTmaTY, LIM_MC1>::launch_batched(args, maps, tiles, ntiles, s); break;
+    case LIM_VANLEER: TmaKernel<ND, EU, PRIM, kTmaTY, LIM_VANLEER>::launch_batched(args, maps, tiles, ntiles, s); break;
+    default: TmaKernel<ND, EU, PRIM, kTmaTY, 0>::launch_batched(args, maps, tiles, ntiles, s); break;
+  }
 }
 
 template <int ND, int TY>

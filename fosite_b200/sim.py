@@ -66,6 +66,7 @@ def lib(exact=False):
     L.fgpu_batch_size.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.fgpu_batch_run.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_int)]
     L.fgpu_batch_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+    L.fgpu_batch_layout.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
     L.fgpu_batch_enqueue.argtypes = [C.c_void_p, C.c_int64]
     L.fgpu_batch_collect.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
     _libs[exact] = L
@@ -273,6 +274,12 @@ class Batch:
     def autotune(self, reps=3):
         v = C.c_int(0)
         self._check(self.L.fgpu_batch_autotune(self.b, int(reps), C.byref(v)))
+        return int(v.value)
+
+    def layout(self):
+        """The batch's stage layout (0/2/3 shared-memory tiles, 6 TMA-staged tiles)."""
+        v = C.c_int(0)
+        self._check(self.L.fgpu_batch_layout(self.b, C.byref(v)))
         return int(v.value)
 
     def close(self):

@@ -320,8 +320,13 @@ int  fgpu_batch_run(fgpu_batch* b, int64_t nsteps, int* active);
  * updates the members' status. */
 int  fgpu_batch_enqueue(fgpu_batch* b, int64_t nsteps);
 int  fgpu_batch_collect(fgpu_batch* b, int* active);
-/* fgpu_autotune for the batched stage kernel. */
+/* fgpu_autotune for the batched stage kernel: times the shared-memory tile layouts
+ * 0, 2, 3 and, for fixed-step 2D batches whose every stage it serves, the
+ * TMA-staged layout 6 (the layout the batch starts with when its first member's
+ * layout is 6 or 7), and keeps the fastest. */
 int  fgpu_batch_autotune(fgpu_batch* b, int reps, int* variant);
+/* the batch's current stage layout */
+int  fgpu_batch_layout(const fgpu_batch* b, int* variant);
 
 /* CalcTimestep for callers that cannot allocate device memory (no counterpart
  * in the reference).  Takes a config and a caller-owned device state in the

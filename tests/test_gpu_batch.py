@@ -53,6 +53,66 @@ def test_disk_ensemble_matches_single_grids(exact):
     b.close()
 
 
+@pytest.mark.parametrize("exact", [True, False])
+def test_disk_ensemble_tma_layout(exact, monkeypatch):
+    """The TMA-staged batched layout (6, one block per tile, tensor maps of every member's stage
+    inputs in a device table): every member equals its lone run on the TMA layout bit for bit,
+    and on the exact build also its lone run on the base tile."""
+    from fosite_b200.sim import Batch
+    monkeypatch.setenv("FGPU_STAGE_VARIANT", "6")
+    specs = _disk_specs(7)
+    members = [_disk_member(*sp, exact=exact) for sp in specs]
+    alone = [_disk_member(*sp, exact=exact) for sp in specs]
+    monkeypatch.setenv("FGPU_STAGE_VARIANT", "0")
+    base = [_disk_member(*sp, exact=exact) for sp in specs] if exact else []
+    b = Batch(members)
+    assert b.layout() == 6
+    assert b.run(21) == len(members)
+    for s in alone + base:
+        rc, done = s.run(21)
+        assert rc == 0 and done == 21
+    for m, s in zip(members, alone):
+        assert (m.status().time, m.status().dt) == (s.status().time, s.status().dt)
+        assert np.array_equal(m.get(abi.CVAR), s.get(abi.CVAR))
+    for m, s in zip(members, base):
+        assert np.array_equal(m.get(abi.CVAR), s.get(abi.CVAR))
+    b.close()
+
+
+@pytest.mark.parametrize("limiters", [(abi.VANLEER, abi.VANLEER, abi.VANLEER),
+                                      (abi.MINMOD, abi.MONOCENT, abi.VANLEER)])
+def test_euler2d_tma_batch_limiters_and_autotune(limiters, monkeypatch):
+    """Euler members on the TMA batched layout with one compiled-in limiter, and with mixed
+    limiters (MC with theta 1.3 among them: the kernel reads limiter and theta per member);
+    the tuner's pick keeps every result."""
+    from fosite_b200.sim import Batch, Simulation
+    monkeypatch.setenv("FGPU_STAGE_VARIANT", "6")
+    sizes = [(40, 36), (64, 20), (34, 50)]
+
+    def make():
+        out = []
+        for k, (n, lim) in enumerate(zip(sizes, limiters)):
+            cfg, p, _ = _khi(n=n, limiter=lim, theta=1.3 if lim == abi.MONOCENT else 1.0,
+                             variables=abi.PRIMITIVE, seed=80 + k)
+            s = Simulation(cfg, exact=True)
+            s.set_state(abi.PVAR, p)
+            s.first_step()
+            out.append(s)
+        return out
+    members, alone = make(), make()
+    b = Batch(members)
+    assert b.layout() == 6
+    b.run(9)
+    v = b.autotune(2)
+    assert v in (0, 2, 3, 6)
+    b.run(9)
+    for s in alone:
+        s.run(18)
+    for m, s in zip(members, alone):
+        assert np.array_equal(m.get(abi.CVAR), s.get(abi.CVAR))
+    b.close()
+
+
 def test_members_stop_independently():
     """A member that reaches its stop time idles while the others go on."""
     from fosite_b200.sim import Batch, Simulation
