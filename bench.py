@@ -134,6 +134,27 @@ def peak_hbm():
         return 6650.0, "fallback"
 
 
+def l2_read_gbs(device, mb=16, passes=64, reps=20):
+    """Read bandwidth of an L2-resident array, measured live with CUDA events: one reduction
+    kernel reads a `mb` MB array `passes` times (a stride-0 view), so the array stays in the
+    126 MB L2 and no launch gap enters the figure.  The denominator of the L2-relative fraction
+    of grids whose stage working set stays in L2."""
+    import torch
+    n = mb * (1 << 20) // 8
+    a = torch.ones(n, dtype=torch.float64, device=device)
+    v = a.view(1, n).expand(passes, n)
+    for _ in range(3):
+        v.sum()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        v.sum()
+    e1.record()
+    torch.cuda.synchronize()
+    return float(n) * 8 * passes * reps / (e0.elapsed_time(e1) * 1e-3) / 1e9
+
+
 def load_traffic_profile(name):
     """DRAM bytes per stage launch per cell from the committed ncu summary, or None."""
     try:
@@ -338,6 +359,8 @@ def run_own(args, world, rank, local):
         sim.close()
         if not args.no_extras:
             run_ensemble(args, world, rank, local, emit=False)   # same collective steps as rank 0
+            run_serve(args, world, rank, local, emit=False, rates=SERVE_EXTRA["rate"],
+                      requests=SERVE_EXTRA["requests"], t_scale=1.0)
         return
     peak, peak_kind = peak_hbm()
     achieved = stp.stage_bytes / (stp.stage_ms * 1e-3) / 1e9 if stp.stage_ms > 0 else None
@@ -347,6 +370,23 @@ def run_own(args, world, rank, local):
         traffic = prof["dram_bytes_per_cell"] * n_cells
     cb = cpu_baseline(args.workload, budget_s=args.cpu_budget) if world == 1 and not args.no_cpu else None
     bpc = algorithmic_bytes_per_cell_update(args.workload, sim.vnum)
+    # where the time of a step goes: kernel time (every launch bracketed by events, direct
+    # launches) against the graph-replayed step of the timed region; the rest is the gaps
+    # between dependent kernels (launch latency, block ramp-up and drain)
+    kern_ms = (stp.stage_ms + stp.other_ms) / args.steps
+    breakdown = {"graph_ms_per_step": ms_max / args.steps, "kernels_ms_per_step": kern_ms,
+                 "stage_ms_per_step": stp.stage_ms / args.steps, "other_ms_per_step": stp.other_ms / args.steps,
+                 "launches_per_step": stp.launches / args.steps,
+                 "gap_ms_per_step": ms_max / args.steps - kern_ms}
+    # grids whose stage working set (the stage's algorithmic bytes) fits in L2: the fraction of
+    # a measured L2-resident copy as well
+    l2 = None
+    per_launch = stp.stage_bytes / max(1, stp.stage_launches)
+    if achieved and per_launch < 96e6:
+        l2peak = l2_read_gbs(local)
+        l2 = {"achieved": achieved, "peak": l2peak, "unit": "GB/s", "frac": achieved / l2peak,
+              "peak_kind": "measured live: one reduction kernel reading a 16 MB L2-resident array 64 times",
+              "working_set_mb": per_launch / 1e6}
     line = {
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
@@ -369,6 +409,8 @@ def run_own(args, world, rank, local):
                      "launch_ms_avg": stp.stage_ms / max(1, stp.stage_launches),
                      "timing": "CUDA events around each stage launch on the library's stream, in a second "
                                "run of the same number of steps (single steps) after the timed region"},
+        "step_breakdown": breakdown,
+        "l2_roofline": l2,
         "cpu_baseline": cb,
         "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": nstate * 8,
                 "d2h_bytes_per_step": nstate * 8},
@@ -382,8 +424,20 @@ def run_own(args, world, rank, local):
         line["ensemble"] = {k: ens[k] for k in ("value", "unit", "ms_per_step", "speedup_vs_plain",
                                                   "identical_to_plain", "plain_loop", "member_steps_per_s")}
         line["ensemble"]["config"] = {k: ens["config"][k] for k in ("description", "members", "cells")}
+        # one serving rate at the full problem times (t_scale 1): p50 / p99 time to solution
+        srv = run_serve(args, world, rank, local, emit=False, rates=SERVE_EXTRA["rate"],
+                        requests=SERVE_EXTRA["requests"], t_scale=1.0)
+        r = srv["rates"][0]
+        line["serve"] = {"rate_req_s": r["rate_req_s"], "requests": r["requests"], "p50_s": r["p50_s"],
+                         "p99_s": r["p99_s"], "makespan_s": r["makespan_s"],
+                         "cell_updates_per_s": r["cell_updates_per_s"], "t_scale": 1.0,
+                         "mix": srv["config"]["mix"]}
     print(json.dumps(line), flush=True)
 
+
+# the serving point of the default line: Poisson arrivals at 20 requests/s, 24 requests of the
+# full mix integrated to their full end times
+SERVE_EXTRA = {"rate": "20", "requests": 24}
 
 ENSEMBLE_DESC = ("96 independent 2D isothermal disks, Nr in [64,384], Nphi in [128,768] (multiples of 32), "
                  "cs/vK in [0.03,0.1], sigma index in [-1.5,-0.5], mixed cylindrical/logcylindrical, SSPRK3, "
@@ -476,19 +530,23 @@ def run_ensemble(args, world=1, rank=0, local=0, emit=True):
     return line
 
 
-def run_serve(args, world=1, rank=0, local=0):
+def run_serve(args, world=1, rank=0, local=0, emit=True, rates=None, requests=None, t_scale=None):
     """Poisson request streams at swept rates through the continuous-batching server.
 
     With N ranks each GPU serves the requests dealt to it round-robin (the stream's
-    arrival times are kept); latencies are gathered on rank 0."""
+    arrival times are kept); latencies are gathered on rank 0.  rates / requests / t_scale
+    override the command line; emit=False returns rank 0's line instead of printing it."""
+    rates = args.rates if rates is None else rates
+    requests = args.requests if requests is None else requests
+    t_scale = args.t_scale if t_scale is None else t_scale
     from fosite_b200 import replicas
     from fosite_b200.serve import Server, poisson_stream
     import torch
     torch.cuda.set_device(local)
     free, total = torch.cuda.mem_get_info()
     out = []
-    for rate in [float(r) for r in args.rates.split(",")]:
-        reqs = replicas.partition(poisson_stream(rate, args.requests, seed=int(rate), t_scale=args.t_scale), rank, world)
+    for rate in [float(r) for r in str(rates).split(",")]:
+        reqs = replicas.partition(poisson_stream(rate, requests, seed=int(rate), t_scale=t_scale), rank, world)
         from fosite_b200.serve import build_problem
         for r in reqs:               # requests arrive with their initial data
             r.payload = build_problem(r)
@@ -512,12 +570,14 @@ def run_serve(args, world=1, rank=0, local=0):
         return
     line = {"metric": "p50/p99 time-to-solution, cell-updates/s", "unit": "s", "n_gpus": world,
             "higher_is_better": False, "dtype": "f64", "data": "synthetic (seeded Poisson streams)",
-            "config": {"workload": "serve", "requests_per_rate": args.requests, "t_scale": args.t_scale,
+            "config": {"workload": "serve", "requests_per_rate": requests, "t_scale": t_scale,
                        "chunk_steps": args.chunk, "payload": "initial data generated before the stream starts "
                                                              "(requests carry their data)",
                        "mix": "2D KHI 64^2-1024^2, 2D disks 64x128-512x1024, 3D pulses 32^3-128^3"},
             "rates": out}
-    print(json.dumps(line), flush=True)
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 def main():
@@ -536,7 +596,7 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=120.0)
     ap.add_argument("--cpu-budget", type=float, default=25.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-extras", action="store_true", help="skip the ensemble comparison of the default line")
+    ap.add_argument("--no-extras", action="store_true", help="skip the ensemble comparison and the serving point of the default line")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:

@@ -137,7 +137,7 @@ template <bool EU>
 void launch_batched_fargo_t(fgpu_batch* b, bool w) {
   if (w) {
     if (b->fdir == 1) batched_fargo_w_kernel<EU, 1><<<b->nfwb, 256, 0, b->stream>>>(b->d_fw, b->d_fwb);
-    else batched_fargo_w_kernel<EU, 2><<<b->nfwb, 256, 0, b->stream>>>(b->d_fw, b->d_fwb);
+    else batched_fargo_w_kernel<EU, 2><<<b->nfwb, FW_NT, 0, b->stream>>>(b->d_fw, b->d_fwb);
   } else {
     if (b->fdir == 1) batched_fargo_advect_kernel<EU, 1><<<b->nfab, 256, 0, b->stream>>>(b->d_fa, b->d_fab);
     else batched_fargo_advect_kernel<EU, 2><<<b->nfab, FA_TX * FA_TY, 0, b->stream>>>(b->d_fa, b->d_fab);
@@ -657,7 +657,7 @@ int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
   }
   // tensor maps of every stage input for the TMA layout: fixed-step 2D members whose stages
   // it serves (the same conditions as a lone grid's), the limiter compiled in when shared
-  if (b->nd == 2 && !b->embedded && !b->fdir) {
+  if (b->nd == 2 && !b->embedded) {
     std::vector<CUtensorMap> maps(args.size());
     bool ok = true;
     int lim = -2;
@@ -880,6 +880,11 @@ int fgpu_autotune(fgpu_handle* h, int reps, int* variant) {
       A.ctl = nullptr;
       A.cfl_mode = 0;
     }
+  } else if (h->fargo && !h->vis && !h->accrete && !h->butcher && !h->adaptive_me && h->order >= 3) {
+    // a middle FARGO Shu-Osher stage with its frame changes (scratch in, scratch out)
+    A = fargo_stage_args(h, fargo_step_of(h), 2);
+    A.ctl = nullptr;
+    A.cfl_mode = 0;
   }
   const int cand[8] = {0, 2, 3, 4, 5, 1, 6, 7};
   // 3D: the z extent a block marches through (smaller chunks give small grids more blocks);
@@ -897,8 +902,8 @@ int fgpu_autotune(fgpu_handle* h, int reps, int* variant) {
   for (int v : cand) {
     // layout 1 lacks these features (Butcher steps gate their stages or form the next stage's state)
     if (v == 1 && (h->fargo || h->accrete || h->vis || h->butcher)) continue;
-    // layouts 6, 7 (TMA-staged planes) serve grids without FARGO, viscosity or accretion, even nx
-    if (v >= 6 && (h->fargo || h->accrete || h->vis || h->g.nx % 2 != 0)) continue;
+    // layouts 6, 7 (TMA-staged planes) serve grids without viscosity or accretion, even nx
+    if (v >= 6 && (h->accrete || h->vis || h->g.nx % 2 != 0)) continue;
     if (v == 7 && h->nd == 3) continue;   // the 32 x 4 TMA tile is built for 2D meshes
     // the taller tiles (4, 5) differ from the oracle in the last bit on FARGO transport along x
     // with a user-supplied background velocity; such grids keep the 32 x 8 tiles

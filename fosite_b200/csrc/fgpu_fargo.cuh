@@ -26,14 +26,17 @@ struct FargoWArgs {
 // pvar is the primitive state of the last ComputeRHS after its
 // SubtractBackgroundVelocityY and this routine's AddBackgroundVelocityY, i.e.
 // (vy - w_prev) + w_prev.  The sum runs in j order like the reference loop, so
-// the result is bitwise reproducible: a block owns WX columns; per chunk of WR
-// rows its threads evaluate the WR x WX terms in parallel into shared memory,
-// then one thread per column adds them in order.
-constexpr int FW_WX = 8, FW_WY = 32, FW_RPT = 4, FW_WR = FW_WY * FW_RPT;
+// the result is bitwise reproducible: a block owns FW_WX columns; per chunk of FW_RC
+// rows (one chunk for up to 512 rows) its FW_NT threads evaluate the terms in parallel
+// into shared memory, each thread FW_RC / (FW_NT / FW_WX) rows of one column with their
+// loads in flight together, then one thread per column adds the chunk's terms in order
+// (shared-memory loads issued ahead of the dependent adds).
+constexpr int FW_WX = 8, FW_NT = 512, FW_RC = 512;
 template <bool EU>
 __device__ __forceinline__ void fargo_w_body(const FargoWArgs& A, const int bx) {
   using CE = Cells<2, EU>;
-  __shared__ double terms[FW_WR][FW_WX + 1];
+  constexpr int RPT = FW_RC / (FW_NT / FW_WX);   // rows per thread and chunk
+  __shared__ double terms[FW_RC][FW_WX];
   if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
   if (gated_out(A.ctl, A.gate)) return;
   const Grid& g = A.g;
@@ -45,10 +48,10 @@ __device__ __forceinline__ void fargo_w_body(const FargoWArgs& A, const int bx) 
   const double wf = valid ? A.wfac[ip] : 0.0;
   const double wp = (valid && A.w_prev) ? A.w_prev[ip] : 0.0;
   double wi = 0.0;
-  for (int j0 = 0; j0 < g.ny; j0 += FW_WR) {
+  for (int j0 = 0; j0 < g.ny; j0 += FW_RC) {
 #pragma unroll
-    for (int r = 0; r < FW_RPT; ++r) {
-      const int q = ty + FW_WY * r, j = j0 + q;
+    for (int r = 0; r < RPT; ++r) {
+      const int q = ty + (FW_NT / FW_WX) * r, j = j0 + q;
       double t = 0.0;
       if (valid && j < g.ny) {
         double p[Phys<2, EU>::V];
@@ -62,15 +65,23 @@ __device__ __forceinline__ void fargo_w_body(const FargoWArgs& A, const int bx) 
     }
     __syncthreads();
     if (ty == 0 && valid) {
-      const int nq = min(FW_WR, g.ny - j0);
-      for (int q = 0; q < nq; ++q) wi = wi + terms[q][tx];
+      const int nq = min(FW_RC, g.ny - j0);
+      int q = 0;
+      for (; q + 8 <= nq; q += 8) {
+        double t[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) t[u] = terms[q + u][tx];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) wi = wi + t[u];
+      }
+      for (; q < nq; ++q) wi = wi + terms[q][tx];
     }
     __syncthreads();
   }
   if (ty == 0 && valid) A.w_out[ip] = wi / (double)g.ny;
 }
 template <bool EU>
-__global__ void __launch_bounds__(FW_WX* FW_WY) fargo_w_kernel(const __grid_constant__ FargoWArgs A) {
+__global__ void __launch_bounds__(FW_NT) fargo_w_kernel(const __grid_constant__ FargoWArgs A) {
   fargo_w_body<EU>(A, blockIdx.x);
 }
 
@@ -342,8 +353,8 @@ __global__ void __launch_bounds__(256) fargo_advect_x_kernel(const __grid_consta
 // block and the member's block count); every FARGO member of a batch transports along the
 // same direction (DIR)
 template <bool EU, int DIR>
-__global__ void __launch_bounds__(256) batched_fargo_w_kernel(const FargoWArgs* __restrict__ args,
-                                                              const int4* __restrict__ blocks) {
+__global__ void __launch_bounds__(DIR == 1 ? 256 : FW_NT) batched_fargo_w_kernel(const FargoWArgs* __restrict__ args,
+                                                                                 const int4* __restrict__ blocks) {
   const int4 T = blocks[blockIdx.x];
   if constexpr (DIR == 1) fargo_w_x_body<EU>(args[T.x], T.y);
   else fargo_w_body<EU>(args[T.x], T.y);

@@ -521,13 +521,13 @@ const CUtensorMap* stage_tmap(fgpu_handle* h, const double* base, int tx, int ty
 }
 
 // The TMA layout serves stages whose input is a plain or formed state (no k-sums at the stencil
-// points) without FARGO frame changes, viscous source or accretion rows, on meshes whose x
-// extent is even (16-byte strides of the tensor map).
+// points) without viscous source or accretion rows, on meshes whose x extent is even (16-byte
+// strides of the tensor map); FARGO frame changes on 2D meshes.
 bool tma_eligible(const fgpu_handle* h, const StageArgs& A) {
   const StateRef& S = A.rin.base ? A.rin : A.in;
-  return h->g.nx % 2 == 0 && !h->fargo && !h->vis && !A.visc && !A.brow && !A.w_sub && !A.flux_out && S.nk == 0 &&
-         !S.pre.n &&
-         !A.in.pre.n && !A.yn_chain.n && !A.y0_chain.n && !A.err_chain.n && tmap_encoder() != nullptr;
+  const bool frames = h->fargo || A.w_sub || S.pre.n || A.in.pre.n || A.yn_chain.n || A.y0_chain.n || A.err_chain.n;
+  return h->g.nx % 2 == 0 && (!frames || h->nd == 2) && !h->vis && !A.visc && !A.brow && !A.flux_out && S.nk == 0 &&
+         (S.pre.n == 0 || &S == &A.in) && tmap_encoder() != nullptr;
 }
 
 template <int ND, bool EU, bool PRIM>
@@ -1007,8 +1007,8 @@ int launch_fargo_w(fgpu_handle* h, const StateRef& in, const double* w_prev, dou
       else fargo_w_x_kernel<false><<<blocks, FX_WX * FX_WY, 0, h->stream>>>(F);
     } else {
       unsigned blocks = (unsigned)((h->g.nx + 4 + FW_WX - 1) / FW_WX);
-      if (h->euler) fargo_w_kernel<true><<<blocks, FW_WX * FW_WY, 0, h->stream>>>(F);
-      else fargo_w_kernel<false><<<blocks, FW_WX * FW_WY, 0, h->stream>>>(F);
+      if (h->euler) fargo_w_kernel<true><<<blocks, FW_NT, 0, h->stream>>>(F);
+      else fargo_w_kernel<false><<<blocks, FW_NT, 0, h->stream>>>(F);
     }
     CUDA_TRY(h, cudaGetLastError());
     return FGPU_OK;

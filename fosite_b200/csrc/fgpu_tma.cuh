@@ -20,8 +20,8 @@
 //     the flux code is specialised for its direction; the common limiters (minmod, MC with
 //     theta = 1, van Leer) are compiled in.
 // Requirements (checked on the host): even nx (16-byte strides of the tensor map), no
-// FARGO frame changes, no viscous source, no accretion rows, a plain or formed stage
-// input (no k-sums in the stencil).
+// viscous source, no accretion rows, a plain or formed stage input (no k-sums in the
+// stencil).  FARGO frame changes (2D) are applied where the staged points are converted.
 #pragma once
 #include <cuda.h>
 #include <type_traits>
@@ -130,10 +130,14 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
   const StateRef& SR = A.rin.base ? A.rin : A.in;
   const int lim = LIM > 0 ? LIM : A.limiter;
   const bool crec = LIM > 0 ? false : A.constant_recon != 0;   // constant reconstruction (no slopes)
+  // FARGO (2D): the stage input's frame changes (the chain of the stored state) and the
+  // subtraction of the background velocity apply to every staged point
+  constexpr bool FG = ND == 2;
+  const bool frames = FG && (A.w_sub != nullptr || A.in.pre.n != 0);
   // the staged values are the reconstruction variables as they stand (a formed primitive
-  // stage state, or a conservative state without the CHECK_PMIN round trip), else every
-  // staged point is converted once
-  const bool raw_ok = PRIM ? (SR.ready != 0) : !roundtrip;
+  // stage state, or a conservative state without the CHECK_PMIN round trip or frame
+  // changes), else every staged point is converted once
+  const bool raw_ok = PRIM ? (SR.ready != 0) : (!roundtrip && !frames);
   const int tid = threadIdx.x;
   const int tx = tid % TX, ty = tid / TX;
   const int i0 = bx * TX, j0 = by * TY;
@@ -147,19 +151,26 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
   const bool xy_ghosts = i0 == 0 || i0 + ex + 2 > g.nx || j0 == 0 || j0 + ey + 2 > g.ny;
   const bool prep_sync = !raw_ok || xy_ghosts;
 
-  // reconstruction variables of a raw staged value (in place), and of a face ghost
-  auto conv = [&](double* u) {
+  // reconstruction variables of a raw staged value of cell (gi, gj) (in place), and of a face
+  // ghost; with FARGO the stored state's frame chain first, the co-moving frame last (the
+  // order of ComputeRHS: AddBackgroundVelocity, CenterBoundary, SubtractBackgroundVelocity)
+  auto conv = [&](double* u, int gi, int gj) {
+    if (FG && A.in.pre.n) apply_chain<V>(A.in.pre, u, g, gi, gj);
     if (PRIM) {
       double p[V];
       PH::c2p(u, p, P);
       if (roundtrip) p[V - 1] = dmax(p[V - 1], P.pmin);
+      if (FG && A.w_sub) sub_velocity(p, A.w_sub[fargo_ix(g, gi, gj)], g.fdir);
 #pragma unroll
       for (int v = 0; v < V; ++v) u[v] = p[v];
-    } else if (roundtrip) {
-      double p[V];
-      PH::c2p(u, p, P);
-      p[V - 1] = dmax(p[V - 1], P.pmin);
-      PH::p2c(p, u, P);
+    } else {
+      if (roundtrip) {
+        double p[V];
+        PH::c2p(u, p, P);
+        p[V - 1] = dmax(p[V - 1], P.pmin);
+        PH::p2c(p, u, P);
+      }
+      if (FG && A.w_sub) frame_change<V>(u, -1.0, A.w_sub[fargo_ix(g, gi, gj)], g.fdir);
     }
   };
   auto ghost = [&](int d, int gi, int gj, int gk, double* R) {
@@ -167,10 +178,12 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
     CE::face_ghost_p(SR, g, P, M, d, gi, gj, gk, p);
     if (roundtrip) p[V - 1] = dmax(p[V - 1], P.pmin);
     if (PRIM) {
+      if (FG && A.w_sub) sub_velocity(p, A.w_sub[fargo_ix(g, gi, gj)], g.fdir);
 #pragma unroll
       for (int v = 0; v < V; ++v) R[v] = p[v];
     } else {
       PH::p2c(p, R, P);
+      if (FG && A.w_sub) frame_change<V>(R, -1.0, A.w_sub[fargo_ix(g, gi, gj)], g.fdir);
     }
   };
   // A face ghost of a staged plane from its mirror cell in the same box, for the boundaries
@@ -223,7 +236,7 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
   };
   auto col_finish = [&](int gk, double* u) {
     if (gk < 0 || gk >= g.nz) ghost(2, i, j, gk, u);
-    else if (!raw_ok) conv(u);
+    else if (!raw_ok) conv(u, i, j);
   };
 
   auto slot = [&](int kp) { return ring + ((kp - k0) % NSLOT) * L::PLANE; };
@@ -282,7 +295,7 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
           } else {
 #pragma unroll
             for (int v = 0; v < V; ++v) R[v] = S[v * RHW + ly * RW + lx];
-            conv(R);
+            conv(R, gi, gj);
           }
 #pragma unroll
           for (int v = 0; v < V; ++v) S[v * RHW + ly * RW + lx] = R[v];

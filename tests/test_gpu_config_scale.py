@@ -104,13 +104,16 @@ def test_khi256_product_build_and_conservation():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("exact", [True, False])
-def test_disk512_fargo(exact):
+@pytest.mark.parametrize("exact,variant", [(True, None), (False, None), (True, 6), (False, 7)])
+def test_disk512_fargo(exact, variant, monkeypatch):
     """Logcylindrical isothermal disk 512x1024 with FARGO and absorbing radial boundaries (tuned
-    layout): one step against the oracle run here, 2000 steps against the pinned rows."""
+    layout, and the TMA-staged tiles with their frame changes): one step against the oracle run
+    here, 2000 steps against the pinned rows."""
     pin = _pin("disk512")
     cfg, p, extra = problems.disk2d(nr=512, nphi=1024, fargo=1)
-    g = _sim(cfg, p, extra, exact)
+    g = _sim(cfg, p, extra, exact, variant, monkeypatch)
+    if variant is not None:
+        assert g.stage_layout()[0] == variant
     o = pyoracle.Oracle(cfg)
     o.set_sound_speeds(np.broadcast_to(extra["bccsound"], o.shape), np.broadcast_to(extra["fcsound"], (4,) + o.shape))
     o.set_state(abi.PVAR, p)

@@ -4,9 +4,10 @@ The stage kernel comes in several tile layouts (shared-memory tiles 0/2/3/4/5, t
 warp-shuffle window 1, the tile whose halo planes arrive by TMA bulk tensor copies 6),
 picked per grid by the tuner; FGPU_STAGE_VARIANT / FGPU_KCHUNK force one.  Every layout
 must give the oracle's numbers bit for bit on the --fmad=false build, and the product
-build must stay within the north-star tolerance.  Launches the TMA layout does not serve
-(FARGO, viscosity, accretion, odd x extent) run on layout 0; those cases check that the
-fallback keeps the results too.
+build must stay within 1e-12 relative L1 of it.  The TMA layout applies FARGO's frame
+changes where it converts the staged points; launches it does not serve (viscosity,
+accretion, odd x extent) run on layout 0, and those cases check that the fallback keeps
+the results too.
 """
 import numpy as np
 import pytest

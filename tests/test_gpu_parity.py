@@ -3,7 +3,7 @@
 The --fmad=false build must agree with the oracle bit for bit (the only
 exceptions are cases with absorbing boundaries or a POWERLAW viscosity exponent,
 where CUDA's exp/log/pow may differ from glibc's by an ulp: tolerance 1e-13).  The product build (FMA on)
-must stay within the north-star tolerance: relative L1 <= 1e-12 after one step
+must stay within relative L1 <= 1e-12 after one step
 and <= 1e-9 after many steps.
 """
 import numpy as np
