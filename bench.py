@@ -134,27 +134,6 @@ def peak_hbm():
         return 6650.0, "fallback"
 
 
-def l2_read_gbs(device, mb=16, passes=64, reps=20):
-    """Read bandwidth of an L2-resident array, measured live with CUDA events: one reduction
-    kernel reads a `mb` MB array `passes` times (a stride-0 view), so the array stays in the
-    126 MB L2 and no launch gap enters the figure.  The denominator of the L2-relative fraction
-    of grids whose stage working set stays in L2."""
-    import torch
-    n = mb * (1 << 20) // 8
-    a = torch.ones(n, dtype=torch.float64, device=device)
-    v = a.view(1, n).expand(passes, n)
-    for _ in range(3):
-        v.sum()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record()
-    for _ in range(reps):
-        v.sum()
-    e1.record()
-    torch.cuda.synchronize()
-    return float(n) * 8 * passes * reps / (e0.elapsed_time(e1) * 1e-3) / 1e9
-
-
 def load_traffic_profile(name):
     """DRAM bytes per stage launch per cell from the committed ncu summary, or None."""
     try:
@@ -300,7 +279,9 @@ def run_own(args, world, rank, local):
     # stage-kernel layout: measured on this GPU by the library's tuner unless forced
     forced = os.environ.get("FGPU_STAGE_VARIANT")
     variant = int(forced) if forced is not None else sim.autotune(3)
-    sim.run(args.warmup)         # also captures the device-clock graphs
+    # warm-up (also captures the device-clock graphs: at least one 16-step graph when the timed
+    # run replays one, so that no capture falls inside the timed region)
+    sim.run(max(args.warmup, min(args.steps, 16)))
     n_cells = cfg.inum * cfg.jnum * cfg.knum
 
     # ---- device-resident timed region (no per-launch instrumentation)
@@ -383,9 +364,11 @@ def run_own(args, world, rank, local):
     l2 = None
     per_launch = stp.stage_bytes / max(1, stp.stage_launches)
     if achieved and per_launch < 96e6:
+        from fosite_b200.sim import l2_read_gbs
         l2peak = l2_read_gbs(local)
         l2 = {"achieved": achieved, "peak": l2peak, "unit": "GB/s", "frac": achieved / l2peak,
-              "peak_kind": "measured live: one reduction kernel reading a 16 MB L2-resident array 64 times",
+              "peak_kind": "measured live: one launch reading a 16 MB L2-resident array 512 times "
+                           "(fgpu_measure_l2_read)",
               "working_set_mb": per_launch / 1e6}
     line = {
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
@@ -422,7 +405,9 @@ def run_own(args, world, rank, local):
         # the batched ensemble against the loop of plain per-grid runs (96 disks), same steps
         ens = run_ensemble(args, world, rank, local, emit=False)
         line["ensemble"] = {k: ens[k] for k in ("value", "unit", "ms_per_step", "speedup_vs_plain",
-                                                  "identical_to_plain", "plain_loop", "member_steps_per_s")}
+                                                  "speedup_vs_plain_tuned", "identical_to_plain", "identity_check",
+                                                  "plain_loop", "plain_loop_tuned", "member_steps_per_s")}
+        line["ensemble"]["layout"] = ens["config"]["variant"]
         line["ensemble"]["config"] = {k: ens["config"][k] for k in ("description", "members", "cells")}
         # one serving rate at the full problem times (t_scale 1): p50 / p99 time to solution
         srv = run_serve(args, world, rank, local, emit=False, rates=SERVE_EXTRA["rate"],
@@ -442,7 +427,7 @@ SERVE_EXTRA = {"rate": "20", "requests": 24}
 ENSEMBLE_DESC = ("96 independent 2D isothermal disks, Nr in [64,384], Nphi in [128,768] (multiples of 32), "
                  "cs/vK in [0.03,0.1], sigma index in [-1.5,-0.5], mixed cylindrical/logcylindrical, SSPRK3, "
                  "point mass, one launch per stage over every member's tiles, CUDA-graph captured, autotuned; "
-                 "the plain loop steps each member alone, each member's stage layout autotuned")
+                 "the plain loops step each member alone (default stage layout / each member's layout autotuned)")
 
 
 def ensemble_members(n=96, seed=4000):
@@ -480,16 +465,23 @@ def run_ensemble(args, world=1, rank=0, local=0, emit=True):
             s.first_step()
             sims.append(s)
         return sims
-    members, plain = make(), make()
+    forced = os.environ.get("FGPU_STAGE_VARIANT")
+    members, plain, tuned = make(), make(), make()
     cells = sum(c.inum * c.jnum for c, _, _ in probs)
     b = Batch(members)
     variant = b.autotune(3)
-    b.run(args.warmup)
-    plain_layouts = {}
+    # warm-up of at least one 16-step graph, so that graph capture stays outside the timed loops
+    wsteps = max(args.warmup, 16)
+    b.run(wsteps)
+    # the plain per-grid loop as the API gives it (default stage layout), and with every member's
+    # stage layout autotuned
+    tuned_layouts = {}
     for s in plain:
+        s.run(wsteps)
+    for s in tuned:
         v = s.autotune(3)
-        plain_layouts[v] = plain_layouts.get(v, 0) + 1
-        s.run(args.warmup)
+        tuned_layouts[v] = tuned_layouts.get(v, 0) + 1
+        s.run(wsteps)
     clk = ClockSampler(local)
     clk.start()
     barrier(world)
@@ -497,16 +489,36 @@ def run_ensemble(args, world=1, rank=0, local=0, emit=True):
     b.run(args.steps)                      # returns after the device finished (status read back)
     t_batch = time.perf_counter() - t0
     clocks = clk.stop()
-    barrier(world)
-    t0 = time.perf_counter()
-    for s in plain:
-        s.run(args.steps)
-    t_plain = time.perf_counter() - t0
-    same = all(np.array_equal(m.get(abi.CVAR), s.get(abi.CVAR)) for m, s in zip(members, plain))
+
+    def loop(sims):
+        barrier(world)
+        t = time.perf_counter()
+        for s in sims:
+            s.run(args.steps)
+        return allmax(time.perf_counter() - t, world)
+    t_plain = loop(plain)
+    t_tuned = loop(tuned)
+    # identity: every member against its lone run on the batch's stage layout (the product
+    # build's layouts may differ from one another in the last bit; each equals the oracle bit for
+    # bit on the --fmad=false build)
+    for s in plain + tuned:
+        s.close()
+    os.environ["FGPU_STAGE_VARIANT"] = str(b.layout())
+    try:
+        check = make()
+    finally:
+        if forced is None:
+            os.environ.pop("FGPU_STAGE_VARIANT", None)
+        else:
+            os.environ["FGPU_STAGE_VARIANT"] = forced
+    for s in check:
+        s.run(wsteps + args.steps)
+    same = all(np.array_equal(m.get(abi.CVAR), s.get(abi.CVAR)) for m, s in zip(members, check))
+    for s in check:
+        s.close()
     value, cells_all, ms_batch = replicas.job_throughput(cells * args.steps, 1e3 * t_batch) if world > 1 else \
         (cells * args.steps / t_batch, cells * args.steps, 1e3 * t_batch)
     t_batch = ms_batch * 1e-3
-    t_plain = allmax(t_plain, world)
     same = allsum(0.0 if same else 1.0, world) == 0.0
     members_all = len(all_probs)
     cells = int(allsum(cells, world))
@@ -522,8 +534,13 @@ def run_ensemble(args, world=1, rank=0, local=0, emit=True):
                        "parallelism": "members dealt round-robin over %d GPU(s)" % world},
             "member_steps_per_s": members_all * args.steps / t_batch,
             "plain_loop": {"value": cells * args.steps / t_plain, "ms_per_step": 1e3 * t_plain / args.steps,
-                           "layouts_rank0": {str(k): v for k, v in sorted(plain_layouts.items())}},
-            "speedup_vs_plain": t_plain / t_batch, "identical_to_plain": bool(same), "clocks": clocks}
+                           "layouts": "the library's default (shared-memory tile 0)"},
+            "plain_loop_tuned": {"value": cells * args.steps / t_tuned, "ms_per_step": 1e3 * t_tuned / args.steps,
+                                 "layouts_rank0": {str(k): v for k, v in sorted(tuned_layouts.items())}},
+            "speedup_vs_plain": t_plain / t_batch, "speedup_vs_plain_tuned": t_tuned / t_batch,
+            "identical_to_plain": bool(same),
+            "identity_check": "every member's state against its lone run on the batch's stage layout",
+            "clocks": clocks}
     b.close()
     if emit:
         print(json.dumps(line), flush=True)

@@ -558,8 +558,15 @@ __device__ __forceinline__ void kt_flux(int d_rt, const double* RL, const double
     return ND == 3 ? (vn == 1 ? q[1] : (vn == 2 ? q[2] : q[3])) : (vn == 1 ? q[1] : q[2]);
   };
   double uL = normal(pL), uR = normal(pR);
+#ifdef FGPU_EXACT
   double am = dmin(dmin(0.0, dmin(0., uR - csR)), dmin(0., uL - csL));
   double ap = dmax(dmax(0.0, dmax(0., uR + csR)), dmax(0., uL + csL));
+#else
+  // the same extrema with two native min/max each (a zero result may differ in sign, which
+  // no flux component sees: it enters as a product and in ap - am)
+  double am = dmin(0.0, dmin(uR - csR, uL - csL));
+  double ap = dmax(0.0, dmax(uR + csR, uL + csL));
+#endif
   double fL[V], fR[V];
   fL[0] = pL[0] * uL;
   fR[0] = pR[0] * uR;

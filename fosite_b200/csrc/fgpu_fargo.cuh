@@ -85,6 +85,68 @@ __global__ void __launch_bounds__(FW_NT) fargo_w_kernel(const __grid_constant__ 
   fargo_w_body<EU>(A, blockIdx.x);
 }
 
+// The same sums for a single grid in two passes, so that the terms (a cell's primitive
+// velocity, or an absorbing / reflecting ghost of a boundary column, which costs many times an
+// interior term) spread over every SM: fargo_w_terms_kernel writes term (ip, j) to a scratch
+// array, one per thread; fargo_w_sum_kernel adds each column's terms in j order, a block per
+// FS_WX columns staging FS_RC rows at a time in shared memory, one thread per column adding.
+template <bool EU>
+__global__ void __launch_bounds__(256) fargo_w_terms_kernel(const __grid_constant__ FargoWArgs A,
+                                                            double* __restrict__ terms) {
+  using CE = Cells<2, EU>;
+  if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
+  if (gated_out(A.ctl, A.gate)) return;
+  const Grid& g = A.g;
+  const int nxp = g.nx + 4;
+  const long long t = blockIdx.x * 256LL + threadIdx.x;
+  if (t >= (long long)nxp * g.ny) return;
+  const int ip = (int)(t % nxp), j = (int)(t / nxp);
+  const int i = ip - 2;
+  double p[Phys<2, EU>::V];
+  if (i < 0 || i >= g.nx) CE::face_ghost_p(A.in, g, A.ph, A.mt, 0, i, j, 0, p);
+  else CE::interior_p(A.in, g, A.ph, i, j, 0, p);
+  double vy = p[2];
+  if (A.w_prev) {
+    const double wp = A.w_prev[ip];
+    vy = (vy - wp) + wp;
+  }
+  terms[t] = vy * A.wfac[ip];
+}
+constexpr int FS_WX = 8, FS_NT = 1024, FS_RC = 512;
+__global__ void __launch_bounds__(FS_NT) fargo_w_sum_kernel(const __grid_constant__ FargoWArgs A,
+                                                            const double* __restrict__ terms) {
+  __shared__ double st[FS_RC * FS_WX];
+  if (A.ctl && (A.ctl->stop | A.ctl->brk)) return;
+  if (gated_out(A.ctl, A.gate)) return;
+  const Grid& g = A.g;
+  const int nxp = g.nx + 4;
+  const int c0 = blockIdx.x * FS_WX;
+  double wi = 0.0;
+  for (int j0 = 0; j0 < g.ny; j0 += FS_RC) {
+    const int nq = min(FS_RC, g.ny - j0);
+#pragma unroll 4
+    for (int e = threadIdx.x; e < FS_RC * FS_WX; e += FS_NT) {
+      const int q = e / FS_WX, c = e % FS_WX;
+      st[e] = (q < nq && c0 + c < nxp) ? __ldg(terms + (long long)(j0 + q) * nxp + c0 + c) : 0.0;
+    }
+    __syncthreads();
+    if (threadIdx.x < FS_WX) {
+      const int c = threadIdx.x;
+      int q = 0;
+      for (; q + 8 <= nq; q += 8) {
+        double t[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) t[u] = st[(q + u) * FS_WX + c];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) wi = wi + t[u];
+      }
+      for (; q < nq; ++q) wi = wi + st[q * FS_WX + c];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x < FS_WX && c0 + (int)threadIdx.x < nxp) A.w_out[c0 + threadIdx.x] = wi / (double)g.ny;
+}
+
 // CalcBackgroundVelocity for direction 1 (timedisc_base.f90:2262-2282):
 //   w(j) = SUM_i pvar(i,j,vx)*wfactor(j) / INUM over the interior i, for every padded row j
 // (the y-ghost rows come from the boundary fill), with vx = (vx - w_prev) + w_prev as for

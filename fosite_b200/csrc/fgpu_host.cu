@@ -185,6 +185,7 @@ struct fgpu_handle {
   int fdir = 2;                 // transport along x (1, w by padded j) or y (2, w by padded i)
   int nw = 0;                   // padded length of w along the other direction
   double* d_w = nullptr;        // [w | w_new | wfactor of direction 1]
+  double* d_fw_terms = nullptr; // direction 2: the background-velocity sum's terms [ny][nx+4]
   int fargo_phase = 0;
   bool fargo_tmp_fresh = true;  // Butcher + FARGO: the stage vectors' frame flags are still unset
   // point-mass accretion: d_acc = [bx (ny) | bxold (ny) | brow (ny) | mass, mdot]
@@ -1006,9 +1007,11 @@ int launch_fargo_w(fgpu_handle* h, const StateRef& in, const double* w_prev, dou
       if (h->euler) fargo_w_x_kernel<true><<<blocks, FX_WX * FX_WY, 0, h->stream>>>(F);
       else fargo_w_x_kernel<false><<<blocks, FX_WX * FX_WY, 0, h->stream>>>(F);
     } else {
-      unsigned blocks = (unsigned)((h->g.nx + 4 + FW_WX - 1) / FW_WX);
-      if (h->euler) fargo_w_kernel<true><<<blocks, FW_NT, 0, h->stream>>>(F);
-      else fargo_w_kernel<false><<<blocks, FW_NT, 0, h->stream>>>(F);
+      const long long nt = (long long)(h->g.nx + 4) * h->g.ny;
+      const unsigned tb = (unsigned)((nt + 255) / 256), sb = (unsigned)((h->g.nx + 4 + FS_WX - 1) / FS_WX);
+      if (h->euler) fargo_w_terms_kernel<true><<<tb, 256, 0, h->stream>>>(F, h->d_fw_terms);
+      else fargo_w_terms_kernel<false><<<tb, 256, 0, h->stream>>>(F, h->d_fw_terms);
+      fargo_w_sum_kernel<<<sb, FS_NT, 0, h->stream>>>(F, h->d_fw_terms);
     }
     CUDA_TRY(h, cudaGetLastError());
     return FGPU_OK;
@@ -1656,6 +1659,23 @@ int validate(fgpu_handle* h) {
 }  // namespace
 
 // ======================================================================= C ABI
+// The grid reads the whole array `passes` times (grid-stride, 16-byte loads that bypass L1, so
+// every pass comes from L2); the sums go to out only if they are non-zero (the array holds
+// zeros), which keeps the loads without writing.
+__global__ void __launch_bounds__(512) l2_read_probe_kernel(const double2* __restrict__ a, size_t n2, int passes,
+                                                            double* out) {
+  double s0 = 0.0, s1 = 0.0;
+  const size_t stride = (size_t)gridDim.x * 512;
+  for (int p = 0; p < passes; ++p)
+#pragma unroll 4
+    for (size_t q = (size_t)blockIdx.x * 512 + threadIdx.x; q < n2; q += stride) {
+      const double2 v = __ldcg(a + q);
+      s0 += v.x;
+      s1 += v.y;
+    }
+  if (s0 + s1 != 0.0) out[threadIdx.x] = s0 + s1;
+}
+
 extern "C" {
 
 void fgpu_config_init(fgpu_config* c) {
@@ -1756,7 +1776,9 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
   }
   if (!rc && h->fargo) {
     h->nw = h->fdir == 1 ? h->g.ny + 4 : h->nxp;
-    if (cudaMalloc(&h->d_w, sizeof(double) * 3 * h->nw) != cudaSuccess) rc = set_err(h, FGPU_ENOMEM, "fargo arrays");
+    if (cudaMalloc(&h->d_w, sizeof(double) * 3 * h->nw) != cudaSuccess ||
+        (h->fdir != 1 && cudaMalloc(&h->d_fw_terms, sizeof(double) * (size_t)h->nxp * h->g.ny) != cudaSuccess))
+      rc = set_err(h, FGPU_ENOMEM, "fargo arrays");
     else cudaMemsetAsync(h->d_w, 0, sizeof(double) * 3 * h->nw, h->stream);
     if (!rc && h->fdir == 1) {
       // wfactor(j) (timedisc_base.f90:435-441): the narrowest x-width of the first interior
@@ -1806,6 +1828,7 @@ void fgpu_destroy(fgpu_handle* h) {
   if (h->d_flux) cudaFree(h->d_flux);
   if (h->d_metric) cudaFree(h->d_metric);
   if (h->d_w) cudaFree(h->d_w);
+  if (h->d_fw_terms) cudaFree(h->d_fw_terms);
   if (h->d_acc) cudaFree(h->d_acc);
   if (h->d_visc) cudaFree(h->d_visc);
   if (h->d_dynvis) cudaFree(h->d_dynvis);
@@ -2556,6 +2579,37 @@ int fgpu_set_stream(fgpu_handle* h, void* stream) {
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   if (!h->own_stream) h->own_stream = h->stream;
   h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+  return FGPU_OK;
+}
+
+int fgpu_measure_l2_read(int device, int mb, int passes, double* gbs) {
+  if (!gbs || mb < 1 || mb > 64 || passes < 1) return FGPU_EARG;
+  if (cudaSetDevice(device) != cudaSuccess) return FGPU_ECUDA;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const size_t n2 = (size_t)mb * (1u << 20) / 16;
+  double2* a = nullptr;
+  double* out = nullptr;
+  if (cudaMalloc(&a, n2 * 16) != cudaSuccess) return FGPU_ENOMEM;
+  if (cudaMalloc(&out, sizeof(double) * 1024) != cudaSuccess) { cudaFree(a); return FGPU_ENOMEM; }
+  cudaMemset(a, 0, n2 * 16);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const unsigned blocks = (unsigned)(4 * sms);
+  l2_read_probe_kernel<<<blocks, 512>>>(a, n2, passes, out);
+  cudaEventRecord(e0);
+  l2_read_probe_kernel<<<blocks, 512>>>(a, n2, passes, out);
+  cudaEventRecord(e1);
+  cudaError_t e = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(a);
+  cudaFree(out);
+  if (e != cudaSuccess || ms <= 0.f) return FGPU_ECUDA;
+  *gbs = (double)n2 * 16.0 * passes / (ms * 1e-3) / 1e9;
   return FGPU_OK;
 }
 

@@ -78,8 +78,8 @@ STAGES = {abi.DORMAND_PRINCE: 7, abi.RK_FEHLBERG: 6, abi.CASH_KARP: 6, abi.SSPRK
 def footprint_bytes(cfg):
     """Device bytes of one admitted grid: its state arrays (stored state and two stage
     scratch arrays for the fixed-step scheme; stored state, cold state, m k-arrays and the
-    formed stage state for an embedded scheme of m stages), the padded download scratch and
-    the metric."""
+    formed stage state for an embedded scheme of m stages), the padded download scratch, the
+    metric and, with FARGO along y, the background-velocity terms."""
     nd = 3 if cfg.knum > 1 else 2
     vnum = 1 + nd + (1 if cfg.physics == abi.EULER else 0)
     n = cfg.inum * cfg.jnum * cfg.knum
@@ -90,7 +90,8 @@ def footprint_bytes(cfg):
         if cfg.method in (abi.RK_FEHLBERG, abi.SSPRK) and cfg.tdorder == 3:
             m = 3
         arrays = 3 + m
-    return 8 * vnum * (arrays * n + 2 * npad) + 8 * 40 * (cfg.inum + 4) + (1 << 16)
+    fargo_terms = (cfg.inum + 4) * cfg.jnum if cfg.fargo_method and cfg.fargo_direction != 1 else 0
+    return 8 * vnum * (arrays * n + 2 * npad) + 8 * 40 * (cfg.inum + 4) + 8 * fargo_terms + (1 << 16)
 
 
 def kernel_class(cfg):

@@ -67,10 +67,20 @@ def lib(exact=False):
     L.fgpu_batch_run.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_int)]
     L.fgpu_batch_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
     L.fgpu_batch_layout.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
+    L.fgpu_measure_l2_read.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]
     L.fgpu_batch_enqueue.argtypes = [C.c_void_p, C.c_int64]
     L.fgpu_batch_collect.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
     _libs[exact] = L
     return L
+
+
+def l2_read_gbs(device=0, mb=16, passes=512):
+    """Measured read bandwidth (GB/s) of an L2-resident array of mb MB (fgpu_measure_l2_read)."""
+    v = C.c_double(0.0)
+    rc = lib().fgpu_measure_l2_read(int(device), int(mb), int(passes), C.byref(v))
+    if rc != 0:
+        raise FositeError(rc, "fgpu_measure_l2_read failed")
+    return float(v.value)
 
 
 class FositeError(RuntimeError):

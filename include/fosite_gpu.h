@@ -378,6 +378,11 @@ typedef struct fgpu_stats {
 int fgpu_set_profiling(fgpu_handle* h, int on);
 int fgpu_get_stats(fgpu_handle* h, fgpu_stats* st);
 int fgpu_reset_stats(fgpu_handle* h);
+/* Read bandwidth (GB/s) of an L2-resident array of mb MB (at most 64) on the device:
+ * one launch whose grid reads the array `passes` times (16-byte loads), timed with
+ * CUDA events after a warm-up launch; the denominator of L2-relative roofline
+ * fractions for grids whose working set stays in L2. */
+int fgpu_measure_l2_read(int device, int mb, int passes, double* gbs);
 
 #ifdef __cplusplus
 }
