@@ -20,6 +20,8 @@ struct fgpu_batch {
   StageArgs* d_args = nullptr;   // [order][n] step stages, then [n] RHS probes of the tuner
   CUtensorMap* d_maps = nullptr; // [order + 1][n] tensor maps of the stage inputs of d_args (layout 6)
   int tma_lim = -1;              // compiled-in limiter of layout 6, -1 when the batch cannot use it
+  int4* d_tcols = nullptr;       // layout 6: (member, bx, byb, 0), columns of kchunk tiles per block
+  int ntcols = 0;
   BndArgs* d_bnd = nullptr;      // [n]
   int4* d_tiles = nullptr;
   int ntiles = 0;
@@ -73,52 +75,20 @@ int bset_err(fgpu_batch* b, int code, const std::string& msg) {
                       std::string(#call) + ": " + cudaGetErrorString(e_));                   \
   } while (0)
 
-template <class K>
-int persistent_grid(fgpu_batch* b, K kernel, int threads, size_t smem, int ntiles) {
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
-    per_sm = 1;
-  return std::max(1, std::min(ntiles, per_sm * b->sms));
-}
-
-template <int ND, bool EU, bool PRIM, int MINB>
-void launch_batched_layout(fgpu_batch* b, const StageArgs* args) {
-  constexpr int TY = TileShapes<ND>::TY;
-  constexpr int T = 32 * TY;
-  constexpr size_t SM = TileLayout<ND, EU, PRIM, 32, TY, MINB>::SMEM;
-  auto k = batched_stage_kernel<ND, EU, PRIM, 32, TY, MINB>;
-  k<<<persistent_grid(b, k, T, SM, b->ntiles), T, SM, b->stream>>>(args, b->d_tiles, b->ntiles);
-}
-
-// batches keep the base tile height (their tile queue is built for it): layouts 0, 2, 3
-template <int ND, bool EU, bool PRIM>
-int launch_batched_stage_t(fgpu_batch* b, const StageArgs* args, int variant) {
-  using S = TileShapes<ND>;
-  if (variant == 2) launch_batched_layout<ND, EU, PRIM, S::M2>(b, args);
-  else if (variant == 3) launch_batched_layout<ND, EU, PRIM, S::M3>(b, args);
-  else launch_batched_layout<ND, EU, PRIM, 1>(b, args);
-  BCUDA_TRY(b, cudaGetLastError());
-  return FGPU_OK;
-}
-
 int launch_batched_stage(fgpu_batch* b, const StageArgs* args, int variant) {
   if (variant == 6) {   // TMA-staged tiles: tensor maps parallel to the step and probe tables
     if (!b->d_maps || args < b->d_args || args >= b->d_args + (size_t)(b->order + 1) * b->m.size())
       return bset_err(b, FGPU_EUNSUPPORTED, "the TMA layout serves fixed-step 2D batches only");
     BCUDA_TRY(b, tma_batched_launch_2d(b->euler, b->prim, b->tma_lim, args, b->d_maps + (args - b->d_args),
-                                       b->d_tiles, b->ntiles, b->stream));
+                                       b->d_tcols, b->ntcols, b->stream));
     return FGPU_OK;
   }
-  if (b->nd == 2) {
-    if (b->euler) return b->prim ? launch_batched_stage_t<2, true, true>(b, args, variant)
-                                 : launch_batched_stage_t<2, true, false>(b, args, variant);
-    return b->prim ? launch_batched_stage_t<2, false, true>(b, args, variant)
-                   : launch_batched_stage_t<2, false, false>(b, args, variant);
-  }
-  if (b->euler) return b->prim ? launch_batched_stage_t<3, true, true>(b, args, variant)
-                               : launch_batched_stage_t<3, true, false>(b, args, variant);
-  return b->prim ? launch_batched_stage_t<3, false, true>(b, args, variant)
-                 : launch_batched_stage_t<3, false, false>(b, args, variant);
+  // the shared-memory base tile of the batch's tile queue: layouts 0, 2, 3
+  if (b->nd == 2)
+    BCUDA_TRY(b, legacy_batched_launch_2d(b->euler, b->prim, variant, args, b->d_tiles, b->ntiles, b->sms, b->stream));
+  else
+    BCUDA_TRY(b, legacy_batched_launch_3d(b->euler, b->prim, variant, args, b->d_tiles, b->ntiles, b->sms, b->stream));
+  return FGPU_OK;
 }
 
 int launch_batched_boundary(fgpu_batch* b) {
@@ -618,7 +588,7 @@ int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
     args[(size_t)b->order * n + i] = R;
     bnd[i] = h->fargo ? fargo_closing_bnd(h, F) : bnd_args(h, h->buf[0], h->roundtrip_cfg, FIN_STEP);
     const Grid& g = h->g;
-    const int TY = b->nd == 2 ? 8 : 4;
+    const int TY = b->nd == 2 ? kBaseTY2 : kBaseTY3;
     const int tx = (g.nx + 31) / 32, ty = (g.ny + TY - 1) / TY;
     const int tz = b->nd == 3 ? (g.nz + h->kchunk - 1) / h->kchunk : 1;
     for (int z = 0; z < tz; ++z)
@@ -674,8 +644,23 @@ int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
       lim = lim == -2 ? l : (lim == l ? lim : 0);
     }
     if (ok && !args.empty()) {
+      // blocks of tpb tiles along y (the boxes double-buffered); the 2D stage arguments carry
+      // tpb in kchunk, which the shared-memory tiles of 2D meshes do not read
+      const int tpb = tma_tiles_per_block(b->ntiles, 3);
+      std::vector<int4> cols;
+      for (int i = 0; i < n; ++i) {
+        const Grid& g = b->m[i]->g;
+        const int tx = (g.nx + kTmaTX - 1) / kTmaTX, tyb = ((g.ny + kTmaTY - 1) / kTmaTY + tpb - 1) / tpb;
+        for (int y = 0; y < tyb; ++y)
+          for (int x = 0; x < tx; ++x) cols.push_back(make_int4(i, x, y, 0));
+      }
+      for (auto& A : args) A.kchunk = tpb;
+      b->ntcols = (int)cols.size();
       if (cudaMalloc(&b->d_maps, sizeof(CUtensorMap) * maps.size()) != cudaSuccess ||
-          cudaMemcpy(b->d_maps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+          cudaMemcpy(b->d_maps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+          cudaMalloc(&b->d_tcols, sizeof(int4) * cols.size()) != cudaSuccess ||
+          cudaMemcpy(b->d_tcols, cols.data(), sizeof(int4) * cols.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+          cudaMemcpy(b->d_args, args.data(), sizeof(StageArgs) * args.size(), cudaMemcpyHostToDevice) != cudaSuccess)
         return fail(FGPU_ENOMEM, "batch tensor maps");
       b->tma_lim = lim;
       if (h0->variant >= 6) b->variant = 6;
@@ -692,6 +677,7 @@ void fgpu_batch_destroy(fgpu_batch* b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->d_args) cudaFree(b->d_args);
   if (b->d_maps) cudaFree(b->d_maps);
+  if (b->d_tcols) cudaFree(b->d_tcols);
   if (b->d_bnd) cudaFree(b->d_bnd);
   if (b->d_tiles) cudaFree(b->d_tiles);
   if (b->d_bblocks) cudaFree(b->d_bblocks);

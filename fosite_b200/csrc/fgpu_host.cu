@@ -24,12 +24,12 @@
 #include <cstdlib>
 #include "../../include/fosite_gpu.h"
 #include "fgpu_kernels_misc.cuh"
-#include "fgpu_stage2.cuh"
 #include "fgpu_fargo.cuh"
 #include "fgpu_visc.cuh"
 #include "fgpu_ddmath.h"
 #include "fgpu_bt.cuh"
 #include "fgpu_tma_launch.h"
+#include "fgpu_stage_launch.h"
 
 using namespace fgpu;
 
@@ -427,51 +427,15 @@ int upload_metric(fgpu_handle* h) {
 }
 
 // ---------------------------------------------------------------- launchers
-// A shared-memory tile layout of the stage kernel: TX x TY cells per block,
-// MINB resident blocks per SM requested from the register allocator.
-template <int ND, bool EU, bool PRIM, int TX, int TY, int MINB>
-struct TileLayout {
-  static constexpr size_t SMEM = stage_smem_bytes<Phys<ND, EU>::V, TX, TY>();
-  // the tiles use more than the default 48 KB of dynamic shared memory: opt in (per device)
-  static void configure(bool batched) {
-    cudaFuncSetAttribute(stage_kernel<ND, EU, PRIM, TX, TY, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)SMEM);
-    if (batched)
-      cudaFuncSetAttribute(batched_stage_kernel<ND, EU, PRIM, TX, TY, MINB>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
-  }
-  static void launch(const Grid& g, int kchunk, cudaStream_t s, const StageArgs& A) {
-    const int kz = ND == 3 ? (g.nz + kchunk - 1) / kchunk : 1;
-    dim3 grid((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, kz);
-    stage_kernel<ND, EU, PRIM, TX, TY, MINB><<<grid, TX * TY, SMEM, s>>>(A);
-  }
-};
-// Layouts by variant id: 0 the base tile (2D 32x8, 3D 32x4 marching in z), 2/3 the
-// base tile with a register cap for more resident blocks (2D 2/3, 3D 4/6 per SM),
-// 4 a taller tile (2D 32x16, 3D 32x8 with 2 blocks per SM) that halves the y halo;
-// 1 is the warp-shuffle kernel of fgpu_stage2.cuh.
-template <int ND> struct TileShapes;
-template <> struct TileShapes<2> { static constexpr int TY = 8, M2 = 2, M3 = 3, TY4 = 16, M4 = 1, M5 = 1; };
-template <> struct TileShapes<3> { static constexpr int TY = 4, M2 = 4, M3 = 6, TY4 = 8, M4 = 2, M5 = 3; };
-
-template <int ND, bool EU, bool PRIM>
-void configure_stage_kernels_t() {
-  using S = TileShapes<ND>;
-  TileLayout<ND, EU, PRIM, 32, S::TY, 1>::configure(true);
-  TileLayout<ND, EU, PRIM, 32, S::TY, S::M2>::configure(true);
-  TileLayout<ND, EU, PRIM, 32, S::TY, S::M3>::configure(true);
-  TileLayout<ND, EU, PRIM, 32, S::TY4, S::M4>::configure(false);
-  TileLayout<ND, EU, PRIM, 32, S::TY4, S::M5>::configure(false);
-  if (ND == 3) tma_stage_configure_3d(EU, PRIM);
-  else tma_stage_configure_2d(EU, PRIM);
-}
+// (the shared-memory stage layouts are launched through fgpu_stage_launch.h, the TMA-staged
+// ones through fgpu_tma_launch.h)
 void configure_stage_kernels(int nd, bool e, bool p) {
   if (nd == 2) {
-    if (e) p ? configure_stage_kernels_t<2, true, true>() : configure_stage_kernels_t<2, true, false>();
-    else p ? configure_stage_kernels_t<2, false, true>() : configure_stage_kernels_t<2, false, false>();
+    legacy_stage_configure_2d(e, p);
+    tma_stage_configure_2d(e, p);
   } else {
-    if (e) p ? configure_stage_kernels_t<3, true, true>() : configure_stage_kernels_t<3, true, false>();
-    else p ? configure_stage_kernels_t<3, false, true>() : configure_stage_kernels_t<3, false, false>();
+    legacy_stage_configure_3d(e, p);
+    tma_stage_configure_3d(e, p);
   }
 }
 
@@ -533,10 +497,8 @@ bool tma_eligible(const fgpu_handle* h, const StageArgs& A) {
 
 template <int ND, bool EU, bool PRIM>
 int launch_stage_t(fgpu_handle* h, StageArgs& A) {
-  using S = TileShapes<ND>;
   A.kchunk = h->kchunk;
   const Grid& g = h->g;
-  const int kz = ND == 3 ? (g.nz + h->kchunk - 1) / h->kchunk : 1;
   if ((h->variant == 6 || (h->variant == 7 && ND == 2)) && tma_eligible(h, A)) {
     const StateRef& SR = A.rin.base ? A.rin : A.in;
     const int ty = h->variant == 7 ? 4 : kTmaTY;
@@ -555,20 +517,8 @@ int launch_stage_t(fgpu_handle* h, StageArgs& A) {
       (h->variant == 1 && (h->fargo || h->accrete || h->vis || A.gate || A.fnext_out || A.cfl_mode == 3 ||
                            A.flux_out))
           ? 0 : (h->variant >= 6 ? 0 : h->variant);
-  switch (variant) {
-    case 1: {
-      // warp-shuffle layout: 32 x 8 points per block, 30 x 6 output cells
-      constexpr int NW = 8;
-      dim3 grid((g.nx + 29) / 30, (g.ny + NW - 3) / (NW - 2), kz);
-      stage2_kernel<ND, EU, PRIM, NW><<<grid, 32 * NW, 0, h->stream>>>(A);
-      break;
-    }
-    case 2: TileLayout<ND, EU, PRIM, 32, S::TY, S::M2>::launch(g, h->kchunk, h->stream, A); break;
-    case 3: TileLayout<ND, EU, PRIM, 32, S::TY, S::M3>::launch(g, h->kchunk, h->stream, A); break;
-    case 4: TileLayout<ND, EU, PRIM, 32, S::TY4, S::M4>::launch(g, h->kchunk, h->stream, A); break;
-    case 5: TileLayout<ND, EU, PRIM, 32, S::TY4, S::M5>::launch(g, h->kchunk, h->stream, A); break;
-    default: TileLayout<ND, EU, PRIM, 32, S::TY, 1>::launch(g, h->kchunk, h->stream, A); break;
-  }
+  if (ND == 3) CUDA_TRY(h, legacy_stage_launch_3d(EU, PRIM, variant, g, h->kchunk, h->stream, A));
+  else CUDA_TRY(h, legacy_stage_launch_2d(EU, PRIM, variant, g, h->stream, A));
   CUDA_TRY(h, cudaGetLastError());
   return FGPU_OK;
 }

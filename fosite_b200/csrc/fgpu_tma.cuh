@@ -7,7 +7,9 @@
 //     copy (cp.async.bulk.tensor, 4-D map x, y, z, variable) completing on an mbarrier;
 //     a 3D tile marches along z with a ring of three plane slots, the copy of plane k+3
 //     issued while plane k is computed, so the stencil reads each cell from HBM once per
-//     stage and never waits on a load in its inner phases;
+//     stage and never waits on a load in its inner phases; a 2D block computes a column of
+//     tiles with two box slots, the copy of the next tile in flight while one is computed,
+//     and reduces its CFL / error maxima once for the column;
 //   * interior tiles need no boundary logic at all; tiles touching an x or y face fill
 //     their ghost cells once per plane in shared memory (CenterBoundary rules,
 //     boundary_generic.f90:287-418), the z ghosts of the own column come from the same
@@ -93,7 +95,9 @@ struct TmaLayout {
   static constexpr size_t SMEM = 8 * ((size_t)NSLOT * PLANE + NSX + NSY + NFX + NFY + NSLOT);
   static_assert(PLANE_BYTES % 128 == 0, "plane slots must stay 128-byte aligned");
 };
-template <int ND> struct TmaSlots { static constexpr int N = ND == 3 ? 3 : 1; };
+// plane slots: a 3D tile's ring of three z planes; a 2D block's two boxes (the tile being
+// computed and the next tile of its column, whose copy is in flight)
+template <int ND> struct TmaSlots { static constexpr int N = ND == 3 ? 3 : 2; };
 
 // ------------------------------------------------------------------ the tile
 // LIM > 0: the limiter is compiled in (linear reconstruction with that limiter); LIM = 0: the
@@ -140,16 +144,35 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
   const bool raw_ok = PRIM ? (SR.ready != 0) : (!roundtrip && !frames);
   const int tid = threadIdx.x;
   const int tx = tid % TX, ty = tid / TX;
-  const int i0 = bx * TX, j0 = by * TY;
-  const int ex = min(TX, g.nx - i0), ey = min(TY, g.ny - j0);
-  const bool own = tx < ex && ty < ey;
-  const int i = i0 + tx, j = j0 + ty;
+  const int i0 = bx * TX;
+  const int ex = min(TX, g.nx - i0);
+  const int i = i0 + tx;
   const int ip = i + 2;
-  int k0 = 0, k1 = 1;
-  if (ND == 3) { k0 = bz * A.kchunk; k1 = min(g.nz, k0 + A.kchunk); }
+  // 3D: planes k0 .. k1-1 of the tile (bx, by); 2D: the block computes tiles jb0 .. jb0+k1-1 of
+  // column bx (by counts blocks of A.kchunk tiles), "plane" kp being tile jb0 + kp
+  int k0 = 0, k1 = 1, jb0 = by;
+  if (ND == 3) {
+    k0 = bz * A.kchunk;
+    k1 = min(g.nz, k0 + A.kchunk);
+  } else {
+    jb0 = by * A.kchunk;
+    k1 = min(A.kchunk, (g.ny + TY - 1) / TY - jb0);
+  }
+  auto tile_j0 = [&](int kp) { return ND == 3 ? by * TY : (jb0 + kp) * TY; };
+  int j0 = tile_j0(k0), ey = min(TY, g.ny - j0);
+  bool own = tx < ex && ty < ey;
+  int j = j0 + ty;
   // the tile's staged box reaches ghost cells of an x or y face
-  const bool xy_ghosts = i0 == 0 || i0 + ex + 2 > g.nx || j0 == 0 || j0 + ey + 2 > g.ny;
-  const bool prep_sync = !raw_ok || xy_ghosts;
+  bool xy_ghosts = i0 == 0 || i0 + ex + 2 > g.nx || j0 == 0 || j0 + ey + 2 > g.ny;
+  bool prep_sync = !raw_ok || xy_ghosts;
+  auto set_tile = [&](int kp) {   // 2D: the block's current tile becomes tile jb0 + kp
+    j0 = tile_j0(kp);
+    ey = min(TY, g.ny - j0);
+    own = tx < ex && ty < ey;
+    j = j0 + ty;
+    xy_ghosts = i0 == 0 || i0 + ex + 2 > g.nx || j0 == 0 || j0 + ey + 2 > g.ny;
+    prep_sync = !raw_ok || xy_ghosts;
+  };
 
   // reconstruction variables of a raw staged value of cell (gi, gj) (in place), and of a face
   // ghost; with FARGO the stored state's frame chain first, the co-moving frame last (the
@@ -243,10 +266,11 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
   auto issue = [&](int kp) {   // one thread: the tensor copy of plane kp's box into its slot
     unsigned long long* b = &mbar[(kp - k0) % NSLOT];
     mbar_expect_tx(b, L::PLANE_BYTES);
-    tma_load_box<ND + 1>(slot(kp), tmap, b, i0 - 2, j0 - 2, kp);
+    tma_load_box<ND + 1>(slot(kp), tmap, b, i0 - 2, tile_j0(kp) - 2, ND == 3 ? kp : 0);
   };
-  // planes k0 .. k1-1 are staged by tensor copies (k0 .. k0+2 now, then plane k+2 once every
-  // thread is past plane k-1); the own column of planes k1, k1+1 comes from the lookahead
+  // planes k0 .. k1-1 are staged by tensor copies (the first NSLOT now, then plane
+  // k+NSLOT-1 once every thread is past plane k-1); 3D: the own column of planes k1, k1+1
+  // comes from the lookahead
   if (tid == 0) {
     abort_flag = 0;
     for (int s = 0; s < NSLOT; ++s) mbar_init(&mbar[s], 1);
@@ -291,7 +315,7 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
         if (gx || gy || !raw_ok) {
           double R[V];
           if (gx || gy) {
-            if (!box_ghost(S, gx ? 0 : 1, lx, ly, gi, gj, R)) ghost(gx ? 0 : 1, gi, gj, kp, R);
+            if (!box_ghost(S, gx ? 0 : 1, lx, ly, gi, gj, R)) ghost(gx ? 0 : 1, gi, gj, ND == 3 ? kp : 0, R);
           } else {
 #pragma unroll
             for (int v = 0; v < V; ++v) R[v] = S[v * RHW + ly * RW + lx];
@@ -330,9 +354,10 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
   auto prefetch_epilogue = [&](int kp) {
     if (kp >= k1) return;
     const int rows = TY * V * nstreams;
+    const int pj0 = tile_j0(kp), pey = min(TY, g.ny - pj0), pk = ND == 3 ? kp : 0;
     for (int r = tid; r < rows; r += NT) {
       const int jr = r % TY, vq = r / TY, v = vq % V, q = vq / V;
-      if (jr < ey) bulk_prefetch_l2(stream(q) + (long long)v * g.n + CE::lin(g, i0, j0 + jr, kp), 8u * ex);
+      if (jr < pey) bulk_prefetch_l2(stream(q) + (long long)v * g.n + CE::lin(g, i0, pj0 + jr, pk), 8u * ex);
     }
   };
 
@@ -373,8 +398,6 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
                                M.dAzB[ip], P, Fzm);
       col_load(k0 + 2, la);
     }
-  } else {
-    prepare(0);
   }
   prefetch_epilogue(k0);
 
@@ -384,7 +407,12 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
   for (int k = k0; k < k1; ++k) {
     const double* S = slot(k);
     const int oc = (ty + 2) * RW + tx + 2;   // the own cell in a staged plane
-    if (ND == 3) prepare(k + 1);
+    if (ND == 3) {
+      prepare(k + 1);
+    } else {
+      set_tile(k);
+      prepare(k);
+    }
     // ---- z: slope at k+1 and the flux at k+1/2 of the own column (planes k, k+1 staged, k+2
     // from the lookahead, whose registers then take plane k+3's raw values)
     double divZ[V];
@@ -441,8 +469,8 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
       }
     }
     __syncthreads();
-    // every thread is past plane k-1's epilogue: its slot takes plane k+2
-    if (ND == 3 && tid == 0 && k >= k0 + 1 && k + 2 < k1) { issue(k + 2); ++issued; }
+    // every thread is past plane k-1's epilogue: its slot takes plane k+NSLOT-1
+    if (tid == 0 && k >= k0 + 1 && k + NSLOT - 1 < k1) { issue(k + NSLOT - 1); ++issued; }
     // ---- x and y interface fluxes of plane k: warp-sized chunks of items, each chunk of one
     // direction, so that the direction is a compile-time constant of the flux code
     auto xy_flux = [&](auto dir, int t) {
@@ -498,7 +526,7 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
     }
     __syncthreads();
     if (abort_flag) { aborted = true; break; }   // block-uniform: read after the barrier
-    if (ND == 3) prefetch_epilogue(k + 1);
+    prefetch_epilogue(k + 1);
     // ---- divergence, sources and the stage's consumer (no barrier after it: the slot of
     // plane k is next written after the following plane's slope barrier)
     if (own) {
@@ -511,7 +539,7 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
         rhs[v] = (divX + divY) + (ND == 3 ? divZ[v] : 0.0);
         R0[v] = S[v * RHW + oc];
       }
-      stage_cell_epilogue<ND, EU, PRIM>(A, i, j, k, R0, rhs, dt, cflv, errv, flags);
+      stage_cell_epilogue<ND, EU, PRIM>(A, i, j, ND == 3 ? k : 0, R0, rhs, dt, cflv, errv, flags);
     }
   }
 
@@ -542,10 +570,11 @@ __global__ void __launch_bounds__(TX* TY, MINB)
   tma_stage_tile<ND, EU, PRIM, TX, TY, LIM>(A, &tmap, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
-// Batched ensemble on the TMA layout: one block per tile of the flattened tile queue of many
-// independent grids, tile t = (grid, bx, by, bz); args[grid] are the grid's stage arguments and
-// maps[grid] the tensor map of its stage input (global memory, 64-byte aligned, written by the
-// host before the launch).
+// Batched ensemble on the TMA layout: one block per entry of the flattened queue of many
+// independent grids, entry (grid, bx, byb, 0) the column of kchunk tiles that a block of the
+// single-grid kernel computes; args[grid] are the grid's stage arguments and maps[grid] the
+// tensor map of its stage input (global memory, 64-byte aligned, written by the host before
+// the launch).
 template <int ND, bool EU, bool PRIM, int TX, int TY, int MINB, int LIM>
 __global__ void __launch_bounds__(TX* TY, MINB)
     batched_tma_stage_kernel(const StageArgs* __restrict__ args, const CUtensorMap* __restrict__ maps,

@@ -5,6 +5,7 @@
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <cstdlib>
 #include "fgpu_kernels.cuh"
 
 namespace fgpu {
@@ -21,12 +22,30 @@ cudaError_t tma_stage_launch_2d(bool euler, bool prim, int limiter, bool constan
                                 cudaStream_t s, const StageArgs& A, const CUtensorMap& map);
 cudaError_t tma_stage_launch_3d(bool euler, bool prim, int limiter, bool constant_recon, const Grid& g, int kchunk,
                                 cudaStream_t s, const StageArgs& A, const CUtensorMap& map);
-// Batched ensembles of 2D grids on the 32 x 8 TMA layout: one block per tile of the tile queue
-// (grid, bx, by, 0); args[grid] and maps[grid] (device arrays) the stage arguments and the
-// tensor map of the stage input of each grid; lim the compiled-in limiter shared by every grid
-// (compiled_limiter), 0 when the grids differ or read it from their arguments.
+// Batched ensembles of 2D grids on the 32 x 8 TMA layout: one block per entry (grid, bx, byb, 0)
+// of the block queue, the block computing tiles byb * kchunk .. of column bx of the grid, kchunk
+// taken from the grid's stage arguments; args[grid] and maps[grid] (device arrays) the stage
+// arguments and the tensor map of the stage input of each grid; lim the compiled-in limiter
+// shared by every grid (compiled_limiter), 0 when the grids differ or read it from their
+// arguments.
 cudaError_t tma_batched_launch_2d(bool euler, bool prim, int lim, const StageArgs* args, const CUtensorMap* maps,
                                   const int4* tiles, int ntiles, cudaStream_t s);
+// 2D TMA tiles computed by one block (a column of tiles whose boxes are double-buffered): as
+// many as keep about three waves of resident blocks on the device, at most 8; FGPU_TMA_TPB
+// fixes the count
+inline int tma_tiles_per_block(long long tiles, int blocks_per_sm) {
+  if (const char* e = std::getenv("FGPU_TMA_TPB")) {
+    const int v = std::atoi(e);
+    if (v > 0) return v;
+  }
+  static int sms = [] {
+    int d = 0, n = 148;
+    if (cudaGetDevice(&d) == cudaSuccess) cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, d);
+    return n > 0 ? n : 148;
+  }();
+  const long long per = tiles / (3LL * sms * blocks_per_sm);
+  return (int)(per < 1 ? 1 : (per > 8 ? 8 : per));
+}
 // the limiter code a stage's TMA kernel is compiled for: minmod, MC with theta = 1 (LIM_MC1),
 // van Leer; 0 when the kernel reads limiter, theta and reconstruction order from the arguments
 inline int compiled_limiter(int limiter, bool constant_recon, double theta) {

@@ -27,9 +27,18 @@ struct TmaKernel {
     batched_tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM><<<ntiles, kTmaTX * TY, SMEM, s>>>(args, maps, tiles);
   }
   static void launch(const Grid& g, int kchunk, cudaStream_t s, const StageArgs& A, const CUtensorMap& map) {
-    const int kz = ND == 3 ? (g.nz + kchunk - 1) / kchunk : 1;
-    dim3 grid((g.nx + kTmaTX - 1) / kTmaTX, (g.ny + TY - 1) / TY, kz);
-    tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM><<<grid, kTmaTX * TY, SMEM, s>>>(A, map);
+    const int tx = (g.nx + kTmaTX - 1) / kTmaTX, ty = (g.ny + TY - 1) / TY;
+    if (ND == 3) {
+      dim3 grid(tx, ty, (g.nz + kchunk - 1) / kchunk);
+      tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM><<<grid, kTmaTX * TY, SMEM, s>>>(A, map);
+    } else {
+      // 2D: each block computes a column of tma_tiles_per_block tiles, the next tile's box
+      // arriving while the current one is computed
+      StageArgs B = A;
+      B.kchunk = tma_tiles_per_block((long long)tx * ty, MINB);
+      dim3 grid(tx, (ty + B.kchunk - 1) / B.kchunk, 1);
+      tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM><<<grid, kTmaTX * TY, SMEM, s>>>(B, map);
+    }
   }
 };
 

@@ -53,13 +53,15 @@ def test_disk_ensemble_matches_single_grids(exact):
     b.close()
 
 
-@pytest.mark.parametrize("exact", [True, False])
-def test_disk_ensemble_tma_layout(exact, monkeypatch):
-    """The TMA-staged batched layout (6, one block per tile, tensor maps of every member's stage
-    inputs in a device table): every member equals its lone run on the TMA layout bit for bit,
-    and on the exact build also its lone run on the base tile."""
+@pytest.mark.parametrize("exact,tpb", [(True, None), (False, None), (True, 3)])
+def test_disk_ensemble_tma_layout(exact, tpb, monkeypatch):
+    """The TMA-staged batched layout (6, one block per column of tiles, tensor maps of every
+    member's stage inputs in a device table): every member equals its lone run on the TMA
+    layout bit for bit, and on the exact build also its lone run on the base tile."""
     from fosite_b200.sim import Batch
     monkeypatch.setenv("FGPU_STAGE_VARIANT", "6")
+    if tpb:
+        monkeypatch.setenv("FGPU_TMA_TPB", str(tpb))
     specs = _disk_specs(7)
     members = [_disk_member(*sp, exact=exact) for sp in specs]
     alone = [_disk_member(*sp, exact=exact) for sp in specs]

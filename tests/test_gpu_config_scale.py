@@ -62,11 +62,13 @@ def _check_status(g, pin, tag):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("variant", [None, 4, 6])
-def test_khi256_bitwise_1000_steps(variant, monkeypatch):
+@pytest.mark.parametrize("variant,tpb", [(None, None), (4, None), (6, None), (6, 4)])
+def test_khi256_bitwise_1000_steps(variant, tpb, monkeypatch):
     """KHI 256^2, SSPRK3: the exact build's state after 1 and 1000 steps is the oracle's bit for
-    bit (tuned layout, shared-memory tile, TMA-staged tile)."""
+    bit (tuned layout, shared-memory tile, TMA-staged tile, TMA tiles in columns of four)."""
     pin = _pin("khi256")
+    if tpb:
+        monkeypatch.setenv("FGPU_TMA_TPB", str(tpb))
     cfg, p, extra = problems.khi2d(n=256)
     g = _sim(cfg, p, extra, True, variant, monkeypatch)
     g.first_step()

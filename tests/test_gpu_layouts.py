@@ -60,6 +60,31 @@ def test_tma_layout_bitwise(name, monkeypatch):
     g.close()
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_tma_2d_tile_columns_bitwise(name, monkeypatch):
+    """2D blocks computing columns of three TMA tiles (the next tile's box in flight, the last
+    column partial where the tile rows do not divide): four steps equal the oracle's bit for
+    bit on the exact build."""
+    _force(monkeypatch, 6)
+    monkeypatch.setenv("FGPU_TMA_TPB", "3")
+    cfg, o, g = _pair(name, exact=True)
+    if cfg.knum > 1:
+        g.close()
+        pytest.skip("3D case: z-marching tiles")
+    tol = 1e-13 if _inexact(cfg) else 0.0
+    assert o.first_step() == 0
+    assert g.first_step() == 0
+    for s in range(4):
+        assert o.step() == g.step()
+        so, sg = o.status(), g.status()
+        assert sg.iter == so.iter and sg.n_adj == so.n_adj
+        if tol == 0.0:
+            assert sg.time == so.time and sg.dt == so.dt, (s, sg.time, so.time)
+        _compare(cfg, o, g, tol, "step %d" % s)
+    g.close()
+
+
 # 3D Dormand-Prince with at least three tiles (x: 32-wide tiles, y: 4- or 8-high tiles, z:
 # chunks of 16) in every direction, reflecting walls and a Gaussian pulse
 def _multi_tile():
