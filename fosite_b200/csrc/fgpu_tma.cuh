@@ -101,14 +101,16 @@ template <int ND> struct TmaSlots { static constexpr int N = ND == 3 ? 3 : 2; };
 
 // ------------------------------------------------------------------ the tile
 // LIM > 0: the limiter is compiled in (linear reconstruction with that limiter); LIM = 0: the
-// limiter and the reconstruction order are read from the arguments
-template <int ND, bool EU, bool PRIM, int TX, int TY, int LIM>
+// limiter and the reconstruction order are read from the arguments.  NT threads (at least
+// TX * TY; thread t owns cell (t % TX, t / TX) of the tile when t < TX * TY, the others share
+// the halo, slope and flux items)
+template <int ND, bool EU, bool PRIM, int TX, int TY, int LIM, int NT = TX * TY>
 __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtensorMap* tmap, const int bx, const int by,
                                                const int bz) {
   using PH = Phys<ND, EU>;
   using CE = Cells<ND, EU>;
   constexpr int V = PH::V;
-  constexpr int NT = TX * TY;
+  static_assert(NT >= TX * TY && NT % 32 == 0, "every cell of the tile needs a thread");
   constexpr int NSLOT = TmaSlots<ND>::N;
   using L = TmaLayout<V, TX, TY, NSLOT>;
   constexpr int RW = L::RW, RHW = L::RH * L::RW;
@@ -564,10 +566,10 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
   }
 }
 
-template <int ND, bool EU, bool PRIM, int TX, int TY, int MINB, int LIM>
-__global__ void __launch_bounds__(TX* TY, MINB)
+template <int ND, bool EU, bool PRIM, int TX, int TY, int MINB, int LIM, int NT = TX * TY>
+__global__ void __launch_bounds__(NT, MINB)
     tma_stage_kernel(const __grid_constant__ StageArgs A, const __grid_constant__ CUtensorMap tmap) {
-  tma_stage_tile<ND, EU, PRIM, TX, TY, LIM>(A, &tmap, blockIdx.x, blockIdx.y, blockIdx.z);
+  tma_stage_tile<ND, EU, PRIM, TX, TY, LIM, NT>(A, &tmap, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Batched ensemble on the TMA layout: one block per entry of the flattened queue of many
@@ -575,15 +577,25 @@ __global__ void __launch_bounds__(TX* TY, MINB)
 // single-grid kernel computes; args[grid] are the grid's stage arguments and maps[grid] the
 // tensor map of its stage input (global memory, 64-byte aligned, written by the host before
 // the launch).
-template <int ND, bool EU, bool PRIM, int TX, int TY, int MINB, int LIM>
-__global__ void __launch_bounds__(TX* TY, MINB)
+template <int ND, bool EU, bool PRIM, int TX, int TY, int MINB, int LIM, int NT = TX * TY>
+__global__ void __launch_bounds__(NT, MINB)
     batched_tma_stage_kernel(const StageArgs* __restrict__ args, const CUtensorMap* __restrict__ maps,
                              const int4* __restrict__ tiles) {
+  // the grid's arguments are copied into shared memory once per block: the tile then reads
+  // them at fixed shared offsets instead of through global-memory address arithmetic
+  __shared__ StageArgs sA;
+  static_assert(sizeof(StageArgs) % 8 == 0, "argument copy by 8-byte words");
   const int4 T = tiles[blockIdx.x];
   const CUtensorMap* map = maps + T.x;
   if (threadIdx.x == 0)
     asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
-  tma_stage_tile<ND, EU, PRIM, TX, TY, LIM>(args[T.x], map, T.y, T.z, T.w);
+  {
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(args + T.x);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sA);
+    for (int w = threadIdx.x; w < (int)(sizeof(StageArgs) / 8); w += NT) dst[w] = __ldg(src + w);
+  }
+  __syncthreads();
+  tma_stage_tile<ND, EU, PRIM, TX, TY, LIM, NT>(sA, map, T.y, T.z, T.w);
 }
 
 }  // namespace fgpu

@@ -14,30 +14,31 @@ template <int ND, int TY> struct TmaMinBlocks { static constexpr int N = ND == 3
 template <int ND, bool EU, bool PRIM, int TY, int LIM>
 struct TmaKernel {
   static constexpr int MINB = TmaMinBlocks<ND, TY>::N;
+  static constexpr int NTH = kTmaTX * TY;   // one thread per cell
   static constexpr size_t SMEM = TmaLayout<Phys<ND, EU>::V, kTmaTX, TY, TmaSlots<ND>::N>::SMEM;
   static void configure() {
-    cudaFuncSetAttribute(tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM>,
+    cudaFuncSetAttribute(tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM, NTH>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
     if (ND == 2 && TY == kTmaTY)
-      cudaFuncSetAttribute(batched_tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM>,
+      cudaFuncSetAttribute(batched_tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM, NTH>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
   }
   static void launch_batched(const StageArgs* args, const CUtensorMap* maps, const int4* tiles, int ntiles,
                              cudaStream_t s) {
-    batched_tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM><<<ntiles, kTmaTX * TY, SMEM, s>>>(args, maps, tiles);
+    batched_tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM, NTH><<<ntiles, NTH, SMEM, s>>>(args, maps, tiles);
   }
   static void launch(const Grid& g, int kchunk, cudaStream_t s, const StageArgs& A, const CUtensorMap& map) {
     const int tx = (g.nx + kTmaTX - 1) / kTmaTX, ty = (g.ny + TY - 1) / TY;
     if (ND == 3) {
       dim3 grid(tx, ty, (g.nz + kchunk - 1) / kchunk);
-      tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM><<<grid, kTmaTX * TY, SMEM, s>>>(A, map);
+      tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM, NTH><<<grid, NTH, SMEM, s>>>(A, map);
     } else {
       // 2D: each block computes a column of tma_tiles_per_block tiles, the next tile's box
       // arriving while the current one is computed
       StageArgs B = A;
       B.kchunk = tma_tiles_per_block((long long)tx * ty, MINB);
       dim3 grid(tx, (ty + B.kchunk - 1) / B.kchunk, 1);
-      tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM><<<grid, kTmaTX * TY, SMEM, s>>>(B, map);
+      tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM, NTH><<<grid, NTH, SMEM, s>>>(B, map);
     }
   }
 };
