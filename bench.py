@@ -339,7 +339,7 @@ def run_own(args, world, rank, local):
     if rank != 0:
         sim.close()
         if not args.no_extras:
-            run_ensemble(args, world, rank, local, emit=False)   # same collective steps as rank 0
+            run_ensemble(args, world, rank, local, emit=False, steps=ENSEMBLE_EXTRA_STEPS)   # as rank 0
             run_serve(args, world, rank, local, emit=False, rates=SERVE_EXTRA["rate"],
                       requests=SERVE_EXTRA["requests"], t_scale=1.0)
         return
@@ -403,11 +403,12 @@ def run_own(args, world, rank, local):
     sim.close()
     if not args.no_extras:
         # the batched ensemble against the loop of plain per-grid runs (96 disks), same steps
-        ens = run_ensemble(args, world, rank, local, emit=False)
+        ens = run_ensemble(args, world, rank, local, emit=False, steps=ENSEMBLE_EXTRA_STEPS)
         line["ensemble"] = {k: ens[k] for k in ("value", "unit", "ms_per_step", "speedup_vs_plain",
                                                   "speedup_vs_plain_tuned", "identical_to_plain", "identity_check",
                                                   "plain_loop", "plain_loop_tuned", "member_steps_per_s")}
         line["ensemble"]["layout"] = ens["config"]["variant"]
+        line["ensemble"]["steps"] = ens["steps"]
         line["ensemble"]["config"] = {k: ens["config"][k] for k in ("description", "members", "cells")}
         # one serving rate at the full problem times (t_scale 1): p50 / p99 time to solution
         srv = run_serve(args, world, rank, local, emit=False, rates=SERVE_EXTRA["rate"],
@@ -420,6 +421,9 @@ def run_own(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+# steps of the ensemble comparison in the default line: two 16-step graphs for the batch and for
+# every plain member, so that both loops replay captured graphs
+ENSEMBLE_EXTRA_STEPS = 32
 # the serving point of the default line: Poisson arrivals at 20 requests/s, 24 requests of the
 # full mix integrated to their full end times
 SERVE_EXTRA = {"rate": "20", "requests": 24}
@@ -443,12 +447,16 @@ def ensemble_members(n=96, seed=4000):
     return out
 
 
-def run_ensemble(args, world=1, rank=0, local=0, emit=True):
+def run_ensemble(args, world=1, rank=0, local=0, emit=True, steps=None):
     """Batched ensemble against a loop of plain per-grid runs of the same members.
 
     With N ranks the members are dealt round-robin to the GPUs (no collective in the
     step); the job time is the slowest rank's.  emit=False returns rank 0's line instead
-    of printing it (None on the other ranks)."""
+    of printing it (None on the other ranks); steps overrides --steps."""
+    import copy
+    if steps is not None:
+        args = copy.copy(args)
+        args.steps = steps
     import torch
     from fosite_b200 import abi, replicas
     from fosite_b200.sim import Batch, Simulation
