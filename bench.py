@@ -348,7 +348,7 @@ def run_own(args, world, rank, local):
     prof = load_traffic_profile(args.workload)
     traffic = None
     if prof and stp.stage_launches:
-        traffic = prof["dram_bytes_per_cell"] * n_cells
+        traffic = prof.get("by_layout", {}).get(str(variant), prof["dram_bytes_per_cell"]) * n_cells
     cb = cpu_baseline(args.workload, budget_s=args.cpu_budget) if world == 1 and not args.no_cpu else None
     bpc = algorithmic_bytes_per_cell_update(args.workload, sim.vnum)
     # where the time of a step goes: kernel time (every launch bracketed by events, direct
