@@ -5,10 +5,11 @@ Two variants are built from the same sources:
   lib/libfosite_gpu_exact.so  --fmad=false: every operation rounded as in the
                               reference's CPU build; used to prove bit-level
                               agreement with the CPU oracle
-Each variant links five translation units compiled in parallel: fgpu_host.cu (the C ABI, host
+Each variant links six translation units compiled in parallel: fgpu_host.cu (the C ABI, host
 drivers, boundary / FARGO / viscosity / Runge-Kutta control kernels), the shared-memory stage
 kernels of 2D and 3D meshes (fgpu_stage_2d.cu, fgpu_stage_3d.cu) and the TMA-staged stage
-kernels of 2D and 3D meshes (fgpu_tma_2d.cu, fgpu_tma_3d.cu).
+kernels (fgpu_tma_2d.cu: 2D 32 x 8 tiles and batches, fgpu_tma_2d4.cu: 2D 32 x 4 tiles,
+fgpu_tma_3d.cu).
 """
 import os
 import subprocess
@@ -19,7 +20,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 BUILDDIR = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-UNITS = ["fgpu_host.cu", "fgpu_stage_2d.cu", "fgpu_stage_3d.cu", "fgpu_tma_2d.cu", "fgpu_tma_3d.cu"]
+UNITS = ["fgpu_host.cu", "fgpu_stage_2d.cu", "fgpu_stage_3d.cu", "fgpu_tma_2d.cu", "fgpu_tma_2d4.cu", "fgpu_tma_3d.cu"]
 
 
 def nvcc():

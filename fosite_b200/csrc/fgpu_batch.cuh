@@ -22,6 +22,7 @@ struct fgpu_batch {
   int tma_lim = -1;              // compiled-in limiter of layout 6, -1 when the batch cannot use it
   int4* d_tcols = nullptr;       // layout 6: (member, bx, byb, 0), columns of kchunk tiles per block
   int ntcols = 0;
+  std::vector<char> tma_red;     // layout 6: per row of d_args, whether some member's stage reduces
   BndArgs* d_bnd = nullptr;      // [n]
   int4* d_tiles = nullptr;
   int ntiles = 0;
@@ -79,8 +80,9 @@ int launch_batched_stage(fgpu_batch* b, const StageArgs* args, int variant) {
   if (variant == 6) {   // TMA-staged tiles: tensor maps parallel to the step and probe tables
     if (!b->d_maps || args < b->d_args || args >= b->d_args + (size_t)(b->order + 1) * b->m.size())
       return bset_err(b, FGPU_EUNSUPPORTED, "the TMA layout serves fixed-step 2D batches only");
-    BCUDA_TRY(b, tma_batched_launch_2d(b->euler, b->prim, b->tma_lim, args, b->d_maps + (args - b->d_args),
-                                       b->d_tcols, b->ntcols, b->stream));
+    const size_t row = (size_t)(args - b->d_args) / b->m.size();
+    BCUDA_TRY(b, tma_batched_launch_2d(b->euler, b->prim, b->tma_lim, b->tma_red[row] != 0, args,
+                                       b->d_maps + (args - b->d_args), b->d_tcols, b->ntcols, b->stream));
     return FGPU_OK;
   }
   // the shared-memory base tile of the batch's tile queue: layouts 0, 2, 3
@@ -656,6 +658,10 @@ int fgpu_batch_create(fgpu_handle* const* members, int n, fgpu_batch** out) {
       }
       for (auto& A : args) A.kchunk = tpb;
       b->ntcols = (int)cols.size();
+      // stages whose arguments reduce CFL / CheckData / error maxima for some member
+      b->tma_red.assign(b->order + 1, 0);
+      for (size_t q = 0; q < args.size(); ++q)
+        if (args[q].cfl_mode || args[q].last_stage || args[q].err_low) b->tma_red[q / n] = 1;
       if (cudaMalloc(&b->d_maps, sizeof(CUtensorMap) * maps.size()) != cudaSuccess ||
           cudaMemcpy(b->d_maps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
           cudaMalloc(&b->d_tcols, sizeof(int4) * cols.size()) != cudaSuccess ||

@@ -103,8 +103,10 @@ template <int ND> struct TmaSlots { static constexpr int N = ND == 3 ? 3 : 2; };
 // LIM > 0: the limiter is compiled in (linear reconstruction with that limiter); LIM = 0: the
 // limiter and the reconstruction order are read from the arguments.  NT threads (at least
 // TX * TY; thread t owns cell (t % TX, t / TX) of the tile when t < TX * TY, the others share
-// the halo, slope and flux items)
-template <int ND, bool EU, bool PRIM, int TX, int TY, int LIM, int NT = TX * TY>
+// the halo, slope and flux items).  RED = false: a stage without CFL, CheckData or error-norm
+// reduction (cfl_mode 0, not the last stage, no err_low), whose maxima are then dead code and
+// hold no registers across the planes.
+template <int ND, bool EU, bool PRIM, int TX, int TY, int LIM, int NT = TX * TY, bool RED = true>
 __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtensorMap* tmap, const int bx, const int by,
                                                const int bz) {
   using PH = Phys<ND, EU>;
@@ -557,7 +559,7 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
     return;
   }
   const bool err_out = A.last_stage || A.err_low;
-  if (A.ctl && (A.cfl_mode || err_out)) {
+  if (RED && A.ctl && (A.cfl_mode || err_out)) {
     int nv = A.cfl_mode ? (M.vis ? 4 : (ND == 3 ? 3 : 1)) : 0;
     double vals[4] = {cflv[0], cflv[1], cflv[2], cflv[3]};
     if (err_out && !A.cfl_mode) { vals[0] = errv; nv = 1; }
@@ -566,10 +568,10 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
   }
 }
 
-template <int ND, bool EU, bool PRIM, int TX, int TY, int MINB, int LIM, int NT = TX * TY>
+template <int ND, bool EU, bool PRIM, int TX, int TY, int MINB, int LIM, int NT = TX * TY, bool RED = true>
 __global__ void __launch_bounds__(NT, MINB)
     tma_stage_kernel(const __grid_constant__ StageArgs A, const __grid_constant__ CUtensorMap tmap) {
-  tma_stage_tile<ND, EU, PRIM, TX, TY, LIM, NT>(A, &tmap, blockIdx.x, blockIdx.y, blockIdx.z);
+  tma_stage_tile<ND, EU, PRIM, TX, TY, LIM, NT, RED>(A, &tmap, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Batched ensemble on the TMA layout: one block per entry of the flattened queue of many
@@ -577,7 +579,7 @@ __global__ void __launch_bounds__(NT, MINB)
 // single-grid kernel computes; args[grid] are the grid's stage arguments and maps[grid] the
 // tensor map of its stage input (global memory, 64-byte aligned, written by the host before
 // the launch).
-template <int ND, bool EU, bool PRIM, int TX, int TY, int MINB, int LIM, int NT = TX * TY>
+template <int ND, bool EU, bool PRIM, int TX, int TY, int MINB, int LIM, int NT = TX * TY, bool RED = true>
 __global__ void __launch_bounds__(NT, MINB)
     batched_tma_stage_kernel(const StageArgs* __restrict__ args, const CUtensorMap* __restrict__ maps,
                              const int4* __restrict__ tiles) {
@@ -595,7 +597,7 @@ __global__ void __launch_bounds__(NT, MINB)
     for (int w = threadIdx.x; w < (int)(sizeof(StageArgs) / 8); w += NT) dst[w] = __ldg(src + w);
   }
   __syncthreads();
-  tma_stage_tile<ND, EU, PRIM, TX, TY, LIM, NT>(sA, map, T.y, T.z, T.w);
+  tma_stage_tile<ND, EU, PRIM, TX, TY, LIM, NT, RED>(sA, map, T.y, T.z, T.w);
 }
 
 }  // namespace fgpu

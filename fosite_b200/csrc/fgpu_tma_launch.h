@@ -28,8 +28,14 @@ cudaError_t tma_stage_launch_3d(bool euler, bool prim, int limiter, bool constan
 // arguments and the tensor map of the stage input of each grid; lim the compiled-in limiter
 // shared by every grid (compiled_limiter), 0 when the grids differ or read it from their
 // arguments.
-cudaError_t tma_batched_launch_2d(bool euler, bool prim, int lim, const StageArgs* args, const CUtensorMap* maps,
-                                  const int4* tiles, int ntiles, cudaStream_t s);
+// red: some grid's stage reduces CFL / CheckData / error-norm maxima (else the kernel form without
+// the reductions runs).
+cudaError_t tma_batched_launch_2d(bool euler, bool prim, int lim, bool red, const StageArgs* args,
+                                  const CUtensorMap* maps, const int4* tiles, int ntiles, cudaStream_t s);
+// the 32 x 4 tiles (own translation unit)
+cudaError_t tma_stage_launch_2d4(bool euler, bool prim, int limiter, bool constant_recon, const Grid& g,
+                                 cudaStream_t s, const StageArgs& A, const CUtensorMap& map);
+void tma_stage_configure_2d4(bool euler, bool prim);
 // 2D TMA tiles computed by one block (a column of tiles whose boxes are double-buffered): as
 // many as keep about three waves of resident blocks on the device, at most 8; FGPU_TMA_TPB
 // fixes the count

@@ -1,5 +1,5 @@
-// fgpu_tma_nd.cuh -- instantiations of the TMA-staged stage kernel for one dimensionality
-// (included by fgpu_tma_2d.cu and fgpu_tma_3d.cu).
+// fgpu_tma_nd.cuh -- instantiations of the TMA-staged stage kernel for one dimensionality and
+// tile height (included by fgpu_tma_2d.cu, fgpu_tma_2d4.cu and fgpu_tma_3d.cu).
 #pragma once
 #include "fgpu_tma.cuh"
 #include "fgpu_tma_launch.h"
@@ -11,34 +11,51 @@ namespace {
 // three (2D), the 32 x 4 tile (2D) six
 template <int ND, int TY> struct TmaMinBlocks { static constexpr int N = ND == 3 ? 2 : (TY == 4 ? 6 : 3); };
 
+// a stage that reduces CFL / CheckData / error-norm maxima; the others run the kernel form whose
+// maxima are compiled out (their registers go to the stencil: 10% on the 3D Butcher stages)
+inline bool stage_reduces(const StageArgs& A) { return A.cfl_mode || A.last_stage || A.err_low; }
+
 template <int ND, bool EU, bool PRIM, int TY, int LIM>
 struct TmaKernel {
   static constexpr int MINB = TmaMinBlocks<ND, TY>::N;
   static constexpr int NTH = kTmaTX * TY;   // one thread per cell
   static constexpr size_t SMEM = TmaLayout<Phys<ND, EU>::V, kTmaTX, TY, TmaSlots<ND>::N>::SMEM;
-  static void configure() {
-    cudaFuncSetAttribute(tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM, NTH>,
+  template <bool RED>
+  static void configure_red() {
+    cudaFuncSetAttribute(tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM, NTH, RED>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
-    if (ND == 2 && TY == kTmaTY)
-      cudaFuncSetAttribute(batched_tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM, NTH>,
+    if constexpr (ND == 2 && TY == kTmaTY)
+      cudaFuncSetAttribute(batched_tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM, NTH, RED>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
   }
-  static void launch_batched(const StageArgs* args, const CUtensorMap* maps, const int4* tiles, int ntiles,
+  static void configure() {
+    configure_red<true>();
+    configure_red<false>();
+  }
+  static void launch_batched(bool red, const StageArgs* args, const CUtensorMap* maps, const int4* tiles, int ntiles,
                              cudaStream_t s) {
-    batched_tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM, NTH><<<ntiles, NTH, SMEM, s>>>(args, maps, tiles);
+    if constexpr (ND == 2 && TY == kTmaTY) {
+      if (red)
+        batched_tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM, NTH, true><<<ntiles, NTH, SMEM, s>>>(args, maps, tiles);
+      else
+        batched_tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM, NTH, false><<<ntiles, NTH, SMEM, s>>>(args, maps, tiles);
+    }
   }
   static void launch(const Grid& g, int kchunk, cudaStream_t s, const StageArgs& A, const CUtensorMap& map) {
     const int tx = (g.nx + kTmaTX - 1) / kTmaTX, ty = (g.ny + TY - 1) / TY;
-    if (ND == 3) {
+    const bool red = stage_reduces(A);
+    if constexpr (ND == 3) {
       dim3 grid(tx, ty, (g.nz + kchunk - 1) / kchunk);
-      tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM, NTH><<<grid, NTH, SMEM, s>>>(A, map);
+      if (red) tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM, NTH, true><<<grid, NTH, SMEM, s>>>(A, map);
+      else tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM, NTH, false><<<grid, NTH, SMEM, s>>>(A, map);
     } else {
       // 2D: each block computes a column of tma_tiles_per_block tiles, the next tile's box
       // arriving while the current one is computed
       StageArgs B = A;
       B.kchunk = tma_tiles_per_block((long long)tx * ty, MINB);
       dim3 grid(tx, (ty + B.kchunk - 1) / B.kchunk, 1);
-      tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM, NTH><<<grid, NTH, SMEM, s>>>(B, map);
+      if (red) tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM, NTH, true><<<grid, NTH, SMEM, s>>>(B, map);
+      else tma_stage_kernel<ND, EU, PRIM, kTmaTX, TY, MINB, LIM, NTH, false><<<grid, NTH, SMEM, s>>>(B, map);
     }
   }
 };
@@ -78,13 +95,13 @@ cudaError_t launch_nd(bool euler, bool prim, int limiter, bool constant_recon, c
 }
 
 template <int ND, bool EU, bool PRIM>
-void launch_batched_lim(int lim, const StageArgs* args, const CUtensorMap* maps, const int4* tiles, int ntiles,
-                        cudaStream_t s) {
+void launch_batched_lim(int lim, bool red, const StageArgs* args, const CUtensorMap* maps, const int4* tiles,
+                        int ntiles, cudaStream_t s) {
   switch (lim) {
-    case LIM_MINMOD: TmaKernel<ND, EU, PRIM, kTmaTY, LIM_MINMOD>::launch_batched(args, maps, tiles, ntiles, s); break;
-    case LIM_MC1: TmaKernel<ND, EU, PRIM, kTmaTY, LIM_MC1>::launch_batched(args, maps, tiles, ntiles, s); break;
-    case LIM_VANLEER: TmaKernel<ND, EU, PRIM, kTmaTY, LIM_VANLEER>::launch_batched(args, maps, tiles, ntiles, s); break;
-    default: TmaKernel<ND, EU, PRIM, kTmaTY, 0>::launch_batched(args, maps, tiles, ntiles, s); break;
+    case LIM_MINMOD: TmaKernel<ND, EU, PRIM, kTmaTY, LIM_MINMOD>::launch_batched(red, args, maps, tiles, ntiles, s); break;
+    case LIM_MC1: TmaKernel<ND, EU, PRIM, kTmaTY, LIM_MC1>::launch_batched(red, args, maps, tiles, ntiles, s); break;
+    case LIM_VANLEER: TmaKernel<ND, EU, PRIM, kTmaTY, LIM_VANLEER>::launch_batched(red, args, maps, tiles, ntiles, s); break;
+    default: TmaKernel<ND, EU, PRIM, kTmaTY, 0>::launch_batched(red, args, maps, tiles, ntiles, s); break;
   }
 }
 
