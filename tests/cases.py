@@ -335,6 +335,45 @@ def _axis_disk(n=(28, 36), euler=False, seed=91):
     return c, p, {}
 
 
+def _axis_cyl3d(n=(16, 20, 12), seed=93):
+    """A 3D cylindrical mesh (r, phi, z) reaching the axis: AXIS at r = 0, reflecting at r = 1,
+    periodic in phi, reflecting in z; isothermal rotating gas with a density bump."""
+    c = abi.default_config()
+    c.inum, c.jnum, c.knum = n
+    c.geometry = abi.CYLINDRICAL
+    c.xmin, c.xmax, c.ymin, c.ymax, c.zmin, c.zmax = 0.0, 1.0, -np.pi, np.pi, 0.0, 1.0
+    c.physics = abi.EULER_ISOTHERM
+    c.csiso = 0.5
+    c.limiter = abi.VANLEER
+    c.variables = abi.PRIMITIVE
+    c.method = abi.MODIFIED_EULER
+    c.tdorder = 3
+    c.tol_rel = 10.0
+    c.cfl = 0.4
+    c.stoptime = 1.0e3
+    c.bc[:6] = [abi.AXIS, abi.REFLECTING, abi.PERIODIC, abi.PERIODIC, abi.REFLECTING, abi.REFLECTING]
+    abi.finalize_config(c)
+    X, Y, Z, _ = problems.centers(c)
+    rng = np.random.default_rng(seed)
+    p = np.zeros((4,) + X.shape)
+    p[0] = (1.0 + 0.3 * np.exp(-((X - 0.4) ** 2 + (Z - 0.5) ** 2) / 0.02) * (1 + np.cos(Y))
+            + 0.01 * rng.uniform(-1, 1, X.shape))
+    p[1] = 0.05 * rng.uniform(-1, 1, X.shape)
+    p[2] = 0.5 * X * np.exp(-X ** 2) + 0.02 * rng.uniform(-1, 1, X.shape)
+    p[3] = 0.02 * rng.uniform(-1, 1, X.shape)
+    return c, p, {}
+
+
+def _axis_fargo(n=(28, 36), fargo=1, seed=95):
+    """The axis disk with FARGO transport along phi (type 1: the background velocity includes
+    the axis ghost columns)."""
+    c, p, extra = _axis_disk(n=n, seed=seed)
+    c.fargo_method = fargo
+    c.fargo_direction = 2
+    abi.finalize_config(c)
+    return c, p, extra
+
+
 def khi_fargo(fargo, direction=1, n=(24, 24), visc=False, seed=11):
     """tests/KHI2D.f90's FARGO legs (:81-150, config :168-245, InitData :300-360): ideal-gas KHI,
     KT + MONOCENT (theta 1.2) on conservative variables, periodic box, FARGO type 1 or 2 along
@@ -411,6 +450,8 @@ CASES = {
     "euler_fargo_shear_cons": lambda: _euler_fargo(),
     "khi_fargo1_x": lambda: khi_fargo(1, n=(28, 24)),
     "iso_axis_cyl": lambda: _axis_disk(),
+    "iso_axis_cyl3d": lambda: _axis_cyl3d(),
+    "iso_axis_cyl_fargo": lambda: _axis_fargo(),
     "euler_axis_cyl_dopri": lambda: _butcher(_axis_disk(n=(24, 32), euler=True), abi.DORMAND_PRINCE, 5, 1e-4),
     "disk_fargo_ssprk5_logcyl": lambda: _butcher(_disk_fargo(), abi.SSPRK, 5),
     "disk_fargo2_dopri_cyl": lambda: _butcher(_disk_fargo2(), abi.DORMAND_PRINCE, 5, 1e-4),
