@@ -157,7 +157,7 @@ __device__ __forceinline__ void prefetch_l2(const double* p) {
 // solutions and error norm, CheckData and CFL partial maxima).  R0: the cell's reconstruction
 // variables; rhs: (divX + divY) + divZ on entry, the full right-hand side after the sources.
 // Shared by the stage kernels of every tile layout.
-template <int ND, bool EU, bool PRIM>
+template <int ND, bool EU, bool PRIM, bool KSEQ = false>
 __device__ __forceinline__ void stage_cell_epilogue(const StageArgs& A, const int i, const int j, const int k,
                                                     const double* R0, double* rhs, const double dt, double* cflv,
                                                     double& errv, int& flags) {
@@ -310,14 +310,21 @@ __device__ __forceinline__ void stage_cell_epilogue(const StageArgs& A, const in
       double u[V];
 #pragma unroll
       for (int v = 0; v < V; ++v) u[v] = __ldg(S.base + (long long)v * g.n + idx);
-      // the earlier stages' k (unrolled to the tableau limit, so all loads issue together)
+      // the earlier stages' k: unrolled to the tableau limit, so that all loads issue together,
+      // or (KSEQ: kernels short of registers, whose streams the L2 prefetch has brought in) one
+      // k at a time
+      auto kterm = [&](int q) {
+        const double a = S.dt_dev ? S.coef[q] * *S.dt_dev : S.coef[q];
 #pragma unroll
-      for (int q = 0; q < FGPU_MAXK - 1; ++q) {
-        if (q + 1 < S.nk) {
-          const double a = S.dt_dev ? S.coef[q] * *S.dt_dev : S.coef[q];
+        for (int v = 0; v < V; ++v) u[v] = u[v] - a * __ldg(S.K[q] + (long long)v * g.n + idx);
+      };
+      if (KSEQ) {
+#pragma unroll 1
+        for (int q = 0; q + 1 < S.nk; ++q) kterm(q);
+      } else {
 #pragma unroll
-          for (int v = 0; v < V; ++v) u[v] = u[v] - a * __ldg(S.K[q] + (long long)v * g.n + idx);
-        }
+        for (int q = 0; q < FGPU_MAXK - 1; ++q)
+          if (q + 1 < S.nk) kterm(q);
       }
       {
         const double a = S.dt_dev ? S.coef[S.nk - 1] * *S.dt_dev : S.coef[S.nk - 1];
@@ -434,18 +441,23 @@ __device__ __forceinline__ void stage_cell_epilogue(const StageArgs& A, const in
     double hi[V], lo[V];
 #pragma unroll
     for (int v = 0; v < V; ++v) hi[v] = lo[v] = __ldg(A.in.base + (long long)v * g.n + idx);
+    auto kterm = [&](int q) {
+      const double bh = dtd ? A.bh_dt[q] * *dtd : A.bh_dt[q];
+      const double bl = dtd ? A.bl_dt[q] * *dtd : A.bl_dt[q];
 #pragma unroll
-    for (int q = 0; q < FGPU_MAXK - 1; ++q) {
-      if (q + 1 < A.nstage) {
-        const double bh = dtd ? A.bh_dt[q] * *dtd : A.bh_dt[q];
-        const double bl = dtd ? A.bl_dt[q] * *dtd : A.bl_dt[q];
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-          const double kq = __ldg(A.in.K[q] + (long long)v * g.n + idx);
-          lo[v] = lo[v] - bl * kq;
-          hi[v] = hi[v] - bh * kq;
-        }
+      for (int v = 0; v < V; ++v) {
+        const double kq = __ldg(A.in.K[q] + (long long)v * g.n + idx);
+        lo[v] = lo[v] - bl * kq;
+        hi[v] = hi[v] - bh * kq;
       }
+    };
+    if (KSEQ) {
+#pragma unroll 1
+      for (int q = 0; q + 1 < A.nstage; ++q) kterm(q);
+    } else {
+#pragma unroll
+      for (int q = 0; q < FGPU_MAXK - 1; ++q)
+        if (q + 1 < A.nstage) kterm(q);
     }
     {
       const int q = A.nstage - 1;

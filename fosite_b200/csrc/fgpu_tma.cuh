@@ -15,7 +15,10 @@
 //     boundary_generic.f90:287-418), the z ghosts of the own column come from the same
 //     rules;
 //   * the own column's z neighbours come from the ring (planes k, k+1) and a register
-//     lookahead (plane k+2, loaded one plane early);
+//     lookahead (plane k+2, loaded one plane early); its z slope and flux are computed after
+//     the plane's x-y fluxes, right before the epilogue that consumes them;
+//   * stages that reduce nothing (no CFL, CheckData or error norm) run a form of the kernel
+//     whose maxima are compiled out: registers decide the speed of this kernel;
 //   * the epilogue's streams (base and earlier k of a Butcher stage, the Shu-Osher start
 //     state) are brought into L2 one plane ahead by bulk prefetches, one tile row per thread;
 //   * the x and y interface fluxes run in warp-sized chunks of one direction each, so that
@@ -301,6 +304,7 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
     if (tid == 0) waited = kp + 1 - k0;
     if (prep_sync) {
       double* S = slot(kp);
+
       constexpr int NXB = (TX + 4) * TY, NYB = TX * 4;
       for (int t = tid; t < NXB + NYB; t += NT) {
         int lx, ly;
@@ -417,32 +421,6 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
       set_tile(k);
       prepare(k);
     }
-    // ---- z: slope at k+1 and the flux at k+1/2 of the own column (planes k, k+1 staged, k+2
-    // from the lookahead, whose registers then take plane k+3's raw values)
-    double divZ[V];
-    if (ND == 3 && own) {
-      const double* S1 = slot(k + 1);
-      col_finish(k + 2, la);
-      double sz1[V], RL[V], RR[V], Fzp[V];
-      const double oT = M.offzT[k + 2], oB = M.offzB[k + 1 + 2];
-#pragma unroll
-      for (int v = 0; v < V; ++v) {
-        const double r0 = S[v * RHW + oc], r1 = S1[v * RHW + oc];
-        sz1[v] = crec ? 0.0 : slope(lim, A.theta, A.invd[2], r0, r1, la[v]);
-        RL[v] = crec ? r0 : r0 + sz0[v] * oT;
-        RR[v] = crec ? r1 : r1 + sz1[v] * oB;
-      }
-      col_load(k + 3, la);
-      kt_flux<ND, EU, PRIM, 2>(2, RL, RR, EU ? 0.0 : M.cs[6 * M.nxp + ip], EU ? 0.0 : M.cs[5 * M.nxp + ip],
-                               M.dAzB[ip], P, Fzp);
-      const double dVz = M.dxdydV[ip];
-#pragma unroll
-      for (int v = 0; v < V; ++v) {
-        divZ[v] = dVz * (Fzp[v] - Fzm[v]);
-        Fzm[v] = Fzp[v];
-        sz0[v] = sz1[v];
-      }
-    }
     // ---- x and y slopes of plane k: items over the full tile shape (ey rows x ex+2 cells for x,
     // ey+2 rows x ex cells for y), one code path for both directions, the ones outside a
     // partial edge tile skipped
@@ -531,6 +509,33 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
     __syncthreads();
     if (abort_flag) { aborted = true; break; }   // block-uniform: read after the barrier
     prefetch_epilogue(k + 1);
+    double divZ[V];
+    // ---- z: slope at k+1 and the flux at k+1/2 of the own column (planes k, k+1 staged, k+2
+    // from the lookahead, whose registers then take plane k+3's raw values), computed after
+    // the x-y fluxes so that divZ is live only into the epilogue (5% on the 3D stage)
+    if (ND == 3 && own) {
+      const double* S1 = slot(k + 1);
+      col_finish(k + 2, la);
+      double sz1[V], RL[V], RR[V], Fzp[V];
+      const double oT = M.offzT[k + 2], oB = M.offzB[k + 1 + 2];
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const double r0 = S[v * RHW + oc], r1 = S1[v * RHW + oc];
+        sz1[v] = crec ? 0.0 : slope(lim, A.theta, A.invd[2], r0, r1, la[v]);
+        RL[v] = crec ? r0 : r0 + sz0[v] * oT;
+        RR[v] = crec ? r1 : r1 + sz1[v] * oB;
+      }
+      col_load(k + 3, la);
+      kt_flux<ND, EU, PRIM, 2>(2, RL, RR, EU ? 0.0 : M.cs[6 * M.nxp + ip], EU ? 0.0 : M.cs[5 * M.nxp + ip],
+                               M.dAzB[ip], P, Fzp);
+      const double dVz = M.dxdydV[ip];
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        divZ[v] = dVz * (Fzp[v] - Fzm[v]);
+        Fzm[v] = Fzp[v];
+        sz0[v] = sz1[v];
+      }
+    }
     // ---- divergence, sources and the stage's consumer (no barrier after it: the slot of
     // plane k is next written after the following plane's slope barrier)
     if (own) {
@@ -543,7 +548,7 @@ __device__ __forceinline__ void tma_stage_tile(const StageArgs& A, const CUtenso
         rhs[v] = (divX + divY) + (ND == 3 ? divZ[v] : 0.0);
         R0[v] = S[v * RHW + oc];
       }
-      stage_cell_epilogue<ND, EU, PRIM>(A, i, j, ND == 3 ? k : 0, R0, rhs, dt, cflv, errv, flags);
+      stage_cell_epilogue<ND, EU, PRIM, ND == 3>(A, i, j, ND == 3 ? k : 0, R0, rhs, dt, cflv, errv, flags);
     }
   }
 
