@@ -163,6 +163,10 @@ struct fgpu_handle {
   bool materialize = true;      // Butcher stages: form the stage's reconstruction variables once per cell
   bool fuse_form = true;        // ... stage m's kernel forms stage m+1's (buffers alternate), only stage 2 by form_kernel
   bool fuse_end = true;         // the last stage's kernel also forms the high/low-order solutions and the error norm
+  // fixed-step Shu-Osher with primitive reconstruction: stage n < order also writes the
+  // primitive variables of its result (d_pform[(n-1)%2]), which stage n+1's stencil reads
+  bool so_form = false;
+  double* d_pform[2] = {nullptr, nullptr};
   double* d_ready = nullptr;    // ... into this array (one state)
   int variant = 0;              // stage kernel layout: 0 shared-memory tile, 1 warp-shuffle window,
                                 // 2/3 tile with a register cap for more resident blocks, 4 taller tile,
@@ -515,7 +519,7 @@ int launch_stage_t(fgpu_handle* h, StageArgs& A) {
   // (a variant-6 launch that the TMA layout does not serve runs on the base tile)
   const int variant =
       (h->variant == 1 && (h->fargo || h->accrete || h->vis || A.gate || A.fnext_out || A.cfl_mode == 3 ||
-                           A.flux_out))
+                           A.flux_out || A.out_prim))
           ? 0 : (h->variant >= 6 ? 0 : h->variant);
   if (ND == 3) CUDA_TRY(h, legacy_stage_launch_3d(EU, PRIM, variant, g, h->kchunk, h->stream, A));
   else CUDA_TRY(h, legacy_stage_launch_2d(EU, PRIM, variant, g, h->stream, A));
@@ -875,6 +879,14 @@ StageArgs shu_osher_stage(fgpu_handle* h, int n) {
   A.dt_dev = &h->d_ctl->dt;
   A.out = (n == h->order && h->order > 1) ? P : ((n % 2 == 1) ? Abuf : Bbuf);
   if (n == h->order) { A.cfl_mode = 1; A.cfl_roundtrip = h->roundtrip_cfg ? 1 : 0; }
+  if (h->so_form) {
+    // the primitive form of A (stage 1's result) and B (stage 2's) beside the states
+    if (n < h->order) A.out_prim = h->d_pform[(n - 1) % 2];
+    if (n >= 2) {
+      A.rin = plain_state(h->d_pform[(n - 2) % 2], false);
+      A.rin.ready = 1;
+    }
+  }
   return A;
 }
 
@@ -1679,6 +1691,9 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
     if (const char* e = std::getenv("FGPU_MATERIALIZE")) h->materialize = std::atoi(e) != 0;
     if (const char* e = std::getenv("FGPU_FUSE_FORM")) h->fuse_form = std::atoi(e) != 0;
     if (const char* e = std::getenv("FGPU_FUSE_END")) h->fuse_end = std::atoi(e) != 0;
+    // FGPU_FORM_SO=0 converts every staged point of the Shu-Osher stages instead
+    h->so_form = true;
+    if (const char* e = std::getenv("FGPU_FORM_SO")) h->so_form = std::atoi(e) != 0;
     // FARGO with a Butcher scheme: the stencil forms each stage state with its frame changes
     if (h->fargo && h->butcher) h->materialize = false;
     h->fuse_form = h->fuse_form && h->materialize;
@@ -1708,6 +1723,15 @@ int fgpu_create(const fgpu_config* cfg, int device, fgpu_handle** out) {
       cudaMemsetAsync(p, 0, bytes, h->stream);
       h->buf.push_back(p);
     }
+  }
+  // the primitive forms of the Shu-Osher stage results (fixed step, primitive reconstruction,
+  // no frame changes, accretion rows or viscous source between the stages)
+  h->so_form = h->so_form && h->prim && !h->butcher && !h->adaptive_me && !h->fargo && !h->accrete && !h->vis &&
+               h->order >= 2;
+  for (int b = 0; b < (h->order >= 3 ? 2 : 1) && !rc && h->so_form; ++b) {
+    size_t bytes = sizeof(double) * h->V * h->g.n;
+    if (cudaMalloc(&h->d_pform[b], bytes) != cudaSuccess) rc = set_err(h, FGPU_ENOMEM, "device memory for state arrays");
+    else cudaMemsetAsync(h->d_pform[b], 0, bytes, h->stream);
   }
   if (!rc && h->accrete) {
     size_t na = 3 * (size_t)h->g.ny + 2;
@@ -1774,6 +1798,7 @@ void fgpu_destroy(fgpu_handle* h) {
   if (h->graph) cudaGraphExecDestroy(h->graph);
   if (h->bt_graph) cudaGraphExecDestroy(h->bt_graph);
   for (double* p : h->buf) cudaFree(p);
+  for (double* p : h->d_pform) if (p) cudaFree(p);
   if (h->d_pad) cudaFree(h->d_pad);
   if (h->d_flux) cudaFree(h->d_flux);
   if (h->d_metric) cudaFree(h->d_metric);

@@ -64,6 +64,10 @@ struct StageArgs {
   // err_low (ComputeError, timedisc_base.f90:1012-1053) reduced into ctl->err
   double* out2;
   double eta2;
+  // Shu-Osher stage followed by another (primitive reconstruction): the new state's
+  // primitive variables, which the next stage's stencil reads ready-made (its rin, ready = 1)
+  // instead of converting every staged point; null = off
+  double* out_prim;
   const double* err_low;
   Chain err_chain;         // FARGO: frame changes of err_low before the comparison
   // point-mass accretion: the boundary row of this RHS through the outbound x face,
@@ -369,6 +373,13 @@ __device__ __forceinline__ void stage_cell_epilogue(const StageArgs& A, const in
     for (int v = 0; v < V; ++v) {
       y[v] = yn[v] - dt * rhs[v] + A.eta * (y0[v] - yn[v] + dt * rhs[v]);
       A.out[(long long)v * g.n + idx] = y[v];
+    }
+    if (PRIM && A.out_prim) {
+      // Cons2Prim of the new state, the conversion the next stage applies to its input
+      double p[V];
+      PH::c2p(y, p, P);
+#pragma unroll
+      for (int v = 0; v < V; ++v) A.out_prim[(long long)v * g.n + idx] = p[v];
     }
     if (A.out2) {
 #pragma unroll

@@ -77,7 +77,8 @@ STAGES = {abi.DORMAND_PRINCE: 7, abi.RK_FEHLBERG: 6, abi.CASH_KARP: 6, abi.SSPRK
 
 def footprint_bytes(cfg):
     """Device bytes of one admitted grid: its state arrays (stored state and two stage
-    scratch arrays for the fixed-step scheme; stored state, cold state, m k-arrays and the
+    scratch arrays for the fixed-step scheme, with primitive reconstruction their primitive
+    forms too; stored state, cold state, m k-arrays and the
     formed stage state for an embedded scheme of m stages), the padded download scratch, the
     metric and, with FARGO along y, the background-velocity terms."""
     nd = 3 if cfg.knum > 1 else 2
@@ -85,6 +86,8 @@ def footprint_bytes(cfg):
     n = cfg.inum * cfg.jnum * cfg.knum
     npad = (cfg.inum + 4) * (cfg.jnum + 4) * (cfg.knum + 4 if nd == 3 else 1)
     arrays = 3
+    if cfg.method == abi.MODIFIED_EULER and cfg.variables == abi.PRIMITIVE and cfg.tol_rel >= 1.0:
+        arrays += 2     # the primitive forms of the two scratch stage results
     if cfg.method != abi.MODIFIED_EULER:
         m = STAGES.get(cfg.method, 7)
         if cfg.method in (abi.RK_FEHLBERG, abi.SSPRK) and cfg.tdorder == 3:
